@@ -1,0 +1,477 @@
+// extern "C" entry points of libfhb200.so (declared in include/fhb200.h).
+#include <cstdio>
+#include <string>
+
+#include "../../include/fhb200.h"
+#include "fhb_kernels.cuh"
+#include "fhb_runners.h"
+
+struct fhb_context {
+  fhb::Context* impl;
+};
+
+namespace fhb {
+Context* build_context(int bits, int log_n, const uint64_t* moduli, int num_q, int num_p, int device,
+                       int* status);
+void destroy_context(Context* c);
+const char* last_error();
+
+namespace {
+
+constexpr int kMinLogN = 12;
+constexpr int kMaxLogN = 17;
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    cudaGetDevice(&prev_);
+    if (prev_ != device) cudaSetDevice(device);
+    dev_ = device;
+  }
+  ~DeviceGuard() {
+    if (prev_ != dev_) cudaSetDevice(prev_);
+  }
+
+ private:
+  int prev_ = 0, dev_ = 0;
+};
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+int check_ptr(const void* p, const char* name) {
+  if (!p) return fail(-2, std::string(name) + " is NULL");
+  if (!aligned16(p)) return fail(-2, std::string(name) + " is not 16-byte aligned");
+  return 0;
+}
+
+int check_level(const Context& c, int level) {
+  if (level < 0 || level >= c.num_q) return fail(-4, "level out of range [0, num_q)");
+  return 0;
+}
+
+uint32_t galois_inverse(uint32_t g, int log_n) {
+  // inverse of odd g modulo 2^(log_n + 1) by Newton iteration
+  uint64_t x = 1;
+  for (int i = 0; i < 6; ++i) x *= 2 - uint64_t(g) * x;
+  return uint32_t(x & ((uint64_t{2} << log_n) - 1));
+}
+
+int check_galois(const Context& c, uint32_t g) {
+  if (!(g & 1) || g >= (2u << c.log_n)) return fail(-5, "galois element must be odd and < 2N");
+  return 0;
+}
+
+int elementwise_grid(int64_t total) {
+  int64_t blocks = (total + 255) / 256;
+  const int64_t cap = 148 * 32;
+  return int(blocks < 1 ? 1 : (blocks > cap ? cap : blocks));
+}
+
+#define FHB_LOGN_SWITCH(T, FN, ...)                                   \
+  switch (c.log_n) {                                                  \
+    case 12: return FN<T, 12>(__VA_ARGS__);                           \
+    case 13: return FN<T, 13>(__VA_ARGS__);                           \
+    case 14: return FN<T, 14>(__VA_ARGS__);                           \
+    case 15: return FN<T, 15>(__VA_ARGS__);                           \
+    case 16: return FN<T, 16>(__VA_ARGS__);                           \
+    case 17: return FN<T, 17>(__VA_ARGS__);                           \
+    default: return fail(-7, "log_n outside the supported 12..17"); \
+  }
+
+#define FHB_DISPATCH(FN, ...)                 \
+  if (c.bits == 64) {                         \
+    FHB_LOGN_SWITCH(uint64_t, FN, __VA_ARGS__) \
+  } else {                                    \
+    FHB_LOGN_SWITCH(uint32_t, FN, __VA_ARGS__) \
+  }
+
+int forward(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool mont,
+            cudaStream_t st) {
+  FHB_DISPATCH(run_forward, c, in, out, polys, rows, row_start, mont, st);
+}
+int inverse(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
+            cudaStream_t st) {
+  FHB_DISPATCH(run_inverse, c, in, out, polys, rows, row_start, kind, st);
+}
+int mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
+             cudaStream_t st) {
+  FHB_DISPATCH(run_mul_coef, c, a, b, out, batch, level, st);
+}
+int ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
+            int level, cudaStream_t st) {
+  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st);
+}
+int prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st) {
+  FHB_DISPATCH(run_prepare, c, digits, prepared, batch, level, st);
+}
+int apply_prepared(const Context& c, const void* prepared, const void* key, void* acc0, void* acc1,
+                   int64_t batch, int level, uint32_t galois, cudaStream_t st) {
+  FHB_DISPATCH(run_apply_prepared, c, prepared, key, acc0, acc1, batch, level, galois, st);
+}
+
+template <typename T>
+int modup(const Context& c, const void* comp, void* digits, int64_t batch, int level, uint32_t galois,
+          cudaStream_t st) {
+  const int limbs = c.num_q - level;
+  const uint32_t ginv = galois == 1 ? 0u : galois_inverse(galois, c.log_n);
+  k_modup_digits<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
+      (const T*)comp, (T*)digits, batch, limbs, c.log_n, level, ginv, tables<T>(c), level_tables<T>(c, level));
+  return cuda_status(cudaGetLastError(), "k_modup_digits");
+}
+
+template <typename T>
+int moddown(const Context& c, const void* t0, const void* t1, const void* a0, const void* a1, void* out,
+            int64_t batch, int level, uint32_t add0_galois, int rescale, cudaStream_t st) {
+  const uint32_t ginv = add0_galois == 1 ? 0u : galois_inverse(add0_galois, c.log_n);
+  k_moddown<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
+      (const T*)t0, (const T*)t1, (const T*)a0, (const T*)a1, (T*)out, batch, c.log_n, level, c.num_q, c.num_p,
+      ginv, rescale, tables<T>(c), level_tables<T>(c, level));
+  return cuda_status(cudaGetLastError(), "k_moddown");
+}
+
+template <typename T>
+int rescale(const Context& c, const void* in, void* out, int64_t polys, int level, int nearest, cudaStream_t st) {
+  const int limbs = c.num_q - level;
+  k_rescale<T><<<elementwise_grid(polys * (limbs - 1) << c.log_n), 256, 0, st>>>(
+      (const T*)in, (T*)out, polys, limbs, c.log_n, level, nearest, tables<T>(c), level_tables<T>(c, level));
+  return cuda_status(cudaGetLastError(), "k_rescale");
+}
+
+template <typename T>
+int automorphism(const Context& c, const void* in, void* out, int64_t batch, int rows, int row_start,
+                 uint32_t galois, cudaStream_t st) {
+  k_automorphism<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
+      (const T*)in, (T*)out, batch, rows, row_start, c.log_n, galois_inverse(galois, c.log_n), tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_automorphism");
+}
+
+template <typename T>
+int add(const Context& c, const void* a, const void* b, void* out, int64_t polys, int level, int lazy,
+        cudaStream_t st) {
+  const int limbs = c.num_q - level;
+  k_add_canonical<T><<<elementwise_grid(polys * limbs << c.log_n), 256, 0, st>>>(
+      (const T*)a, (const T*)b, (T*)out, polys, limbs, c.log_n, level, lazy, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_add_canonical");
+}
+
+template <typename T>
+int mul_ntt(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
+            cudaStream_t st) {
+  const int limbs = c.num_q - level;
+  k_mul_ntt<T><<<elementwise_grid(batch * limbs << c.log_n), 256, 0, st>>>(
+      (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_mul_ntt");
+}
+
+template <typename T>
+int rns_binary(const Context& c, const void* a, const void* b, void* out, int64_t batch, int rows, int row_start,
+               int op, int b_mode, cudaStream_t st) {
+  k_rns_binary<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
+      (const T*)a, (const T*)b, (T*)out, batch, rows, row_start, c.log_n, op, b_mode, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_rns_binary");
+}
+
+template <typename T>
+int lift_signed(const Context& c, const void* x, void* out, int64_t batch, int rows, int row_start,
+                cudaStream_t st) {
+  k_lift_signed<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
+      (const int64_t*)x, (T*)out, batch, rows, row_start, c.log_n, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_lift_signed");
+}
+
+#define FHB_WORD(FN, ...) (c.bits == 64 ? FN<uint64_t>(__VA_ARGS__) : FN<uint32_t>(__VA_ARGS__))
+
+int64_t word_bytes(const Context& c) { return c.bits / 8; }
+
+struct Scratch {
+  char* coef;    // [3, B, L, N]
+  char* digits;  // [B, L, N]
+  char* t0;      // [B, L+P, N]
+  char* t1;      // [B, L+P, N]
+};
+
+Scratch carve(const Context& c, void* base, int64_t batch, int level) {
+  const int64_t w = word_bytes(c), n = c.n(), l = c.num_q - level, lp = l + c.num_p;
+  char* p = static_cast<char*>(base);
+  Scratch s;
+  s.coef = p;
+  s.digits = s.coef + 3 * batch * l * n * w;
+  s.t0 = s.digits + batch * l * n * w;
+  s.t1 = s.t0 + batch * lp * n * w;
+  return s;
+}
+
+}  // namespace
+}  // namespace fhb
+
+using fhb::Context;
+using fhb::fail;
+
+#define CTX_OR_FAIL()                                              \
+  if (!ctx || !ctx->impl) return fail(-1, "context is NULL");      \
+  const Context& c = *ctx->impl;                                   \
+  fhb::DeviceGuard guard_(c.device);                               \
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream)
+
+#define TRY(expr)                 \
+  do {                            \
+    int rc_ = (expr);             \
+    if (rc_ != 0) return rc_;     \
+  } while (0)
+
+extern "C" {
+
+int fhb_version(void) { return 1; }
+
+const char* fhb_last_error(void) { return fhb::last_error(); }
+
+int fhb_context_create(int residue_bits, int log_n, const uint64_t* moduli, int num_q, int num_p, int device,
+                       fhb_context** out) {
+  if (!out || !moduli) return fail(-2, "NULL argument");
+  if (residue_bits != 64 && residue_bits != 32) return fail(-2, "residue_bits must be 64 or 32");
+  if (log_n < fhb::kMinLogN || log_n > fhb::kMaxLogN) return fail(-7, "log_n outside the supported 12..17");
+  if (num_q < 1 || num_p < 1 || num_p > fhb::kMaxDigitWidth) return fail(-2, "need num_q >= 1 and 1 <= num_p <= 8");
+  const uint64_t bound = residue_bits == 64 ? (uint64_t{1} << 60) : (uint64_t{1} << 28);
+  for (int i = 0; i < num_q + num_p; ++i) {
+    const uint64_t q = moduli[i];
+    if (q < 3 || q >= bound || !(q & 1) || (q - 1) % (uint64_t{2} << log_n) != 0)
+      return fail(-2, "modulus " + std::to_string(i) + " is not an odd NTT prime below the word bound");
+  }
+  fhb::DeviceGuard guard(device);
+  int status = 0;
+  fhb::Context* c = fhb::build_context(residue_bits, log_n, moduli, num_q, num_p, device, &status);
+  if (!c) return status ? status : fail(-3, "context construction failed");
+  *out = new fhb_context{c};
+  return 0;
+}
+
+int fhb_context_destroy(fhb_context* ctx) {
+  if (!ctx) return 0;
+  fhb::destroy_context(ctx->impl);
+  delete ctx;
+  return 0;
+}
+
+int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi) {
+  if (!ctx || !ctx->impl || !psi) return fail(-1, "NULL argument");
+  if (prime_id < 0 || prime_id >= ctx->impl->qp()) return fail(-4, "prime id out of range");
+  *psi = ctx->impl->roots[prime_id];
+  return 0;
+}
+
+int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                    int input_montgomery, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return fhb::forward(c, in, out, batch * rows, rows, row_start, input_montgomery != 0, st);
+}
+
+int fhb_inverse_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                    int output_kind, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  if (output_kind < 0 || output_kind > 3) return fail(-2, "unknown inverse output kind");
+  return fhb::inverse(c, in, out, batch * rows, rows, row_start, output_kind, st);
+}
+
+int fhb_ckks_multiply(const fhb_context* ctx, const void* a, const void* b, void* out, int64_t batch, int level,
+                      fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(a, "a"));
+  TRY(fhb::check_ptr(b, "b"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_level(c, level));
+  return FHB_WORD(fhb::mul_ntt, c, a, b, out, batch, level, st);
+}
+
+int fhb_ckks_multiply_to_coefficient(const fhb_context* ctx, const void* a, const void* b, void* out,
+                                     int64_t batch, int level, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(a, "a"));
+  TRY(fhb::check_ptr(b, "b"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_level(c, level));
+  return fhb::mul_coef(c, a, b, out, batch, level, st);
+}
+
+int fhb_ckks_modup_digits(const fhb_context* ctx, const void* comp, void* digits, int64_t batch, int level,
+                          uint32_t galois, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(comp, "comp"));
+  TRY(fhb::check_ptr(digits, "digits"));
+  TRY(fhb::check_level(c, level));
+  TRY(fhb::check_galois(c, galois));
+  return FHB_WORD(fhb::modup, c, comp, digits, batch, level, galois, st);
+}
+
+int fhb_ckks_keyswitch_core(const fhb_context* ctx, const void* digits, const void* key, void* acc0, void* acc1,
+                            int64_t batch, int level, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(digits, "digits"));
+  TRY(fhb::check_ptr(key, "key"));
+  TRY(fhb::check_ptr(acc0, "acc0"));
+  TRY(fhb::check_ptr(acc1, "acc1"));
+  TRY(fhb::check_level(c, level));
+  return fhb::ks_core(c, digits, key, acc0, acc1, batch, level, st);
+}
+
+int fhb_ckks_moddown(const fhb_context* ctx, const void* t0, const void* t1, const void* add0, const void* add1,
+                     void* out, int64_t batch, int level, uint32_t add0_galois, int rescale, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(t0, "t0"));
+  TRY(fhb::check_ptr(t1, "t1"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_level(c, level));
+  TRY(fhb::check_galois(c, add0_galois));
+  if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
+  return FHB_WORD(fhb::moddown, c, t0, t1, add0, add1, out, batch, level, add0_galois, rescale, st);
+}
+
+int fhb_ckks_prepare_rotation(const fhb_context* ctx, const void* digits, void* prepared, int64_t batch, int level,
+                              fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(digits, "digits"));
+  TRY(fhb::check_ptr(prepared, "prepared"));
+  TRY(fhb::check_level(c, level));
+  return fhb::prepare(c, digits, prepared, batch, level, st);
+}
+
+int fhb_ckks_apply_prepared_rotation(const fhb_context* ctx, const void* prepared, const void* key, void* acc0,
+                                     void* acc1, int64_t batch, int level, uint32_t galois, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(prepared, "prepared"));
+  TRY(fhb::check_ptr(key, "key"));
+  TRY(fhb::check_ptr(acc0, "acc0"));
+  TRY(fhb::check_ptr(acc1, "acc1"));
+  TRY(fhb::check_level(c, level));
+  TRY(fhb::check_galois(c, galois));
+  return fhb::apply_prepared(c, prepared, key, acc0, acc1, batch, level, galois, st);
+}
+
+int fhb_ckks_rescale(const fhb_context* ctx, const void* in, void* out, int64_t polys, int level, int nearest,
+                     fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_level(c, level));
+  if (level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
+  return FHB_WORD(fhb::rescale, c, in, out, polys, level, nearest, st);
+}
+
+int fhb_ckks_automorphism(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                          uint32_t galois, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_galois(c, galois));
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  if (in == out) return fail(-2, "automorphism cannot run in place");
+  return FHB_WORD(fhb::automorphism, c, in, out, batch, rows, row_start, galois, st);
+}
+
+int fhb_ckks_add(const fhb_context* ctx, const void* a, const void* b, void* out, int64_t polys, int level,
+                 int lazy, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(a, "a"));
+  TRY(fhb::check_ptr(b, "b"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_level(c, level));
+  return FHB_WORD(fhb::add, c, a, b, out, polys, level, lazy, st);
+}
+
+int fhb_rns_binary(const fhb_context* ctx, int op, const void* a, const void* b, void* out, int64_t batch, int rows,
+                   int row_start, int b_mode, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(a, "a"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (op != fhb::kOpNegCanon) TRY(fhb::check_ptr(b, "b"));
+  if (op < 0 || op > fhb::kOpNegCanon) return fail(-2, "unknown RNS op");
+  if (b_mode < 0 || b_mode > 2) return fail(-2, "unknown operand broadcast mode");
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return FHB_WORD(fhb::rns_binary, c, a, b, out, batch, rows, row_start, op, b_mode, st);
+}
+
+int fhb_rns_lift_signed(const fhb_context* ctx, const int64_t* coefficients, void* out, int64_t batch, int rows,
+                        int row_start, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(coefficients, "coefficients"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return FHB_WORD(fhb::lift_signed, c, coefficients, out, batch, rows, row_start, st);
+}
+
+int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, int level) {
+  if (!ctx || !ctx->impl) return -1;
+  const Context& c = *ctx->impl;
+  if (level < 0 || level >= c.num_q || batch < 0) return -1;
+  const int64_t l = c.num_q - level, lp = l + c.num_p;
+  return (3 * l + l + 2 * lp) * batch * c.n() * fhb::word_bytes(c);
+}
+
+static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* key, const void* add0,
+                          const void* add1, uint32_t add0_galois, void* out, int64_t batch, int level, int rescale,
+                          cudaStream_t st) {
+  TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st));
+  return FHB_WORD(fhb::moddown, c, s.t0, s.t1, add0, add1, out, batch, level, add0_galois, rescale, st);
+}
+
+int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* key, void* out, void* scratch,
+                         int64_t scratch_bytes, int64_t batch, int level, int rescale, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(ct3, "ct3"));
+  TRY(fhb::check_ptr(key, "key"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_ptr(scratch, "scratch"));
+  TRY(fhb::check_level(c, level));
+  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
+  const int limbs = c.num_q - level;
+  const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
+  TRY(fhb::inverse(c, ct3, s.coef, 3 * batch * limbs, limbs, level, fhb::kInvStandard, st));
+  const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
+  TRY(FHB_WORD(fhb::modup, c, s.coef + 2 * comp, s.digits, batch, level, 1u, st));
+  return keyswitch_tail(c, s, key, s.coef, s.coef + comp, 1u, out, batch, level, rescale, st);
+}
+
+int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const void* b, const void* key, void* out,
+                                  void* scratch, int64_t scratch_bytes, int64_t batch, int level, int rescale,
+                                  fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(a, "a"));
+  TRY(fhb::check_ptr(b, "b"));
+  TRY(fhb::check_ptr(key, "key"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_ptr(scratch, "scratch"));
+  TRY(fhb::check_level(c, level));
+  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
+  const int limbs = c.num_q - level;
+  const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
+  TRY(fhb::mul_coef(c, a, b, s.coef, batch, level, st));
+  const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
+  TRY(FHB_WORD(fhb::modup, c, s.coef + 2 * comp, s.digits, batch, level, 1u, st));
+  return keyswitch_tail(c, s, key, s.coef, s.coef + comp, 1u, out, batch, level, rescale, st);
+}
+
+int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,
+                    int64_t scratch_bytes, int64_t batch, int level, uint32_t galois, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(ct, "ct"));
+  TRY(fhb::check_ptr(key, "key"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_ptr(scratch, "scratch"));
+  TRY(fhb::check_level(c, level));
+  TRY(fhb::check_galois(c, galois));
+  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  const int limbs = c.num_q - level;
+  const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
+  const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
+  TRY(FHB_WORD(fhb::modup, c, static_cast<const char*>(ct) + comp, s.digits, batch, level, galois, st));
+  return keyswitch_tail(c, s, key, ct, nullptr, galois, out, batch, level, 0, st);
+}
+
+}  // extern "C"

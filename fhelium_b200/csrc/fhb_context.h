@@ -1,0 +1,81 @@
+// Device-resident tables for one CKKS modulus chain (host-side definition).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "fhb_arith.cuh"
+
+namespace fhb {
+
+constexpr int kMaxDigitWidth = 8;  // hybrid digit width bound (= P count)
+
+// One active hybrid digit at one level.
+struct DigitDesc {
+  int32_t prime0;     // first prime id of the digit (component-local row = prime0 - level)
+  int32_t alpha;      // number of primes in the digit
+  int32_t key_digit;  // stable level-zero key digit index
+  int32_t pad;
+};
+
+// Word-size dependent device tables.  All TwPair entries are (w, Shoup(w)).
+template <typename T>
+struct ChainTables {
+  PrimeInfo<T>* prime = nullptr;  // [QP]
+  TwPair<T>* tw_fwd = nullptr;    // [QP][N]  psi^{br(k)}
+  TwPair<T>* tw_inv = nullptr;    // [QP][N]  psi^{-br(k)}
+  // ModDown by P (level independent): Garner constants of the P part and, per
+  // prime id, Mp_k mod q and P^{-1} mod q.
+  TwPair<T>* p_garner = nullptr;  // [8][8]
+  TwPair<T>* p_mix = nullptr;     // [8][QP]
+  TwPair<T>* p_inv = nullptr;     // [QP]
+};
+
+// Per-level key-switch / rescale tables (device).
+template <typename T>
+struct LevelTables {
+  int num_digits = 0;
+  DigitDesc* digits = nullptr;    // [nd]
+  TwPair<T>* garner = nullptr;    // [nd][8][8]: [k][i<k] = M_i mod b_k, [k][k] = M_k^{-1} mod b_k
+  TwPair<T>* ext = nullptr;       // [nd][8][QP]: M_r mod p  (M_0 = 1)
+  TwPair<T>* rescale_inv = nullptr;  // [QP]: q_level^{-1} mod p (rows > level)
+};
+
+struct Context {
+  int bits = 0;        // 64 or 32
+  int log_n = 0;
+  int num_q = 0;
+  int num_p = 0;
+  int device = 0;
+  std::vector<uint64_t> moduli;
+  std::vector<uint64_t> roots;  // primitive 2N-th roots psi
+  ChainTables<uint64_t> t64;
+  ChainTables<uint32_t> t32;
+  std::vector<LevelTables<uint64_t>> lv64;
+  std::vector<LevelTables<uint32_t>> lv32;
+  std::vector<void*> allocations;
+  int qp() const { return num_q + num_p; }
+  int n() const { return 1 << log_n; }
+};
+
+template <typename T>
+inline const ChainTables<T>& tables(const Context& c);
+template <>
+inline const ChainTables<uint64_t>& tables<uint64_t>(const Context& c) { return c.t64; }
+template <>
+inline const ChainTables<uint32_t>& tables<uint32_t>(const Context& c) { return c.t32; }
+template <typename T>
+inline const LevelTables<T>& level_tables(const Context& c, int level);
+template <>
+inline const LevelTables<uint64_t>& level_tables<uint64_t>(const Context& c, int level) { return c.lv64[level]; }
+template <>
+inline const LevelTables<uint32_t>& level_tables<uint32_t>(const Context& c, int level) { return c.lv32[level]; }
+
+// Host-side status plumbing shared by the C ABI.
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_status(cudaError_t e, const char* where);
+
+}  // namespace fhb

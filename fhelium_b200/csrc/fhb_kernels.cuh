@@ -1,0 +1,635 @@
+// CKKS evaluation kernels for sm_100a (device code).
+//
+// Residue tensors are the reference layout: contiguous [*batch, limb, N]
+// with limb j belonging to prime id (row_start + j) of the level-zero chain
+// [Q | P] (fhelium/core/ciphertext.py:26-67).  A ciphertext component at
+// level l holds prime ids [l, num_q); its Q+P extension holds [l, num_q+num_p).
+#pragma once
+#include "fhb_context.h"
+#include "fhb_ntt.cuh"
+
+namespace fhb {
+
+enum InverseOut : int { kInvMontgomery = 0, kInvStandardLazy = 1, kInvStandard = 2, kInvCentered = 3 };
+
+// ---- 16-residue thread-contiguous vector access ----------------------------
+template <typename T>
+__device__ __forceinline__ void load16(const T* p, T (&v)[16]) {
+  if constexpr (sizeof(T) == 8) {
+    const ulonglong2* q = reinterpret_cast<const ulonglong2*>(p);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const ulonglong2 x = q[i];
+      v[2 * i] = x.x;
+      v[2 * i + 1] = x.y;
+    }
+  } else {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint4 x = q[i];
+      v[4 * i] = x.x; v[4 * i + 1] = x.y; v[4 * i + 2] = x.z; v[4 * i + 3] = x.w;
+    }
+  }
+}
+template <typename T>
+__device__ __forceinline__ void store16(T* p, const T (&v)[16]) {
+  if constexpr (sizeof(T) == 8) {
+    ulonglong2* q = reinterpret_cast<ulonglong2*>(p);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) q[i] = make_ulonglong2(v[2 * i], v[2 * i + 1]);
+  } else {
+    uint4* q = reinterpret_cast<uint4*>(p);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q[i] = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  }
+}
+
+template <typename T, int LOGN>
+__device__ __forceinline__ int cluster_rank() {
+  if constexpr (NttGeom<T, LOGN>::kC > 1) return int(cg::this_cluster().block_rank());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Plain forward NTT: standard -> NTT/Montgomery (x R) or Montgomery -> NTT.
+// Output lazy [0, 2q) as in csrc/ops/ntt/forward_ntt.cpp:19-22.
+template <typename T, int LOGN, bool TO_MONT>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start,
+              ChainTables<T> tabs) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const int64_t poly = blockIdx.x / G::kC;
+  const int pid = row_start + int(poly % rows);
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const T* src = in + poly * G::kN + int64_t(rank) * G::kM;
+  for (int i = threadIdx.x; i < G::kM; i += G::kThreads) {
+    T v = src[i];
+    if constexpr (TO_MONT) v = Word<T>::shoup(v, p.rmod, p.rmod_s, p.q);
+    s[G::sidx(i)] = v;
+  }
+  T v[16];
+  Ntt<T, LOGN>::forward(s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v);
+#pragma unroll
+  for (int e = 0; e < 16; ++e) v[e] = csub(v[e], p.twice_q);
+  store16(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * 16, v);
+}
+
+template <typename T>
+struct InvEpilogue {
+  T* dst;
+  PrimeInfo<T> p;
+  T c, cs;
+  int kind;
+  __device__ __forceinline__ void operator()(int pos, T v) const {
+    v = Word<T>::shoup(v, c, cs, p.q);  // [0, 2q)
+    if (kind >= kInvStandard) v = csub(v, p.q);
+    if (kind == kInvCentered) v = v <= (p.q >> 1) ? v : v - p.q;
+    dst[pos] = v;
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ InvEpilogue<T> make_inv_epilogue(T* dst, const PrimeInfo<T>& p, int kind,
+                                                            bool montgomery_input) {
+  InvEpilogue<T> e{dst, p, p.ninv, p.ninv_s, kind};
+  if (kind != kInvMontgomery && montgomery_input) {
+    e.c = p.ninv_rinv;
+    e.cs = p.ninv_rinv_s;
+  }
+  return e;
+}
+
+// Plain inverse NTT from NTT/Montgomery lazy input.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start, int kind,
+              ChainTables<T> tabs) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const int64_t poly = blockIdx.x / G::kC;
+  const int pid = row_start + int(poly % rows);
+  const PrimeInfo<T> p = tabs.prime[pid];
+  T v[16];
+  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * 16, v);
+  InvEpilogue<T> epi = make_inv_epilogue<T>(out + poly * G::kN, p, kind, true);
+  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, epi);
+}
+
+// ---------------------------------------------------------------------------
+// Fused tensor product + inverse NTT (HMult feeding relinearisation).
+// a, b: [2, B, L, N] NTT/Montgomery lazy; out: [3, B, L, N] coefficient/standard
+// canonical = INTT of (a0 b0, a0 b1 + a1 b0, a1 b1)
+// (fhelium/engine/ckks_engine.py:1570-1606 then :1655-1660).
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
+                     int64_t batch, int limbs, int level, ChainTables<T> tabs) {
+  using G = NttGeom<T, LOGN>;
+  using W = Word<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const int64_t poly = blockIdx.x / G::kC;  // over [3, B, L]
+  const int64_t comp_stride = batch * limbs * G::kN;
+  const int comp = int(poly / (batch * limbs));
+  const int64_t rest = poly % (batch * limbs);
+  const int pid = level + int(rest % limbs);
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const int64_t off = rest * G::kN + int64_t(rank) * G::kM + threadIdx.x * 16;
+  T v[16], x[16], y[16];
+  const T* a0 = a + off;
+  const T* a1 = a + comp_stride + off;
+  const T* b0 = b + off;
+  const T* b1 = b + comp_stride + off;
+  load16(comp == 2 ? a1 : a0, x);
+  load16(comp == 0 ? b0 : b1, y);
+#pragma unroll
+  for (int e = 0; e < 16; ++e) v[e] = W::mont(x[e], y[e], p.q, p.neg_inv);
+  if (comp == 1) {
+    load16(a1, x);
+    load16(b0, y);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[e] = csub(v[e] + W::mont(x[e], y[e], p.q, p.neg_inv), p.twice_q);
+  }
+  InvEpilogue<T> epi = make_inv_epilogue<T>(out + comp * comp_stride + rest * G::kN, p, kInvStandard, true);
+  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, epi);
+}
+
+// NTT-domain tensor product only (reference multiply): out [3, B, L, N] lazy.
+template <typename T>
+__global__ void k_mul_ntt(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
+                          int64_t batch, int limbs, int log_n, int level, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * limbs * n;
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+    const PrimeInfo<T> p = tabs.prime[level + int((i >> log_n) % limbs)];
+    const T x0 = a[i], x1 = a[total + i], y0 = b[i], y1 = b[total + i];
+    out[i] = Word<T>::mont(x0, y0, p.q, p.neg_inv);
+    out[total + i] = csub(Word<T>::mont(x0, y1, p.q, p.neg_inv) + Word<T>::mont(x1, y0, p.q, p.neg_inv), p.twice_q);
+    out[2 * total + i] = Word<T>::mont(x1, y1, p.q, p.neg_inv);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Galois automorphism sigma_g on a coefficient-domain residue: destination j
+// reads source (j g^{-1} mod 2N) with a sign flip when that index >= N
+// (fhelium/engine/galois.py:49-83, derived in-kernel, no gather table).
+__device__ __forceinline__ int galois_source(int j, int log_n, uint32_t ginv, bool& negate) {
+  const uint64_t two_n_mask = (uint64_t{2} << log_n) - 1;
+  const uint32_t i = uint32_t((uint64_t(j) * ginv) & two_n_mask);
+  negate = i >> log_n;
+  return int(i & ((1u << log_n) - 1));
+}
+
+// NTT-domain automorphism gather (bit-reversed evaluation order):
+// destination k reads br(((2 br(k) + 1) g mod 2N - 1) / 2)
+// (fhelium/engine/hybrid_keyswitch.py:506-528).
+__device__ __forceinline__ int galois_ntt_source(int k, int log_n, uint32_t g) {
+  const uint32_t br = __brev(uint32_t(k)) >> (32 - log_n);
+  const uint32_t e = uint32_t((uint64_t(2 * br + 1) * g) & ((uint64_t{2} << log_n) - 1));
+  return int(__brev((e - 1) >> 1) >> (32 - log_n));
+}
+
+// ---------------------------------------------------------------------------
+// ModUp stage 1: Garner mixed-radix digits of every active hybrid digit
+// (fhelium/engine/hybrid_keyswitch.py:95-170, exact same digits as
+// csrc/ops/rns/cpu/rns_arithmetic_cpu.cpp:482-615).  comp: [B, L, N]
+// coefficient/standard (canonical or lazy [0, 2q)); digits: [B, L, N],
+// row r holds the mixed-radix digit of the prime in row r.  When ginv != 0
+// the input is first mapped through sigma_g (rotation).
+template <typename T>
+__global__ void k_modup_digits(const T* __restrict__ comp, T* __restrict__ digits, int64_t batch,
+                               int limbs, int log_n, int level, uint32_t ginv, ChainTables<T> tabs,
+                               LevelTables<T> lt) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * n;
+  using W = Word<T>;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t bi = idx >> log_n;
+    const int k = int(idx & (n - 1));
+    bool neg = false;
+    const int srck = ginv ? galois_source(k, log_n, ginv, neg) : k;
+    const T* src = comp + bi * limbs * n;
+    T* dst = digits + bi * limbs * n;
+    for (int a = 0; a < lt.num_digits; ++a) {
+      const DigitDesc d = lt.digits[a];
+      const TwPair<T>* g = lt.garner + a * kMaxDigitWidth * kMaxDigitWidth;
+      T dig[kMaxDigitWidth];
+      for (int r = 0; r < d.alpha; ++r) {
+        const int row = d.prime0 - level + r;
+        const PrimeInfo<T> p = tabs.prime[d.prime0 + r];
+        T x = csub(src[row * n + srck], p.q);
+        if (neg && x) x = p.q - x;
+        T acc = 0;
+        for (int i = 0; i < r; ++i) {
+          const TwPair<T> c = g[r * kMaxDigitWidth + i];
+          acc = csub(acc + csub(W::shoup(dig[i], c.w, c.wp, p.q), p.q), p.q);
+        }
+        if (r > 0) {
+          const TwPair<T> inv = g[r * kMaxDigitWidth + r];
+          x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
+        }
+        dig[r] = x;
+        dst[row * n + k] = x;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Key-switch accumulators of one thread: 2 x 16 residues kept in shared
+// memory ([element][thread], conflict-free) when the CTA has room next to the
+// NTT working block, otherwise in the thread's own slots of the output rows.
+template <typename T, int LOGN>
+struct KsAcc {
+  using G = NttGeom<T, LOGN>;
+  static constexpr bool kSmem = (G::kSmemElems + 2 * G::kM) * sizeof(T) <= 200 * 1024;
+  static constexpr size_t smem_bytes() { return (G::kSmemElems + (kSmem ? 2 * G::kM : 0)) * sizeof(T); }
+  T* c0;
+  T* c1;
+  int stride;
+  __device__ __forceinline__ KsAcc(T* s, T* g0, T* g1) {
+    if constexpr (kSmem) {
+      c0 = s + G::kSmemElems + threadIdx.x;
+      c1 = c0 + G::kM;
+      stride = G::kThreads;
+    } else {
+      c0 = g0;
+      c1 = g1;
+      stride = 1;
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) c0[e * stride] = c1[e * stride] = 0;
+  }
+  __device__ __forceinline__ void mac(int e, T x, T k0, T k1, const PrimeInfo<T>& p) {
+    c0[e * stride] = csub(c0[e * stride] + Word<T>::mont(x, k0, p.q, p.neg_inv), p.twice_q);
+    c1[e * stride] = csub(c1[e * stride] + Word<T>::mont(x, k1, p.q, p.neg_inv), p.twice_q);
+  }
+  __device__ __forceinline__ void get(int which, T (&v)[16]) const {
+    const T* c = which ? c1 : c0;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[e] = c[e * stride];
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Fused ModUp stage 2 + forward NTT + key inner product + inverse NTT.
+// One cluster per (ciphertext b, destination row j of Q_l P).  For every
+// active digit: extend the mixed-radix digits to prime p_j exactly
+// (sum_r d_r M_r mod p_j), transform, multiply by the key digit row and
+// accumulate; finally inverse-transform both accumulators to
+// coefficient/standard canonical rows.  Equals, modulo p_j, the reference's
+// per-digit basis extension + forward NTT + keyswitch_accumulate + the
+// inverse NTT at the start of ModDown (fhelium/engine/hybrid_keyswitch.py:
+// 321-371, 530-546).  key: [D, 2, QP0, N] NTT/Montgomery level-zero rows.
+// acc0/acc1: [B, QP_l, N]; they double as accumulation scratch.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
+                 T* __restrict__ acc1, int q_limbs, int qp_limbs, int level, int qp0,
+                 ChainTables<T> tabs, LevelTables<T> lt) {
+  using G = NttGeom<T, LOGN>;
+  using W = Word<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const int64_t poly = blockIdx.x / G::kC;  // over [B, QP_l]
+  const int64_t bi = poly / qp_limbs;
+  const int jrow = int(poly % qp_limbs);
+  const int pid = level + jrow;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
+  const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * 16;
+  KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    const TwPair<T>* ext = lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid;
+    __syncthreads();
+    for (int i = threadIdx.x; i < G::kM; i += G::kThreads) {
+      T y = 0;
+      for (int r = 0; r < d.alpha; ++r) {
+        const TwPair<T> c = ext[int64_t(r) * qp0];
+        const T x = dig[int64_t(d.prime0 - level + r) * G::kN + i];
+        y = csub(y + W::shoup(x, c.w, c.wp, p.q), p.twice_q);
+      }
+      s[G::sidx(i)] = y;
+    }
+    T v[16], k0[16], k1[16];
+    Ntt<T, LOGN>::forward(s, twf, p.q, p.twice_q, rank, v);
+    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
+    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
+    load16(key0, k0);
+    load16(key1, k1);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc.mac(e, csub(v[e], p.twice_q), k0[e], k1[e], p);
+  }
+  __syncthreads();
+  T v[16];
+  acc.get(0, v);
+  InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
+  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e0);
+  acc.get(1, v);
+  InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
+  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e1);
+}
+
+// Hoisting stage 1: materialise NTT-domain extended digits once
+// (fhelium/engine/hybrid_keyswitch.py:373-417).  prepared: [D_l, B, QP_l, N]
+// standard NTT-domain values in [0, 2p).
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64_t batch, int q_limbs,
+                   int qp_limbs, int level, int qp0, ChainTables<T> tabs, LevelTables<T> lt) {
+  using G = NttGeom<T, LOGN>;
+  using W = Word<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const int64_t poly = blockIdx.x / G::kC;  // over [B, QP_l]
+  const int64_t bi = poly / qp_limbs;
+  const int jrow = int(poly % qp_limbs);
+  const int pid = level + jrow;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
+  const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * 16;
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    const TwPair<T>* ext = lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid;
+    __syncthreads();
+    for (int i = threadIdx.x; i < G::kM; i += G::kThreads) {
+      T y = 0;
+      for (int r = 0; r < d.alpha; ++r) {
+        const TwPair<T> c = ext[int64_t(r) * qp0];
+        const T x = dig[int64_t(d.prime0 - level + r) * G::kN + i];
+        y = csub(y + W::shoup(x, c.w, c.wp, p.q), p.twice_q);
+      }
+      s[G::sidx(i)] = y;
+    }
+    T v[16];
+    Ntt<T, LOGN>::forward(s, twf, p.q, p.twice_q, rank, v);
+#pragma unroll
+    for (int e = 0; e < 16; ++e) v[e] = csub(v[e], p.twice_q);
+    store16(prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN + own, v);
+  }
+}
+
+// Hoisting stage 2: per rotation step, NTT-domain automorphism of the
+// prepared digits + key inner product + inverse NTT of both accumulators
+// (fhelium/engine/hybrid_keyswitch.py:419-469).
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ key, T* __restrict__ acc0,
+                          T* __restrict__ acc1, int64_t batch, int qp_limbs, int level, int qp0,
+                          uint32_t galois, ChainTables<T> tabs, LevelTables<T> lt) {
+  using G = NttGeom<T, LOGN>;
+  using W = Word<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const int64_t poly = blockIdx.x / G::kC;
+  const int jrow = int(poly % qp_limbs);
+  const int pid = level + jrow;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const int own = rank * G::kM + threadIdx.x * 16;
+  KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    const T* pr = prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN;
+    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
+    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
+#pragma unroll 4
+    for (int e = 0; e < 16; ++e) {
+      const int src = galois ? galois_ntt_source(own + e, LOGN, galois) : own + e;
+      acc.mac(e, __ldg(pr + src), __ldg(key0 + e), __ldg(key1 + e), p);
+    }
+  }
+  __syncthreads();
+  T v[16];
+  acc.get(0, v);
+  InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
+  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e0);
+  acc.get(1, v);
+  InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
+  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e1);
+}
+
+// ---------------------------------------------------------------------------
+// ModDown by P fused with the final addition and, optionally, the rescale by
+// the leading prime.  t0/t1: [B, QP_l, N] canonical coefficient rows;
+// add0/add1 (nullable): [B, Q_l, N] canonical, add0 optionally read through
+// sigma_g (rotation of c0).  Result per Q row i (prime q):
+//   v_i = (t_i - [t]_P) P^{-1} + add_i  (mod q)
+// which is exactly the sequential divide-by-p_j chain of
+// csrc/ops/ckks/cpu/ckks_cpu.cpp:474-601 (both compute (t - [t]_P)/P over
+// the integers), then (when rescale) the nearest-rounded division by the
+// leading prime of csrc/ops/ckks/cpu/ckks_cpu.cpp:203-262:
+//   out_i = (v_i - v_0) q_0^{-1} + [v_0 > q_0/2]  (mod q_i), i >= 1.
+// out: [2, B, Q_l (- 1 if rescale), N] canonical.
+template <typename T>
+__global__ void k_moddown(const T* __restrict__ t0, const T* __restrict__ t1, const T* __restrict__ add0,
+                          const T* __restrict__ add1, T* __restrict__ out, int64_t batch, int log_n,
+                          int level, int num_q, int num_p, uint32_t add0_ginv, int rescale,
+                          ChainTables<T> tabs, LevelTables<T> lt) {
+  using W = Word<T>;
+  const int64_t n = int64_t(1) << log_n;
+  const int q_limbs = num_q - level;
+  const int qp_limbs = q_limbs + num_p;
+  const int out_limbs = q_limbs - (rescale ? 1 : 0);
+  const int64_t total = batch * n;
+  const int qp0 = num_q + num_p;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t bi = idx >> log_n;
+    const int k = int(idx & (n - 1));
+    bool neg = false;
+    const int ak = add0_ginv ? galois_source(k, log_n, add0_ginv, neg) : k;
+    for (int c = 0; c < 2; ++c) {
+      const T* t = (c == 0 ? t0 : t1) + bi * qp_limbs * n;
+      const T* ad = c == 0 ? add0 : add1;
+      const int kk = c == 0 ? ak : k;
+      const bool nn = c == 0 ? neg : false;
+      // Garner digits of the P part
+      T e[kMaxDigitWidth];
+      for (int r = 0; r < num_p; ++r) {
+        const PrimeInfo<T> p = tabs.prime[num_q + r];
+        T x = t[(q_limbs + r) * n + k];
+        T acc = 0;
+        for (int i = 0; i < r; ++i) {
+          const TwPair<T> g = tabs.p_garner[r * kMaxDigitWidth + i];
+          acc = csub(acc + csub(W::shoup(e[i], g.w, g.wp, p.q), p.q), p.q);
+        }
+        if (r > 0) {
+          const TwPair<T> inv = tabs.p_garner[r * kMaxDigitWidth + r];
+          x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
+        }
+        e[r] = x;
+      }
+      T* o = out + (int64_t(c) * batch + bi) * out_limbs * n;
+      T v0 = 0;
+      for (int i = 0; i < q_limbs; ++i) {
+        const int pid = level + i;
+        const PrimeInfo<T> p = tabs.prime[pid];
+        T sub = 0;
+        for (int r = 0; r < num_p; ++r) {
+          const TwPair<T> m = tabs.p_mix[r * qp0 + pid];
+          sub = csub(sub + csub(W::shoup(e[r], m.w, m.wp, p.q), p.q), p.q);
+        }
+        const TwPair<T> pinv = tabs.p_inv[pid];
+        T v = csub(t[i * n + k] + p.q - sub, p.q);
+        v = csub(W::shoup(v, pinv.w, pinv.wp, p.q), p.q);
+        if (ad) {
+          T x = csub(ad[(bi * q_limbs + i) * n + kk], p.q);
+          if (nn && x) x = p.q - x;
+          v = csub(v + x, p.q);
+        }
+        if (!rescale) {
+          o[i * n + k] = v;
+        } else if (i == 0) {
+          v0 = v;
+        } else {
+          const T x0 = reduce_any(v0, p);
+          const TwPair<T> inv = lt.rescale_inv[pid];
+          T r = csub(W::shoup(csub(v + p.q - x0, p.q), inv.w, inv.wp, p.q), p.q);
+          r += (v0 > (tabs.prime[level].q >> 1)) ? 1 : 0;
+          o[(i - 1) * n + k] = csub(r, p.q);
+        }
+      }
+    }
+  }
+}
+
+// Standalone rescale of coefficient/standard components: in [K, L, N] ->
+// out [K, L-1, N] (csrc/ops/ckks/cpu/ckks_cpu.cpp:203-262).
+template <typename T>
+__global__ void k_rescale(const T* __restrict__ in, T* __restrict__ out, int64_t polys, int limbs, int log_n,
+                          int level, int nearest, ChainTables<T> tabs, LevelTables<T> lt) {
+  using W = Word<T>;
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = polys * (limbs - 1) * n;
+  const T half = tabs.prime[level].q >> 1;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int k = int(idx & (n - 1));
+    const int64_t rowi = idx >> log_n;
+    const int i = int(rowi % (limbs - 1)) + 1;
+    const int64_t pl = rowi / (limbs - 1);
+    const int pid = level + i;
+    const PrimeInfo<T> p = tabs.prime[pid];
+    const T v0 = in[pl * limbs * n + k];
+    const T x0 = reduce_any(v0, p);
+    const T v = reduce_any(in[(pl * limbs + i) * n + k], p);
+    const TwPair<T> inv = lt.rescale_inv[pid];
+    T r = csub(W::shoup(csub(v + p.q - x0, p.q), inv.w, inv.wp, p.q), p.q);
+    if (nearest) r += (v0 > half) ? 1 : 0;
+    out[idx] = csub(r, p.q);
+  }
+}
+
+// Coefficient-domain automorphism: out = sigma_g(in), canonical
+// (csrc/ops/ckks/cpu/ckks_cpu.cpp:287-380).
+template <typename T>
+__global__ void k_automorphism(const T* __restrict__ in, T* __restrict__ out, int64_t batch, int rows,
+                               int row_start, int log_n, uint32_t ginv, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * rows * n;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int k = int(idx & (n - 1));
+    const int64_t row = idx >> log_n;
+    const PrimeInfo<T> p = tabs.prime[row_start + int(row % rows)];
+    bool neg = false;
+    const int src = galois_source(k, log_n, ginv, neg);
+    T x = csub(in[row * n + src], p.q);
+    if (neg && x) x = p.q - x;
+    out[idx] = x;
+  }
+}
+
+// Pointwise RNS arithmetic over [batch, rows, N] whose rows are prime ids
+// [row_start, row_start + rows) (fhelium_rns_ops.montgomery_mul / add_lazy /
+// sub_lazy / add_canonical / sub_canonical, csrc/ops/rns/rns_arithmetic.cpp:
+// 30-72, rns_canonical_arithmetic.cpp:15-23).  b_mode 0: b has a's shape;
+// 1: b is [rows, N] shared by every batch item; 2: b is [rows] (one scalar
+// per row, montgomery_mul_row_scalars_).
+enum RnsOp : int { kOpMontMul = 0, kOpAddLazy = 1, kOpSubLazy = 2, kOpAddCanon = 3, kOpSubCanon = 4,
+                   kOpNegCanon = 5 };
+
+template <typename T>
+__global__ void k_rns_binary(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out, int64_t batch,
+                             int rows, int row_start, int log_n, int op, int b_mode, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t per = int64_t(rows) * n;
+  const int64_t total = batch * per;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int row = int((idx >> log_n) % rows);
+    const PrimeInfo<T> p = tabs.prime[row_start + row];
+    const T x = a[idx];
+    const T y = op == kOpNegCanon ? T(0) : (b_mode == 0 ? b[idx] : (b_mode == 1 ? b[idx % per] : b[row]));
+    T r;
+    switch (op) {
+      case kOpMontMul: r = Word<T>::mont(x, y, p.q, p.neg_inv); break;
+      case kOpAddLazy: r = csub(x + y, p.twice_q); break;
+      case kOpSubLazy: r = csub(x + p.twice_q - y, p.twice_q); break;
+      case kOpAddCanon: r = csub(reduce_any(x, p) + reduce_any(y, p), p.q); break;
+      case kOpSubCanon: r = csub(reduce_any(x, p) + p.q - reduce_any(y, p), p.q); break;
+      default: { const T c = reduce_any(x, p); r = c ? p.q - c : T(0); }
+    }
+    out[idx] = r;
+  }
+}
+
+// Lift signed integer coefficients [batch, N] (int64) into every row:
+// out[b, r, k] = x[b, k] mod q_r, canonical (fhelium_rns_ops.
+// lift_centered_coefficients, csrc/ops/rns/cuda/rns_arithmetic_cuda.cu:211).
+template <typename T>
+__global__ void k_lift_signed(const int64_t* __restrict__ x, T* __restrict__ out, int64_t batch, int rows,
+                              int row_start, int log_n, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * rows * n;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int k = int(idx & (n - 1));
+    const int64_t br = idx >> log_n;
+    const int row = int(br % rows);
+    const int64_t bi = br / rows;
+    const PrimeInfo<T> p = tabs.prime[row_start + row];
+    const int64_t v = x[bi * n + k];
+    const uint64_t mag = v < 0 ? uint64_t(0) - uint64_t(v) : uint64_t(v);
+    uint64_t m;
+    if constexpr (sizeof(T) == 8) {
+      m = csub(Word<uint64_t>::shoup(mag, 1, p.one_s, p.q), p.q);
+    } else {
+      m = mag % p.q;
+    }
+    out[idx] = T(v < 0 && m ? p.q - m : m);
+  }
+}
+
+// Canonical addition (add / add_canonical): out = a + b mod q.
+template <typename T>
+__global__ void k_add_canonical(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
+                                int64_t polys, int limbs, int log_n, int level, int lazy, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = polys * limbs * n;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const PrimeInfo<T> p = tabs.prime[level + int((idx >> log_n) % limbs)];
+    if (lazy) {
+      out[idx] = csub(a[idx] + b[idx], p.twice_q);
+    } else {
+      out[idx] = csub(csub(a[idx], p.q) + csub(b[idx], p.q), p.q);
+    }
+  }
+}
+
+}  // namespace fhb

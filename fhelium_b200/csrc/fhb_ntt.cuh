@@ -1,0 +1,286 @@
+// Negacyclic NTT core for one residue polynomial held by a thread-block
+// cluster.
+//
+// Transform (same as the reference, csrc/ops/ntt/forward_ntt.cpp:15-21):
+//   A[k] = sum_n a[n] psi^{(2 br(k) + 1) n}  (mod q), bit-reversed output,
+// computed as radix-2 decimation in frequency where stage s, group g uses the
+// twiddle psi^{br(2^s + g)}; the inverse runs Gentleman-Sande stages with
+// psi^{-br(.)} in the mirrored order.  Any implementation of this linear map
+// yields the same residues, so the kernels below are free to organise the
+// butterflies for the hardware.
+//
+// Layout on the GPU: a polynomial of N = 2^LOGN residues is split across a
+// cluster of C = 2^LOGC CTAs; CTA r owns the contiguous block
+// [r*M, (r+1)*M), M = N / C, in its shared memory (padded every 2^PAD
+// elements so that strided accesses spread over all banks).
+//   * the first LOGC forward stages (half spans >= M) pair elements held by
+//     different CTAs: each CTA transforms 1/C of the columns through
+//     distributed shared memory (ld/st.shared::cluster);
+//   * the remaining LOGM stages are CTA-local, done in register passes of
+//     3 or 4 stages (radix-8/16 per thread, 16 residues per thread);
+//   * the last forward pass leaves every thread with 16 consecutive outputs
+//     in registers, which the caller's epilogue consumes (store, or fused
+//     key multiply-accumulate).
+// The inverse mirrors this: the first pass starts from 16 consecutive
+// values per thread (from registers), the cross-CTA stages come last.
+// Forward butterflies keep Harvey's lazy range [0, 4q), inverse ones [0, 2q).
+#pragma once
+#include <cooperative_groups.h>
+
+#include "fhb_arith.cuh"
+
+namespace fhb {
+namespace cg = cooperative_groups;
+
+constexpr int clamp_int(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+template <typename T, int LOGN>
+struct NttGeom {
+  static constexpr int kLogN = LOGN;
+  static constexpr int kN = 1 << LOGN;
+  static constexpr int kLogC = clamp_int(LOGN - 13, 0, 3);
+  static constexpr int kC = 1 << kLogC;
+  static constexpr int kLogM = LOGN - kLogC;
+  static constexpr int kM = 1 << kLogM;
+  static constexpr int kE = 16;  // residues per thread
+  static constexpr int kThreads = kM / kE;
+  static constexpr int kPadShift = sizeof(T) == 8 ? 4 : 5;
+  static constexpr int kSmemElems = kM + (kM >> kPadShift);
+  static constexpr int kPasses = (kLogM + 3) / 4;
+  static constexpr int kNum4 = kLogM - 3 * kPasses;
+  static constexpr int pass_k(int j) { return j >= kPasses - kNum4 ? 4 : 3; }
+  static constexpr int pass_a(int j) { return j == 0 ? 0 : pass_a(j - 1) + pass_k(j - 1); }
+  // inverse pass j is forward pass kPasses-1-j; its lowest half-span exponent
+  static constexpr int inv_k(int j) { return pass_k(kPasses - 1 - j); }
+  static constexpr int inv_l(int j) { return j == 0 ? 0 : inv_l(j - 1) + inv_k(j - 1); }
+  __device__ __forceinline__ static int sidx(int n) { return n + (n >> kPadShift); }
+};
+
+template <typename T>
+__device__ __forceinline__ TwPair<T> ldtw(const TwPair<T>* tw, int i) {
+  if constexpr (sizeof(T) == 8) {
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(tw + i));
+    return TwPair<T>{v.x, v.y};
+  } else {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(tw + i));
+    return TwPair<T>{v.x, v.y};
+  }
+}
+
+template <typename T, int LOGN>
+struct Ntt {
+  using G = NttGeom<T, LOGN>;
+  using W = Word<T>;
+  static constexpr int E = G::kE;
+
+  __device__ __forceinline__ static void fwd_bfly(T& x, T& y, const TwPair<T>& w, T q, T twoq) {
+    const T xx = csub(x, twoq);
+    const T t = W::shoup(y, w.w, w.wp, q);
+    x = xx + t;
+    y = xx - t + twoq;
+  }
+  __device__ __forceinline__ static void inv_bfly(T& x, T& y, const TwPair<T>& w, T q, T twoq) {
+    const T s = x + y;
+    const T d = x - y + twoq;
+    x = csub(s, twoq);
+    y = W::shoup(d, w.w, w.wp, q);
+  }
+
+  // ---- forward -----------------------------------------------------------
+  __device__ __forceinline__ static void fwd_cross(T* s, const TwPair<T>* tw, T q, T twoq, int rank) {
+    if constexpr (G::kC > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      T* rs[G::kC];
+#pragma unroll
+      for (int c = 0; c < G::kC; ++c) rs[c] = cl.map_shared_rank(s, c);
+      constexpr int kCols = G::kM / G::kC;
+#pragma unroll
+      for (int u = 0; u < kCols / G::kThreads; ++u) {
+        const int m = rank * kCols + u * G::kThreads + threadIdx.x;
+        const int sm = G::sidx(m);
+        T x[G::kC];
+#pragma unroll
+        for (int c = 0; c < G::kC; ++c) x[c] = rs[c][sm];
+#pragma unroll
+        for (int st = 0; st < G::kLogC; ++st) {
+          const int h = G::kC >> (st + 1);
+#pragma unroll
+          for (int c = 0; c < G::kC; ++c)
+            if (!(c & h)) fwd_bfly(x[c], x[c + h], ldtw(tw, (1 << st) + (c >> (G::kLogC - st))), q, twoq);
+        }
+#pragma unroll
+        for (int c = 0; c < G::kC; ++c) rs[c][sm] = x[c];
+      }
+    }
+  }
+
+  template <int A, int K, bool LAST>
+  __device__ __forceinline__ static void fwd_pass(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                  T (&out)[E]) {
+    constexpr int kLogHl = G::kLogM - A - K;
+    constexpr int kHl = 1 << kLogHl;
+    constexpr int kGs = 1 << K;
+    constexpr int kNg = E >> K;
+#pragma unroll
+    for (int u = 0; u < kNg; ++u) {
+      const int gid = LAST ? threadIdx.x * kNg + u : u * G::kThreads + threadIdx.x;
+      const int n0 = (gid & (kHl - 1)) | ((gid >> kLogHl) << (kLogHl + K));
+      T v[kGs];
+#pragma unroll
+      for (int i = 0; i < kGs; ++i) v[i] = s[G::sidx(n0 + i * kHl)];
+      const int ng0 = rank * G::kM + n0;
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const int st = G::kLogC + A + b;
+        const int h = kGs >> (b + 1);
+#pragma unroll
+        for (int i = 0; i < kGs; ++i)
+          if (!(i & h)) {
+            const int ng = ng0 + i * kHl;
+            fwd_bfly(v[i], v[i + h], ldtw(tw, (1 << st) + (ng >> (LOGN - st))), q, twoq);
+          }
+      }
+      if constexpr (LAST) {
+#pragma unroll
+        for (int i = 0; i < kGs; ++i) out[u * kGs + i] = v[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < kGs; ++i) s[G::sidx(n0 + i * kHl)] = v[i];
+      }
+    }
+  }
+
+  template <int J>
+  __device__ __forceinline__ static void fwd_local(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                   T (&out)[E]) {
+    constexpr int K = G::pass_k(J);
+    constexpr int A = G::pass_a(J);
+    if constexpr (J == G::kPasses - 1) {
+      fwd_pass<A, K, true>(s, tw, q, twoq, rank, out);
+    } else {
+      fwd_pass<A, K, false>(s, tw, q, twoq, rank, out);
+      __syncthreads();
+      fwd_local<J + 1>(s, tw, q, twoq, rank, out);
+    }
+  }
+
+  // Forward transform of the block already staged in s (values < 4q).
+  // On return out[e] holds the (lazy, < 4q) output at local position
+  // threadIdx.x * 16 + e of CTA `rank`.
+  __device__ __forceinline__ static void forward(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                 T (&out)[E]) {
+    if constexpr (G::kC > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      cl.sync();
+      fwd_cross(s, tw, q, twoq, rank);
+      cl.sync();
+    } else {
+      __syncthreads();
+    }
+    fwd_local<0>(s, tw, q, twoq, rank, out);
+  }
+
+  // ---- inverse -----------------------------------------------------------
+  // Epilogue functor: epi(global_position, value in [0, 2q)).
+  template <int L, int K, bool FIRST, bool STORE, class Epi>
+  __device__ __forceinline__ static void inv_pass(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                  const T (&in)[E], Epi& epi) {
+    constexpr int kHl = 1 << L;
+    constexpr int kGs = 1 << K;
+    constexpr int kNg = E >> K;
+#pragma unroll
+    for (int u = 0; u < kNg; ++u) {
+      const int gid = FIRST ? threadIdx.x * kNg + u : u * G::kThreads + threadIdx.x;
+      const int n0 = (gid & (kHl - 1)) | ((gid >> L) << (L + K));
+      T v[kGs];
+#pragma unroll
+      for (int i = 0; i < kGs; ++i) v[i] = FIRST ? in[u * kGs + i] : s[G::sidx(n0 + i * kHl)];
+      const int ng0 = rank * G::kM + n0;
+#pragma unroll
+      for (int b = 0; b < K; ++b) {
+        const int j = L + b;  // half-span exponent
+        const int h = 1 << b;
+#pragma unroll
+        for (int i = 0; i < kGs; ++i)
+          if (!(i & h)) {
+            const int ng = ng0 + i * kHl;
+            inv_bfly(v[i], v[i + h], ldtw(tw, (G::kN >> (j + 1)) + (ng >> (j + 1))), q, twoq);
+          }
+      }
+      if constexpr (STORE) {
+#pragma unroll
+        for (int i = 0; i < kGs; ++i) epi(ng0 + i * kHl, v[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < kGs; ++i) s[G::sidx(n0 + i * kHl)] = v[i];
+      }
+    }
+  }
+
+  template <int J, class Epi>
+  __device__ __forceinline__ static void inv_local(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                   const T (&in)[E], Epi& epi) {
+    constexpr int K = G::inv_k(J);
+    constexpr int L = G::inv_l(J);
+    constexpr bool kLast = J == G::kPasses - 1;
+    constexpr bool kStore = kLast && G::kC == 1;
+    inv_pass<L, K, J == 0, kStore>(s, tw, q, twoq, rank, in, epi);
+    if constexpr (!kLast) {
+      __syncthreads();
+      inv_local<J + 1>(s, tw, q, twoq, rank, in, epi);
+    }
+  }
+
+  template <class Epi>
+  __device__ __forceinline__ static void inv_cross(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                   Epi& epi) {
+    if constexpr (G::kC > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      T* rs[G::kC];
+#pragma unroll
+      for (int c = 0; c < G::kC; ++c) rs[c] = cl.map_shared_rank(s, c);
+      constexpr int kCols = G::kM / G::kC;
+#pragma unroll
+      for (int u = 0; u < kCols / G::kThreads; ++u) {
+        const int m = rank * kCols + u * G::kThreads + threadIdx.x;
+        const int sm = G::sidx(m);
+        T x[G::kC];
+#pragma unroll
+        for (int c = 0; c < G::kC; ++c) x[c] = rs[c][sm];
+#pragma unroll
+        for (int b = 0; b < G::kLogC; ++b) {
+          const int j = G::kLogM + b;
+          const int h = 1 << b;
+#pragma unroll
+          for (int c = 0; c < G::kC; ++c)
+            if (!(c & h)) {
+              const int ng = c * G::kM + m;
+              inv_bfly(x[c], x[c + h], ldtw(tw, (G::kN >> (j + 1)) + (ng >> (j + 1))), q, twoq);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < G::kC; ++c) epi(c * G::kM + m, x[c]);
+      }
+    }
+  }
+
+  // Inverse transform of the values `in` (thread-contiguous layout, as left
+  // by `forward`, each < 2q).  Every output is handed to epi(position, v)
+  // with v in [0, 2q); s is scratch.  Ends with a cluster barrier so that
+  // shared memory may be reused (and so that peers never outlive reads).
+  template <class Epi>
+  __device__ __forceinline__ static void inverse(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+                                                 const T (&in)[E], Epi& epi) {
+    inv_local<0>(s, tw, q, twoq, rank, in, epi);
+    if constexpr (G::kC > 1) {
+      cg::cluster_group cl = cg::this_cluster();
+      cl.sync();
+      inv_cross(s, tw, q, twoq, rank, epi);
+      cl.sync();
+    } else {
+      __syncthreads();
+    }
+  }
+};
+
+}  // namespace fhb

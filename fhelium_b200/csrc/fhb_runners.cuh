@@ -1,0 +1,100 @@
+// Cluster launchers for the NTT-based kernels.  Each is explicitly
+// instantiated per LOGN in its own translation unit (fhb_inst_logn.cu), so
+// the kernel templates compile in parallel.
+#pragma once
+#include "fhb_kernels.cuh"
+
+namespace fhb {
+
+template <typename T, int LOGN, typename... KArgs, typename... Args>
+int launch_cluster(void (*kernel)(KArgs...), int64_t polys, size_t smem, cudaStream_t stream, Args... args) {
+  using G = NttGeom<T, LOGN>;
+  if (polys <= 0) return 0;
+  if (polys * G::kC > 0x7fffffffLL) return fail(-6, "too many polynomials for one launch");
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(unsigned(polys * G::kC));
+  cfg.blockDim = dim3(G::kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = G::kC;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = G::kC > 1 ? 1 : 0;
+  return cuda_status(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...), "cluster launch");
+}
+
+template <typename T, int LOGN>
+constexpr size_t ntt_smem() {
+  return size_t(NttGeom<T, LOGN>::kSmemElems) * sizeof(T);
+}
+
+// ---- per (T, LOGN) launchers --------------------------------------------
+template <typename T, int LOGN>
+int run_forward(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start,
+                bool mont, cudaStream_t st) {
+  if (mont)
+    return launch_cluster<T, LOGN>(k_ntt_forward<T, LOGN, false>, polys, ntt_smem<T, LOGN>(), st,
+                                   (const T*)in, (T*)out, rows, row_start, tables<T>(c));
+  return launch_cluster<T, LOGN>(k_ntt_forward<T, LOGN, true>, polys, ntt_smem<T, LOGN>(), st, (const T*)in,
+                                 (T*)out, rows, row_start, tables<T>(c));
+}
+
+template <typename T, int LOGN>
+int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
+                cudaStream_t st) {
+  return launch_cluster<T, LOGN>(k_ntt_inverse<T, LOGN>, polys, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out,
+                                 rows, row_start, kind, tables<T>(c));
+}
+
+template <typename T, int LOGN>
+int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
+                 cudaStream_t st) {
+  const int limbs = c.num_q - level;
+  return launch_cluster<T, LOGN>(k_mul_to_coefficient<T, LOGN>, 3 * batch * limbs, ntt_smem<T, LOGN>(), st,
+                                 (const T*)a, (const T*)b, (T*)out, batch, limbs, level, tables<T>(c));
+}
+
+template <typename T, int LOGN>
+int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
+                int level, cudaStream_t st) {
+  const int ql = c.num_q - level, qpl = ql + c.num_p;
+  return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
+                                 (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, ql, qpl, level, c.qp(),
+                                 tables<T>(c), level_tables<T>(c, level));
+}
+
+template <typename T, int LOGN>
+int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level,
+                cudaStream_t st) {
+  const int ql = c.num_q - level, qpl = ql + c.num_p;
+  return launch_cluster<T, LOGN>(k_prepare_rotation<T, LOGN>, batch * qpl, ntt_smem<T, LOGN>(), st,
+                                 (const T*)digits, (T*)prepared, batch, ql, qpl, level, c.qp(), tables<T>(c),
+                                 level_tables<T>(c, level));
+}
+
+template <typename T, int LOGN>
+int run_apply_prepared(const Context& c, const void* prepared, const void* key, void* acc0, void* acc1,
+                       int64_t batch, int level, uint32_t galois, cudaStream_t st) {
+  const int ql = c.num_q - level, qpl = ql + c.num_p;
+  return launch_cluster<T, LOGN>(k_apply_prepared_rotation<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
+                                 (const T*)prepared, (const T*)key, (T*)acc0, (T*)acc1, batch, qpl, level, c.qp(),
+                                 galois == 1 ? 0u : galois, tables<T>(c), level_tables<T>(c, level));
+}
+
+// Explicit instantiation of every runner for one (T, LOGN).
+#define FHB_INSTANTIATE_RUNNERS(T, LOGN)                                                                       \
+  template int run_forward<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, bool, cudaStream_t);   \
+  template int run_inverse<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, int, cudaStream_t);    \
+  template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, cudaStream_t); \
+  template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
+                                    cudaStream_t);                                                              \
+  template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
+  template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
+                                           uint32_t, cudaStream_t);
+
+}  // namespace fhb

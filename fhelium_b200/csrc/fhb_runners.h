@@ -1,0 +1,26 @@
+// Declarations of the per-(word, LOGN) cluster launchers; definitions in
+// fhb_runners.cuh, instantiated in fhb_inst_logn.cu (one object per LOGN).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fhb_context.h"
+
+namespace fhb {
+template <typename T, int LOGN>
+int run_forward(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool mont,
+                cudaStream_t st);
+template <typename T, int LOGN>
+int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
+                cudaStream_t st);
+template <typename T, int LOGN>
+int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
+                 cudaStream_t st);
+template <typename T, int LOGN>
+int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
+                int level, cudaStream_t st);
+template <typename T, int LOGN>
+int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
+template <typename T, int LOGN>
+int run_apply_prepared(const Context& c, const void* prepared, const void* key, void* acc0, void* acc1,
+                       int64_t batch, int level, uint32_t galois, cudaStream_t st);
+}  // namespace fhb

@@ -1,0 +1,513 @@
+"""CkksEngine: the reference's public CKKS API on B200 kernels.
+
+Mirrors fhelium.CkksEngine (fhelium/engine/ckks_engine.py:55-2400): the
+same method names, value states and level/scale bookkeeping.  Every residue
+operation runs in libfhb200.so through the C ABI (include/fhb200.h); the
+engine allocates outputs with torch on the engine's CUDA device, issues the
+calls on the current torch stream and never synchronises.  There is no CPU
+path: constructing an engine without CUDA or without the library raises.
+
+Randomness: the reference draws from the external `triton_csprng` package.
+This engine draws from a seeded torch generator on the device instead
+(uniform residues, uniform ternary secrets, rounded Gaussians with
+sigma = config.sigma), and encode rounds to nearest rather than
+stochastically.  Everything after encryption is a deterministic function of
+the keys and ciphertexts and matches the reference bit for bit.
+"""
+
+from __future__ import annotations
+
+import math
+from typing import Iterable, Sequence
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .config import CkksConfig, Preset
+from .encoding import decode_coefficients, encode_real_coefficients
+from .values import (Ciphertext, KeySwitchKey, PublicKey, RelinearizationKey, RotationKey, RotationKeySet,
+                     SecretKey)
+
+
+def galois_element(n: int, step: int, generator: int = 3) -> int:
+    """fhelium/engine/galois.py:10-26: g = gen^(+-step) mod 2N."""
+    e = -int(step) if generator == 5 else int(step)
+    return pow(generator, e % n, 2 * n)
+
+
+class CkksEngine:
+    def __init__(self, ckks_config: CkksConfig | Preset | dict | str | None = None, *,
+                 device: torch.device | str | None = None, allow_sk_gen: bool = True,
+                 galois_generator: int = 3, rng_seed: int | None = None, ntt_backend: str | None = None):
+        if ckks_config is None:
+            ckks_config = Preset.slots16384_scale40_levels16_int64
+        if isinstance(ckks_config, (Preset, str, dict)):
+            ckks_config = CkksConfig.parse(ckks_config)
+        self.config = ckks_config
+        if galois_generator not in (3, 5):
+            raise ValueError("galois_generator must be 3 or 5")
+        device = torch.device(device if device is not None else "cuda")
+        if device.type != "cuda":
+            raise ValueError("fhelium_b200 runs on CUDA devices only (no CPU path)")
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA is not available")
+        if device.index is None:
+            device = torch.device("cuda", torch.cuda.current_device())
+        self.device = device
+        self.galois_generator = galois_generator
+        self.allow_sk_gen = allow_sk_gen
+        self.ntt_backend = ntt_backend or "b200_cluster_radix16"
+        cfg = self.config
+        self.n = cfg.N
+        self.log_n = cfg.logN
+        self.num_q = cfg.num_q_primes
+        self.num_p = cfg.num_p_primes
+        self.dtype = cfg.torch_dtype
+        self.moduli = cfg.moduli
+        self.ctx = nat.NativeContext(64 if cfg.buffer_bit_length == 62 else 32, cfg.logN, cfg.moduli,
+                                     self.num_q, self.num_p, device)
+        self._gen = torch.Generator(device=device)
+        self._gen.manual_seed(0 if rng_seed is None else int(rng_seed))
+        self._secret_key: SecretKey | None = None
+        self._public_key: PublicKey | None = None
+        self._relinearization_key: RelinearizationKey | None = None
+        self._rotation_keys = RotationKeySet()
+        self._scratch: torch.Tensor | None = None
+        self.level_digits = self._digit_layout()
+
+    # ------------------------------------------------------------------
+    # layout
+    # ------------------------------------------------------------------
+    def _digit_layout(self) -> list[list[tuple[int, tuple[int, ...]]]]:
+        """(key_digit_index, prime ids) per level (fhelium/engine/rns/decomposition.py:18-53)."""
+        scale = list(range(self.num_q - 1))
+        w = self.num_p
+        level0 = [tuple(scale[s:s + w]) for s in range(0, len(scale), w)] + [(self.num_q - 1,)]
+        out = []
+        for level in range(self.num_q):
+            out.append([(kd, tuple(i for i in d if i >= level)) for kd, d in enumerate(level0)
+                        if any(i >= level for i in d)])
+        return out
+
+    @property
+    def num_slots(self) -> int:
+        return self.n // 2
+
+    @property
+    def public_level_count(self) -> int:
+        return self.config.num_scale_primes
+
+    @property
+    def key_digit_count(self) -> int:
+        return len(self.level_digits[0])
+
+    def _stream(self) -> int:
+        return nat.stream_of(self.device)
+
+    def _empty(self, *shape: int) -> torch.Tensor:
+        return torch.empty(shape, dtype=self.dtype, device=self.device)
+
+    def _scratch_for(self, batch: int, level: int) -> tuple[torch.Tensor, int]:
+        nbytes = int(self.ctx.lib.fhb_ckks_keyswitch_scratch_bytes(self.ctx.handle, batch, level))
+        if self._scratch is None or self._scratch.numel() < nbytes:
+            self._scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self._scratch, nbytes
+
+    def _check_ct(self, ct: Ciphertext) -> None:
+        if ct.data.device != self.device or ct.data.dtype != self.dtype:
+            raise ValueError("ciphertext tensor is not on this engine's device/dtype")
+        if ct.data.size(-1) != self.n or ct.limb_count != self.num_q - ct.level:
+            raise ValueError("ciphertext layout does not match its level")
+        if not ct.data.is_contiguous():
+            raise ValueError("ciphertext data must be contiguous")
+
+    # ------------------------------------------------------------------
+    # NTT domain transitions (fhelium/engine/ckks_engine.py:867-986)
+    # ------------------------------------------------------------------
+    def forward_ntt(self, x: torch.Tensor, row_start: int, *, montgomery_input: bool = False,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+        out = torch.empty_like(x) if out is None else out
+        rows = x.size(-2)
+        batch = x.numel() // (rows * self.n)
+        self.ctx.call("fhb_forward_ntt", nat.ptr(x), nat.ptr(out), batch, rows, row_start,
+                      1 if montgomery_input else 0, self._stream())
+        return out
+
+    def inverse_ntt(self, x: torch.Tensor, row_start: int, *, output: int = nat.INV_STANDARD,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+        out = torch.empty_like(x) if out is None else out
+        rows = x.size(-2)
+        batch = x.numel() // (rows * self.n)
+        self.ctx.call("fhb_inverse_ntt", nat.ptr(x), nat.ptr(out), batch, rows, row_start, output,
+                      self._stream())
+        return out
+
+    def coefficient_domain_to_ntt_domain(self, ct: Ciphertext) -> Ciphertext:
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard")
+        self._check_ct(ct)
+        data = self.forward_ntt(ct.data, ct.level)
+        return Ciphertext(data, ct.level, ct.scale, "ntt", "montgomery")
+
+    def ntt_domain_to_coefficient_domain(self, ct: Ciphertext) -> Ciphertext:
+        ct.assert_state(polynomial_domain="ntt", residue_representation="montgomery")
+        self._check_ct(ct)
+        data = self.inverse_ntt(ct.data, ct.level)
+        return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
+
+    # ------------------------------------------------------------------
+    # arithmetic
+    # ------------------------------------------------------------------
+    def _binary(self, op: int, a: torch.Tensor, b: torch.Tensor | None, row_start: int, *, b_mode: int = 0,
+                out: torch.Tensor | None = None) -> torch.Tensor:
+        out = torch.empty_like(a) if out is None else out
+        rows = a.size(-2)
+        batch = a.numel() // (rows * self.n)
+        self.ctx.call("fhb_rns_binary", op, nat.ptr(a), nat.ptr(b), nat.ptr(out), batch, rows, row_start,
+                      b_mode, self._stream())
+        return out
+
+    def add(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+        """Componentwise modular sum (fhelium/engine/ckks_engine.py:1708-1750)."""
+        self._assert_same_layout(lhs, rhs)
+        if lhs.scale != rhs.scale:
+            raise ValueError("add requires equal scales")
+        lazy = lhs.polynomial_domain == "ntt"
+        out = torch.empty_like(lhs.data)
+        polys = lhs.component_count * lhs.batch_size
+        self.ctx.call("fhb_ckks_add", nat.ptr(lhs.data), nat.ptr(rhs.data), nat.ptr(out), polys, lhs.level,
+                      1 if lazy else 0, self._stream())
+        return Ciphertext(out, lhs.level, lhs.scale, lhs.polynomial_domain, lhs.residue_representation)
+
+    def _assert_same_layout(self, a: Ciphertext, b: Ciphertext) -> None:
+        self._check_ct(a)
+        self._check_ct(b)
+        if (a.level, a.polynomial_domain, a.residue_representation, a.component_count, a.batch_shape) != \
+                (b.level, b.polynomial_domain, b.residue_representation, b.component_count, b.batch_shape):
+            raise ValueError("ciphertext layouts differ")
+
+    def multiply(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+        """NTT-domain tensor product (fhelium/engine/ckks_engine.py:1530-1606)."""
+        lhs.assert_state(polynomial_domain="ntt", residue_representation="montgomery", components=2)
+        self._assert_same_layout(lhs, rhs)
+        out = self._empty(3, *lhs.data.shape[1:])
+        self.ctx.call("fhb_ckks_multiply", nat.ptr(lhs.data), nat.ptr(rhs.data), nat.ptr(out), lhs.batch_size,
+                      lhs.level, self._stream())
+        return Ciphertext(out, lhs.level, lhs.scale * rhs.scale, "ntt", "montgomery")
+
+    def relinearize(self, ct: Ciphertext, relinearization_key: RelinearizationKey | None = None) -> Ciphertext:
+        """fhelium/engine/ckks_engine.py:1608-1675: returns coefficient/standard."""
+        ct.assert_state(polynomial_domain="ntt", residue_representation="montgomery", components=3)
+        self._check_ct(ct)
+        key = relinearization_key or self.relinearization_key
+        out = self._empty(2, *ct.data.shape[1:])
+        scratch, nbytes = self._scratch_for(ct.batch_size, ct.level)
+        self.ctx.call("fhb_ckks_relinearize", nat.ptr(ct.data), nat.ptr(key.data), nat.ptr(out), nat.ptr(scratch),
+                      nbytes, ct.batch_size, ct.level, 0, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
+
+    def rescale_to_next_drop_prime(self, *, level: int) -> int:
+        if level + 1 > self.public_level_count:
+            raise ValueError("no further public rescale level")
+        return self.moduli[level]
+
+    def rescale_to_next_output_scale(self, input_scale: float, *, level: int) -> float:
+        return float(input_scale) / float(self.rescale_to_next_drop_prime(level=level))
+
+    def rescale_to_next_level(self, ct: Ciphertext, *, rounding: str = "nearest") -> Ciphertext:
+        """fhelium/engine/ckks_rescale.py:339-377 (coefficient/standard input)."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard")
+        self._check_ct(ct)
+        if rounding not in ("nearest", "floor"):
+            raise ValueError("rounding must be 'nearest' or 'floor'")
+        scale = self.rescale_to_next_output_scale(ct.scale, level=ct.level)
+        out = self._empty(ct.component_count, *ct.batch_shape, ct.limb_count - 1, self.n)
+        self.ctx.call("fhb_ckks_rescale", nat.ptr(ct.data), nat.ptr(out), ct.component_count * ct.batch_size,
+                      ct.level, 1 if rounding == "nearest" else 0, self._stream())
+        return Ciphertext(out, ct.level + 1, scale, "coefficient", "standard")
+
+    def multiply_relinearize_rescale(self, lhs: Ciphertext, rhs: Ciphertext,
+                                     relinearization_key: RelinearizationKey | None = None,
+                                     *, rescale: bool = True) -> Ciphertext:
+        """multiply -> relinearize -> rescale_to_next_level in one fused
+        pipeline (four kernel launches); bit-identical to the three calls."""
+        lhs.assert_state(polynomial_domain="ntt", residue_representation="montgomery", components=2)
+        self._assert_same_layout(lhs, rhs)
+        key = relinearization_key or self.relinearization_key
+        out_limbs = lhs.limb_count - (1 if rescale else 0)
+        scale = lhs.scale * rhs.scale
+        if rescale:
+            scale = self.rescale_to_next_output_scale(scale, level=lhs.level)
+        out = self._empty(2, *lhs.batch_shape, out_limbs, self.n)
+        scratch, nbytes = self._scratch_for(lhs.batch_size, lhs.level)
+        self.ctx.call("fhb_ckks_multiply_relinearize", nat.ptr(lhs.data), nat.ptr(rhs.data), nat.ptr(key.data),
+                      nat.ptr(out), nat.ptr(scratch), nbytes, lhs.batch_size, lhs.level, 1 if rescale else 0,
+                      self._stream())
+        return Ciphertext(out, lhs.level + (1 if rescale else 0), scale, "coefficient", "standard")
+
+    # ------------------------------------------------------------------
+    # rotations (fhelium/engine/ckks_engine.py:2183-2300, 3726-3897)
+    # ------------------------------------------------------------------
+    def _canonical_step(self, step: int) -> int:
+        return int(step) % self.num_slots
+
+    def galois_element_for_step(self, step: int) -> int:
+        return galois_element(self.n, self._canonical_step(step) % self.n, self.galois_generator)
+
+    def rotation_key(self, rotation_step: int) -> RotationKey:
+        step = self._canonical_step(rotation_step)
+        if step not in self._rotation_keys:
+            if not self.allow_sk_gen:
+                raise KeyError(f"no rotation key for step {rotation_step}")
+            self._rotation_keys[step] = self.create_rotation_key(step)
+        return self._rotation_keys[step]
+
+    def rotate_by_step(self, ct: Ciphertext, rotation_step: int) -> Ciphertext:
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        step = self._canonical_step(rotation_step)
+        if step == 0:
+            return ct.clone()
+        return self.rotate_with_key(ct, self.rotation_key(step))
+
+    def rotate_with_key(self, ct: Ciphertext, key: RotationKey) -> Ciphertext:
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        out = torch.empty_like(ct.data)
+        scratch, nbytes = self._scratch_for(ct.batch_size, ct.level)
+        self.ctx.call("fhb_ckks_rotate", nat.ptr(ct.data), nat.ptr(key.data), nat.ptr(out), nat.ptr(scratch), nbytes,
+                      ct.batch_size, ct.level, key.galois_element, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
+
+    def prepare_rotation_digits(self, ct: Ciphertext) -> torch.Tensor:
+        """Hoisted ModUp of c1: [digit, *batch, Q_l + P, N] NTT-domain digits."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        b, level = ct.batch_size, ct.level
+        digits = self._empty(b, ct.limb_count, self.n)
+        self.ctx.call("fhb_ckks_modup_digits", nat.ptr(ct.c1), nat.ptr(digits), b, level, 1, self._stream())
+        nd = len(self.level_digits[level])
+        prepared = self._empty(nd, b, ct.limb_count + self.num_p, self.n)
+        self.ctx.call("fhb_ckks_prepare_rotation", nat.ptr(digits), nat.ptr(prepared), b, level, self._stream())
+        return prepared
+
+    def apply_prepared_rotation(self, ct: Ciphertext, prepared: torch.Tensor, key: RotationKey) -> Ciphertext:
+        b, level = ct.batch_size, ct.level
+        qp = ct.limb_count + self.num_p
+        t = self._empty(2, b, qp, self.n)
+        self.ctx.call("fhb_ckks_apply_prepared_rotation", nat.ptr(prepared), nat.ptr(key.data), nat.ptr(t[0]),
+                      nat.ptr(t[1]), b, level, key.galois_element, self._stream())
+        out = torch.empty_like(ct.data)
+        self.ctx.call("fhb_ckks_moddown", nat.ptr(t[0]), nat.ptr(t[1]), nat.ptr(ct.c0), None, nat.ptr(out), b,
+                      level, key.galois_element, 0, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
+
+    def rotate_many_by_steps(self, ct: Ciphertext, rotation_steps: Sequence[int], *,
+                             use_hoisting: bool = True) -> list[Ciphertext]:
+        steps = [self._canonical_step(s) for s in rotation_steps]
+        nonzero = [s for s in steps if s != 0]
+        if not use_hoisting or len(nonzero) < 2:
+            return [self.rotate_by_step(ct, s) for s in steps]
+        prepared = self.prepare_rotation_digits(ct)
+        return [ct.clone() if s == 0 else self.apply_prepared_rotation(ct, prepared, self.rotation_key(s))
+                for s in steps]
+
+    # ------------------------------------------------------------------
+    # keys (fhelium/engine/key_generator.py)
+    # ------------------------------------------------------------------
+    def _uniform_rows(self, *shape_prefix: int, rows: Iterable[int]) -> torch.Tensor:
+        rows = list(rows)
+        out = torch.empty((*shape_prefix, len(rows), self.n), dtype=torch.int64, device=self.device)
+        for j, pid in enumerate(rows):
+            out[..., j, :] = torch.randint(0, self.moduli[pid], (*shape_prefix, self.n), generator=self._gen,
+                                           device=self.device, dtype=torch.int64)
+        return out.to(self.dtype)
+
+    def _ternary(self, *shape: int) -> torch.Tensor:
+        return torch.randint(-1, 2, shape, generator=self._gen, device=self.device, dtype=torch.int64)
+
+    def _gaussian(self, *shape: int) -> torch.Tensor:
+        x = torch.randn(shape, generator=self._gen, device=self.device, dtype=torch.float64) * self.config.sigma
+        return torch.round(x).to(torch.int64)
+
+    def _lift(self, coeffs: torch.Tensor, row_start: int, rows: int) -> torch.Tensor:
+        """Signed int64 [..., N] -> canonical residues [..., rows, N]."""
+        coeffs = coeffs.contiguous()
+        batch = coeffs.numel() // self.n
+        out = self._empty(*coeffs.shape[:-1], rows, self.n)
+        self.ctx.call("fhb_rns_lift_signed", nat.ptr(coeffs), nat.ptr(out), batch, rows, row_start, self._stream())
+        return out
+
+    @property
+    def qp_rows(self) -> int:
+        return self.num_q + self.num_p
+
+    def create_secret_key(self) -> SecretKey:
+        s = self._lift(self._ternary(self.n), 0, self.qp_rows)
+        return SecretKey(self.forward_ntt(s, 0))
+
+    @property
+    def secret_key(self) -> SecretKey:
+        if self._secret_key is None:
+            if not self.allow_sk_gen:
+                raise RuntimeError("secret-key generation is disabled")
+            self._secret_key = self.create_secret_key()
+        return self._secret_key
+
+    def set_secret_key(self, key: SecretKey) -> None:
+        self._secret_key = key
+
+    def _encrypt_zero_qp(self, s: torch.Tensor, rows: int, uniform: torch.Tensor | None = None):
+        """(e - a s, a) over the first `rows` level-zero rows, NTT/Montgomery."""
+        a = self._uniform_rows(rows=range(rows)) if uniform is None else uniform
+        e = self.forward_ntt(self._lift(self._gaussian(self.n), 0, rows), 0)
+        a_s = self._binary(nat.OP_MONTGOMERY_MUL, a, s[:rows].contiguous(), 0)
+        return self._binary(nat.OP_SUB_LAZY, e, a_s, 0), a
+
+    def create_public_key(self, secret_key: SecretKey | None = None) -> PublicKey:
+        s = (secret_key or self.secret_key).data
+        k0, k1 = self._encrypt_zero_qp(s, self.num_q)
+        return PublicKey(torch.stack([k0, k1]))
+
+    @property
+    def public_key(self) -> PublicKey:
+        if self._public_key is None:
+            self._public_key = self.create_public_key()
+        return self._public_key
+
+    def create_key_switch_key(self, source: SecretKey, destination: SecretKey) -> KeySwitchKey:
+        """Digit d: (-a s_dst + e + P s_src on the digit's rows, a)
+        (fhelium/engine/key_generator.py:197-262)."""
+        P = math.prod(self.moduli[self.num_q:])
+        R = 1 << (62 if self.dtype == torch.int64 else 30)
+        p_mont = torch.tensor([(P * R) % q for q in self.moduli[: self.num_q]], dtype=self.dtype,
+                              device=self.device)
+        src_q = source.data[: self.num_q].contiguous()
+        p_src = self._binary(nat.OP_MONTGOMERY_MUL, src_q, p_mont, 0, b_mode=2)
+        digits = []
+        for kd, ids in self.level_digits[0]:
+            k0, k1 = self._encrypt_zero_qp(destination.data, self.qp_rows)
+            lo, hi = ids[0], ids[-1] + 1
+            k0[lo:hi] = self._binary(nat.OP_ADD_LAZY, k0[lo:hi].contiguous(), p_src[lo:hi].contiguous(), lo)
+            digits.append(torch.stack([k0, k1]))
+        return KeySwitchKey(torch.stack(digits))
+
+    def create_relinearization_key(self, secret_key: SecretKey | None = None) -> RelinearizationKey:
+        s = secret_key or self.secret_key
+        s2 = self._binary(nat.OP_MONTGOMERY_MUL, s.data, s.data, 0)
+        return RelinearizationKey(self.create_key_switch_key(SecretKey(s2), s).data)
+
+    @property
+    def relinearization_key(self) -> RelinearizationKey:
+        if self._relinearization_key is None:
+            self._relinearization_key = self.create_relinearization_key()
+        return self._relinearization_key
+
+    def set_relinearization_key(self, key: RelinearizationKey) -> None:
+        self._relinearization_key = key
+
+    def create_rotation_key(self, rotation_step: int, secret_key: SecretKey | None = None) -> RotationKey:
+        """Key from sigma_g(s) back to s (fhelium/engine/key_generator.py:364-412)."""
+        s = secret_key or self.secret_key
+        step = self._canonical_step(rotation_step)
+        g = self.galois_element_for_step(step)
+        coef = self.inverse_ntt(s.data, 0, output=nat.INV_MONTGOMERY)
+        rot = torch.empty_like(coef)
+        self.ctx.call("fhb_ckks_automorphism", nat.ptr(coef), nat.ptr(rot), 1, self.qp_rows, 0, g, self._stream())
+        rs = self.forward_ntt(rot, 0, montgomery_input=True)
+        ksk = self.create_key_switch_key(SecretKey(rs), s)
+        return RotationKey(ksk.data, rotation_step=step, galois_element=g)
+
+    def generate_rotation_keys(self, steps: Iterable[int]) -> None:
+        for st in steps:
+            self.rotation_key(st)
+
+    @property
+    def rotation_keys(self) -> RotationKeySet:
+        return self._rotation_keys
+
+    def set_rotation_key(self, key: RotationKey) -> None:
+        self._rotation_keys[self._canonical_step(key.rotation_step)] = key
+
+    # ------------------------------------------------------------------
+    # encode / encrypt / decrypt (fhelium/engine/ckks_engine.py:508-866)
+    # ------------------------------------------------------------------
+    def encode_coefficients(self, message, scale: float) -> torch.Tensor:
+        m = torch.as_tensor(message, device=self.device)
+        if m.ndim == 0:
+            m = m.expand(self.num_slots)
+        if m.size(-1) > self.num_slots:
+            raise ValueError("message longer than the slot count")
+        coeffs = encode_real_coefficients(m.to(self.device), self.n, self.galois_generator) * float(scale)
+        if coeffs.abs().max().item() >= 2.0 ** 62:
+            raise ValueError("encoded coefficients exceed the int64 range; lower the scale")
+        return torch.round(coeffs).to(torch.int64)
+
+    def encrypt_message(self, message, public_key: PublicKey | None = None, *, level: int = 0,
+                        scale: float | None = None) -> Ciphertext:
+        """Encode + public-key encryption, coefficient/standard output."""
+        if not 0 <= level < self.public_level_count:
+            raise ValueError("level out of range")
+        scale = float(self.config.default_scale if scale is None else scale)
+        pk = (public_key or self.public_key).data[:, level:].contiguous()
+        coeffs = self.encode_coefficients(message, scale)
+        batch_shape = tuple(coeffs.shape[:-1])
+        L = self.num_q - level
+        m = self.forward_ntt(self._lift(coeffs, level, L), level)
+        v = self.forward_ntt(self._lift(self._ternary(*batch_shape, self.n), level, L), level)
+        e0 = self.forward_ntt(self._lift(self._gaussian(*batch_shape, self.n), level, L), level)
+        e1 = self.forward_ntt(self._lift(self._gaussian(*batch_shape, self.n), level, L), level)
+        c0 = self._binary(nat.OP_MONTGOMERY_MUL, v, pk[0].contiguous(), level, b_mode=1)
+        c0 = self._binary(nat.OP_ADD_LAZY, c0, e0, level)
+        c0 = self._binary(nat.OP_ADD_LAZY, c0, m, level)
+        c1 = self._binary(nat.OP_MONTGOMERY_MUL, v, pk[1].contiguous(), level, b_mode=1)
+        c1 = self._binary(nat.OP_ADD_LAZY, c1, e1, level)
+        data = self.inverse_ntt(torch.stack([c0, c1]), level)
+        return Ciphertext(data, level, scale, "coefficient", "standard")
+
+    def _phase(self, ct: Ciphertext, secret_key: SecretKey | None = None) -> torch.Tensor:
+        """c0 + c1 s (+ c2 s^2) in coefficient/standard canonical form."""
+        s = (secret_key or self.secret_key).data[ct.level: self.num_q].contiguous()
+        data = ct.data if ct.polynomial_domain == "ntt" else self.forward_ntt(ct.data, ct.level)
+        acc = data[0].contiguous()
+        s_pow = s
+        for i in range(1, ct.component_count):
+            term = self._binary(nat.OP_MONTGOMERY_MUL, data[i].contiguous(), s_pow, ct.level, b_mode=1)
+            acc = self._binary(nat.OP_ADD_LAZY, acc, term, ct.level)
+            if i + 1 < ct.component_count:
+                s_pow = self._binary(nat.OP_MONTGOMERY_MUL, s_pow, s, ct.level)
+        return self.inverse_ntt(acc, ct.level)
+
+    def decrypt_coefficients(self, ct: Ciphertext, secret_key: SecretKey | None = None) -> np.ndarray:
+        """Centred integer coefficients of the phase (exact CRT over enough
+        trailing primes to cover the value's magnitude)."""
+        self._check_ct(ct)
+        phase = self._phase(ct, secret_key).cpu().numpy().astype(object)
+        need_bits = max(62, int(math.log2(max(ct.scale, 2.0))) + 30)
+        ids, bits = [], 0
+        for pid in reversed(range(ct.level, self.num_q)):
+            ids.append(pid)
+            bits += self.moduli[pid].bit_length() - 1
+            if bits >= need_bits:
+                break
+        rows = [pid - ct.level for pid in ids]
+        x = phase[..., rows[0], :]
+        mod = self.moduli[ids[0]]
+        for r, pid in zip(rows[1:], ids[1:]):
+            q = self.moduli[pid]
+            inv = pow(mod, -1, q)
+            t = ((phase[..., r, :] - x) % q) * inv % q
+            x = x + t * mod
+            mod *= q
+        x = np.where(x > mod // 2, x - mod, x)
+        return x
+
+    def decrypt_message(self, ct: Ciphertext, secret_key: SecretKey | None = None, *,
+                        is_real: bool = False) -> torch.Tensor:
+        coeffs = self.decrypt_coefficients(ct, secret_key)
+        vals = torch.tensor(np.asarray(coeffs, dtype=np.float64), dtype=torch.float64)
+        slots = decode_coefficients(vals, self.n, self.galois_generator) / ct.scale
+        return slots.real if is_real else slots
+
+    def __repr__(self) -> str:
+        return f"CkksEngine({self.config}, device={self.device})"

@@ -1,0 +1,212 @@
+/*
+ * fhelium_b200 C ABI: B200 (sm_100a) kernels for the CKKS evaluation path of
+ * visualDust/fhelium.
+ *
+ * Conventions shared by every entry point
+ * ----------------------------------------
+ *  - Residue buffers are device pointers to contiguous little-endian words,
+ *    uint64 for the int64 family (62-bit buffer, primes < 2^60) and uint32
+ *    for the int32 family (30-bit buffer, primes < 2^28), laid out exactly
+ *    like the reference's tensors: [*batch, limb, N] with limb j holding the
+ *    residue modulo prime id (level + j) of the level-zero chain
+ *    [scale q..., base q, p...]  (reference fhelium/core/ciphertext.py:26-67,
+ *    fhelium/engine/rns/chain.py).  Ciphertexts are [component, *batch, limb, N].
+ *  - Residue states follow the reference: NTT domain = Montgomery form
+ *    (x * 2^62 or x * 2^30 mod q), lazy in [0, 2q); coefficient domain =
+ *    standard form, canonical in [0, q).
+ *  - Every call is asynchronous on `stream` (a cudaStream_t, NULL = legacy
+ *    default stream), allocates nothing, and returns 0 on success, a
+ *    negative value for an invalid argument and 1000 + cudaError_t for a CUDA
+ *    failure; fhb_last_error() gives the message of the calling thread's last
+ *    failure.  Buffers must be 16-byte aligned and must not overlap unless an
+ *    entry point says so.
+ *  - Each entry point names the reference interface it replaces
+ *    (file:line in the reference project).
+ */
+#ifndef FHB200_H
+#define FHB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fhb_context fhb_context;
+typedef void* fhb_stream; /* cudaStream_t */
+
+enum fhb_inverse_output {
+  FHB_INV_MONTGOMERY = 0,    /* coefficient/Montgomery lazy [0, 2q) */
+  FHB_INV_STANDARD_LAZY = 1, /* coefficient/standard lazy [0, 2q) */
+  FHB_INV_STANDARD = 2,      /* coefficient/standard canonical [0, q) */
+  FHB_INV_CENTERED = 3       /* coefficient/standard centred (signed) */
+};
+
+int fhb_version(void);
+const char* fhb_last_error(void);
+
+/* Build the device tables (twiddles with Shoup companions, Montgomery
+ * constants, hybrid-digit Garner/extension constants for every level, ModDown
+ * and rescale constants) of one modulus chain on `device`.  moduli =
+ * num_q + num_p primes in reference order.  residue_bits is 64 or 32.
+ * Replaces the table construction of RnsRuntime / CkksEngine.__init__
+ * (fhelium/engine/rns/runtime.py:136-216, fhelium/engine/ckks_engine.py:
+ * 2952-3068).  This is set-up: it allocates and copies synchronously. */
+int fhb_context_create(int residue_bits, int log_n, const uint64_t* moduli, int num_q, int num_p,
+                       int device, fhb_context** out);
+int fhb_context_destroy(fhb_context* ctx);
+/* The primitive 2N-th root psi used for prime `prime_id` (same choice as
+ * fhelium/engine/ntt/plans/twiddles.py:10-20). */
+int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
+
+/* Forward negacyclic NTT of `batch` x `rows` polynomials whose rows are prime
+ * ids [row_start, row_start + rows).  input_montgomery = 0: standard input,
+ * output x R (forward_ntt_to_montgomery_*); = 1: Montgomery input
+ * (forward_ntt_montgomery_*).  Output lazy [0, 2q).  in == out allowed.
+ * Replaces fhelium_ntt_ops.forward_ntt_{to_montgomery,montgomery}_compact_
+ * grouped_smem_ (csrc/ops/ntt/forward_ntt.cpp:25-67,
+ * csrc/ops/ntt/cuda/forward_ntt_cuda.cpp:77-90). */
+int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
+                    int row_start, int input_montgomery, fhb_stream stream);
+
+/* Inverse NTT from NTT/Montgomery lazy input, output per fhb_inverse_output.
+ * in == out allowed.  Replaces fhelium_ntt_ops.inverse_ntt_{montgomery,
+ * to_standard_lazy,to_standard,to_centered}_compact_grouped_smem_
+ * (csrc/ops/ntt/inverse_ntt.cpp:23-73). */
+int fhb_inverse_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
+                    int row_start, int output_kind, fhb_stream stream);
+
+/* NTT-domain tensor product of two level-`level` ciphertexts a, b
+ * [2, batch, L, N] -> out [3, batch, L, N] (Montgomery lazy).  Replaces
+ * CkksEngine.multiply (fhelium/engine/ckks_engine.py:1530-1606: four
+ * fhelium_rns_ops.montgomery_mul + one add_lazy). */
+int fhb_ckks_multiply(const fhb_context* ctx, const void* a, const void* b, void* out, int64_t batch,
+                      int level, fhb_stream stream);
+
+/* Tensor product fused with the inverse NTT of all three products:
+ * out [3, batch, L, N] coefficient/standard canonical.  Equals multiply
+ * followed by the three inverse_to_standard_ calls that open
+ * CkksEngine.relinearize (fhelium/engine/ckks_engine.py:1655-1660). */
+int fhb_ckks_multiply_to_coefficient(const fhb_context* ctx, const void* a, const void* b, void* out,
+                                     int64_t batch, int level, fhb_stream stream);
+
+/* ModUp stage 1: Garner mixed-radix digits of every active hybrid digit of a
+ * coefficient/standard component comp [batch, L, N] -> digits [batch, L, N].
+ * galois != 1 first applies sigma_g (X -> X^g) to comp.  Replaces the
+ * per-digit fhelium_rns_ops.mixed_radix_decompose calls
+ * (fhelium/engine/hybrid_keyswitch.py:95-170,
+ * csrc/ops/rns/cuda/mixed_radix_cuda.cu:31-79) and, for rotations, the
+ * coefficient automorphism of c1 (csrc/ops/ckks/cuda/automorphism_cuda.cu:15-31). */
+int fhb_ckks_modup_digits(const fhb_context* ctx, const void* comp, void* digits, int64_t batch,
+                          int level, uint32_t galois, fhb_stream stream);
+
+/* Fused ModUp stage 2 + forward NTT + key inner product + inverse NTT.
+ * digits [batch, L, N] (from fhb_ckks_modup_digits); key [D, 2, QP0, N]
+ * NTT/Montgomery (reference KeySwitchKey layout, key_generator.py:243-262);
+ * acc0, acc1 [batch, L + P, N] receive coefficient/standard canonical rows.
+ * Replaces, per digit, mixed_radix_basis_extend_to_montgomery + the forward
+ * NTT + keyswitch_accumulate_digit_products_ and the two inverse NTTs of
+ * _moddown_switch_accumulators (fhelium/engine/hybrid_keyswitch.py:321-371,
+ * 530-546; csrc/ops/ckks/cuda/keyswitch_cuda.cu:198-292). */
+int fhb_ckks_keyswitch_core(const fhb_context* ctx, const void* digits, const void* key, void* acc0,
+                            void* acc1, int64_t batch, int level, fhb_stream stream);
+
+/* ModDown by P, fused with the final addition and optionally the rescale.
+ * t0, t1 [batch, L + P, N] canonical; add0, add1 [batch, L, N] canonical or
+ * NULL; add0 is read through sigma_g when add0_galois != 1.
+ * out [2, batch, L - (rescale ? 1 : 0), N] canonical.  Replaces
+ * fhelium_ckks_ops.keyswitch_moddown_qp_to_q (csrc/ops/ckks/ckks.cpp:82-84),
+ * the d + correction / add_canonical that follows it
+ * (fhelium/engine/ckks_engine.py:1664-1667, :3334-3350) and
+ * rescale_drop_leading_prime_nearest (csrc/ops/ckks/ckks.cpp:61-64). */
+int fhb_ckks_moddown(const fhb_context* ctx, const void* t0, const void* t1, const void* add0,
+                     const void* add1, void* out, int64_t batch, int level, uint32_t add0_galois,
+                     int rescale, fhb_stream stream);
+
+/* Hoisting: NTT-domain extended digits of one ModUp, prepared
+ * [D_l, batch, L + P, N].  Replaces HybridKeySwitcher.prepare_rotation_digits
+ * (fhelium/engine/hybrid_keyswitch.py:373-417). */
+int fhb_ckks_prepare_rotation(const fhb_context* ctx, const void* digits, void* prepared, int64_t batch,
+                              int level, fhb_stream stream);
+
+/* Hoisting: per step, NTT-domain sigma_g of the prepared digits, key inner
+ * product and inverse NTT into acc0/acc1 [batch, L + P, N].  Replaces
+ * _apply_prepared_rotation (fhelium/engine/hybrid_keyswitch.py:419-469). */
+int fhb_ckks_apply_prepared_rotation(const fhb_context* ctx, const void* prepared, const void* key,
+                                     void* acc0, void* acc1, int64_t batch, int level, uint32_t galois,
+                                     fhb_stream stream);
+
+/* Rescale `polys` coefficient/standard polynomials [polys, L, N] ->
+ * [polys, L - 1, N] by the leading prime (nearest or truncating).  Replaces
+ * fhelium_ckks_ops.rescale_drop_leading_prime_{nearest,truncate}
+ * (csrc/ops/ckks/ckks.cpp:57-72, csrc/ops/ckks/cuda/rescale_cuda.cu:22-92). */
+int fhb_ckks_rescale(const fhb_context* ctx, const void* in, void* out, int64_t polys, int level,
+                     int nearest, fhb_stream stream);
+
+/* Coefficient-domain Galois automorphism sigma_g of [batch, rows, N] (rows =
+ * prime ids [row_start, row_start + rows)), canonical output, in != out.
+ * Replaces fhelium_ckks_ops.apply_coefficient_galois_automorphism
+ * (csrc/ops/ckks/ckks.cpp:73-76). */
+int fhb_ckks_automorphism(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                          uint32_t galois, fhb_stream stream);
+
+/* out = a + b (mod q) over [polys, L, N]; lazy = 1 keeps [0, 2q)
+ * (fhelium_rns_ops.add_lazy), lazy = 0 gives canonical output
+ * (fhelium_rns_ops.add_canonical, csrc/ops/rns/rns_canonical_arithmetic.cpp:15-23). */
+int fhb_ckks_add(const fhb_context* ctx, const void* a, const void* b, void* out, int64_t polys,
+                 int level, int lazy, fhb_stream stream);
+
+enum fhb_rns_op {
+  FHB_OP_MONTGOMERY_MUL = 0, /* REDC(a b): fhelium_rns_ops.montgomery_mul */
+  FHB_OP_ADD_LAZY = 1,       /* fhelium_rns_ops.add_lazy */
+  FHB_OP_SUB_LAZY = 2,       /* fhelium_rns_ops.sub_lazy */
+  FHB_OP_ADD_CANONICAL = 3,  /* fhelium_rns_ops.add_canonical */
+  FHB_OP_SUB_CANONICAL = 4,  /* fhelium_rns_ops.sub_canonical */
+  FHB_OP_NEGATE = 5          /* canonical negation (b unused) */
+};
+
+/* Pointwise RNS arithmetic on [batch, rows, N] (rows = prime ids
+ * [row_start, row_start + rows)).  b_mode 0: b has a's shape; 1: b is
+ * [rows, N] shared by the batch; 2: b is [rows] row scalars
+ * (montgomery_mul_row_scalars_).  out may alias a.  Replaces
+ * csrc/ops/rns/rns_arithmetic.cpp:30-72 and
+ * csrc/ops/rns/rns_canonical_arithmetic.cpp:15-23. */
+int fhb_rns_binary(const fhb_context* ctx, int op, const void* a, const void* b, void* out, int64_t batch, int rows,
+                   int row_start, int b_mode, fhb_stream stream);
+
+/* Lift signed int64 coefficients [batch, N] into canonical residues
+ * [batch, rows, N].  Replaces fhelium_rns_ops.lift_centered_coefficients
+ * (csrc/ops/rns/rns_arithmetic.cpp:30-72). */
+int fhb_rns_lift_signed(const fhb_context* ctx, const int64_t* coefficients, void* out, int64_t batch, int rows,
+                        int row_start, fhb_stream stream);
+
+/* Scratch bytes needed by fhb_ckks_relinearize / fhb_ckks_rotate. */
+int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, int level);
+
+/* HMult-result relinearisation (optionally fused with the rescale):
+ * ct3 [3, batch, L, N] NTT/Montgomery -> out [2, batch, L (- 1), N]
+ * coefficient/standard canonical.  Replaces CkksEngine.relinearize
+ * (+ rescale_to_next_level) (fhelium/engine/ckks_engine.py:1608-1675,
+ * fhelium/engine/ckks_rescale.py:339-377).  scratch: device buffer of at
+ * least fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level) bytes. */
+int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* key, void* out,
+                         void* scratch, int64_t scratch_bytes, int64_t batch, int level, int rescale,
+                         fhb_stream stream);
+
+/* HMult + relinearise (+ rescale) in one call: a, b [2, batch, L, N]
+ * NTT/Montgomery -> out [2, batch, L (- 1), N] coefficient/standard. */
+int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const void* b, const void* key,
+                                  void* out, void* scratch, int64_t scratch_bytes, int64_t batch, int level,
+                                  int rescale, fhb_stream stream);
+
+/* Rotation with a direct key: ct [2, batch, L, N] coefficient/standard ->
+ * out [2, batch, L, N].  galois = Galois element g of the step.  Replaces
+ * CkksEngine._apply_rotation_key (fhelium/engine/ckks_engine.py:3822-3897). */
+int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,
+                    int64_t scratch_bytes, int64_t batch, int level, uint32_t galois, fhb_stream stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FHB200_H */

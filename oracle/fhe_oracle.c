@@ -350,3 +350,22 @@ void orc_ntt_automorphism(int64_t* out, const int64_t* in, int64_t batch,
   for (int64_t row = 0; row < batch * limbs; ++row)
     for (int64_t k = 0; k < n; ++k) out[row * n + k] = in[row * n + src[k]];
 }
+
+/* Bit-reversed psi^{br(k)} R and psi^{-br(k)} R mod q tables for one prime
+ * (fhelium/engine/ntt/plans/twiddles.py:45-84 followed by the Montgomery
+ * conversion of fhelium/engine/rns/runtime.py:201-203). */
+static uint64_t mulmod_u(uint64_t a, uint64_t b, uint64_t q) { return (uint64_t)((u128)a * b % q); }
+void orc_twiddles(uint64_t q, uint64_t psi, uint64_t psi_inv, int log_n, int radix_bits,
+                  int64_t* fwd, int64_t* inv) {
+  const int64_t n = (int64_t)1 << log_n;
+  const uint64_t r = (uint64_t)(((u128)1 << radix_bits) % q);
+  uint64_t pw = 1, pwi = 1;
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t br = 0;
+    for (int b = 0; b < log_n; ++b) br |= ((i >> b) & 1) << (log_n - 1 - b);
+    fwd[br] = (int64_t)mulmod_u(pw, r, q);
+    inv[br] = (int64_t)mulmod_u(pwi, r, q);
+    pw = mulmod_u(pw, psi, q);
+    pwi = mulmod_u(pwi, psi_inv, q);
+  }
+}

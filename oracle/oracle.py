@@ -297,15 +297,12 @@ class OracleContext:
     @cached_property
     def twiddles(self) -> tuple:
         """Montgomery-form bit-reversed psi and psi^-1 powers per prime."""
-        br = bit_reverse_table(self.log_n)
         fwd = np.empty((len(self.moduli), self.n), dtype=np.int64)
         inv = np.empty_like(fwd)
         for j, q in enumerate(self.moduli):
             psi = primitive_2nth_root(q, self.n)
-            f = _powers_mod(psi, self.n, q)[br]
-            i = _powers_mod(pow(psi, -1, q), self.n, q)[br]
-            fwd[j] = np.array([(int(v) * self.R) % q for v in f], dtype=np.int64)
-            inv[j] = np.array([(int(v) * self.R) % q for v in i], dtype=np.int64)
+            lib().orc_twiddles(ctypes.c_uint64(q), ctypes.c_uint64(psi), ctypes.c_uint64(pow(psi, -1, q)),
+                               INT(self.log_n), INT(self.radix_bits), _p(fwd[j]), _p(inv[j]))
         return fwd, inv
 
     # --- layout (fhelium/engine/rns/{chain,decomposition,layout}.py) ---------
