@@ -1,0 +1,395 @@
+"""Benchmark: CKKS HMult + relinearize + rescale throughput at logN=16, L=35.
+
+Workload (one step): 32 top-level ciphertext pairs of preset
+slots32768_scale40_levels34_int64 (N = 2^16, 35 Q primes + 4 P primes,
+dnum = 10 hybrid digits), each encrypting float64 messages uniform in
+[-0.05, 0.05] (seed 2 + rank), multiplied, relinearised with the
+relinearisation key and rescaled - the whole batch per step.
+
+  value       ops/s with the inputs resident in HBM (device time, CUDA events,
+              max over ranks); the batch (2.35 GB of inputs) is larger than
+              L2 (126 MB), so every step streams from HBM.
+  e2e         the same metric through the public API with the inputs in pinned
+              host memory: per step the host->device copy of both input
+              ciphertext batches and the device->host copy of the result are
+              inside the timed region.
+  roofline    the dominant kernel (fused key-switch core) timed alone with
+              CUDA events on its launch stream: algorithmic bytes per launch /
+              duration against the measured HBM copy bandwidth.
+  cpu_baseline  the reference's own CPU operators (compiled from its sources
+              into oracle/_ref) driven in the reference engine's order, on a
+              bounded sample (a few ciphertexts) with all host threads.
+
+Multi-GPU (torchrun): every rank runs the same per-GPU batch on its own
+ciphertexts (independent objects, no collective on the data path);
+`value` = all ranks' ops / max-over-ranks time ("scaling": "weak").
+
+`--impl reference` times the reference CPU implementation (the same
+operators) on this workload's config and prints its own JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PRESET = "slots32768_scale40_levels34_int64"
+METRIC = "hmult_relin_rescale_ops_per_s_logN16_L35"
+UNIT = "ops/s"
+CONFIG = {
+    "workload": "HMult+relinearize+rescale, preset slots32768_scale40_levels34_int64 "
+                "(logN=16, L=35 Q + 4 P primes, dnum=10), batch of top-level ciphertext pairs",
+    "logN": 16, "limbs": 35, "special_primes": 4, "dnum": 10,
+    "l2_policy": "inputs larger than L2 (2.35 GB per step at batch 32)",
+}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def _barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _max_over_ranks(x: float, ws: int, device) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _messages(batch, slots, seed):
+    g = torch.Generator().manual_seed(seed)
+    return torch.rand((batch, slots), dtype=torch.float64, generator=g) * 0.1 - 0.05
+
+
+def _time_events(fn, steps, stream):
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end) / steps
+
+
+def cpu_reference_sample(n_ops: int, threads: int, level: int = 0):
+    """Time the reference CPU operators on `n_ops` HMult+relin+rescale ops
+    (one ciphertext pair each).  Returns (ops/s, kind, sample text)."""
+    from fhelium_b200.config import CkksConfig
+    from oracle import oracle as orc
+    from oracle.ref_pipeline import ReferenceCpuPipeline, available
+    cfg = CkksConfig.parse(PRESET)
+    ctx = orc.OracleContext(cfg.moduli, cfg.logN, cfg.num_q_primes, cfg.num_p_primes, 62, cfg.scale_bits)
+    rng = np.random.default_rng(5)
+    rows = ctx.q_rows(level)
+    q = np.array(cfg.moduli, dtype=np.int64)
+
+    def uni(shape, rws, bound=1):
+        return (rng.integers(0, 1 << 62, size=(*shape, len(rws), cfg.N)) % (bound * q[rws][:, None])).astype(np.int64)
+
+    key = uni((len(ctx.digits_at_level(0)), 2), list(range(len(cfg.moduli))))
+    a, b = uni((2,), rows, 2), uni((2,), rows, 2)
+    if available():
+        pipe = ReferenceCpuPipeline(ctx, threads=threads)
+        ta, tb, tk = (torch.from_numpy(x) for x in (a, b, key))
+        pipe.multiply_relinearize_rescale(ta, tb, tk, level)  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(n_ops):
+            pipe.multiply_relinearize_rescale(ta, tb, tk, level)
+        dt = time.perf_counter() - t0
+        return n_ops / dt, "reference", threads, f"{n_ops} ops of one ciphertext pair at L=35 (reference CPU operators)"
+    # the oracle port (single thread C restatement)
+    t0 = time.perf_counter()
+    ctx.rescale(ctx.relinearize(ctx.multiply(a, b, level), key, level), level)
+    dt = time.perf_counter() - t0
+    return 1 / dt, "port", 1, "1 op of one ciphertext pair at L=35 (oracle C restatement)"
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    per_step = []
+    for _ in range(args.warmup):
+        cpu_reference_sample(1, threads)
+    for _ in range(args.steps):
+        v, kind, cores, sample = cpu_reference_sample(2, threads)
+        per_step.append(v)
+    value = statistics.median(per_step)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": dict(CONFIG, batch=1, parallelism="host threads"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-extras", action="store_true", help="skip rotation/parity/CPU legs")
+    args = ap.parse_args()
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+
+    from fhelium_b200 import _native as nat
+    from fhelium_b200.config import CkksConfig
+    from fhelium_b200.engine import CkksEngine
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfg = CkksConfig.parse(PRESET)
+    eng = CkksEngine(cfg, device=dev, rng_seed=1234 + rank)
+    B = args.batch
+    x = _messages(B, eng.num_slots, 2 + 2 * rank)
+    y = _messages(B, eng.num_slots, 3 + 2 * rank)
+    ca = eng.coefficient_domain_to_ntt_domain(eng.encrypt_message(x))
+    cb = eng.coefficient_domain_to_ntt_domain(eng.encrypt_message(y))
+    rlk = eng.relinearization_key
+    stream = torch.cuda.current_stream(dev)
+
+    state = {}
+
+    def step():
+        state["out"] = eng.multiply_relinearize_rescale(ca, cb, rlk)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clocks:
+        _barrier(ws)
+        torch.cuda.synchronize(dev)
+        ms = _time_events(step, args.steps, stream)
+        torch.cuda.synchronize(dev)
+        _barrier(ws)
+    ms = _max_over_ranks(ms, ws, dev)
+    value = ws * B / (ms / 1000.0)
+    launches_per_step = 4  # mul->INTT, ModUp digits, key-switch core, ModDown+rescale
+
+    # ---- end to end through the public API with host buffers -------------
+    host_a = ca.data.cpu().pin_memory()
+    host_b = cb.data.cpu().pin_memory()
+    out_host = torch.empty((2, B, cfg.num_q_primes - 1, cfg.N), dtype=torch.int64).pin_memory()
+    from fhelium_b200.values import Ciphertext
+
+    def e2e_step():
+        da = host_a.to(dev, non_blocking=True)
+        db = host_b.to(dev, non_blocking=True)
+        r = eng.multiply_relinearize_rescale(Ciphertext(da, 0, ca.scale, "ntt", "montgomery"),
+                                             Ciphertext(db, 0, cb.scale, "ntt", "montgomery"), rlk)
+        out_host.copy_(r.data, non_blocking=True)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize(dev)
+    _barrier(ws)
+    e2e_ms = _time_events(e2e_step, e2e_steps, stream)
+    e2e_ms = _max_over_ranks(e2e_ms, ws, dev)
+    h2d = host_a.numel() * 8 + host_b.numel() * 8
+    d2h = out_host.numel() * 8
+
+    # ---- dominant kernel alone: fused key-switch core --------------------
+    lib, h = eng.ctx.lib, eng.ctx.handle
+    L = cfg.num_q_primes
+    coef = torch.empty((3, B, L, cfg.N), dtype=torch.int64, device=dev)
+    digits = torch.empty((B, L, cfg.N), dtype=torch.int64, device=dev)
+    t = torch.empty((2, B, L + cfg.num_p_primes, cfg.N), dtype=torch.int64, device=dev)
+    s = stream.cuda_stream
+    kernels = {
+        "mul_to_coefficient": lambda: lib.fhb_ckks_multiply_to_coefficient(h, nat.ptr(ca.data), nat.ptr(cb.data),
+                                                                             nat.ptr(coef), B, 0, s),
+        "modup_digits": lambda: lib.fhb_ckks_modup_digits(h, nat.ptr(coef[2]), nat.ptr(digits), B, 0, 1, s),
+        "keyswitch_core": lambda: lib.fhb_ckks_keyswitch_core(h, nat.ptr(digits), nat.ptr(rlk.data), nat.ptr(t[0]),
+                                                              nat.ptr(t[1]), B, 0, s),
+        "moddown_rescale": lambda: lib.fhb_ckks_moddown(h, nat.ptr(t[0]), nat.ptr(t[1]), nat.ptr(coef[0]),
+                                                        nat.ptr(coef[1]), nat.ptr(state["out"].data), B, 0, 1, 1, s),
+    }
+    per_kernel = {}
+    for name, fn in kernels.items():
+        fn()
+        torch.cuda.synchronize(dev)
+        per_kernel[name] = _time_events(fn, max(2, min(args.steps, 5)), stream)
+    mib = 1 << 20
+    limb = cfg.N * 8
+    ks_bytes = B * (L + 2 * (L + cfg.num_p_primes)) * limb + 10 * 2 * (L + cfg.num_p_primes) * limb
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    achieved = ks_bytes / (per_kernel["keyswitch_core"] / 1000.0) / 1e9
+    step_bytes = B * (4 * L + 2 * (L - 1)) * limb + 10 * 2 * (L + cfg.num_p_primes) * limb
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "keyswitch_core_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tr = json.load(open(tpath))
+            traffic = tr["bytes_per_ciphertext"] * B + tr.get("bytes_fixed", 0)
+        except Exception:
+            traffic = None
+
+    extras = {}
+    if not args.no_extras:
+        # unfused reference-order path: multiply, relinearize, rescale separately
+        def plain_step():
+            state["plain"] = eng.rescale_to_next_level(eng.relinearize(eng.multiply(ca, cb), rlk))
+        plain_step()
+        torch.cuda.synchronize(dev)
+        plain_ms = _time_events(plain_step, max(2, min(args.steps, 5)), stream)
+        extras["plain_path_ops_per_s"] = B / (plain_ms / 1000.0)
+        extras["fused_equals_plain"] = bool(torch.equal(state["plain"].data, state["out"].data))
+        # rotation throughput (coefficient-domain ciphertexts at level 1)
+        rot_in = state["out"]
+        eng.rotation_key(1)
+        rot_ms = _time_events(lambda: eng.rotate_by_step(rot_in, 1), max(2, min(args.steps, 5)), stream)
+        extras["rotate_ops_per_s"] = B / (rot_ms / 1000.0)
+        steps16 = list(range(1, 17))
+        eng.generate_rotation_keys(steps16)
+        h_ms = _time_events(lambda: eng.rotate_many_by_steps(rot_in, steps16), 2, stream)
+        extras["hoisted_rotations_16_ops_per_s"] = 16 * B / (h_ms / 1000.0)
+        # decrypted error of the product (first ciphertext)
+        dec = eng.decrypt_message(Ciphertext(state["out"].data[:, :1].contiguous(), 1, state["out"].scale),
+                                  is_real=True)
+        extras["decrypt_max_abs_err"] = float((dec[0] - (x[0] * y[0])).abs().max())
+        # bit-exact vs the reference's own CPU operators on ciphertext 0
+        try:
+            from oracle import oracle as orc
+            from oracle.ref_pipeline import ReferenceCpuPipeline, available
+            if available() and rank == 0:
+                ctx = orc.OracleContext(cfg.moduli, cfg.logN, cfg.num_q_primes, cfg.num_p_primes, 62, cfg.scale_bits)
+                pipe = ReferenceCpuPipeline(ctx, threads=os.cpu_count())
+                ref = pipe.multiply_relinearize_rescale(ca.data[:, 0].cpu(), cb.data[:, 0].cpu(), rlk.data.cpu(), 0)
+                extras["bit_exact_vs_reference_cpu"] = bool(torch.equal(ref, state["out"].data[:, 0].cpu()))
+        except Exception as exc:  # report, never hide
+            extras["bit_exact_vs_reference_cpu"] = f"error: {exc}"
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_extras:
+        threads = os.cpu_count() or 1
+        v, kind, cores, sample = cpu_reference_sample(2, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    csum = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded uniform messages, engine-generated keys)",
+        "config": dict(CONFIG, batch_per_gpu=B, global_batch=B * ws, parallelism=f"independent ciphertexts x{ws}"),
+        "e2e": {"value": ws * B / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": {"kernel": "k_keyswitch_core", "bound": "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": ks_bytes, "launch_ms": per_kernel["keyswitch_core"],
+                     "note": "int64 Montgomery/Shoup arithmetic on CUDA cores: the kernel is integer-ALU bound"},
+        "kernel_ms": per_kernel,
+        "step_algorithmic_gbs": step_bytes / (ms / 1000.0) / 1e9,
+        "clocks": csum,
+        "cpu_baseline": cpu,
+        "extras": extras,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

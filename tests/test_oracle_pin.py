@@ -200,3 +200,20 @@ def test_automorphisms_match_reference(ref_ops, family, step):
     nsrc = orc.ntt_galois_source_indices(ctx.n, g)
     ref = _np(ref_ops.fhelium_ckks_ops.apply_ntt_galois_automorphism(_t(x, ctx), torch.from_numpy(nsrc)))
     np.testing.assert_array_equal(orc.ntt_automorphism(x, nsrc), ref)
+
+
+@pytest.mark.parametrize("family,level", [("int64", 0), ("int64_p4", 30), ("int32", 2)])
+def test_reference_pipeline_matches_oracle_engine_path(ref_ops, family, level):
+    """The reference's own CPU operators, driven in the reference engine's
+    order, equal the oracle's HMult -> relinearize -> rescale bit for bit."""
+    from oracle.ref_pipeline import ReferenceCpuPipeline
+    ctx = CONTEXTS[family]()
+    rng = np.random.default_rng(21)
+    rows = ctx.q_rows(level)
+    a, b = _lazy(rng, ctx, rows), _lazy(rng, ctx, rows)
+    key = np.stack([np.stack([_uniform(rng, ctx, ctx.qp_rows(0), batch=1)[0] for _ in range(2)])
+                    for _ in ctx.digits_at_level(0)])
+    pipe = ReferenceCpuPipeline(ctx)
+    got = _np(pipe.multiply_relinearize_rescale(_t(a, ctx), _t(b, ctx), _t(key, ctx), level))
+    want = ctx.rescale(ctx.relinearize(ctx.multiply(a, b, level), key, level), level)
+    np.testing.assert_array_equal(got, want)
