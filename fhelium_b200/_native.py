@@ -45,6 +45,8 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_relinearize": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_multiply_relinearize": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_rotate": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _U32, _P]),
+    "fhb_ckks_relinearize_noalloc": (_I, [_P, _P, _P, _P, _I64, _I, _I, _P]),
+    "fhb_ckks_relinearize_noalloc_max_scratch_bytes": (_I64, []),
 }
 
 OP_MONTGOMERY_MUL, OP_ADD_LAZY, OP_SUB_LAZY, OP_ADD_CANONICAL, OP_SUB_CANONICAL, OP_NEGATE = range(6)

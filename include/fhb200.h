@@ -193,6 +193,22 @@ int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* ke
                          void* scratch, int64_t scratch_bytes, int64_t batch, int level, int rescale,
                          fhb_stream stream);
 
+/* fhb_ckks_relinearize for callers that cannot allocate device memory.  No
+ * counterpart in the reference.  Same arguments and result as
+ * fhb_ckks_relinearize minus the scratch buffer: the scratch is a fixed
+ * 32 MiB array inside the library (fhb_ckks_relinearize_noalloc_max_scratch_bytes),
+ * held by every GPU that loads it until the process exits.  Meant for code
+ * that is handed only its input and output buffers, e.g. a plugin inside a
+ * host framework whose memory pool owns all device memory, or a serving loop
+ * that must not allocate.  Batches needing more than the fixed size
+ * (fhb_ckks_keyswitch_scratch_bytes) are rejected with an error.  The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress) and
+ * should come before any stream capture.  All calls share the array: calls
+ * that can overlap on the GPU (other streams, other host threads) race. */
+int fhb_ckks_relinearize_noalloc(const fhb_context* ctx, const void* ct3, const void* key, void* out, int64_t batch,
+                                 int level, int rescale, fhb_stream stream);
+int64_t fhb_ckks_relinearize_noalloc_max_scratch_bytes(void);
+
 /* HMult + relinearise (+ rescale) in one call: a, b [2, batch, L, N]
  * NTT/Montgomery -> out [2, batch, L (- 1), N] coefficient/standard. */
 int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const void* b, const void* key,
