@@ -81,13 +81,13 @@ k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
 template <typename T>
 struct InvEpilogue {
   T* dst;
-  PrimeInfo<T> p;
+  T q;
   T c, cs;
   int kind;
   __device__ __forceinline__ void operator()(int pos, T v) const {
-    v = Word<T>::shoup(v, c, cs, p.q);  // [0, 2q)
-    if (kind >= kInvStandard) v = csub(v, p.q);
-    if (kind == kInvCentered) v = v <= (p.q >> 1) ? v : v - p.q;
+    v = Word<T>::shoup(v, c, cs, q);  // [0, 2q)
+    if (kind >= kInvStandard) v = csub(v, q);
+    if (kind == kInvCentered) v = v <= (q >> 1) ? v : v - q;
     dst[pos] = v;
   }
 };
@@ -95,7 +95,7 @@ struct InvEpilogue {
 template <typename T>
 __device__ __forceinline__ InvEpilogue<T> make_inv_epilogue(T* dst, const PrimeInfo<T>& p, int kind,
                                                             bool montgomery_input) {
-  InvEpilogue<T> e{dst, p, p.ninv, p.ninv_s, kind};
+  InvEpilogue<T> e{dst, p.q, p.ninv, p.ninv_s, kind};
   if (kind != kInvMontgomery && montgomery_input) {
     e.c = p.ninv_rinv;
     e.cs = p.ninv_rinv_s;
@@ -244,14 +244,65 @@ __global__ void k_modup_digits(const T* __restrict__ comp, T* __restrict__ digit
 }
 
 // ---------------------------------------------------------------------------
+// Twiddle placement for kernels that transform several polynomials of one
+// prime (key switching): the CTA's forward (then inverse) twiddles are staged
+// once into shared memory when they fit next to the NTT working block.
+#ifndef FHB_TW_SMEM
+#define FHB_TW_SMEM 0
+#endif
+template <typename T, int LOGN>
+struct KsTw {
+  using G = NttGeom<T, LOGN>;
+  static constexpr size_t kData = size_t(G::kSmemElems) * sizeof(T);
+  static constexpr size_t kTwBytes = size_t(G::kM) * sizeof(TwPair<T>);
+  static constexpr bool kShared = FHB_TW_SMEM && kData + kTwBytes <= 227 * 1024;
+  const TwPair<T>* gf;
+  const TwPair<T>* gi;
+  TwPair<T>* st;
+  int rank;
+  __device__ __forceinline__ KsTw(unsigned char* smem, const TwPair<T>* fwd_row, const TwPair<T>* inv_row, int r)
+      : gf(fwd_row), gi(inv_row), st(reinterpret_cast<TwPair<T>*>(smem + kData)), rank(r) {}
+  __device__ __forceinline__ void stage(bool inverse) {
+    if constexpr (kShared) {
+      __syncthreads();
+      TwShared<T, LOGN>::stage(st, inverse ? gi : gf, rank, inverse);
+      __syncthreads();
+    }
+  }
+  __device__ __forceinline__ void forward(T* data, const PrimeInfo<T>& p, T (&v)[16]) const {
+    if constexpr (kShared) {
+      Ntt<T, LOGN, TwShared<T, LOGN>>::forward(data, TwShared<T, LOGN>{gf, st, rank * G::kM}, p.q, p.twice_q, rank, v);
+    } else {
+      Ntt<T, LOGN>::forward(data, TwGlobal<T, LOGN>(gf), p.q, p.twice_q, rank, v);
+    }
+  }
+  template <class Epi>
+  __device__ __forceinline__ void inverse(T* data, const PrimeInfo<T>& p, const T (&v)[16], Epi& epi) const {
+    if constexpr (kShared) {
+      Ntt<T, LOGN, TwShared<T, LOGN>>::inverse(data, TwShared<T, LOGN>{gi, st, rank * G::kM}, p.q, p.twice_q, rank, v,
+                                               epi);
+    } else {
+      Ntt<T, LOGN>::inverse(data, TwGlobal<T, LOGN>(gi), p.q, p.twice_q, rank, v, epi);
+    }
+  }
+};
+
 // Key-switch accumulators of one thread: 2 x 16 residues kept in shared
 // memory ([element][thread], conflict-free) when the CTA has room next to the
-// NTT working block, otherwise in the thread's own slots of the output rows.
+// NTT working block (and the twiddles are not staged there), otherwise in the
+// thread's own slots of the output rows.
 template <typename T, int LOGN>
 struct KsAcc {
   using G = NttGeom<T, LOGN>;
-  static constexpr bool kSmem = (G::kSmemElems + 2 * G::kM) * sizeof(T) <= 200 * 1024;
-  static constexpr size_t smem_bytes() { return (G::kSmemElems + (kSmem ? 2 * G::kM : 0)) * sizeof(T); }
+#ifndef FHB_KS_ACC_SMEM
+#define FHB_KS_ACC_SMEM 1
+#endif
+  static constexpr bool kSmem = FHB_KS_ACC_SMEM && !KsTw<T, LOGN>::kShared &&
+                                (G::kSmemElems + 2 * G::kM) * sizeof(T) <= 200 * 1024;
+  static constexpr size_t smem_bytes() {
+    return KsTw<T, LOGN>::kShared ? KsTw<T, LOGN>::kData + KsTw<T, LOGN>::kTwBytes
+                                  : (G::kSmemElems + (kSmem ? 2 * G::kM : 0)) * sizeof(T);
+  }
   T* c0;
   T* c1;
   int stride;
@@ -278,6 +329,32 @@ struct KsAcc {
     for (int e = 0; e < 16; ++e) v[e] = c[e * stride];
   }
 };
+
+// acc += v * key (both key components), streaming the key rows in 16-byte
+// pieces so that only two key words per component are live at a time.
+template <typename T, class Acc>
+__device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[16], const T* key0, const T* key1,
+                                        const PrimeInfo<T>& p) {
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(key0) + i);
+      const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(key1) + i);
+      acc.mac(2 * i, csub(v[2 * i], p.twice_q), a.x, b.x, p);
+      acc.mac(2 * i + 1, csub(v[2 * i + 1], p.twice_q), a.y, b.y, p);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const uint4 a = __ldg(reinterpret_cast<const uint4*>(key0) + i);
+      const uint4 b = __ldg(reinterpret_cast<const uint4*>(key1) + i);
+      acc.mac(4 * i, csub(v[4 * i], p.twice_q), a.x, b.x, p);
+      acc.mac(4 * i + 1, csub(v[4 * i + 1], p.twice_q), a.y, b.y, p);
+      acc.mac(4 * i + 2, csub(v[4 * i + 2], p.twice_q), a.z, b.z, p);
+      acc.mac(4 * i + 3, csub(v[4 * i + 3], p.twice_q), a.w, b.w, p);
+    }
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Fused ModUp stage 2 + forward NTT + key inner product + inverse NTT.
@@ -309,6 +386,8 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * 16;
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
+  KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(false);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
     const TwPair<T>* ext = lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid;
@@ -322,23 +401,20 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
       }
       s[G::sidx(i)] = y;
     }
-    T v[16], k0[16], k1[16];
-    Ntt<T, LOGN>::forward(s, twf, p.q, p.twice_q, rank, v);
+    T v[16];
+    tw.forward(s, p, v);
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
     const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
-    load16(key0, k0);
-    load16(key1, k1);
-#pragma unroll
-    for (int e = 0; e < 16; ++e) acc.mac(e, csub(v[e], p.twice_q), k0[e], k1[e], p);
+    key_mac<T>(acc, v, key0, key1, p);
   }
-  __syncthreads();
+  tw.stage(true);
   T v[16];
   acc.get(0, v);
   InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
-  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e0);
+  tw.inverse(s, p, v, e0);
   acc.get(1, v);
   InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
-  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e1);
+  tw.inverse(s, p, v, e1);
 }
 
 // Hoisting stage 1: materialise NTT-domain extended digits once
@@ -361,6 +437,8 @@ k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
   const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * 16;
+  KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(false);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
     const TwPair<T>* ext = lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid;
@@ -375,7 +453,7 @@ k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64
       s[G::sidx(i)] = y;
     }
     T v[16];
-    Ntt<T, LOGN>::forward(s, twf, p.q, p.twice_q, rank, v);
+    tw.forward(s, p, v);
 #pragma unroll
     for (int e = 0; e < 16; ++e) v[e] = csub(v[e], p.twice_q);
     store16(prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN + own, v);
@@ -401,6 +479,7 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
   const PrimeInfo<T> p = tabs.prime[pid];
   const int own = rank * G::kM + threadIdx.x * 16;
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
+  KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
     const T* pr = prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN;
@@ -412,14 +491,14 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
       acc.mac(e, __ldg(pr + src), __ldg(key0 + e), __ldg(key1 + e), p);
     }
   }
-  __syncthreads();
+  tw.stage(true);
   T v[16];
   acc.get(0, v);
   InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
-  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e0);
+  tw.inverse(s, p, v, e0);
   acc.get(1, v);
   InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
-  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, e1);
+  tw.inverse(s, p, v, e1);
 }
 
 // ---------------------------------------------------------------------------

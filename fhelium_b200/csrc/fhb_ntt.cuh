@@ -67,11 +67,72 @@ __device__ __forceinline__ TwPair<T> ldtw(const TwPair<T>* tw, int i) {
   }
 }
 
+// Twiddle accessors.  Forward stage st pairs use psi^{br(2^st + (ng >> (LOGN-st)))},
+// inverse half-span exponent j uses psi^{-br((N >> (j+1)) + (ng >> (j+1)))}.
+// TwGlobal reads the prime's row straight from global memory (L2).
 template <typename T, int LOGN>
+struct TwGlobal {
+  const TwPair<T>* g;
+  __device__ __forceinline__ TwGlobal(const TwPair<T>* row) : g(row) {}
+  __device__ __forceinline__ TwPair<T> fwd(int st, int ng) const { return ldtw(g, (1 << st) + (ng >> (LOGN - st))); }
+  __device__ __forceinline__ TwPair<T> inv(int j, int ng) const {
+    return ldtw(g, ((1 << LOGN) >> (j + 1)) + (ng >> (j + 1)));
+  }
+};
+
+// TwShared serves the CTA-local stages from a copy in shared memory of just
+// the twiddles this CTA's block [rank*M, (rank+1)*M) uses (M - 1 pairs), so a
+// kernel that transforms several polynomials of the same prime loads them
+// once.  Layout: forward local stage a at offset 2^a - 1 (2^a entries);
+// inverse local exponent j at offset M - (M >> j) (M >> (j+1) entries).
+// Cross-CTA stages (at most 7 distinct twiddles) still read global memory.
+template <typename T, int LOGN>
+struct TwShared {
+  using G = NttGeom<T, LOGN>;
+  const TwPair<T>* g;
+  const TwPair<T>* s;
+  int base;
+  __device__ __forceinline__ TwPair<T> fwd(int st, int ng) const {
+    if (st < G::kLogC) return ldtw(g, (1 << st) + (ng >> (LOGN - st)));
+    const int a = st - G::kLogC;
+    return s[(1 << a) - 1 + ((ng - base) >> (G::kLogM - a))];
+  }
+  __device__ __forceinline__ TwPair<T> inv(int j, int ng) const {
+    if (j >= G::kLogM) return ldtw(g, ((1 << LOGN) >> (j + 1)) + (ng >> (j + 1)));
+    return s[(G::kM - (G::kM >> j)) + ((ng - base) >> (j + 1))];
+  }
+  // Copy this CTA's forward (inverse = false) or inverse twiddles from the
+  // global row `row` into s_out (caller synchronises afterwards).
+  __device__ __forceinline__ static void stage(TwPair<T>* s_out, const TwPair<T>* row, int rank, bool inverse) {
+    for (int idx = threadIdx.x; idx < G::kM - 1; idx += blockDim.x) {
+      int src;
+      if (!inverse) {
+        const int a = 31 - __clz(idx + 1);
+        src = (1 << (G::kLogC + a)) + (rank << a) + (idx + 1 - (1 << a));
+      } else {
+        const int j = G::kLogM - 1 - (31 - __clz(G::kM - idx - 1));
+        const int off = G::kM - (G::kM >> j);
+        src = ((1 << LOGN) >> (j + 1)) + ((rank * G::kM) >> (j + 1)) + (idx - off);
+      }
+      s_out[idx] = ldtw(row, src);
+    }
+  }
+};
+
+template <typename T, int LOGN, class TW = TwGlobal<T, LOGN>>
 struct Ntt {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   static constexpr int E = G::kE;
+
+  // threadIdx.x behind an empty volatile asm: every transform recomputes its
+  // per-thread addresses instead of the compiler hoisting all of them out of
+  // the caller's digit loop (which used to exhaust the register budget).
+  __device__ __forceinline__ static int tid() {
+    int t = threadIdx.x;
+    asm volatile("" : "+r"(t));
+    return t;
+  }
 
   __device__ __forceinline__ static void fwd_bfly(T& x, T& y, const TwPair<T>& w, T q, T twoq) {
     const T xx = csub(x, twoq);
@@ -87,35 +148,32 @@ struct Ntt {
   }
 
   // ---- forward -----------------------------------------------------------
-  __device__ __forceinline__ static void fwd_cross(T* s, const TwPair<T>* tw, T q, T twoq, int rank) {
+  __device__ __forceinline__ static void fwd_cross(T* s, const TW& tw, T q, T twoq, int rank) {
     if constexpr (G::kC > 1) {
       cg::cluster_group cl = cg::this_cluster();
-      T* rs[G::kC];
-#pragma unroll
-      for (int c = 0; c < G::kC; ++c) rs[c] = cl.map_shared_rank(s, c);
       constexpr int kCols = G::kM / G::kC;
 #pragma unroll
       for (int u = 0; u < kCols / G::kThreads; ++u) {
-        const int m = rank * kCols + u * G::kThreads + threadIdx.x;
+        const int m = rank * kCols + u * G::kThreads + tid();
         const int sm = G::sidx(m);
         T x[G::kC];
 #pragma unroll
-        for (int c = 0; c < G::kC; ++c) x[c] = rs[c][sm];
+        for (int c = 0; c < G::kC; ++c) x[c] = *cl.map_shared_rank(s + sm, c);
 #pragma unroll
         for (int st = 0; st < G::kLogC; ++st) {
           const int h = G::kC >> (st + 1);
 #pragma unroll
           for (int c = 0; c < G::kC; ++c)
-            if (!(c & h)) fwd_bfly(x[c], x[c + h], ldtw(tw, (1 << st) + (c >> (G::kLogC - st))), q, twoq);
+            if (!(c & h)) fwd_bfly(x[c], x[c + h], tw.fwd(st, c * G::kM), q, twoq);
         }
 #pragma unroll
-        for (int c = 0; c < G::kC; ++c) rs[c][sm] = x[c];
+        for (int c = 0; c < G::kC; ++c) *cl.map_shared_rank(s + sm, c) = x[c];
       }
     }
   }
 
   template <int A, int K, bool LAST>
-  __device__ __forceinline__ static void fwd_pass(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  __device__ __forceinline__ static void fwd_pass(T* s, const TW& tw, T q, T twoq, int rank,
                                                   T (&out)[E]) {
     constexpr int kLogHl = G::kLogM - A - K;
     constexpr int kHl = 1 << kLogHl;
@@ -123,7 +181,7 @@ struct Ntt {
     constexpr int kNg = E >> K;
 #pragma unroll
     for (int u = 0; u < kNg; ++u) {
-      const int gid = LAST ? threadIdx.x * kNg + u : u * G::kThreads + threadIdx.x;
+      const int gid = LAST ? tid() * kNg + u : u * G::kThreads + tid();
       const int n0 = (gid & (kHl - 1)) | ((gid >> kLogHl) << (kLogHl + K));
       T v[kGs];
 #pragma unroll
@@ -137,7 +195,7 @@ struct Ntt {
         for (int i = 0; i < kGs; ++i)
           if (!(i & h)) {
             const int ng = ng0 + i * kHl;
-            fwd_bfly(v[i], v[i + h], ldtw(tw, (1 << st) + (ng >> (LOGN - st))), q, twoq);
+            fwd_bfly(v[i], v[i + h], tw.fwd(st, ng), q, twoq);
           }
       }
       if constexpr (LAST) {
@@ -151,7 +209,7 @@ struct Ntt {
   }
 
   template <int J>
-  __device__ __forceinline__ static void fwd_local(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  __device__ __forceinline__ static void fwd_local(T* s, const TW& tw, T q, T twoq, int rank,
                                                    T (&out)[E]) {
     constexpr int K = G::pass_k(J);
     constexpr int A = G::pass_a(J);
@@ -166,8 +224,8 @@ struct Ntt {
 
   // Forward transform of the block already staged in s (values < 4q).
   // On return out[e] holds the (lazy, < 4q) output at local position
-  // threadIdx.x * 16 + e of CTA `rank`.
-  __device__ __forceinline__ static void forward(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  // tid() * 16 + e of CTA `rank`.
+  __device__ __forceinline__ static void forward(T* s, const TW& tw, T q, T twoq, int rank,
                                                  T (&out)[E]) {
     if constexpr (G::kC > 1) {
       cg::cluster_group cl = cg::this_cluster();
@@ -183,14 +241,14 @@ struct Ntt {
   // ---- inverse -----------------------------------------------------------
   // Epilogue functor: epi(global_position, value in [0, 2q)).
   template <int L, int K, bool FIRST, bool STORE, class Epi>
-  __device__ __forceinline__ static void inv_pass(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  __device__ __forceinline__ static void inv_pass(T* s, const TW& tw, T q, T twoq, int rank,
                                                   const T (&in)[E], Epi& epi) {
     constexpr int kHl = 1 << L;
     constexpr int kGs = 1 << K;
     constexpr int kNg = E >> K;
 #pragma unroll
     for (int u = 0; u < kNg; ++u) {
-      const int gid = FIRST ? threadIdx.x * kNg + u : u * G::kThreads + threadIdx.x;
+      const int gid = FIRST ? tid() * kNg + u : u * G::kThreads + tid();
       const int n0 = (gid & (kHl - 1)) | ((gid >> L) << (L + K));
       T v[kGs];
 #pragma unroll
@@ -204,7 +262,7 @@ struct Ntt {
         for (int i = 0; i < kGs; ++i)
           if (!(i & h)) {
             const int ng = ng0 + i * kHl;
-            inv_bfly(v[i], v[i + h], ldtw(tw, (G::kN >> (j + 1)) + (ng >> (j + 1))), q, twoq);
+            inv_bfly(v[i], v[i + h], tw.inv(j, ng), q, twoq);
           }
       }
       if constexpr (STORE) {
@@ -218,7 +276,7 @@ struct Ntt {
   }
 
   template <int J, class Epi>
-  __device__ __forceinline__ static void inv_local(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  __device__ __forceinline__ static void inv_local(T* s, const TW& tw, T q, T twoq, int rank,
                                                    const T (&in)[E], Epi& epi) {
     constexpr int K = G::inv_k(J);
     constexpr int L = G::inv_l(J);
@@ -232,21 +290,18 @@ struct Ntt {
   }
 
   template <class Epi>
-  __device__ __forceinline__ static void inv_cross(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  __device__ __forceinline__ static void inv_cross(T* s, const TW& tw, T q, T twoq, int rank,
                                                    Epi& epi) {
     if constexpr (G::kC > 1) {
       cg::cluster_group cl = cg::this_cluster();
-      T* rs[G::kC];
-#pragma unroll
-      for (int c = 0; c < G::kC; ++c) rs[c] = cl.map_shared_rank(s, c);
       constexpr int kCols = G::kM / G::kC;
 #pragma unroll
       for (int u = 0; u < kCols / G::kThreads; ++u) {
-        const int m = rank * kCols + u * G::kThreads + threadIdx.x;
+        const int m = rank * kCols + u * G::kThreads + tid();
         const int sm = G::sidx(m);
         T x[G::kC];
 #pragma unroll
-        for (int c = 0; c < G::kC; ++c) x[c] = rs[c][sm];
+        for (int c = 0; c < G::kC; ++c) x[c] = *cl.map_shared_rank(s + sm, c);
 #pragma unroll
         for (int b = 0; b < G::kLogC; ++b) {
           const int j = G::kLogM + b;
@@ -255,7 +310,7 @@ struct Ntt {
           for (int c = 0; c < G::kC; ++c)
             if (!(c & h)) {
               const int ng = c * G::kM + m;
-              inv_bfly(x[c], x[c + h], ldtw(tw, (G::kN >> (j + 1)) + (ng >> (j + 1))), q, twoq);
+              inv_bfly(x[c], x[c + h], tw.inv(j, ng), q, twoq);
             }
         }
 #pragma unroll
@@ -269,7 +324,7 @@ struct Ntt {
   // with v in [0, 2q); s is scratch.  Ends with a cluster barrier so that
   // shared memory may be reused (and so that peers never outlive reads).
   template <class Epi>
-  __device__ __forceinline__ static void inverse(T* s, const TwPair<T>* tw, T q, T twoq, int rank,
+  __device__ __forceinline__ static void inverse(T* s, const TW& tw, T q, T twoq, int rank,
                                                  const T (&in)[E], Epi& epi) {
     inv_local<0>(s, tw, q, twoq, rank, in, epi);
     if constexpr (G::kC > 1) {

@@ -72,7 +72,7 @@ template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level,
                 cudaStream_t st) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
-  return launch_cluster<T, LOGN>(k_prepare_rotation<T, LOGN>, batch * qpl, ntt_smem<T, LOGN>(), st,
+  return launch_cluster<T, LOGN>(k_prepare_rotation<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
                                  (const T*)digits, (T*)prepared, batch, ql, qpl, level, c.qp(), tables<T>(c),
                                  level_tables<T>(c, level));
 }
