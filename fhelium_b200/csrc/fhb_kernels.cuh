@@ -12,13 +12,13 @@ namespace fhb {
 
 enum InverseOut : int { kInvMontgomery = 0, kInvStandardLazy = 1, kInvStandard = 2, kInvCentered = 3 };
 
-// ---- 16-residue thread-contiguous vector access ----------------------------
-template <typename T>
-__device__ __forceinline__ void load16(const T* p, T (&v)[16]) {
+// ---- thread-contiguous vector access (E residues per thread) ----------------------------
+template <typename T, int E>
+__device__ __forceinline__ void load16(const T* p, T (&v)[E]) {
   if constexpr (sizeof(T) == 8) {
     const ulonglong2* q = reinterpret_cast<const ulonglong2*>(p);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < E / 2; ++i) {
       const ulonglong2 x = q[i];
       v[2 * i] = x.x;
       v[2 * i + 1] = x.y;
@@ -26,22 +26,22 @@ __device__ __forceinline__ void load16(const T* p, T (&v)[16]) {
   } else {
     const uint4* q = reinterpret_cast<const uint4*>(p);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < E / 4; ++i) {
       const uint4 x = q[i];
       v[4 * i] = x.x; v[4 * i + 1] = x.y; v[4 * i + 2] = x.z; v[4 * i + 3] = x.w;
     }
   }
 }
-template <typename T>
-__device__ __forceinline__ void store16(T* p, const T (&v)[16]) {
+template <typename T, int E>
+__device__ __forceinline__ void store16(T* p, const T (&v)[E]) {
   if constexpr (sizeof(T) == 8) {
     ulonglong2* q = reinterpret_cast<ulonglong2*>(p);
 #pragma unroll
-    for (int i = 0; i < 8; ++i) q[i] = make_ulonglong2(v[2 * i], v[2 * i + 1]);
+    for (int i = 0; i < E / 2; ++i) q[i] = make_ulonglong2(v[2 * i], v[2 * i + 1]);
   } else {
     uint4* q = reinterpret_cast<uint4*>(p);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) q[i] = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    for (int i = 0; i < E / 4; ++i) q[i] = make_uint4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
   }
 }
 
@@ -71,11 +71,11 @@ k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
     if constexpr (TO_MONT) v = Word<T>::shoup(v, p.rmod, p.rmod_s, p.q);
     s[G::sidx(i)] = v;
   }
-  T v[16];
+  T v[G::kE];
   Ntt<T, LOGN>::forward(s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v);
 #pragma unroll
-  for (int e = 0; e < 16; ++e) v[e] = csub(v[e], p.twice_q);
-  store16(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * 16, v);
+  for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+  store16(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
 }
 
 template <typename T>
@@ -115,8 +115,8 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
   const int64_t poly = blockIdx.x / G::kC;
   const int pid = row_start + int(poly % rows);
   const PrimeInfo<T> p = tabs.prime[pid];
-  T v[16];
-  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * 16, v);
+  T v[G::kE];
+  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
   InvEpilogue<T> epi = make_inv_epilogue<T>(out + poly * G::kN, p, kind, true);
   Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, epi);
 }
@@ -141,8 +141,8 @@ k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __rest
   const int64_t rest = poly % (batch * limbs);
   const int pid = level + int(rest % limbs);
   const PrimeInfo<T> p = tabs.prime[pid];
-  const int64_t off = rest * G::kN + int64_t(rank) * G::kM + threadIdx.x * 16;
-  T v[16], x[16], y[16];
+  const int64_t off = rest * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  T v[G::kE], x[G::kE], y[G::kE];
   const T* a0 = a + off;
   const T* a1 = a + comp_stride + off;
   const T* b0 = b + off;
@@ -150,12 +150,12 @@ k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __rest
   load16(comp == 2 ? a1 : a0, x);
   load16(comp == 0 ? b0 : b1, y);
 #pragma unroll
-  for (int e = 0; e < 16; ++e) v[e] = W::mont(x[e], y[e], p.q, p.neg_inv);
+  for (int e = 0; e < G::kE; ++e) v[e] = W::mont(x[e], y[e], p.q, p.neg_inv);
   if (comp == 1) {
     load16(a1, x);
     load16(b0, y);
 #pragma unroll
-    for (int e = 0; e < 16; ++e) v[e] = csub(v[e] + W::mont(x[e], y[e], p.q, p.neg_inv), p.twice_q);
+    for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e] + W::mont(x[e], y[e], p.q, p.neg_inv), p.twice_q);
   }
   InvEpilogue<T> epi = make_inv_epilogue<T>(out + comp * comp_stride + rest * G::kN, p, kInvStandard, true);
   Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, epi);
@@ -269,7 +269,7 @@ struct KsTw {
       __syncthreads();
     }
   }
-  __device__ __forceinline__ void forward(T* data, const PrimeInfo<T>& p, T (&v)[16]) const {
+  __device__ __forceinline__ void forward(T* data, const PrimeInfo<T>& p, T (&v)[G::kE]) const {
     if constexpr (kShared) {
       Ntt<T, LOGN, TwShared<T, LOGN>>::forward(data, TwShared<T, LOGN>{gf, st, rank * G::kM}, p.q, p.twice_q, rank, v);
     } else {
@@ -277,7 +277,7 @@ struct KsTw {
     }
   }
   template <class Epi>
-  __device__ __forceinline__ void inverse(T* data, const PrimeInfo<T>& p, const T (&v)[16], Epi& epi) const {
+  __device__ __forceinline__ void inverse(T* data, const PrimeInfo<T>& p, const T (&v)[G::kE], Epi& epi) const {
     if constexpr (kShared) {
       Ntt<T, LOGN, TwShared<T, LOGN>>::inverse(data, TwShared<T, LOGN>{gi, st, rank * G::kM}, p.q, p.twice_q, rank, v,
                                                epi);
@@ -317,27 +317,27 @@ struct KsAcc {
       stride = 1;
     }
 #pragma unroll
-    for (int e = 0; e < 16; ++e) c0[e * stride] = c1[e * stride] = 0;
+    for (int e = 0; e < G::kE; ++e) c0[e * stride] = c1[e * stride] = 0;
   }
   __device__ __forceinline__ void mac(int e, T x, T k0, T k1, const PrimeInfo<T>& p) {
     c0[e * stride] = csub(c0[e * stride] + Word<T>::mont(x, k0, p.q, p.neg_inv), p.twice_q);
     c1[e * stride] = csub(c1[e * stride] + Word<T>::mont(x, k1, p.q, p.neg_inv), p.twice_q);
   }
-  __device__ __forceinline__ void get(int which, T (&v)[16]) const {
+  __device__ __forceinline__ void get(int which, T (&v)[G::kE]) const {
     const T* c = which ? c1 : c0;
 #pragma unroll
-    for (int e = 0; e < 16; ++e) v[e] = c[e * stride];
+    for (int e = 0; e < G::kE; ++e) v[e] = c[e * stride];
   }
 };
 
 // acc += v * key (both key components), streaming the key rows in 16-byte
 // pieces so that only two key words per component are live at a time.
-template <typename T, class Acc>
-__device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[16], const T* key0, const T* key1,
+template <typename T, class Acc, int E>
+__device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[E], const T* key0, const T* key1,
                                         const PrimeInfo<T>& p) {
   if constexpr (sizeof(T) == 8) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < E / 2; ++i) {
       const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(key0) + i);
       const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(key1) + i);
       acc.mac(2 * i, csub(v[2 * i], p.twice_q), a.x, b.x, p);
@@ -345,7 +345,7 @@ __device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[16], const T* key
     }
   } else {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < E / 4; ++i) {
       const uint4 a = __ldg(reinterpret_cast<const uint4*>(key0) + i);
       const uint4 b = __ldg(reinterpret_cast<const uint4*>(key1) + i);
       acc.mac(4 * i, csub(v[4 * i], p.twice_q), a.x, b.x, p);
@@ -384,7 +384,7 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
   const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
-  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * 16;
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
@@ -401,14 +401,14 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
       }
       s[G::sidx(i)] = y;
     }
-    T v[16];
+    T v[G::kE];
     tw.forward(s, p, v);
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
     const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
-    key_mac<T>(acc, v, key0, key1, p);
+    key_mac(acc, v, key0, key1, p);
   }
   tw.stage(true);
-  T v[16];
+  T v[G::kE];
   acc.get(0, v);
   InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e0);
@@ -436,7 +436,7 @@ k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
   const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
-  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * 16;
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
   for (int a = 0; a < lt.num_digits; ++a) {
@@ -452,10 +452,10 @@ k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64
       }
       s[G::sidx(i)] = y;
     }
-    T v[16];
+    T v[G::kE];
     tw.forward(s, p, v);
 #pragma unroll
-    for (int e = 0; e < 16; ++e) v[e] = csub(v[e], p.twice_q);
+    for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
     store16(prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN + own, v);
   }
 }
@@ -477,7 +477,7 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
   const int jrow = int(poly % qp_limbs);
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
-  const int own = rank * G::kM + threadIdx.x * 16;
+  const int own = rank * G::kM + threadIdx.x * G::kE;
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   for (int a = 0; a < lt.num_digits; ++a) {
@@ -486,13 +486,13 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
     const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
 #pragma unroll 4
-    for (int e = 0; e < 16; ++e) {
+    for (int e = 0; e < G::kE; ++e) {
       const int src = galois ? galois_ntt_source(own + e, LOGN, galois) : own + e;
       acc.mac(e, __ldg(pr + src), __ldg(key0 + e), __ldg(key1 + e), p);
     }
   }
   tw.stage(true);
-  T v[16];
+  T v[G::kE];
   acc.get(0, v);
   InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e0);

@@ -42,13 +42,25 @@ struct NttGeom {
   static constexpr int kC = 1 << kLogC;
   static constexpr int kLogM = LOGN - kLogC;
   static constexpr int kM = 1 << kLogM;
-  static constexpr int kE = 16;  // residues per thread
+#ifndef FHB_NTT_E
+#define FHB_NTT_E 8
+#endif
+  // Residues per thread.  8 (1024 threads for M = 8192) beats 16 (512
+  // threads): the kernels are latency bound and twice the resident warps
+  // hide more of it (key-switch core 33.9 vs 43.4 ms at L=35, batch 32).
+  static constexpr int kE = FHB_NTT_E;
   static constexpr int kThreads = kM / kE;
   static constexpr int kPadShift = sizeof(T) == 8 ? 4 : 5;
   static constexpr int kSmemElems = kM + (kM >> kPadShift);
-  static constexpr int kPasses = (kLogM + 3) / 4;
-  static constexpr int kNum4 = kLogM - 3 * kPasses;
-  static constexpr int pass_k(int j) { return j >= kPasses - kNum4 ? 4 : 3; }
+  // Register passes: radix-8/16 (3 or 4 stages) for 16 residues per thread,
+  // radix-8 for 8; the last forward pass is always a full one, so its
+  // outputs are thread-contiguous.
+  static constexpr int kMaxK = kE == 16 ? 4 : 3;
+  static constexpr int kPasses = kMaxK == 4 ? (kLogM + 3) / 4 : (kLogM + 2) / 3;
+  static constexpr int kNum4 = kMaxK == 4 ? kLogM - 3 * kPasses : 0;
+  static constexpr int pass_k(int j) {
+    return kMaxK == 4 ? (j >= kPasses - kNum4 ? 4 : 3) : (j == 0 ? kLogM - 3 * (kPasses - 1) : 3);
+  }
   static constexpr int pass_a(int j) { return j == 0 ? 0 : pass_a(j - 1) + pass_k(j - 1); }
   // inverse pass j is forward pass kPasses-1-j; its lowest half-span exponent
   static constexpr int inv_k(int j) { return pass_k(kPasses - 1 - j); }
@@ -183,20 +195,25 @@ struct Ntt {
     for (int u = 0; u < kNg; ++u) {
       const int gid = LAST ? tid() * kNg + u : u * G::kThreads + tid();
       const int n0 = (gid & (kHl - 1)) | ((gid >> kLogHl) << (kLogHl + K));
+      const int ng0 = rank * G::kM + n0;
+      // All 2^K - 1 twiddles of the group are fetched before any butterfly so
+      // their (L1/L2) latencies overlap; stage b uses 2^b of them, selected
+      // by the top b bits of the element index within the group.
+      TwPair<T> w[kGs - 1];
+#pragma unroll
+      for (int b = 0; b < K; ++b)
+#pragma unroll
+        for (int j = 0; j < (1 << b); ++j)
+          w[(1 << b) - 1 + j] = tw.fwd(G::kLogC + A + b, ng0 + ((j << (K - b)) << kLogHl));
       T v[kGs];
 #pragma unroll
       for (int i = 0; i < kGs; ++i) v[i] = s[G::sidx(n0 + i * kHl)];
-      const int ng0 = rank * G::kM + n0;
 #pragma unroll
       for (int b = 0; b < K; ++b) {
-        const int st = G::kLogC + A + b;
         const int h = kGs >> (b + 1);
 #pragma unroll
         for (int i = 0; i < kGs; ++i)
-          if (!(i & h)) {
-            const int ng = ng0 + i * kHl;
-            fwd_bfly(v[i], v[i + h], tw.fwd(st, ng), q, twoq);
-          }
+          if (!(i & h)) fwd_bfly(v[i], v[i + h], w[(1 << b) - 1 + (i >> (K - b))], q, twoq);
       }
       if constexpr (LAST) {
 #pragma unroll
@@ -250,20 +267,24 @@ struct Ntt {
     for (int u = 0; u < kNg; ++u) {
       const int gid = FIRST ? tid() * kNg + u : u * G::kThreads + tid();
       const int n0 = (gid & (kHl - 1)) | ((gid >> L) << (L + K));
+      const int ng0 = rank * G::kM + n0;
+      // Prefetch the group's 2^K - 1 twiddles: stage b (half span 2^(L+b))
+      // has 2^(K-1-b) of them, selected by the element-index bits above b.
+      TwPair<T> w[kGs - 1];
+#pragma unroll
+      for (int b = 0; b < K; ++b)
+#pragma unroll
+        for (int m = 0; m < (1 << (K - 1 - b)); ++m)
+          w[kGs - (kGs >> b) + m] = tw.inv(L + b, ng0 + ((m << (b + 1)) << L));
       T v[kGs];
 #pragma unroll
       for (int i = 0; i < kGs; ++i) v[i] = FIRST ? in[u * kGs + i] : s[G::sidx(n0 + i * kHl)];
-      const int ng0 = rank * G::kM + n0;
 #pragma unroll
       for (int b = 0; b < K; ++b) {
-        const int j = L + b;  // half-span exponent
         const int h = 1 << b;
 #pragma unroll
         for (int i = 0; i < kGs; ++i)
-          if (!(i & h)) {
-            const int ng = ng0 + i * kHl;
-            inv_bfly(v[i], v[i + h], tw.inv(j, ng), q, twoq);
-          }
+          if (!(i & h)) inv_bfly(v[i], v[i + h], w[kGs - (kGs >> b) + (i >> (b + 1))], q, twoq);
       }
       if constexpr (STORE) {
 #pragma unroll
