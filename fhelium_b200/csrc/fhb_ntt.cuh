@@ -48,7 +48,8 @@ struct NttGeom {
   // Residues per thread.  8 (1024 threads for M = 8192) beats 16 (512
   // threads): the kernels are latency bound and twice the resident warps
   // hide more of it (key-switch core 33.9 vs 43.4 ms at L=35, batch 32).
-  static constexpr int kE = FHB_NTT_E;
+  // (16 when 8 would need more than 1024 threads: N = 2^17, M = 16384.)
+  static constexpr int kE = (kM / FHB_NTT_E > 1024) ? 16 : FHB_NTT_E;
   static constexpr int kThreads = kM / kE;
   static constexpr int kPadShift = sizeof(T) == 8 ? 4 : 5;
   static constexpr int kSmemElems = kM + (kM >> kPadShift);
