@@ -156,6 +156,45 @@ def _time_events(fn, steps, stream):
     return start.elapsed_time(end) / steps
 
 
+def ntt_int32_primes(count: int = 36, log_n: int = 16) -> list[int]:
+    """The first `count` distinct catalog primes with 4q < 2^30 and q = 1 mod 2N
+    from the int32 families (25-bit scale primes, then 28-bit message primes)."""
+    from fhelium_b200.config import prime_catalog
+    cat = prime_catalog()
+    n = 1 << log_n
+    out = []
+    for q in list(cat["scale"][(25, n)]) + list(cat["message"][(28, n)]):
+        if q not in out and 4 * q < 2 ** 30 and (q - 1) % (2 * n) == 0:
+            out.append(q)
+    return out[:count]
+
+
+def ntt_leg(dev, stream, steps):
+    """Standalone forward + inverse NTT: N = 2^16, 36 int32 limbs, batch 64,
+    residues uniform in [0, q_i) (seed 1).  Round trip checked bit-exact."""
+    from fhelium_b200 import _native as nat
+    primes = ntt_int32_primes()
+    ctx = nat.NativeContext(32, 16, primes, len(primes) - 1, 1, dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(1)
+    B, L, N = 64, len(primes), 1 << 16
+    q = torch.tensor(primes, dtype=torch.int64, device=dev).view(1, L, 1)
+    x = (torch.randint(0, 1 << 62, (B, L, N), generator=g, device=dev, dtype=torch.int64) % q).to(torch.int32)
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    s = stream.cuda_stream
+    fwd = lambda: nat.check(ctx.lib.fhb_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), B, L, 0, 0, s), "ntt")
+    inv = lambda: nat.check(ctx.lib.fhb_inverse_ntt(ctx.handle, y.data_ptr(), z.data_ptr(), B, L, 0, 2, s), "intt")
+    fwd_ms = _time_events(fwd, max(3, steps), stream)
+    inv_ms = _time_events(inv, max(3, steps), stream)
+    exact = bool(torch.equal(x, z))
+    nbytes = 2 * B * L * N * 4  # read + write per direction
+    ctx.close()
+    return {"forward_ms": fwd_ms, "inverse_ms": inv_ms, "roundtrip_bit_exact": exact,
+            "forward_gbs": nbytes / (fwd_ms / 1e3) / 1e9, "inverse_gbs": nbytes / (inv_ms / 1e3) / 1e9,
+            "limb_ntts_per_s": 2 * B * L / ((fwd_ms + inv_ms) / 1e3)}
+
+
 def cpu_reference_sample(n_ops: int, threads: int, level: int = 0):
     """Time the reference CPU operators on `n_ops` HMult+relin+rescale ops
     (one ciphertext pair each).  Returns (ops/s, kind, sample text)."""
@@ -342,6 +381,7 @@ def main() -> int:
         eng.generate_rotation_keys(steps16)
         h_ms = _time_events(lambda: eng.rotate_many_by_steps(rot_in, steps16), 2, stream)
         extras["hoisted_rotations_16_ops_per_s"] = 16 * B / (h_ms / 1000.0)
+        extras["ntt_int32_logN16_36limbs_batch64"] = ntt_leg(dev, stream, args.steps)
         # decrypted error of the product (first ciphertext)
         dec = eng.decrypt_message(Ciphertext(state["out"].data[:, :1].contiguous(), 1, state["out"].scale),
                                   is_real=True)
