@@ -45,6 +45,9 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_relinearize": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_multiply_relinearize": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_rotate": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _U32, _P]),
+    "fhb_ckks_monomial": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
+    "fhb_ckks_modraise": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
+    "fhb_rns_add_constant": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_relinearize_noalloc": (_I, [_P, _P, _P, _P, _I64, _I, _I, _P]),
     "fhb_ckks_relinearize_noalloc_max_scratch_bytes": (_I64, []),
 }

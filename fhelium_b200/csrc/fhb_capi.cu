@@ -179,6 +179,31 @@ int lift_signed(const Context& c, const void* x, void* out, int64_t batch, int r
   return cuda_status(cudaGetLastError(), "k_lift_signed");
 }
 
+template <typename T>
+int monomial(const Context& c, const void* in, void* out, int64_t batch, int rows, int row_start, int k,
+             cudaStream_t st) {
+  k_monomial<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
+      (const T*)in, (T*)out, batch, rows, row_start, c.log_n, k, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_monomial");
+}
+
+template <typename T>
+int modraise(const Context& c, const void* in, void* out, int64_t batch, int rows, int row_start, int src_prime,
+             cudaStream_t st) {
+  k_modraise<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
+      (const T*)in, (T*)out, batch, rows, row_start, src_prime, c.log_n, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_modraise");
+}
+
+template <typename T>
+int add_constant(const Context& c, void* data, const void* constants, int64_t batch, int rows, int row_start,
+                 int all_slots, cudaStream_t st) {
+  const int64_t total = all_slots ? (batch * rows << c.log_n) : batch * rows;
+  k_add_constant<T><<<elementwise_grid(total), 256, 0, st>>>((T*)data, (const T*)constants, batch, rows, row_start,
+                                                             c.log_n, all_slots, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_add_constant");
+}
+
 #define FHB_WORD(FN, ...) (c.bits == 64 ? FN<uint64_t>(__VA_ARGS__) : FN<uint32_t>(__VA_ARGS__))
 
 int64_t word_bytes(const Context& c) { return c.bits / 8; }
@@ -402,6 +427,36 @@ int fhb_rns_lift_signed(const fhb_context* ctx, const int64_t* coefficients, voi
   TRY(fhb::check_ptr(out, "out"));
   if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
   return FHB_WORD(fhb::lift_signed, c, coefficients, out, batch, rows, row_start, st);
+}
+
+int fhb_ckks_monomial(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start, int k,
+                      fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (in == out) return fail(-2, "monomial multiplication cannot run in place");
+  if (k < 0 || k >= 2 * c.n()) return fail(-2, "monomial exponent must be in [0, 2N)");
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return FHB_WORD(fhb::monomial, c, in, out, batch, rows, row_start, k, st);
+}
+
+int fhb_ckks_modraise(const fhb_context* ctx, const void* in, void* out, int64_t batch, int src_prime, int rows,
+                      int row_start, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (src_prime < 0 || src_prime >= c.qp()) return fail(-4, "source prime out of range");
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return FHB_WORD(fhb::modraise, c, in, out, batch, rows, row_start, src_prime, st);
+}
+
+int fhb_rns_add_constant(const fhb_context* ctx, void* data, const void* constants, int64_t batch, int rows,
+                         int row_start, int all_slots, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(data, "data"));
+  if (!constants) return fail(-2, "constants is NULL");
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return FHB_WORD(fhb::add_constant, c, data, constants, batch, rows, row_start, all_slots ? 1 : 0, st);
 }
 
 int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, int level) {

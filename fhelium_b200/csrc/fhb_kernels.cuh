@@ -694,6 +694,75 @@ __global__ void k_lift_signed(const int64_t* __restrict__ x, T* __restrict__ out
   }
 }
 
+// Multiplication by the monomial X^k in Z[X]/(X^N + 1), coefficient domain:
+// out[j] = in[j - k] for j >= k, -in[j - k + N] for j < k (0 <= k < 2N,
+// k >= N negates once more).  Canonical output.
+template <typename T>
+__global__ void k_monomial(const T* __restrict__ in, T* __restrict__ out, int64_t batch, int rows, int row_start,
+                           int log_n, int k, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * rows * n;
+  const bool flip_all = k >= n;
+  const int kk = int(k % n);
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int j = int(idx & (n - 1));
+    const int64_t row = idx >> log_n;
+    const PrimeInfo<T> p = tabs.prime[row_start + int(row % rows)];
+    int src = j - kk;
+    bool neg = flip_all;
+    if (src < 0) {
+      src += int(n);
+      neg = !neg;
+    }
+    T x = csub(in[row * n + src], p.q);
+    if (neg && x) x = p.q - x;
+    out[idx] = x;
+  }
+}
+
+// ModRaise: centred lift of coefficient/standard residues modulo the single
+// prime `src_prime` to every row of [row_start, row_start + rows): the
+// represented integer is taken in (-q/2, q/2] (fhelium/experimental/bootstrap/
+// _modraise.py, centred basis extension).  in [batch, N], out [batch, rows, N].
+template <typename T>
+__global__ void k_modraise(const T* __restrict__ in, T* __restrict__ out, int64_t batch, int rows, int row_start,
+                           int src_prime, int log_n, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * rows * n;
+  const T qs = tabs.prime[src_prime].q;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int k = int(idx & (n - 1));
+    const int64_t br = idx >> log_n;
+    const int row = int(br % rows);
+    const int64_t bi = br / rows;
+    const PrimeInfo<T> p = tabs.prime[row_start + row];
+    const T v = csub(in[bi * n + k], qs);
+    const bool negative = v > (qs >> 1);
+    const T mag = negative ? qs - v : v;
+    T r = reduce_any(mag, p);
+    out[idx] = (negative && r) ? p.q - r : r;
+  }
+}
+
+// Add a per-row constant (canonical residues c[row]) to coefficient 0
+// (coefficient domain, `all_slots` = 0) or to every NTT slot (`all_slots` = 1).
+template <typename T>
+__global__ void k_add_constant(T* __restrict__ data, const T* __restrict__ c, int64_t batch, int rows, int row_start,
+                               int log_n, int all_slots, ChainTables<T> tabs) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = all_slots ? batch * rows * n : batch * rows;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t row = all_slots ? (idx >> log_n) : idx;
+    const int r = int(row % rows);
+    const PrimeInfo<T> p = tabs.prime[row_start + r];
+    const int64_t at = all_slots ? idx : row * n;
+    data[at] = csub(csub(data[at], p.q) + c[r], p.q);
+  }
+}
+
 // Canonical addition (add / add_canonical): out = a + b mod q.
 template <typename T>
 __global__ void k_add_canonical(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,

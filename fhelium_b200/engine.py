@@ -246,6 +246,112 @@ class CkksEngine:
         return Ciphertext(out, lhs.level + (1 if rescale else 0), scale, "coefficient", "standard")
 
     # ------------------------------------------------------------------
+    # plaintexts, scalars, monomials, level changes
+    # (fhelium/engine/ckks_engine.py:508-700, 1208-1430, 1964-2180;
+    #  fhelium/experimental/bootstrap/_ops.py)
+    # ------------------------------------------------------------------
+    def encode_plaintext(self, slots, *, level: int, scale: float) -> torch.Tensor:
+        """Slots -> NTT/Montgomery plaintext [*batch, Q_level, N] at `scale`."""
+        coeffs = self.encode_coefficients(slots, scale)
+        return self.forward_ntt(self._lift(coeffs, level, self.num_q - level), level)
+
+    def multiply_plaintext(self, ct: Ciphertext, plaintext: torch.Tensor, plaintext_scale: float) -> Ciphertext:
+        """NTT-domain ct x pt (no rescale); pt [L, N] is shared by every
+        component and batch item (fhelium/engine/ckks_engine.py:2077-2170)."""
+        ct.assert_state(polynomial_domain="ntt", residue_representation="montgomery")
+        self._check_ct(ct)
+        out = self._binary(nat.OP_MONTGOMERY_MUL, ct.data, plaintext, ct.level, b_mode=1)
+        return Ciphertext(out, ct.level, ct.scale * plaintext_scale, "ntt", "montgomery")
+
+    def _row_constants(self, value: int, level: int, *, montgomery: bool) -> torch.Tensor:
+        R = 1 << (62 if self.dtype == torch.int64 else 30)
+        vals = [(int(value) * (R if montgomery else 1)) % self.moduli[i] for i in range(level, self.num_q)]
+        return torch.tensor(vals, dtype=self.dtype, device=self.device)
+
+    def multiply_integer(self, ct: Ciphertext, value: int, *, scale_factor: float | None = None) -> Ciphertext:
+        """Multiply every residue by the integer `value` (no rescale); the
+        scale is multiplied by `scale_factor` (default: value)."""
+        self._check_ct(ct)
+        consts = self._row_constants(value, ct.level, montgomery=True)
+        out = self._binary(nat.OP_MONTGOMERY_MUL, ct.data, consts, ct.level, b_mode=2)
+        if ct.polynomial_domain == "coefficient":
+            out = self._binary(nat.OP_ADD_CANONICAL, out, torch.zeros_like(consts), ct.level, b_mode=2)
+        factor = float(value) if scale_factor is None else scale_factor
+        return Ciphertext(out, ct.level, ct.scale * factor, ct.polynomial_domain, ct.residue_representation)
+
+    def add_constant(self, ct: Ciphertext, value: float) -> Ciphertext:
+        """Add `value` to every slot (round(value * scale) to the constant term)."""
+        self._check_ct(ct)
+        out = ct.data.clone()
+        c = int(round(float(value) * ct.scale))
+        ntt = ct.polynomial_domain == "ntt"
+        consts = self._row_constants(c, ct.level, montgomery=ntt)
+        self.ctx.call("fhb_rns_add_constant", nat.ptr(out[0]), nat.ptr(consts), ct.batch_size, ct.limb_count,
+                      ct.level, 1 if ntt else 0, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, ct.polynomial_domain, ct.residue_representation)
+
+    def subtract(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+        self._assert_same_layout(lhs, rhs)
+        op = nat.OP_SUB_LAZY if lhs.polynomial_domain == "ntt" else nat.OP_SUB_CANONICAL
+        out = self._binary(op, lhs.data, rhs.data, lhs.level)
+        return Ciphertext(out, lhs.level, lhs.scale, lhs.polynomial_domain, lhs.residue_representation)
+
+    def multiply_by_monomial(self, ct: Ciphertext, k: int) -> Ciphertext:
+        """ct * X^k in Z[X]/(X^N + 1) (coefficient domain)."""
+        ct.assert_state(polynomial_domain="coefficient")
+        self._check_ct(ct)
+        out = torch.empty_like(ct.data)
+        k %= 2 * self.n
+        self.ctx.call("fhb_ckks_monomial", nat.ptr(ct.data), nat.ptr(out), ct.component_count * ct.batch_size,
+                      ct.limb_count, ct.level, k, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, ct.polynomial_domain, ct.residue_representation)
+
+    def mod_switch_to_level(self, ct: Ciphertext, level: int) -> Ciphertext:
+        """Drop leading Q rows without dividing (fhelium/engine/ckks_engine.py:1278-1345)."""
+        if level < ct.level or level >= self.num_q:
+            raise ValueError("target level must be at or below the ciphertext's level")
+        data = ct.data[..., level - ct.level:, :].contiguous()
+        return Ciphertext(data, level, ct.scale, ct.polynomial_domain, ct.residue_representation)
+
+    def reinterpret_at_scale(self, ct: Ciphertext, scale: float) -> Ciphertext:
+        return Ciphertext(ct.data, ct.level, float(scale), ct.polynomial_domain, ct.residue_representation)
+
+    def modulus_raise(self, ct: Ciphertext, target_level: int = 0) -> Ciphertext:
+        """Centred lift of a one-prime (structural base) coefficient ciphertext
+        to Q_target (fhelium/experimental/bootstrap/_modraise.py:338)."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard")
+        if ct.level != self.num_q - 1:
+            raise ValueError("ModRaise starts from the single structural base prime")
+        rows = self.num_q - target_level
+        out = self._empty(*ct.data.shape[:-2], rows, self.n)
+        polys = ct.component_count * ct.batch_size
+        self.ctx.call("fhb_ckks_modraise", nat.ptr(ct.data), nat.ptr(out), polys, self.num_q - 1, rows,
+                      target_level, self._stream())
+        return Ciphertext(out, target_level, ct.scale, "coefficient", "standard")
+
+    def create_galois_key(self, galois: int, secret_key: SecretKey | None = None, *, rotation_step: int = 0) -> RotationKey:
+        """Key switching sigma_g(s) -> s for any odd g (rotations, conjugation)."""
+        s = secret_key or self.secret_key
+        coef = self.inverse_ntt(s.data, 0, output=nat.INV_MONTGOMERY)
+        rot = torch.empty_like(coef)
+        self.ctx.call("fhb_ckks_automorphism", nat.ptr(coef), nat.ptr(rot), 1, self.qp_rows, 0, galois,
+                      self._stream())
+        rs = self.forward_ntt(rot, 0, montgomery_input=True)
+        ksk = self.create_key_switch_key(SecretKey(rs), s)
+        return RotationKey(ksk.data, rotation_step=rotation_step, galois_element=galois)
+
+    def create_conjugation_key(self, secret_key: SecretKey | None = None) -> RotationKey:
+        """sigma_{2N-1}: complex conjugation of every slot
+        (fhelium/engine/key_generator.py:create_conjugation_key)."""
+        return self.create_galois_key(2 * self.n - 1, secret_key)
+
+    def conjugate(self, ct: Ciphertext, key: RotationKey) -> Ciphertext:
+        """fhelium/engine/ckks_engine.py:2348-2398."""
+        if key.galois_element != 2 * self.n - 1:
+            raise ValueError("not a conjugation key")
+        return self.rotate_with_key(ct, key)
+
+    # ------------------------------------------------------------------
     # rotations (fhelium/engine/ckks_engine.py:2183-2300, 3726-3897)
     # ------------------------------------------------------------------
     def _canonical_step(self, step: int) -> int:
@@ -408,15 +514,8 @@ class CkksEngine:
 
     def create_rotation_key(self, rotation_step: int, secret_key: SecretKey | None = None) -> RotationKey:
         """Key from sigma_g(s) back to s (fhelium/engine/key_generator.py:364-412)."""
-        s = secret_key or self.secret_key
         step = self._canonical_step(rotation_step)
-        g = self.galois_element_for_step(step)
-        coef = self.inverse_ntt(s.data, 0, output=nat.INV_MONTGOMERY)
-        rot = torch.empty_like(coef)
-        self.ctx.call("fhb_ckks_automorphism", nat.ptr(coef), nat.ptr(rot), 1, self.qp_rows, 0, g, self._stream())
-        rs = self.forward_ntt(rot, 0, montgomery_input=True)
-        ksk = self.create_key_switch_key(SecretKey(rs), s)
-        return RotationKey(ksk.data, rotation_step=step, galois_element=g)
+        return self.create_galois_key(self.galois_element_for_step(step), secret_key, rotation_step=step)
 
     def generate_rotation_keys(self, steps: Iterable[int]) -> None:
         for st in steps:

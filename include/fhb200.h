@@ -180,6 +180,27 @@ int fhb_rns_binary(const fhb_context* ctx, int op, const void* a, const void* b,
 int fhb_rns_lift_signed(const fhb_context* ctx, const int64_t* coefficients, void* out, int64_t batch, int rows,
                         int row_start, fhb_stream stream);
 
+/* Multiply [batch, rows, N] coefficient/standard polynomials by X^k
+ * (0 <= k < 2N) in Z[X]/(X^N + 1); in != out.  Replaces the bootstrap's
+ * monomial multiplication (fhelium/experimental/bootstrap/_full_slot.py:
+ * _multiply_by_monomial). */
+int fhb_ckks_monomial(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start, int k,
+                      fhb_stream stream);
+
+/* ModRaise: centred lift of [batch, N] coefficient/standard residues modulo
+ * prime `src_prime` to [batch, rows, N] over prime ids [row_start,
+ * row_start + rows).  Replaces the bootstrap's modulus raise
+ * (fhelium/experimental/bootstrap/_modraise.py:338). */
+int fhb_ckks_modraise(const fhb_context* ctx, const void* in, void* out, int64_t batch, int src_prime, int rows,
+                      int row_start, fhb_stream stream);
+
+/* data[b, r, 0] += constants[r] (coefficient domain, all_slots = 0) or
+ * data[b, r, :] += constants[r] (NTT domain, all_slots = 1), canonical
+ * constants; in place.  Replaces the constant additions of the bootstrap's
+ * polynomial evaluators (fhelium/experimental/bootstrap/_polynomial.py). */
+int fhb_rns_add_constant(const fhb_context* ctx, void* data, const void* constants, int64_t batch, int rows,
+                         int row_start, int all_slots, fhb_stream stream);
+
 /* Scratch bytes needed by fhb_ckks_relinearize / fhb_ckks_rotate. */
 int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, int level);
 
