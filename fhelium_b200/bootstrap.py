@@ -32,8 +32,9 @@ Modular reduction: x = u / B' with u = t / q_b (t the raised coefficient),
 z0 ~ cos(2 pi (B' x - 1/4) / 2^R) by Chebyshev interpolation of degree 44 on
 [-1, 1], then R double-angle steps z <- 2 z^2 - 1 give sin(2 pi u); the factor
 q_b / (2 pi Delta) returning to message units is folded into SlotsToCoeffs.
-All ciphertext products are relinearised and rescaled, then reinterpreted at
-the default scale (scale primes lie within 2^-30 of Delta).
+All ciphertext products are relinearised and rescaled with their actual
+scales tracked; terms are aligned to a common level and scale by integer
+constants before every addition.
 """
 
 from __future__ import annotations
@@ -280,22 +281,33 @@ class FullSlotBootstrap:
             result = inner if result is None else eng.add(result, inner)
         return result
 
+    # Scales are tracked exactly inside the modular reduction: the 50-bit
+    # primes differ from 2^50 by up to ~6e-6 relative, and the double-angle
+    # chain amplifies any unaccounted scale error by 2^R.
     def _mul(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
         eng = self.engine
         level = max(a.level, b.level)
         a = eng.mod_switch_to_level(a, level)
-        b = eng.mod_switch_to_level(b, level)
         an = eng.coefficient_domain_to_ntt_domain(a)
-        bn = an if b is a else eng.coefficient_domain_to_ntt_domain(b)
-        out = eng.multiply_relinearize_rescale(an, bn)
-        return eng.reinterpret_at_scale(out, self.delta)
+        if b is None:
+            bn = an
+        else:
+            bn = eng.coefficient_domain_to_ntt_domain(eng.mod_switch_to_level(b, level))
+        return eng.multiply_relinearize_rescale(an, bn)
 
-    def _scalar(self, ct: Ciphertext, value: float) -> Ciphertext:
-        """ct * value with one rescale (value encoded at scale Delta)."""
+    def _scaled(self, ct: Ciphertext, level: int, scale: float, value: float = 1.0) -> Ciphertext:
+        """value * ct moved to `level` (> ct.level) with actual scale exactly
+        `scale`: mod-switch to level-1, multiply by the integer
+        round(value * scale * q_(level-1) / ct.scale), rescale."""
         eng = self.engine
-        c = int(round(value * self.delta))
-        out = eng.multiply_integer(ct, c, scale_factor=self.delta)
-        return eng.reinterpret_at_scale(eng.rescale_to_next_level(out), self.delta)
+        if level <= ct.level:
+            raise ValueError("_scaled needs a deeper target level")
+        src = eng.mod_switch_to_level(ct, level - 1)
+        q = eng.moduli[level - 1]
+        c = int(round(value * scale * q / ct.scale))
+        out = eng.multiply_integer(src, c, scale_factor=c / value if value else 1.0)
+        out = eng.rescale_to_next_level(out)
+        return eng.reinterpret_at_scale(out, scale)
 
     def _chebyshev(self, x: Ciphertext) -> Ciphertext:
         eng = self.engine
@@ -303,19 +315,18 @@ class FullSlotBootstrap:
         for k in range(2, self.degree + 1):
             a = 1 << (math.ceil(math.log2(k)) - 1)
             b = k - a
-            prod = self._mul(T[a], T[b])
+            prod = self._mul(T[a], None if a == b else T[b])
             two = eng.add(prod, prod)
             if a == b:
                 T[k] = eng.add_constant(two, -1.0)
             else:
-                lower = eng.mod_switch_to_level(T[a - b], two.level)
-                T[k] = eng.subtract(two, eng.reinterpret_at_scale(lower, two.scale))
-        deepest = max(t.level for t in T.values())
+                T[k] = eng.subtract(two, self._scaled(T[a - b], two.level, two.scale))
+        final = max(t.level for t in T.values()) + 1
         acc = None
         for k in range(1, self.degree + 1):
             if abs(self.seed[k]) < 1e-15:
                 continue
-            term = self._scalar(eng.mod_switch_to_level(T[k], deepest), float(self.seed[k]))
+            term = self._scaled(T[k], final, self.delta, float(self.seed[k]))
             acc = term if acc is None else eng.add(acc, term)
         return eng.add_constant(acc, float(self.seed[0]))
 
@@ -323,7 +334,7 @@ class FullSlotBootstrap:
         eng = self.engine
         z = self._chebyshev(x)
         for _ in range(self.R):
-            sq = self._mul(z, z)
+            sq = self._mul(z, None)
             z = eng.add_constant(eng.add(sq, sq), -1.0)
         return z
 
