@@ -286,7 +286,7 @@ class FullSlotBootstrap:
     # chain amplifies any unaccounted scale error by 2^R.
     def _mul(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
         eng = self.engine
-        level = max(a.level, b.level)
+        level = a.level if b is None else max(a.level, b.level)
         a = eng.mod_switch_to_level(a, level)
         an = eng.coefficient_domain_to_ntt_domain(a)
         if b is None:
