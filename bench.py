@@ -195,6 +195,98 @@ def ntt_leg(dev, stream, steps):
             "limb_ntts_per_s": 2 * B * L / ((fwd_ms + inv_ms) / 1e3)}
 
 
+def bootstrap_leg(dev, stream, batch=8, steps=2):
+    """Full-slot bootstrap of `batch` ciphertexts, preset
+    slots32768_scale50_levels27_int64 + base_prime_bits=50, generator 5,
+    slots with real and imaginary parts uniform in [-1, 1] (seed 4)."""
+    import math
+    from fhelium_b200.bootstrap import FullSlotBootstrap
+    from fhelium_b200.config import CkksConfig
+    from fhelium_b200.engine import CkksEngine
+    cfg = CkksConfig.parse("slots32768_scale50_levels27_int64", base_prime_bits=50)
+    eng = CkksEngine(cfg, device=dev, galois_generator=5, rng_seed=5)
+    bs = FullSlotBootstrap(eng)
+    t0 = time.perf_counter()
+    bs.generate_keys()
+    bs.precompute()
+    torch.cuda.synchronize(dev)
+    setup_s = time.perf_counter() - t0
+    g = torch.Generator().manual_seed(4)
+    n = eng.num_slots
+    m = (torch.rand((batch, n), dtype=torch.float64, generator=g) * 2 - 1) \
+        + 1j * (torch.rand((batch, n), dtype=torch.float64, generator=g) * 2 - 1)
+    ct = eng.encrypt_message(m, level=eng.public_level_count - 1)
+    state = {}
+
+    def step():
+        state["out"] = bs(ct)
+
+    step()
+    torch.cuda.synchronize(dev)
+    ms = _time_events(step, steps, stream)
+    err = (eng.decrypt_message(state["out"]) - m).abs()
+    out = {"batch": batch, "ms_per_call": ms, "ms_per_bootstrap": ms / batch,
+           "bootstraps_per_s": batch / (ms / 1e3), "output_level": state["out"].level,
+           "max_abs_err": float(err.max()), "mean_abs_err": float(err.mean()),
+           "precision_bits": -math.log2(float(err.max())), "setup_s": setup_s,
+           "rotation_keys": len(bs.rotation_steps())}
+    del bs, eng, ct, state
+    torch.cuda.empty_cache()
+    return out
+
+
+def mixed_batch_leg(dev, stream, count=512, steps=3):
+    """Mixed-level batch at slots32768_scale40_levels34_int64: `count`
+    ciphertexts with limb counts uniform in 3..35 (uniform [-0.05, 0.05]
+    messages), each with a seeded op (HMult+relin+rescale with a same-level
+    partner, or a rotation by a step uniform in +-[1, 2^14]).  The batched
+    form (one CUDA graph, knobs from the autotuner) against one engine call
+    sequence per ciphertext; every result compared bit for bit."""
+    from fhelium_b200 import autotune
+    from fhelium_b200.batch import HMULT, MixedBatchExecutor, run_per_ciphertext, sample_mixed_workload
+    from fhelium_b200.engine import CkksEngine
+    eng = CkksEngine(PRESET, device=dev, rng_seed=9)
+    levels, ops = sample_mixed_workload(eng.num_q, count, seed=0)
+    msgs = _messages(count, eng.num_slots, 3)
+    cts = [eng.encrypt_message(msgs[i], level=lv) for i, lv in enumerate(levels)]
+    t0 = time.perf_counter()
+    for op in ops:
+        if op.kind != HMULT:
+            eng.rotation_key(op.step)
+    torch.cuda.synchronize(dev)
+    keygen_s = time.perf_counter() - t0
+    ex = MixedBatchExecutor(eng, cts, ops)
+    tune = autotune.tune_mixed_batch(eng, ex, ks_orders=(0, 1), streams=(1, 2, 4), repeats=2)
+    ex.run()
+    torch.cuda.synchronize(dev)
+    batched_ms = _time_events(ex.run, max(3, steps), stream)
+
+    def per_ct():
+        run_per_ciphertext(eng, cts, ops)
+
+    per_ct()
+    torch.cuda.synchronize(dev)
+    loop_ms = _time_events(per_ct, 2, stream)
+    mismatches = 0
+    for i, op in enumerate(ops):
+        want = run_per_ciphertext(eng, cts, [op])[0]
+        if not torch.equal(ex.result_view(i), want.data.view(2, -1, eng.n)):
+            mismatches += 1
+    n_rot = sum(1 for op in ops if op.kind != HMULT)
+    out = {"ciphertexts": count, "hmult_ops": count - n_rot, "rotate_ops": n_rot,
+           "distinct_rotation_keys": len({eng._canonical_step(op.step) for op in ops if op.kind != HMULT}),
+           "groups": len(ex.groups), "library_launches_per_pass": ex.launches_per_run,
+           "batched_graph_ms": batched_ms, "batched_ops_per_s": count / (batched_ms / 1e3),
+           "per_ciphertext_ms": loop_ms, "per_ciphertext_ops_per_s": count / (loop_ms / 1e3),
+           "speedup": loop_ms / batched_ms, "bit_exact_mismatches": mismatches,
+           "autotune": {"ks_order": tune["ks_order"], "streams": tune["streams"], "cached": tune["cached"],
+                        "candidates": tune.get("candidates")},
+           "keygen_s": keygen_s}
+    del ex, cts, eng
+    torch.cuda.empty_cache()
+    return out
+
+
 def cpu_reference_sample(n_ops: int, threads: int, level: int = 0):
     """Time the reference CPU operators on `n_ops` HMult+relin+rescale ops
     (one ciphertext pair each).  Returns (ops/s, kind, sample text)."""
@@ -260,10 +352,25 @@ def main() -> int:
     ap.add_argument("--batch", type=int, default=32)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-extras", action="store_true", help="skip rotation/parity/CPU legs")
+    ap.add_argument("--mixed-count", type=int, default=512, help="ciphertexts of the mixed-level leg (0: skip)")
+    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed"], default=None,
+                    help="run only this side leg on one GPU and print its result (profiling aid)")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.impl == "reference":
         return run_reference(args, ws, rank)
+    if args.leg is not None:
+        dev = torch.device("cuda", local)
+        torch.cuda.set_device(dev)
+        stream = torch.cuda.current_stream(dev)
+        if args.leg == "ntt_int32":
+            res = ntt_leg(dev, stream, args.steps)
+        elif args.leg == "bootstrap":
+            res = bootstrap_leg(dev, stream, steps=max(1, args.steps))
+        else:
+            res = mixed_batch_leg(dev, stream, args.mixed_count, args.steps)
+        print(json.dumps({"leg": args.leg, **res}), flush=True)
+        return 0
 
     from fhelium_b200 import _native as nat
     from fhelium_b200.config import CkksConfig
@@ -382,6 +489,9 @@ def main() -> int:
         h_ms = _time_events(lambda: eng.rotate_many_by_steps(rot_in, steps16), 2, stream)
         extras["hoisted_rotations_16_ops_per_s"] = 16 * B / (h_ms / 1000.0)
         extras["ntt_int32_logN16_36limbs_batch64"] = ntt_leg(dev, stream, args.steps)
+        extras["bootstrap_logN16_batch8"] = bootstrap_leg(dev, stream)
+        if args.mixed_count > 0:
+            extras["mixed_level_batch"] = mixed_batch_leg(dev, stream, args.mixed_count, args.steps)
         # decrypted error of the product (first ciphertext)
         dec = eng.decrypt_message(Ciphertext(state["out"].data[:, :1].contiguous(), 1, state["out"].scale),
                                   is_real=True)

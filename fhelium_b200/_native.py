@@ -27,6 +27,8 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_context_create": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, _I, ctypes.POINTER(_P)]),
     "fhb_context_destroy": (_I, [_P]),
     "fhb_context_root": (_I, [_P, _I, ctypes.POINTER(ctypes.c_uint64)]),
+    "fhb_context_set_tuning": (_I, [_P, _I, _I]),
+    "fhb_context_get_tuning": (_I, [_P, _I, ctypes.POINTER(_I)]),
     "fhb_forward_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_inverse_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_multiply": (_I, [_P, _P, _P, _P, _I64, _I, _P]),
@@ -45,6 +47,7 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_relinearize": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_multiply_relinearize": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_rotate": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _U32, _P]),
+    "fhb_ckks_rotate_multi": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _P]),
     "fhb_ckks_monomial": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_modraise": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_rns_add_constant": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),

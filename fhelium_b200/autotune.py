@@ -1,0 +1,114 @@
+"""Measured choice of the launch knobs of a batched workload.
+
+The knobs a run can change without recompiling:
+
+* ``ks_order`` (FHB_TUNE_KS_ORDER): the work order of the key-switch
+  clusters, 0 = the limbs of one ciphertext back to back (the digits of one
+  ciphertext stay in L2 while its limbs are processed), 1 = one limb across
+  the batch back to back (the key rows of one prime are shared by the whole
+  batch, which pays when every item uses the same key);
+* ``streams``: how many graph branches the mixed-batch executor spreads its
+  (kind, level) groups over, i.e. how many groups run side by side.
+
+The NTT geometry (cluster width, residues per thread, radix of the register
+passes) is fixed per ring degree when the library is compiled; every
+runtime knob above is picked here by timing CUDA-graph replays on the
+caller's own workload.  Winners are cached in a JSON file keyed by device,
+ring, modulus chain and workload shape, so a later process with the same
+workload skips the search.  The reference has no autotuner (its launch
+shapes are fixed in csrc/ops/ntt/cuda/*.cu).
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import threading
+from typing import Iterable
+
+import torch
+
+_LOCK = threading.Lock()
+
+
+def default_cache_path() -> str:
+    env = os.environ.get("FHB200_AUTOTUNE_CACHE")
+    if env:
+        return env
+    return os.path.join(os.path.expanduser("~"), ".cache", "fhelium_b200", "autotune.json")
+
+
+def _load(path: str) -> dict:
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        return data if isinstance(data, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(path: str, key: str, entry: dict) -> None:
+    with _LOCK:
+        data = _load(path)
+        data[key] = entry
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        tmp = f"{path}.{os.getpid()}.tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+
+
+def workload_key(engine, executor) -> str:
+    """Device + ring + chain + the multiset of (kind, level, items) groups."""
+    shape = sorted((g.kind, g.level, g.items) for g in executor.groups)
+    digest = hashlib.sha256(json.dumps(shape).encode()).hexdigest()[:16]
+    chain = hashlib.sha256(json.dumps([int(m) for m in engine.moduli]).encode()).hexdigest()[:12]
+    dev = torch.cuda.get_device_name(engine.device)
+    return f"{dev}|logN={engine.log_n}|q={engine.num_q}|p={engine.num_p}|chain={chain}|mixed={digest}"
+
+
+def time_replays(run, device, *, warmup: int = 1, repeats: int = 3) -> float:
+    """Median milliseconds of `run()` on the current stream (CUDA events)."""
+    for _ in range(warmup):
+        run()
+    stream = torch.cuda.current_stream(device)
+    times = []
+    for _ in range(repeats):
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        start.record(stream)
+        run()
+        stop.record(stream)
+        stop.synchronize()
+        times.append(start.elapsed_time(stop))
+    times.sort()
+    return times[len(times) // 2]
+
+
+def tune_mixed_batch(engine, executor, *, ks_orders: Iterable[int] = (0, 1), streams: Iterable[int] = (1, 2, 3, 4),
+                     repeats: int = 3, cache_path: str | None = None, use_cache: bool = True) -> dict:
+    """Pick (ks_order, streams) for `executor` by timing graph replays.
+
+    Leaves the executor configured with the winner and returns
+    ``{"ks_order", "streams", "ms", "candidates": [...], "cached": bool}``.
+    """
+    cache_path = cache_path or default_cache_path()
+    key = workload_key(engine, executor)
+    if use_cache:
+        hit = _load(cache_path).get(key)
+        if hit and {"ks_order", "streams"} <= set(hit):
+            executor.configure(streams=int(hit["streams"]), ks_order=int(hit["ks_order"]))
+            return dict(hit, cached=True)
+    results = []
+    for order in ks_orders:
+        for s in streams:
+            executor.configure(streams=s, ks_order=order)
+            ms = time_replays(executor.run, engine.device, repeats=repeats)
+            results.append({"ks_order": int(order), "streams": int(s), "ms": ms})
+    best = min(results, key=lambda r: r["ms"])
+    executor.configure(streams=best["streams"], ks_order=best["ks_order"])
+    entry = dict(best, candidates=results)
+    _store(cache_path, key, entry)
+    return dict(entry, cached=False)

@@ -1,0 +1,309 @@
+"""Mixed-level batched execution of independent CKKS operations.
+
+A batch of ciphertexts at different levels, each with its own operation
+(multiply -> relinearize -> rescale with a same-level partner, or a rotation
+by its own step), runs as ONE CUDA graph launch:
+
+* operations are grouped by (kind, level); each group runs as one fused
+  launch sequence over all of its items: one forward NTT + the four-launch
+  fused HMult/relinearise/rescale for multiplications, and the three-launch
+  ``fhb_ckks_rotate_multi`` for rotations, where every item carries its own
+  Galois element and key pointer, so mixed steps share one launch;
+* groups are spread over ``streams`` capture branches (longest group first
+  onto the least loaded branch), so the small levels, which fill only part
+  of the 148 SMs, run side by side;
+* the whole launch sequence, including the gathers of the inputs into each
+  group's contiguous [2, items, limbs, N] arena, is captured once and
+  replayed.
+
+The reference runs such a batch as one engine call per ciphertext
+(``CkksEngine.multiply``/``relinearize``/``rescale_to_next_level``,
+fhelium/engine/ckks_engine.py:1530-1675, and ``rotate_by_step``,
+fhelium/engine/ckks_engine.py:2183-2300, 3822-3897).
+:func:`run_per_ciphertext` is that loop on this library; both produce the
+same residues bit for bit.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .values import Ciphertext
+
+HMULT = "multiply_relinearize_rescale"
+ROTATE = "rotate_by_step"
+
+
+@dataclass(frozen=True)
+class MixedOp:
+    """One operation of a mixed batch.
+
+    kind    HMULT or ROTATE
+    index   the ciphertext operated on
+    partner the same-level right-hand operand (HMULT)
+    step    the rotation step (ROTATE)
+    """
+
+    kind: str
+    index: int
+    partner: int = -1
+    step: int = 0
+
+
+def sample_mixed_workload(num_q: int, count: int, *, min_limbs: int = 3, max_limbs: int | None = None,
+                          max_step: int = 1 << 14, seed: int = 0) -> tuple[list[int], list[MixedOp]]:
+    """Seeded mixed workload: limb counts uniform in [min_limbs, max_limbs]
+    (engine level = num_q - limbs) and, per ciphertext, an operation drawn
+    uniformly: HMULT with a uniformly drawn same-level partner, or ROTATE by a
+    step uniform in +-[1, max_step]."""
+    max_limbs = num_q if max_limbs is None else max_limbs
+    if not 2 <= min_limbs <= max_limbs <= num_q:
+        raise ValueError("need 2 <= min_limbs <= max_limbs <= num_q")
+    rng = np.random.default_rng(seed)
+    limbs = rng.integers(min_limbs, max_limbs + 1, size=count)
+    levels = [int(num_q - x) for x in limbs]
+    by_level: dict[int, list[int]] = {}
+    for i, lv in enumerate(levels):
+        by_level.setdefault(lv, []).append(i)
+    ops = []
+    kinds = rng.integers(0, 2, size=count)
+    for i in range(count):
+        if kinds[i] == 0:
+            peers = by_level[levels[i]]
+            ops.append(MixedOp(HMULT, i, partner=int(peers[rng.integers(0, len(peers))])))
+        else:
+            magnitude = int(rng.integers(1, max_step + 1))
+            ops.append(MixedOp(ROTATE, i, step=magnitude if rng.integers(0, 2) else -magnitude))
+    return levels, ops
+
+
+@dataclass
+class _Group:
+    kind: str
+    level: int
+    ops: list[int]  # op indices, in item order
+    limbs: int
+    stream: int = 0
+    inp: torch.Tensor | None = None   # HMULT [2(a|b), 2, B, L, N]; ROTATE [2, B, L, N]
+    out: torch.Tensor | None = None   # [2, B, L', N]
+    galois: torch.Tensor | None = None  # ROTATE: int32 [B] (device)
+    key_ptrs: torch.Tensor | None = None  # ROTATE: int64 [B] (device)
+    keys: list = field(default_factory=list)  # keeps the rotation keys alive
+
+    @property
+    def items(self) -> int:
+        return len(self.ops)
+
+    def cost(self, num_p: int) -> int:
+        # key-switch work ~ items x (Q_l + P) x digits; digits grow with limbs
+        return self.items * (self.limbs + num_p) * (self.limbs + num_p)
+
+
+class MixedBatchExecutor:
+    """Runs a fixed mixed batch (ciphertexts + ops) as one CUDA graph.
+
+    ciphertexts: coefficient/standard two-component ciphertexts of batch
+    size 1, any levels.  ops: one MixedOp per result.  The inputs are read
+    in place on every run, so updating their tensors between runs is seen.
+    """
+
+    def __init__(self, engine, ciphertexts: Sequence[Ciphertext], ops: Sequence[MixedOp], *,
+                 streams: int = 2, ks_order: int | None = None, use_graph: bool = True):
+        self.engine = engine
+        self.cts = list(ciphertexts)
+        self.ops = list(ops)
+        self.use_graph = use_graph
+        self._validate()
+        self._slot: dict[int, tuple[_Group, int]] = {}
+        self._copies: set[int] = set()
+        self.groups = self._plan()
+        self._alloc()
+        self._streams: list[torch.cuda.Stream] = []
+        self._scratch: list[torch.Tensor] = []
+        self._graph: torch.cuda.CUDAGraph | None = None
+        self.streams = 0
+        self.ks_order = None
+        self.configure(streams=streams, ks_order=ks_order)
+
+    # ---------------------------------------------------------------- plan
+    def _validate(self) -> None:
+        eng = self.engine
+        for ct in self.cts:
+            ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+            eng._check_ct(ct)
+            if ct.batch_size != 1:
+                raise ValueError("mixed batches take ciphertexts of batch size 1")
+        for op in self.ops:
+            if not 0 <= op.index < len(self.cts):
+                raise ValueError(f"op {op} refers to a missing ciphertext")
+            if op.kind == HMULT:
+                if not 0 <= op.partner < len(self.cts):
+                    raise ValueError(f"op {op} has no partner")
+                a, b = self.cts[op.index], self.cts[op.partner]
+                if a.level != b.level:
+                    raise ValueError(f"op {op}: partner is at another level")
+                if a.limb_count < 2:
+                    raise ValueError(f"op {op}: no level left to rescale into")
+            elif op.kind != ROTATE:
+                raise ValueError(f"unknown op kind {op.kind!r}")
+
+    def _plan(self) -> list[_Group]:
+        eng = self.engine
+        table: dict[tuple[str, int], _Group] = {}
+        for i, op in enumerate(self.ops):
+            ct = self.cts[op.index]
+            if op.kind == ROTATE and eng._canonical_step(op.step) == 0:
+                self._copies.add(i)
+                continue
+            key = (op.kind, ct.level)
+            if key not in table:
+                table[key] = _Group(op.kind, ct.level, [], ct.limb_count)
+            grp = table[key]
+            self._slot[i] = (grp, len(grp.ops))
+            grp.ops.append(i)
+        return sorted(table.values(), key=lambda g: (g.level, g.kind))
+
+    def _alloc(self) -> None:
+        eng = self.engine
+        n = eng.n
+        for g in self.groups:
+            b, lm = g.items, g.limbs
+            if g.kind == HMULT:
+                g.inp = eng._empty(2, 2, b, lm, n)
+                g.out = eng._empty(2, b, lm - 1, n)
+            else:
+                g.inp = eng._empty(2, b, lm, n)
+                g.out = eng._empty(2, b, lm, n)
+                g.keys = [eng.rotation_key(self.ops[i].step) for i in g.ops]
+                g.galois = torch.tensor([k.galois_element for k in g.keys], dtype=torch.int32, device=eng.device)
+                g.key_ptrs = torch.tensor([k.data.data_ptr() for k in g.keys], dtype=torch.int64,
+                                          device=eng.device)
+        self._relin = eng.relinearization_key if any(g.kind == HMULT for g in self.groups) else None
+
+    def configure(self, *, streams: int | None = None, ks_order: int | None = None) -> None:
+        """Set the branch count and key-switch work order; drops the graph."""
+        eng = self.engine
+        if streams is not None:
+            if streams < 1:
+                raise ValueError("streams must be >= 1")
+            self.streams = int(streams)
+        if ks_order is not None:
+            self.ks_order = int(ks_order)
+        self._graph = None
+        loads = [0] * self.streams
+        for g in sorted(self.groups, key=lambda g: -g.cost(eng.num_p)):
+            s = min(range(self.streams), key=lambda i: loads[i])
+            g.stream = s
+            loads[s] += g.cost(eng.num_p)
+        while len(self._streams) < self.streams:
+            self._streams.append(torch.cuda.Stream(eng.device))
+        need = [0] * self.streams
+        for g in self.groups:
+            nb = int(eng.ctx.lib.fhb_ckks_keyswitch_scratch_bytes(eng.ctx.handle, g.items, g.level))
+            need[g.stream] = max(need[g.stream], nb)
+        self._scratch = [torch.empty(max(nb, 16), dtype=torch.uint8, device=eng.device) for nb in need]
+
+    # ---------------------------------------------------------------- run
+    def _issue_group(self, g: _Group, stream: torch.cuda.Stream, scratch: torch.Tensor) -> None:
+        eng = self.engine
+        ctx = eng.ctx
+        st = stream.cuda_stream
+        with torch.cuda.stream(stream):
+            if g.kind == HMULT:
+                torch.stack([self.cts[self.ops[i].index].data.view(2, g.limbs, eng.n) for i in g.ops], dim=1,
+                            out=g.inp[0])
+                torch.stack([self.cts[self.ops[i].partner].data.view(2, g.limbs, eng.n) for i in g.ops], dim=1,
+                            out=g.inp[1])
+            else:
+                torch.stack([self.cts[self.ops[i].index].data.view(2, g.limbs, eng.n) for i in g.ops], dim=1,
+                            out=g.inp)
+        if g.kind == HMULT:
+            ctx.call("fhb_forward_ntt", nat.ptr(g.inp), nat.ptr(g.inp), 4 * g.items, g.limbs, g.level, 0, st)
+            ctx.call("fhb_ckks_multiply_relinearize", nat.ptr(g.inp[0]), nat.ptr(g.inp[1]),
+                     nat.ptr(self._relin.data), nat.ptr(g.out), nat.ptr(scratch), scratch.numel(), g.items,
+                     g.level, 1, st)
+        else:
+            ctx.call("fhb_ckks_rotate_multi", nat.ptr(g.inp), nat.ptr(g.key_ptrs), nat.ptr(g.galois),
+                     nat.ptr(g.out), nat.ptr(scratch), scratch.numel(), g.items, g.level, st)
+
+    def _issue(self) -> None:
+        eng = self.engine
+        if self.ks_order is not None:
+            eng.ctx.call("fhb_context_set_tuning", 0, self.ks_order)
+        cur = torch.cuda.current_stream(eng.device)
+        branches = self._streams[:self.streams]
+        for s in branches:
+            s.wait_stream(cur)
+        for g in self.groups:
+            self._issue_group(g, branches[g.stream], self._scratch[g.stream])
+        for s in branches:
+            cur.wait_stream(s)
+
+    def capture(self) -> None:
+        eng = self.engine
+        self._issue()  # first run eagerly: sets kernel attributes outside the capture
+        torch.cuda.synchronize(eng.device)
+        graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(eng.device)
+        cap.wait_stream(torch.cuda.current_stream(eng.device))
+        with torch.cuda.graph(graph, stream=cap):
+            self._issue()
+        torch.cuda.current_stream(eng.device).wait_stream(cap)
+        self._graph = graph
+
+    def run(self) -> None:
+        """One pass over the whole batch on the current stream."""
+        if not self.use_graph:
+            self._issue()
+            return
+        if self._graph is None:
+            self.capture()
+        self._graph.replay()
+
+    @property
+    def launches_per_run(self) -> int:
+        """Library kernels one run launches (excluding the input gathers)."""
+        return sum(5 if g.kind == HMULT else 3 for g in self.groups)
+
+    # ---------------------------------------------------------------- results
+    def result_view(self, op_index: int) -> torch.Tensor:
+        """[2, limbs, N] view of op `op_index`'s result inside its group arena."""
+        if op_index in self._copies:
+            return self.cts[self.ops[op_index].index].data.view(2, -1, self.engine.n)
+        g, j = self._slot[op_index]
+        return g.out[:, j]
+
+    def result(self, op_index: int) -> Ciphertext:
+        eng = self.engine
+        op = self.ops[op_index]
+        ct = self.cts[op.index]
+        data = self.result_view(op_index).contiguous().view(2, *ct.batch_shape, -1, eng.n)
+        if op_index in self._copies:
+            return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
+        if op.kind == HMULT:
+            scale = eng.rescale_to_next_output_scale(ct.scale * self.cts[op.partner].scale, level=ct.level)
+            return Ciphertext(data, ct.level + 1, scale, "coefficient", "standard")
+        return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
+
+    def results(self) -> list[Ciphertext]:
+        return [self.result(i) for i in range(len(self.ops))]
+
+
+def run_per_ciphertext(engine, ciphertexts: Sequence[Ciphertext], ops: Sequence[MixedOp]) -> list[Ciphertext]:
+    """The unbatched form: one engine call sequence per operation, exactly as
+    a caller of the reference engine issues them."""
+    out = []
+    for op in ops:
+        a = ciphertexts[op.index]
+        if op.kind == HMULT:
+            b = ciphertexts[op.partner]
+            out.append(engine.multiply_relinearize_rescale(engine.coefficient_domain_to_ntt_domain(a),
+                                                           engine.coefficient_domain_to_ntt_domain(b)))
+        else:
+            out.append(engine.rotate_by_step(a, op.step))
+    return out

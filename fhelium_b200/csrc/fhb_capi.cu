@@ -98,8 +98,8 @@ int mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t 
   FHB_DISPATCH(run_mul_coef, c, a, b, out, batch, level, st);
 }
 int ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-            int level, cudaStream_t st) {
-  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st);
+            int level, cudaStream_t st, const uint64_t* item_keys = nullptr) {
+  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys);
 }
 int prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st) {
   FHB_DISPATCH(run_prepare, c, digits, prepared, batch, level, st);
@@ -111,21 +111,23 @@ int apply_prepared(const Context& c, const void* prepared, const void* key, void
 
 template <typename T>
 int modup(const Context& c, const void* comp, void* digits, int64_t batch, int level, uint32_t galois,
-          cudaStream_t st) {
+          cudaStream_t st, const uint32_t* item_galois = nullptr) {
   const int limbs = c.num_q - level;
   const uint32_t ginv = galois == 1 ? 0u : galois_inverse(galois, c.log_n);
   k_modup_digits<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
-      (const T*)comp, (T*)digits, batch, limbs, c.log_n, level, ginv, tables<T>(c), level_tables<T>(c, level));
+      (const T*)comp, (T*)digits, batch, limbs, c.log_n, level, ginv, item_galois, tables<T>(c),
+      level_tables<T>(c, level));
   return cuda_status(cudaGetLastError(), "k_modup_digits");
 }
 
 template <typename T>
 int moddown(const Context& c, const void* t0, const void* t1, const void* a0, const void* a1, void* out,
-            int64_t batch, int level, uint32_t add0_galois, int rescale, cudaStream_t st) {
+            int64_t batch, int level, uint32_t add0_galois, int rescale, cudaStream_t st,
+            const uint32_t* item_galois = nullptr) {
   const uint32_t ginv = add0_galois == 1 ? 0u : galois_inverse(add0_galois, c.log_n);
   k_moddown<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
       (const T*)t0, (const T*)t1, (const T*)a0, (const T*)a1, (T*)out, batch, c.log_n, level, c.num_q, c.num_p,
-      ginv, rescale, tables<T>(c), level_tables<T>(c, level));
+      ginv, item_galois, rescale, tables<T>(c), level_tables<T>(c, level));
   return cuda_status(cudaGetLastError(), "k_moddown");
 }
 
@@ -281,6 +283,21 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi) {
   if (!ctx || !ctx->impl || !psi) return fail(-1, "NULL argument");
   if (prime_id < 0 || prime_id >= ctx->impl->qp()) return fail(-4, "prime id out of range");
   *psi = ctx->impl->roots[prime_id];
+  return 0;
+}
+
+int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
+  if (!ctx || !ctx->impl) return fail(-1, "context is NULL");
+  if (param != FHB_TUNE_KS_ORDER) return fail(-2, "unknown tuning parameter");
+  if (value != 0 && value != 1) return fail(-2, "key-switch work order must be 0 or 1");
+  ctx->impl->ks_order = value;
+  return 0;
+}
+
+int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value) {
+  if (!ctx || !ctx->impl || !value) return fail(-1, "NULL argument");
+  if (param != FHB_TUNE_KS_ORDER) return fail(-2, "unknown tuning parameter");
+  *value = ctx->impl->ks_order;
   return 0;
 }
 
@@ -510,6 +527,24 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
   TRY(FHB_WORD(fhb::modup, c, s.coef + 2 * comp, s.digits, batch, level, 1u, st));
   return keyswitch_tail(c, s, key, s.coef, s.coef + comp, 1u, out, batch, level, rescale, st);
+}
+
+int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t* key_ptrs, const uint32_t* galois,
+                          void* out, void* scratch, int64_t scratch_bytes, int64_t batch, int level,
+                          fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(ct, "ct"));
+  TRY(fhb::check_ptr(out, "out"));
+  TRY(fhb::check_ptr(scratch, "scratch"));
+  if (!key_ptrs || !galois) return fail(-2, "key_ptrs and galois must be device arrays of batch entries");
+  TRY(fhb::check_level(c, level));
+  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  const int limbs = c.num_q - level;
+  const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
+  const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
+  TRY(FHB_WORD(fhb::modup, c, static_cast<const char*>(ct) + comp, s.digits, batch, level, 1u, st, galois));
+  TRY(fhb::ks_core(c, s.digits, nullptr, s.t0, s.t1, batch, level, st, key_ptrs));
+  return FHB_WORD(fhb::moddown, c, s.t0, s.t1, ct, nullptr, out, batch, level, 1u, 0, st, galois);
 }
 
 int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,

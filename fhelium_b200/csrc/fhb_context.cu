@@ -220,6 +220,20 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+int ensure_dynamic_smem(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<int, const void*>, int>> done;
+  int device = 0;
+  cudaGetDevice(&device);
+  std::lock_guard<std::mutex> lock(mu);
+  for (const auto& e : done)
+    if (e.first.first == device && e.first.second == kernel && e.second >= bytes) return 0;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute");
+  done.push_back({{device, kernel}, bytes});
+  return 0;
+}
+
 int cuda_status(cudaError_t e, const char* where) {
   if (e == cudaSuccess) return 0;
   set_error(std::string(where) + ": " + cudaGetErrorString(e));

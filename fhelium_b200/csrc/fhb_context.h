@@ -56,6 +56,7 @@ struct Context {
   std::vector<LevelTables<uint64_t>> lv64;
   std::vector<LevelTables<uint32_t>> lv32;
   std::vector<void*> allocations;
+  int ks_order = 0;  // tuning: work order of the key-switch clusters (see ks_work)
   int qp() const { return num_q + num_p; }
   int n() const { return 1 << log_n; }
 };
@@ -77,5 +78,9 @@ inline const LevelTables<uint32_t>& level_tables<uint32_t>(const Context& c, int
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_status(cudaError_t e, const char* where);
+// Opt `kernel` into `bytes` of dynamic shared memory on the current device,
+// once per (device, kernel): later launches (also those recorded into CUDA
+// graphs) make no further runtime calls.
+int ensure_dynamic_smem(const void* kernel, int bytes);
 
 }  // namespace fhb

@@ -187,6 +187,14 @@ __device__ __forceinline__ int galois_source(int j, int log_n, uint32_t ginv, bo
   return int(i & ((1u << log_n) - 1));
 }
 
+// Inverse of an odd Galois element modulo 2N (Newton iteration mod 2^32).
+__device__ __forceinline__ uint32_t galois_inverse_dev(uint32_t g, int log_n) {
+  uint32_t x = 1;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) x *= 2u - g * x;
+  return x & ((2u << log_n) - 1);
+}
+
 // NTT-domain automorphism gather (bit-reversed evaluation order):
 // destination k reads br(((2 br(k) + 1) g mod 2N - 1) / 2)
 // (fhelium/engine/hybrid_keyswitch.py:506-528).
@@ -205,8 +213,8 @@ __device__ __forceinline__ int galois_ntt_source(int k, int log_n, uint32_t g) {
 // the input is first mapped through sigma_g (rotation).
 template <typename T>
 __global__ void k_modup_digits(const T* __restrict__ comp, T* __restrict__ digits, int64_t batch,
-                               int limbs, int log_n, int level, uint32_t ginv, ChainTables<T> tabs,
-                               LevelTables<T> lt) {
+                               int limbs, int log_n, int level, uint32_t ginv,
+                               const uint32_t* __restrict__ item_galois, ChainTables<T> tabs, LevelTables<T> lt) {
   const int64_t n = int64_t(1) << log_n;
   const int64_t total = batch * n;
   using W = Word<T>;
@@ -215,7 +223,9 @@ __global__ void k_modup_digits(const T* __restrict__ comp, T* __restrict__ digit
     const int64_t bi = idx >> log_n;
     const int k = int(idx & (n - 1));
     bool neg = false;
-    const int srck = ginv ? galois_source(k, log_n, ginv, neg) : k;
+    // per-item Galois elements (mixed-step rotation batches) override ginv
+    const uint32_t gi = item_galois ? (item_galois[bi] == 1 ? 0u : galois_inverse_dev(item_galois[bi], log_n)) : ginv;
+    const int srck = gi ? galois_source(k, log_n, gi, neg) : k;
     const T* src = comp + bi * limbs * n;
     T* dst = digits + bi * limbs * n;
     for (int a = 0; a < lt.num_digits; ++a) {
@@ -330,6 +340,23 @@ struct KsAcc {
   }
 };
 
+// Work order of the per-(ciphertext, row) clusters of the key-switch kernels:
+// order 0 runs the rows of one ciphertext back to back; order 1 runs row j of
+// every ciphertext back to back, so concurrently resident clusters read the
+// same key rows (chosen by the autotuner).
+__device__ __forceinline__ void ks_work(int64_t cluster, int qp_limbs, int64_t batch, int order, int64_t& poly,
+                                        int64_t& bi, int& jrow) {
+  if (order == 0) {
+    poly = cluster;
+    bi = poly / qp_limbs;
+    jrow = int(poly % qp_limbs);
+  } else {
+    jrow = int(cluster / batch);
+    bi = cluster % batch;
+    poly = bi * qp_limbs + jrow;
+  }
+}
+
 // acc += v * key (both key components), streaming the key rows in 16-byte
 // pieces so that only two key words per component are live at a time.
 template <typename T, class Acc, int E>
@@ -370,21 +397,22 @@ __device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[E], const T* key0
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
-                 T* __restrict__ acc1, int q_limbs, int qp_limbs, int level, int qp0,
-                 ChainTables<T> tabs, LevelTables<T> lt) {
+                 T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
+                 const unsigned long long* __restrict__ item_keys, ChainTables<T> tabs, LevelTables<T> lt) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;  // over [B, QP_l]
-  const int64_t bi = poly / qp_limbs;
-  const int jrow = int(poly % qp_limbs);
+  int64_t poly, bi;  // poly over [B, QP_l]
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
   const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  if (item_keys) key = reinterpret_cast<const T*>(item_keys[bi]);  // mixed-key batch
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
@@ -423,15 +451,15 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64_t batch, int q_limbs,
-                   int qp_limbs, int level, int qp0, ChainTables<T> tabs, LevelTables<T> lt) {
+                   int qp_limbs, int level, int qp0, int order, ChainTables<T> tabs, LevelTables<T> lt) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;  // over [B, QP_l]
-  const int64_t bi = poly / qp_limbs;
-  const int jrow = int(poly % qp_limbs);
+  int64_t poly, bi;  // poly over [B, QP_l]
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
@@ -467,14 +495,16 @@ template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ key, T* __restrict__ acc0,
                           T* __restrict__ acc1, int64_t batch, int qp_limbs, int level, int qp0,
-                          uint32_t galois, ChainTables<T> tabs, LevelTables<T> lt) {
+                          uint32_t galois, int order, ChainTables<T> tabs, LevelTables<T> lt) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;
-  const int jrow = int(poly % qp_limbs);
+  int64_t poly, bi;
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  (void)bi;
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const int own = rank * G::kM + threadIdx.x * G::kE;
@@ -516,8 +546,9 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
 template <typename T>
 __global__ void k_moddown(const T* __restrict__ t0, const T* __restrict__ t1, const T* __restrict__ add0,
                           const T* __restrict__ add1, T* __restrict__ out, int64_t batch, int log_n,
-                          int level, int num_q, int num_p, uint32_t add0_ginv, int rescale,
-                          ChainTables<T> tabs, LevelTables<T> lt) {
+                          int level, int num_q, int num_p, uint32_t add0_ginv,
+                          const uint32_t* __restrict__ item_galois, int rescale, ChainTables<T> tabs,
+                          LevelTables<T> lt) {
   using W = Word<T>;
   const int64_t n = int64_t(1) << log_n;
   const int q_limbs = num_q - level;
@@ -530,7 +561,9 @@ __global__ void k_moddown(const T* __restrict__ t0, const T* __restrict__ t1, co
     const int64_t bi = idx >> log_n;
     const int k = int(idx & (n - 1));
     bool neg = false;
-    const int ak = add0_ginv ? galois_source(k, log_n, add0_ginv, neg) : k;
+    const uint32_t gi =
+        item_galois ? (item_galois[bi] == 1 ? 0u : galois_inverse_dev(item_galois[bi], log_n)) : add0_ginv;
+    const int ak = gi ? galois_source(k, log_n, gi, neg) : k;
     for (int c = 0; c < 2; ++c) {
       const T* t = (c == 0 ? t0 : t1) + bi * qp_limbs * n;
       const T* ad = c == 0 ? add0 : add1;

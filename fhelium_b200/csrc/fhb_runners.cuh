@@ -11,8 +11,8 @@ int launch_cluster(void (*kernel)(KArgs...), int64_t polys, size_t smem, cudaStr
   using G = NttGeom<T, LOGN>;
   if (polys <= 0) return 0;
   if (polys * G::kC > 0x7fffffffLL) return fail(-6, "too many polynomials for one launch");
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-  if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute");
+  const int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), int(smem));
+  if (rc != 0) return rc;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(unsigned(polys * G::kC));
   cfg.blockDim = dim3(G::kThreads);
@@ -61,11 +61,12 @@ int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int6
 
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st) {
+                int level, cudaStream_t st, const uint64_t* item_keys) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
   return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
-                                 (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, ql, qpl, level, c.qp(),
-                                 tables<T>(c), level_tables<T>(c, level));
+                                 (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(),
+                                 c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys), tables<T>(c),
+                                 level_tables<T>(c, level));
 }
 
 template <typename T, int LOGN>
@@ -73,8 +74,8 @@ int run_prepare(const Context& c, const void* digits, void* prepared, int64_t ba
                 cudaStream_t st) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
   return launch_cluster<T, LOGN>(k_prepare_rotation<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
-                                 (const T*)digits, (T*)prepared, batch, ql, qpl, level, c.qp(), tables<T>(c),
-                                 level_tables<T>(c, level));
+                                 (const T*)digits, (T*)prepared, batch, ql, qpl, level, c.qp(), c.ks_order,
+                                 tables<T>(c), level_tables<T>(c, level));
 }
 
 template <typename T, int LOGN>
@@ -83,7 +84,7 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   const int ql = c.num_q - level, qpl = ql + c.num_p;
   return launch_cluster<T, LOGN>(k_apply_prepared_rotation<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
                                  (const T*)prepared, (const T*)key, (T*)acc0, (T*)acc1, batch, qpl, level, c.qp(),
-                                 galois == 1 ? 0u : galois, tables<T>(c), level_tables<T>(c, level));
+                                 galois == 1 ? 0u : galois, c.ks_order, tables<T>(c), level_tables<T>(c, level));
 }
 
 // Explicit instantiation of every runner for one (T, LOGN).
@@ -92,7 +93,7 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   template int run_inverse<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, int, cudaStream_t);    \
   template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, cudaStream_t); \
   template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
-                                    cudaStream_t);                                                              \
+                                    cudaStream_t, const uint64_t*);                                             \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);

@@ -17,7 +17,7 @@ int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int6
                  cudaStream_t st);
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st);
+                int level, cudaStream_t st, const uint64_t* item_keys);
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
 template <typename T, int LOGN>

@@ -385,6 +385,24 @@ class CkksEngine:
                       ct.batch_size, ct.level, key.galois_element, self._stream())
         return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
 
+    def rotate_items_with_keys(self, ct: Ciphertext, keys: Sequence[RotationKey]) -> Ciphertext:
+        """Rotates batch item b of `ct` with keys[b] (mixed steps, one launch
+        sequence); bit-identical to rotating every item on its own."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        if len(keys) != ct.batch_size:
+            raise ValueError("need one rotation key per batch item")
+        galois = torch.tensor([k.galois_element for k in keys], dtype=torch.int32, device=self.device)
+        for k in keys:
+            if k.data.device != self.device or k.data.dtype != self.dtype or not k.data.is_contiguous():
+                raise ValueError("rotation keys must be contiguous tensors on this engine's device/dtype")
+        key_ptrs = torch.tensor([k.data.data_ptr() for k in keys], dtype=torch.int64, device=self.device)
+        out = torch.empty_like(ct.data)
+        scratch, nbytes = self._scratch_for(ct.batch_size, ct.level)
+        self.ctx.call("fhb_ckks_rotate_multi", nat.ptr(ct.data), nat.ptr(key_ptrs), nat.ptr(galois), nat.ptr(out),
+                      nat.ptr(scratch), nbytes, ct.batch_size, ct.level, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
+
     def prepare_rotation_digits(self, ct: Ciphertext) -> torch.Tensor:
         """Hoisted ModUp of c1: [digit, *batch, Q_l + P, N] NTT-domain digits."""
         ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)

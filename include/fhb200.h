@@ -59,6 +59,14 @@ int fhb_context_destroy(fhb_context* ctx);
  * fhelium/engine/ntt/plans/twiddles.py:10-20). */
 int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
 
+/* Launch tuning of a context (set by the autotuner, fhelium_b200/autotune.py).
+ * FHB_TUNE_KS_ORDER: work order of the key-switch clusters, 0 = the rows of
+ * one ciphertext back to back, 1 = one row across the batch back to back.
+ * No counterpart in the reference (its launches have no tunable order). */
+enum fhb_tuning_param { FHB_TUNE_KS_ORDER = 0 };
+int fhb_context_set_tuning(fhb_context* ctx, int param, int value);
+int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);
+
 /* Forward negacyclic NTT of `batch` x `rows` polynomials whose rows are prime
  * ids [row_start, row_start + rows).  input_montgomery = 0: standard input,
  * output x R (forward_ntt_to_montgomery_*); = 1: Montgomery input
@@ -241,6 +249,17 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
  * CkksEngine._apply_rotation_key (fhelium/engine/ckks_engine.py:3822-3897). */
 int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,
                     int64_t scratch_bytes, int64_t batch, int level, uint32_t galois, fhb_stream stream);
+
+/* Mixed-step rotation of one level: item b of ct [2, batch, L, N]
+ * (coefficient/standard) is rotated by its own Galois element galois[b]
+ * with the key at key_ptrs[b] (a device address of a [digits, 2, QP, N]
+ * key).  key_ptrs and galois are DEVICE arrays of batch entries.  Replaces
+ * a loop of CkksEngine._apply_rotation_key calls, one per ciphertext
+ * (fhelium/engine/ckks_engine.py:3822-3897), with one launch sequence.
+ * The reference has no batched mixed-step counterpart. */
+int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t* key_ptrs, const uint32_t* galois,
+                          void* out, void* scratch, int64_t scratch_bytes, int64_t batch, int level,
+                          fhb_stream stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,107 @@
+"""Mixed-level batches: one CUDA graph over every (kind, level) group against
+one engine call sequence per ciphertext, bit for bit, and the autotuner."""
+
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from fhelium_b200 import autotune
+from fhelium_b200.batch import HMULT, ROTATE, MixedBatchExecutor, MixedOp, run_per_ciphertext, sample_mixed_workload
+from fhelium_b200.config import Preset
+from fhelium_b200.engine import CkksEngine
+
+pytestmark = pytest.mark.gpu
+
+
+def _workload(eng, count, seed, max_step):
+    levels, ops = sample_mixed_workload(eng.num_q, count, max_step=max_step, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    cts = [eng.encrypt_message(rng.uniform(-0.05, 0.05, eng.num_slots), level=lv) for lv in levels]
+    return cts, ops
+
+
+@pytest.fixture(scope="module")
+def small():
+    eng = CkksEngine(Preset.slots8192_scale40_levels7_int64, rng_seed=3)
+    cts, ops = _workload(eng, 40, seed=11, max_step=1 << 12)
+    want = run_per_ciphertext(eng, cts, ops)
+    return eng, cts, ops, want
+
+
+@pytest.mark.parametrize("streams,use_graph", [(1, False), (1, True), (3, True)])
+def test_mixed_batch_bit_exact(small, streams, use_graph):
+    eng, cts, ops, want = small
+    ex = MixedBatchExecutor(eng, cts, ops, streams=streams, use_graph=use_graph)
+    for _ in range(2):  # replays read the inputs afresh
+        ex.run()
+    torch.cuda.synchronize()
+    kinds = {op.kind for op in ops}
+    assert kinds == {HMULT, ROTATE}
+    for i, w in enumerate(want):
+        got = ex.result(i)
+        assert (got.level, got.scale) == (w.level, w.scale)
+        assert torch.equal(got.data, w.data), f"op {i} ({ops[i]}) differs"
+
+
+def test_mixed_batch_decrypts(small):
+    eng, cts, ops, _ = small
+    ex = MixedBatchExecutor(eng, cts, ops, streams=2)
+    ex.run()
+    for i, op in enumerate(ops[:12]):
+        x = eng.decrypt_message(cts[op.index], is_real=True)
+        got = eng.decrypt_message(ex.result(i), is_real=True)
+        if op.kind == HMULT:
+            want = x * eng.decrypt_message(cts[op.partner], is_real=True)
+        else:
+            want = torch.roll(x, shifts=op.step, dims=-1)
+        assert float((got - want).abs().max()) < 2e-5
+
+
+def test_inputs_updated_between_replays(small):
+    eng, cts, ops, _ = small
+    mine = [c.clone() for c in cts]
+    ex = MixedBatchExecutor(eng, mine, ops, streams=2)
+    ex.run()
+    first = ex.result(0).data.clone()
+    i0 = ops[0].index
+    other = next(j for j, c in enumerate(cts) if j != i0 and c.level == cts[i0].level)
+    mine[i0].data.copy_(cts[other].data)
+    ex.run()
+    assert not torch.equal(ex.result(0).data, first)
+    mine[i0].data.copy_(cts[i0].data)
+    ex.run()
+    assert torch.equal(ex.result(0).data, first)
+
+
+def test_zero_step_is_a_copy(small):
+    eng, cts, _, _ = small
+    ops = [MixedOp(ROTATE, 0, step=0), MixedOp(ROTATE, 1, step=eng.num_slots), MixedOp(HMULT, 2, partner=2)]
+    ex = MixedBatchExecutor(eng, cts, ops, streams=1)
+    ex.run()
+    assert torch.equal(ex.result(0).data, cts[0].data)
+    assert torch.equal(ex.result(1).data, cts[1].data)
+
+
+def test_rejects_cross_level_partner(small):
+    eng, cts, _, _ = small
+    a = next(i for i, c in enumerate(cts) if c.level != cts[0].level)
+    with pytest.raises(ValueError):
+        MixedBatchExecutor(eng, cts, [MixedOp(HMULT, 0, partner=a)])
+
+
+def test_autotune_picks_and_caches(small, tmp_path):
+    eng, cts, ops, want = small
+    ex = MixedBatchExecutor(eng, cts, ops, streams=1)
+    path = str(tmp_path / "tune.json")
+    first = autotune.tune_mixed_batch(eng, ex, streams=(1, 2), repeats=1, cache_path=path)
+    assert not first["cached"] and len(first["candidates"]) == 4
+    assert (ex.streams, ex.ks_order) == (first["streams"], first["ks_order"])
+    with open(path) as f:
+        assert autotune.workload_key(eng, ex) in json.load(f)
+    second = autotune.tune_mixed_batch(eng, ex, streams=(1, 2), repeats=1, cache_path=path)
+    assert second["cached"] and second["streams"] == first["streams"]
+    ex.run()
+    for i, w in enumerate(want):
+        assert torch.equal(ex.result(i).data, w.data)

@@ -113,6 +113,22 @@ def test_rotate_matches_oracle(family, log_n, level, step):
     np.testing.assert_array_equal(to_np(got.data), want)
 
 
+@pytest.mark.parametrize("family,log_n,level", CASES)
+def test_mixed_step_rotation_matches_oracle(family, log_n, level):
+    """fhb_ckks_rotate_multi: every batch item with its own step and key."""
+    cfg, eng, orc, rng = _setup(family, log_n, level, 8)
+    rows = orc.q_rows(level)
+    steps = [1, -3, 8, 0x155 % eng.num_slots]
+    ct = uniform_residues(rng, cfg.moduli, rows, (2, len(steps)), cfg.N)
+    keys_np = [random_key(rng, cfg, cfg.N) for _ in steps]
+    keys = [RotationKey(to_dev(k, cfg), rotation_step=s % eng.num_slots, galois_element=eng.galois_element_for_step(s))
+            for k, s in zip(keys_np, steps)]
+    got = eng.rotate_items_with_keys(Ciphertext(to_dev(ct, cfg), level, 1.0), keys)
+    want = np.stack([orc.rotate(ct[:, b], s % eng.num_slots, k, level)
+                     for b, (s, k) in enumerate(zip(steps, keys_np))], axis=1)
+    np.testing.assert_array_equal(to_np(got.data), want)
+
+
 @pytest.mark.parametrize("family,log_n,level", CASES[:4])
 def test_hoisted_rotations_match_oracle(family, log_n, level):
     cfg, eng, orc, rng = _setup(family, log_n, level, 6)
