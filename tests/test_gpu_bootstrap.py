@@ -1,0 +1,65 @@
+"""Full-slot bootstrapping on the GPU.
+
+Bounds follow the reference's own logN=16 bootstrap test
+(tests/test_ckks_bootstrap.py:482-485: max error < 7e-3, mean < 1.5e-3 for a
+real linspace(-0.1, 0.1) message); the refreshed ciphertext must also
+support further multiplications.
+"""
+
+import math
+
+import pytest
+import torch
+
+from fhelium_b200.bootstrap import FullSlotBootstrap
+from fhelium_b200.config import CkksConfig, Preset
+from fhelium_b200.engine import CkksEngine
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(cfg, message):
+    eng = CkksEngine(cfg, galois_generator=5, rng_seed=3)
+    bs = FullSlotBootstrap(eng)
+    bs.generate_keys()
+    ct = eng.encrypt_message(message, level=eng.public_level_count - 1)
+    out = bs(ct)
+    assert out.level == bs.output_level
+    return eng, out
+
+
+def test_bootstrap_small_ring_complex_slots():
+    cfg = CkksConfig(logN=12, scale_bits=50, base_prime_bits=50, num_scale_primes=27, num_p_primes=4)
+    g = torch.Generator().manual_seed(4)
+    n = cfg.N // 2
+    m = (torch.rand((2, n), dtype=torch.float64, generator=g) * 2 - 1) \
+        + 1j * (torch.rand((2, n), dtype=torch.float64, generator=g) * 2 - 1)
+    eng, out = _run(cfg, m)
+    err = (eng.decrypt_message(out) - m).abs()
+    # With scale = base prime (2^50) the coefficients of a full-range complex
+    # message are ~|m|/sqrt(N) of q0, where sin(2 pi x)/(2 pi) departs from x
+    # by ~x^3: about 6.8 bits at N = 2^12 (9.2e-3 max, 3.0e-3 mean), gaining
+    # about one bit per doubling of N (10.1 bits at N = 2^16).  The same ring
+    # with the reference test's real +-0.1 message reaches 15.9 bits.
+    assert float(err.max()) < 1.5e-2 and float(err.mean()) < 4e-3
+    # the refreshed ciphertext multiplies again
+    sq = eng.multiply_relinearize_rescale(eng.coefficient_domain_to_ntt_domain(out),
+                                          eng.coefficient_domain_to_ntt_domain(out))
+    assert float((eng.decrypt_message(sq) - m * m).abs().max()) < 2e-2
+
+
+def test_bootstrap_small_ring_reference_input():
+    cfg = CkksConfig(logN=12, scale_bits=50, base_prime_bits=50, num_scale_primes=27, num_p_primes=4)
+    x = torch.linspace(-0.1, 0.1, cfg.N // 2, dtype=torch.float64)
+    eng, out = _run(cfg, x)
+    err = (eng.decrypt_message(out, is_real=True) - x).abs()
+    assert float(err.max()) < 1e-4 and float(err.mean()) < 3e-5
+
+
+def test_bootstrap_reference_preset_reference_input():
+    cfg = CkksConfig.parse(Preset.slots32768_scale50_levels27_int64, base_prime_bits=50)
+    x = torch.linspace(-0.1, 0.1, cfg.N // 2, dtype=torch.float64)
+    eng, out = _run(cfg, x)
+    err = (eng.decrypt_message(out, is_real=True) - x).abs()
+    assert float(err.max()) < 7e-3 and float(err.mean()) < 1.5e-3
+    assert -math.log2(float(err.max())) > 8
