@@ -172,8 +172,11 @@ def ntt_int32_primes(count: int = 36, log_n: int = 16) -> list[int]:
 
 def ntt_leg(dev, stream, steps):
     """Standalone forward + inverse NTT: N = 2^16, 36 int32 limbs, batch 64,
-    residues uniform in [0, q_i) (seed 1).  Round trip checked bit-exact."""
+    residues uniform in [0, q_i) (seed 1).  Timed with the default launch
+    shape (8 residues per thread) and with the autotuner's pick; the round
+    trip is checked bit-exact under both."""
     from fhelium_b200 import _native as nat
+    from fhelium_b200 import autotune
     primes = ntt_int32_primes()
     ctx = nat.NativeContext(32, 16, primes, len(primes) - 1, 1, dev)
     g = torch.Generator(device=dev)
@@ -186,14 +189,27 @@ def ntt_leg(dev, stream, steps):
     s = stream.cuda_stream
     fwd = lambda: nat.check(ctx.lib.fhb_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), B, L, 0, 0, s), "ntt")
     inv = lambda: nat.check(ctx.lib.fhb_inverse_ntt(ctx.handle, y.data_ptr(), z.data_ptr(), B, L, 0, 2, s), "intt")
-    fwd_ms = _time_events(fwd, max(3, steps), stream)
-    inv_ms = _time_events(inv, max(3, steps), stream)
-    exact = bool(torch.equal(x, z))
     nbytes = 2 * B * L * N * 4  # read + write per direction
+    for _ in range(3):  # warm-up (clocks, caches, kernel attributes)
+        fwd()
+        inv()
+    torch.cuda.synchronize(dev)
+    out = {}
+    for tag in ("plain", "tuned"):
+        if tag == "tuned":
+            tune = autotune.tune_ntt(ctx, x, L, use_cache=False)
+            out["autotune"] = {k: tune[k] for k in ("forward_ept", "inverse_ept", "candidates")}
+        fwd_ms = _time_events(fwd, max(3, steps), stream)
+        inv_ms = _time_events(inv, max(3, steps), stream)
+        out[tag] = {"forward_ms": fwd_ms, "inverse_ms": inv_ms, "roundtrip_bit_exact": bool(torch.equal(x, z)),
+                    "forward_gbs": nbytes / (fwd_ms / 1e3) / 1e9, "inverse_gbs": nbytes / (inv_ms / 1e3) / 1e9,
+                    "limb_ntts_per_s": 2 * B * L / ((fwd_ms + inv_ms) / 1e3)}
+        z.zero_()
+        fwd()
+        inv()
+        out[tag]["roundtrip_bit_exact"] = bool(torch.equal(x, z))
     ctx.close()
-    return {"forward_ms": fwd_ms, "inverse_ms": inv_ms, "roundtrip_bit_exact": exact,
-            "forward_gbs": nbytes / (fwd_ms / 1e3) / 1e9, "inverse_gbs": nbytes / (inv_ms / 1e3) / 1e9,
-            "limb_ntts_per_s": 2 * B * L / ((fwd_ms + inv_ms) / 1e3)}
+    return out
 
 
 def bootstrap_leg(dev, stream, batch=8, steps=2):

@@ -55,6 +55,7 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_relinearize_noalloc_max_scratch_bytes": (_I64, []),
 }
 
+TUNE_KS_ORDER, TUNE_NTT_FORWARD_EPT, TUNE_NTT_INVERSE_EPT = range(3)
 OP_MONTGOMERY_MUL, OP_ADD_LAZY, OP_SUB_LAZY, OP_ADD_CANONICAL, OP_SUB_CANONICAL, OP_NEGATE = range(6)
 INV_MONTGOMERY, INV_STANDARD_LAZY, INV_STANDARD, INV_CENTERED = range(4)
 
@@ -129,6 +130,14 @@ class NativeContext:
     def root(self, prime_id: int) -> int:
         out = ctypes.c_uint64()
         check(self.lib.fhb_context_root(self.handle, prime_id, ctypes.byref(out)), "fhb_context_root")
+        return int(out.value)
+
+    def set_tuning(self, param: int, value: int) -> None:
+        check(self.lib.fhb_context_set_tuning(self.handle, param, value), "fhb_context_set_tuning")
+
+    def get_tuning(self, param: int) -> int:
+        out = ctypes.c_int()
+        check(self.lib.fhb_context_get_tuning(self.handle, param, ctypes.byref(out)), "fhb_context_get_tuning")
         return int(out.value)
 
     def call(self, name: str, *args) -> None:

@@ -8,12 +8,15 @@ The knobs a run can change without recompiling:
   the batch back to back (the key rows of one prime are shared by the whole
   batch, which pays when every item uses the same key);
 * ``streams``: how many graph branches the mixed-batch executor spreads its
-  (kind, level) groups over, i.e. how many groups run side by side.
+  (kind, level) groups over, i.e. how many groups run side by side;
+* ``ntt_forward_ept`` / ``ntt_inverse_ept`` (FHB_TUNE_NTT_{FORWARD,INVERSE}_EPT):
+  residues per thread of the standalone transforms, i.e. the NTT's register
+  radix and tile: 8 residues (radix-8 passes, 1024 threads per CTA at
+  N = 2^16) or 16 (radix-16 passes, 512 threads).
 
-The NTT geometry (cluster width, residues per thread, radix of the register
-passes) is fixed per ring degree when the library is compiled; every
-runtime knob above is picked here by timing CUDA-graph replays on the
-caller's own workload.  Winners are cached in a JSON file keyed by device,
+The cluster width (CTAs per polynomial) is fixed per ring degree when the
+library is compiled; every runtime knob above is picked here by timing the
+caller's own workload (CUDA-graph replays for batches).  Winners are cached in a JSON file keyed by device,
 ring, modulus chain and workload shape, so a later process with the same
 workload skips the search.  The reference has no autotuner (its launch
 shapes are fixed in csrc/ops/ntt/cuda/*.cu).
@@ -85,6 +88,45 @@ def time_replays(run, device, *, warmup: int = 1, repeats: int = 3) -> float:
         times.append(start.elapsed_time(stop))
     times.sort()
     return times[len(times) // 2]
+
+
+def tune_ntt(ctx, x: torch.Tensor, rows: int, row_start: int = 0, *, candidates: Iterable[int] = (8, 16),
+             repeats: int = 5, cache_path: str | None = None, use_cache: bool = True) -> dict:
+    """Pick residues per thread of the forward and of the inverse NTT for
+    polynomials shaped like `x` ([..., rows, N] residues of prime ids
+    [row_start, row_start + rows) on ctx's device) and leave `ctx` set to the
+    winners.  Returns ``{"forward_ept", "inverse_ept", "forward_ms", ...}``."""
+    from . import _native as nat
+    cache_path = cache_path or default_cache_path()
+    n = x.size(-1)
+    batch = x.numel() // (rows * n)
+    dev = x.device
+    bits = 32 if x.element_size() == 4 else 64
+    key = f"{torch.cuda.get_device_name(dev)}|ntt|bits={bits}|N={n}|rows={rows}|row_start={row_start}|batch={batch}"
+    if use_cache:
+        hit = _load(cache_path).get(key)
+        if hit and {"forward_ept", "inverse_ept"} <= set(hit):
+            ctx.set_tuning(nat.TUNE_NTT_FORWARD_EPT, int(hit["forward_ept"]))
+            ctx.set_tuning(nat.TUNE_NTT_INVERSE_EPT, int(hit["inverse_ept"]))
+            return dict(hit, cached=True)
+    y = torch.empty_like(x)
+    z = torch.empty_like(x)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    fwd = lambda: ctx.call("fhb_forward_ntt", x.data_ptr(), y.data_ptr(), batch, rows, row_start, 0, st)
+    inv = lambda: ctx.call("fhb_inverse_ntt", y.data_ptr(), z.data_ptr(), batch, rows, row_start, 2, st)
+    entry: dict = {"candidates": {}}
+    for name, param, fn in (("forward", nat.TUNE_NTT_FORWARD_EPT, fwd), ("inverse", nat.TUNE_NTT_INVERSE_EPT, inv)):
+        times = {}
+        for ept in candidates:
+            ctx.set_tuning(param, int(ept))
+            times[int(ept)] = time_replays(fn, dev, warmup=2, repeats=repeats)
+        best = min(times, key=times.get)
+        ctx.set_tuning(param, best)
+        entry[f"{name}_ept"] = best
+        entry[f"{name}_ms"] = times[best]
+        entry["candidates"][name] = {str(k): v for k, v in times.items()}
+    _store(cache_path, key, entry)
+    return dict(entry, cached=False)
 
 
 def tune_mixed_batch(engine, executor, *, ks_orders: Iterable[int] = (0, 1), streams: Iterable[int] = (1, 2, 3, 4),

@@ -288,17 +288,29 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi) {
 
 int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
   if (!ctx || !ctx->impl) return fail(-1, "context is NULL");
-  if (param != FHB_TUNE_KS_ORDER) return fail(-2, "unknown tuning parameter");
-  if (value != 0 && value != 1) return fail(-2, "key-switch work order must be 0 or 1");
-  ctx->impl->ks_order = value;
-  return 0;
+  switch (param) {
+    case FHB_TUNE_KS_ORDER:
+      if (value != 0 && value != 1) return fail(-2, "key-switch work order must be 0 or 1");
+      ctx->impl->ks_order = value;
+      return 0;
+    case FHB_TUNE_NTT_FORWARD_EPT:
+    case FHB_TUNE_NTT_INVERSE_EPT:
+      if (value != 0 && value != 8 && value != 16) return fail(-2, "residues per thread must be 0, 8 or 16");
+      (param == FHB_TUNE_NTT_FORWARD_EPT ? ctx->impl->ntt_ept_fwd : ctx->impl->ntt_ept_inv) = value;
+      return 0;
+    default:
+      return fail(-2, "unknown tuning parameter");
+  }
 }
 
 int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value) {
   if (!ctx || !ctx->impl || !value) return fail(-1, "NULL argument");
-  if (param != FHB_TUNE_KS_ORDER) return fail(-2, "unknown tuning parameter");
-  *value = ctx->impl->ks_order;
-  return 0;
+  switch (param) {
+    case FHB_TUNE_KS_ORDER: *value = ctx->impl->ks_order; return 0;
+    case FHB_TUNE_NTT_FORWARD_EPT: *value = ctx->impl->ntt_ept_fwd; return 0;
+    case FHB_TUNE_NTT_INVERSE_EPT: *value = ctx->impl->ntt_ept_inv; return 0;
+    default: return fail(-2, "unknown tuning parameter");
+  }
 }
 
 int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,

@@ -57,6 +57,8 @@ struct Context {
   std::vector<LevelTables<uint32_t>> lv32;
   std::vector<void*> allocations;
   int ks_order = 0;  // tuning: work order of the key-switch clusters (see ks_work)
+  int ntt_ept_fwd = 0;  // tuning: residues per thread of the standalone forward NTT (0 = default)
+  int ntt_ept_inv = 0;  // tuning: same for the inverse NTT and the fused HMult -> inverse NTT
   int qp() const { return num_q + num_p; }
   int n() const { return 1 << log_n; }
 };

@@ -54,25 +54,34 @@ __device__ __forceinline__ int cluster_rank() {
 // ---------------------------------------------------------------------------
 // Plain forward NTT: standard -> NTT/Montgomery (x R) or Montgomery -> NTT.
 // Output lazy [0, 2q) as in csrc/ops/ntt/forward_ntt.cpp:19-22.
-template <typename T, int LOGN, bool TO_MONT>
-__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+// Source of a plain forward transform: the input row, optionally taken to
+// Montgomery form on the fly.  Plain loads: `in` may alias the output.
+template <typename T, bool TO_MONT>
+struct RowSource {
+  const T* in;
+  T c, cs, q;
+  __device__ __forceinline__ T operator()(int pos) const {
+    T v = in[pos];
+    if constexpr (TO_MONT) v = Word<T>::shoup(v, c, cs, q);
+    return v;
+  }
+};
+
+template <typename T, int LOGN, bool TO_MONT, int EPT = 0>
+__global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start,
               ChainTables<T> tabs) {
-  using G = NttGeom<T, LOGN>;
+  using G = NttGeom<T, LOGN, EPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
   const int64_t poly = blockIdx.x / G::kC;
   const int pid = row_start + int(poly % rows);
   const PrimeInfo<T> p = tabs.prime[pid];
-  const T* src = in + poly * G::kN + int64_t(rank) * G::kM;
-  for (int i = threadIdx.x; i < G::kM; i += G::kThreads) {
-    T v = src[i];
-    if constexpr (TO_MONT) v = Word<T>::shoup(v, p.rmod, p.rmod_s, p.q);
-    s[G::sidx(i)] = v;
-  }
+  RowSource<T, TO_MONT> src{in + poly * G::kN, p.rmod, p.rmod_s, p.q};
   T v[G::kE];
-  Ntt<T, LOGN>::forward(s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v);
+  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::forward_from(src, s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q,
+                                                     rank, v);
 #pragma unroll
   for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
   store16(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
@@ -104,11 +113,11 @@ __device__ __forceinline__ InvEpilogue<T> make_inv_epilogue(T* dst, const PrimeI
 }
 
 // Plain inverse NTT from NTT/Montgomery lazy input.
-template <typename T, int LOGN>
-__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+template <typename T, int LOGN, int EPT = 0>
+__global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start, int kind,
               ChainTables<T> tabs) {
-  using G = NttGeom<T, LOGN>;
+  using G = NttGeom<T, LOGN, EPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
@@ -118,7 +127,8 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
   T v[G::kE];
   load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
   InvEpilogue<T> epi = make_inv_epilogue<T>(out + poly * G::kN, p, kind, true);
-  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, epi);
+  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v,
+                                                epi);
 }
 
 // ---------------------------------------------------------------------------
@@ -126,11 +136,11 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
 // a, b: [2, B, L, N] NTT/Montgomery lazy; out: [3, B, L, N] coefficient/standard
 // canonical = INTT of (a0 b0, a0 b1 + a1 b0, a1 b1)
 // (fhelium/engine/ckks_engine.py:1570-1606 then :1655-1660).
-template <typename T, int LOGN>
-__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+template <typename T, int LOGN, int EPT = 0>
+__global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
                      int64_t batch, int limbs, int level, ChainTables<T> tabs) {
-  using G = NttGeom<T, LOGN>;
+  using G = NttGeom<T, LOGN, EPT>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
@@ -158,7 +168,8 @@ k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __rest
     for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e] + W::mont(x[e], y[e], p.q, p.neg_inv), p.twice_q);
   }
   InvEpilogue<T> epi = make_inv_epilogue<T>(out + comp * comp_stride + rest * G::kN, p, kInvStandard, true);
-  Ntt<T, LOGN>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v, epi);
+  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v,
+                                                epi);
 }
 
 // NTT-domain tensor product only (reference multiply): out [3, B, L, N] lazy.
@@ -279,11 +290,13 @@ struct KsTw {
       __syncthreads();
     }
   }
-  __device__ __forceinline__ void forward(T* data, const PrimeInfo<T>& p, T (&v)[G::kE]) const {
+  template <class Src>
+  __device__ __forceinline__ void forward_from(Src& src, T* data, const PrimeInfo<T>& p, T (&v)[G::kE]) const {
     if constexpr (kShared) {
-      Ntt<T, LOGN, TwShared<T, LOGN>>::forward(data, TwShared<T, LOGN>{gf, st, rank * G::kM}, p.q, p.twice_q, rank, v);
+      Ntt<T, LOGN, TwShared<T, LOGN>>::forward_from(src, data, TwShared<T, LOGN>{gf, st, rank * G::kM}, p.q,
+                                                    p.twice_q, rank, v);
     } else {
-      Ntt<T, LOGN>::forward(data, TwGlobal<T, LOGN>(gf), p.q, p.twice_q, rank, v);
+      Ntt<T, LOGN>::forward_from(src, data, TwGlobal<T, LOGN>(gf), p.q, p.twice_q, rank, v);
     }
   }
   template <class Epi>
@@ -337,6 +350,27 @@ struct KsAcc {
     const T* c = which ? c1 : c0;
 #pragma unroll
     for (int e = 0; e < G::kE; ++e) v[e] = c[e * stride];
+  }
+};
+
+// Exact basis extension of one hybrid digit to destination prime p, as the
+// source of the forward transform: sum_r d_r (M_r mod p), lazy [0, 2p).
+// dig: the digit's first mixed-radix row of this ciphertext; ext: the
+// extension constants of the digit for prime p (entry r at ext[r * qp0]).
+template <typename T>
+struct ExtSource {
+  const T* dig;
+  const TwPair<T>* ext;
+  int qp0, alpha, log_n;
+  T q, twice_q;
+  __device__ __forceinline__ T operator()(int pos) const {
+    T y = 0;
+    for (int r = 0; r < alpha; ++r) {
+      const TwPair<T> c = ext[int64_t(r) * qp0];
+      const T x = dig[(int64_t(r) << log_n) + pos];
+      y = csub(y + Word<T>::shoup(x, c.w, c.wp, q), twice_q);
+    }
+    return y;
   }
 };
 
@@ -410,7 +444,7 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
-  const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
+  const T* dig = digits + bi * q_limbs * int64_t(G::kN);
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
   if (item_keys) key = reinterpret_cast<const T*>(item_keys[bi]);  // mixed-key batch
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
@@ -418,19 +452,10 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   tw.stage(false);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
-    const TwPair<T>* ext = lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid;
-    __syncthreads();
-    for (int i = threadIdx.x; i < G::kM; i += G::kThreads) {
-      T y = 0;
-      for (int r = 0; r < d.alpha; ++r) {
-        const TwPair<T> c = ext[int64_t(r) * qp0];
-        const T x = dig[int64_t(d.prime0 - level + r) * G::kN + i];
-        y = csub(y + W::shoup(x, c.w, c.wp, p.q), p.twice_q);
-      }
-      s[G::sidx(i)] = y;
-    }
+    ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
+                     qp0, d.alpha, LOGN, p.q, p.twice_q};
     T v[G::kE];
-    tw.forward(s, p, v);
+    tw.forward_from(src, s, p, v);
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
     const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
     key_mac(acc, v, key0, key1, p);
@@ -463,25 +488,16 @@ k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
-  const T* dig = digits + bi * q_limbs * int64_t(G::kN) + int64_t(rank) * G::kM;
+  const T* dig = digits + bi * q_limbs * int64_t(G::kN);
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
-    const TwPair<T>* ext = lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid;
-    __syncthreads();
-    for (int i = threadIdx.x; i < G::kM; i += G::kThreads) {
-      T y = 0;
-      for (int r = 0; r < d.alpha; ++r) {
-        const TwPair<T> c = ext[int64_t(r) * qp0];
-        const T x = dig[int64_t(d.prime0 - level + r) * G::kN + i];
-        y = csub(y + W::shoup(x, c.w, c.wp, p.q), p.twice_q);
-      }
-      s[G::sidx(i)] = y;
-    }
+    ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
+                     qp0, d.alpha, LOGN, p.q, p.twice_q};
     T v[G::kE];
-    tw.forward(s, p, v);
+    tw.forward_from(src, s, p, v);
 #pragma unroll
     for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
     store16(prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN + own, v);

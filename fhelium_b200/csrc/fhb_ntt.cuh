@@ -14,15 +14,18 @@
 // [r*M, (r+1)*M), M = N / C, in its shared memory (padded every 2^PAD
 // elements so that strided accesses spread over all banks).
 //   * the first LOGC forward stages (half spans >= M) pair elements held by
-//     different CTAs: each CTA transforms 1/C of the columns through
-//     distributed shared memory (ld/st.shared::cluster);
+//     different CTAs: each CTA reads the C inputs of 1/C of the columns
+//     straight from their source (global memory), transforms them in
+//     registers and pushes the results into the owning CTAs' shared memory
+//     (st.shared::cluster);
 //   * the remaining LOGM stages are CTA-local, done in register passes of
-//     3 or 4 stages (radix-8/16 per thread, 16 residues per thread);
-//   * the last forward pass leaves every thread with 16 consecutive outputs
+//     3 or 4 stages (radix-8/16 per thread, E = 8 or 16 residues per thread);
+//   * the last forward pass leaves every thread with E consecutive outputs
 //     in registers, which the caller's epilogue consumes (store, or fused
 //     key multiply-accumulate).
-// The inverse mirrors this: the first pass starts from 16 consecutive
-// values per thread (from registers), the cross-CTA stages come last.
+// The inverse mirrors this: the first pass starts from E consecutive
+// values per thread (from registers), the cross-CTA stages come last and
+// read the other CTAs' blocks through distributed shared memory.
 // Forward butterflies keep Harvey's lazy range [0, 4q), inverse ones [0, 2q).
 #pragma once
 #include <cooperative_groups.h>
@@ -34,7 +37,8 @@ namespace cg = cooperative_groups;
 
 constexpr int clamp_int(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-template <typename T, int LOGN>
+// EPT = residues per thread (8 or 16; 0 = the default for the ring).
+template <typename T, int LOGN, int EPT = 0>
 struct NttGeom {
   static constexpr int kLogN = LOGN;
   static constexpr int kN = 1 << LOGN;
@@ -49,7 +53,9 @@ struct NttGeom {
   // threads): the kernels are latency bound and twice the resident warps
   // hide more of it (key-switch core 33.9 vs 43.4 ms at L=35, batch 32).
   // (16 when 8 would need more than 1024 threads: N = 2^17, M = 16384.)
-  static constexpr int kE = (kM / FHB_NTT_E > 1024) ? 16 : FHB_NTT_E;
+  static constexpr int kReqE = EPT ? EPT : FHB_NTT_E;
+  static_assert(kReqE == 8 || kReqE == 16, "8 or 16 residues per thread");
+  static constexpr int kE = (kM / kReqE > 1024) ? 16 : kReqE;
   static constexpr int kThreads = kM / kE;
   static constexpr int kPadShift = sizeof(T) == 8 ? 4 : 5;
   static constexpr int kSmemElems = kM + (kM >> kPadShift);
@@ -132,9 +138,9 @@ struct TwShared {
   }
 };
 
-template <typename T, int LOGN, class TW = TwGlobal<T, LOGN>>
+template <typename T, int LOGN, class TW = TwGlobal<T, LOGN>, int EPT = 0>
 struct Ntt {
-  using G = NttGeom<T, LOGN>;
+  using G = NttGeom<T, LOGN, EPT>;
   using W = Word<T>;
   static constexpr int E = G::kE;
 
@@ -161,27 +167,32 @@ struct Ntt {
   }
 
   // ---- forward -----------------------------------------------------------
-  __device__ __forceinline__ static void fwd_cross(T* s, const TW& tw, T q, T twoq, int rank) {
-    if constexpr (G::kC > 1) {
-      cg::cluster_group cl = cg::this_cluster();
-      constexpr int kCols = G::kM / G::kC;
+  // Cross-CTA stages straight from the source: CTA `rank` owns the columns
+  // m in [rank*M/C, (rank+1)*M/C) of the first log C stages; it reads the C
+  // inputs of each column from `src` (global memory), runs the stages in
+  // registers and pushes the results into the owning CTAs' shared memory
+  // (remote stores, which do not stall the issuing thread).
+  template <class Src>
+  __device__ __forceinline__ static void fwd_cross_push(Src& src, T* s, const TW& tw, T q, T twoq, int rank) {
+    cg::cluster_group cl = cg::this_cluster();
+    constexpr int kCols = G::kM / G::kC;
+    static_assert(kCols % G::kThreads == 0, "columns per CTA must be a multiple of the thread count");
 #pragma unroll
-      for (int u = 0; u < kCols / G::kThreads; ++u) {
-        const int m = rank * kCols + u * G::kThreads + tid();
-        const int sm = G::sidx(m);
-        T x[G::kC];
+    for (int u = 0; u < kCols / G::kThreads; ++u) {
+      const int m = rank * kCols + u * G::kThreads + tid();
+      const int sm = G::sidx(m);
+      T x[G::kC];
 #pragma unroll
-        for (int c = 0; c < G::kC; ++c) x[c] = *cl.map_shared_rank(s + sm, c);
+      for (int c = 0; c < G::kC; ++c) x[c] = src(c * G::kM + m);
 #pragma unroll
-        for (int st = 0; st < G::kLogC; ++st) {
-          const int h = G::kC >> (st + 1);
+      for (int st = 0; st < G::kLogC; ++st) {
+        const int h = G::kC >> (st + 1);
 #pragma unroll
-          for (int c = 0; c < G::kC; ++c)
-            if (!(c & h)) fwd_bfly(x[c], x[c + h], tw.fwd(st, c * G::kM), q, twoq);
-        }
-#pragma unroll
-        for (int c = 0; c < G::kC; ++c) *cl.map_shared_rank(s + sm, c) = x[c];
+        for (int c = 0; c < G::kC; ++c)
+          if (!(c & h)) fwd_bfly(x[c], x[c + h], tw.fwd(st, c * G::kM), q, twoq);
       }
+#pragma unroll
+      for (int c = 0; c < G::kC; ++c) *cl.map_shared_rank(s + sm, c) = x[c];
     }
   }
 
@@ -240,17 +251,23 @@ struct Ntt {
     }
   }
 
-  // Forward transform of the block already staged in s (values < 4q).
-  // On return out[e] holds the (lazy, < 4q) output at local position
-  // tid() * 16 + e of CTA `rank`.
-  __device__ __forceinline__ static void forward(T* s, const TW& tw, T q, T twoq, int rank,
-                                                 T (&out)[E]) {
+  // Forward transform of one polynomial whose input residues (< 4q) are
+  // produced on demand: src(pos) returns the input at position pos of the
+  // polynomial (0 <= pos < N).  On return out[e] holds the (lazy, < 4q)
+  // output at local position tid() * E + e of CTA `rank`.  Starts with a
+  // (cluster) barrier, so shared memory still being read by a previous
+  // transform of this CTA or cluster is never overwritten.
+  template <class Src>
+  __device__ __forceinline__ static void forward_from(Src& src, T* s, const TW& tw, T q, T twoq, int rank,
+                                                      T (&out)[E]) {
     if constexpr (G::kC > 1) {
       cg::cluster_group cl = cg::this_cluster();
       cl.sync();
-      fwd_cross(s, tw, q, twoq, rank);
+      fwd_cross_push(src, s, tw, q, twoq, rank);
       cl.sync();
     } else {
+      __syncthreads();
+      for (int i = tid(); i < G::kM; i += G::kThreads) s[G::sidx(i)] = src(i);
       __syncthreads();
     }
     fwd_local<0>(s, tw, q, twoq, rank, out);
@@ -311,6 +328,11 @@ struct Ntt {
     }
   }
 
+  // Cross-CTA inverse stages over the columns m in [rank*M/C, (rank+1)*M/C):
+  // the C elements of a column are read from the C CTAs' shared memory
+  // (ld.shared::cluster).  Pulling here measured faster than pushing them
+  // from the last local pass (one more register array live across a
+  // cluster barrier).
   template <class Epi>
   __device__ __forceinline__ static void inv_cross(T* s, const TW& tw, T q, T twoq, int rank,
                                                    Epi& epi) {
@@ -342,9 +364,10 @@ struct Ntt {
   }
 
   // Inverse transform of the values `in` (thread-contiguous layout, as left
-  // by `forward`, each < 2q).  Every output is handed to epi(position, v)
-  // with v in [0, 2q); s is scratch.  Ends with a cluster barrier so that
-  // shared memory may be reused (and so that peers never outlive reads).
+  // by `forward_from`, each < 2q).  Every output is handed to
+  // epi(position, v) with v in [0, 2q); s is scratch.  Ends with a cluster
+  // barrier so that shared memory may be reused (and so that peers never
+  // outlive reads).
   template <class Epi>
   __device__ __forceinline__ static void inverse(T* s, const TW& tw, T q, T twoq, int rank,
                                                  const T (&in)[E], Epi& epi) {

@@ -6,9 +6,9 @@
 
 namespace fhb {
 
-template <typename T, int LOGN, typename... KArgs, typename... Args>
+template <typename T, int LOGN, int EPT = 0, typename... KArgs, typename... Args>
 int launch_cluster(void (*kernel)(KArgs...), int64_t polys, size_t smem, cudaStream_t stream, Args... args) {
-  using G = NttGeom<T, LOGN>;
+  using G = NttGeom<T, LOGN, EPT>;
   if (polys <= 0) return 0;
   if (polys * G::kC > 0x7fffffffLL) return fail(-6, "too many polynomials for one launch");
   const int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kernel), int(smem));
@@ -34,19 +34,32 @@ constexpr size_t ntt_smem() {
 }
 
 // ---- per (T, LOGN) launchers --------------------------------------------
+// The standalone transforms exist with 8 and 16 residues per thread (radix-8
+// passes over 1024 threads or radix-16 passes over 512 for N = 2^16); the
+// context's tuning values pick one per direction (0 = the ring's default).
+template <typename T, int LOGN, int EPT>
+int run_forward_e(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool mont,
+                  cudaStream_t st) {
+  if (mont)
+    return launch_cluster<T, LOGN, EPT>(k_ntt_forward<T, LOGN, false, EPT>, polys, ntt_smem<T, LOGN>(), st,
+                                        (const T*)in, (T*)out, rows, row_start, tables<T>(c));
+  return launch_cluster<T, LOGN, EPT>(k_ntt_forward<T, LOGN, true, EPT>, polys, ntt_smem<T, LOGN>(), st,
+                                      (const T*)in, (T*)out, rows, row_start, tables<T>(c));
+}
+
 template <typename T, int LOGN>
 int run_forward(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start,
                 bool mont, cudaStream_t st) {
-  if (mont)
-    return launch_cluster<T, LOGN>(k_ntt_forward<T, LOGN, false>, polys, ntt_smem<T, LOGN>(), st,
-                                   (const T*)in, (T*)out, rows, row_start, tables<T>(c));
-  return launch_cluster<T, LOGN>(k_ntt_forward<T, LOGN, true>, polys, ntt_smem<T, LOGN>(), st, (const T*)in,
-                                 (T*)out, rows, row_start, tables<T>(c));
+  if (c.ntt_ept_fwd == 16) return run_forward_e<T, LOGN, 16>(c, in, out, polys, rows, row_start, mont, st);
+  return run_forward_e<T, LOGN, 0>(c, in, out, polys, rows, row_start, mont, st);
 }
 
 template <typename T, int LOGN>
 int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
                 cudaStream_t st) {
+  if (c.ntt_ept_inv == 16)
+    return launch_cluster<T, LOGN, 16>(k_ntt_inverse<T, LOGN, 16>, polys, ntt_smem<T, LOGN>(), st, (const T*)in,
+                                       (T*)out, rows, row_start, kind, tables<T>(c));
   return launch_cluster<T, LOGN>(k_ntt_inverse<T, LOGN>, polys, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out,
                                  rows, row_start, kind, tables<T>(c));
 }
@@ -55,6 +68,9 @@ template <typename T, int LOGN>
 int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
                  cudaStream_t st) {
   const int limbs = c.num_q - level;
+  if (c.ntt_ept_inv == 16)
+    return launch_cluster<T, LOGN, 16>(k_mul_to_coefficient<T, LOGN, 16>, 3 * batch * limbs, ntt_smem<T, LOGN>(),
+                                       st, (const T*)a, (const T*)b, (T*)out, batch, limbs, level, tables<T>(c));
   return launch_cluster<T, LOGN>(k_mul_to_coefficient<T, LOGN>, 3 * batch * limbs, ntt_smem<T, LOGN>(), st,
                                  (const T*)a, (const T*)b, (T*)out, batch, limbs, level, tables<T>(c));
 }

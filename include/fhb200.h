@@ -62,8 +62,12 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
 /* Launch tuning of a context (set by the autotuner, fhelium_b200/autotune.py).
  * FHB_TUNE_KS_ORDER: work order of the key-switch clusters, 0 = the rows of
  * one ciphertext back to back, 1 = one row across the batch back to back.
- * No counterpart in the reference (its launches have no tunable order). */
-enum fhb_tuning_param { FHB_TUNE_KS_ORDER = 0 };
+ * FHB_TUNE_NTT_FORWARD_EPT / FHB_TUNE_NTT_INVERSE_EPT: residues per thread of
+ * the standalone forward / inverse NTT (and of the fused HMult -> inverse
+ * NTT): 8 = radix-8 register passes, 16 = radix-16 passes over half the
+ * threads, 0 = the ring's default.  Results do not depend on any of these.
+ * No counterpart in the reference (its launch shapes are fixed). */
+enum fhb_tuning_param { FHB_TUNE_KS_ORDER = 0, FHB_TUNE_NTT_FORWARD_EPT = 1, FHB_TUNE_NTT_INVERSE_EPT = 2 };
 int fhb_context_set_tuning(fhb_context* ctx, int param, int value);
 int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);
 

@@ -45,7 +45,8 @@ def test_bootstrap_small_ring_complex_slots():
     # the refreshed ciphertext multiplies again
     sq = eng.multiply_relinearize_rescale(eng.coefficient_domain_to_ntt_domain(out),
                                           eng.coefficient_domain_to_ntt_domain(out))
-    assert float((eng.decrypt_message(sq) - m * m).abs().max()) < 2e-2
+    # |m| <= sqrt(2): the square's error is about 2|m| times the input's
+    assert float((eng.decrypt_message(sq) - m * m).abs().max()) < 4e-2
 
 
 def test_bootstrap_small_ring_reference_input():

@@ -10,6 +10,7 @@ equal modulo q.
 import numpy as np
 import pytest
 
+from fhelium_b200 import _native as nat
 from fhelium_b200.engine import CkksEngine
 from fhelium_b200.values import Ciphertext, RelinearizationKey, RotationKey
 from oracle import oracle as orc_mod
@@ -63,9 +64,11 @@ def test_relinearize_matches_oracle(family, log_n, level):
     np.testing.assert_array_equal(to_np(got.data), want)
 
 
+@pytest.mark.parametrize("ept", [0, 16])
 @pytest.mark.parametrize("family,log_n,level", CASES)
-def test_fused_multiply_relinearize_rescale_matches_oracle(family, log_n, level):
+def test_fused_multiply_relinearize_rescale_matches_oracle(family, log_n, level, ept):
     cfg, eng, orc, rng = _setup(family, log_n, level, 3)
+    eng.ctx.set_tuning(nat.TUNE_NTT_INVERSE_EPT, ept)  # inverse-NTT variant of the fused HMult
     if level + 1 >= cfg.num_q_primes:
         pytest.skip("no rescale at the last level")
     rows = orc.q_rows(level)

@@ -14,10 +14,14 @@ pytestmark = pytest.mark.gpu
 CASES = [("int64_logn16", k) for k in (12, 13, 14, 15, 16)] + [("int32_logn16", k) for k in (12, 14, 16)]
 
 
+@pytest.mark.parametrize("ept", [8, 16])
 @pytest.mark.parametrize("family,log_n", CASES)
-def test_forward_inverse_match_oracle(family, log_n):
+def test_forward_inverse_match_oracle(family, log_n, ept):
     cfg = reduced_ring(CONFIGS[family](), log_n)
     eng = CkksEngine(cfg)
+    # radix-8 (8 residues per thread) and radix-16 (16) launch variants
+    eng.ctx.set_tuning(nat.TUNE_NTT_FORWARD_EPT, ept)
+    eng.ctx.set_tuning(nat.TUNE_NTT_INVERSE_EPT, ept)
     orc = oracle_for(cfg, log_n)
     rng = np.random.default_rng(100 + log_n)
     rows = list(range(0, min(6, cfg.num_q_primes))) + list(range(cfg.num_q_primes, cfg.num_q_primes + cfg.num_p_primes))
