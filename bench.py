@@ -542,6 +542,8 @@ def main() -> int:
                      "algorithmic_bytes_per_launch": ks_bytes, "launch_ms": per_kernel["keyswitch_core"],
                      "note": "int64 Montgomery/Shoup arithmetic on CUDA cores: the kernel is integer-ALU bound"},
         "kernel_ms": per_kernel,
+        "kernel_ms_note": "each public entry point timed alone on the same inputs; the fused step runs the "
+                          "HMult->INTT for d2 only and folds d0, d1 into the key-switch accumulators",
         "step_algorithmic_gbs": step_bytes / (ms / 1000.0) / 1e9,
         "clocks": csum,
         "cpu_baseline": cpu,

@@ -151,15 +151,21 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
     for (int i = 0; i < k; ++i) pg[k * kMaxDigitWidth + i] = pair<T>(prefix_product_mod(pm, i, pm[k]), pm[k]);
     pg[k * kMaxDigitWidth + k] = pair<T>(invmod(prefix_product_mod(pm, k, pm[k]), pm[k]), pm[k]);
   }
-  std::vector<TwPair<T>> pmix(size_t(kMaxDigitWidth) * qp, TwPair<T>{0, 0}), pinv(qp, TwPair<T>{0, 0});
+  std::vector<TwPair<T>> pmix(size_t(kMaxDigitWidth) * qp, TwPair<T>{0, 0}), pinv(qp, TwPair<T>{0, 0}),
+      prinv(qp, TwPair<T>{0, 0});
   for (int pid = 0; pid < qp; ++pid) {
     const uint64_t m = c.moduli[pid];
     for (int k = 0; k < c.num_p; ++k) pmix[size_t(k) * qp + pid] = pair<T>(prefix_product_mod(pm, k, m), m);
-    if (pid < c.num_q) pinv[pid] = pair<T>(invmod(prefix_product_mod(pm, c.num_p, m), m), m);
+    if (pid < c.num_q) {
+      const uint64_t p_mod = prefix_product_mod(pm, c.num_p, m);
+      pinv[pid] = pair<T>(invmod(p_mod, m), m);
+      prinv[pid] = pair<T>(mulmod(p_mod, invmod(powmod(2, radix_bits, m), m), m), m);
+    }
   }
   t.p_garner = upload(c, pg);
   t.p_mix = upload(c, pmix);
   t.p_inv = upload(c, pinv);
+  t.p_rinv = upload(c, prinv);
 
   // ---- per level: hybrid digits, Garner and extension constants, rescale --
   std::vector<std::vector<int>> level0;
@@ -207,7 +213,7 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
     lt.rescale_inv = upload(c, rs);
     if (!lt.digits || !lt.garner || !lt.ext || !lt.rescale_inv) return false;
   }
-  return t.prime && t.tw_fwd && t.tw_inv && t.p_garner && t.p_mix && t.p_inv;
+  return t.prime && t.tw_fwd && t.tw_inv && t.p_garner && t.p_mix && t.p_inv && t.p_rinv;
 }
 
 }  // namespace

@@ -31,6 +31,10 @@ struct ChainTables {
   TwPair<T>* p_garner = nullptr;  // [8][8]
   TwPair<T>* p_mix = nullptr;     // [8][QP]
   TwPair<T>* p_inv = nullptr;     // [QP]
+  // P R^{-1} mod q for the Q primes: Shoup(x, .) of a Montgomery-form NTT
+  // value x = y R gives P y, the form in which an addend d enters the key-
+  // switch accumulators before ModDown ((t + P d - [t]_P) / P = (t - [t]_P) / P + d).
+  TwPair<T>* p_rinv = nullptr;    // [QP]
 };
 
 // Per-level key-switch / rescale tables (device).

@@ -133,21 +133,23 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
 
 // ---------------------------------------------------------------------------
 // Fused tensor product + inverse NTT (HMult feeding relinearisation).
-// a, b: [2, B, L, N] NTT/Montgomery lazy; out: [3, B, L, N] coefficient/standard
-// canonical = INTT of (a0 b0, a0 b1 + a1 b0, a1 b1)
-// (fhelium/engine/ckks_engine.py:1570-1606 then :1655-1660).
+// a, b: [2, B, L, N] NTT/Montgomery lazy; out: [3 - comp_first, B, L, N]
+// coefficient/standard canonical = INTT of components comp_first..2 of
+// (a0 b0, a0 b1 + a1 b0, a1 b1) (fhelium/engine/ckks_engine.py:1570-1606
+// then :1655-1660).  comp_first = 2 produces only d2, the component the key
+// switch decomposes.
 template <typename T, int LOGN, int EPT = 0>
 __global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
-                     int64_t batch, int limbs, int level, ChainTables<T> tabs) {
+                     int64_t batch, int limbs, int level, int comp_first, ChainTables<T> tabs) {
   using G = NttGeom<T, LOGN, EPT>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;  // over [3, B, L]
+  const int64_t poly = blockIdx.x / G::kC;  // over [3 - comp_first, B, L]
   const int64_t comp_stride = batch * limbs * G::kN;
-  const int comp = int(poly / (batch * limbs));
+  const int comp = comp_first + int(poly / (batch * limbs));
   const int64_t rest = poly % (batch * limbs);
   const int pid = level + int(rest % limbs);
   const PrimeInfo<T> p = tabs.prime[pid];
@@ -167,7 +169,8 @@ k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __rest
 #pragma unroll
     for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e] + W::mont(x[e], y[e], p.q, p.neg_inv), p.twice_q);
   }
-  InvEpilogue<T> epi = make_inv_epilogue<T>(out + comp * comp_stride + rest * G::kN, p, kInvStandard, true);
+  InvEpilogue<T> epi =
+      make_inv_epilogue<T>(out + (comp - comp_first) * comp_stride + rest * G::kN, p, kInvStandard, true);
   Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v,
                                                 epi);
 }
@@ -417,6 +420,33 @@ __device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[E], const T* key0
   }
 }
 
+// Addends folded into the key-switch accumulators of a Q row before their
+// inverse NTT (so that ModDown returns KS(d2) + d directly): acc += P d,
+// with d in NTT/Montgomery form (d R) and P R^{-1} as Shoup constant.
+//   mode 1 (relinearisation): d_k = c_k of the NTT-domain ct3;
+//   mode 2 (HMult): d_0 = a0 b0, d_1 = a0 b1 + a1 b0 from the operands.
+// a, b point at this thread's first element of component 0; comp_stride
+// is the distance to component 1.
+enum KsAddMode : int { kAddNone = 0, kAddCt3 = 1, kAddProduct = 2 };
+
+template <typename T, int E>
+__device__ __forceinline__ void ks_add_p_scaled(T (&v)[E], int which, int mode, const T* a, const T* b,
+                                                int64_t comp_stride, const PrimeInfo<T>& p, TwPair<T> ps) {
+  using W = Word<T>;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    T d;
+    if (mode == kAddCt3) {
+      d = a[which * comp_stride + e];
+    } else if (which == 0) {
+      d = W::mont(a[e], b[e], p.q, p.neg_inv);
+    } else {
+      d = W::mont(a[e], b[comp_stride + e], p.q, p.neg_inv) + W::mont(a[comp_stride + e], b[e], p.q, p.neg_inv);
+    }
+    v[e] = csub(v[e] + W::shoup(d, ps.w, ps.wp, p.q), p.twice_q);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Fused ModUp stage 2 + forward NTT + key inner product + inverse NTT.
 // One cluster per (ciphertext b, destination row j of Q_l P).  For every
@@ -432,7 +462,8 @@ template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
                  T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
-                 const unsigned long long* __restrict__ item_keys, ChainTables<T> tabs, LevelTables<T> lt) {
+                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ add_a,
+                 const T* __restrict__ add_b, int add_mode, ChainTables<T> tabs, LevelTables<T> lt) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -461,11 +492,16 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
     key_mac(acc, v, key0, key1, p);
   }
   tw.stage(true);
+  const bool add = add_mode != kAddNone && jrow < q_limbs;
+  const int64_t add_off = (bi * q_limbs + jrow) * int64_t(G::kN) + own;
+  const int64_t add_stride = batch * q_limbs * int64_t(G::kN);
   T v[G::kE];
   acc.get(0, v);
+  if (add) ks_add_p_scaled(v, 0, add_mode, add_a + add_off, add_b + add_off, add_stride, p, tabs.p_rinv[pid]);
   InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e0);
   acc.get(1, v);
+  if (add) ks_add_p_scaled(v, 1, add_mode, add_a + add_off, add_b + add_off, add_stride, p, tabs.p_rinv[pid]);
   InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e1);
 }

@@ -14,10 +14,11 @@ int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int 
                 cudaStream_t st);
 template <typename T, int LOGN>
 int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
-                 cudaStream_t st);
+                 int comp_first, cudaStream_t st);
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st, const uint64_t* item_keys);
+                int level, cudaStream_t st, const uint64_t* item_keys, const void* add_a, const void* add_b,
+                int add_mode);
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
 template <typename T, int LOGN>
