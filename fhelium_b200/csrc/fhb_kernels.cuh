@@ -60,10 +60,14 @@ template <typename T, bool TO_MONT>
 struct RowSource {
   const T* in;
   T c, cs, q;
-  __device__ __forceinline__ T operator()(int pos) const {
-    T v = in[pos];
-    if constexpr (TO_MONT) v = Word<T>::shoup(v, c, cs, q);
-    return v;
+  template <int C>
+  __device__ __forceinline__ void column(int m, int stride, T (&x)[C]) const {
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+      T v = in[k * stride + m];
+      if constexpr (TO_MONT) v = Word<T>::shoup(v, c, cs, q);
+      x[k] = v;
+    }
   }
 };
 
@@ -366,14 +370,18 @@ struct ExtSource {
   const TwPair<T>* ext;
   int qp0, alpha, log_n;
   T q, twice_q;
-  __device__ __forceinline__ T operator()(int pos) const {
-    T y = 0;
+  // x[k] = extension of the digit at position k * stride + m; the digit's
+  // rows are the outer loop so each constant is loaded once per column.
+  template <int C>
+  __device__ __forceinline__ void column(int m, int stride, T (&x)[C]) const {
+#pragma unroll
+    for (int k = 0; k < C; ++k) x[k] = 0;
     for (int r = 0; r < alpha; ++r) {
       const TwPair<T> c = ext[int64_t(r) * qp0];
-      const T x = dig[(int64_t(r) << log_n) + pos];
-      y = csub(y + Word<T>::shoup(x, c.w, c.wp, q), twice_q);
+      const T* row = dig + (int64_t(r) << log_n) + m;
+#pragma unroll
+      for (int k = 0; k < C; ++k) x[k] = csub(x[k] + Word<T>::shoup(row[k * stride], c.w, c.wp, q), twice_q);
     }
-    return y;
   }
 };
 
@@ -447,6 +455,22 @@ __device__ __forceinline__ void ks_add_p_scaled(T (&v)[E], int which, int mode, 
   }
 }
 
+// For a Q row that belongs to the digit being processed, the exact extension
+// of the digit is d2 itself (modulo that row's prime), so its forward NTT is
+// d2's NTT-domain residue, which the caller already has: c2 of ct3 (mode 1)
+// or a1 b1 (mode 2).  v receives it in standard form, [0, 2q).
+template <typename T, int E>
+__device__ __forceinline__ void ks_own_digit_ntt(T (&v)[E], int mode, const T* a, const T* b, int64_t comp_stride,
+                                                 const PrimeInfo<T>& p) {
+  using W = Word<T>;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const T x = mode == kAddCt3 ? a[2 * comp_stride + e]
+                                : W::mont(a[comp_stride + e], b[comp_stride + e], p.q, p.neg_inv);
+    v[e] = W::shoup(x, p.rinv, p.rinv_s, p.q);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Fused ModUp stage 2 + forward NTT + key inner product + inverse NTT.
 // One cluster per (ciphertext b, destination row j of Q_l P).  For every
@@ -481,20 +505,25 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
+  const bool add = add_mode != kAddNone && jrow < q_limbs;
+  const int64_t add_off = (bi * q_limbs + jrow) * int64_t(G::kN) + own;
+  const int64_t add_stride = batch * q_limbs * int64_t(G::kN);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
-    ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
-                     qp0, d.alpha, LOGN, p.q, p.twice_q};
     T v[G::kE];
-    tw.forward_from(src, s, p, v);
+    if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
+      // uniform over the cluster: skipping the transform skips its barriers everywhere
+      ks_own_digit_ntt(v, add_mode, add_a + add_off, add_b + add_off, add_stride, p);
+    } else {
+      ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
+                       qp0, d.alpha, LOGN, p.q, p.twice_q};
+      tw.forward_from(src, s, p, v);
+    }
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
     const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
     key_mac(acc, v, key0, key1, p);
   }
   tw.stage(true);
-  const bool add = add_mode != kAddNone && jrow < q_limbs;
-  const int64_t add_off = (bi * q_limbs + jrow) * int64_t(G::kN) + own;
-  const int64_t add_stride = batch * q_limbs * int64_t(G::kN);
   T v[G::kE];
   acc.get(0, v);
   if (add) ks_add_p_scaled(v, 0, add_mode, add_a + add_off, add_b + add_off, add_stride, p, tabs.p_rinv[pid]);

@@ -182,8 +182,7 @@ struct Ntt {
       const int m = rank * kCols + u * G::kThreads + tid();
       const int sm = G::sidx(m);
       T x[G::kC];
-#pragma unroll
-      for (int c = 0; c < G::kC; ++c) x[c] = src(c * G::kM + m);
+      src.column(m, G::kM, x);
 #pragma unroll
       for (int st = 0; st < G::kLogC; ++st) {
         const int h = G::kC >> (st + 1);
@@ -252,8 +251,8 @@ struct Ntt {
   }
 
   // Forward transform of one polynomial whose input residues (< 4q) are
-  // produced on demand: src(pos) returns the input at position pos of the
-  // polynomial (0 <= pos < N).  On return out[e] holds the (lazy, < 4q)
+  // produced on demand: src.column(m, stride, x) fills x[c] with the input
+  // at position c * stride + m of the polynomial (0 <= position < N).  On return out[e] holds the (lazy, < 4q)
   // output at local position tid() * E + e of CTA `rank`.  Starts with a
   // (cluster) barrier, so shared memory still being read by a previous
   // transform of this CTA or cluster is never overwritten.
@@ -267,7 +266,11 @@ struct Ntt {
       cl.sync();
     } else {
       __syncthreads();
-      for (int i = tid(); i < G::kM; i += G::kThreads) s[G::sidx(i)] = src(i);
+      for (int i = tid(); i < G::kM; i += G::kThreads) {
+        T x[1];
+        src.column(i, 0, x);
+        s[G::sidx(i)] = x[0];
+      }
       __syncthreads();
     }
     fwd_local<0>(s, tw, q, twoq, rank, out);
