@@ -252,6 +252,37 @@ def bootstrap_leg(dev, stream, batch=8, steps=2):
     return out
 
 
+def ops_leg(dev, stream, batch=2, steps=3):
+    """Every evaluation op of the path once per step at logN=16, L=35 on
+    `batch` ciphertexts (a small case for per-kernel profiles): fused
+    HMult+relin+rescale, relinearize of an NTT-domain product, rescale,
+    rotation by one step, 4 hoisted rotations, forward and inverse NTT of a
+    ciphertext.  Returns per-op CUDA-event milliseconds."""
+    from fhelium_b200.engine import CkksEngine
+    eng = CkksEngine(PRESET, device=dev, rng_seed=11)
+    x = _messages(batch, eng.num_slots, 5)
+    ct = eng.encrypt_message(x)
+    ca = eng.coefficient_domain_to_ntt_domain(ct)
+    steps4 = [1, 2, 3, 4]
+    eng.generate_rotation_keys(steps4)
+    ct3 = eng.multiply(ca, ca)
+    ops = {
+        "multiply_relinearize_rescale": lambda: eng.multiply_relinearize_rescale(ca, ca),
+        "relinearize": lambda: eng.relinearize(ct3),
+        "rescale": lambda: eng.rescale_to_next_level(ct),
+        "rotate": lambda: eng.rotate_by_step(ct, 1),
+        "hoisted_rotations_4": lambda: eng.rotate_many_by_steps(ct, steps4),
+        "forward_ntt": lambda: eng.coefficient_domain_to_ntt_domain(ct),
+        "inverse_ntt": lambda: eng.ntt_domain_to_coefficient_domain(ca),
+    }
+    out = {}
+    for name, fn in ops.items():
+        fn()
+        torch.cuda.synchronize(dev)
+        out[name + "_ms"] = _time_events(fn, max(1, steps), stream)
+    return {"batch": batch, **out}
+
+
 def mixed_batch_leg(dev, stream, count=512, steps=3):
     """Mixed-level batch at slots32768_scale40_levels34_int64: `count`
     ciphertexts with limb counts uniform in 3..35 (uniform [-0.05, 0.05]
@@ -370,7 +401,7 @@ def main() -> int:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-extras", action="store_true", help="skip rotation/parity/CPU legs")
     ap.add_argument("--mixed-count", type=int, default=512, help="ciphertexts of the mixed-level leg (0: skip)")
-    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed"], default=None,
+    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed", "ops"], default=None,
                     help="run only this side leg on one GPU and print its result (profiling aid)")
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -384,6 +415,8 @@ def main() -> int:
             res = ntt_leg(dev, stream, args.steps)
         elif args.leg == "bootstrap":
             res = bootstrap_leg(dev, stream, steps=max(1, args.steps))
+        elif args.leg == "ops":
+            res = ops_leg(dev, stream, batch=args.batch, steps=args.steps)
         else:
             res = mixed_batch_leg(dev, stream, args.mixed_count, args.steps)
         print(json.dumps({"leg": args.leg, **res}), flush=True)

@@ -510,6 +510,8 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   const int64_t add_stride = batch * q_limbs * int64_t(G::kN);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
+    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
+    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
     T v[G::kE];
     if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
       // uniform over the cluster: skipping the transform skips its barriers everywhere
@@ -519,8 +521,6 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
                        qp0, d.alpha, LOGN, p.q, p.twice_q};
       tw.forward_from(src, s, p, v);
     }
-    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
-    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
     key_mac(acc, v, key0, key1, p);
   }
   tw.stage(true);
