@@ -93,14 +93,13 @@ int inverse(const Context& c, const void* in, void* out, int64_t polys, int rows
             cudaStream_t st) {
   FHB_DISPATCH(run_inverse, c, in, out, polys, rows, row_start, kind, st);
 }
-int mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level, int comp_first,
+int mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
              cudaStream_t st) {
-  FHB_DISPATCH(run_mul_coef, c, a, b, out, batch, level, comp_first, st);
+  FHB_DISPATCH(run_mul_coef, c, a, b, out, batch, level, st);
 }
 int ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-            int level, cudaStream_t st, const uint64_t* item_keys = nullptr, const void* add_a = nullptr,
-            const void* add_b = nullptr, int add_mode = kAddNone) {
-  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys, add_a, add_b, add_mode);
+            int level, cudaStream_t st, const uint64_t* item_keys = nullptr, const void* ct3 = nullptr) {
+  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys, ct3);
 }
 int prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st) {
   FHB_DISPATCH(run_prepare, c, digits, prepared, batch, level, st);
@@ -350,7 +349,7 @@ int fhb_ckks_multiply_to_coefficient(const fhb_context* ctx, const void* a, cons
   TRY(fhb::check_ptr(b, "b"));
   TRY(fhb::check_ptr(out, "out"));
   TRY(fhb::check_level(c, level));
-  return fhb::mul_coef(c, a, b, out, batch, level, 0, st);
+  return fhb::mul_coef(c, a, b, out, batch, level, st);
 }
 
 int fhb_ckks_modup_digits(const fhb_context* ctx, const void* comp, void* digits, int64_t batch, int level,
@@ -504,13 +503,13 @@ static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* k
   return FHB_WORD(fhb::moddown, c, s.t0, s.t1, add0, add1, out, batch, level, add0_galois, rescale, st);
 }
 
-// Key switch of d2 whose addends (d0, d1) are NTT-domain values folded into
-// the accumulators as P d before ModDown (relinearisation: add_mode 1 with
-// a = ct3; HMult: add_mode 2 with the operands a, b).
-static int keyswitch_tail_ntt_add(const Context& c, const fhb::Scratch& s, const void* key, const void* a,
-                                  const void* b, int add_mode, void* out, int64_t batch, int level, int rescale,
-                                  cudaStream_t st) {
-  TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st, nullptr, a, b, add_mode));
+// Relinearisation of an NTT-domain ct3 (coefficient-domain c2 already in
+// s.t0): ModUp of c2, the key-switch core with c0, c1 folded in as P c_k
+// (NTT domain) and c2's own-digit rows reused, ModDown (+ rescale).
+static int relinearize_tail(const Context& c, const fhb::Scratch& s, const void* key, const void* ct3, void* out,
+                            int64_t batch, int level, int rescale, cudaStream_t st) {
+  TRY(FHB_WORD(fhb::modup, c, s.t0, s.digits, batch, level, 1u, st));
+  TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st, nullptr, ct3));
   return FHB_WORD(fhb::moddown, c, s.t0, s.t1, nullptr, nullptr, out, batch, level, 1u, rescale, st);
 }
 
@@ -527,10 +526,9 @@ int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* ke
   const int limbs = c.num_q - level;
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
-  TRY(fhb::inverse(c, static_cast<const char*>(ct3) + 2 * comp, s.coef, batch * limbs, limbs, level,
+  TRY(fhb::inverse(c, static_cast<const char*>(ct3) + 2 * comp, s.t0, batch * limbs, limbs, level,
                    fhb::kInvStandard, st));
-  TRY(FHB_WORD(fhb::modup, c, s.coef, s.digits, batch, level, 1u, st));
-  return keyswitch_tail_ntt_add(c, s, key, ct3, nullptr, fhb::kAddCt3, out, batch, level, rescale, st);
+  return relinearize_tail(c, s, key, ct3, out, batch, level, rescale, st);
 }
 
 int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const void* b, const void* key, void* out,
@@ -547,10 +545,12 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
   const int limbs = c.num_q - level;
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
-  (void)limbs;
-  TRY(fhb::mul_coef(c, a, b, s.coef, batch, level, 2, st));
-  TRY(FHB_WORD(fhb::modup, c, s.coef, s.digits, batch, level, 1u, st));
-  return keyswitch_tail_ntt_add(c, s, key, a, b, fhb::kAddProduct, out, batch, level, rescale, st);
+  const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
+  // ct3 = a x b into the scratch (elementwise, every SM), then the
+  // relinearisation of an NTT-domain ct3
+  TRY(FHB_WORD(fhb::mul_ntt, c, a, b, s.coef, batch, level, st));
+  TRY(fhb::inverse(c, s.coef + 2 * comp, s.t0, batch * limbs, limbs, level, fhb::kInvStandard, st));
+  return relinearize_tail(c, s, key, s.coef, out, batch, level, rescale, st);
 }
 
 int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t* key_ptrs, const uint32_t* galois,

@@ -136,24 +136,22 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
 }
 
 // ---------------------------------------------------------------------------
-// Fused tensor product + inverse NTT (HMult feeding relinearisation).
-// a, b: [2, B, L, N] NTT/Montgomery lazy; out: [3 - comp_first, B, L, N]
-// coefficient/standard canonical = INTT of components comp_first..2 of
-// (a0 b0, a0 b1 + a1 b0, a1 b1) (fhelium/engine/ckks_engine.py:1570-1606
-// then :1655-1660).  comp_first = 2 produces only d2, the component the key
-// switch decomposes.
+// Fused tensor product + inverse NTT.
+// a, b: [2, B, L, N] NTT/Montgomery lazy; out: [3, B, L, N] coefficient/standard
+// canonical = INTT of (a0 b0, a0 b1 + a1 b0, a1 b1)
+// (fhelium/engine/ckks_engine.py:1570-1606 then :1655-1660).
 template <typename T, int LOGN, int EPT = 0>
 __global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
-                     int64_t batch, int limbs, int level, int comp_first, ChainTables<T> tabs) {
+                     int64_t batch, int limbs, int level, ChainTables<T> tabs) {
   using G = NttGeom<T, LOGN, EPT>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;  // over [3 - comp_first, B, L]
+  const int64_t poly = blockIdx.x / G::kC;  // over [3, B, L]
   const int64_t comp_stride = batch * limbs * G::kN;
-  const int comp = comp_first + int(poly / (batch * limbs));
+  const int comp = int(poly / (batch * limbs));
   const int64_t rest = poly % (batch * limbs);
   const int pid = level + int(rest % limbs);
   const PrimeInfo<T> p = tabs.prime[pid];
@@ -173,8 +171,7 @@ k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __rest
 #pragma unroll
     for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e] + W::mont(x[e], y[e], p.q, p.neg_inv), p.twice_q);
   }
-  InvEpilogue<T> epi =
-      make_inv_epilogue<T>(out + (comp - comp_first) * comp_stride + rest * G::kN, p, kInvStandard, true);
+  InvEpilogue<T> epi = make_inv_epilogue<T>(out + comp * comp_stride + rest * G::kN, p, kInvStandard, true);
   Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v,
                                                 epi);
 }
@@ -428,47 +425,28 @@ __device__ __forceinline__ void key_mac(Acc& acc, const T (&v)[E], const T* key0
   }
 }
 
-// Addends folded into the key-switch accumulators of a Q row before their
-// inverse NTT (so that ModDown returns KS(d2) + d directly): acc += P d,
-// with d in NTT/Montgomery form (d R) and P R^{-1} as Shoup constant.
-//   mode 1 (relinearisation): d_k = c_k of the NTT-domain ct3;
-//   mode 2 (HMult): d_0 = a0 b0, d_1 = a0 b1 + a1 b0 from the operands.
-// a, b point at this thread's first element of component 0; comp_stride
-// is the distance to component 1.
-enum KsAddMode : int { kAddNone = 0, kAddCt3 = 1, kAddProduct = 2 };
-
+// Relinearisation of an NTT-domain ct3 = (c0, c1, c2): for a Q row the
+// addends c0, c1 are folded into the key-switch accumulators before their
+// inverse NTT, as P c_k, so that ModDown returns KS(c2) + c_k directly
+// ((t + P c - [t]_P) / P = (t - [t]_P) / P + c).  c_k is in Montgomery form
+// (c R) and P R^{-1} mod q is the Shoup constant.  ct3 points at this
+// thread's first element of component 0; comp_stride is the component pitch.
 template <typename T, int E>
-__device__ __forceinline__ void ks_add_p_scaled(T (&v)[E], int which, int mode, const T* a, const T* b,
-                                                int64_t comp_stride, const PrimeInfo<T>& p, TwPair<T> ps) {
+__device__ __forceinline__ void ks_add_p_scaled(T (&v)[E], int which, const T* ct3, int64_t comp_stride,
+                                                const PrimeInfo<T>& p, TwPair<T> ps) {
   using W = Word<T>;
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    T d;
-    if (mode == kAddCt3) {
-      d = a[which * comp_stride + e];
-    } else if (which == 0) {
-      d = W::mont(a[e], b[e], p.q, p.neg_inv);
-    } else {
-      d = W::mont(a[e], b[comp_stride + e], p.q, p.neg_inv) + W::mont(a[comp_stride + e], b[e], p.q, p.neg_inv);
-    }
-    v[e] = csub(v[e] + W::shoup(d, ps.w, ps.wp, p.q), p.twice_q);
-  }
+  for (int e = 0; e < E; ++e) v[e] = csub(v[e] + W::shoup(ct3[which * comp_stride + e], ps.w, ps.wp, p.q), p.twice_q);
 }
 
 // For a Q row that belongs to the digit being processed, the exact extension
-// of the digit is d2 itself (modulo that row's prime), so its forward NTT is
-// d2's NTT-domain residue, which the caller already has: c2 of ct3 (mode 1)
-// or a1 b1 (mode 2).  v receives it in standard form, [0, 2q).
+// of the digit is c2 itself (modulo that row's prime), so its forward NTT is
+// c2's NTT-domain residue: v = c2 R * R^{-1}, standard form, [0, 2q).
 template <typename T, int E>
-__device__ __forceinline__ void ks_own_digit_ntt(T (&v)[E], int mode, const T* a, const T* b, int64_t comp_stride,
+__device__ __forceinline__ void ks_own_digit_ntt(T (&v)[E], const T* ct3, int64_t comp_stride,
                                                  const PrimeInfo<T>& p) {
-  using W = Word<T>;
 #pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const T x = mode == kAddCt3 ? a[2 * comp_stride + e]
-                                : W::mont(a[comp_stride + e], b[comp_stride + e], p.q, p.neg_inv);
-    v[e] = W::shoup(x, p.rinv, p.rinv_s, p.q);
-  }
+  for (int e = 0; e < E; ++e) v[e] = Word<T>::shoup(ct3[2 * comp_stride + e], p.rinv, p.rinv_s, p.q);
 }
 
 // ---------------------------------------------------------------------------
@@ -486,8 +464,8 @@ template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
                  T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
-                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ add_a,
-                 const T* __restrict__ add_b, int add_mode, ChainTables<T> tabs, LevelTables<T> lt) {
+                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ ct3,
+                 ChainTables<T> tabs, LevelTables<T> lt) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -505,9 +483,9 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
-  const bool add = add_mode != kAddNone && jrow < q_limbs;
-  const int64_t add_off = (bi * q_limbs + jrow) * int64_t(G::kN) + own;
-  const int64_t add_stride = batch * q_limbs * int64_t(G::kN);
+  const bool add = ct3 != nullptr && jrow < q_limbs;
+  const T* ct3_own = add ? ct3 + (bi * q_limbs + jrow) * int64_t(G::kN) + own : nullptr;
+  const int64_t ct3_stride = batch * q_limbs * int64_t(G::kN);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
@@ -515,7 +493,7 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
     T v[G::kE];
     if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
       // uniform over the cluster: skipping the transform skips its barriers everywhere
-      ks_own_digit_ntt(v, add_mode, add_a + add_off, add_b + add_off, add_stride, p);
+      ks_own_digit_ntt(v, ct3_own, ct3_stride, p);
     } else {
       ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
                        qp0, d.alpha, LOGN, p.q, p.twice_q};
@@ -526,11 +504,11 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   tw.stage(true);
   T v[G::kE];
   acc.get(0, v);
-  if (add) ks_add_p_scaled(v, 0, add_mode, add_a + add_off, add_b + add_off, add_stride, p, tabs.p_rinv[pid]);
+  if (add) ks_add_p_scaled(v, 0, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
   InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e0);
   acc.get(1, v);
-  if (add) ks_add_p_scaled(v, 1, add_mode, add_a + add_off, add_b + add_off, add_stride, p, tabs.p_rinv[pid]);
+  if (add) ks_add_p_scaled(v, 1, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
   InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e1);
 }

@@ -66,26 +66,24 @@ int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int 
 
 template <typename T, int LOGN>
 int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
-                 int comp_first, cudaStream_t st) {
+                 cudaStream_t st) {
   const int limbs = c.num_q - level;
-  const int64_t polys = (3 - comp_first) * batch * limbs;
+  const int64_t polys = 3 * batch * limbs;
   if (c.ntt_ept_inv == 16)
     return launch_cluster<T, LOGN, 16>(k_mul_to_coefficient<T, LOGN, 16>, polys, ntt_smem<T, LOGN>(), st,
-                                       (const T*)a, (const T*)b, (T*)out, batch, limbs, level, comp_first,
-                                       tables<T>(c));
+                                       (const T*)a, (const T*)b, (T*)out, batch, limbs, level, tables<T>(c));
   return launch_cluster<T, LOGN>(k_mul_to_coefficient<T, LOGN>, polys, ntt_smem<T, LOGN>(), st, (const T*)a,
-                                 (const T*)b, (T*)out, batch, limbs, level, comp_first, tables<T>(c));
+                                 (const T*)b, (T*)out, batch, limbs, level, tables<T>(c));
 }
 
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st, const uint64_t* item_keys, const void* add_a, const void* add_b,
-                int add_mode) {
+                int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
   return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
                                  (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(),
-                                 c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys), (const T*)add_a,
-                                 (const T*)add_b, add_mode, tables<T>(c), level_tables<T>(c, level));
+                                 c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys), (const T*)ct3,
+                                 tables<T>(c), level_tables<T>(c, level));
 }
 
 template <typename T, int LOGN>
@@ -110,10 +108,9 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
 #define FHB_INSTANTIATE_RUNNERS(T, LOGN)                                                                       \
   template int run_forward<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, bool, cudaStream_t);   \
   template int run_inverse<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, int, cudaStream_t);    \
-  template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, int,       \
-                                     cudaStream_t);                                                            \
+  template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, cudaStream_t); \
   template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
-                                    cudaStream_t, const uint64_t*, const void*, const void*, int);              \
+                                    cudaStream_t, const uint64_t*, const void*);                                \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);

@@ -14,11 +14,10 @@ int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int 
                 cudaStream_t st);
 template <typename T, int LOGN>
 int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
-                 int comp_first, cudaStream_t st);
+                 cudaStream_t st);
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st, const uint64_t* item_keys, const void* add_a, const void* add_b,
-                int add_mode);
+                int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3);
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
 template <typename T, int LOGN>
