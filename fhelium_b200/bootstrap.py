@@ -30,7 +30,8 @@ so every transform stage keeps the ciphertext scale exactly.
 
 Modular reduction: x = u / B' with u = t / q_b (t the raised coefficient),
 z0 ~ cos(2 pi (B' x - 1/4) / 2^R) by Chebyshev interpolation of degree 44 on
-[-1, 1], then R double-angle steps z <- 2 z^2 - 1 give sin(2 pi u); the factor
+[-1, 1] (evaluated by Paterson-Stockmeyer in the Chebyshev basis), then R
+double-angle steps z <- 2 z^2 - 1 give sin(2 pi u); the factor
 q_b / (2 pi Delta) returning to message units is folded into SlotsToCoeffs.
 All ciphertext products are relinearised and rescaled with their actual
 scales tracked; terms are aligned to a common level and scale by integer
@@ -172,7 +173,7 @@ class FullSlotBootstrap:
 
     def __init__(self, engine: CkksEngine, *, input_bound: int = 1024, double_angle_iterations: int = 7,
                  chebyshev_degree: int = 44, baby_step: int = 16, split: int = 7,
-                 modulus_raise_target_level: int = 0):
+                 modulus_raise_target_level: int = 0, ps_baby: int = 8):
         if engine.galois_generator != 5:
             raise ValueError("full-slot bootstrapping uses the generator-5 slot order")
         self.engine = engine
@@ -203,7 +204,8 @@ class FullSlotBootstrap:
         phase = 2 ** self.R
         self.seed = chebyshev_coefficients(
             lambda x: np.cos(2.0 * np.pi * (self.bound * x - 0.25) / phase), self.degree)
-        self.cheb_depth = math.ceil(math.log2(self.degree))
+        self.ps_baby = ps_baby
+        self.cheb_depth = self._ps_depth()
         self.levels = self._level_schedule()
         self._pt_cache: dict = {}
 
@@ -212,7 +214,7 @@ class FullSlotBootstrap:
         l0 = self.target
         cts = [l0, l0 + 1]
         evalmod_in = l0 + 2
-        evalmod_out = evalmod_in + self.cheb_depth + 1 + self.R
+        evalmod_out = evalmod_in + self.cheb_depth + self.R
         stc = [evalmod_out, evalmod_out + 1]
         return {"cts": cts, "evalmod_in": evalmod_in, "evalmod_out": evalmod_out, "stc": stc,
                 "output": evalmod_out + 2}
@@ -309,10 +311,75 @@ class FullSlotBootstrap:
         out = eng.rescale_to_next_level(out)
         return eng.reinterpret_at_scale(out, scale)
 
+    # -- Chebyshev series by Paterson-Stockmeyer -------------------------------
+    # p = sum_k c_k T_k is split as p = q T_g + r with T_g the largest giant
+    # (g = m 2^i <= deg p, baby bound m) using T_j T_g = (T_(j+g) + T_|g-j|) / 2,
+    # recursively, down to leaves of degree < m evaluated from the babies
+    # T_1..T_m by scalar products.  Non-scalar products: m - 1 babies, the
+    # giants, and one per inner node (15 for degree 44, m = 8, against 43 for
+    # the whole basis T_1..T_44); the multiplicative depth is the same.
+    @staticmethod
+    def _cheb_split(c: np.ndarray, g: int) -> tuple[np.ndarray, np.ndarray]:
+        deg = len(c) - 1
+        q = np.zeros(deg - g + 1)
+        r = c[:g].astype(np.float64).copy()
+        q[0] = c[g]
+        for j in range(1, deg - g + 1):
+            q[j] = 2.0 * c[g + j]
+            r[g - j] -= c[g + j]
+        return q, r
+
+    @staticmethod
+    def _trim(c: np.ndarray) -> np.ndarray:
+        scale = max(float(np.max(np.abs(c))), 1e-300)
+        k = len(c)
+        while k > 1 and abs(c[k - 1]) < 1e-15 * scale:
+            k -= 1
+        return c[:k]
+
+    def _baby_levels(self) -> dict[int, int]:
+        lv = {1: 0}
+        for k in range(2, self.ps_baby + 1):
+            a = 1 << (math.ceil(math.log2(k)) - 1)
+            lv[k] = max(lv[a], lv[k - a]) + 1
+        return lv
+
+    def _giants(self) -> list[int]:
+        g, out = self.ps_baby, []
+        while g <= self.degree:
+            out.append(g)
+            g *= 2
+        return out
+
+    def _ps_depth(self) -> int:
+        """Levels consumed by the Chebyshev evaluation (symbolic dry run of
+        _ps_eval's level arithmetic)."""
+        lv = self._baby_levels()
+        for g in self._giants():
+            if g not in lv:
+                lv[g] = lv[g // 2] + 1
+        return self._ps_level(self._trim(np.asarray(self.seed, dtype=np.float64)), lv)
+
+    def _ps_level(self, c: np.ndarray, lv: dict[int, int]) -> int:
+        deg = len(c) - 1
+        if deg < self.ps_baby:
+            used = [lv[k] for k in range(1, deg + 1) if c[k] != 0.0]
+            return (max(used) if used else 0) + 1
+        g = max(x for x in self._giants() if x <= deg)
+        q, r = self._cheb_split(c, g)
+        q, r = self._trim(q), self._trim(r)
+        if len(q) == 1:
+            top = lv[g] + 1
+        else:
+            top = max(self._ps_level(q, lv), lv[g]) + 1
+        if len(r) == 1:  # a constant remainder is added to the top term
+            return top
+        return max(top, self._ps_level(r, lv) + 1)
+
     def _chebyshev(self, x: Ciphertext) -> Ciphertext:
         eng = self.engine
         T = {1: x}
-        for k in range(2, self.degree + 1):
+        for k in range(2, self.ps_baby + 1):
             a = 1 << (math.ceil(math.log2(k)) - 1)
             b = k - a
             prod = self._mul(T[a], None if a == b else T[b])
@@ -321,14 +388,41 @@ class FullSlotBootstrap:
                 T[k] = eng.add_constant(two, -1.0)
             else:
                 T[k] = eng.subtract(two, self._scaled(T[a - b], two.level, two.scale))
-        final = max(t.level for t in T.values()) + 1
-        acc = None
-        for k in range(1, self.degree + 1):
-            if abs(self.seed[k]) < 1e-15:
-                continue
-            term = self._scaled(T[k], final, self.delta, float(self.seed[k]))
-            acc = term if acc is None else eng.add(acc, term)
-        return eng.add_constant(acc, float(self.seed[0]))
+        for g in self._giants():
+            if g not in T:
+                sq = self._mul(T[g // 2], None)
+                T[g] = eng.add_constant(eng.add(sq, sq), -1.0)
+        out = self._ps_eval(self._trim(np.asarray(self.seed, dtype=np.float64)), T)
+        target = x.level + self.cheb_depth
+        if out.level < target:
+            out = self._scaled(out, target, self.delta)
+        return out
+
+    def _ps_eval(self, c: np.ndarray, T: dict[int, Ciphertext]) -> Ciphertext:
+        eng = self.engine
+        deg = len(c) - 1
+        if deg < self.ps_baby:
+            used = [k for k in range(1, deg + 1) if c[k] != 0.0]
+            final = max(T[k].level for k in used) + 1
+            acc = None
+            for k in used:
+                term = self._scaled(T[k], final, self.delta, float(c[k]))
+                acc = term if acc is None else eng.add(acc, term)
+            return eng.add_constant(acc, float(c[0]))
+        g = max(x for x in self._giants() if x <= deg)
+        q, r = self._cheb_split(c, g)
+        q, r = self._trim(q), self._trim(r)
+        if len(q) == 1:
+            top = self._scaled(T[g], T[g].level + 1, self.delta, float(q[0]))
+        else:
+            top = self._mul(self._ps_eval(q, T), T[g])
+        if len(r) == 1:
+            return eng.add_constant(top, float(r[0])) if r[0] != 0.0 else top
+        low = self._ps_eval(r, T)
+        level = max(top.level, low.level + 1)
+        if level > top.level:
+            top = self._scaled(top, level, self.delta)
+        return eng.add(top, self._scaled(low, level, top.scale))
 
     def _eval_mod(self, x: Ciphertext) -> Ciphertext:
         eng = self.engine
@@ -353,8 +447,16 @@ class FullSlotBootstrap:
         conj = eng.conjugate(t, self._conj)
         real = eng.add(t, conj)
         imag = eng.multiply_by_monomial(eng.subtract(t, conj), 3 * self.n)
-        real = self._eval_mod(real)
-        imag = self._eval_mod(imag)
+        # both halves through one modular reduction (twice the batch per launch)
+        shape = real.data.shape
+        rows, n = shape[-2], shape[-1]
+        flat = [h.data.reshape(2, -1, rows, n) for h in (real, imag)]
+        b = flat[0].size(1)
+        both = self._eval_mod(Ciphertext(torch.cat(flat, dim=1), real.level, real.scale,
+                                         real.polynomial_domain, real.residue_representation))
+        out_shape = (2, *shape[1:-2], both.data.size(-2), n)
+        real = Ciphertext(both.data[:, :b].reshape(out_shape).contiguous(), both.level, both.scale)
+        imag = Ciphertext(both.data[:, b:].reshape(out_shape).contiguous(), both.level, both.scale)
         imag = eng.multiply_by_monomial(imag, self.n)
         z = eng.add(real, eng.reinterpret_at_scale(eng.mod_switch_to_level(imag, real.level), real.scale))
         z = self._linear(z, "stc0", self.stc_plans[0])
