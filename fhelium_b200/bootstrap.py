@@ -260,21 +260,37 @@ class FullSlotBootstrap:
             self._plaintexts(f"stc{i}", plan, self.levels["stc"][i])
 
     # -- homomorphic pieces -----------------------------------------------------
+    def _table(self, name: str, plan: _BsgsPlan) -> torch.Tensor:
+        """[giants, babies] int32 device table of plaintext entry indices (-1: none)."""
+        key = ("table", name)
+        if key not in self._pt_cache:
+            t = np.full((len(plan.giants), plan.baby), -1, dtype=np.int32)
+            gidx = {k: i for i, k in enumerate(plan.giants)}
+            for e, (k, b, _) in enumerate(plan.entries):
+                t[gidx[k], b] = e
+            self._pt_cache[key] = torch.from_numpy(t).to(self.engine.device)
+        return self._pt_cache[key]
+
     def _linear(self, ct: Ciphertext, name: str, plan: _BsgsPlan) -> Ciphertext:
         eng = self.engine
         pts = self._plaintexts(name, plan, ct.level)
+        table = self._table(name, plan)
         shifts = plan.baby_shifts
         rotated = eng.rotate_many_by_steps(ct, [(-s) % self.n for s in shifts])
-        rot_ntt = [eng.coefficient_domain_to_ntt_domain(r) for r in rotated]
+        # the baby rotations in the NTT domain, stacked [babies, 2, *batch, L, N]
+        rot = torch.empty((len(rotated), *ct.data.shape), dtype=ct.data.dtype, device=ct.data.device)
+        for i, r in enumerate(rotated):
+            eng.forward_ntt(r.data, r.level, out=rot[i])
+        del rotated
+        inner_all = torch.empty((len(plan.giants), *ct.data.shape), dtype=ct.data.dtype, device=ct.data.device)
+        eng.ctx.call("fhb_ckks_bsgs_inner_product", rot.data_ptr(), rot[0].numel(), pts.data_ptr(), pts[0].numel(),
+                     table.data_ptr(), len(plan.giants), plan.baby, inner_all.data_ptr(), inner_all[0].numel(),
+                     2 * ct.batch_size, ct.limb_count, ct.level, eng._stream())
+        del rot
         q = float(eng.moduli[ct.level])
         result = None
-        for k in plan.giants:
-            inner = None
-            for idx, (kk, b, _) in enumerate(plan.entries):
-                if kk != k:
-                    continue
-                term = eng.multiply_plaintext(rot_ntt[b], pts[idx], q)
-                inner = term if inner is None else eng.add(inner, term)
+        for gi, k in enumerate(plan.giants):
+            inner = Ciphertext(inner_all[gi], ct.level, ct.scale * q, "ntt", "montgomery")
             inner = eng.rescale_to_next_level(eng.ntt_domain_to_coefficient_domain(inner))
             inner = eng.reinterpret_at_scale(inner, ct.scale)
             shift = plan.unit * plan.baby * k

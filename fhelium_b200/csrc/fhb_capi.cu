@@ -174,6 +174,16 @@ int rns_binary(const Context& c, const void* a, const void* b, void* out, int64_
 }
 
 template <typename T>
+int bsgs_inner(const Context& c, const void* rot, int64_t rot_stride, const void* pts, int64_t pt_stride,
+               const int* table, int giants, int babies, void* out, int64_t out_stride, int64_t polys, int rows,
+               int row_start, cudaStream_t st) {
+  k_bsgs_inner<T><<<elementwise_grid(polys * rows << c.log_n), 256, 0, st>>>(
+      (const T*)rot, rot_stride, (const T*)pts, pt_stride, table, giants, babies, (T*)out, out_stride, polys, rows,
+      row_start, c.log_n, tables<T>(c));
+  return cuda_status(cudaGetLastError(), "k_bsgs_inner");
+}
+
+template <typename T>
 int lift_signed(const Context& c, const void* x, void* out, int64_t batch, int rows, int row_start,
                 cudaStream_t st) {
   k_lift_signed<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
@@ -551,6 +561,23 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   TRY(FHB_WORD(fhb::mul_ntt, c, a, b, s.coef, batch, level, st));
   TRY(fhb::inverse(c, s.coef + 2 * comp, s.t0, batch * limbs, limbs, level, fhb::kInvStandard, st));
   return relinearize_tail(c, s, key, s.coef, out, batch, level, rescale, st);
+}
+
+int fhb_ckks_bsgs_inner_product(const fhb_context* ctx, const void* rot, int64_t rot_stride, const void* pts,
+                                int64_t pt_stride, const int32_t* table, int giants, int babies, void* out,
+                                int64_t out_stride, int64_t polys, int rows, int row_start, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(rot, "rot"));
+  TRY(fhb::check_ptr(pts, "pts"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (!table) return fail(-2, "table is NULL");
+  if (giants < 1 || babies < 1 || polys < 0) return fail(-2, "need giants >= 1, babies >= 1, polys >= 0");
+  if (rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  const int64_t per = int64_t(rows) << c.log_n;
+  if (rot_stride < polys * per || out_stride < polys * per || pt_stride < per)
+    return fail(-2, "strides smaller than one baby / giant / plaintext");
+  return FHB_WORD(fhb::bsgs_inner, c, rot, rot_stride, pts, pt_stride, table, giants, babies, out, out_stride, polys,
+                  rows, row_start, st);
 }
 
 int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t* key_ptrs, const uint32_t* galois,

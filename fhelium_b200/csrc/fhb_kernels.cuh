@@ -759,6 +759,50 @@ __global__ void k_rns_binary(const T* __restrict__ a, const T* __restrict__ b, T
   }
 }
 
+// Baby-step/giant-step inner products of a diagonal linear transform, all
+// giant steps of one transform group in one pass:
+//   out[k] = sum_b rot[b] (.) pts[table[k][b]]      (NTT/Montgomery, lazy)
+// rot: [babies][polys][rows][N] baby rotations; pts: [entries][rows][N]
+// diagonal plaintexts shared by every poly; table: [giants][babies] entry
+// index or -1.  Each baby residue is read once and multiplied into up to 16
+// giant accumulators held in registers.  Replaces the per-diagonal
+// plaintext product + add of the reference's BSGS evaluation
+// (fhelium/experimental/bootstrap/_linear.py:235-393).
+template <typename T>
+__global__ void k_bsgs_inner(const T* __restrict__ rot, int64_t rot_stride, const T* __restrict__ pts,
+                             int64_t pt_stride, const int* __restrict__ table, int giants, int babies,
+                             T* __restrict__ out, int64_t out_stride, int64_t polys, int rows, int row_start,
+                             int log_n, ChainTables<T> tabs) {
+  constexpr int kAcc = 16;
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t per = int64_t(rows) * n;
+  const int64_t total = polys * per;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t in_poly = idx % per;  // row * N + coefficient
+    const int row = int(in_poly >> log_n);
+    const PrimeInfo<T> p = tabs.prime[row_start + row];
+    for (int g0 = 0; g0 < giants; g0 += kAcc) {
+      T acc[kAcc];
+#pragma unroll
+      for (int j = 0; j < kAcc; ++j) acc[j] = 0;
+      for (int b = 0; b < babies; ++b) {
+        const T x = rot[b * rot_stride + idx];
+#pragma unroll
+        for (int j = 0; j < kAcc; ++j) {
+          if (g0 + j >= giants) break;
+          const int e = table[(g0 + j) * babies + b];
+          if (e >= 0)
+            acc[j] = csub(acc[j] + Word<T>::mont(x, pts[e * pt_stride + in_poly], p.q, p.neg_inv), p.twice_q);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kAcc; ++j)
+        if (g0 + j < giants) out[(g0 + j) * out_stride + idx] = acc[j];
+    }
+  }
+}
+
 // Lift signed integer coefficients [batch, N] (int64) into every row:
 // out[b, r, k] = x[b, k] mod q_r, canonical (fhelium_rns_ops.
 // lift_centered_coefficients, csrc/ops/rns/cuda/rns_arithmetic_cuda.cu:211).

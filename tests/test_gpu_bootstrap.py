@@ -64,3 +64,34 @@ def test_bootstrap_reference_preset_reference_input():
     err = (eng.decrypt_message(out, is_real=True) - x).abs()
     assert float(err.max()) < 7e-3 and float(err.mean()) < 1.5e-3
     assert -math.log2(float(err.max())) > 8
+
+
+def test_bsgs_inner_product_matches_plaintext_products():
+    """fhb_ckks_bsgs_inner_product against the per-diagonal plaintext product
+    and addition it replaces (equal modulo q)."""
+    import numpy as np
+    from fhelium_b200.values import Ciphertext
+    cfg = CkksConfig(logN=12, scale_bits=50, base_prime_bits=50, num_scale_primes=5, num_p_primes=2)
+    eng = CkksEngine(cfg, galois_generator=5, rng_seed=9)
+    level, babies, giants, batch = 1, 5, 3, 2
+    limbs = eng.num_q - level
+    q = torch.tensor([eng.moduli[level + i] for i in range(limbs)], dtype=torch.int64).view(limbs, 1)
+    g = torch.Generator().manual_seed(12)
+    rot = torch.randint(0, 1 << 62, (babies, 2, batch, limbs, eng.n), generator=g) % (2 * q)
+    pts = torch.randint(0, 1 << 62, (7, limbs, eng.n), generator=g) % q
+    table = torch.tensor([[0, -1, 1, 2, -1], [3, 4, -1, -1, 5], [-1, -1, 6, -1, -1]], dtype=torch.int32)
+    rot_d, pts_d, table_d = rot.cuda(), pts.cuda(), table.cuda()
+    out = torch.empty((giants, 2, batch, limbs, eng.n), dtype=torch.int64, device="cuda")
+    eng.ctx.call("fhb_ckks_bsgs_inner_product", rot_d.data_ptr(), rot_d[0].numel(), pts_d.data_ptr(),
+                 pts_d[0].numel(), table_d.data_ptr(), giants, babies, out.data_ptr(), out[0].numel(), 2 * batch,
+                 limbs, level, eng._stream())
+    for k in range(giants):
+        want = None
+        for b in range(babies):
+            e = int(table[k, b])
+            if e < 0:
+                continue
+            term = eng.multiply_plaintext(Ciphertext(rot_d[b], level, 1.0, "ntt", "montgomery"), pts_d[e], 1.0)
+            want = term if want is None else eng.add(want, term)
+        qd = q.cuda()
+        assert torch.equal(out[k] % qd, want.data % qd)
