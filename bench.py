@@ -266,7 +266,23 @@ def ops_leg(dev, stream, batch=2, steps=3):
     steps4 = [1, 2, 3, 4]
     eng.generate_rotation_keys(steps4)
     ct3 = eng.multiply(ca, ca)
+    # BSGS inner products as in a bootstrap transform group: 16 baby
+    # rotations x 4 giant steps over 64 diagonal plaintexts
+    g16 = torch.Generator(device=dev)
+    g16.manual_seed(7)
+    qcol = torch.tensor(eng.moduli[:eng.num_q], dtype=torch.int64, device=dev).view(-1, 1)
+    rot = torch.randint(0, 1 << 62, (16, *ca.data.shape), generator=g16, device=dev) % qcol
+    pts = torch.randint(0, 1 << 62, (64, eng.num_q, eng.n), generator=g16, device=dev) % qcol
+    table = torch.arange(64, dtype=torch.int32, device=dev).view(4, 16)
+    inner = torch.empty((4, *ca.data.shape), dtype=torch.int64, device=dev)
+
+    def bsgs():
+        eng.ctx.call("fhb_ckks_bsgs_inner_product", rot.data_ptr(), rot[0].numel(), pts.data_ptr(), pts[0].numel(),
+                     table.data_ptr(), 4, 16, inner.data_ptr(), inner[0].numel(), 2 * batch, eng.num_q, 0,
+                     stream.cuda_stream)
+
     ops = {
+        "bsgs_inner_product_16x4": bsgs,
         "multiply_relinearize_rescale": lambda: eng.multiply_relinearize_rescale(ca, ca),
         "relinearize": lambda: eng.relinearize(ct3),
         "rescale": lambda: eng.rescale_to_next_level(ct),
