@@ -278,7 +278,7 @@ def ops_leg(dev, stream, batch=2, steps=3):
 
     def bsgs():
         eng.ctx.call("fhb_ckks_bsgs_inner_product", rot.data_ptr(), rot[0].numel(), pts.data_ptr(), pts[0].numel(),
-                     table.data_ptr(), 4, 16, inner.data_ptr(), inner[0].numel(), 2 * batch, eng.num_q, 0,
+                     64, table.data_ptr(), 4, 16, inner.data_ptr(), inner[0].numel(), 2 * batch, eng.num_q, 0,
                      stream.cuda_stream)
 
     ops = {

@@ -284,7 +284,8 @@ class FullSlotBootstrap:
         del rotated
         inner_all = torch.empty((len(plan.giants), *ct.data.shape), dtype=ct.data.dtype, device=ct.data.device)
         eng.ctx.call("fhb_ckks_bsgs_inner_product", rot.data_ptr(), rot[0].numel(), pts.data_ptr(), pts[0].numel(),
-                     table.data_ptr(), len(plan.giants), plan.baby, inner_all.data_ptr(), inner_all[0].numel(),
+                     pts.size(0), table.data_ptr(), len(plan.giants), plan.baby, inner_all.data_ptr(),
+                     inner_all[0].numel(),
                      2 * ct.batch_size, ct.limb_count, ct.level, eng._stream())
         del rot
         q = float(eng.moduli[ct.level])

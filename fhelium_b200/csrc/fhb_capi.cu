@@ -175,8 +175,20 @@ int rns_binary(const Context& c, const void* a, const void* b, void* out, int64_
 
 template <typename T>
 int bsgs_inner(const Context& c, const void* rot, int64_t rot_stride, const void* pts, int64_t pt_stride,
-               const int* table, int giants, int babies, void* out, int64_t out_stride, int64_t polys, int rows,
-               int row_start, cudaStream_t st) {
+               int entries, const int* table, int giants, int babies, void* out, int64_t out_stride, int64_t polys,
+               int rows, int row_start, cudaStream_t st) {
+  const size_t staged = size_t(entries) * 32 * sizeof(T);
+  // staging pays once a plaintext slice is shared by a warp's worth of
+  // polynomials per block (8 warps); below that the direct kernel is faster
+  if (entries > 0 && staged <= 96 * 1024 && polys >= 8) {
+    const int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(k_bsgs_inner_staged<T>), int(staged));
+    if (rc != 0) return rc;
+    const int64_t blocks = (int64_t(rows) << c.log_n) / 32;
+    k_bsgs_inner_staged<T><<<unsigned(blocks), 256, staged, st>>>(
+        (const T*)rot, rot_stride, (const T*)pts, pt_stride, entries, table, giants, babies, (T*)out, out_stride,
+        polys, rows, row_start, c.log_n, tables<T>(c));
+    return cuda_status(cudaGetLastError(), "k_bsgs_inner_staged");
+  }
   k_bsgs_inner<T><<<elementwise_grid(polys * rows << c.log_n), 256, 0, st>>>(
       (const T*)rot, rot_stride, (const T*)pts, pt_stride, table, giants, babies, (T*)out, out_stride, polys, rows,
       row_start, c.log_n, tables<T>(c));
@@ -564,20 +576,22 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
 }
 
 int fhb_ckks_bsgs_inner_product(const fhb_context* ctx, const void* rot, int64_t rot_stride, const void* pts,
-                                int64_t pt_stride, const int32_t* table, int giants, int babies, void* out,
-                                int64_t out_stride, int64_t polys, int rows, int row_start, fhb_stream stream) {
+                                int64_t pt_stride, int entries, const int32_t* table, int giants, int babies,
+                                void* out, int64_t out_stride, int64_t polys, int rows, int row_start,
+                                fhb_stream stream) {
   CTX_OR_FAIL();
   TRY(fhb::check_ptr(rot, "rot"));
   TRY(fhb::check_ptr(pts, "pts"));
   TRY(fhb::check_ptr(out, "out"));
   if (!table) return fail(-2, "table is NULL");
-  if (giants < 1 || babies < 1 || polys < 0) return fail(-2, "need giants >= 1, babies >= 1, polys >= 0");
+  if (giants < 1 || babies < 1 || polys < 0 || entries < 1)
+    return fail(-2, "need giants >= 1, babies >= 1, entries >= 1, polys >= 0");
   if (rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
   const int64_t per = int64_t(rows) << c.log_n;
   if (rot_stride < polys * per || out_stride < polys * per || pt_stride < per)
     return fail(-2, "strides smaller than one baby / giant / plaintext");
-  return FHB_WORD(fhb::bsgs_inner, c, rot, rot_stride, pts, pt_stride, table, giants, babies, out, out_stride, polys,
-                  rows, row_start, st);
+  return FHB_WORD(fhb::bsgs_inner, c, rot, rot_stride, pts, pt_stride, entries, table, giants, babies, out,
+                  out_stride, polys, rows, row_start, st);
 }
 
 int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t* key_ptrs, const uint32_t* galois,

@@ -803,6 +803,54 @@ __global__ void k_bsgs_inner(const T* __restrict__ rot, int64_t rot_stride, cons
   }
 }
 
+// Same inner products with the plaintext rows staged in shared memory, so
+// that each plaintext residue leaves HBM once however many polynomials share
+// it.  One block per (row, 32 consecutive coefficients): the block stages
+// the 32-coefficient slice of every plaintext entry (entries * 32 words),
+// then each warp takes polynomials warp, warp + 8, ... with lane = the
+// coefficient.  Requires entries * 32 * sizeof(T) of dynamic shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_bsgs_inner_staged(const T* __restrict__ rot, int64_t rot_stride, const T* __restrict__ pts, int64_t pt_stride,
+                    int entries, const int* __restrict__ table, int giants, int babies, T* __restrict__ out,
+                    int64_t out_stride, int64_t polys, int rows, int row_start, int log_n, ChainTables<T> tabs) {
+  constexpr int kAcc = 16;
+  constexpr int kTile = 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sp = reinterpret_cast<T*>(smem_raw);  // [entries][kTile]
+  const int64_t n = int64_t(1) << log_n;
+  const int tiles_per_row = int(n / kTile);
+  const int row = blockIdx.x / tiles_per_row;
+  const int64_t col0 = int64_t(blockIdx.x % tiles_per_row) * kTile;
+  const int64_t in_poly0 = int64_t(row) * n + col0;  // row * N + first coefficient of the tile
+  for (int i = threadIdx.x; i < entries * kTile; i += blockDim.x)
+    sp[i] = pts[int64_t(i / kTile) * pt_stride + in_poly0 + (i % kTile)];
+  __syncthreads();
+  const PrimeInfo<T> p = tabs.prime[row_start + row];
+  const int lane = threadIdx.x % kTile;
+  const int64_t per = int64_t(rows) * n;
+  for (int64_t poly = threadIdx.x / kTile; poly < polys; poly += blockDim.x / kTile) {
+    const int64_t idx = poly * per + in_poly0 + lane;
+    for (int g0 = 0; g0 < giants; g0 += kAcc) {
+      T acc[kAcc];
+#pragma unroll
+      for (int j = 0; j < kAcc; ++j) acc[j] = 0;
+      for (int b = 0; b < babies; ++b) {
+        const T x = rot[b * rot_stride + idx];
+#pragma unroll
+        for (int j = 0; j < kAcc; ++j) {
+          if (g0 + j >= giants) break;
+          const int e = table[(g0 + j) * babies + b];
+          if (e >= 0) acc[j] = csub(acc[j] + Word<T>::mont(x, sp[e * kTile + lane], p.q, p.neg_inv), p.twice_q);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kAcc; ++j)
+        if (g0 + j < giants) out[(g0 + j) * out_stride + idx] = acc[j];
+    }
+  }
+}
+
 // Lift signed integer coefficients [batch, N] (int64) into every row:
 // out[b, r, k] = x[b, k] mod q_r, canonical (fhelium_rns_ops.
 // lift_centered_coefficients, csrc/ops/rns/cuda/rns_arithmetic_cuda.cu:211).

@@ -259,14 +259,16 @@ int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, voi
  *   out[k] = sum_b rot[b] (.) pts[table[k * babies + b]]
  * for k < giants, skipping table entries < 0.  rot: babies blocks of `polys`
  * NTT/Montgomery polynomials [polys, rows, N] (block pitch rot_stride
- * words); pts: plaintext rows [rows, N] (pitch pt_stride words), shared by
- * every polynomial; out: giants blocks (pitch out_stride words), lazy
- * Montgomery products.  table is a DEVICE int32 array.  Replaces the
- * per-diagonal plaintext product and addition of the reference's BSGS
- * evaluation (fhelium/experimental/bootstrap/_linear.py:235-393). */
+ * words); pts: `entries` plaintexts [rows, N] (pitch pt_stride words),
+ * shared by every polynomial; out: giants blocks (pitch out_stride words),
+ * lazy Montgomery products.  table is a DEVICE int32 array whose entries
+ * are < entries.  Replaces the per-diagonal plaintext product and addition
+ * of the reference's BSGS evaluation
+ * (fhelium/experimental/bootstrap/_linear.py:235-393). */
 int fhb_ckks_bsgs_inner_product(const fhb_context* ctx, const void* rot, int64_t rot_stride, const void* pts,
-                                int64_t pt_stride, const int32_t* table, int giants, int babies, void* out,
-                                int64_t out_stride, int64_t polys, int rows, int row_start, fhb_stream stream);
+                                int64_t pt_stride, int entries, const int32_t* table, int giants, int babies,
+                                void* out, int64_t out_stride, int64_t polys, int rows, int row_start,
+                                fhb_stream stream);
 
 /* Mixed-step rotation of one level: item b of ct [2, batch, L, N]
  * (coefficient/standard) is rotated by its own Galois element galois[b]

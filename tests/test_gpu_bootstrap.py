@@ -66,14 +66,15 @@ def test_bootstrap_reference_preset_reference_input():
     assert -math.log2(float(err.max())) > 8
 
 
-def test_bsgs_inner_product_matches_plaintext_products():
+@pytest.mark.parametrize("batch", [1, 2, 9])  # direct kernel below 8 polynomials, staged from 8
+def test_bsgs_inner_product_matches_plaintext_products(batch):
     """fhb_ckks_bsgs_inner_product against the per-diagonal plaintext product
     and addition it replaces (equal modulo q)."""
     import numpy as np
     from fhelium_b200.values import Ciphertext
     cfg = CkksConfig(logN=12, scale_bits=50, base_prime_bits=50, num_scale_primes=5, num_p_primes=2)
     eng = CkksEngine(cfg, galois_generator=5, rng_seed=9)
-    level, babies, giants, batch = 1, 5, 3, 2
+    level, babies, giants = 1, 5, 3
     limbs = eng.num_q - level
     q = torch.tensor([eng.moduli[level + i] for i in range(limbs)], dtype=torch.int64).view(limbs, 1)
     g = torch.Generator().manual_seed(12)
@@ -83,7 +84,7 @@ def test_bsgs_inner_product_matches_plaintext_products():
     rot_d, pts_d, table_d = rot.cuda(), pts.cuda(), table.cuda()
     out = torch.empty((giants, 2, batch, limbs, eng.n), dtype=torch.int64, device="cuda")
     eng.ctx.call("fhb_ckks_bsgs_inner_product", rot_d.data_ptr(), rot_d[0].numel(), pts_d.data_ptr(),
-                 pts_d[0].numel(), table_d.data_ptr(), giants, babies, out.data_ptr(), out[0].numel(), 2 * batch,
+                 pts_d[0].numel(), 7, table_d.data_ptr(), giants, babies, out.data_ptr(), out[0].numel(), 2 * batch,
                  limbs, level, eng._stream())
     for k in range(giants):
         want = None
