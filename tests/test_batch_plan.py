@@ -47,3 +47,10 @@ def test_cache_round_trip(tmp_path):
         f.write("not json")
     assert autotune._load(path) == {}
     json.dumps(autotune.default_cache_path())
+
+
+def test_streaming_chunks_cover_the_batch():
+    from fhelium_b200.streaming import _chunks
+    assert _chunks(7, 3) == [(0, 3), (3, 5), (5, 7)]
+    assert _chunks(2, 5) == [(0, 1), (1, 2)]
+    assert _chunks(32, 4) == [(0, 8), (8, 16), (16, 24), (24, 32)]
