@@ -290,14 +290,22 @@ class FullSlotBootstrap:
         del rot
         q = float(eng.moduli[ct.level])
         result = None
+        rotated, keys = [], []
         for gi, k in enumerate(plan.giants):
             inner = Ciphertext(inner_all[gi], ct.level, ct.scale * q, "ntt", "montgomery")
             inner = eng.rescale_to_next_level(eng.ntt_domain_to_coefficient_domain(inner))
             inner = eng.reinterpret_at_scale(inner, ct.scale)
             shift = plan.unit * plan.baby * k
             if shift % self.n:
-                inner = eng.rotate_by_step(inner, (-shift) % self.n)
-            result = inner if result is None else eng.add(result, inner)
+                rotated.append(inner)
+                keys.append(eng.rotation_key((-shift) % self.n))
+            else:
+                result = inner if result is None else eng.add(result, inner)
+        del inner_all
+        if rotated:
+            # the giant-step rotations summed before a single ModDown
+            summed = eng.rotate_and_sum(rotated, keys)
+            result = summed if result is None else eng.add(result, summed)
         return result
 
     # Scales are tracked exactly inside the modular reduction: the 50-bit

@@ -101,6 +101,10 @@ int ks_core(const Context& c, const void* digits, const void* key, void* acc0, v
             int level, cudaStream_t st, const uint64_t* item_keys = nullptr, const void* ct3 = nullptr) {
   FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys, ct3);
 }
+int ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
+           int64_t batch, int level, cudaStream_t st) {
+  FHB_DISPATCH(run_ks_sum, c, digits, key_ptrs, acc0, acc1, giants, batch, level, st);
+}
 int prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st) {
   FHB_DISPATCH(run_prepare, c, digits, prepared, batch, level, st);
 }
@@ -573,6 +577,18 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   TRY(FHB_WORD(fhb::mul_ntt, c, a, b, s.coef, batch, level, st));
   TRY(fhb::inverse(c, s.coef + 2 * comp, s.t0, batch * limbs, limbs, level, fhb::kInvStandard, st));
   return relinearize_tail(c, s, key, s.coef, out, batch, level, rescale, st);
+}
+
+int fhb_ckks_keyswitch_sum(const fhb_context* ctx, const void* digits, const uint64_t* key_ptrs, void* acc0,
+                           void* acc1, int giants, int64_t batch, int level, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(digits, "digits"));
+  TRY(fhb::check_ptr(acc0, "acc0"));
+  TRY(fhb::check_ptr(acc1, "acc1"));
+  if (!key_ptrs) return fail(-2, "key_ptrs is NULL");
+  if (giants < 1 || batch < 0) return fail(-2, "need giants >= 1 and batch >= 0");
+  TRY(fhb::check_level(c, level));
+  return fhb::ks_sum(c, digits, key_ptrs, acc0, acc1, giants, batch, level, st);
 }
 
 int fhb_ckks_bsgs_inner_product(const fhb_context* ctx, const void* rot, int64_t rot_stride, const void* pts,

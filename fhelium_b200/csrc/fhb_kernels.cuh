@@ -513,6 +513,58 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   tw.inverse(s, p, v, e1);
 }
 
+// Sum of key switches of several ciphertexts with their own keys, reduced
+// before the inverse NTT: acc = sum_g sum_d NTT(ext_d(digits[g])) * key_g[d]
+// for every (ciphertext b, row j) unit, then one inverse NTT of each
+// accumulator.  Followed by one ModDown, this is the "lazy ModDown" sum of
+// rotations sum_g KS_g(sigma_g(c1_g)) (each term differs from its own ModDown
+// by the rounding of the division by P, i.e. the sum is within `giants`
+// units of the sum of separately rounded rotations).  digits: [G][B][L][N]
+// ModUp digits (sigma_g applied); key_ptrs: device array of G key addresses;
+// acc0/acc1: [B][QP_l][N].  Used for the giant steps of bootstrapping's
+// linear transforms (the reference rotates and adds each giant step,
+// fhelium/experimental/bootstrap/_linear.py:235-393).
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_keyswitch_sum(const T* __restrict__ digits, const unsigned long long* __restrict__ key_ptrs, T* __restrict__ acc0,
+                T* __restrict__ acc1, int giants, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
+                int order, ChainTables<T> tabs, LevelTables<T> lt) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  int64_t poly, bi;
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  const int pid = level + jrow;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
+  KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(false);
+  for (int gi = 0; gi < giants; ++gi) {
+    const T* dig = digits + (int64_t(gi) * batch + bi) * q_limbs * int64_t(G::kN);
+    const T* key = reinterpret_cast<const T*>(key_ptrs[gi]);
+    for (int a = 0; a < lt.num_digits; ++a) {
+      const DigitDesc d = lt.digits[a];
+      ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
+                       qp0, d.alpha, LOGN, p.q, p.twice_q};
+      T v[G::kE];
+      tw.forward_from(src, s, p, v);
+      key_mac(acc, v, key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own,
+              key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own, p);
+    }
+  }
+  tw.stage(true);
+  T v[G::kE];
+  acc.get(0, v);
+  InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0 + poly * G::kN, p, kInvStandard, false);
+  tw.inverse(s, p, v, e0);
+  acc.get(1, v);
+  InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
+  tw.inverse(s, p, v, e1);
+}
+
 // Hoisting stage 1: materialise NTT-domain extended digits once
 // (fhelium/engine/hybrid_keyswitch.py:373-417).  prepared: [D_l, B, QP_l, N]
 // standard NTT-domain values in [0, 2p).

@@ -87,6 +87,16 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
 }
 
 template <typename T, int LOGN>
+int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
+               int64_t batch, int level, cudaStream_t st) {
+  const int ql = c.num_q - level, qpl = ql + c.num_p;
+  return launch_cluster<T, LOGN>(k_keyswitch_sum<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
+                                 (const T*)digits, reinterpret_cast<const unsigned long long*>(key_ptrs), (T*)acc0,
+                                 (T*)acc1, giants, batch, ql, qpl, level, c.qp(), c.ks_order, tables<T>(c),
+                                 level_tables<T>(c, level));
+}
+
+template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level,
                 cudaStream_t st) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
@@ -111,6 +121,8 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, cudaStream_t); \
   template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
                                     cudaStream_t, const uint64_t*, const void*);                                \
+  template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
+                                   cudaStream_t);                                                               \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);

@@ -403,6 +403,44 @@ class CkksEngine:
                       nat.ptr(scratch), nbytes, ct.batch_size, ct.level, self._stream())
         return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
 
+    def rotate_and_sum(self, cts: Sequence[Ciphertext], keys: Sequence[RotationKey]) -> Ciphertext:
+        """sum_i rotate_with_key(cts[i], keys[i]) with one ModDown for the
+        whole sum: ModUp of every sigma_g(c1), the key switches accumulated
+        in the NTT domain (fhb_ckks_keyswitch_sum), one inverse NTT and one
+        ModDown with sum_i sigma_g(c0_i) added.  The sum is rounded once
+        instead of once per term, so it is within len(cts) units of the sum
+        of separately rounded rotations (not bit-identical to it)."""
+        if not cts or len(cts) != len(keys):
+            raise ValueError("need one rotation key per ciphertext")
+        first = cts[0]
+        for ct in cts:
+            ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+            self._check_ct(ct)
+            if (ct.level, ct.data.shape, ct.scale) != (first.level, first.data.shape, first.scale):
+                raise ValueError("rotate_and_sum needs ciphertexts of one level, shape and scale")
+        b, level, limbs = first.batch_size, first.level, first.limb_count
+        st = self._stream()
+        digits = self._empty(len(cts), b, limbs, self.n)
+        for i, (ct, key) in enumerate(zip(cts, keys)):
+            self.ctx.call("fhb_ckks_modup_digits", nat.ptr(ct.c1), nat.ptr(digits[i]), b, level, key.galois_element, st)
+        key_ptrs = torch.tensor([k.data.data_ptr() for k in keys], dtype=torch.int64, device=self.device)
+        t = self._empty(2, b, limbs + self.num_p, self.n)
+        self.ctx.call("fhb_ckks_keyswitch_sum", nat.ptr(digits), nat.ptr(key_ptrs), nat.ptr(t[0]), nat.ptr(t[1]),
+                      len(cts), b, level, st)
+        add0 = None
+        for ct, key in zip(cts, keys):
+            rot = self._empty(*ct.c0.shape)
+            self.ctx.call("fhb_ckks_automorphism", nat.ptr(ct.c0), nat.ptr(rot), b, limbs, level, key.galois_element,
+                          st)
+            if add0 is None:
+                add0 = rot
+            else:
+                self.ctx.call("fhb_ckks_add", nat.ptr(add0), nat.ptr(rot), nat.ptr(add0), b, level, 0, st)
+        out = torch.empty_like(first.data)
+        self.ctx.call("fhb_ckks_moddown", nat.ptr(t[0]), nat.ptr(t[1]), nat.ptr(add0), None, nat.ptr(out), b, level,
+                      1, 0, st)
+        return Ciphertext(out, level, first.scale, "coefficient", "standard")
+
     def prepare_rotation_digits(self, ct: Ciphertext) -> torch.Tensor:
         """Hoisted ModUp of c1: [digit, *batch, Q_l + P, N] NTT-domain digits."""
         ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)

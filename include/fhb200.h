@@ -254,6 +254,17 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
 int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,
                     int64_t scratch_bytes, int64_t batch, int level, uint32_t galois, fhb_stream stream);
 
+/* Key switches of `giants` ciphertexts with their own keys, summed before
+ * the inverse NTT ("lazy ModDown"): digits [giants, batch, L, N] from
+ * fhb_ckks_modup_digits (sigma_g applied per giant), key_ptrs a DEVICE array
+ * of `giants` key addresses ([D, 2, QP0, N] each); acc0, acc1 [batch, L+P, N]
+ * receive coefficient/standard rows for one fhb_ckks_moddown.  The result is
+ * within `giants` units of the sum of separately rounded key switches.
+ * Replaces the rotate-and-add of every giant step of the reference's BSGS
+ * linear transforms (fhelium/experimental/bootstrap/_linear.py:235-393). */
+int fhb_ckks_keyswitch_sum(const fhb_context* ctx, const void* digits, const uint64_t* key_ptrs, void* acc0,
+                           void* acc1, int giants, int64_t batch, int level, fhb_stream stream);
+
 /* Baby-step/giant-step inner products of a diagonal linear transform
  * (bootstrapping's CoeffsToSlots / SlotsToCoeffs):
  *   out[k] = sum_b rot[b] (.) pts[table[k * babies + b]]

@@ -96,3 +96,28 @@ def test_bsgs_inner_product_matches_plaintext_products(batch):
             want = term if want is None else eng.add(want, term)
         qd = q.cuda()
         assert torch.equal(out[k] % qd, want.data % qd)
+
+
+def test_rotate_and_sum_close_to_separate_rotations():
+    """One ModDown for a sum of rotations: within the number of terms of the
+    separately rounded sum (exact modulo that rounding), and decrypts the same."""
+    import numpy as np
+    cfg = CkksConfig.parse(Preset.slots8192_scale40_levels7_int64)
+    eng = CkksEngine(cfg, rng_seed=6)
+    rng = np.random.default_rng(3)
+    steps = [1, 5, -7, 64]
+    cts = [eng.encrypt_message(rng.uniform(-0.05, 0.05, (2, eng.num_slots)), level=1) for _ in steps]
+    keys = [eng.rotation_key(s) for s in steps]
+    got = eng.rotate_and_sum(cts, keys)
+    want = None
+    for ct, key in zip(cts, keys):
+        r = eng.rotate_with_key(ct, key)
+        want = r if want is None else eng.add(want, r)
+    q = torch.tensor([eng.moduli[1 + i] for i in range(got.limb_count)], dtype=torch.int64,
+                     device=got.data.device).view(-1, 1)
+    diff = (got.data - want.data) % q
+    centered = torch.where(diff > q // 2, diff - q, diff)
+    # one integer k per coefficient, the same in every prime, |k| <= terms
+    assert int(centered.abs().max()) <= len(steps)
+    assert torch.equal(centered, centered[..., :1, :].expand_as(centered))
+    assert float((eng.decrypt_message(got) - eng.decrypt_message(want)).abs().max()) < 1e-5
