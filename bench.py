@@ -208,6 +208,17 @@ def ntt_leg(dev, stream, steps):
         fwd()
         inv()
         out[tag]["roundtrip_bit_exact"] = bool(torch.equal(x, z))
+    # integer-pipe roof: Shoup products per transform (N/2 log N butterflies
+    # + the N x R or x N^-1 pass) against the int32 probe's rate
+    probe_out = torch.empty(148 * 8 * 256, dtype=torch.int32, device=dev)
+    probe = lambda: nat.check(ctx.lib.fhb_modmul_probe(ctx.handle, probe_out.data_ptr(), 148 * 8, 2048, s), "probe")
+    probe()
+    torch.cuda.synchronize(dev)
+    peak = 148 * 8 * 256 * 8 * 2048 / (_time_events(probe, 3, stream) / 1e3)
+    per_dir = B * L * (N // 2 * 16 + N)
+    out["alu_roofline"] = {"unit": "modular products/s", "peak": peak,
+                           "forward_frac": per_dir / (out["tuned"]["forward_ms"] / 1e3) / peak,
+                           "inverse_frac": per_dir / (out["tuned"]["inverse_ms"] / 1e3) / peak}
     ctx.close()
     return out
 
@@ -534,6 +545,25 @@ def main() -> int:
     except Exception:
         peak, peak_src = 6650.0, "fallback"
     achieved = ks_bytes / (per_kernel["keyswitch_core"] / 1000.0) / 1e9
+    # The key-switch core is bound by 64-bit modular products on the integer
+    # pipes, so it is also measured against their attainable rate: modular
+    # products per launch (Shoup butterflies of 10 forward and 2 inverse
+    # transforms per row, the basis extension's sum_r alpha_r = L Shoup
+    # products per digit row, 2 Montgomery key products per digit, the N^-1
+    # epilogue) over the probe's rate of independent Shoup chains.
+    n_, logn_ = cfg.N, cfg.logN
+    dnum_ = len(eng.level_digits[0])
+    bfly_ = n_ // 2 * logn_
+    qp_ = L + cfg.num_p_primes
+    ks_modmul = B * qp_ * (dnum_ * bfly_ + L * n_ + 2 * dnum_ * n_ + 2 * (bfly_ + n_))
+    probe_out = torch.empty(148 * 8 * 256, dtype=torch.int64, device=dev)
+    probe_iters = 2048
+    probe = lambda: nat.check(lib.fhb_modmul_probe(h, probe_out.data_ptr(), 148 * 8, probe_iters, s), "probe")
+    probe()
+    torch.cuda.synchronize(dev)
+    probe_ms = _time_events(probe, 3, stream)
+    modmul_peak = 148 * 8 * 256 * 8 * probe_iters / (probe_ms / 1000.0)
+    modmul_achieved = ks_modmul / (per_kernel["keyswitch_core"] / 1000.0)
     step_bytes = B * (4 * L + 2 * (L - 1)) * limb + 10 * 2 * (L + cfg.num_p_primes) * limb
     # DRAM bytes of one k_keyswitch_core launch: 1275 MB measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on a batch-2 launch, work
@@ -596,6 +626,11 @@ def main() -> int:
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "chunks": e2e_chunks["chunks"],
                 "chunk_trials_ms": trial},
         "gpu_launches": launches_per_step * args.steps,
+        "alu_roofline": {"kernel": "k_keyswitch_core", "unit": "modular products/s",
+                         "modmul_per_launch": ks_modmul, "achieved": modmul_achieved, "peak": modmul_peak,
+                         "frac": modmul_achieved / modmul_peak,
+                         "peak_source": "fhb_modmul_probe: 148x8 CTAs x 256 threads x 8 independent Shoup chains, "
+                                        "timed in this run"},
         "roofline": {"kernel": "k_keyswitch_core", "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": ks_bytes, "launch_ms": per_kernel["keyswitch_core"],

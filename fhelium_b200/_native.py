@@ -23,6 +23,7 @@ _I64 = ctypes.c_int64
 _U32 = ctypes.c_uint32
 SIGNATURES: dict[str, tuple] = {
     "fhb_version": (_I, []),
+    "fhb_modmul_probe": (_I, [_P, _P, _I, _I, _P]),
     "fhb_last_error": (ctypes.c_char_p, []),
     "fhb_context_create": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, _I, ctypes.POINTER(_P)]),
     "fhb_context_destroy": (_I, [_P]),

@@ -276,6 +276,17 @@ extern "C" {
 
 int fhb_version(void) { return 1; }
 
+int fhb_modmul_probe(const fhb_context* ctx, void* out, int blocks, int iters, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(out, "out"));
+  if (blocks < 1 || iters < 1) return fail(-2, "need blocks >= 1 and iters >= 1");
+  if (c.bits == 64)
+    fhb::k_modmul_probe<uint64_t><<<blocks, 256, 0, st>>>((uint64_t*)out, iters, fhb::tables<uint64_t>(c));
+  else
+    fhb::k_modmul_probe<uint32_t><<<blocks, 256, 0, st>>>((uint32_t*)out, iters, fhb::tables<uint32_t>(c));
+  return fhb::cuda_status(cudaGetLastError(), "k_modmul_probe");
+}
+
 const char* fhb_last_error(void) { return fhb::last_error(); }
 
 int fhb_context_create(int residue_bits, int log_n, const uint64_t* moduli, int num_q, int num_p, int device,

@@ -903,6 +903,29 @@ k_bsgs_inner_staged(const T* __restrict__ rot, int64_t rot_stride, const T* __re
   }
 }
 
+// Throughput probe of the modular multiplication the kernels are built on:
+// every thread runs 8 independent chains of `iters` Shoup products by a
+// per-prime constant (the butterfly's product) on registers only and writes
+// the results so nothing is optimised away.  Gives the attainable rate of
+// 64-bit (32-bit) modular products on the integer pipes, the roof that the
+// NTT-heavy kernels are measured against.
+template <typename T>
+__global__ void k_modmul_probe(T* __restrict__ out, int iters, ChainTables<T> tabs) {
+  const PrimeInfo<T> p = tabs.prime[0];
+  const TwPair<T> w = tabs.tw_fwd[1];
+  T x[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) x[i] = T(threadIdx.x + i * 977 + blockIdx.x) % p.q;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = Word<T>::shoup(x[i], w.w, w.wp, p.q);
+  }
+  T acc = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc ^= x[i];
+  out[blockIdx.x * int64_t(blockDim.x) + threadIdx.x] = acc;
+}
+
 // Lift signed integer coefficients [batch, N] (int64) into every row:
 // out[b, r, k] = x[b, k] mod q_r, canonical (fhelium_rns_ops.
 // lift_centered_coefficients, csrc/ops/rns/cuda/rns_arithmetic_cuda.cu:211).

@@ -43,6 +43,13 @@ enum fhb_inverse_output {
 };
 
 int fhb_version(void);
+
+/* Diagnostic: blocks x 256 threads each run 8 independent chains of `iters`
+ * Shoup modular products (the butterfly product) on registers and write one
+ * word per thread to out (blocks * 256 words): blocks * 256 * 8 * iters
+ * products, the attainable modular-multiplication rate the NTT-based
+ * kernels are measured against.  No counterpart in the reference. */
+int fhb_modmul_probe(const fhb_context* ctx, void* out, int blocks, int iters, fhb_stream stream);
 const char* fhb_last_error(void);
 
 /* Build the device tables (twiddles with Shoup companions, Montgomery
