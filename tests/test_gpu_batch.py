@@ -105,3 +105,23 @@ def test_autotune_picks_and_caches(small, tmp_path):
     ex.run()
     for i, w in enumerate(want):
         assert torch.equal(ex.result(i).data, w.data)
+
+
+def test_ntt_autotune_sets_and_caches(tmp_path):
+    from fhelium_b200 import _native as nat
+    eng = CkksEngine(Preset.slots8192_scale40_levels7_int64, rng_seed=2)
+    x = torch.randint(0, 1 << 40, (3, eng.num_q, eng.n), dtype=torch.int64, device="cuda")
+    path = str(tmp_path / "ntt.json")
+    first = autotune.tune_ntt(eng.ctx, x, eng.num_q, cache_path=path, repeats=1)
+    assert not first["cached"] and first["forward_ept"] in (8, 16) and first["inverse_ept"] in (8, 16)
+    assert eng.ctx.get_tuning(nat.TUNE_NTT_FORWARD_EPT) == first["forward_ept"]
+    assert eng.ctx.get_tuning(nat.TUNE_NTT_INVERSE_EPT) == first["inverse_ept"]
+    eng.ctx.set_tuning(nat.TUNE_NTT_FORWARD_EPT, 0)
+    second = autotune.tune_ntt(eng.ctx, x, eng.num_q, cache_path=path)
+    assert second["cached"] and eng.ctx.get_tuning(nat.TUNE_NTT_FORWARD_EPT) == first["forward_ept"]
+    # results do not depend on the launch shape
+    outs = []
+    for ept in (8, 16):
+        eng.ctx.set_tuning(nat.TUNE_NTT_FORWARD_EPT, ept)
+        outs.append(eng.forward_ntt(x, 0))
+    assert torch.equal(outs[0], outs[1])
