@@ -158,16 +158,8 @@ def _time_events(fn, steps, stream):
 
 
 def ntt_int32_primes(count: int = 36, log_n: int = 16) -> list[int]:
-    """The first `count` distinct catalog primes with 4q < 2^30 and q = 1 mod 2N
-    from the int32 families (25-bit scale primes, then 28-bit message primes)."""
-    from fhelium_b200.config import prime_catalog
-    cat = prime_catalog()
-    n = 1 << log_n
-    out = []
-    for q in list(cat["scale"][(25, n)]) + list(cat["message"][(28, n)]):
-        if q not in out and 4 * q < 2 ** 30 and (q - 1) % (2 * n) == 0:
-            out.append(q)
-    return out[:count]
+    from fhelium_b200.config import int32_ntt_primes
+    return int32_ntt_primes(count, log_n)
 
 
 def ntt_leg(dev, stream, steps):

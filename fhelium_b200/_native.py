@@ -24,6 +24,11 @@ _U32 = ctypes.c_uint32
 SIGNATURES: dict[str, tuple] = {
     "fhb_version": (_I, []),
     "fhb_modmul_probe": (_I, [_P, _P, _I, _I, _P]),
+    "fhb_tc_ntt_prepare": (_I, [_P]),
+    "fhb_tc_forward_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _P]),
+    "fhb_tc_inverse_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _P]),
+    "fhb_tc_ntt_status": (_I, [_P, ctypes.POINTER(_I)]),
+    "fhb_tc_ntt_tables_host": (_I, [ctypes.c_uint64, ctypes.c_uint64, _I, _P, _P]),
     "fhb_last_error": (ctypes.c_char_p, []),
     "fhb_context_create": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, _I, ctypes.POINTER(_P)]),
     "fhb_context_destroy": (_I, [_P]),

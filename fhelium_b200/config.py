@@ -75,6 +75,19 @@ def prime_catalog() -> dict[str, dict[tuple[int, int], tuple[int, ...]]]:
     return out
 
 
+def int32_ntt_primes(count: int = 36, log_n: int = 16) -> list[int]:
+    """The first `count` distinct catalog primes with 4q < 2^30 and q = 1 mod 2N
+    from the int32 families (25-bit scale primes, then 28-bit message primes):
+    the limb set of the standalone int32 NTT workload (N = 2^16, 36 limbs)."""
+    cat = prime_catalog()
+    n = 1 << log_n
+    out: list[int] = []
+    for q in list(cat["scale"][(25, n)]) + list(cat["message"][(28, n)]):
+        if q not in out and 4 * q < 2 ** 30 and (q - 1) % (2 * n) == 0:
+            out.append(q)
+    return out[:count]
+
+
 class CkksConfig:
     r"""Immutable CKKS parameters over $\mathbb{Z}[X]/(X^N+1)$.
 

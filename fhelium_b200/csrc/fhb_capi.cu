@@ -369,6 +369,52 @@ int fhb_inverse_ntt(const fhb_context* ctx, const void* in, void* out, int64_t b
   return fhb::inverse(c, in, out, batch * rows, rows, row_start, output_kind, st);
 }
 
+int fhb_tc_ntt_prepare(const fhb_context* ctx) {
+  fhb_stream stream = nullptr;
+  CTX_OR_FAIL();
+  (void)st;
+  (void)c;
+  return fhb::tc_ntt_prepare(*ctx->impl);
+}
+
+static int tc_transform(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                        bool inverse, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(in, "in"));
+  TRY(fhb::check_ptr(out, "out"));
+  if (batch < 0 || rows < 1 || row_start < 0 || row_start + rows > c.qp()) return fail(-4, "row interval out of range");
+  return fhb::tc_ntt(*ctx->impl, in, out, batch * rows, rows, row_start, inverse, st);
+}
+
+int fhb_tc_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                       fhb_stream stream) {
+  return tc_transform(ctx, in, out, batch, rows, row_start, false, stream);
+}
+
+int fhb_tc_inverse_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows, int row_start,
+                       fhb_stream stream) {
+  return tc_transform(ctx, in, out, batch, rows, row_start, true, stream);
+}
+
+int fhb_tc_ntt_status(const fhb_context* ctx, int* flag) {
+  fhb_stream stream = nullptr;
+  CTX_OR_FAIL();
+  (void)st;
+  (void)c;
+  if (!flag) return fail(-2, "flag is NULL");
+  return fhb::tc_ntt_status(*ctx->impl, flag);
+}
+
+int fhb_tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post) {
+  if (!bmat) return fail(-2, "bmat is NULL");
+  if (pass < 0 || pass > 3) return fail(-2, "pass must be 0..3");
+  if (q < 3 || q >= (uint64_t{1} << 28) || !(q & 1) || (q - 1) % (uint64_t{2} << 16) != 0)
+    return fail(-2, "q must be an odd NTT prime below 2^28 for N = 2^16");
+  if (psi == 0 || psi >= q) return fail(-2, "psi out of range");
+  fhb::tc_ntt_tables_host(q, psi, pass, bmat, reinterpret_cast<fhb::TwPair<uint32_t>*>(post));
+  return 0;
+}
+
 int fhb_ckks_multiply(const fhb_context* ctx, const void* a, const void* b, void* out, int64_t batch, int level,
                       fhb_stream stream) {
   CTX_OR_FAIL();

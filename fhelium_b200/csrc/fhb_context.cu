@@ -274,6 +274,7 @@ void destroy_context(Context* c) {
   cudaSetDevice(c->device);
   for (void* p : c->allocations) cudaFree(p);
   cudaSetDevice(prev);
+  delete c->tc;
   delete c;
 }
 

@@ -1,6 +1,7 @@
 // Device-resident tables for one CKKS modulus chain (host-side definition).
 #pragma once
 #include <cstdint>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -47,6 +48,15 @@ struct LevelTables {
   TwPair<T>* rescale_inv = nullptr;  // [QP]: q_level^{-1} mod p (rows > level)
 };
 
+// Tables of the exact int8 tensor-core NTT (int32 residues, N = 2^16), built
+// on first use.  All device arrays are owned through Context::allocations.
+struct TcNttTables {
+  uint8_t* bmat[4] = {};              // per pass: [QP][4 tiles][32 chunks][8192] digit matrices
+  TwPair<uint32_t>* post[2] = {};     // pass-1 twiddles of forward / inverse: [QP][N]
+  uint32_t* qinfo = nullptr;          // [QP][2]: q, -q^{-1} mod 2^32
+  int* err = nullptr;                 // device flag: a bounded wait gave up
+};
+
 struct Context {
   int bits = 0;        // 64 or 32
   int log_n = 0;
@@ -63,6 +73,8 @@ struct Context {
   int ks_order = 0;  // tuning: work order of the key-switch clusters (see ks_work)
   int ntt_ept_fwd = 0;  // tuning: residues per thread of the standalone forward NTT (0 = default)
   int ntt_ept_inv = 0;  // tuning: same for the inverse NTT and the fused HMult -> inverse NTT
+  TcNttTables* tc = nullptr;  // tensor-core NTT tables (null until prepared)
+  std::mutex tc_mutex;
   int qp() const { return num_q + num_p; }
   int n() const { return 1 << log_n; }
 };
@@ -79,6 +91,16 @@ template <>
 inline const LevelTables<uint64_t>& level_tables<uint64_t>(const Context& c, int level) { return c.lv64[level]; }
 template <>
 inline const LevelTables<uint32_t>& level_tables<uint32_t>(const Context& c, int level) { return c.lv32[level]; }
+
+// Exact int8 tensor-core NTT (fhb_tc_ntt.cu).  tc_ntt_prepare builds the
+// tables once (blocking); tc_ntt runs both passes of one direction;
+// tc_ntt_status reads and clears the device error flag (synchronising);
+// tc_ntt_tables_host fills one pass's tables for one prime on the host.
+int tc_ntt_prepare(Context& c);
+int tc_ntt(Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool inverse,
+           cudaStream_t st);
+int tc_ntt_status(Context& c, int* flag);
+void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, TwPair<uint32_t>* post);
 
 // Host-side status plumbing shared by the C ABI.
 void set_error(const std::string& msg);

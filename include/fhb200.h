@@ -88,6 +88,35 @@ int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);
 int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
                     int row_start, int input_montgomery, fhb_stream stream);
 
+/* Exact int8 tensor-core forms of the two transforms above (tcgen05.mma
+ * kind::i8, int32 accumulation in tensor memory): a 256 x 256 four-step
+ * NTT whose two matrix passes run over the residues' four bytes and
+ * byte-split constant matrices, reduced exactly in the epilogue.  int32
+ * contexts with log_n = 16 only (else -7).
+ *   fhb_tc_forward_ntt: standard input -> NTT/Montgomery output, canonical
+ *     [0, q): equal mod q to fhb_forward_ntt(input_montgomery = 0), whose
+ *     output is lazy [0, 2q) (forward_ntt_to_montgomery_compact_grouped_smem_,
+ *     csrc/ops/ntt/forward_ntt.cpp:25-67).
+ *   fhb_tc_inverse_ntt: NTT/Montgomery input (any word value) -> standard
+ *     canonical, bit-identical to fhb_inverse_ntt(output_kind = 2)
+ *     (inverse_ntt_to_standard_compact_grouped_smem_, csrc/ops/ntt/
+ *     inverse_ntt.cpp:23-73).
+ * in == out allowed; no scratch.  The first call builds the constant
+ * matrices (4 MiB per prime, blocking) unless fhb_tc_ntt_prepare ran.
+ * fhb_tc_ntt_status synchronises, returns in *flag whether a bounded wait
+ * inside the kernels gave up since the last call (outputs then invalid),
+ * and clears the flag.  fhb_tc_ntt_tables_host (host only, no device) fills
+ * one pass's byte matrices (1 MiB, the kernels' shared-memory layout) and,
+ * for passes 0 and 2, the N elementwise twiddle pairs (w, floor(w 2^32 / q)),
+ * for a prime q < 2^28 with primitive 2N-th root psi at N = 2^16. */
+int fhb_tc_ntt_prepare(const fhb_context* ctx);
+int fhb_tc_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
+                       int row_start, fhb_stream stream);
+int fhb_tc_inverse_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
+                       int row_start, fhb_stream stream);
+int fhb_tc_ntt_status(const fhb_context* ctx, int* flag);
+int fhb_tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post);
+
 /* Inverse NTT from NTT/Montgomery lazy input, output per fhb_inverse_output.
  * in == out allowed.  Replaces fhelium_ntt_ops.inverse_ntt_{montgomery,
  * to_standard_lazy,to_standard,to_centered}_compact_grouped_smem_
