@@ -40,7 +40,7 @@
 // digits).  The A tile (128 rows x 256 x 4 digit planes = 128 KB) is written
 // once into shared memory by all threads; the B chunks (8 KB each, laid out
 // on the host in the tensor cores' canonical K-major layout) stream through
-// an 8-stage ring by bulk copies; two TMEM accumulator sets of 256 columns
+// a 12-stage ring by bulk copies; two TMEM accumulator sets of 256 columns
 // let the epilogue of tile j overlap the MMAs of tile j + 1.
 //
 // Roles (256 threads): warps 0-3 epilogue (TMEM lanes 32 w .. 32 w + 31),
@@ -64,12 +64,14 @@ constexpr int kTiles = 4;                // 64-column output tiles per CTA
 constexpr int kTileCols = 64;
 constexpr int kChunksPerTile = 32;       // 8 K-chunks x 4 data digits
 constexpr int kChunkBytes = 8192;        // B chunk: 256 (e, column) rows x 32 bytes of K
-constexpr int kStages = 8;
+constexpr int kStages = 12;
 constexpr int kPlaneBytes = kRowsPerCta * kSide;  // one data digit plane of the A tile
 constexpr int kABytes = 4 * kPlaneBytes;
 constexpr int kBBytes = kStages * kChunkBytes;
-constexpr int kBarrierBytes = 256;
+constexpr int kBarrierBytes = 512;  // 2 x 12 + 5 mbarriers, TMEM slot, abort flag
 constexpr int kSmemBytes = 1024 + kABytes + kBBytes + kBarrierBytes;
+static_assert(8 * (2 * kStages + 5) + 8 <= kBarrierBytes, "barrier area too small");
+static_assert(kSmemBytes <= 232448, "shared memory per CTA");
 constexpr int kThreads = 256;
 constexpr int kTmemCols = 512;
 constexpr size_t kPassBytesPerPrime = size_t(kTiles) * kChunksPerTile * kChunkBytes;  // 1 MiB
@@ -116,17 +118,25 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait for the phase of `parity` to complete.  Returns false when
-// the CTA aborted (abort != nullptr) or the time limit passed; the latter
-// raises the abort flag and the device error flag.
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort, int* err) {
-  const unsigned long long t0 = global_ns();
-  for (uint32_t it = 0;; ++it) {
+// the CTA aborted (abort != nullptr) or about one second passed; the latter
+// raises the abort flag and the device error flag.  The global timer is read
+// only every 1024 polls: the common case is a barrier that completes within
+// a few polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort, int* err) {
+  if (mbar_test(bar, parity)) return true;
+  unsigned long long t0 = 0;
+  for (uint32_t it = 1;; ++it) {
     if (mbar_test(bar, parity)) return true;
     if (abort && *abort) return false;
-    if ((it & 63) == 63 && global_ns() - t0 > kWaitNs) {
-      if (abort) *abort = 1;
-      atomicExch(err, 1);
-      return false;
+    if ((it & 1023) == 0) {
+      const unsigned long long t = global_ns();
+      if (t0 == 0) {
+        t0 = t;
+      } else if (t - t0 > kWaitNs) {
+        if (abort) *abort = 1;
+        atomicExch(err, 1);
+        return false;
+      }
     }
   }
 }
@@ -197,7 +207,7 @@ struct PassArgs {
   const uint8_t* bmat;                // [QP][4][32][8192]
   const TwPair<uint32_t>* post;       // [QP][N] or null
   const uint32_t* qinfo;              // [QP][2]
-  int64_t polys;
+  int64_t batch;                      // polynomials per row (polys = batch x rows)
   int rows;
   int row_start;
   int* err;
@@ -216,7 +226,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   const uint32_t a_addr = base;
   const uint32_t b_addr = base + kABytes;
   uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + kABytes + kBBytes);
-  // barrier slots: full[8] empty[8] acc_full[2] acc_empty[2] drain[1]
+  // barrier slots: full[kStages] empty[kStages] acc_full[2] acc_empty[2] drain[1]
   const uint32_t bar0 = smem_addr(bars);
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
   auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
@@ -227,9 +237,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t poly = blockIdx.x >> 1;
+  // prime-major order: consecutive CTAs share a prime, so its constant
+  // matrices stay in L2 while they are streamed
+  const int64_t pair = blockIdx.x >> 1;
+  const int row = int(pair / args.batch);
+  const int64_t poly = (pair - int64_t(row) * args.batch) * args.rows + row;
   const int m0 = (blockIdx.x & 1) * kRowsPerCta;
-  const int prime = args.row_start + int(poly % args.rows);
+  const int prime = args.row_start + row;
   const uint32_t* src = args.in + poly * (int64_t(1) << kLogN);
   uint32_t* dst = args.out + poly * (int64_t(1) << kLogN);
   const uint8_t* bsrc = args.bmat + size_t(prime) * kPassBytesPerPrime;
@@ -272,34 +286,54 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   if (COLUMN) {
     // unit = (row, 16 consecutive k); a warp covers 32 consecutive rows so
     // every load is one 128-byte line and every 16-byte store is conflict-free.
-    for (int u = tid; u < kRowsPerCta * 16; u += kThreads) {
-      const int row = u & (kRowsPerCta - 1), k16 = u >> 7;
-      uint32_t v[16];
+    // Two units per step keep 32 loads per thread in flight.
+    for (int u0 = tid; u0 < kRowsPerCta * 16; u0 += 2 * kThreads) {
+      uint32_t v[2][16];
 #pragma unroll
-      for (int t = 0; t < 16; ++t) v[t] = src[(k16 * 16 + t) * kSide + m0 + row];
-      uint32_t w[4][4];
+      for (int h = 0; h < 2; ++h) {
+        const int u = u0 + h * kThreads, r = u & (kRowsPerCta - 1), k16 = u >> 7;
 #pragma unroll
-      for (int g = 0; g < 4; ++g)
-        byte_transpose(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3], w[0][g], w[1][g], w[2][g], w[3][g]);
-      const uint32_t off = a_offset(row, k16 * 16);
+        for (int t = 0; t < 16; ++t) v[h][t] = src[(k16 * 16 + t) * kSide + m0 + r];
+      }
 #pragma unroll
-      for (int d = 0; d < 4; ++d)
-        *reinterpret_cast<uint4*>(a_tile + d * kPlaneBytes + off) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+      for (int h = 0; h < 2; ++h) {
+        const int u = u0 + h * kThreads, r = u & (kRowsPerCta - 1), k16 = u >> 7;
+        uint32_t w[4][4];
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+          byte_transpose(v[h][4 * g], v[h][4 * g + 1], v[h][4 * g + 2], v[h][4 * g + 3], w[0][g], w[1][g], w[2][g],
+                         w[3][g]);
+        const uint32_t off = a_offset(r, k16 * 16);
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+          *reinterpret_cast<uint4*>(a_tile + d * kPlaneBytes + off) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+      }
     }
   } else {
     // unit = (row, 4 consecutive k); lane = 8 rows x 4 k-quads, so the
-    // 32 four-byte stores of a warp fall in 32 distinct banks.
+    // 32 four-byte stores of a warp fall in 32 distinct banks.  Eight units
+    // per step keep eight 16-byte loads per thread in flight.
     const int r8 = lane >> 2, q4 = lane & 3;
-    for (int wu = warp; wu < 16 * 16; wu += kThreads / 32) {
-      const int row = (wu >> 4) * 8 + r8, k = ((wu & 15) * 4 + q4) * 4;
-      const uint4 v = *reinterpret_cast<const uint4*>(src + (m0 + row) * kSide + k);
-      uint32_t w0, w1, w2, w3;
-      byte_transpose(v.x, v.y, v.z, v.w, w0, w1, w2, w3);
-      const uint32_t off = a_offset(row, k);
-      *reinterpret_cast<uint32_t*>(a_tile + 0 * kPlaneBytes + off) = w0;
-      *reinterpret_cast<uint32_t*>(a_tile + 1 * kPlaneBytes + off) = w1;
-      *reinterpret_cast<uint32_t*>(a_tile + 2 * kPlaneBytes + off) = w2;
-      *reinterpret_cast<uint32_t*>(a_tile + 3 * kPlaneBytes + off) = w3;
+    for (int wu0 = warp; wu0 < 16 * 16; wu0 += 8 * (kThreads / 32)) {
+      uint4 v[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        const int wu = wu0 + h * (kThreads / 32);
+        const int r = (wu >> 4) * 8 + r8, k = ((wu & 15) * 4 + q4) * 4;
+        v[h] = *reinterpret_cast<const uint4*>(src + (m0 + r) * kSide + k);
+      }
+#pragma unroll
+      for (int h = 0; h < 8; ++h) {
+        const int wu = wu0 + h * (kThreads / 32);
+        const int r = (wu >> 4) * 8 + r8, k = ((wu & 15) * 4 + q4) * 4;
+        uint32_t w0, w1, w2, w3;
+        byte_transpose(v[h].x, v[h].y, v[h].z, v[h].w, w0, w1, w2, w3);
+        const uint32_t off = a_offset(r, k);
+        *reinterpret_cast<uint32_t*>(a_tile + 0 * kPlaneBytes + off) = w0;
+        *reinterpret_cast<uint32_t*>(a_tile + 1 * kPlaneBytes + off) = w1;
+        *reinterpret_cast<uint32_t*>(a_tile + 2 * kPlaneBytes + off) = w2;
+        *reinterpret_cast<uint32_t*>(a_tile + 3 * kPlaneBytes + off) = w3;
+      }
     }
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -549,7 +583,7 @@ int launch_pass(const Context& c, const uint32_t* in, uint32_t* out, int pass, i
   using namespace tcntt;
   auto kern = k_tc_ntt_pass<COLUMN, POST>;
   if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), kSmemBytes)) return rc;
-  PassArgs a{in, out, c.tc->bmat[pass], POST ? c.tc->post[pass / 2] : nullptr, c.tc->qinfo, polys, rows,
+  PassArgs a{in, out, c.tc->bmat[pass], POST ? c.tc->post[pass / 2] : nullptr, c.tc->qinfo, polys / rows, rows,
              row_start, c.tc->err};
   kern<<<dim3(unsigned(polys * 2)), kThreads, kSmemBytes, st>>>(a);
   return cuda_status(cudaGetLastError(), "k_tc_ntt_pass");
