@@ -31,6 +31,7 @@ operators) on this workload's config and prints its own JSON line.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -157,6 +158,17 @@ def _time_events(fn, steps, stream):
     return start.elapsed_time(end) / steps
 
 
+def _int8_peak_tops() -> tuple[float, str]:
+    """Dense int8 tensor peak: twice the measured dense bf16 GEMM rate (the
+    B200's dense int8 rate is twice its bf16 rate), else twice the bf16
+    fallback."""
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return 2.0 * float(peaks["bf16_tflops"]), "2 x measured bf16 burst"
+    except Exception:
+        return 2.0 * 1590.0, "2 x fallback bf16"
+
+
 def ntt_int32_primes(count: int = 36, log_n: int = 16) -> list[int]:
     from fhelium_b200.config import int32_ntt_primes
     return int32_ntt_primes(count, log_n)
@@ -200,6 +212,42 @@ def ntt_leg(dev, stream, steps):
         fwd()
         inv()
         out[tag]["roundtrip_bit_exact"] = bool(torch.equal(x, z))
+    # exact int8 tensor-core form: two 256 x 256 x 256 passes per direction
+    # over 4 x 4 byte-digit products; 2 N (n1 + n2) d_a d_b int8 operations
+    # per limb-polynomial and direction
+    tc = {}
+    nat.check(ctx.lib.fhb_tc_ntt_prepare(ctx.handle), "tc prepare")
+    tfwd = lambda: nat.check(ctx.lib.fhb_tc_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), B, L, 0, s), "tc ntt")
+    tinv = lambda: nat.check(ctx.lib.fhb_tc_inverse_ntt(ctx.handle, y.data_ptr(), z.data_ptr(), B, L, 0, s), "tc intt")
+    for _ in range(3):
+        tfwd()
+        tinv()
+    tc["forward_ms"] = _time_events(tfwd, max(3, steps), stream)
+    tc["inverse_ms"] = _time_events(tinv, max(3, steps), stream)
+    y_tc = torch.empty_like(x)
+    nat.check(ctx.lib.fhb_tc_forward_ntt(ctx.handle, x.data_ptr(), y_tc.data_ptr(), B, L, 0, s), "tc ntt")
+    fwd()  # CUDA-core forward into y
+    tc["forward_equals_plain_mod_q"] = bool(torch.equal(y_tc.to(torch.int64), y.to(torch.int64) % q))
+    z.zero_()
+    nat.check(ctx.lib.fhb_tc_inverse_ntt(ctx.handle, y.data_ptr(), z.data_ptr(), B, L, 0, s), "tc intt")
+    tc["inverse_of_plain_bit_exact"] = bool(torch.equal(x, z))
+    z.zero_()
+    nat.check(ctx.lib.fhb_tc_inverse_ntt(ctx.handle, y_tc.data_ptr(), z.data_ptr(), B, L, 0, s), "tc intt")
+    tc["roundtrip_bit_exact"] = bool(torch.equal(x, z))
+    flag = ctypes.c_int(-1)
+    nat.check(ctx.lib.fhb_tc_ntt_status(ctx.handle, ctypes.byref(flag)), "tc status")
+    tc["wait_timeouts"] = flag.value
+    int8_ops = B * L * 2 * N * (256 + 256) * 4 * 4
+    int8_peak, src = _int8_peak_tops()
+    tc["int8_tops_forward"] = int8_ops / (tc["forward_ms"] / 1e3) / 1e12
+    tc["int8_tops_inverse"] = int8_ops / (tc["inverse_ms"] / 1e3) / 1e12
+    tc["int8_peak_tops"] = int8_peak
+    tc["int8_peak_source"] = src
+    tc["tensor_frac_forward"] = tc["int8_tops_forward"] / int8_peak
+    tc["tensor_frac_inverse"] = tc["int8_tops_inverse"] / int8_peak
+    tc["forward_gbs"] = nbytes / (tc["forward_ms"] / 1e3) / 1e9
+    tc["inverse_gbs"] = nbytes / (tc["inverse_ms"] / 1e3) / 1e9
+    out["tensor_core"] = tc
     # integer-pipe roof: Shoup products per transform (N/2 log N butterflies
     # + the N x R or x N^-1 pass) against the int32 probe's rate
     probe_out = torch.empty(148 * 8 * 256, dtype=torch.int32, device=dev)
