@@ -48,7 +48,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PRESET = "slots32768_scale40_levels34_int64"
-KS_TRAFFIC_BYTES_PER_CIPHERTEXT = 1275.17e6 / 2  # ncu, k_keyswitch_core, batch 2 (profiles/)
+KS_TRAFFIC_BYTES_BATCH32 = 12741399552 + 2934590720  # ncu dram read + write, k_keyswitch_core, batch 32 (profiles/)
 METRIC = "hmult_relin_rescale_ops_per_s_logN16_L35"
 UNIT = "ops/s"
 CONFIG = {
@@ -605,11 +605,12 @@ def main() -> int:
     modmul_peak = 148 * 8 * 256 * 8 * probe_iters / (probe_ms / 1000.0)
     modmul_achieved = ks_modmul / (per_kernel["keyswitch_core"] / 1000.0)
     step_bytes = B * (4 * L + 2 * (L - 1)) * limb + 10 * 2 * (L + cfg.num_p_primes) * limb
-    # DRAM bytes of one k_keyswitch_core launch: 1275 MB measured by ncu
-    # (dram__bytes_read.sum + dram__bytes_write.sum) on a batch-2 launch, work
-    # order 0; the key is streamed again for every ciphertext, so the traffic
-    # scales with the batch and is scaled here by the units processed.
-    traffic = KS_TRAFFIC_BYTES_PER_CIPHERTEXT * B if cfg.logN == 16 and L == 35 else None
+    # DRAM bytes of one k_keyswitch_core launch: 15.7 GB measured by ncu
+    # (dram__bytes_read.sum + dram__bytes_write.sum) on the batch-32 launch of
+    # this command, work order 2 (groups of four ciphertexts share the key
+    # rows); every destination row re-reads the digit rows of its group, so
+    # the traffic grows with the batch and is scaled by the units processed.
+    traffic = KS_TRAFFIC_BYTES_BATCH32 * B / 32 if cfg.logN == 16 and L == 35 else None
 
     extras = {}
     if not args.no_extras:

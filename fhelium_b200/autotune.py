@@ -6,7 +6,9 @@ The knobs a run can change without recompiling:
   clusters, 0 = the limbs of one ciphertext back to back (the digits of one
   ciphertext stay in L2 while its limbs are processed), 1 = one limb across
   the batch back to back (the key rows of one prime are shared by the whole
-  batch, which pays when every item uses the same key);
+  batch, which pays when every item uses the same key), 2 = one limb across
+  a group of four ciphertexts, group by group (both the key rows of the limb
+  and the group's digits stay in L2);
 * ``streams``: how many graph branches the mixed-batch executor spreads its
   (kind, level) groups over, i.e. how many groups run side by side;
 * ``ntt_forward_ept`` / ``ntt_inverse_ept`` (FHB_TUNE_NTT_{FORWARD,INVERSE}_EPT):
@@ -129,7 +131,7 @@ def tune_ntt(ctx, x: torch.Tensor, rows: int, row_start: int = 0, *, candidates:
     return dict(entry, cached=False)
 
 
-def tune_mixed_batch(engine, executor, *, ks_orders: Iterable[int] = (0, 1), streams: Iterable[int] = (1, 2, 3, 4),
+def tune_mixed_batch(engine, executor, *, ks_orders: Iterable[int] = (0, 1, 2), streams: Iterable[int] = (1, 2, 3, 4),
                      repeats: int = 3, cache_path: str | None = None, use_cache: bool = True) -> dict:
     """Pick (ks_order, streams) for `executor` by timing graph replays.
 

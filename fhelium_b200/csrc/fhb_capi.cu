@@ -327,7 +327,7 @@ int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
   if (!ctx || !ctx->impl) return fail(-1, "context is NULL");
   switch (param) {
     case FHB_TUNE_KS_ORDER:
-      if (value != 0 && value != 1) return fail(-2, "key-switch work order must be 0 or 1");
+      if (value < 0 || value > 2) return fail(-2, "key-switch work order must be 0, 1 or 2");
       ctx->impl->ks_order = value;
       return 0;
     case FHB_TUNE_NTT_FORWARD_EPT:

@@ -70,7 +70,7 @@ struct Context {
   std::vector<LevelTables<uint64_t>> lv64;
   std::vector<LevelTables<uint32_t>> lv32;
   std::vector<void*> allocations;
-  int ks_order = 0;  // tuning: work order of the key-switch clusters (see ks_work)
+  int ks_order = 2;  // tuning: work order of the key-switch clusters (see ks_work)
   int ntt_ept_fwd = 0;  // tuning: residues per thread of the standalone forward NTT (0 = default)
   int ntt_ept_inv = 0;  // tuning: same for the inverse NTT and the fused HMult -> inverse NTT
   TcNttTables* tc = nullptr;  // tensor-core NTT tables (null until prepared)

@@ -385,16 +385,32 @@ struct ExtSource {
 // Work order of the per-(ciphertext, row) clusters of the key-switch kernels:
 // order 0 runs the rows of one ciphertext back to back; order 1 runs row j of
 // every ciphertext back to back, so concurrently resident clusters read the
-// same key rows (chosen by the autotuner).
+// same key rows; order 2 runs row j of a group of kKsGroup ciphertexts back
+// to back, group by group, so both the key rows of j (shared by the group)
+// and the group's digit rows (read for every destination row) stay in L2
+// (chosen by the autotuner).
+constexpr int kKsGroup = 4;
 __device__ __forceinline__ void ks_work(int64_t cluster, int qp_limbs, int64_t batch, int order, int64_t& poly,
                                         int64_t& bi, int& jrow) {
   if (order == 0) {
     poly = cluster;
     bi = poly / qp_limbs;
     jrow = int(poly % qp_limbs);
-  } else {
+  } else if (order == 1) {
     jrow = int(cluster / batch);
     bi = cluster % batch;
+    poly = bi * qp_limbs + jrow;
+  } else {
+    const int64_t full = batch - batch % kKsGroup;  // ciphertexts in whole groups
+    if (cluster < full * qp_limbs) {
+      const int64_t g = cluster / (int64_t(qp_limbs) * kKsGroup), r = cluster % (int64_t(qp_limbs) * kKsGroup);
+      jrow = int(r / kKsGroup);
+      bi = g * kKsGroup + r % kKsGroup;
+    } else {
+      const int64_t c2 = cluster - full * qp_limbs, rest = batch - full;
+      jrow = int(c2 / rest);
+      bi = full + c2 % rest;
+    }
     poly = bi * qp_limbs + jrow;
   }
 }

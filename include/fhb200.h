@@ -68,7 +68,8 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
 
 /* Launch tuning of a context (set by the autotuner, fhelium_b200/autotune.py).
  * FHB_TUNE_KS_ORDER: work order of the key-switch clusters, 0 = the rows of
- * one ciphertext back to back, 1 = one row across the batch back to back.
+ * one ciphertext back to back, 1 = one row across the batch back to back,
+ * 2 = one row across a group of four ciphertexts, group by group (default).
  * FHB_TUNE_NTT_FORWARD_EPT / FHB_TUNE_NTT_INVERSE_EPT: residues per thread of
  * the standalone forward / inverse NTT (and of the fused HMult -> inverse
  * NTT): 8 = radix-8 register passes, 16 = radix-16 passes over half the

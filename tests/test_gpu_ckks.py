@@ -64,6 +64,27 @@ def test_relinearize_matches_oracle(family, log_n, level):
     np.testing.assert_array_equal(to_np(got.data), want)
 
 
+@pytest.mark.parametrize("family,log_n,level", CASES[:2])
+def test_keyswitch_work_orders_agree(family, log_n, level):
+    """Every key-switch work order (rows of one ciphertext, one row across the
+    batch, one row across groups of four) gives the same result; batch 6
+    leaves a partial group for order 2."""
+    cfg, eng, orc, rng = _setup(family, log_n, level, 4)
+    rows = orc.q_rows(level)
+    ct3 = uniform_residues(rng, cfg.moduli, rows, (3, 6), cfg.N, lazy=True)
+    key = random_key(rng, cfg, cfg.N)
+    rlk = RelinearizationKey(to_dev(key, cfg))
+    outs = []
+    for order in (0, 1, 2):
+        eng.ctx.set_tuning(nat.TUNE_KS_ORDER, order)
+        got = eng.relinearize(Ciphertext(to_dev(ct3, cfg), level, 1.0, "ntt", "montgomery"), rlk)
+        outs.append(to_np(got.data))
+    eng.ctx.set_tuning(nat.TUNE_KS_ORDER, 0)
+    np.testing.assert_array_equal(outs[0][:, 5], orc.relinearize(ct3[:, 5], key, level))
+    np.testing.assert_array_equal(outs[1], outs[0])
+    np.testing.assert_array_equal(outs[2], outs[0])
+
+
 @pytest.mark.parametrize("ept", [0, 16])
 @pytest.mark.parametrize("family,log_n,level", CASES)
 def test_fused_multiply_relinearize_rescale_matches_oracle(family, log_n, level, ept):
