@@ -407,7 +407,7 @@ int fhb_tc_ntt_status(const fhb_context* ctx, int* flag) {
 
 int fhb_tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post) {
   if (!bmat) return fail(-2, "bmat is NULL");
-  if (pass < 0 || pass > 3) return fail(-2, "pass must be 0..3");
+  if (pass < 0 || pass > 5) return fail(-2, "pass must be 0..5");
   if (q < 3 || q >= (uint64_t{1} << 28) || !(q & 1) || (q - 1) % (uint64_t{2} << 16) != 0)
     return fail(-2, "q must be an odd NTT prime below 2^28 for N = 2^16");
   if (psi == 0 || psi >= q) return fail(-2, "psi out of range");

@@ -51,8 +51,8 @@ struct LevelTables {
 // Tables of the exact int8 tensor-core NTT (int32 residues, N = 2^16), built
 // on first use.  All device arrays are owned through Context::allocations.
 struct TcNttTables {
-  uint8_t* bmat[4] = {};              // per pass: [QP][4 tiles][32 chunks][8192] digit matrices
-  TwPair<uint32_t>* post[2] = {};     // pass-1 twiddles of forward / inverse: [QP][N]
+  uint8_t* bmat[6] = {};              // per pass: [QP][byte matrix of the pass] (64 KiB or 4 KiB per prime)
+  TwPair<uint32_t>* post[6] = {};     // per pass with a twiddle: [QP][N] in output order, else null
   uint32_t* qinfo = nullptr;          // [QP][2]: q, -q^{-1} mod 2^32
   int* err = nullptr;                 // device flag: a bounded wait gave up
 };
@@ -100,6 +100,7 @@ int tc_ntt_prepare(Context& c);
 int tc_ntt(Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool inverse,
            cudaStream_t st);
 int tc_ntt_status(Context& c, int* flag);
+size_t tc_ntt_table_bytes(int pass);
 void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, TwPair<uint32_t>* post);
 
 // Host-side status plumbing shared by the C ABI.

@@ -1,54 +1,53 @@
 // Exact integer tensor-core NTT for int32 residues (q < 2^28) at N = 2^16 on
 // the 5th-generation tensor cores: tcgen05.mma kind::i8 with int32
-// accumulators in tensor memory (TMEM), operands staged in shared memory.
+// accumulators in tensor memory (TMEM), operands in shared memory.
 //
-// Four-step form with N = 256 x 256.  Write the polynomial as the row-major
-// matrix X[i1][i2] = x[256 i1 + i2] and the output (bit-reversed order, as
-// the CUDA-core form and the reference: out[k] = sum_n x[n] psi^{(2 br16(k)
-// + 1) n}, csrc/ops/ntt/forward_ntt.cpp:15-21) as O[r][c] = out[256 r + c].
-// With br16(256 r + c) = br8(r) + 256 br8(c) and psi^{2N} = 1,
+// Three-pass form, N = 64 x 64 x 16.  Write the input index as
+// n = 1024 i1 + 16 i2 + i3 and the output position (bit-reversed order, as
+// the CUDA-core form and the reference: out[p] = sum_n x[n] psi^{(2 br16(p) +
+// 1) n}, csrc/ops/ntt/forward_ntt.cpp:15-21) as p = 1024 P1 + 16 P2 + P3, so
+// br16(p) = m1 + 64 m2 + 4096 m3 with m1 = br6(P1), m2 = br6(P2), m3 = br4(P3).
+// Expanding (2 br16(p) + 1) n modulo 2N and dropping the multiples of 2N:
 //
-//   Y[r][i2] = T1[r][i2] sum_i1 W1[r][i1] X[i1][i2]     (forward pass 1)
-//   O[r][c]  = sum_i2 Y[r][i2] W2[i2][c]                (forward pass 2)
+//   pass 1: Y1[P1][i2][i3] = R psi^{16 i2 (2 m1 + 1)} sum_i1 x[i1][i2][i3] psi^{1024 i1 (2 m1 + 1)}
+//   pass 2: Y2[P1][P2][i3] = psi^{(2 m1 + 1) i3 + 128 m2 i3} sum_i2 Y1[P1][i2][i3] psi^{2048 m2 i2}
+//   pass 3: out[P1][P2][P3] = sum_i3 Y2[P1][P2][i3] psi^{8192 m3 i3}
 //
-//   W1[r][i1] = psi^{256 i1 (2 br8(r) + 1)},  T1[r][i2] = R psi^{i2 (2 br8(r) + 1)},
-//   W2[i2][c] = psi^{512 i2 br8(c)}           (R = 2^30: Montgomery output).
+// (R = 2^30: Montgomery output).  The inverse runs the passes in the opposite
+// order with psi^{-1}; its first pass carries N^{-1} R^{-1}.
 //
-// The inverse runs the two passes backwards with psi^{-1}; its first pass
-// carries N^{-1} R^{-1} (Montgomery input, standard output):
-//
-//   E[r][i2]  = T1'[r][i2] sum_c O[r][c] W2'[c][i2],    W2'[c][i2] = psi^{-512 br8(c) i2}
-//   x[i1][i2] = sum_r W1'[i1][r] E[r][i2],              W1'[i1][r] = psi^{-256 i1 (2 br8(r) + 1)}
-//   T1'[r][i2] = N^{-1} R^{-1} psi^{-i2 (2 br8(r) + 1)}.
-//
-// Every pass is one GEMM D[m][n] = sum_k A[m][k] B[k][n] mod q with the data
-// as A (rows m) and the constant matrix as B; a pass whose data index k runs
-// along memory rows reads A transposed ("column" passes: forward 1, inverse
-// 2), the others read it row-wise; D is stored in the orientation the next
-// pass reads.  The product is exact with unsigned 8-bit digits: the data
-// splits into its four bytes A = sum_d 2^{8d} A_d, the constant side is
-// pre-scaled per data digit, B^(d) = 2^{8d} 2^{32} B mod q, and split into
-// bytes B^(d) = sum_e 2^{8e} B^(d)_e.  Tensor-core accumulator e collects
-// sum_d A_d B^(d)_e (4 x 256 products of bytes: < 2^26, exact in int32), the
-// epilogue forms S = sum_e 2^{8e} acc_e < 2^51 and one Montgomery reduction
-// by 2^32 returns S 2^{-32} = (A B mod q) in [0, 2q); the optional
+// Every pass is a batch of independent length-n products
+// D[m][n] = sum_k A[m][k] W[k][n] mod q over "instances" m (n = 64 or 16
+// outputs per instance); an instance's k-th input and n-th output sit at
+// f(m) + k S and f(m) + n S in the polynomial, with f and S fixed per pass
+// (pass 1: f(m) = m, S = 1024; pass 2: f(m) = (m / 16) 1024 + m % 16,
+// S = 16; pass 3: f(m) = 16 m, S = 1).  The product is exact with unsigned
+// 8-bit digits: the residues split into their four bytes A = sum_d 2^{8d} A_d,
+// the constant matrix is pre-scaled per data byte, W^(d) = 2^{8d} 2^{32} W mod
+// q, and split into bytes W^(d) = sum_e 2^{8e} W^(d)_e.  Tensor-core
+// accumulator e collects sum_{d,k} A_d W^(d)_e (K = 4 n byte products,
+// < 2^24), the epilogue forms S = sum_e 2^{8e} acc_e < 2^49 and one
+// Montgomery reduction by 2^32 returns (A W mod q) in [0, 2q); the optional
 // elementwise twiddle is a Shoup product and the result is made canonical.
 //
-// CTA = 128 rows (m) of one polynomial x all 256 output columns, in four
-// tiles of 64 columns.  One MMA is M = 128, N = 256 (the 4 twiddle bytes e
-// x 64 columns), K = 32 bytes; a tile is 32 MMAs (8 K-chunks x 4 data
-// digits).  The A tile (128 rows x 256 x 4 digit planes = 128 KB) is written
-// once into shared memory by all threads; the B chunks (8 KB each, laid out
-// on the host in the tensor cores' canonical K-major layout) stream through
-// a 12-stage ring by bulk copies; two TMEM accumulator sets of 256 columns
-// let the epilogue of tile j overlap the MMAs of tile j + 1.
-//
-// Roles (256 threads): warps 0-3 epilogue (TMEM lanes 32 w .. 32 w + 31),
-// warp 4 lane 0 bulk-copy producer, warp 5 TMEM owner and lane 0 MMA issuer.
-// Every mbarrier wait is bounded (about one second of the global timer); a
-// wait that gives up sets a CTA abort flag that releases every other wait,
-// raises the device error flag, and the CTA drains its own bulk copies and
-// MMAs (again with bounded waits) before it frees TMEM and exits.
+// The constant matrix of a pass is small enough to stay in shared memory (64
+// KiB for n = 64, 4 KiB for n = 16), so a persistent CTA loads it once per
+// prime and then streams units of 128 instances of that prime through a
+// double-buffered pipeline:
+//   producer (warp 8, lane 0): bulk copies of a unit's raw words into a raw
+//       buffer (one copy for contiguous units, one per k row otherwise);
+//   transposers (warps 4-7): raw words -> the four byte planes of the A tile
+//       (K-major canonical layout, K = 4 n bytes: [A_0 | A_1 | A_2 | A_3]);
+//   MMA issuer (warp 9, lane 0): n / 8 MMAs of M = 128, N = 4 n (twiddle bytes
+//       e x n outputs), K = 32 into one of two TMEM accumulator sets;
+//   epilogue (warps 0-3, TMEM lane quarter w): recombination, twiddle, store.
+// Raw buffers, A tiles and accumulator sets alternate between two slots, so
+// the copies of unit i + 1, the transposition and MMAs of unit i and the
+// epilogue of unit i - 1 overlap.  Every mbarrier wait is bounded (about one
+// second of the global timer); a wait that gives up sets a CTA abort flag that
+// releases every other wait and raises the device error flag, and the CTA
+// drains its own bulk copies and MMAs (again with bounded waits) before it
+// frees TMEM and exits.
 #include <cstring>
 #include <vector>
 
@@ -58,29 +57,41 @@ namespace fhb {
 namespace tcntt {
 
 constexpr int kLogN = 16;
-constexpr int kSide = 256;
-constexpr int kRowsPerCta = 128;
-constexpr int kTiles = 4;                // 64-column output tiles per CTA
-constexpr int kTileCols = 64;
-constexpr int kChunksPerTile = 32;       // 8 K-chunks x 4 data digits
-constexpr int kChunkBytes = 8192;        // B chunk: 256 (e, column) rows x 32 bytes of K
-constexpr int kStages = 12;
-constexpr int kPlaneBytes = kRowsPerCta * kSide;  // one data digit plane of the A tile
-constexpr int kABytes = 4 * kPlaneBytes;
-constexpr int kBBytes = kStages * kChunkBytes;
-constexpr int kBarrierBytes = 512;  // 2 x 12 + 5 mbarriers, TMEM slot, abort flag
-constexpr int kSmemBytes = 1024 + kABytes + kBBytes + kBarrierBytes;
-static_assert(8 * (2 * kStages + 5) + 8 <= kBarrierBytes, "barrier area too small");
-static_assert(kSmemBytes <= 232448, "shared memory per CTA");
-constexpr int kThreads = 256;
-constexpr int kTmemCols = 512;
-constexpr size_t kPassBytesPerPrime = size_t(kTiles) * kChunksPerTile * kChunkBytes;  // 1 MiB
+constexpr int kPolyWords = 1 << kLogN;
+constexpr int kUnit = 128;                // instances per unit (MMA M)
+constexpr int kThreads = 320;             // 10 warps
+constexpr int kProducerWarp = 8;
+constexpr int kMmaWarp = 9;
+constexpr int kTransposeWarps = 4;        // warps 4..7
+constexpr int kEpilogueWarps = 4;         // warps 0..3
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
+// Pass geometry: NK = outputs (and inputs) per instance.
+template <int NK>
+struct Geom {
+  static constexpr int kKBytes = 4 * NK;                 // K of the concatenated digit planes
+  static constexpr int kNmma = 4 * NK;                   // MMA N: 4 twiddle bytes x NK outputs
+  static constexpr int kSteps = kKBytes / 32;            // MMAs per unit
+  static constexpr int kSbo = kKBytes / 16 * 128;        // 8-row group stride (A and B)
+  static constexpr int kBBytes = kNmma * kKBytes;        // constant byte matrix
+  static constexpr int kABytes = kUnit * kKBytes;        // one A tile
+  static constexpr int kRawBytes = kUnit * NK * 4;       // one unit's raw words
+  static constexpr int kTmemCols = 2 * kNmma;            // two accumulator sets
+  static constexpr int kUnitsPerPoly = (kPolyWords / NK) / kUnit;
+};
+
+constexpr int kBarrierBytes = 256;
+// smem: [B | raw 0 | raw 1 | A 0 | A 1 | barriers]
+template <int NK>
+constexpr int smem_bytes() {
+  return 1024 + Geom<NK>::kBBytes + 2 * Geom<NK>::kRawBytes + 2 * Geom<NK>::kABytes + kBarrierBytes;
+}
+static_assert(smem_bytes<64>() <= 232448, "shared memory per CTA");
+
 // tcgen05 instruction descriptor: D int32 (c_format 2 at bit 4), A and B
-// unsigned 8-bit (formats 0), both K-major, N = 256 (N >> 3 at bit 17),
-// M = 128 (M >> 4 at bit 24).
-constexpr uint32_t kInstrDesc = (2u << 4) | ((256u >> 3) << 17) | ((128u >> 4) << 24);
+// unsigned 8-bit (formats 0), both K-major, N (N >> 3 at bit 17), M = 128
+// (M >> 4 at bit 24).
+constexpr uint32_t instr_desc(uint32_t n) { return (2u << 4) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
 
 // ---------------------------------------------------------------- device ---
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -141,6 +152,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
   }
 }
 
+// A warp-uniform bounded wait: lane 0 polls and broadcasts the verdict, so
+// warp-collective instructions after it run with all 32 lanes or none.
+__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, volatile int* abort, int* err, int lane) {
+  return __shfl_sync(0xffffffffu, lane == 0 ? mbar_wait(bar, parity, abort, err) : false, 0);
+}
+
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
                "l"(src), "r"(bytes), "r"(bar)
@@ -156,13 +173,14 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
 }
 
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t accumulate) {
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                       uint32_t accumulate) {
   const uint32_t mask = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
-      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(kInstrDesc), "r"(accumulate), "r"(mask));
+      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -195,76 +213,101 @@ __device__ __forceinline__ void byte_transpose(uint32_t v0, uint32_t v1, uint32_
   o3 = __byte_perm(b, e, 0x7632);
 }
 
-// Offset of byte (row, k) of one digit plane of the A tile (rows 0..127,
-// k 0..255): core matrix (row / 8, k / 16) at (row / 8) * 2048 + (k / 16) * 128.
-__device__ __forceinline__ uint32_t a_offset(int row, int k) {
-  return uint32_t((row & 7) * 16 + (row >> 3) * 2048 + (k >> 4) * 128 + (k & 15));
+// Instance map of a pass kind (1: f(m) = m, S = 1024; 2: f(m) = (m / 16)
+// 1024 + m % 16, S = 16; 3: f(m) = 16 m, S = 1): offset of instance m within
+// a polynomial, and the stride between its successive inputs / outputs.
+template <int KIND>
+__device__ __forceinline__ int inst_offset(int m) {
+  if (KIND == 1) return m;
+  if (KIND == 2) return (m >> 4) * 1024 + (m & 15);
+  return m * 16;
+}
+template <int KIND>
+constexpr int inst_stride() {
+  return KIND == 1 ? 1024 : (KIND == 2 ? 16 : 1);
+}
+
+// Word index of input k of local instance ml in a unit's raw buffer:
+// kind 1 keeps one 128-word row per k, kinds 2 and 3 copy the unit's
+// contiguous span as it lies in the polynomial.
+template <int KIND, int NK>
+__device__ __forceinline__ int raw_index(int ml, int k) {
+  if (KIND == 1) return k * kUnit + ml;
+  if (KIND == 2) return (ml >> 4) * 1024 + k * 16 + (ml & 15);
+  return ml * NK + k;
 }
 
 struct PassArgs {
   const uint32_t* in;
   uint32_t* out;
-  const uint8_t* bmat;                // [QP][4][32][8192]
-  const TwPair<uint32_t>* post;       // [QP][N] or null
+  const uint8_t* bmat;                // [QP][byte matrix]
+  const TwPair<uint32_t>* post;       // [QP][N] in output order, or null
   const uint32_t* qinfo;              // [QP][2]
   int64_t batch;                      // polynomials per row (polys = batch x rows)
   int rows;
   int row_start;
+  int ctas_per_row;
   int* err;
 };
 
-// COLUMN: A[m][k] = in[k * 256 + m] and D[m][n] -> out[n * 256 + m];
-// otherwise A[m][k] = in[m * 256 + k] and D[m][n] -> out[m * 256 + n].
-// in == out is allowed (plain loads: a CTA reads its slab before it writes it).
-template <bool COLUMN, bool POST>
+// in == out is allowed: a unit's outputs occupy exactly the words its raw
+// copy read, and a unit's output is written only after its raw copy landed.
+template <int KIND, int NK, bool POST>
 __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
+  using G = Geom<NK>;
+  constexpr int S = inst_stride<KIND>();
   extern __shared__ uint8_t smem_raw[];
-  const uint32_t raw = smem_addr(smem_raw);
-  const uint32_t base = (raw + 1023u) & ~1023u;
-  uint8_t* const gbase = smem_raw + (base - raw);
-  uint8_t* const a_tile = gbase;
-  const uint32_t a_addr = base;
-  const uint32_t b_addr = base + kABytes;
-  uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + kABytes + kBBytes);
-  // barrier slots: full[kStages] empty[kStages] acc_full[2] acc_empty[2] drain[1]
+  const uint32_t raw0 = smem_addr(smem_raw);
+  const uint32_t base = (raw0 + 1023u) & ~1023u;
+  uint8_t* const gbase = smem_raw + (base - raw0);
+  const uint32_t b_addr = base;
+  const uint32_t rawbuf_addr = base + G::kBBytes;
+  const uint32_t* const rawbuf = reinterpret_cast<const uint32_t*>(gbase + G::kBBytes);
+  const uint32_t a_addr = base + G::kBBytes + 2 * G::kRawBytes;
+  uint8_t* const a_tile = gbase + G::kBBytes + 2 * G::kRawBytes;
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + G::kBBytes + 2 * G::kRawBytes + 2 * G::kABytes);
   const uint32_t bar0 = smem_addr(bars);
-  auto full_bar = [&](int s) { return bar0 + 8u * s; };
-  auto empty_bar = [&](int s) { return bar0 + 8u * (kStages + s); };
-  auto accf_bar = [&](int b) { return bar0 + 8u * (2 * kStages + b); };
-  auto acce_bar = [&](int b) { return bar0 + 8u * (2 * kStages + 2 + b); };
-  const uint32_t drain_bar = bar0 + 8u * (2 * kStages + 4);
-  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(gbase + kABytes + kBBytes + 8 * (2 * kStages + 5));
+  // barriers: b_full, raw_full[2], raw_empty[2], a_full[2], a_empty[2], acc_full[2], acc_empty[2], drain
+  const uint32_t bfull_bar = bar0;
+  auto rawf_bar = [&](int b) { return bar0 + 8u * (1 + b); };
+  auto rawe_bar = [&](int b) { return bar0 + 8u * (3 + b); };
+  auto af_bar = [&](int b) { return bar0 + 8u * (5 + b); };
+  auto ae_bar = [&](int b) { return bar0 + 8u * (7 + b); };
+  auto accf_bar = [&](int b) { return bar0 + 8u * (9 + b); };
+  auto acce_bar = [&](int b) { return bar0 + 8u * (11 + b); };
+  const uint32_t drain_bar = bar0 + 8u * 13;
+  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // prime-major order: consecutive CTAs share a prime, so its constant
-  // matrices stay in L2 while they are streamed
-  const int64_t pair = blockIdx.x >> 1;
-  const int row = int(pair / args.batch);
-  const int64_t poly = (pair - int64_t(row) * args.batch) * args.rows + row;
-  const int m0 = (blockIdx.x & 1) * kRowsPerCta;
+  // CTA -> (prime row, contiguous range of its units); a unit = (polynomial
+  // of the row, block of 128 instances)
+  const int row = blockIdx.x / args.ctas_per_row, part = blockIdx.x % args.ctas_per_row;
+  const int64_t units = args.batch * G::kUnitsPerPoly;
+  const int64_t u_begin = units * part / args.ctas_per_row, u_end = units * (part + 1) / args.ctas_per_row;
+  const int nu = int(u_end - u_begin);
   const int prime = args.row_start + row;
-  const uint32_t* src = args.in + poly * (int64_t(1) << kLogN);
-  uint32_t* dst = args.out + poly * (int64_t(1) << kLogN);
-  const uint8_t* bsrc = args.bmat + size_t(prime) * kPassBytesPerPrime;
+  auto unit_poly = [&](int i) { return ((u_begin + i) / G::kUnitsPerPoly) * args.rows + row; };
+  auto unit_m0 = [&](int i) { return int((u_begin + i) % G::kUnitsPerPoly) * kUnit; };
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(full_bar(s), 1);
-      mbar_init(empty_bar(s), 1);
-    }
+    mbar_init(bfull_bar, 1);
     for (int b = 0; b < 2; ++b) {
+      mbar_init(rawf_bar(b), 1);
+      mbar_init(rawe_bar(b), kTransposeWarps);
+      mbar_init(af_bar(b), kTransposeWarps);
+      mbar_init(ae_bar(b), 1);
       mbar_init(accf_bar(b), 1);
-      mbar_init(acce_bar(b), 4);
+      mbar_init(acce_bar(b), kEpilogueWarps);
     }
     mbar_init(drain_bar, 1);
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 5) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
-                 "r"(kTmemCols));
+                 "r"(G::kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -272,144 +315,136 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  // The producer starts the B ring before the A tile is staged.
-  int issued = 0;
-  const bool producer = warp == 4 && lane == 0;
-  if (producer) {
-    for (; issued < kStages; ++issued) {
-      mbar_expect_tx(full_bar(issued), kChunkBytes);
-      bulk_load(b_addr + issued * kChunkBytes, bsrc + size_t(issued) * kChunkBytes, kChunkBytes, full_bar(issued));
-    }
-  }
-
-  // Stage the A tile: four byte planes of rows m0 .. m0 + 127.
-  if (COLUMN) {
-    // unit = (row, 16 consecutive k); a warp covers 32 consecutive rows so
-    // every load is one 128-byte line and every 16-byte store is conflict-free.
-    // Two units per step keep 32 loads per thread in flight.
-    for (int u0 = tid; u0 < kRowsPerCta * 16; u0 += 2 * kThreads) {
-      uint32_t v[2][16];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int u = u0 + h * kThreads, r = u & (kRowsPerCta - 1), k16 = u >> 7;
-#pragma unroll
-        for (int t = 0; t < 16; ++t) v[h][t] = src[(k16 * 16 + t) * kSide + m0 + r];
-      }
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int u = u0 + h * kThreads, r = u & (kRowsPerCta - 1), k16 = u >> 7;
-        uint32_t w[4][4];
-#pragma unroll
-        for (int g = 0; g < 4; ++g)
-          byte_transpose(v[h][4 * g], v[h][4 * g + 1], v[h][4 * g + 2], v[h][4 * g + 3], w[0][g], w[1][g], w[2][g],
-                         w[3][g]);
-        const uint32_t off = a_offset(r, k16 * 16);
-#pragma unroll
-        for (int d = 0; d < 4; ++d)
-          *reinterpret_cast<uint4*>(a_tile + d * kPlaneBytes + off) = make_uint4(w[d][0], w[d][1], w[d][2], w[d][3]);
+  if (warp == kProducerWarp && lane == 0) {
+    // constants once, then each unit's raw words
+    const uint8_t* bsrc = args.bmat + size_t(prime) * G::kBBytes;
+    constexpr int kPiece = G::kBBytes < 16384 ? G::kBBytes : 16384;
+    mbar_expect_tx(bfull_bar, G::kBBytes);
+    for (int o = 0; o < G::kBBytes; o += kPiece) bulk_load(b_addr + o, bsrc + o, kPiece, bfull_bar);
+    int i = 0;
+    for (; i < nu; ++i) {
+      const int b = i & 1;
+      if (i >= 2 && !mbar_wait(rawe_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err)) break;
+      const uint32_t* src = args.in + unit_poly(i) * int64_t(kPolyWords) + inst_offset<KIND>(unit_m0(i));
+      const uint32_t dst = rawbuf_addr + b * G::kRawBytes;
+      mbar_expect_tx(rawf_bar(b), G::kRawBytes);
+      if (KIND == 1) {
+        for (int k = 0; k < NK; ++k) bulk_load(dst + k * kUnit * 4, src + k * 1024, kUnit * 4, rawf_bar(b));
+      } else {
+        constexpr int kRawPiece = G::kRawBytes < 8192 ? G::kRawBytes : 8192;
+        for (int o = 0; o < G::kRawBytes; o += kRawPiece)
+          bulk_load(dst + o, reinterpret_cast<const uint8_t*>(src) + o, kRawPiece, rawf_bar(b));
       }
     }
-  } else {
-    // unit = (row, 4 consecutive k); lane = 8 rows x 4 k-quads, so the
-    // 32 four-byte stores of a warp fall in 32 distinct banks.  Eight units
-    // per step keep eight 16-byte loads per thread in flight.
-    const int r8 = lane >> 2, q4 = lane & 3;
-    for (int wu0 = warp; wu0 < 16 * 16; wu0 += 8 * (kThreads / 32)) {
-      uint4 v[8];
-#pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        const int wu = wu0 + h * (kThreads / 32);
-        const int r = (wu >> 4) * 8 + r8, k = ((wu & 15) * 4 + q4) * 4;
-        v[h] = *reinterpret_cast<const uint4*>(src + (m0 + r) * kSide + k);
-      }
-#pragma unroll
-      for (int h = 0; h < 8; ++h) {
-        const int wu = wu0 + h * (kThreads / 32);
-        const int r = (wu >> 4) * 8 + r8, k = ((wu & 15) * 4 + q4) * 4;
-        uint32_t w0, w1, w2, w3;
-        byte_transpose(v[h].x, v[h].y, v[h].z, v[h].w, w0, w1, w2, w3);
-        const uint32_t off = a_offset(r, k);
-        *reinterpret_cast<uint32_t*>(a_tile + 0 * kPlaneBytes + off) = w0;
-        *reinterpret_cast<uint32_t*>(a_tile + 1 * kPlaneBytes + off) = w1;
-        *reinterpret_cast<uint32_t*>(a_tile + 2 * kPlaneBytes + off) = w2;
-        *reinterpret_cast<uint32_t*>(a_tile + 3 * kPlaneBytes + off) = w3;
-      }
+    // after an abort, wait (bounded) for the copies still in flight
+    if (*abort) {
+      mbar_wait(bfull_bar, 0, nullptr, args.err);
+      for (int t = i - 2 < 0 ? 0 : i - 2; t < i; ++t) mbar_wait(rawf_bar(t & 1), (t >> 1) & 1, nullptr, args.err);
     }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  __syncthreads();
-
-  constexpr int kTotalChunks = kTiles * kChunksPerTile;
-  if (producer) {
-    for (; issued < kTotalChunks; ++issued) {
-      const int s = issued % kStages;
-      if (!mbar_wait(empty_bar(s), ((issued / kStages) & 1) ^ 1, abort, args.err)) break;
-      mbar_expect_tx(full_bar(s), kChunkBytes);
-      bulk_load(b_addr + s * kChunkBytes, bsrc + size_t(issued) * kChunkBytes, kChunkBytes, full_bar(s));
-    }
-  } else if (warp == 5 && lane == 0) {
-    bool ok = true;
-    for (int j = 0; j < kTiles && ok; ++j) {
-      const int b = j & 1;
-      if (j >= 2 && !mbar_wait(acce_bar(b), ((j >> 1) - 1) & 1, abort, args.err)) break;
-      tc_fence_after();
-      const uint32_t d_tmem = tmem + uint32_t(b * 256);
-      for (int c = 0; c < kChunksPerTile; ++c) {
-        const int t = j * kChunksPerTile + c, s = t % kStages;
-        if (!mbar_wait(full_bar(s), (t / kStages) & 1, abort, args.err)) {
-          ok = false;
-          break;
+  } else if (warp >= 4 && warp < 4 + kTransposeWarps) {
+    // raw words -> byte planes.  A thread unit = (instance, 4 consecutive k);
+    // a warp covers 8 instances x 4 k-quads (one 16-k group), so its 32
+    // four-byte stores fall in 32 distinct banks.
+    const int tw = warp - 4, r8 = lane >> 2, q4 = lane & 3;
+    constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);  // (8-instance group, 16-k group)
+    for (int i = 0; i < nu; ++i) {
+      const int b = i & 1;
+      if (!warp_wait(rawf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
+      if (i >= 2 && !warp_wait(ae_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err, lane)) break;
+      const uint32_t* raw = rawbuf + b * (G::kRawBytes / 4);
+      uint8_t* at = a_tile + b * G::kABytes;
+      for (int wu = tw; wu < kWarpUnits; wu += kTransposeWarps) {
+        const int ml = (wu % (kUnit / 8)) * 8 + r8;
+        const int k = (wu / (kUnit / 8)) * 16 + q4 * 4;
+        uint32_t v0, v1, v2, v3;
+        if (KIND == 3) {
+          const uint4 v = *reinterpret_cast<const uint4*>(raw + raw_index<KIND, NK>(ml, k));
+          v0 = v.x;
+          v1 = v.y;
+          v2 = v.z;
+          v3 = v.w;
+        } else {
+          v0 = raw[raw_index<KIND, NK>(ml, k)];
+          v1 = raw[raw_index<KIND, NK>(ml, k + 1)];
+          v2 = raw[raw_index<KIND, NK>(ml, k + 2)];
+          v3 = raw[raw_index<KIND, NK>(ml, k + 3)];
         }
-        tc_fence_after();
-        const int kc = c >> 2, d = c & 3;
-        const uint64_t a_desc = smem_desc(a_addr + d * kPlaneBytes + kc * 256, 128, 2048);
-        const uint64_t b_desc = smem_desc(b_addr + s * kChunkBytes, 128, 256);
-        mma_i8(d_tmem, a_desc, b_desc, c > 0 ? 1u : 0u);
-        mma_commit(empty_bar(s));
+        uint32_t w[4];
+        byte_transpose(v0, v1, v2, v3, w[0], w[1], w[2], w[3]);
+        // byte (ml, kappa) of the K-major tile, kappa = d NK + k
+        const uint32_t rowoff = uint32_t((ml & 7) * 16 + (ml >> 3) * G::kSbo);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) {
+          const int kap = d * NK + k;
+          *reinterpret_cast<uint32_t*>(at + rowoff + (kap >> 4) * 128 + (kap & 15)) = w[d];
+        }
       }
-      if (ok) mma_commit(accf_bar(b));
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(rawe_bar(b));
+        mbar_arrive(af_bar(b));
+      }
     }
-  } else if (warp < 4) {
+  } else if (warp == kMmaWarp && lane == 0) {
+    constexpr uint32_t kIdesc = instr_desc(G::kNmma);
+    bool ok = mbar_wait(bfull_bar, 0, abort, args.err);
+    for (int i = 0; i < nu && ok; ++i) {
+      const int b = i & 1;
+      if (!mbar_wait(af_bar(b), (i >> 1) & 1, abort, args.err) ||
+          (i >= 2 && !mbar_wait(acce_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err))) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d_tmem = tmem + uint32_t(b * G::kNmma);
+      const uint32_t a_base = a_addr + b * G::kABytes;
+#pragma unroll
+      for (int st = 0; st < G::kSteps; ++st)
+        mma_i8(d_tmem, smem_desc(a_base + st * 256, 128, G::kSbo), smem_desc(b_addr + st * 256, 128, G::kSbo),
+               kIdesc, st > 0 ? 1u : 0u);
+      mma_commit(ae_bar(b));
+      mma_commit(accf_bar(b));
+    }
+  } else if (warp < kEpilogueWarps) {
     const uint32_t q = args.qinfo[2 * prime], qneg = args.qinfo[2 * prime + 1];
     const TwPair<uint32_t>* post = POST ? args.post + (size_t(prime) << kLogN) : nullptr;
-    const int m = m0 + warp * 32 + lane;
+    const int ml = warp * 32 + lane;
     const uint32_t lane_addr = uint32_t(warp * 32) << 16;
-    for (int j = 0; j < kTiles; ++j) {
-      const int b = j & 1;
-      // one lane waits and the verdict is broadcast, so the warp-collective
-      // tcgen05.ld below always runs with all 32 lanes (or none)
-      const bool ready = __shfl_sync(0xffffffffu, lane == 0 ? mbar_wait(accf_bar(b), (j >> 1) & 1, abort, args.err)
-                                                           : false, 0);
-      if (!ready) break;
+    for (int i = 0; i < nu; ++i) {
+      const int b = i & 1;
+      const int off = inst_offset<KIND>(unit_m0(i) + ml);
+      uint32_t* dst = args.out + unit_poly(i) * int64_t(kPolyWords) + off;
+      const TwPair<uint32_t>* tw = POST ? post + off : nullptr;
+      if (!warp_wait(accf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
       tc_fence_after();
 #pragma unroll 1
-      for (int cc = 0; cc < kTileCols / 16; ++cc) {
+      for (int c0 = 0; c0 < NK; c0 += 16) {
         uint32_t acc[4][16];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) tmem_ld16(tmem + lane_addr + uint32_t(b * 256 + e * 64 + cc * 16), acc[e]);
+        for (int e = 0; e < 4; ++e) tmem_ld16(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
         tmem_wait_ld();
-        const int n0 = j * kTileCols + cc * 16;
         uint32_t res[16];
 #pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          uint64_t s = uint64_t(acc[0][i]) + (uint64_t(acc[1][i]) << 8) + (uint64_t(acc[2][i]) << 16) +
-                       (uint64_t(acc[3][i]) << 24);
-          const uint32_t mm = uint32_t(s) * qneg;
-          uint32_t r = uint32_t((s + uint64_t(mm) * q) >> 32);  // S 2^-32 mod q, in [0, 2q)
+        for (int j = 0; j < 16; ++j) {
+          const uint64_t sum = uint64_t(acc[0][j]) + (uint64_t(acc[1][j]) << 8) + (uint64_t(acc[2][j]) << 16) +
+                               (uint64_t(acc[3][j]) << 24);
+          const uint32_t mm = uint32_t(sum) * qneg;
+          uint32_t r = uint32_t((sum + uint64_t(mm) * q) >> 32);  // S 2^-32 mod q, in [0, 2q)
           if (POST) {
-            const TwPair<uint32_t> tw = post[COLUMN ? (n0 + i) * kSide + m : m * kSide + n0 + i];
-            const uint32_t qh = __umulhi(r, tw.wp);
-            r = r * tw.w - qh * q;  // Shoup: [0, 2q)
+            const TwPair<uint32_t> t = tw[(c0 + j) * S];
+            const uint32_t qh = __umulhi(r, t.wp);
+            r = r * t.w - qh * q;  // Shoup: [0, 2q)
           }
-          res[i] = r >= q ? r - q : r;
+          res[j] = r >= q ? r - q : r;
         }
-        if (COLUMN) {
+        if (S == 1) {
+          uint4* o = reinterpret_cast<uint4*>(dst + c0);
 #pragma unroll
-          for (int i = 0; i < 16; ++i) dst[(n0 + i) * kSide + m] = res[i];
+          for (int j = 0; j < 4; ++j) o[j] = make_uint4(res[4 * j], res[4 * j + 1], res[4 * j + 2], res[4 * j + 3]);
         } else {
-          uint4* o = reinterpret_cast<uint4*>(dst + m * kSide + n0);
 #pragma unroll
-          for (int i = 0; i < 4; ++i) o[i] = make_uint4(res[4 * i], res[4 * i + 1], res[4 * i + 2], res[4 * i + 3]);
+          for (int j = 0; j < 16; ++j) dst[(c0 + j) * S] = res[j];
         }
       }
       tc_fence_before();
@@ -419,22 +454,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   }
 
   __syncthreads();
-  // Drain what this CTA started before TMEM is freed and the CTA exits: all
-  // MMAs (and the arrivals they signal) always, the bulk copies in flight
-  // after an abort.
-  if (warp == 5 && lane == 0) {
+  // Drain the MMAs (and the arrivals they signal) before TMEM is freed.
+  if (warp == kMmaWarp && lane == 0) {
     mma_commit(drain_bar);
     mbar_wait(drain_bar, 0, nullptr, args.err);
-  } else if (producer && *abort) {
-    for (int t = issued - kStages < 0 ? 0 : issued - kStages; t < issued; ++t)
-      mbar_wait(full_bar(t % kStages), (t / kStages) & 1, nullptr, args.err);
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == kMmaWarp) {
     __syncwarp();
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::kTmemCols));
   }
 }
 
@@ -453,69 +483,90 @@ uint64_t powmod64(uint64_t b, uint64_t e, uint64_t q) {
   return r;
 }
 
-uint32_t br8(uint32_t v) {
+uint32_t brev(uint32_t v, int bits) {
   uint32_t r = 0;
-  for (int i = 0; i < 8; ++i, v >>= 1) r = (r << 1) | (v & 1);
+  for (int i = 0; i < bits; ++i, v >>= 1) r = (r << 1) | (v & 1);
   return r;
 }
 
-// Constant matrix B[k][n] of `pass` (0, 1: forward passes 1, 2; 2, 3:
-// inverse passes 1, 2) as an exponent of psi modulo 2N.
+// Pass table: 0, 1, 2 = forward passes 1, 2, 3; 3, 4, 5 = inverse passes
+// over the instance maps of passes 3, 2, 1 (the inverse runs backwards).
+constexpr int kPassNk[6] = {64, 64, 16, 16, 64, 64};
+constexpr bool kPassPost[6] = {true, true, false, true, true, false};
+
+// Exponent of psi (mod 2N) of the constant matrix W[k][n] of a pass.
 uint32_t pass_exponent(int pass, uint32_t k, uint32_t n) {
   const uint32_t mask = (2u << kLogN) - 1;
   switch (pass) {
-    case 0: return (256u * k * (2u * br8(n) + 1u)) & mask;              // W1[n = r][k = i1]
-    case 1: return (512u * k * br8(n)) & mask;                           // W2[k = i2][n = c]
-    case 2: return (0u - 512u * br8(k) * n) & mask;                      // W2'[k = c][n = i2]
-    default: return (0u - 256u * n * (2u * br8(k) + 1u)) & mask;         // W1'[n = i1][k = r]
+    case 0: return (1024u * k * (2u * brev(n, 6) + 1u)) & mask;          // k = i1, n = P1
+    case 1: return (2048u * brev(n, 6) * k) & mask;                      // k = i2, n = P2
+    case 2: return (8192u * brev(n, 4) * k) & mask;                      // k = i3, n = P3
+    case 3: return (0u - 8192u * brev(k, 4) * n) & mask;                 // k = P3, n = i3
+    case 4: return (0u - 2048u * brev(k, 6) * n) & mask;                 // k = P2, n = i2
+    default: return (0u - 1024u * n * (2u * brev(k, 6) + 1u)) & mask;   // k = P1, n = i1
   }
-}
-
-// Byte offset of (row, k) in one B chunk (256 rows x 32 bytes, K-major).
-inline size_t b_offset(uint32_t row, uint32_t kk) {
-  return (row & 7) * 16 + (row >> 3) * 256 + (kk >> 4) * 128 + (kk & 15);
 }
 
 }  // namespace tcntt
 
-// Fill the digit matrices of one pass for one prime (1 MiB at `bmat`) and,
-// for passes 0 and 2, the elementwise twiddles (N pairs at `post`).
+size_t tc_ntt_table_bytes(int pass) {
+  if (pass < 0 || pass > 5) return 0;
+  const int nk = tcntt::kPassNk[pass];
+  return size_t(4 * nk) * size_t(4 * nk);
+}
+
+// Fill the byte matrix of one pass for one prime (tc_ntt_table_bytes(pass)
+// bytes at `bmat`, the kernel's shared-memory layout: row e * NK + n, byte
+// d * NK + k of a K-major canonical tile with 8-row groups NK * 32 bytes
+// apart) and, for passes with a twiddle, the N twiddle pairs (w, floor(w
+// 2^32 / q)) in output order at `post`.
 void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, TwPair<uint32_t>* post) {
   using namespace tcntt;
   const uint32_t two_n = 2u << kLogN;
   std::vector<uint32_t> pw(two_n);
   pw[0] = 1;
   for (uint32_t i = 1; i < two_n; ++i) pw[i] = uint32_t(uint64_t(pw[i - 1]) * psi % q);  // q < 2^28
+  const uint32_t nk = uint32_t(kPassNk[pass]);
+  const uint32_t sbo = nk * 32;
   uint64_t scale[4];
   for (int d = 0; d < 4; ++d) scale[d] = powmod64(2, 8 * d + 32, q);
-  for (uint32_t k = 0; k < kSide; ++k) {
-    for (uint32_t n = 0; n < kSide; ++n) {
+  for (uint32_t k = 0; k < nk; ++k) {
+    for (uint32_t n = 0; n < nk; ++n) {
       const uint64_t w = pw[pass_exponent(pass, k, n)];
-      const uint32_t j = n / kTileCols, col = n % kTileCols, kc = k / 32, kk = k % 32;
-      for (int d = 0; d < 4; ++d) {
+      for (uint32_t d = 0; d < 4; ++d) {
         const uint32_t wd = uint32_t(w * scale[d] % q);
-        uint8_t* chunk = bmat + (size_t(j) * kChunksPerTile + kc * 4 + d) * kChunkBytes;
-        for (int e = 0; e < 4; ++e) chunk[b_offset(uint32_t(e) * kTileCols + col, kk)] = uint8_t(wd >> (8 * e));
+        const uint32_t kap = d * nk + k;
+        for (uint32_t e = 0; e < 4; ++e) {
+          const uint32_t r = e * nk + n;
+          bmat[(r & 7) * 16 + (r >> 3) * sbo + (kap >> 4) * 128 + (kap & 15)] = uint8_t(wd >> (8 * e));
+        }
       }
     }
   }
-  if (post && (pass == 0 || pass == 2)) {
-    const uint64_t r = powmod64(2, 30, q);
-    uint64_t c = r;
-    if (pass == 2) {
-      const uint64_t rinv = powmod64(r, q - 2, q), ninv = powmod64((uint64_t(1) << kLogN) % q, q - 2, q);
-      c = mulmod64(rinv, ninv, q);
-    }
-    for (uint32_t r = 0; r < kSide; ++r) {
-      const uint32_t odd = 2u * br8(r) + 1u;
-      for (uint32_t i2 = 0; i2 < kSide; ++i2) {
-        uint32_t ex = (i2 * odd) & (two_n - 1);
-        if (pass == 2) ex = (two_n - ex) & (two_n - 1);
+  if (!post || !kPassPost[pass]) return;
+  const uint64_t R = powmod64(2, 30, q);
+  const uint64_t ninv_rinv = mulmod64(powmod64(R, q - 2, q), powmod64((uint64_t(1) << kLogN) % q, q - 2, q), q);
+  for (uint32_t p1 = 0; p1 < 64; ++p1) {
+    const uint32_t odd1 = 2u * brev(p1, 6) + 1u;
+    for (uint32_t a = 0; a < 64; ++a) {
+      for (uint32_t i3 = 0; i3 < 16; ++i3) {
+        // output address 1024 p1 + 16 a + i3 in every twiddled pass
+        uint32_t ex;
+        uint64_t c = 1;
+        if (pass == 0) {  // a = i2: R psi^{16 i2 (2 m1 + 1)}
+          ex = (16u * a * odd1) & (two_n - 1);
+          c = R;
+        } else if (pass == 1 || pass == 3) {  // a = P2: psi^{+-((2 m1 + 1) i3 + 128 m2 i3)}
+          ex = (odd1 * i3 + 128u * brev(a, 6) * i3) & (two_n - 1);
+          if (pass == 3) {
+            ex = (two_n - ex) & (two_n - 1);
+            c = ninv_rinv;
+          }
+        } else {  // pass 4, a = i2: psi^{-16 i2 (2 m1 + 1)}
+          ex = (two_n - ((16u * a * odd1) & (two_n - 1))) & (two_n - 1);
+        }
         const uint32_t w = uint32_t(mulmod64(pw[ex], c, q));
-        // forward pass 1 stores D[m = i2][n = r] column-wise (index n * 256 + m);
-        // inverse pass 1 stores D[m = r][n = i2] row-wise (index m * 256 + n):
-        // both are r * 256 + i2.
-        post[r * kSide + i2] = TwPair<uint32_t>{w, uint32_t((uint64_t(w) << 32) / q)};
+        post[1024 * p1 + 16 * a + i3] = TwPair<uint32_t>{w, uint32_t((uint64_t(w) << 32) / q)};
       }
     }
   }
@@ -542,17 +593,18 @@ int tc_ntt_prepare(Context& c) {
     return e != cudaSuccess ? cuda_status(e, where) : fail(-6, std::string("out of memory: ") + where);
   };
   const size_t n = size_t(1) << kLogN;
-  std::vector<uint8_t> bm(size_t(qp) * kPassBytesPerPrime);
   std::vector<TwPair<uint32_t>> post(size_t(qp) * n);
-  for (int pass = 0; pass < 4; ++pass) {
+  for (int pass = 0; pass < 6; ++pass) {
+    const size_t tb = tc_ntt_table_bytes(pass);
+    std::vector<uint8_t> bm(size_t(qp) * tb);
     for (int j = 0; j < qp; ++j)
-      tc_ntt_tables_host(c.moduli[j], c.roots[j], pass, bm.data() + size_t(j) * kPassBytesPerPrime,
-                         (pass == 0 || pass == 2) ? post.data() + size_t(j) * n : nullptr);
+      tc_ntt_tables_host(c.moduli[j], c.roots[j], pass, bm.data() + size_t(j) * tb,
+                         kPassPost[pass] ? post.data() + size_t(j) * n : nullptr);
     t->bmat[pass] = static_cast<uint8_t*>(dev_alloc(bm.size()));
     if (!t->bmat[pass] || cudaMemcpy(t->bmat[pass], bm.data(), bm.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-      return give_up("tensor-core NTT digit matrices");
-    if (pass == 0 || pass == 2) {
-      auto*& dst = t->post[pass / 2];
+      return give_up("tensor-core NTT byte matrices");
+    if (kPassPost[pass]) {
+      auto*& dst = t->post[pass];
       dst = static_cast<TwPair<uint32_t>*>(dev_alloc(post.size() * sizeof(post[0])));
       if (!dst || cudaMemcpy(dst, post.data(), post.size() * sizeof(post[0]), cudaMemcpyHostToDevice) != cudaSuccess)
         return give_up("tensor-core NTT twiddles");
@@ -577,36 +629,43 @@ int tc_ntt_prepare(Context& c) {
 }
 
 namespace {
-template <bool COLUMN, bool POST>
+template <int KIND, int NK, bool POST>
 int launch_pass(const Context& c, const uint32_t* in, uint32_t* out, int pass, int64_t polys, int rows,
                 int row_start, cudaStream_t st) {
   using namespace tcntt;
-  auto kern = k_tc_ntt_pass<COLUMN, POST>;
-  if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), kSmemBytes)) return rc;
-  PassArgs a{in, out, c.tc->bmat[pass], POST ? c.tc->post[pass / 2] : nullptr, c.tc->qinfo, polys / rows, rows,
-             row_start, c.tc->err};
-  kern<<<dim3(unsigned(polys * 2)), kThreads, kSmemBytes, st>>>(a);
+  auto kern = k_tc_ntt_pass<KIND, NK, POST>;
+  const int smem = smem_bytes<NK>();
+  if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return rc;
+  // persistent CTAs: at most one per SM (148), each streaming units of one prime
+  const int64_t batch = polys / rows;
+  const int64_t units = batch * Geom<NK>::kUnitsPerPoly;
+  int64_t per_row = 148 / rows;
+  if (per_row > units) per_row = units;
+  if (per_row < 1) per_row = 1;
+  PassArgs a{in, out, c.tc->bmat[pass], POST ? c.tc->post[pass] : nullptr, c.tc->qinfo, batch, rows,
+             row_start, int(per_row), c.tc->err};
+  kern<<<dim3(unsigned(rows * per_row)), kThreads, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "k_tc_ntt_pass");
 }
 }  // namespace
 
-// Both passes of a direction; the second runs in place on `out` (each CTA
-// reads its whole 128-row (or 128-column) slab into shared memory before it
-// writes the same slab, and the two CTAs of a polynomial own disjoint slabs),
-// so in == out is allowed and no scratch is needed.
+// The three passes of a direction; passes after the first run in place on
+// `out` (every unit writes exactly the words its raw copy read, after the
+// copy landed), so in == out is allowed and no scratch is needed.
 int tc_ntt(Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool inverse,
            cudaStream_t st) {
   if (int rc = tc_ntt_prepare(c)) return rc;
   if (polys == 0) return 0;
-  if (polys * 2 > 0x7FFFFFFFll) return fail(-4, "too many polynomials for one launch");
   const auto* x = static_cast<const uint32_t*>(in);
   auto* y = static_cast<uint32_t*>(out);
   if (!inverse) {
-    if (int rc = launch_pass<true, true>(c, x, y, 0, polys, rows, row_start, st)) return rc;
-    return launch_pass<false, false>(c, y, y, 1, polys, rows, row_start, st);
+    if (int rc = launch_pass<1, 64, true>(c, x, y, 0, polys, rows, row_start, st)) return rc;
+    if (int rc = launch_pass<2, 64, true>(c, y, y, 1, polys, rows, row_start, st)) return rc;
+    return launch_pass<3, 16, false>(c, y, y, 2, polys, rows, row_start, st);
   }
-  if (int rc = launch_pass<false, true>(c, x, y, 2, polys, rows, row_start, st)) return rc;
-  return launch_pass<true, false>(c, y, y, 3, polys, rows, row_start, st);
+  if (int rc = launch_pass<3, 16, true>(c, x, y, 3, polys, rows, row_start, st)) return rc;
+  if (int rc = launch_pass<2, 64, true>(c, y, y, 4, polys, rows, row_start, st)) return rc;
+  return launch_pass<1, 64, false>(c, y, y, 5, polys, rows, row_start, st);
 }
 
 int tc_ntt_status(Context& c, int* flag) {

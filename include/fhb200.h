@@ -90,9 +90,9 @@ int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t b
                     int row_start, int input_montgomery, fhb_stream stream);
 
 /* Exact int8 tensor-core forms of the two transforms above (tcgen05.mma
- * kind::i8, int32 accumulation in tensor memory): a 256 x 256 four-step
- * NTT whose two matrix passes run over the residues' four bytes and
- * byte-split constant matrices, reduced exactly in the epilogue.  int32
+ * kind::i8, int32 accumulation in tensor memory): a 64 x 64 x 16 three-pass
+ * NTT whose passes run over the residues' four bytes and byte-split constant
+ * matrices held in shared memory, reduced exactly in the epilogue.  int32
  * contexts with log_n = 16 only (else -7).
  *   fhb_tc_forward_ntt: standard input -> NTT/Montgomery output, canonical
  *     [0, q): equal mod q to fhb_forward_ntt(input_montgomery = 0), whose
@@ -102,14 +102,16 @@ int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t b
  *     canonical, bit-identical to fhb_inverse_ntt(output_kind = 2)
  *     (inverse_ntt_to_standard_compact_grouped_smem_, csrc/ops/ntt/
  *     inverse_ntt.cpp:23-73).
- * in == out allowed; no scratch.  The first call builds the constant
- * matrices (4 MiB per prime, blocking) unless fhb_tc_ntt_prepare ran.
- * fhb_tc_ntt_status synchronises, returns in *flag whether a bounded wait
- * inside the kernels gave up since the last call (outputs then invalid),
- * and clears the flag.  fhb_tc_ntt_tables_host (host only, no device) fills
- * one pass's byte matrices (1 MiB, the kernels' shared-memory layout) and,
- * for passes 0 and 2, the N elementwise twiddle pairs (w, floor(w 2^32 / q)),
- * for a prime q < 2^28 with primitive 2N-th root psi at N = 2^16. */
+ * in == out allowed; no scratch.  The first call builds the constants
+ * (byte matrices and twiddles, about 2 MiB per prime, blocking) unless
+ * fhb_tc_ntt_prepare ran.  fhb_tc_ntt_status synchronises, returns in *flag
+ * whether a bounded wait inside the kernels gave up since the last call
+ * (outputs then invalid), and clears the flag.  fhb_tc_ntt_tables_host (host
+ * only, no device) fills, for a prime q < 2^28 with primitive 2N-th root psi
+ * at N = 2^16, the byte matrix of one pass (passes 0-2 forward, 3-5 inverse;
+ * 64 KiB for passes 0, 1, 4, 5 and 4 KiB for passes 2, 3, in the kernels'
+ * shared-memory layout) and, for the twiddled passes 0, 1, 3, 4 when post is
+ * not NULL, the N twiddle pairs (w, floor(w 2^32 / q)) in output order. */
 int fhb_tc_ntt_prepare(const fhb_context* ctx);
 int fhb_tc_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
                        int row_start, fhb_stream stream);
