@@ -411,7 +411,7 @@ int fhb_tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, ui
   if (q < 3 || q >= (uint64_t{1} << 28) || !(q & 1) || (q - 1) % (uint64_t{2} << 16) != 0)
     return fail(-2, "q must be an odd NTT prime below 2^28 for N = 2^16");
   if (psi == 0 || psi >= q) return fail(-2, "psi out of range");
-  fhb::tc_ntt_tables_host(q, psi, pass, bmat, reinterpret_cast<fhb::TwPair<uint32_t>*>(post));
+  fhb::tc_ntt_tables_host(q, psi, pass, bmat, post);
   return 0;
 }
 

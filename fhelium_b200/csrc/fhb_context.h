@@ -52,7 +52,7 @@ struct LevelTables {
 // on first use.  All device arrays are owned through Context::allocations.
 struct TcNttTables {
   uint8_t* bmat[6] = {};              // per pass: [QP][byte matrix of the pass] (64 KiB or 4 KiB per prime)
-  TwPair<uint32_t>* post[6] = {};     // per pass with a twiddle: [QP][N] in output order, else null
+  uint32_t* post[6] = {};             // per pass with a twiddle: [QP][N] t 2^32 mod q in output order, else null
   uint32_t* qinfo = nullptr;          // [QP][2]: q, -q^{-1} mod 2^32
   int* err = nullptr;                 // device flag: a bounded wait gave up
 };
@@ -101,7 +101,7 @@ int tc_ntt(Context& c, const void* in, void* out, int64_t polys, int rows, int r
            cudaStream_t st);
 int tc_ntt_status(Context& c, int* flag);
 size_t tc_ntt_table_bytes(int pass);
-void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, TwPair<uint32_t>* post);
+void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post);
 
 // Host-side status plumbing shared by the C ABI.
 void set_error(const std::string& msg);

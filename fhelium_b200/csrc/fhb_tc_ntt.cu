@@ -28,7 +28,9 @@
 // accumulator e collects sum_{d,k} A_d W^(d)_e (K = 4 n byte products,
 // < 2^24), the epilogue forms S = sum_e 2^{8e} acc_e < 2^49 and one
 // Montgomery reduction by 2^32 returns (A W mod q) in [0, 2q); the optional
-// elementwise twiddle is a Shoup product and the result is made canonical.
+// elementwise twiddle t is stored as t 2^32 mod q and applied by a second
+// reduction by 2^32 (exact for inputs < 2q < 2^32 / q), and the result is made
+// canonical.
 //
 // The constant matrix of a pass is small enough to stay in shared memory (64
 // KiB for n = 64, 4 KiB for n = 16), so a persistent CTA loads it once per
@@ -41,9 +43,10 @@
 //   MMA issuer (warp 9, lane 0): n / 8 MMAs of M = 128, N = 4 n (twiddle bytes
 //       e x n outputs), K = 32 into one of two TMEM accumulator sets;
 //   epilogue (warps 0-3, TMEM lane quarter w): recombination, twiddle, store.
-// Raw buffers, A tiles and accumulator sets alternate between two slots, so
-// the copies of unit i + 1, the transposition and MMAs of unit i and the
-// epilogue of unit i - 1 overlap.  Every mbarrier wait is bounded (about one
+// Raw buffers rotate over three slots, A tiles and accumulator sets over two,
+// so the copies of units i + 1 and i + 2, the transposition and MMAs of unit i
+// and the epilogue of unit i - 1 overlap; the epilogue requests a unit's
+// twiddles before it waits for the unit's accumulators.  Every mbarrier wait is bounded (about one
 // second of the global timer); a wait that gives up sets a CTA abort flag that
 // releases every other wait and raises the device error flag, and the CTA
 // drains its own bulk copies and MMAs (again with bounded waits) before it
@@ -81,10 +84,11 @@ struct Geom {
 };
 
 constexpr int kBarrierBytes = 256;
-// smem: [B | raw 0 | raw 1 | A 0 | A 1 | barriers]
+constexpr int kRawSlots = 3;
+// smem: [B | raw 0..2 | A 0 | A 1 | barriers]
 template <int NK>
 constexpr int smem_bytes() {
-  return 1024 + Geom<NK>::kBBytes + 2 * Geom<NK>::kRawBytes + 2 * Geom<NK>::kABytes + kBarrierBytes;
+  return 1024 + Geom<NK>::kBBytes + kRawSlots * Geom<NK>::kRawBytes + 2 * Geom<NK>::kABytes + kBarrierBytes;
 }
 static_assert(smem_bytes<64>() <= 232448, "shared memory per CTA");
 
@@ -241,7 +245,7 @@ struct PassArgs {
   const uint32_t* in;
   uint32_t* out;
   const uint8_t* bmat;                // [QP][byte matrix]
-  const TwPair<uint32_t>* post;       // [QP][N] in output order, or null
+  const uint32_t* post;               // [QP][N] twiddles t 2^32 mod q in output order, or null
   const uint32_t* qinfo;              // [QP][2]
   int64_t batch;                      // polynomials per row (polys = batch x rows)
   int rows;
@@ -263,20 +267,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   const uint32_t b_addr = base;
   const uint32_t rawbuf_addr = base + G::kBBytes;
   const uint32_t* const rawbuf = reinterpret_cast<const uint32_t*>(gbase + G::kBBytes);
-  const uint32_t a_addr = base + G::kBBytes + 2 * G::kRawBytes;
-  uint8_t* const a_tile = gbase + G::kBBytes + 2 * G::kRawBytes;
-  uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + G::kBBytes + 2 * G::kRawBytes + 2 * G::kABytes);
+  const uint32_t a_addr = base + G::kBBytes + kRawSlots * G::kRawBytes;
+  uint8_t* const a_tile = gbase + G::kBBytes + kRawSlots * G::kRawBytes;
+  uint64_t* const bars =
+      reinterpret_cast<uint64_t*>(gbase + G::kBBytes + kRawSlots * G::kRawBytes + 2 * G::kABytes);
   const uint32_t bar0 = smem_addr(bars);
-  // barriers: b_full, raw_full[2], raw_empty[2], a_full[2], a_empty[2], acc_full[2], acc_empty[2], drain
+  // barriers: b_full, raw_full[3], raw_empty[3], a_full[2], a_empty[2], acc_full[2], acc_empty[2], drain
   const uint32_t bfull_bar = bar0;
-  auto rawf_bar = [&](int b) { return bar0 + 8u * (1 + b); };
-  auto rawe_bar = [&](int b) { return bar0 + 8u * (3 + b); };
-  auto af_bar = [&](int b) { return bar0 + 8u * (5 + b); };
-  auto ae_bar = [&](int b) { return bar0 + 8u * (7 + b); };
-  auto accf_bar = [&](int b) { return bar0 + 8u * (9 + b); };
-  auto acce_bar = [&](int b) { return bar0 + 8u * (11 + b); };
-  const uint32_t drain_bar = bar0 + 8u * 13;
-  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 14);
+  auto rawf_bar = [&](int r) { return bar0 + 8u * (1 + r); };
+  auto rawe_bar = [&](int r) { return bar0 + 8u * (4 + r); };
+  auto af_bar = [&](int b) { return bar0 + 8u * (7 + b); };
+  auto ae_bar = [&](int b) { return bar0 + 8u * (9 + b); };
+  auto accf_bar = [&](int b) { return bar0 + 8u * (11 + b); };
+  auto acce_bar = [&](int b) { return bar0 + 8u * (13 + b); };
+  const uint32_t drain_bar = bar0 + 8u * 15;
+  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 16);
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -292,9 +297,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
 
   if (tid == 0) {
     mbar_init(bfull_bar, 1);
+    for (int r = 0; r < kRawSlots; ++r) {
+      mbar_init(rawf_bar(r), 1);
+      mbar_init(rawe_bar(r), kTransposeWarps);
+    }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(rawf_bar(b), 1);
-      mbar_init(rawe_bar(b), kTransposeWarps);
       mbar_init(af_bar(b), kTransposeWarps);
       mbar_init(ae_bar(b), 1);
       mbar_init(accf_bar(b), 1);
@@ -323,23 +330,24 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
     for (int o = 0; o < G::kBBytes; o += kPiece) bulk_load(b_addr + o, bsrc + o, kPiece, bfull_bar);
     int i = 0;
     for (; i < nu; ++i) {
-      const int b = i & 1;
-      if (i >= 2 && !mbar_wait(rawe_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err)) break;
+      const int r = i % kRawSlots, use = i / kRawSlots;
+      if (i >= kRawSlots && !mbar_wait(rawe_bar(r), (use & 1) ^ 1, abort, args.err)) break;
       const uint32_t* src = args.in + unit_poly(i) * int64_t(kPolyWords) + inst_offset<KIND>(unit_m0(i));
-      const uint32_t dst = rawbuf_addr + b * G::kRawBytes;
-      mbar_expect_tx(rawf_bar(b), G::kRawBytes);
+      const uint32_t dst = rawbuf_addr + r * G::kRawBytes;
+      mbar_expect_tx(rawf_bar(r), G::kRawBytes);
       if (KIND == 1) {
-        for (int k = 0; k < NK; ++k) bulk_load(dst + k * kUnit * 4, src + k * 1024, kUnit * 4, rawf_bar(b));
+        for (int k = 0; k < NK; ++k) bulk_load(dst + k * kUnit * 4, src + k * 1024, kUnit * 4, rawf_bar(r));
       } else {
         constexpr int kRawPiece = G::kRawBytes < 8192 ? G::kRawBytes : 8192;
         for (int o = 0; o < G::kRawBytes; o += kRawPiece)
-          bulk_load(dst + o, reinterpret_cast<const uint8_t*>(src) + o, kRawPiece, rawf_bar(b));
+          bulk_load(dst + o, reinterpret_cast<const uint8_t*>(src) + o, kRawPiece, rawf_bar(r));
       }
     }
     // after an abort, wait (bounded) for the copies still in flight
     if (*abort) {
       mbar_wait(bfull_bar, 0, nullptr, args.err);
-      for (int t = i - 2 < 0 ? 0 : i - 2; t < i; ++t) mbar_wait(rawf_bar(t & 1), (t >> 1) & 1, nullptr, args.err);
+      for (int t = i - kRawSlots < 0 ? 0 : i - kRawSlots; t < i; ++t)
+        mbar_wait(rawf_bar(t % kRawSlots), (t / kRawSlots) & 1, nullptr, args.err);
     }
   } else if (warp >= 4 && warp < 4 + kTransposeWarps) {
     // raw words -> byte planes.  A thread unit = (instance, 4 consecutive k);
@@ -348,10 +356,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
     const int tw = warp - 4, r8 = lane >> 2, q4 = lane & 3;
     constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);  // (8-instance group, 16-k group)
     for (int i = 0; i < nu; ++i) {
-      const int b = i & 1;
-      if (!warp_wait(rawf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
+      const int b = i & 1, r = i % kRawSlots;
+      if (!warp_wait(rawf_bar(r), (i / kRawSlots) & 1, abort, args.err, lane)) break;
       if (i >= 2 && !warp_wait(ae_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err, lane)) break;
-      const uint32_t* raw = rawbuf + b * (G::kRawBytes / 4);
+      const uint32_t* raw = rawbuf + r * (G::kRawBytes / 4);
       uint8_t* at = a_tile + b * G::kABytes;
       for (int wu = tw; wu < kWarpUnits; wu += kTransposeWarps) {
         const int ml = (wu % (kUnit / 8)) * 8 + r8;
@@ -382,7 +390,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) {
-        mbar_arrive(rawe_bar(b));
+        mbar_arrive(rawe_bar(r));
         mbar_arrive(af_bar(b));
       }
     }
@@ -408,18 +416,33 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
     }
   } else if (warp < kEpilogueWarps) {
     const uint32_t q = args.qinfo[2 * prime], qneg = args.qinfo[2 * prime + 1];
-    const TwPair<uint32_t>* post = POST ? args.post + (size_t(prime) << kLogN) : nullptr;
+    const uint32_t* post = POST ? args.post + (size_t(prime) << kLogN) : nullptr;
     const int ml = warp * 32 + lane;
     const uint32_t lane_addr = uint32_t(warp * 32) << 16;
     for (int i = 0; i < nu; ++i) {
       const int b = i & 1;
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
       uint32_t* dst = args.out + unit_poly(i) * int64_t(kPolyWords) + off;
-      const TwPair<uint32_t>* tw = POST ? post + off : nullptr;
+      const uint32_t* tw = POST ? post + off : nullptr;
+      // the first chunk's twiddles are requested before the wait, each
+      // chunk requests the next one's
+      uint32_t t_cur[16], t_next[16];
+      if (POST) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) t_next[j] = tw[j * S];
+      }
       if (!warp_wait(accf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
       tc_fence_after();
 #pragma unroll 1
       for (int c0 = 0; c0 < NK; c0 += 16) {
+        if (POST) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) t_cur[j] = t_next[j];
+          if (c0 + 16 < NK) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) t_next[j] = tw[(c0 + 16 + j) * S];
+          }
+        }
         uint32_t acc[4][16];
 #pragma unroll
         for (int e = 0; e < 4; ++e) tmem_ld16(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
@@ -432,9 +455,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
           const uint32_t mm = uint32_t(sum) * qneg;
           uint32_t r = uint32_t((sum + uint64_t(mm) * q) >> 32);  // S 2^-32 mod q, in [0, 2q)
           if (POST) {
-            const TwPair<uint32_t> t = tw[(c0 + j) * S];
-            const uint32_t qh = __umulhi(r, t.wp);
-            r = r * t.w - qh * q;  // Shoup: [0, 2q)
+            const uint64_t pr = uint64_t(r) * t_cur[j];  // < 2 q^2 < q 2^32
+            const uint32_t m2 = uint32_t(pr) * qneg;
+            r = uint32_t((pr + uint64_t(m2) * q) >> 32);  // r t mod q, in [0, 2q)
           }
           res[j] = r >= q ? r - q : r;
         }
@@ -518,9 +541,9 @@ size_t tc_ntt_table_bytes(int pass) {
 // Fill the byte matrix of one pass for one prime (tc_ntt_table_bytes(pass)
 // bytes at `bmat`, the kernel's shared-memory layout: row e * NK + n, byte
 // d * NK + k of a K-major canonical tile with 8-row groups NK * 32 bytes
-// apart) and, for passes with a twiddle, the N twiddle pairs (w, floor(w
-// 2^32 / q)) in output order at `post`.
-void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, TwPair<uint32_t>* post) {
+// apart) and, for passes with a twiddle, the N twiddles t as t 2^32 mod q in
+// output order at `post`.
+void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post) {
   using namespace tcntt;
   const uint32_t two_n = 2u << kLogN;
   std::vector<uint32_t> pw(two_n);
@@ -565,8 +588,8 @@ void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, TwPai
         } else {  // pass 4, a = i2: psi^{-16 i2 (2 m1 + 1)}
           ex = (two_n - ((16u * a * odd1) & (two_n - 1))) & (two_n - 1);
         }
-        const uint32_t w = uint32_t(mulmod64(pw[ex], c, q));
-        post[1024 * p1 + 16 * a + i3] = TwPair<uint32_t>{w, uint32_t((uint64_t(w) << 32) / q)};
+        const uint64_t w = mulmod64(pw[ex], c, q);
+        post[1024 * p1 + 16 * a + i3] = uint32_t((w << 32) % q);
       }
     }
   }
@@ -593,7 +616,7 @@ int tc_ntt_prepare(Context& c) {
     return e != cudaSuccess ? cuda_status(e, where) : fail(-6, std::string("out of memory: ") + where);
   };
   const size_t n = size_t(1) << kLogN;
-  std::vector<TwPair<uint32_t>> post(size_t(qp) * n);
+  std::vector<uint32_t> post(size_t(qp) * n);
   for (int pass = 0; pass < 6; ++pass) {
     const size_t tb = tc_ntt_table_bytes(pass);
     std::vector<uint8_t> bm(size_t(qp) * tb);
@@ -605,7 +628,7 @@ int tc_ntt_prepare(Context& c) {
       return give_up("tensor-core NTT byte matrices");
     if (kPassPost[pass]) {
       auto*& dst = t->post[pass];
-      dst = static_cast<TwPair<uint32_t>*>(dev_alloc(post.size() * sizeof(post[0])));
+      dst = static_cast<uint32_t*>(dev_alloc(post.size() * sizeof(post[0])));
       if (!dst || cudaMemcpy(dst, post.data(), post.size() * sizeof(post[0]), cudaMemcpyHostToDevice) != cudaSuccess)
         return give_up("tensor-core NTT twiddles");
     }

@@ -111,7 +111,7 @@ int fhb_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t b
  * at N = 2^16, the byte matrix of one pass (passes 0-2 forward, 3-5 inverse;
  * 64 KiB for passes 0, 1, 4, 5 and 4 KiB for passes 2, 3, in the kernels'
  * shared-memory layout) and, for the twiddled passes 0, 1, 3, 4 when post is
- * not NULL, the N twiddle pairs (w, floor(w 2^32 / q)) in output order. */
+ * not NULL, the N twiddles t as t 2^32 mod q (uint32) in output order. */
 int fhb_tc_ntt_prepare(const fhb_context* ctx);
 int fhb_tc_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
                        int row_start, fhb_stream stream);

@@ -2,10 +2,10 @@
 
 The library's host table builder writes, per pass and prime, the byte-split
 constant matrix in the tensor cores' shared-memory layout and the
-elementwise twiddles in output order.  Here the six passes (three forward,
+elementwise twiddles (as t 2^32 mod q) in output order.  Here the six passes (three forward,
 three inverse) are emulated in numpy from those very bytes -- unsigned 8-bit
 digit products with exact accumulation, the epilogue's Montgomery reduction
-by 2^32 and Shoup twiddle, the instance maps of the kernels -- and checked
+by 2^32, the twiddle's second reduction, the instance maps of the kernels -- and checked
 against the oracle's negacyclic NTT: forward equal mod q, inverse
 bit-identical, with the accumulator and range bounds the kernels rely on."""
 
@@ -52,7 +52,7 @@ def _offsets(kind, nk):
 def _tables(lib, q, psi, p):
     nk = NK[p]
     bmat = np.zeros(16 * nk * nk, dtype=np.uint8)
-    post = np.zeros(2 * N, dtype=np.uint32)
+    post = np.zeros(N, dtype=np.uint32)
     rc = lib.fhb_tc_ntt_tables_host(ctypes.c_uint64(q), ctypes.c_uint64(psi), p, bmat.ctypes.data,
                                     post.ctypes.data)
     assert rc == 0
@@ -63,7 +63,7 @@ def _tables(lib, q, psi, p):
     off = (r % 8) * 16 + (r // 8) * (nk * 32) + (kap // 16) * 128 + kap % 16
     full = bmat[off].astype(np.float64)            # [e * nk + n][d * nk + k]
     planes = full.reshape(4, nk, 4, nk).transpose(2, 3, 0, 1)   # [d][k][e][n]
-    return planes, post.reshape(N, 2)
+    return planes, post
 
 
 def _pass(x, p, planes, post, q):
@@ -82,10 +82,10 @@ def _pass(x, p, planes, post, q):
     r = (s + mm * np.uint64(q)) >> np.uint64(32)
     assert r.max() < 2 * q
     if POST[p]:
-        w = post[offs, 0].astype(np.uint64)
-        wp = post[offs, 1].astype(np.uint64)
-        qh = (r * wp) >> np.uint64(32)
-        r = (r * w - qh * np.uint64(q)) & np.uint64(0xFFFFFFFF)
+        pr = r * post[offs].astype(np.uint64)        # twiddle stored as t 2^32 mod q
+        assert pr.max() < q * 2 ** 32
+        m2 = ((pr & np.uint64(0xFFFFFFFF)) * np.uint64(qneg)) & np.uint64(0xFFFFFFFF)
+        r = (pr + m2 * np.uint64(q)) >> np.uint64(32)
         assert r.max() < 2 * q
     out = np.empty(N, dtype=np.int64)
     out[offs] = np.where(r >= q, r - np.uint64(q), r).astype(np.int64)
