@@ -36,13 +36,14 @@
 // KiB for n = 64, 4 KiB for n = 16), so a persistent CTA loads it once per
 // prime and then streams units of 128 instances of that prime through a
 // double-buffered pipeline:
-//   producer (warp 8, lane 0): bulk copies of a unit's raw words into a raw
+//   producer (warp 12, lane 0): bulk copies of a unit's raw words into a raw
 //       buffer (one copy for contiguous units, one per k row otherwise);
-//   transposers (warps 4-7): raw words -> the four byte planes of the A tile
+//   transposers (warps 8-11): raw words -> the four byte planes of the A tile
 //       (K-major canonical layout, K = 4 n bytes: [A_0 | A_1 | A_2 | A_3]);
-//   MMA issuer (warp 9, lane 0): n / 8 MMAs of M = 128, N = 4 n (twiddle bytes
-//       e x n outputs), K = 32 into one of two TMEM accumulator sets;
-//   epilogue (warps 0-3, TMEM lane quarter w): recombination, twiddle, store.
+//   MMA issuer (warp 13, lane 0): n / 8 MMAs of M = 128, N = 4 n (twiddle
+//       bytes e x n outputs), K = 32 into one of two TMEM accumulator sets;
+//   epilogue (warps 0-7; warp w reads TMEM lane quarter w % 4 and the
+//       outputs of half w / 4): recombination, twiddle, store.
 // Raw buffers rotate over three slots, A tiles and accumulator sets over two,
 // so the copies of units i + 1 and i + 2, the transposition and MMAs of unit i
 // and the epilogue of unit i - 1 overlap; the epilogue requests a unit's
@@ -62,11 +63,12 @@ namespace tcntt {
 constexpr int kLogN = 16;
 constexpr int kPolyWords = 1 << kLogN;
 constexpr int kUnit = 128;                // instances per unit (MMA M)
-constexpr int kThreads = 320;             // 10 warps
-constexpr int kProducerWarp = 8;
-constexpr int kMmaWarp = 9;
-constexpr int kTransposeWarps = 4;        // warps 4..7
-constexpr int kEpilogueWarps = 4;         // warps 0..3
+constexpr int kThreads = 448;             // 14 warps
+constexpr int kEpilogueWarps = 8;         // warps 0..7
+constexpr int kTransposeWarp0 = 8;        // warps 8..11
+constexpr int kTransposeWarps = 4;
+constexpr int kProducerWarp = 12;
+constexpr int kMmaWarp = 13;
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
 // Pass geometry: NK = outputs (and inputs) per instance.
@@ -203,6 +205,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Byte transpose of four words: out[d] = byte d of v0 | byte d of v1 << 8 |
@@ -285,6 +293,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int kChunk = NK / 2 < 16 ? NK / 2 : 16;  // epilogue columns per TMEM load
   // CTA -> (prime row, contiguous range of its units); a unit = (polynomial
   // of the row, block of 128 instances)
   const int row = blockIdx.x / args.ctas_per_row, part = blockIdx.x % args.ctas_per_row;
@@ -349,11 +358,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
       for (int t = i - kRawSlots < 0 ? 0 : i - kRawSlots; t < i; ++t)
         mbar_wait(rawf_bar(t % kRawSlots), (t / kRawSlots) & 1, nullptr, args.err);
     }
-  } else if (warp >= 4 && warp < 4 + kTransposeWarps) {
+  } else if (warp >= kTransposeWarp0 && warp < kTransposeWarp0 + kTransposeWarps) {
     // raw words -> byte planes.  A thread unit = (instance, 4 consecutive k);
     // a warp covers 8 instances x 4 k-quads (one 16-k group), so its 32
     // four-byte stores fall in 32 distinct banks.
-    const int tw = warp - 4, r8 = lane >> 2, q4 = lane & 3;
+    const int tw = warp - kTransposeWarp0, r8 = lane >> 2, q4 = lane & 3;
     constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);  // (8-instance group, 16-k group)
     for (int i = 0; i < nu; ++i) {
       const int b = i & 1, r = i % kRawSlots;
@@ -417,8 +426,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   } else if (warp < kEpilogueWarps) {
     const uint32_t q = args.qinfo[2 * prime], qneg = args.qinfo[2 * prime + 1];
     const uint32_t* post = POST ? args.post + (size_t(prime) << kLogN) : nullptr;
-    const int ml = warp * 32 + lane;
-    const uint32_t lane_addr = uint32_t(warp * 32) << 16;
+    const int quarter = warp & 3, half = warp >> 2;
+    const int ml = quarter * 32 + lane;
+    const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
+    constexpr int kHalf = NK / 2;  // outputs of this warp: [half * kHalf, half * kHalf + kHalf)
     for (int i = 0; i < nu; ++i) {
       const int b = i & 1;
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
@@ -429,27 +440,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
       uint32_t t_cur[16], t_next[16];
       if (POST) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) t_next[j] = tw[j * S];
+        for (int j = 0; j < 16 && j < kHalf; ++j) t_next[j] = tw[(half * kHalf + j) * S];
       }
       if (!warp_wait(accf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
       tc_fence_after();
 #pragma unroll 1
-      for (int c0 = 0; c0 < NK; c0 += 16) {
+      for (int c0 = half * kHalf; c0 < half * kHalf + kHalf; c0 += kChunk) {
         if (POST) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) t_cur[j] = t_next[j];
-          if (c0 + 16 < NK) {
+          for (int j = 0; j < kChunk; ++j) t_cur[j] = t_next[j];
+          if (c0 + kChunk < half * kHalf + kHalf) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) t_next[j] = tw[(c0 + 16 + j) * S];
+            for (int j = 0; j < kChunk; ++j) t_next[j] = tw[(c0 + kChunk + j) * S];
           }
         }
         uint32_t acc[4][16];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) tmem_ld16(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
+        for (int e = 0; e < 4; ++e) {
+          if (kChunk == 16)
+            tmem_ld16(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
+          else
+            tmem_ld8(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
+        }
         tmem_wait_ld();
         uint32_t res[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < kChunk; ++j) {
           const uint64_t sum = uint64_t(acc[0][j]) + (uint64_t(acc[1][j]) << 8) + (uint64_t(acc[2][j]) << 16) +
                                (uint64_t(acc[3][j]) << 24);
           const uint32_t mm = uint32_t(sum) * qneg;
@@ -464,10 +480,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
         if (S == 1) {
           uint4* o = reinterpret_cast<uint4*>(dst + c0);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) o[j] = make_uint4(res[4 * j], res[4 * j + 1], res[4 * j + 2], res[4 * j + 3]);
+          for (int j = 0; j < kChunk / 4; ++j)
+            o[j] = make_uint4(res[4 * j], res[4 * j + 1], res[4 * j + 2], res[4 * j + 3]);
         } else {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) dst[(c0 + j) * S] = res[j];
+          for (int j = 0; j < kChunk; ++j) dst[(c0 + j) * S] = res[j];
         }
       }
       tc_fence_before();
