@@ -46,8 +46,8 @@
 //       outputs of half w / 4): recombination, twiddle, store.
 // Raw buffers rotate over three slots, A tiles and accumulator sets over two,
 // so the copies of units i + 1 and i + 2, the transposition and MMAs of unit i
-// and the epilogue of unit i - 1 overlap; the epilogue requests a unit's
-// twiddles before it waits for the unit's accumulators.  Every mbarrier wait is bounded (about one
+// and the epilogue of unit i - 1 overlap; each epilogue warp requests all its
+// twiddles of a unit before it waits for the unit's accumulators.  Every mbarrier wait is bounded (about one
 // second of the global timer); a wait that gives up sets a CTA abort flag that
 // releases every other wait and raises the device error flag, and the CTA
 // drains its own bulk copies and MMAs (again with bounded waits) before it
@@ -435,25 +435,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
       uint32_t* dst = args.out + unit_poly(i) * int64_t(kPolyWords) + off;
       const uint32_t* tw = POST ? post + off : nullptr;
-      // the first chunk's twiddles are requested before the wait, each
-      // chunk requests the next one's
-      uint32_t t_cur[16], t_next[16];
+      // all of this warp's twiddles for the unit are requested before the
+      // wait, so their latency hides behind it
+      uint32_t tws[kHalf];
       if (POST) {
 #pragma unroll
-        for (int j = 0; j < 16 && j < kHalf; ++j) t_next[j] = tw[(half * kHalf + j) * S];
+        for (int j = 0; j < kHalf; ++j) tws[j] = tw[(half * kHalf + j) * S];
       }
       if (!warp_wait(accf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
       tc_fence_after();
-#pragma unroll 1
-      for (int c0 = half * kHalf; c0 < half * kHalf + kHalf; c0 += kChunk) {
-        if (POST) {
 #pragma unroll
-          for (int j = 0; j < kChunk; ++j) t_cur[j] = t_next[j];
-          if (c0 + kChunk < half * kHalf + kHalf) {
-#pragma unroll
-            for (int j = 0; j < kChunk; ++j) t_next[j] = tw[(c0 + kChunk + j) * S];
-          }
-        }
+      for (int cc = 0; cc < kHalf / kChunk; ++cc) {
+        const int c0 = half * kHalf + cc * kChunk;
         uint32_t acc[4][16];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -471,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
           const uint32_t mm = uint32_t(sum) * qneg;
           uint32_t r = uint32_t((sum + uint64_t(mm) * q) >> 32);  // S 2^-32 mod q, in [0, 2q)
           if (POST) {
-            const uint64_t pr = uint64_t(r) * t_cur[j];  // < 2 q^2 < q 2^32
+            const uint64_t pr = uint64_t(r) * tws[cc * kChunk + j];  // < 2 q^2 < q 2^32
             const uint32_t m2 = uint32_t(pr) * qneg;
             r = uint32_t((pr + uint64_t(m2) * q) >> 32);  // r t mod q, in [0, 2q)
           }
