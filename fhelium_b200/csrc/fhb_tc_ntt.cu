@@ -81,17 +81,30 @@ struct Geom {
   static constexpr int kBBytes = kNmma * kKBytes;        // constant byte matrix
   static constexpr int kABytes = kUnit * kKBytes;        // one A tile
   static constexpr int kRawBytes = kUnit * NK * 4;       // one unit's raw words
-  static constexpr int kTmemCols = 2 * kNmma;            // two accumulator sets
   static constexpr int kUnitsPerPoly = (kPolyWords / NK) / kUnit;
+  // pipeline depth: raw copy slots, A tiles, TMEM accumulator sets (n = 16
+  // units are small, so it affords deeper rings)
+  static constexpr int kRawSlots = NK == 64 ? 3 : 8;
+  static constexpr int kASlots = NK == 64 ? 2 : 4;
+  static constexpr int kAccSlots = NK == 64 ? 2 : 4;
+  static constexpr int kTmemCols = kAccSlots * kNmma;
+  // n = 16: two CTAs per SM (their shared memory, TMEM and registers fit)
+  static constexpr int kCtasPerSm = NK == 64 ? 1 : 2;
 };
 
-constexpr int kBarrierBytes = 256;
-constexpr int kRawSlots = 3;
-// smem: [B | raw 0..2 | A 0 | A 1 | barriers]
+constexpr int kBarrierBytes = 512;
+// smem: [B | raw slots | A slots | barriers]
 template <int NK>
 constexpr int smem_bytes() {
-  return 1024 + Geom<NK>::kBBytes + kRawSlots * Geom<NK>::kRawBytes + 2 * Geom<NK>::kABytes + kBarrierBytes;
+  return 1024 + Geom<NK>::kBBytes + Geom<NK>::kRawSlots * Geom<NK>::kRawBytes +
+         Geom<NK>::kASlots * Geom<NK>::kABytes + kBarrierBytes;
 }
+template <int NK>
+constexpr int num_barriers() {
+  return 2 + 2 * (Geom<NK>::kRawSlots + Geom<NK>::kASlots + Geom<NK>::kAccSlots);
+}
+static_assert(8 * num_barriers<16>() + 8 <= kBarrierBytes && 8 * num_barriers<64>() + 8 <= kBarrierBytes,
+              "barrier area");
 static_assert(smem_bytes<64>() <= 232448, "shared memory per CTA");
 
 // tcgen05 instruction descriptor: D int32 (c_format 2 at bit 4), A and B
@@ -265,7 +278,7 @@ struct PassArgs {
 // in == out is allowed: a unit's outputs occupy exactly the words its raw
 // copy read, and a unit's output is written only after its raw copy landed.
 template <int KIND, int NK, bool POST>
-__global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
+__global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(PassArgs args) {
   using G = Geom<NK>;
   constexpr int S = inst_stride<KIND>();
   extern __shared__ uint8_t smem_raw[];
@@ -275,21 +288,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
   const uint32_t b_addr = base;
   const uint32_t rawbuf_addr = base + G::kBBytes;
   const uint32_t* const rawbuf = reinterpret_cast<const uint32_t*>(gbase + G::kBBytes);
+  constexpr int kRawSlots = G::kRawSlots, kASlots = G::kASlots, kAccSlots = G::kAccSlots;
   const uint32_t a_addr = base + G::kBBytes + kRawSlots * G::kRawBytes;
   uint8_t* const a_tile = gbase + G::kBBytes + kRawSlots * G::kRawBytes;
   uint64_t* const bars =
-      reinterpret_cast<uint64_t*>(gbase + G::kBBytes + kRawSlots * G::kRawBytes + 2 * G::kABytes);
+      reinterpret_cast<uint64_t*>(gbase + G::kBBytes + kRawSlots * G::kRawBytes + kASlots * G::kABytes);
   const uint32_t bar0 = smem_addr(bars);
-  // barriers: b_full, raw_full[3], raw_empty[3], a_full[2], a_empty[2], acc_full[2], acc_empty[2], drain
+  // barriers: b_full, raw_full/empty[kRawSlots], a_full/empty[kASlots], acc_full/empty[kAccSlots], drain
   const uint32_t bfull_bar = bar0;
   auto rawf_bar = [&](int r) { return bar0 + 8u * (1 + r); };
-  auto rawe_bar = [&](int r) { return bar0 + 8u * (4 + r); };
-  auto af_bar = [&](int b) { return bar0 + 8u * (7 + b); };
-  auto ae_bar = [&](int b) { return bar0 + 8u * (9 + b); };
-  auto accf_bar = [&](int b) { return bar0 + 8u * (11 + b); };
-  auto acce_bar = [&](int b) { return bar0 + 8u * (13 + b); };
-  const uint32_t drain_bar = bar0 + 8u * 15;
-  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 16);
+  auto rawe_bar = [&](int r) { return bar0 + 8u * (1 + kRawSlots + r); };
+  auto af_bar = [&](int b) { return bar0 + 8u * (1 + 2 * kRawSlots + b); };
+  auto ae_bar = [&](int b) { return bar0 + 8u * (1 + 2 * kRawSlots + kASlots + b); };
+  auto accf_bar = [&](int b) { return bar0 + 8u * (1 + 2 * kRawSlots + 2 * kASlots + b); };
+  auto acce_bar = [&](int b) { return bar0 + 8u * (1 + 2 * kRawSlots + 2 * kASlots + kAccSlots + b); };
+  const uint32_t drain_bar = bar0 + 8u * (num_barriers<NK>() - 1);
+  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + num_barriers<NK>());
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -310,9 +324,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
       mbar_init(rawf_bar(r), 1);
       mbar_init(rawe_bar(r), kTransposeWarps);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kASlots; ++b) {
       mbar_init(af_bar(b), kTransposeWarps);
       mbar_init(ae_bar(b), 1);
+    }
+    for (int b = 0; b < kAccSlots; ++b) {
       mbar_init(accf_bar(b), 1);
       mbar_init(acce_bar(b), kEpilogueWarps);
     }
@@ -365,9 +381,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
     const int tw = warp - kTransposeWarp0, r8 = lane >> 2, q4 = lane & 3;
     constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);  // (8-instance group, 16-k group)
     for (int i = 0; i < nu; ++i) {
-      const int b = i & 1, r = i % kRawSlots;
+      const int b = i % kASlots, r = i % kRawSlots;
       if (!warp_wait(rawf_bar(r), (i / kRawSlots) & 1, abort, args.err, lane)) break;
-      if (i >= 2 && !warp_wait(ae_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err, lane)) break;
+      if (i >= kASlots && !warp_wait(ae_bar(b), ((i / kASlots) & 1) ^ 1, abort, args.err, lane)) break;
       const uint32_t* raw = rawbuf + r * (G::kRawBytes / 4);
       uint8_t* at = a_tile + b * G::kABytes;
       for (int wu = tw; wu < kWarpUnits; wu += kTransposeWarps) {
@@ -407,21 +423,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
     constexpr uint32_t kIdesc = instr_desc(G::kNmma);
     bool ok = mbar_wait(bfull_bar, 0, abort, args.err);
     for (int i = 0; i < nu && ok; ++i) {
-      const int b = i & 1;
-      if (!mbar_wait(af_bar(b), (i >> 1) & 1, abort, args.err) ||
-          (i >= 2 && !mbar_wait(acce_bar(b), ((i >> 1) & 1) ^ 1, abort, args.err))) {
+      const int b = i % kASlots, c = i % kAccSlots;
+      if (!mbar_wait(af_bar(b), (i / kASlots) & 1, abort, args.err) ||
+          (i >= kAccSlots && !mbar_wait(acce_bar(c), ((i / kAccSlots) & 1) ^ 1, abort, args.err))) {
         ok = false;
         break;
       }
       tc_fence_after();
-      const uint32_t d_tmem = tmem + uint32_t(b * G::kNmma);
+      const uint32_t d_tmem = tmem + uint32_t(c * G::kNmma);
       const uint32_t a_base = a_addr + b * G::kABytes;
 #pragma unroll
       for (int st = 0; st < G::kSteps; ++st)
         mma_i8(d_tmem, smem_desc(a_base + st * 256, 128, G::kSbo), smem_desc(b_addr + st * 256, 128, G::kSbo),
                kIdesc, st > 0 ? 1u : 0u);
       mma_commit(ae_bar(b));
-      mma_commit(accf_bar(b));
+      mma_commit(accf_bar(c));
     }
   } else if (warp < kEpilogueWarps) {
     const uint32_t q = args.qinfo[2 * prime], qneg = args.qinfo[2 * prime + 1];
@@ -431,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
     const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
     constexpr int kHalf = NK / 2;  // outputs of this warp: [half * kHalf, half * kHalf + kHalf)
     for (int i = 0; i < nu; ++i) {
-      const int b = i & 1;
+      const int b = i % kAccSlots;
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
       uint32_t* dst = args.out + unit_poly(i) * int64_t(kPolyWords) + off;
       const uint32_t* tw = POST ? post + off : nullptr;
@@ -442,7 +458,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_pass(PassArgs args) {
 #pragma unroll
         for (int j = 0; j < kHalf; ++j) tws[j] = tw[(half * kHalf + j) * S];
       }
-      if (!warp_wait(accf_bar(b), (i >> 1) & 1, abort, args.err, lane)) break;
+      if (!warp_wait(accf_bar(b), (i / kAccSlots) & 1, abort, args.err, lane)) break;
       tc_fence_after();
 #pragma unroll
       for (int cc = 0; cc < kHalf / kChunk; ++cc) {
@@ -669,10 +685,11 @@ int launch_pass(const Context& c, const uint32_t* in, uint32_t* out, int pass, i
   auto kern = k_tc_ntt_pass<KIND, NK, POST>;
   const int smem = smem_bytes<NK>();
   if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return rc;
-  // persistent CTAs: at most one per SM (148), each streaming units of one prime
+  // persistent CTAs: as many as are resident at once (148 SMs), each
+  // streaming units of one prime
   const int64_t batch = polys / rows;
   const int64_t units = batch * Geom<NK>::kUnitsPerPoly;
-  int64_t per_row = 148 / rows;
+  int64_t per_row = 148 * Geom<NK>::kCtasPerSm / rows;
   if (per_row > units) per_row = units;
   if (per_row < 1) per_row = 1;
   PassArgs a{in, out, c.tc->bmat[pass], POST ? c.tc->post[pass] : nullptr, c.tc->qinfo, batch, rows,
