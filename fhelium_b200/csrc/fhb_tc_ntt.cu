@@ -446,17 +446,34 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     const int ml = quarter * 32 + lane;
     const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
     constexpr int kHalf = NK / 2;  // outputs of this warp: [half * kHalf, half * kHalf + kHalf)
+    // twiddles of the next unit are requested one unit ahead when they fit in
+    // registers (n = 16); otherwise all of a unit's are requested before its wait
+    constexpr bool kAhead = kHalf <= 8;
+    uint32_t tws_next[kHalf];
+    if (POST && kAhead && nu > 0) {
+      const uint32_t* tw0 = post + inst_offset<KIND>(unit_m0(0) + ml);
+#pragma unroll
+      for (int j = 0; j < kHalf; ++j) tws_next[j] = tw0[(half * kHalf + j) * S];
+    }
     for (int i = 0; i < nu; ++i) {
       const int b = i % kAccSlots;
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
       uint32_t* dst = args.out + unit_poly(i) * int64_t(kPolyWords) + off;
-      const uint32_t* tw = POST ? post + off : nullptr;
-      // all of this warp's twiddles for the unit are requested before the
-      // wait, so their latency hides behind it
       uint32_t tws[kHalf];
       if (POST) {
+        if (kAhead) {
 #pragma unroll
-        for (int j = 0; j < kHalf; ++j) tws[j] = tw[(half * kHalf + j) * S];
+          for (int j = 0; j < kHalf; ++j) tws[j] = tws_next[j];
+          if (i + 1 < nu) {
+            const uint32_t* tw1 = post + inst_offset<KIND>(unit_m0(i + 1) + ml);
+#pragma unroll
+            for (int j = 0; j < kHalf; ++j) tws_next[j] = tw1[(half * kHalf + j) * S];
+          }
+        } else {
+          const uint32_t* tw = post + off;
+#pragma unroll
+          for (int j = 0; j < kHalf; ++j) tws[j] = tw[(half * kHalf + j) * S];
+        }
       }
       if (!warp_wait(accf_bar(b), (i / kAccSlots) & 1, abort, args.err, lane)) break;
       tc_fence_after();
