@@ -212,9 +212,10 @@ def ntt_leg(dev, stream, steps):
         fwd()
         inv()
         out[tag]["roundtrip_bit_exact"] = bool(torch.equal(x, z))
-    # exact int8 tensor-core form: two 256 x 256 x 256 passes per direction
-    # over 4 x 4 byte-digit products; 2 N (n1 + n2) d_a d_b int8 operations
-    # per limb-polynomial and direction
+    # exact int8 tensor-core form: three passes (64 x 64 x 16) per direction
+    # over 4 x 4 byte-digit products; 2 N (n1 + n2 + n3) d_a d_b int8
+    # operations per limb-polynomial and direction; each pass reads and writes
+    # every residue once (3 HBM round trips per direction)
     tc = {}
     nat.check(ctx.lib.fhb_tc_ntt_prepare(ctx.handle), "tc prepare")
     tfwd = lambda: nat.check(ctx.lib.fhb_tc_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), B, L, 0, s), "tc ntt")
@@ -237,7 +238,7 @@ def ntt_leg(dev, stream, steps):
     flag = ctypes.c_int(-1)
     nat.check(ctx.lib.fhb_tc_ntt_status(ctx.handle, ctypes.byref(flag)), "tc status")
     tc["wait_timeouts"] = flag.value
-    int8_ops = B * L * 2 * N * (256 + 256) * 4 * 4
+    int8_ops = B * L * 2 * N * (64 + 64 + 16) * 4 * 4
     int8_peak, src = _int8_peak_tops()
     tc["int8_tops_forward"] = int8_ops / (tc["forward_ms"] / 1e3) / 1e12
     tc["int8_tops_inverse"] = int8_ops / (tc["inverse_ms"] / 1e3) / 1e12
@@ -247,6 +248,16 @@ def ntt_leg(dev, stream, steps):
     tc["tensor_frac_inverse"] = tc["int8_tops_inverse"] / int8_peak
     tc["forward_gbs"] = nbytes / (tc["forward_ms"] / 1e3) / 1e9
     tc["inverse_gbs"] = nbytes / (tc["inverse_ms"] / 1e3) / 1e9
+    # the passes' own HBM traffic (3 x read + write of every residue) against
+    # the measured copy bandwidth
+    try:
+        hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        hbm = 6650.0
+    tc["pass_traffic_gbs_forward"] = 3 * nbytes / (tc["forward_ms"] / 1e3) / 1e9
+    tc["pass_traffic_gbs_inverse"] = 3 * nbytes / (tc["inverse_ms"] / 1e3) / 1e9
+    tc["hbm_frac_forward"] = tc["pass_traffic_gbs_forward"] / hbm
+    tc["hbm_frac_inverse"] = tc["pass_traffic_gbs_inverse"] / hbm
     out["tensor_core"] = tc
     # integer-pipe roof: Shoup products per transform (N/2 log N butterflies
     # + the N x R or x N^-1 pass) against the int32 probe's rate

@@ -446,15 +446,28 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     const int ml = quarter * 32 + lane;
     const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
     constexpr int kHalf = NK / 2;  // outputs of this warp: [half * kHalf, half * kHalf + kHalf)
+    // a warp's kHalf twiddles of a unit: 16-byte vector loads where they are
+    // contiguous (stride 1), else one coalesced load per output column
+    auto load_tw = [&](const uint32_t* t, uint32_t (&v)[kHalf]) {
+      if (S == 1) {
+#pragma unroll
+        for (int j = 0; j < kHalf / 4; ++j) {
+          const uint4 x = *reinterpret_cast<const uint4*>(t + half * kHalf + 4 * j);
+          v[4 * j] = x.x;
+          v[4 * j + 1] = x.y;
+          v[4 * j + 2] = x.z;
+          v[4 * j + 3] = x.w;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < kHalf; ++j) v[j] = t[(half * kHalf + j) * S];
+      }
+    };
     // twiddles of the next unit are requested one unit ahead when they fit in
     // registers (n = 16); otherwise all of a unit's are requested before its wait
     constexpr bool kAhead = kHalf <= 8;
     uint32_t tws_next[kHalf];
-    if (POST && kAhead && nu > 0) {
-      const uint32_t* tw0 = post + inst_offset<KIND>(unit_m0(0) + ml);
-#pragma unroll
-      for (int j = 0; j < kHalf; ++j) tws_next[j] = tw0[(half * kHalf + j) * S];
-    }
+    if (POST && kAhead && nu > 0) load_tw(post + inst_offset<KIND>(unit_m0(0) + ml), tws_next);
     for (int i = 0; i < nu; ++i) {
       const int b = i % kAccSlots;
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
@@ -464,15 +477,9 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
         if (kAhead) {
 #pragma unroll
           for (int j = 0; j < kHalf; ++j) tws[j] = tws_next[j];
-          if (i + 1 < nu) {
-            const uint32_t* tw1 = post + inst_offset<KIND>(unit_m0(i + 1) + ml);
-#pragma unroll
-            for (int j = 0; j < kHalf; ++j) tws_next[j] = tw1[(half * kHalf + j) * S];
-          }
+          if (i + 1 < nu) load_tw(post + inst_offset<KIND>(unit_m0(i + 1) + ml), tws_next);
         } else {
-          const uint32_t* tw = post + off;
-#pragma unroll
-          for (int j = 0; j < kHalf; ++j) tws[j] = tw[(half * kHalf + j) * S];
+          load_tw(post + off, tws);
         }
       }
       if (!warp_wait(accf_bar(b), (i / kAccSlots) & 1, abort, args.err, lane)) break;
