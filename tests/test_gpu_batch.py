@@ -96,7 +96,8 @@ def test_autotune_picks_and_caches(small, tmp_path):
     ex = MixedBatchExecutor(eng, cts, ops, streams=1)
     path = str(tmp_path / "tune.json")
     first = autotune.tune_mixed_batch(eng, ex, streams=(1, 2), repeats=1, cache_path=path)
-    assert not first["cached"] and len(first["candidates"]) == 4
+    # three key-switch work orders x two branch counts
+    assert not first["cached"] and len(first["candidates"]) == 6
     assert (ex.streams, ex.ks_order) == (first["streams"], first["ks_order"])
     with open(path) as f:
         assert autotune.workload_key(eng, ex) in json.load(f)
