@@ -60,30 +60,18 @@ CONFIG = {
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return ws, rank, local
+    from fhelium_b200 import ranks
+    return ranks.init()
 
 
 def _barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from fhelium_b200 import ranks
+    ranks.barrier(ws)
 
 
 def _max_over_ranks(x: float, ws: int, device) -> float:
-    if ws == 1:
-        return x
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from fhelium_b200 import ranks
+    return ranks.max_over_ranks(x, ws, device)
 
 
 class ClockSampler:
@@ -531,7 +519,8 @@ def main() -> int:
         torch.cuda.synchronize(dev)
         _barrier(ws)
     ms = _max_over_ranks(ms, ws, dev)
-    value = ws * B / (ms / 1000.0)
+    from fhelium_b200 import ranks
+    value = ranks.job_rate(B, ws, ms)
     launches_per_step = 5  # tensor product, INTT of c2, ModUp digits, key-switch core, ModDown+rescale
 
     # ---- end to end through the public API with host buffers -------------
@@ -697,9 +686,8 @@ def main() -> int:
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
-    if ws > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from fhelium_b200 import ranks
+    ranks.finish(ws)
     return 0
 
 
