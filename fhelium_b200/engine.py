@@ -360,6 +360,31 @@ class CkksEngine:
     def galois_element_for_step(self, step: int) -> int:
         return galois_element(self.n, self._canonical_step(step) % self.n, self.galois_generator)
 
+    # --- value files (fhelium/serialization/safetensors.py:47-225) ---------
+    @property
+    def context_id(self) -> str:
+        """SHA-256 identity of this engine's context, as the reference computes
+        it (fhelium/core/context.py:72-83)."""
+        from .serialization import context_id
+        return context_id(self.config, self.galois_generator)
+
+    def save_value(self, value, path, *, allow_secret: bool = False, overwrite: bool = False) -> dict:
+        """Write a ciphertext or key to a value file readable by the reference's
+        fh.load_value (fhelium/serialization/safetensors.py:47-131)."""
+        from .serialization import save_value
+        return save_value(value, path, context_id=self.context_id, allow_secret=allow_secret, overwrite=overwrite)
+
+    def load_value(self, path, *, expected_type=None):
+        """Read a value file written by this library or the reference's
+        fh.save_value onto this engine's device; the file must belong to this
+        engine's context.  Rotation keys get this engine's Galois element."""
+        from .serialization import load_value
+        value = load_value(path, device=self.device, expected_type=expected_type,
+                           expected_context_id=self.context_id)
+        if isinstance(value, RotationKey):
+            value.galois_element = self.galois_element_for_step(value.rotation_step)
+        return value
+
     def rotation_key(self, rotation_step: int) -> RotationKey:
         step = self._canonical_step(rotation_step)
         if step not in self._rotation_keys:

@@ -1,0 +1,101 @@
+"""Value files interchangeable with the reference's (no GPU).
+
+tests/golden/values/*.safetensors were written by the reference's own
+fhelium.serialization.save_value (tests/golden/make_value_files.py).  Each
+must load with fhelium_b200.serialization with the same residues and
+metadata, and writing the loaded value back must reproduce the file's header
+metadata (the manifest text included) and payload exactly; the context id
+must match the reference's hash of the preset."""
+
+import os
+import shutil
+
+import pytest
+import torch
+from safetensors import safe_open
+
+from fhelium_b200 import serialization as ser
+from fhelium_b200.config import CkksConfig
+from fhelium_b200.values import Ciphertext, PublicKey, RelinearizationKey, RotationKey, SecretKey
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+VALUES = os.path.join(HERE, "golden", "values")
+FILES = {"ciphertext": Ciphertext, "public_key": PublicKey, "secret_key": SecretKey,
+         "relinearization_key": RelinearizationKey, "rotation_key": RotationKey}
+CID = ser.context_id(CkksConfig.parse("slots8192_scale40_levels7_int64"))
+
+
+def _payload(path):
+    with safe_open(path, framework="pt", device="cpu") as h:
+        return h.get_tensor("data")
+
+
+@pytest.mark.parametrize("name", sorted(FILES))
+def test_reference_files_load_and_round_trip(name, tmp_path):
+    path = os.path.join(VALUES, name + ".safetensors")
+    manifest = ser.inspect_value(path)
+    assert manifest["context_id"] == CID  # the reference's context hash, reproduced
+    value = ser.load_value(path, expected_type=FILES[name], expected_context_id=CID)
+    assert type(value) is FILES[name]
+    assert torch.equal(value.data, _payload(path))
+    if name == "ciphertext":
+        assert (value.level, value.scale) == (5, 2.0 ** 40)
+        assert (value.polynomial_domain, value.residue_representation, value.modulus_basis) == ("ntt", "montgomery",
+                                                                                               "Q")
+    if name == "rotation_key":
+        assert value.rotation_step == 3
+    out = tmp_path / (name + ".safetensors")
+    written = ser.save_value(value, out, context_id=CID, allow_secret=True)
+    assert written == manifest
+    # same header metadata strings (manifest text included) and payload; the
+    # safetensors writer orders header keys differently from run to run, so
+    # the files are compared entry by entry rather than byte by byte
+    with safe_open(str(out), framework="pt", device="cpu") as a, safe_open(path, framework="pt", device="cpu") as b:
+        assert a.metadata() == b.metadata()
+        assert list(a.keys()) == list(b.keys()) == ["data"]
+        assert torch.equal(a.get_tensor("data"), b.get_tensor("data"))
+
+
+def test_save_refuses_secret_keys_and_existing_files(tmp_path):
+    sk = ser.load_value(os.path.join(VALUES, "secret_key.safetensors"))
+    with pytest.raises(PermissionError):
+        ser.save_value(sk, tmp_path / "sk.safetensors", context_id=CID)
+    ct = ser.load_value(os.path.join(VALUES, "ciphertext.safetensors"))
+    ser.save_value(ct, tmp_path / "ct.safetensors", context_id=CID)
+    with pytest.raises(FileExistsError):
+        ser.save_value(ct, tmp_path / "ct.safetensors", context_id=CID)
+    ser.save_value(ct, tmp_path / "ct.safetensors", context_id=CID, overwrite=True)
+
+
+def test_load_rejects_mismatches(tmp_path):
+    path = os.path.join(VALUES, "ciphertext.safetensors")
+    with pytest.raises(ValueError):
+        ser.load_value(path, expected_context_id="0" * 64)
+    with pytest.raises(TypeError):
+        ser.load_value(path, expected_type=RotationKey)
+    # a manifest that lies about the shape is refused before the payload is used
+    from safetensors.torch import save_file
+    import json
+    with safe_open(path, framework="pt", device="cpu") as h:
+        meta = dict(h.metadata())
+        data = h.get_tensor("data")
+    manifest = json.loads(meta["fhelium.manifest"])
+    manifest["tensor_metadata"]["data"]["shape"][-1] = 8
+    bad = dict(meta, **{"fhelium.manifest": json.dumps(manifest, sort_keys=True, separators=(",", ":"))})
+    save_file({"data": data}, str(tmp_path / "bad.safetensors"), metadata=bad)
+    with pytest.raises(ValueError):
+        ser.load_value(tmp_path / "bad.safetensors")
+    wrong = dict(meta, **{"fhelium.format": "something-else"})
+    save_file({"data": data}, str(tmp_path / "wrong.safetensors"), metadata=wrong)
+    with pytest.raises(ValueError):
+        ser.inspect_value(tmp_path / "wrong.safetensors")
+    shutil.copy(path, tmp_path / "ok.safetensors")
+    assert ser.load_value(tmp_path / "ok.safetensors").level == 5
+
+
+def test_engine_context_id_matches_the_files():
+    from fhelium_b200.engine import CkksEngine
+    eng = CkksEngine.__new__(CkksEngine)  # context id needs only the parameters
+    eng.config = CkksConfig.parse("slots8192_scale40_levels7_int64")
+    eng.galois_generator = 3
+    assert eng.context_id == CID
