@@ -29,7 +29,7 @@ SRCS=(
   "$REF/csrc/ops/ntt/cpu/indexed_ntt_cpu.cpp"
   "$REF/csrc/ops/ckks/cpu/ckks_cpu.cpp"
 )
-# System g++ (see the note on TORCH_CHECK exceptions in DESIGN.md).
+# System g++ by default; CXX_REF overrides it.
 CXX=${CXX_REF:-/usr/bin/g++}
 OBJS=()
 for s in "${SRCS[@]}"; do
