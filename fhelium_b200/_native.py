@@ -61,6 +61,20 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_rns_add_constant": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_relinearize_noalloc": (_I, [_P, _P, _P, _P, _I64, _I, _I, _P]),
     "fhb_ckks_relinearize_noalloc_max_scratch_bytes": (_I64, []),
+    # operator-level entry points (the reference's custom-op schemas)
+    "fhb_op_rns_binary": (_I, [_I, _I, _P, _I64, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _I64, _P]),
+    "fhb_op_rns_unary": (_I, [_I, _I, _P, _I64, _I64, _I, _I64, _P, _I64, _P]),
+    "fhb_op_lift_centered": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P]),
+    "fhb_op_mixed_radix_decompose": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P, _I64, _P, _P, _P, _P,
+                                          _P]),
+    "fhb_op_basis_extend": (_I, [_I, _P, _I64, _I, _P, _I64, _I64, _I, _I64, _P, _I64, _P, _I64, _P]),
+    "fhb_op_keyswitch_accumulate": (_I, [_I, _P, _I64, _P, _I64, _P, _I64, _P, _I64, _I64, _I64, _I, _I64, _P,
+                                         _I64, _P]),
+    "fhb_op_moddown": (_I, [_I, _P, _I64, _P, _I64, _P, _I64, _I64, _I, _I, _I64, _P, _I64, _P, _I64, _P]),
+    "fhb_op_rescale": (_I, [_I, _P, _I64, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P, _I64, _I64, _I, _P]),
+    "fhb_op_coefficient_automorphism": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P, _P, _P]),
+    "fhb_op_ntt_automorphism": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P]),
+    "fhb_context_create_transform": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, ctypes.POINTER(_P)]),
 }
 
 TUNE_KS_ORDER, TUNE_NTT_FORWARD_EPT, TUNE_NTT_INVERSE_EPT = range(3)
@@ -134,6 +148,19 @@ class NativeContext:
         self.handle = handle
         self.lib = lib
         self.device = device
+
+    @classmethod
+    def transform(cls, residue_bits: int, log_n: int, moduli, device: torch.device) -> "NativeContext":
+        """A context whose prime ids 0..len(moduli)-1 are exactly `moduli`, for
+        the transforms and element-wise entry points (fhb_context_create_transform)."""
+        self = cls.__new__(cls)
+        lib = load()
+        arr = (ctypes.c_uint64 * len(moduli))(*[int(m) for m in moduli])
+        handle = _P()
+        check(lib.fhb_context_create_transform(residue_bits, log_n, arr, len(moduli), device.index or 0,
+                                               ctypes.byref(handle)), "fhb_context_create_transform")
+        self.handle, self.lib, self.device = handle, lib, device
+        return self
 
     def root(self, prime_id: int) -> int:
         out = ctypes.c_uint64()

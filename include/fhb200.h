@@ -331,6 +331,111 @@ int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t
                           void* out, void* scratch, int64_t scratch_bytes, int64_t batch, int level,
                           fhb_stream stream);
 
+/* ------------------------------------------------------------------------
+ * Operator-level entry points: one kernel per custom op of the reference,
+ * taking the reference's own operands, so that its operator schemas
+ * (torch.ops.fhelium_{rns,ntt,ckks}_ops) can be served on B200 without a
+ * chain context (fhelium_b200/torch_ops.py registers them).
+ *
+ * residue_bits selects the word (64: int64 family, 32: int32 family); every
+ * table has that word type.  A residue operand is [batch, rows, n] with rows
+ * n words apart and coefficients contiguous; *_batch_stride is its distance
+ * between batch items in words (0 broadcasts a single item).  `params` is the
+ * reference's [8, limb] parameter tensor (rows {2q, q_lo, q_hi, -q^-1 lo,
+ * -q^-1 hi, R^2, Delta R^2, N^-1 R}, csrc/ops/common/rns_parameters.h:6-16)
+ * sliced to the operand's limbs: column j describes row j, rows
+ * param_row_stride words apart.  Outputs carry the integers the reference's
+ * CPU kernels return.  In-place entry points update their operand; outputs
+ * of the others must not overlap their inputs. */
+
+/* op 0 montgomery_mul (canonical), 1 add_lazy, 2 sub_lazy ([0, 2q)),
+ * 3 add_canonical, 4 sub_canonical; rhs_batch_stride 0 = singleton rhs batch.
+ * Replaces fhelium_rns_ops.{montgomery_mul, add_lazy, sub_lazy,
+ * add_canonical(_), sub_canonical(_)} (csrc/ops/rns/rns_arithmetic.cpp:31,46,50,
+ * csrc/ops/rns/rns_canonical_arithmetic.cpp:16-21). */
+int fhb_op_rns_binary(int residue_bits, int op, const void* lhs, int64_t lhs_batch_stride, const void* rhs,
+                      int64_t rhs_batch_stride, void* out, int64_t out_batch_stride, int64_t batch, int rows,
+                      int64_t n, const void* params, int64_t param_row_stride, fhb_stream stream);
+/* In place: op 0 to_montgomery_, 1 from_montgomery_ (canonical),
+ * 2 canonicalize_residues_, 3 center_residues_, 4 shift_residues_positive_
+ * (csrc/ops/rns/rns_arithmetic.cpp:41-59). */
+int fhb_op_rns_unary(int residue_bits, int op, void* residues, int64_t batch_stride, int64_t batch, int rows,
+                     int64_t n, const void* params, int64_t param_row_stride, fhb_stream stream);
+/* out[b, j, k] = coefficients[b, k] + q_j (q_j = twice_modulus[j] / 2).
+ * Replaces fhelium_rns_ops.lift_centered_coefficients
+ * (csrc/ops/rns/rns_arithmetic.cpp:60-62). */
+int fhb_op_lift_centered(int residue_bits, const void* coefficients, int64_t coefficient_batch_stride, void* out,
+                         int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* twice_modulus,
+                         fhb_stream stream);
+/* Garner mixed-radix digits of one hybrid digit (rows <= 8); normalizers
+ * [rows - 1], propagation [rows - 1, propagation_row_stride], the four
+ * split-word vectors [rows].  Replaces fhelium_rns_ops.mixed_radix_decompose
+ * (csrc/ops/rns/rns_arithmetic.cpp:63-68). */
+int fhb_op_mixed_radix_decompose(int residue_bits, const void* source, int64_t source_batch_stride, void* out,
+                                 int64_t out_batch_stride, int64_t batch, int rows, int64_t n,
+                                 const void* normalizers, const void* propagation, int64_t propagation_row_stride,
+                                 const void* modulus_lo, const void* modulus_hi, const void* neg_inv_modulus_lo,
+                                 const void* neg_inv_modulus_hi, fhb_stream stream);
+/* Exact basis extension of digit_rows mixed-radix digits into
+ * destination_rows Montgomery/lazy rows; coefficients [digit_rows - 1,
+ * coefficient_row_stride] (column j for destination row j).  Replaces
+ * fhelium_rns_ops.mixed_radix_basis_extend_to_montgomery
+ * (csrc/ops/rns/rns_arithmetic.cpp:69-72). */
+int fhb_op_basis_extend(int residue_bits, const void* digits, int64_t digits_batch_stride, int digit_rows,
+                        void* out, int64_t out_batch_stride, int64_t batch, int destination_rows, int64_t n,
+                        const void* coefficients, int64_t coefficient_row_stride, const void* params,
+                        int64_t param_row_stride, fhb_stream stream);
+/* In place: acc_c[b, j] += digit[b, j] * key[c, key_row_start + j] (c = 0, 1;
+ * key component c at key_digit + c * key_component_stride words).  Replaces
+ * fhelium_ckks_ops.keyswitch_accumulate_digit_products_
+ * (csrc/ops/ckks/ckks.cpp:85-88, csrc/ops/ckks/cuda/keyswitch_cuda.cu:198-292). */
+int fhb_op_keyswitch_accumulate(int residue_bits, void* acc0, int64_t acc0_batch_stride, void* acc1,
+                                int64_t acc1_batch_stride, const void* digit, int64_t digit_batch_stride,
+                                const void* key_digit, int64_t key_component_stride, int64_t key_row_start,
+                                int64_t batch, int rows, int64_t n, const void* params, int64_t param_row_stride,
+                                fhb_stream stream);
+/* ModDown of coefficient/standard Q and P rows (p_rows <= 16) to canonical Q
+ * rows; inverses [p_rows, inverse_row_stride]; params covers q_rows + p_rows
+ * columns.  Replaces fhelium_ckks_ops.keyswitch_moddown_qp_to_q
+ * (csrc/ops/ckks/ckks.cpp:82-84, csrc/ops/ckks/cuda/keyswitch_cuda.cu:55-196). */
+int fhb_op_moddown(int residue_bits, const void* q_residues, int64_t q_batch_stride, const void* p_residues,
+                   int64_t p_batch_stride, void* out, int64_t out_batch_stride, int64_t batch, int q_rows,
+                   int p_rows, int64_t n, const void* inverses, int64_t inverse_row_stride, const void* params,
+                   int64_t param_row_stride, fhb_stream stream);
+/* Drop the leading prime: remaining [batch, rows, n], dropped [batch, n],
+ * inverse_montgomery [rows]; nearest = 1 rounds (half_drop_prime =
+ * floor(q_drop / 2)), 0 truncates.  Canonical output; out may equal
+ * remaining.  Replaces fhelium_ckks_ops.rescale_drop_leading_prime_{nearest,
+ * truncate}(_) (csrc/ops/ckks/ckks.cpp:60-75, csrc/ops/ckks/cuda/
+ * rescale_cuda.cu:22-54). */
+int fhb_op_rescale(int residue_bits, const void* remaining, int64_t remaining_batch_stride, const void* dropped,
+                   int64_t dropped_batch_stride, void* out, int64_t out_batch_stride, int64_t batch, int rows,
+                   int64_t n, const void* inverse_montgomery, const void* params, int64_t param_row_stride,
+                   int64_t half_drop_prime, int nearest, fhb_stream stream);
+/* Coefficient-domain automorphism from the reference's maps: out[k] =
+ * sign[k] * in[source_indices[k]], canonical.  Replaces
+ * fhelium_ckks_ops.apply_coefficient_galois_automorphism
+ * (csrc/ops/ckks/ckks.cpp:76-78, csrc/ops/ckks/cuda/automorphism_cuda.cu:15-31). */
+int fhb_op_coefficient_automorphism(int residue_bits, const void* in, int64_t in_batch_stride, void* out,
+                                    int64_t out_batch_stride, int64_t batch, int rows, int64_t n,
+                                    const int32_t* source_indices, const int8_t* source_sign,
+                                    const void* twice_moduli, fhb_stream stream);
+/* NTT-domain automorphism: out[k] = in[source_indices[k]].  Replaces
+ * fhelium_ckks_ops.apply_ntt_galois_automorphism (csrc/ops/ckks/ckks.cpp:79-81,
+ * csrc/ops/ckks/cuda/automorphism_cuda.cu:33-44). */
+int fhb_op_ntt_automorphism(int residue_bits, const void* in, int64_t in_batch_stride, void* out,
+                            int64_t out_batch_stride, int64_t batch, int rows, int64_t n,
+                            const int32_t* source_indices, fhb_stream stream);
+/* A context whose prime ids 0..count-1 are exactly `moduli` (plus one
+ * auxiliary special prime of the library's choosing at id `count`), for the
+ * transforms (fhb_forward_ntt, fhb_inverse_ntt, tensor-core forms) and the
+ * element-wise entry points of a parameter-row slice.  Used to serve the
+ * reference's NTT schemas, whose operands carry a slice of rows rather than a
+ * chain (csrc/ops/ntt/forward_ntt.cpp:25-67, inverse_ntt.cpp:23-73).  Set-up:
+ * allocates and copies synchronously. */
+int fhb_context_create_transform(int residue_bits, int log_n, const uint64_t* moduli, int count, int device,
+                                 fhb_context** out);
+
 #ifdef __cplusplus
 }
 #endif

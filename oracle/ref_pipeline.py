@@ -57,19 +57,28 @@ def _schedule(log_n: int):
 
 
 class ReferenceCpuPipeline:
-    def __init__(self, ctx: OracleContext, threads: int | None = None):
-        if not available():
+    """The reference engine's operator sequence.  On "cpu" it runs the
+    reference's own CPU operators (oracle/_ref, required).  With a CUDA
+    `device` the same calls dispatch to whatever CUDA kernels are registered
+    for the reference's schemas (the reference's library is loaded first when
+    present, so that its schema definitions are the ones in use)."""
+
+    def __init__(self, ctx: OracleContext, threads: int | None = None, device: str | torch.device = "cpu"):
+        device = torch.device(device)
+        if device.type == "cpu" and not available():
             raise FileNotFoundError(REF_LIB)
-        torch.ops.load_library(REF_LIB)
+        if available():
+            torch.ops.load_library(REF_LIB)
         if threads:
             torch.set_num_threads(threads)
         self.ctx = ctx
+        self.device = device
         self.dtype = torch.int64 if ctx.radix_bits == 62 else torch.int32
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.dtype)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.dtype).to(device)
         self.params = t(ctx.params)
         fe, fo, ft, ie, io, it = _schedule(ctx.log_n)
         fwd, inv = ctx.twiddles
-        self.fe, self.fo, self.ie, self.io = fe, fo, ie, io
+        self.fe, self.fo, self.ie, self.io = (x.to(device) for x in (fe, fo, ie, io))
         self.fwd_stage = t(np.stack([fwd[j][ft] for j in range(len(ctx.moduli))]))
         self.inv_stage = t(np.stack([inv[j][it] for j in range(len(ctx.moduli))]))
         self._t = t

@@ -1,0 +1,84 @@
+"""Host side of the schema registrations (fhelium_b200.torch_ops), no GPU.
+
+The schemas this library serves must be the reference's own (same names,
+argument names and types, mutability annotations), every one of them must get
+a CUDA kernel, the indexed-NTT schedule it accepts must be the reference's
+radix-2 plan, and operands must be viewed without copies exactly when their
+layout allows it."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ref_pipeline
+
+
+@pytest.fixture(scope="module")
+def torch_ops():
+    if ref_pipeline.available():
+        torch.ops.load_library(ref_pipeline.REF_LIB)   # schema definitions of the reference itself
+    from fhelium_b200 import _native, torch_ops
+    try:
+        _native.load()
+    except _native.NativeLibraryError:
+        pytest.skip("libfhb200.so not built")
+    torch_ops.register()
+    return torch_ops
+
+
+def test_every_served_schema_has_a_cuda_kernel(torch_ops):
+    served = torch_ops.served()
+    assert len(served) == 38
+    for qualname in served:
+        assert torch._C._dispatch_has_kernel_for_dispatch_key(qualname, "CUDA"), qualname
+    torch_ops.register()   # idempotent
+
+
+def test_schemas_are_the_references(torch_ops):
+    if not ref_pipeline.available():
+        pytest.skip("reference operator library not built")
+    for ns, ops in torch_ops.SCHEMAS.items():
+        for name, schema in ops.items():
+            got = str(torch._C._dispatch_find_schema_or_throw(f"{ns}::{name}", "").schema())
+            assert got == f"{ns}::{schema}", (got, schema)
+
+
+@pytest.mark.parametrize("log_n", [4, 10, 12, 16])
+def test_radix2_schedule_is_the_references_plan(torch_ops, log_n):
+    fe, fo, _, ie, io, _ = ref_pipeline._schedule(log_n)
+    e, o = torch_ops._radix2_schedule(log_n, False)
+    assert np.array_equal(e, fe.numpy()) and np.array_equal(o, fo.numpy())
+    e, o = torch_ops._radix2_schedule(log_n, True)
+    assert np.array_equal(e, ie.numpy()) and np.array_equal(o, io.numpy())
+
+
+def test_operand_views(torch_ops):
+    bv = torch_ops._batch_view
+    x = torch.zeros(3, 4, 5, 16, dtype=torch.int64)
+    assert bv(x) == (12, 80)
+    assert bv(x[:, :, 1:]) == (12, 80)            # limb slice: batch stride of the parent
+    assert bv(x[:, 1]) == (3, 320)
+    assert bv(x[0, 0]) == (1, 80)
+    assert bv(x[..., ::2]) is None                 # strided coefficients
+    assert bv(x[:, :, ::2]) is None                # rows not N apart
+    assert bv(x.transpose(0, 1)) is None           # batch dims that do not collapse
+    assert bv(x[:, :, 0], rows_dims=1) == (12, 80)
+    assert bv(x[:1].expand(3, -1, -1, -1)) is None   # a broadcast batch (stride 0) is not a view
+
+
+def test_operand_copy_back(torch_ops):
+    x = torch.arange(2 * 3 * 8, dtype=torch.int64).reshape(2, 3, 8)
+    t = x.transpose(0, 1)                          # [3, 2, 8]: batch dims do not collapse with rows
+    op = torch_ops._Operand(t[:, :, ::2].transpose(0, 1), writable=True)
+    assert op.copied
+    op.t.zero_()
+    op.finish()
+    assert int(x[:, :, ::2].abs().sum()) == 0 and int(x[:, :, 1::2].abs().sum()) > 0
+
+
+def test_find_run(torch_ops):
+    chain = (5, 7, 11, 13, 17)
+    assert torch_ops._find_run(chain, (11, 13)) == 2
+    assert torch_ops._find_run(chain, chain) == 0
+    assert torch_ops._find_run(chain, (7, 13)) is None
+    assert torch_ops._find_run(chain, (17, 19)) is None
