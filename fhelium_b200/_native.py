@@ -74,6 +74,10 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_op_rescale": (_I, [_I, _P, _I64, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P, _I64, _I64, _I, _P]),
     "fhb_op_coefficient_automorphism": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P, _P, _P]),
     "fhb_op_ntt_automorphism": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P]),
+    "fhb_op_mul_compressed": (_I, [_I, _I, _P, _I64, _P, _I64, _I64, _P, _I64, _I64, _I, _I64, _P, _I64, _P]),
+    "fhb_op_add_plaintext": (_I, [_I, _I, _P, _I64, _P, _I64, _I64, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _I64,
+                                  _P]),
+    "fhb_op_mul_row_scalars": (_I, [_I, _P, _I64, _P, _I64, _I64, _I, _I64, _P, _P, _I64, _P]),
     "fhb_context_create_transform": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, ctypes.POINTER(_P)]),
 }
 

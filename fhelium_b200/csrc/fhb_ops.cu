@@ -299,6 +299,72 @@ __global__ void k_op_ntt_automorphism(const T* __restrict__ in, int64_t is, T* _
   for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) out[bi * os + row * n + k] = in[bi * is + row * n + from];
 }
 
+// Index of the stored plaintext word for coefficient k: 0 dense, 1 cyclic
+// repetition (k mod U), 2 contiguous repetition (k / (N / U)), 3 strided
+// support (every (N / U)-th coefficient stored, the rest implicit)
+// (csrc/ops/common/cuda/repetition.cuh:69-86, csrc/ops/ckks/cuda/plaintext_cuda.cu:93-114).
+__device__ __forceinline__ int64_t plaintext_index(int layout, int64_t k, int64_t unique_mask, int shift) {
+  switch (layout) {
+    case 1: return k & unique_mask;
+    case 2: return k >> shift;
+    case 3: return (k & unique_mask) == 0 ? (k >> shift) : -1;
+    default: return k;
+  }
+}
+
+// out = lhs * rhs[index(k)] (Montgomery, canonical): montgomery_mul with a
+// repeated (compressed) right operand.
+template <typename T>
+__global__ void k_op_mul_compressed(int layout, const T* __restrict__ a, int64_t as, const T* __restrict__ b,
+                                    int64_t bs, int64_t unique, int64_t unique_mask, int shift, T* __restrict__ out,
+                                    int64_t os, int64_t batch, int64_t n, const T* __restrict__ params, int64_t ps) {
+  FHB_OP_INDEX
+  const ColumnPrime<T> p = column_prime(params, ps, row);
+  const int64_t idx = plaintext_index(layout, k, unique_mask, shift);
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z)
+    out[bi * os + row * n + k] =
+        mont_canonical(a[bi * as + row * n + k], b[bi * bs + row * unique + idx], p.q, p.neg_inv);
+}
+
+// Plaintext addition to a standard-form ciphertext component: c + p R^-1,
+// canonical, p a coefficient-domain Montgomery residue
+// (csrc/ops/ckks/cuda/plaintext_cuda.cu:1-47).  Strided layout: coefficients
+// off the support take implicit[b, row].
+template <typename T>
+__global__ void k_op_add_plaintext(int layout, const T* __restrict__ ct, int64_t cs, const T* __restrict__ pt,
+                                   int64_t pbs, int64_t extent, int64_t unique_mask, int shift,
+                                   const T* __restrict__ implicit, int64_t ibs, T* __restrict__ out, int64_t os,
+                                   int64_t batch, int64_t n, const T* __restrict__ params, int64_t ps) {
+  FHB_OP_INDEX
+  const ColumnPrime<T> p = column_prime(params, ps, row);
+  const int64_t idx = plaintext_index(layout, k, unique_mask, shift);
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
+    const T pv = idx >= 0 ? pt[bi * pbs + row * extent + idx] : implicit[bi * ibs + row];
+    T v = mont_canonical(ct[bi * cs + row * n + k], p.r2, p.q, p.neg_inv);
+    v = add_lazy2(v, pv, p.twice_q);
+    out[bi * os + row * n + k] = mont_canonical(v, T(1), p.q, p.neg_inv);
+  }
+}
+
+// out = x * scalars[row] (Montgomery, canonical)
+// (csrc/ops/rns/cuda/rns_arithmetic_cuda.cu:175-191).
+template <typename T>
+__global__ void k_op_mul_row_scalars(const T* __restrict__ x, int64_t xs, T* __restrict__ out, int64_t os,
+                                     int64_t batch, int64_t n, const T* __restrict__ scalars,
+                                     const T* __restrict__ params, int64_t ps) {
+  FHB_OP_INDEX
+  const ColumnPrime<T> p = column_prime(params, ps, row);
+  const T s = scalars[row];
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z)
+    out[bi * os + row * n + k] = mont_canonical(x[bi * xs + row * n + k], s, p.q, p.neg_inv);
+}
+
+int log2_exact(int64_t v) {
+  int s = 0;
+  while ((int64_t{1} << s) < v) ++s;
+  return (int64_t{1} << s) == v ? s : -1;
+}
+
 dim3 op_grid(int64_t n, int64_t rows, int64_t batch) {
   const int64_t z = batch < 65535 ? batch : 65535;
   return dim3(static_cast<unsigned>((n + kOpThreads - 1) / kOpThreads), static_cast<unsigned>(rows),
@@ -491,6 +557,64 @@ int fhb_op_ntt_automorphism(int residue_bits, const void* in, int64_t in_batch_s
                fhb::k_op_ntt_automorphism<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0,
                                                (cudaStream_t)stream>>>(
                    (const T*)in, in_batch_stride, (T*)out, out_batch_stride, batch, n, source_indices))
+  return fhb::launch_status();
+}
+
+int fhb_op_mul_compressed(int residue_bits, int layout, const void* lhs, int64_t lhs_batch_stride,
+                          const void* compressed_rhs, int64_t rhs_batch_stride, int64_t unique, void* out,
+                          int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* params,
+                          int64_t param_row_stride, fhb_stream stream) {
+  if (int rc = fhb::check_shape(residue_bits, batch, rows, n)) return rc;
+  if (layout != 1 && layout != 2) return fail(-2, "layout must be 1 (cyclic) or 2 (contiguous)");
+  const int un = fhb::log2_exact(unique), nn = fhb::log2_exact(n);
+  if (un < 0 || nn < 0 || unique >= n) return fail(-4, "unique count must be a power of two below the ring dimension");
+  if (fhb::empty(batch, rows, n)) return 0;
+  FHB_NONNULL(lhs) FHB_NONNULL(compressed_rhs) FHB_NONNULL(out) FHB_NONNULL(params)
+  FHB_DISPATCH(residue_bits,
+               fhb::k_op_mul_compressed<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0,
+                                             (cudaStream_t)stream>>>(
+                   layout, (const T*)lhs, lhs_batch_stride, (const T*)compressed_rhs, rhs_batch_stride, unique,
+                   unique - 1, nn - un, (T*)out, out_batch_stride, batch, n, (const T*)params, param_row_stride))
+  return fhb::launch_status();
+}
+
+int fhb_op_add_plaintext(int residue_bits, int layout, const void* ciphertext, int64_t ciphertext_batch_stride,
+                         const void* plaintext, int64_t plaintext_batch_stride, int64_t plaintext_extent,
+                         const void* implicit_plaintext, int64_t implicit_batch_stride, void* out,
+                         int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* params,
+                         int64_t param_row_stride, fhb_stream stream) {
+  if (int rc = fhb::check_shape(residue_bits, batch, rows, n)) return rc;
+  if (layout < 0 || layout > 3) return fail(-2, "layout must be 0 (dense), 1 (cyclic), 2 (contiguous) or 3 (strided)");
+  const int un = fhb::log2_exact(plaintext_extent), nn = fhb::log2_exact(n);
+  if (layout == 0 && plaintext_extent != n) return fail(-4, "a dense plaintext has N coefficients per row");
+  if (layout != 0 && (un < 0 || nn < 0 || plaintext_extent > n || (layout != 3 && plaintext_extent == n)))
+    return fail(-4, "plaintext extent must be a power of two below the ring dimension");
+  if (layout == 3 && !implicit_plaintext) return fail(-1, "implicit_plaintext is NULL");
+  if (fhb::empty(batch, rows, n)) return 0;
+  FHB_NONNULL(ciphertext) FHB_NONNULL(plaintext) FHB_NONNULL(out) FHB_NONNULL(params)
+  // cyclic: k mod U; contiguous: k >> log2(N/U); strided: support mask N/U - 1, shift log2(N/U)
+  const int64_t mask = layout == 1 ? plaintext_extent - 1 : layout == 3 ? (n / plaintext_extent) - 1 : 0;
+  const int shift = layout >= 2 ? nn - un : 0;
+  FHB_DISPATCH(residue_bits,
+               fhb::k_op_add_plaintext<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0,
+                                            (cudaStream_t)stream>>>(
+                   layout, (const T*)ciphertext, ciphertext_batch_stride, (const T*)plaintext,
+                   plaintext_batch_stride, plaintext_extent, mask, shift, (const T*)implicit_plaintext,
+                   implicit_batch_stride, (T*)out, out_batch_stride, batch, n, (const T*)params, param_row_stride))
+  return fhb::launch_status();
+}
+
+int fhb_op_mul_row_scalars(int residue_bits, const void* residues, int64_t residues_batch_stride, void* out,
+                           int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* row_scalars,
+                           const void* params, int64_t param_row_stride, fhb_stream stream) {
+  if (int rc = fhb::check_shape(residue_bits, batch, rows, n)) return rc;
+  if (fhb::empty(batch, rows, n)) return 0;
+  FHB_NONNULL(residues) FHB_NONNULL(out) FHB_NONNULL(row_scalars) FHB_NONNULL(params)
+  FHB_DISPATCH(residue_bits,
+               fhb::k_op_mul_row_scalars<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0,
+                                              (cudaStream_t)stream>>>(
+                   (const T*)residues, residues_batch_stride, (T*)out, out_batch_stride, batch, n,
+                   (const T*)row_scalars, (const T*)params, param_row_stride))
   return fhb::launch_status();
 }
 

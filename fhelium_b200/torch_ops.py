@@ -23,8 +23,10 @@ B200 unchanged.
   (``fhb_context_create_transform``), built on first use and cached.  The NTT
   uses the reference's root choice; the twiddle tensor passed in is checked once
   (its psi entry) and the indexed forms' schedules once (against the reference's
-  radix-2 schedule); grouped_stage_count only picks a launch shape in the
-  reference and is ignored here.
+  radix-2 schedule) -- once per table tensor and version, remembered through a
+  weak reference, so a new table at a reused address is checked again;
+  grouped_stage_count and shared_memory_log_n only pick launch shapes in the
+  reference and are ignored here.
 * Outputs carry the integers of the reference's CPU kernels, except the NTT
   outputs, which are lazy [0, 2q) like the reference's CUDA kernels (equal mod q).
 * Errors are ``RuntimeError`` (bad dtype, device, shape, overlapping in-place
@@ -38,6 +40,7 @@ B200 unchanged.
 from __future__ import annotations
 
 import threading
+import weakref
 
 import numpy as np
 import torch
@@ -61,6 +64,16 @@ SCHEMAS: dict[str, dict[str, str]] = {
         "shift_residues_positive_": "shift_residues_positive_(Tensor(a!) centered_residues, Tensor rns_params) -> ()",
         "lift_centered_coefficients": "lift_centered_coefficients(Tensor centered_coefficients, "
                                       "Tensor twice_modulus) -> Tensor",
+        "montgomery_mul_cyclic_compressed": "montgomery_mul_cyclic_compressed(Tensor lhs, Tensor compressed_rhs, "
+                                            "Tensor rns_params) -> Tensor",
+        "montgomery_mul_contiguous_compressed": "montgomery_mul_contiguous_compressed(Tensor lhs, "
+                                                "Tensor compressed_rhs, Tensor rns_params) -> Tensor",
+        "montgomery_mul_row_scalars_": "montgomery_mul_row_scalars_(Tensor(a!) residues, Tensor row_scalars, "
+                                       "Tensor rns_params) -> ()",
+        "montgomery_mul_row_scalars_canonical": "montgomery_mul_row_scalars_canonical(Tensor residues, "
+                                                "Tensor row_scalars, Tensor rns_params) -> Tensor",
+        "add_lazy_with_twice_modulus": "add_lazy_with_twice_modulus(Tensor lhs, Tensor rhs, "
+                                       "Tensor twice_modulus) -> Tensor",
         "mixed_radix_decompose": "mixed_radix_decompose(Tensor source_residues, Tensor mixed_radix_normalizers, "
                                  "Tensor mixed_radix_propagation_coefficients, Tensor modulus_lo, "
                                  "Tensor modulus_hi, Tensor neg_inv_modulus_lo, Tensor neg_inv_modulus_hi) -> Tensor",
@@ -92,6 +105,46 @@ SCHEMAS: dict[str, dict[str, str]] = {
                                                                 "forward_twiddles, Tensor rns_params, Tensor "
                                                                 "key_digit_qp, Tensor(b!) accumulator0_qp, "
                                                                 "Tensor(c!) accumulator1_qp, int key_row_start) -> ()",
+        "forward_ntt_montgomery_power_of_two_radix_compact_": "forward_ntt_montgomery_power_of_two_radix_compact_("
+                                                              "Tensor(a!) montgomery_residues, Tensor outer_twiddles, "
+                                                              "Tensor radix_root_powers, Tensor rns_params) -> ()",
+        "forward_ntt_to_montgomery_power_of_two_radix_compact_": "forward_ntt_to_montgomery_power_of_two_radix_"
+                                                                 "compact_(Tensor(a!) standard_residues, Tensor "
+                                                                 "outer_twiddles, Tensor radix_root_powers, "
+                                                                 "Tensor rns_params) -> ()",
+        "forward_ntt_to_montgomery_power_of_two_radix_compact": "forward_ntt_to_montgomery_power_of_two_radix_"
+                                                                "compact(Tensor standard_residues, Tensor "
+                                                                "outer_twiddles, Tensor radix_root_powers, "
+                                                                "Tensor rns_params) -> Tensor",
+        "forward_ntt_montgomery_compact_grouped_smem_override_": "forward_ntt_montgomery_compact_grouped_smem_"
+                                                                 "override_(Tensor(a!) montgomery_residues, Tensor "
+                                                                 "forward_twiddles, Tensor rns_params, int "
+                                                                 "grouped_stage_count, int shared_memory_log_n) -> ()",
+        "forward_ntt_montgomery_power_of_two_radix_compact_override_": "forward_ntt_montgomery_power_of_two_radix_"
+                                                                       "compact_override_(Tensor(a!) "
+                                                                       "montgomery_residues, Tensor outer_twiddles, "
+                                                                       "Tensor radix_root_powers, Tensor rns_params, "
+                                                                       "int shared_memory_log_n) -> ()",
+        "inverse_ntt_montgomery_power_of_two_radix_compact_": "inverse_ntt_montgomery_power_of_two_radix_compact_("
+                                                              "Tensor(a!) montgomery_residues, Tensor outer_twiddles, "
+                                                              "Tensor radix_root_powers, Tensor rns_params) -> ()",
+        "inverse_ntt_to_standard_lazy_power_of_two_radix_compact_": "inverse_ntt_to_standard_lazy_power_of_two_"
+                                                                    "radix_compact_(Tensor(a!) montgomery_residues, "
+                                                                    "Tensor outer_twiddles, Tensor radix_root_powers, "
+                                                                    "Tensor rns_params) -> ()",
+        "inverse_ntt_to_standard_power_of_two_radix_compact_": "inverse_ntt_to_standard_power_of_two_radix_compact_("
+                                                               "Tensor(a!) montgomery_residues, Tensor "
+                                                               "outer_twiddles, Tensor radix_root_powers, "
+                                                               "Tensor rns_params) -> ()",
+        "inverse_ntt_to_centered_power_of_two_radix_compact_": "inverse_ntt_to_centered_power_of_two_radix_compact_("
+                                                               "Tensor(a!) montgomery_residues, Tensor "
+                                                               "outer_twiddles, Tensor radix_root_powers, "
+                                                               "Tensor rns_params) -> ()",
+        "inverse_ntt_montgomery_power_of_two_radix_compact_override_": "inverse_ntt_montgomery_power_of_two_radix_"
+                                                                       "compact_override_(Tensor(a!) "
+                                                                       "montgomery_residues, Tensor outer_twiddles, "
+                                                                       "Tensor radix_root_powers, Tensor rns_params, "
+                                                                       "int shared_memory_log_n) -> ()",
         "inverse_ntt_montgomery_indexed_": "inverse_ntt_montgomery_indexed_(Tensor(a!) montgomery_residues, "
                                            "Tensor even_indices, Tensor odd_indices, Tensor inverse_twiddles, "
                                            "Tensor rns_params) -> ()",
@@ -119,6 +172,28 @@ SCHEMAS: dict[str, dict[str, str]] = {
                                                          "Tensor rns_params, int grouped_stage_count) -> ()",
     },
     "fhelium_ckks_ops": {
+        "add_prepared_plaintext_component": "add_prepared_plaintext_component(Tensor ciphertext_component, "
+                                            "Tensor prepared_plaintext, Tensor rns_params) -> Tensor",
+        "add_prepared_plaintext_component_": "add_prepared_plaintext_component_(Tensor(a!) ciphertext_component, "
+                                             "Tensor prepared_plaintext, Tensor rns_params) -> ()",
+        "add_cyclic_compressed_plaintext_component": "add_cyclic_compressed_plaintext_component(Tensor "
+                                                     "ciphertext_component, Tensor compressed_plaintext, "
+                                                     "Tensor rns_params) -> Tensor",
+        "add_cyclic_compressed_plaintext_component_": "add_cyclic_compressed_plaintext_component_(Tensor(a!) "
+                                                      "ciphertext_component, Tensor compressed_plaintext, "
+                                                      "Tensor rns_params) -> ()",
+        "add_contiguous_compressed_plaintext_component": "add_contiguous_compressed_plaintext_component(Tensor "
+                                                         "ciphertext_component, Tensor compressed_plaintext, "
+                                                         "Tensor rns_params) -> Tensor",
+        "add_contiguous_compressed_plaintext_component_": "add_contiguous_compressed_plaintext_component_(Tensor(a!) "
+                                                          "ciphertext_component, Tensor compressed_plaintext, "
+                                                          "Tensor rns_params) -> ()",
+        "add_strided_plaintext_component": "add_strided_plaintext_component(Tensor ciphertext_component, "
+                                           "Tensor strided_plaintext, Tensor implicit_plaintext, "
+                                           "Tensor rns_params) -> Tensor",
+        "add_strided_plaintext_component_": "add_strided_plaintext_component_(Tensor(a!) ciphertext_component, "
+                                            "Tensor strided_plaintext, Tensor implicit_plaintext, "
+                                            "Tensor rns_params) -> ()",
         "rescale_drop_leading_prime_nearest": "rescale_drop_leading_prime_nearest(Tensor remaining_residues, "
                                               "Tensor drop_prime_inverse_mont, Tensor dropped_residue, "
                                               "Tensor rns_params, int half_drop_prime) -> Tensor",
@@ -150,9 +225,32 @@ _libraries: list = []          # keeps the torch.library registrations alive
 _registered = False
 _contexts: dict = {}           # (bits, log_n, primes, device) -> NativeContext
 _slices: dict = {}             # (bits, log_n, primes, device) -> (NativeContext, first prime id)
-_primes_of: dict = {}          # params identity -> primes tuple
-_checked_twiddles: set = set()
-_checked_schedules: set = set()
+# Verification results and prime lists, remembered per tensor: keyed weakly by the tensor that
+# owns the storage (a view's base), then by the view's offset, shape, strides and version, so a
+# freed table whose address is reused is never mistaken for a checked one.
+_memo: dict = {}               # id(owning tensor) -> {key: value}; dropped when that tensor dies
+
+
+def _memo_key(t: torch.Tensor, tag):
+    return (tag, t.storage_offset(), tuple(t.shape), tuple(t.stride()), t._version)
+
+
+def _anchor(t: torch.Tensor) -> torch.Tensor:
+    return t._base if t._base is not None else t
+
+
+def _memo_get(t: torch.Tensor, tag):
+    entries = _memo.get(id(_anchor(t)))
+    return None if entries is None else entries.get(_memo_key(t, tag))
+
+
+def _memo_put(t: torch.Tensor, tag, value) -> None:
+    anchor = _anchor(t)
+    entries = _memo.get(id(anchor))
+    if entries is None:
+        entries = _memo[id(anchor)] = {}
+        weakref.finalize(anchor, _memo.pop, id(anchor), None)
+    entries[_memo_key(t, tag)] = value
 
 
 # --------------------------------------------------------------------------- helpers
@@ -349,6 +447,85 @@ def shift_residues_positive_(x, rns_params):
     _unary_(4, x, rns_params)
 
 
+def _mul_compressed(layout: int, lhs, rhs, params):
+    _cuda(lhs, "lhs")
+    bits = _bits(lhs, "lhs")
+    _same(rhs, lhs, "compressed_rhs")
+    rows, n = _rows_n(lhs, "lhs")
+    if rhs.dim() < 2 or rhs.shape[-2] != rows:
+        _fail(f"compressed_rhs must be [*batch, {rows}, unique], got {tuple(rhs.shape)}")
+    unique = rhs.shape[-1]
+    if not (0 < unique < n and unique & (unique - 1) == 0 and n % unique == 0):
+        _fail(f"compressed unique count must be a power of two smaller than the ring dimension: {unique} vs {n}")
+    a, b = _Operand(lhs), _Operand(rhs)
+    if b.batch not in (1, a.batch):
+        _fail(f"operand batch counts differ: {a.batch} vs {b.batch}")
+    p, ps = _params(params, lhs, rows)
+    out = torch.empty_like(lhs, memory_format=torch.contiguous_format)
+    with torch.cuda.device(lhs.device):
+        _call("fhb_op_mul_compressed", bits, layout, a.ptr, a.stride, b.ptr, b.stride if b.batch > 1 else 0, unique,
+              out.data_ptr(), rows * n, a.batch, rows, n, p.data_ptr(), ps, _stream(lhs))
+    return out
+
+
+def montgomery_mul_cyclic_compressed(lhs, compressed_rhs, rns_params):
+    return _mul_compressed(1, lhs, compressed_rhs, rns_params)
+
+
+def montgomery_mul_contiguous_compressed(lhs, compressed_rhs, rns_params):
+    return _mul_compressed(2, lhs, compressed_rhs, rns_params)
+
+
+def _row_scalars(x, scalars, params, out=None):
+    _cuda(x, "residues")
+    bits = _bits(x, "residues")
+    rows, n = _rows_n(x, "residues")
+    _same(scalars, x, "row_scalars")
+    if scalars.numel() != rows:
+        _fail(f"row_scalars must have {rows} entries, got {scalars.numel()}")
+    p, ps = _params(params, x, rows)
+    a = _Operand(x)
+    writable = out is not None
+    if out is None:
+        out = torch.empty_like(x, memory_format=torch.contiguous_format)
+    o = _Operand(out, writable=writable)
+    sc = scalars.contiguous()
+    with torch.cuda.device(x.device):
+        _call("fhb_op_mul_row_scalars", bits, a.ptr, a.stride, o.ptr, o.stride, a.batch, rows, n, sc.data_ptr(),
+              p.data_ptr(), ps, _stream(x))
+    o.finish()
+    return out
+
+
+def montgomery_mul_row_scalars_(residues, row_scalars, rns_params):
+    _check_writable(residues, "residues")
+    _row_scalars(residues, row_scalars, rns_params, out=residues)
+
+
+def montgomery_mul_row_scalars_canonical(residues, row_scalars, rns_params):
+    return _row_scalars(residues, row_scalars, rns_params)
+
+
+def add_lazy_with_twice_modulus(lhs, rhs, twice_modulus):
+    _cuda(lhs, "lhs")
+    bits = _bits(lhs, "lhs")
+    _same(rhs, lhs, "rhs")
+    _same(twice_modulus, lhs, "twice_modulus")
+    rows, n = _rows_n(lhs, "lhs")
+    if twice_modulus.numel() != rows or tuple(rhs.shape[-2:]) != (rows, n):
+        _fail("twice_modulus / rhs do not match lhs's limbs")
+    a, b = _Operand(lhs), _Operand(rhs)
+    if b.batch not in (1, a.batch):
+        _fail(f"rhs batch {b.batch} must equal lhs batch {a.batch} or be 1")
+    tm = twice_modulus.contiguous()
+    out = torch.empty_like(lhs, memory_format=torch.contiguous_format)
+    with torch.cuda.device(lhs.device):
+        # ops 1 (add_lazy) reads only parameter row 0: a 2q vector with row stride 0
+        _call("fhb_op_rns_binary", bits, 1, a.ptr, a.stride, b.ptr, b.stride if b.batch > 1 else 0, out.data_ptr(),
+              rows * n, a.batch, rows, n, tm.data_ptr(), 0, _stream(lhs))
+    return out
+
+
 def lift_centered_coefficients(coefficients, twice_modulus):
     _cuda(coefficients, "centered_coefficients")
     bits = _bits(coefficients, "centered_coefficients")
@@ -421,11 +598,10 @@ def mixed_radix_basis_extend_to_montgomery(components, coefficients, rns_params,
 
 # --------------------------------------------------------------------------- ntt ops
 def _primes(params: torch.Tensor) -> tuple:
-    key = (params.data_ptr(), params._version, tuple(params.shape), tuple(params.stride()), params.device)
-    primes = _primes_of.get(key)
+    primes = _memo_get(params, "primes")
     if primes is None:
         primes = tuple(int(v) // 2 for v in params[0].cpu().tolist())
-        _primes_of[key] = primes
+        _memo_put(params, "primes", primes)
     return primes
 
 
@@ -468,12 +644,23 @@ def _find_run(chain: tuple, run: tuple):
 
 
 def _check_twiddles(tw: torch.Tensor, ctx, offset: int, primes: tuple, bits: int, log_n: int, inverse: bool,
-                    indexed: bool):
-    key = (tw.data_ptr(), tw._version, tuple(tw.shape), inverse, indexed)
-    if key in _checked_twiddles:
-        return
+                    indexed: bool, radix_roots: torch.Tensor | None = None):
     n, rows = 1 << log_n, len(primes)
-    if indexed:
+    exponent = 1
+    if radix_roots is not None:
+        # power-of-two radix tables (fhelium/engine/ntt/plans/twiddles.py:152-230): outer twists
+        # [prime, N - 1] and the powers of the radix-th root psi^(2N/radix) [prime, radix]
+        radix = radix_roots.shape[-1] if radix_roots.dim() == 2 else 0
+        if radix not in (4, 8, 16) or radix_roots.shape[0] != rows:
+            _fail(f"radix_root_powers must be [{rows}, 4 | 8 | 16], got {tuple(radix_roots.shape)}")
+        if log_n % {4: 2, 8: 3, 16: 4}[radix]:
+            _fail("Strict radix width must divide log_ring_dimension")
+        if tw.dim() != 2 or tuple(tw.shape) != (rows, n - 1):
+            _fail(f"outer_twiddles must be [{rows}, {n - 1}], got {tuple(tw.shape)}")
+        _same(radix_roots, tw, "radix_root_powers")
+        probe = radix_roots[:, 1]
+        exponent = 2 * n // radix
+    elif indexed:
         if tw.dim() != 3 or tw.shape[0] != rows or tw.shape[2] != n // 2:
             _fail(f"twiddles must be [{rows}, log2(N) stages, {n // 2}], got {tuple(tw.shape)}")
         if tw.shape[1] != log_n:
@@ -483,15 +670,19 @@ def _check_twiddles(tw: torch.Tensor, ctx, offset: int, primes: tuple, bits: int
         if tw.dim() != 2 or tuple(tw.shape) != (rows, n):
             _fail(f"twiddles must be [{rows}, {n}], got {tuple(tw.shape)}")
         probe = tw[:, n // 2]
+    probed = radix_roots if radix_roots is not None else tw
+    tag = ("twiddles", inverse, indexed, radix_roots is not None, primes)
+    if _memo_get(probed, tag):
+        return
     got = [int(v) for v in probe.cpu().tolist()]
     radix = 62 if bits == 64 else 30
     for j, q in enumerate(primes):
-        psi = ctx.root(offset + j)
+        psi = pow(ctx.root(offset + j), exponent, q)
         w = pow(psi, -1, q) if inverse else psi
         if got[j] % q != (w << radix) % q:
             _fail(f"twiddle row {j} does not hold the reference's primitive root (Montgomery form) "
                   f"for modulus {q}")
-    _checked_twiddles.add(key)
+    _memo_put(probed, tag, True)
 
 
 def _radix2_schedule(log_n: int, inverse: bool):
@@ -517,8 +708,8 @@ def _radix2_schedule(log_n: int, inverse: bool):
 
 
 def _check_schedule(even: torch.Tensor, odd: torch.Tensor, log_n: int, inverse: bool):
-    key = (even.data_ptr(), even._version, odd.data_ptr(), odd._version, log_n, inverse)
-    if key in _checked_schedules:
+    tag = ("schedule", log_n, inverse)
+    if _memo_get(even, tag + ("even",)) and _memo_get(odd, tag + ("odd",)):
         return
     n = 1 << log_n
     for t, name in ((even, "even_indices"), (odd, "odd_indices")):
@@ -535,11 +726,12 @@ def _check_schedule(even: torch.Tensor, odd: torch.Tensor, log_n: int, inverse: 
     want_e, want_o = _radix2_schedule(log_n, inverse)
     if not (np.array_equal(e, want_e) and np.array_equal(o, want_o)):
         _fail("fhelium_b200 serves the reference's radix-2 indexed schedule only")
-    _checked_schedules.add(key)
+    _memo_put(even, tag + ("even",), True)
+    _memo_put(odd, tag + ("odd",), True)
 
 
 def _ntt_(x: torch.Tensor, tw: torch.Tensor, params: torch.Tensor, *, inverse: bool, mode: int,
-          schedule=None) -> None:
+          schedule=None, radix_roots=None) -> None:
     """mode: forward 0 = standard input, 1 = Montgomery input; inverse = fhb_inverse_output."""
     _cuda(x, "residues")
     _check_writable(x, "residues")
@@ -547,7 +739,7 @@ def _ntt_(x: torch.Tensor, tw: torch.Tensor, params: torch.Tensor, *, inverse: b
     _same(tw, x, "twiddles")
     if schedule is not None:
         _check_schedule(schedule[0], schedule[1], log_n, inverse)
-    _check_twiddles(tw, ctx, offset, primes, bits, log_n, inverse, schedule is not None)
+    _check_twiddles(tw, ctx, offset, primes, bits, log_n, inverse, schedule is not None, radix_roots)
     rows = len(primes)
     o = _Operand(x, writable=True)
     if o.stride != rows * x.shape[-1] and o.batch > 1:
@@ -583,6 +775,28 @@ def _inv_compact_(kind: int):
     return f
 
 
+def _fwd_radix_(montgomery: int):
+    def f(x, outer, roots, params, shared_memory_log_n=None):
+        _ntt_(x, outer, params, inverse=False, mode=montgomery, radix_roots=roots)
+    return f
+
+
+def _inv_radix_(kind: int):
+    def f(x, outer, roots, params, shared_memory_log_n=None):
+        _ntt_(x, outer, params, inverse=True, mode=kind, radix_roots=roots)
+    return f
+
+
+def forward_ntt_to_montgomery_power_of_two_radix_compact(x, outer, roots, params):
+    y = x.clone(memory_format=torch.contiguous_format)
+    _ntt_(y, outer, params, inverse=False, mode=0, radix_roots=roots)
+    return y
+
+
+def forward_ntt_montgomery_compact_grouped_smem_override_(x, tw, params, grouped_stage_count, shared_memory_log_n):
+    _ntt_(x, tw, params, inverse=False, mode=1)
+
+
 def forward_ntt_to_montgomery_indexed(x, even, odd, tw, params):
     y = x.clone(memory_format=torch.contiguous_format)
     _ntt_(y, tw, params, inverse=False, mode=0, schedule=(even, odd))
@@ -601,6 +815,62 @@ def forward_ntt_montgomery_compact_keyswitch_accumulate_(digit, tw, params, key_
 
 
 # --------------------------------------------------------------------------- ckks ops
+def _add_plaintext(layout: int, ct, pt, params, implicit=None, out=None):
+    _cuda(ct, "ciphertext_component")
+    bits = _bits(ct, "ciphertext_component")
+    _same(pt, ct, "plaintext")
+    rows, n = _rows_n(ct, "ciphertext_component")
+    if pt.dim() < 2 or pt.shape[-2] != rows:
+        _fail(f"plaintext must be [*batch, {rows}, extent], got {tuple(pt.shape)}")
+    extent = pt.shape[-1]
+    if layout == 0 and extent != n:
+        _fail(f"prepared plaintext must have {n} coefficients, got {extent}")
+    if layout in (1, 2) and not (0 < extent < n and extent & (extent - 1) == 0):
+        _fail(f"compressed unique count must be a power of two smaller than the ring dimension: {extent} vs {n}")
+    if layout == 3 and not (0 < extent <= n and extent & (extent - 1) == 0):
+        _fail(f"strided plaintext extent must be a power of two dividing the ring dimension: {extent} vs {n}")
+    c, pl = _Operand(ct), _Operand(pt)
+    if pl.batch not in (1, c.batch):
+        _fail(f"plaintext batch {pl.batch} must equal the ciphertext batch {c.batch} or be 1")
+    imp_ptr, imp_stride = None, 0
+    if layout == 3:
+        _same(implicit, ct, "implicit_plaintext")
+        if implicit.shape[-1] != rows:
+            _fail(f"implicit_plaintext must be [*batch, {rows}], got {tuple(implicit.shape)}")
+        im = _Operand(implicit, rows_dims=1)
+        if im.batch != pl.batch:
+            _fail("implicit_plaintext and strided_plaintext batches differ")
+        imp_ptr, imp_stride = im.ptr, (im.stride if im.batch > 1 else 0)
+    p, ps = _params(params, ct, rows)
+    writable = out is not None
+    if out is None:
+        out = torch.empty_like(ct, memory_format=torch.contiguous_format)
+    o = _Operand(out, writable=writable)
+    with torch.cuda.device(ct.device):
+        _call("fhb_op_add_plaintext", bits, layout, c.ptr, c.stride, pl.ptr, pl.stride if pl.batch > 1 else 0,
+              extent, imp_ptr, imp_stride, o.ptr, o.stride, c.batch, rows, n, p.data_ptr(), ps, _stream(ct))
+    o.finish()
+    return out
+
+
+def _plaintext_op(layout: int, inplace: bool):
+    if layout == 3:
+        def f(ct, strided, implicit, params):
+            if inplace:
+                _check_writable(ct, "ciphertext_component")
+                _add_plaintext(3, ct, strided, params, implicit, out=ct)
+                return None
+            return _add_plaintext(3, ct, strided, params, implicit)
+    else:
+        def f(ct, pt, params):
+            if inplace:
+                _check_writable(ct, "ciphertext_component")
+                _add_plaintext(layout, ct, pt, params, out=ct)
+                return None
+            return _add_plaintext(layout, ct, pt, params)
+    return f
+
+
 def _rescale(remaining, inverse_mont, dropped, params, half, nearest, out=None):
     _cuda(remaining, "remaining_residues")
     bits = _bits(remaining, "remaining_residues")
@@ -745,6 +1015,11 @@ IMPLS = {
         "lift_centered_coefficients": lift_centered_coefficients,
         "mixed_radix_decompose": mixed_radix_decompose,
         "mixed_radix_basis_extend_to_montgomery": mixed_radix_basis_extend_to_montgomery,
+        "montgomery_mul_cyclic_compressed": montgomery_mul_cyclic_compressed,
+        "montgomery_mul_contiguous_compressed": montgomery_mul_contiguous_compressed,
+        "montgomery_mul_row_scalars_": montgomery_mul_row_scalars_,
+        "montgomery_mul_row_scalars_canonical": montgomery_mul_row_scalars_canonical,
+        "add_lazy_with_twice_modulus": add_lazy_with_twice_modulus,
     },
     "fhelium_ntt_ops": {
         "forward_ntt_montgomery_indexed_": _fwd_indexed_(1),
@@ -754,6 +1029,16 @@ IMPLS = {
         "forward_ntt_to_montgomery_compact_grouped_smem_": _fwd_compact_(0),
         "forward_ntt_to_montgomery_compact_grouped_smem": forward_ntt_to_montgomery_compact_grouped_smem,
         "forward_ntt_montgomery_compact_keyswitch_accumulate_": forward_ntt_montgomery_compact_keyswitch_accumulate_,
+        "forward_ntt_montgomery_power_of_two_radix_compact_": _fwd_radix_(1),
+        "forward_ntt_to_montgomery_power_of_two_radix_compact_": _fwd_radix_(0),
+        "forward_ntt_to_montgomery_power_of_two_radix_compact": forward_ntt_to_montgomery_power_of_two_radix_compact,
+        "forward_ntt_montgomery_compact_grouped_smem_override_": forward_ntt_montgomery_compact_grouped_smem_override_,
+        "forward_ntt_montgomery_power_of_two_radix_compact_override_": _fwd_radix_(1),
+        "inverse_ntt_montgomery_power_of_two_radix_compact_": _inv_radix_(_native.INV_MONTGOMERY),
+        "inverse_ntt_to_standard_lazy_power_of_two_radix_compact_": _inv_radix_(_native.INV_STANDARD_LAZY),
+        "inverse_ntt_to_standard_power_of_two_radix_compact_": _inv_radix_(_native.INV_STANDARD),
+        "inverse_ntt_to_centered_power_of_two_radix_compact_": _inv_radix_(_native.INV_CENTERED),
+        "inverse_ntt_montgomery_power_of_two_radix_compact_override_": _inv_radix_(_native.INV_MONTGOMERY),
         "inverse_ntt_montgomery_indexed_": _inv_indexed_(_native.INV_MONTGOMERY),
         "inverse_ntt_to_standard_lazy_indexed_": _inv_indexed_(_native.INV_STANDARD_LAZY),
         "inverse_ntt_to_standard_indexed_": _inv_indexed_(_native.INV_STANDARD),
@@ -764,6 +1049,14 @@ IMPLS = {
         "inverse_ntt_to_centered_compact_grouped_smem_": _inv_compact_(_native.INV_CENTERED),
     },
     "fhelium_ckks_ops": {
+        "add_prepared_plaintext_component": _plaintext_op(0, False),
+        "add_prepared_plaintext_component_": _plaintext_op(0, True),
+        "add_cyclic_compressed_plaintext_component": _plaintext_op(1, False),
+        "add_cyclic_compressed_plaintext_component_": _plaintext_op(1, True),
+        "add_contiguous_compressed_plaintext_component": _plaintext_op(2, False),
+        "add_contiguous_compressed_plaintext_component_": _plaintext_op(2, True),
+        "add_strided_plaintext_component": _plaintext_op(3, False),
+        "add_strided_plaintext_component_": _plaintext_op(3, True),
         "rescale_drop_leading_prime_nearest": rescale_drop_leading_prime_nearest,
         "rescale_drop_leading_prime_nearest_": rescale_drop_leading_prime_nearest_,
         "rescale_drop_leading_prime_truncate": rescale_drop_leading_prime_truncate,

@@ -350,6 +350,9 @@ int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t
 
 /* op 0 montgomery_mul (canonical), 1 add_lazy, 2 sub_lazy ([0, 2q)),
  * 3 add_canonical, 4 sub_canonical; rhs_batch_stride 0 = singleton rhs batch.
+ * Ops 1 and 2 read only parameter row 0 (2q): a twice-modulus vector with
+ * param_row_stride 0 serves add_lazy_with_twice_modulus
+ * (csrc/ops/rns/rns_arithmetic.cpp:47-49).
  * Replaces fhelium_rns_ops.{montgomery_mul, add_lazy, sub_lazy,
  * add_canonical(_), sub_canonical(_)} (csrc/ops/rns/rns_arithmetic.cpp:31,46,50,
  * csrc/ops/rns/rns_canonical_arithmetic.cpp:16-21). */
@@ -426,6 +429,36 @@ int fhb_op_coefficient_automorphism(int residue_bits, const void* in, int64_t in
 int fhb_op_ntt_automorphism(int residue_bits, const void* in, int64_t in_batch_stride, void* out,
                             int64_t out_batch_stride, int64_t batch, int rows, int64_t n,
                             const int32_t* source_indices, fhb_stream stream);
+/* out = lhs * rhs[i(k)] (Montgomery, canonical) with a compressed right
+ * operand of `unique` words per row (a power of two below n): layout 1 cyclic
+ * (i = k mod unique), 2 contiguous (i = k / (n / unique)).  Replaces
+ * fhelium_rns_ops.montgomery_mul_{cyclic,contiguous}_compressed
+ * (csrc/ops/rns/rns_arithmetic.cpp:32-37, csrc/ops/rns/cuda/rns_arithmetic_cuda.cu:55-78). */
+int fhb_op_mul_compressed(int residue_bits, int layout, const void* lhs, int64_t lhs_batch_stride,
+                          const void* compressed_rhs, int64_t rhs_batch_stride, int64_t unique, void* out,
+                          int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* params,
+                          int64_t param_row_stride, fhb_stream stream);
+/* Plaintext addition to a coefficient/standard ciphertext component:
+ * out = c + p R^-1 mod q, canonical, p a coefficient/Montgomery plaintext word
+ * of plaintext_extent words per row.  layout 0 dense (extent n), 1 cyclic,
+ * 2 contiguous repetition (extent a power of two below n), 3 strided
+ * (coefficients k with k mod (n / extent) = 0 stored at k / (n / extent), the
+ * rest take implicit_plaintext[b, row], batch stride implicit_batch_stride).
+ * out may equal ciphertext.  Replaces fhelium_ckks_ops.add_{prepared,
+ * cyclic_compressed,contiguous_compressed,strided}_plaintext_component(_)
+ * (csrc/ops/ckks/ckks.cpp:30-59, csrc/ops/ckks/cuda/plaintext_cuda.cu:1-114). */
+int fhb_op_add_plaintext(int residue_bits, int layout, const void* ciphertext, int64_t ciphertext_batch_stride,
+                         const void* plaintext, int64_t plaintext_batch_stride, int64_t plaintext_extent,
+                         const void* implicit_plaintext, int64_t implicit_batch_stride, void* out,
+                         int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* params,
+                         int64_t param_row_stride, fhb_stream stream);
+/* out = residues * row_scalars[row] (Montgomery, canonical); out may equal
+ * residues.  Replaces fhelium_rns_ops.montgomery_mul_row_scalars_ and
+ * montgomery_mul_row_scalars_canonical (csrc/ops/rns/rns_arithmetic.cpp:38-40,
+ * csrc/ops/rns/rns_canonical_arithmetic.cpp:20-22). */
+int fhb_op_mul_row_scalars(int residue_bits, const void* residues, int64_t residues_batch_stride, void* out,
+                           int64_t out_batch_stride, int64_t batch, int rows, int64_t n, const void* row_scalars,
+                           const void* params, int64_t param_row_stride, fhb_stream stream);
 /* A context whose prime ids 0..count-1 are exactly `moduli` (plus one
  * auxiliary special prime of the library's choosing at id `count`), for the
  * transforms (fhb_forward_ntt, fhb_inverse_ntt, tensor-core forms) and the

@@ -355,3 +355,108 @@ def test_reference_operator_sequence_on_cuda(ops, family, level):
     got = _n(pipe.multiply_relinearize_rescale(_c(a, ctx), _c(b, ctx), _c(key, ctx), level))
     want = ctx.rescale(ctx.relinearize(ctx.multiply(a, b, level), key, level), level)
     np.testing.assert_array_equal(got, want)
+
+
+def _expand(pt, layout, n, implicit=None):
+    """Dense [*, rows, N] form of a repeated / strided plaintext (reference
+    csrc/ops/common/cuda/repetition.cuh:69-86, csrc/ops/ckks/cuda/plaintext_cuda.cu:93-114)."""
+    u = pt.shape[-1]
+    k = np.arange(n)
+    if layout == "cyclic":
+        return pt[..., k % u]
+    if layout == "contiguous":
+        return pt[..., k // (n // u)]
+    stride = n // u
+    dense = np.repeat(implicit[..., None], n, axis=-1)
+    dense[..., ::stride] = pt
+    return dense
+
+
+@pytest.mark.parametrize("family", list(CONTEXTS))
+def test_plaintext_and_compressed_ops(ops, family):
+    ctx = CONTEXTS[family]()
+    rng = np.random.default_rng(17)
+    rows = ctx.q_rows(0)
+    prm = ctx.sub_params(rows)
+    n = ctx.n
+    q = np.array([ctx.moduli[i] for i in rows], dtype=np.int64)[:, None]
+    rns, ck = ops.fhelium_rns_ops, ops.fhelium_ckks_ops
+    a = _lazy(rng, ctx, rows, batch=3)
+    for layout, name in (("cyclic", "montgomery_mul_cyclic_compressed"),
+                         ("contiguous", "montgomery_mul_contiguous_compressed")):
+        comp = _lazy(rng, ctx, rows, batch=1)[..., :64]
+        got = _n(getattr(rns, name)(_c(a, ctx), _c(comp, ctx), _c(prm, ctx)))
+        dense = np.broadcast_to(_expand(comp, layout, n), a.shape)
+        np.testing.assert_array_equal(got, orc.montgomery_mul(a, dense, prm, ctx.radix_bits), err_msg=name)
+        _same_on_cpu(getattr(rns, name), (a, comp, prm), ctx, got)
+    scal = _uniform(rng, ctx, rows, batch=1)[0, :, 0].copy()
+    got = _n(rns.montgomery_mul_row_scalars_canonical(_c(a, ctx), _c(scal, ctx), _c(prm, ctx)))
+    want = orc.montgomery_mul(a, np.broadcast_to(scal[None, :, None], a.shape), prm, ctx.radix_bits)
+    np.testing.assert_array_equal(got, want)
+    x = _c(a, ctx)
+    rns.montgomery_mul_row_scalars_(x, _c(scal, ctx), _c(prm, ctx))
+    np.testing.assert_array_equal(_n(x), want)
+    b = _lazy(rng, ctx, rows, batch=3)
+    tq = (2 * q[:, 0]).copy()
+    got = _n(rns.add_lazy_with_twice_modulus(_c(a, ctx), _c(b, ctx), _c(tq, ctx)))
+    np.testing.assert_array_equal(got, orc.add_lazy(a, b, prm))
+    # plaintext additions: c + p R^-1 mod q, canonical
+    c = _uniform(rng, ctx, rows, batch=3)
+    ones = np.ones_like(c)
+    cases = {
+        "prepared": (_lazy(rng, ctx, rows, batch=3), None),
+        "cyclic_compressed": (_lazy(rng, ctx, rows, batch=1)[..., :128], None),
+        "contiguous_compressed": (_lazy(rng, ctx, rows, batch=1)[..., :32], None),
+        "strided": (_lazy(rng, ctx, rows, batch=3)[..., :256], _uniform(rng, ctx, rows, batch=3)[..., 0].copy()),
+    }
+    for kind, (pt, implicit) in cases.items():
+        if kind == "prepared":
+            dense = pt
+        elif kind == "strided":
+            dense = _expand(pt, "strided", n, implicit)
+        else:
+            dense = _expand(pt, kind.split("_")[0], n)
+        dense = np.broadcast_to(dense, c.shape)
+        want = (c + orc.montgomery_mul(dense, ones, prm, ctx.radix_bits)) % q
+        op = getattr(ck, f"add_{kind}_plaintext_component")
+        args = (c, pt, implicit, prm) if kind == "strided" else (c, pt, prm)
+        got = _n(op(*[_c(v, ctx) for v in args]))
+        np.testing.assert_array_equal(got, want, err_msg=kind)
+        _same_on_cpu(op, args, ctx, got)
+        t = _c(c, ctx)
+        getattr(ck, f"add_{kind}_plaintext_component_")(t, *[_c(v, ctx) for v in args[1:]])
+        np.testing.assert_array_equal(_n(t), want, err_msg=kind + "_")
+
+
+@pytest.mark.parametrize("family,radix", [("int64", 4), ("int64_p4", 16), ("int32", 8)])
+def test_power_of_two_radix_ntt_forms(ops, family, radix):
+    """The reference's power-of-two-radix NTT schemas compute the same transform
+    (same root, same bit-reversed order); their tables are checked for shape and
+    for the radix-th root psi^(2N/radix) in Montgomery form."""
+    ctx = CONTEXTS[family]()
+    if ctx.log_n % {4: 2, 8: 3, 16: 4}[radix]:
+        pytest.skip("radix width does not divide log N")
+    rng = np.random.default_rng(18)
+    rows = ctx.qp_rows(0)
+    prm = ctx.sub_params(rows)
+    n, R = ctx.n, 1 << ctx.radix_bits
+    roots_f, roots_i = [], []
+    for i in rows:
+        qi = ctx.moduli[i]
+        w = pow(orc.primitive_2nth_root(qi, n), 2 * n // radix, qi)
+        wi = pow(w, -1, qi)
+        roots_f.append([(pow(w, k, qi) * R) % qi for k in range(radix)])
+        roots_i.append([(pow(wi, k, qi) * R) % qi for k in range(radix)])
+    outer = np.zeros((len(rows), n - 1), np.int64)   # read for its shape only
+    ntt = ops.fhelium_ntt_ops
+    x = _uniform(rng, ctx, rows)
+    got = _n(ntt.forward_ntt_to_montgomery_power_of_two_radix_compact(_c(x, ctx), _c(outer, ctx),
+                                                                       _c(np.array(roots_f), ctx), _c(prm, ctx)))
+    np.testing.assert_array_equal(_mod(got, ctx, rows), _mod(ctx.forward_to_montgomery(x, rows), ctx, rows))
+    t = _c(got, ctx)
+    ntt.inverse_ntt_to_standard_power_of_two_radix_compact_(t, _c(outer, ctx), _c(np.array(roots_i), ctx),
+                                                            _c(prm, ctx))
+    np.testing.assert_array_equal(_n(t), x)
+    with pytest.raises(RuntimeError, match="primitive root"):
+        ntt.forward_ntt_montgomery_power_of_two_radix_compact_(_c(x, ctx), _c(outer, ctx),
+                                                               _c(np.array(roots_i), ctx), _c(prm, ctx))

@@ -28,7 +28,7 @@ def torch_ops():
 
 def test_every_served_schema_has_a_cuda_kernel(torch_ops):
     served = torch_ops.served()
-    assert len(served) == 38
+    assert len(served) == 61   # every schema of fhelium_{rns,ntt,ckks}_ops
     for qualname in served:
         assert torch._C._dispatch_has_kernel_for_dispatch_key(qualname, "CUDA"), qualname
     torch_ops.register()   # idempotent
@@ -82,3 +82,17 @@ def test_find_run(torch_ops):
     assert torch_ops._find_run(chain, chain) == 0
     assert torch_ops._find_run(chain, (7, 13)) is None
     assert torch_ops._find_run(chain, (17, 19)) is None
+
+
+def test_checks_are_remembered_per_tensor_not_per_address(torch_ops):
+    x = torch.zeros(8, 10, dtype=torch.int64)
+    torch_ops._memo_put(x[:, 2:5], "primes", (1, 2, 3))
+    assert torch_ops._memo_get(x[:, 2:5], "primes") == (1, 2, 3)     # another view of the same slice
+    assert torch_ops._memo_get(x[:, 2:6], "primes") is None          # another slice
+    x.add_(1)
+    assert torch_ops._memo_get(x[:, 2:5], "primes") is None          # modified in place
+    before = len(torch_ops._memo)
+    del x
+    import gc
+    gc.collect()
+    assert len(torch_ops._memo) == before - 1                        # forgotten with the tensor
