@@ -26,8 +26,8 @@ import torch
 from . import _native as nat
 from .config import CkksConfig, Preset
 from .encoding import decode_coefficients, encode_real_coefficients
-from .values import (Ciphertext, KeySwitchKey, PublicKey, RelinearizationKey, RotationKey, RotationKeySet,
-                     SecretKey)
+from .values import (Ciphertext, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey, RotationKey,
+                     RotationKeySet, SecretKey)
 
 
 def galois_element(n: int, step: int, generator: int = 3) -> int:
@@ -143,17 +143,41 @@ class CkksEngine:
                       self._stream())
         return out
 
-    def coefficient_domain_to_ntt_domain(self, ct: Ciphertext) -> Ciphertext:
+    def coefficient_domain_to_ntt_domain(self, ct: "Ciphertext | Plaintext") -> "Ciphertext | Plaintext":
+        if isinstance(ct, Plaintext):
+            return self._plaintext_ntt(ct, forward=True, inplace=False)
         ct.assert_state(polynomial_domain="coefficient", residue_representation="standard")
         self._check_ct(ct)
         data = self.forward_ntt(ct.data, ct.level)
         return Ciphertext(data, ct.level, ct.scale, "ntt", "montgomery")
 
-    def ntt_domain_to_coefficient_domain(self, ct: Ciphertext) -> Ciphertext:
+    def ntt_domain_to_coefficient_domain(self, ct: "Ciphertext | Plaintext") -> "Ciphertext | Plaintext":
+        if isinstance(ct, Plaintext):
+            return self._plaintext_ntt(ct, forward=False, inplace=False)
         ct.assert_state(polynomial_domain="ntt", residue_representation="montgomery")
         self._check_ct(ct)
         data = self.inverse_ntt(ct.data, ct.level)
         return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
+
+    def coefficient_domain_to_ntt_domain_(self, value: "Ciphertext | Plaintext") -> "Ciphertext | Plaintext":
+        """In place (fhelium/engine/ckks_engine.py:876-938)."""
+        if isinstance(value, Plaintext):
+            return self._plaintext_ntt(value, forward=True, inplace=True)
+        value.assert_state(polynomial_domain="coefficient", residue_representation="standard")
+        self._check_ct(value)
+        self.forward_ntt(value.data, value.level, out=value.data)
+        value.polynomial_domain, value.residue_representation = "ntt", "montgomery"
+        return value
+
+    def ntt_domain_to_coefficient_domain_(self, value: "Ciphertext | Plaintext") -> "Ciphertext | Plaintext":
+        """In place (fhelium/engine/ckks_engine.py:940-986)."""
+        if isinstance(value, Plaintext):
+            return self._plaintext_ntt(value, forward=False, inplace=True)
+        value.assert_state(polynomial_domain="ntt", residue_representation="montgomery")
+        self._check_ct(value)
+        self.inverse_ntt(value.data, value.level, out=value.data)
+        value.polynomial_domain, value.residue_representation = "coefficient", "standard"
+        return value
 
     # ------------------------------------------------------------------
     # arithmetic
@@ -167,8 +191,10 @@ class CkksEngine:
                       b_mode, self._stream())
         return out
 
-    def add(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+    def add(self, lhs: Ciphertext, rhs: Ciphertext, *, inplace: bool = False) -> Ciphertext:
         """Componentwise modular sum (fhelium/engine/ckks_engine.py:1708-1750)."""
+        if inplace:
+            return self._replace(lhs, self.add(lhs, rhs))
         self._assert_same_layout(lhs, rhs)
         if lhs.scale != rhs.scale:
             raise ValueError("add requires equal scales")
@@ -255,13 +281,30 @@ class CkksEngine:
         coeffs = self.encode_coefficients(slots, scale)
         return self.forward_ntt(self._lift(coeffs, level, self.num_q - level), level)
 
-    def multiply_plaintext(self, ct: Ciphertext, plaintext: torch.Tensor, plaintext_scale: float) -> Ciphertext:
-        """NTT-domain ct x pt (no rescale); pt [L, N] is shared by every
-        component and batch item (fhelium/engine/ckks_engine.py:2077-2170)."""
+    def multiply_plaintext(self, ct: Ciphertext, plaintext: "Plaintext | torch.Tensor",
+                           plaintext_scale: float | None = None, *, inplace: bool = False) -> Ciphertext:
+        """NTT-domain ct x pt, no rescale; the scale multiplies
+        (fhelium/engine/ckks_engine.py:2077-2170).  `plaintext` is a Plaintext
+        (slots, integer coefficients or NTT/Montgomery RNS at the ciphertext's
+        level; an unbatched one is shared by every batch item), or a raw
+        NTT/Montgomery tensor [Q_level, N] with its scale."""
         ct.assert_state(polynomial_domain="ntt", residue_representation="montgomery")
         self._check_ct(ct)
-        out = self._binary(nat.OP_MONTGOMERY_MUL, ct.data, plaintext, ct.level, b_mode=1)
-        return Ciphertext(out, ct.level, ct.scale * plaintext_scale, "ntt", "montgomery")
+        if isinstance(plaintext, Plaintext):
+            pt = self._plaintext_operand(plaintext, ct, "ntt")
+            scale = ct.scale * plaintext.scale
+        else:
+            if plaintext_scale is None:
+                raise ValueError("a raw plaintext tensor needs its scale")
+            pt, scale = plaintext, ct.scale * plaintext_scale
+        if pt.dim() == 2:
+            out = self._binary(nat.OP_MONTGOMERY_MUL, ct.data, pt.contiguous(), ct.level, b_mode=1)
+        else:
+            out = torch.empty_like(ct.data)
+            for c in range(ct.component_count):
+                self._binary(nat.OP_MONTGOMERY_MUL, ct.data[c], pt.contiguous(), ct.level, out=out[c])
+        result = Ciphertext(out, ct.level, scale, "ntt", "montgomery")
+        return self._replace(ct, result) if inplace else result
 
     def _row_constants(self, value: int, level: int, *, montgomery: bool) -> torch.Tensor:
         R = 1 << (62 if self.dtype == torch.int64 else 30)
@@ -290,7 +333,9 @@ class CkksEngine:
                       ct.level, 1 if ntt else 0, self._stream())
         return Ciphertext(out, ct.level, ct.scale, ct.polynomial_domain, ct.residue_representation)
 
-    def subtract(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+    def subtract(self, lhs: Ciphertext, rhs: Ciphertext, *, inplace: bool = False) -> Ciphertext:
+        if inplace:
+            return self._replace(lhs, self.subtract(lhs, rhs))
         self._assert_same_layout(lhs, rhs)
         op = nat.OP_SUB_LAZY if lhs.polynomial_domain == "ntt" else nat.OP_SUB_CANONICAL
         out = self._binary(op, lhs.data, rhs.data, lhs.level)
@@ -629,8 +674,13 @@ class CkksEngine:
         if not 0 <= level < self.public_level_count:
             raise ValueError("level out of range")
         scale = float(self.config.default_scale if scale is None else scale)
+        return self._encrypt_coefficients(self.encode_coefficients(message, scale), level, scale, public_key)
+
+    def _encrypt_coefficients(self, coeffs: torch.Tensor, level: int, scale: float,
+                              public_key: PublicKey | None) -> Ciphertext:
+        """(v pk0 + e0 + m, v pk1 + e1) of exact integer coefficients [*batch, N]
+        (fhelium/engine/ckks_encryptor.py:181-233)."""
         pk = (public_key or self.public_key).data[:, level:].contiguous()
-        coeffs = self.encode_coefficients(message, scale)
         batch_shape = tuple(coeffs.shape[:-1])
         L = self.num_q - level
         m = self.forward_ntt(self._lift(coeffs, level, L), level)
@@ -688,6 +738,412 @@ class CkksEngine:
         vals = torch.tensor(np.asarray(coeffs, dtype=np.float64), dtype=torch.float64)
         slots = decode_coefficients(vals, self.n, self.galois_generator) / ct.scale
         return slots.real if is_real else slots
+
+    # ------------------------------------------------------------------
+    # Plaintext values (fhelium/engine/ckks_engine.py:508-760,
+    # fhelium/engine/ckks_plaintext_codec.py:78-450)
+    # ------------------------------------------------------------------
+    def _public_level(self, level: int) -> int:
+        if not 0 <= int(level) < self.public_level_count:
+            raise ValueError(f"level {level} outside the public levels 0..{self.final_public_level}")
+        return int(level)
+
+    def _scale_arg(self, scale) -> float:
+        scale = float(self.config.default_scale if scale is None else scale)
+        if not (scale > 0 and math.isfinite(scale)):
+            raise ValueError("scale must be positive and finite")
+        return scale
+
+    def _check_context(self, value) -> None:
+        cid = getattr(value, "context_id", None)
+        if cid not in (None, self.context_id):
+            raise ValueError(f"value belongs to another CKKS context: {cid} != {self.context_id}")
+
+    def _prime_ids(self, level: int, modulus_basis: str) -> tuple:
+        if modulus_basis not in ("Q", "QP"):
+            raise ValueError("modulus_basis must be 'Q' or 'QP'")
+        stop = self.num_q + (self.num_p if modulus_basis == "QP" else 0)
+        return tuple(range(level, stop))
+
+    def plaintext(self, message, *, level: int = 0, scale=None) -> Plaintext:
+        """An unencoded slots plaintext on this engine's device."""
+        level = self._public_level(level)
+        msg = torch.as_tensor(message).detach().clone().to(self.device)
+        return Plaintext(message=msg, level=level, scale=self._scale_arg(scale))
+
+    def encode(self, message, *, level: int = 0, scale=None) -> Plaintext:
+        """Slots -> exact integer coefficients [*batch, N] at `scale`
+        (rounded to nearest; the reference rounds stochastically)."""
+        if isinstance(message, Plaintext):
+            return self._integer_plaintext(message)
+        level = self._public_level(level)
+        scale = self._scale_arg(scale)
+        coeffs = self.encode_coefficients(message, scale)
+        return Plaintext(message=None, data=coeffs, level=level, scale=scale, context_id=self.context_id,
+                         representation="integer_coefficients", polynomial_domain="coefficient")
+
+    def _integer_plaintext(self, pt: Plaintext) -> Plaintext:
+        self._check_context(pt)
+        if pt.is_integer_coefficients:
+            return pt
+        if pt.is_slots:
+            return self.encode(pt.message, level=pt.level, scale=pt.scale)
+        raise ValueError(f"expected slots or integer_coefficients, got {pt.representation}")
+
+    def integer_coefficients_to_rns(self, plaintext: Plaintext, *, modulus_basis: str = "Q") -> Plaintext:
+        """Exact coefficients -> coefficient/standard residues over Q_level (or Q_level P)."""
+        pt = self._integer_plaintext(plaintext)
+        ids = self._prime_ids(pt.level, modulus_basis)
+        data = self._lift(pt.data.to(device=self.device, dtype=torch.int64), pt.level, len(ids))
+        return Plaintext(message=None, data=data, level=pt.level, scale=pt.scale, context_id=self.context_id,
+                         representation="rns", polynomial_domain="coefficient", modulus_basis=modulus_basis,
+                         residue_representation="standard", prime_ids=ids)
+
+    def _rows_mul_const(self, data: torch.Tensor, row_start: int, value_of, *, canonical: bool) -> torch.Tensor:
+        rows = data.size(-2)
+        consts = torch.tensor([value_of(self.moduli[i]) for i in range(row_start, row_start + rows)],
+                              dtype=self.dtype, device=self.device)
+        out = self._binary(nat.OP_MONTGOMERY_MUL, data.contiguous(), consts, row_start, b_mode=2)
+        if canonical:
+            out = self._binary(nat.OP_ADD_CANONICAL, out, torch.zeros_like(consts), row_start, b_mode=2, out=out)
+        return out
+
+    def _rns_plaintext(self, pt: Plaintext) -> Plaintext:
+        self._check_context(pt)
+        if not pt.is_rns:
+            raise ValueError(f"expected an RNS plaintext, got {pt.representation}")
+        return pt
+
+    def standard_residues_to_montgomery_residues(self, plaintext: Plaintext) -> Plaintext:
+        return self.standard_residues_to_montgomery_residues_(plaintext.clone())
+
+    def standard_residues_to_montgomery_residues_(self, plaintext: Plaintext) -> Plaintext:
+        """x -> x R (canonical), in place (fhelium/engine/ckks_engine.py:1036-1060)."""
+        pt = self._rns_plaintext(plaintext)
+        if pt.residue_representation != "standard":
+            raise ValueError("plaintext residues are not in standard form")
+        R2 = lambda q: pow(1 << self.config.buffer_bit_length, 2, q)
+        pt.data = self._rows_mul_const(pt.data, pt.prime_ids[0], R2, canonical=True)
+        pt.residue_representation = "montgomery"
+        return pt
+
+    def montgomery_residues_to_standard_residues(self, plaintext: Plaintext) -> Plaintext:
+        return self.montgomery_residues_to_standard_residues_(plaintext.clone())
+
+    def montgomery_residues_to_standard_residues_(self, plaintext: Plaintext) -> Plaintext:
+        """x R -> x (canonical), in place."""
+        pt = self._rns_plaintext(plaintext)
+        if pt.residue_representation != "montgomery" or pt.polynomial_domain != "coefficient":
+            raise ValueError("expected coefficient-domain Montgomery residues")
+        pt.data = self._rows_mul_const(pt.data, pt.prime_ids[0], lambda q: 1, canonical=True)
+        pt.residue_representation = "standard"
+        return pt
+
+    def _plaintext_ntt(self, pt: Plaintext, *, forward: bool, inplace: bool) -> Plaintext:
+        pt = self._rns_plaintext(pt)
+        if not inplace:
+            pt = pt.clone()
+        start = pt.prime_ids[0]
+        if forward:
+            if pt.polynomial_domain != "coefficient":
+                raise ValueError("plaintext is already in the NTT domain")
+            self.forward_ntt(pt.data, start, montgomery_input=pt.residue_representation == "montgomery",
+                             out=pt.data)
+        else:
+            if pt.polynomial_domain != "ntt":
+                raise ValueError("plaintext is not in the NTT domain")
+            self.inverse_ntt(pt.data, start, output=nat.INV_STANDARD, out=pt.data)
+        pt.polynomial_domain = "ntt" if forward else "coefficient"
+        pt.residue_representation = "montgomery" if forward else "standard"
+        return pt
+
+    def prepare_plaintext_for_addition(self, plaintext: Plaintext, *, modulus_basis: str = "Q") -> Plaintext:
+        """Coefficient-domain Montgomery residues, the operand of add_plaintext."""
+        return self.standard_residues_to_montgomery_residues_(
+            self.integer_coefficients_to_rns(plaintext, modulus_basis=modulus_basis))
+
+    def prepare_plaintext_for_multiplication(self, plaintext: Plaintext, *, modulus_basis: str = "Q") -> Plaintext:
+        """NTT-domain Montgomery residues, the operand of multiply_plaintext."""
+        return self._plaintext_ntt(self.integer_coefficients_to_rns(plaintext, modulus_basis=modulus_basis),
+                                   forward=True, inplace=True)
+
+    def decode(self, plaintext: Plaintext, *, is_real: bool = False) -> torch.Tensor:
+        """Coefficients / scale -> slots [*batch, N/2] on the CPU (complex unless is_real)."""
+        if not isinstance(plaintext, Plaintext):
+            raise TypeError(f"decode expects Plaintext, got {type(plaintext).__name__}")
+        self._check_context(plaintext)
+        if plaintext.is_slots:
+            plaintext = self.encode(plaintext)
+        if plaintext.is_rns:
+            raise ValueError("decode requires integer_coefficients or approximate_coefficients; "
+                             "RNS reconstruction is not implicit")
+        vals = plaintext.data.detach().to("cpu", torch.float64)
+        slots = decode_coefficients(vals, self.n, self.galois_generator) / plaintext.scale
+        return slots.real if is_real else slots
+
+    def encrypt(self, plaintext: Plaintext, public_key: PublicKey | None = None) -> Ciphertext:
+        """Public-key encryption of slots or exact integer coefficients;
+        coefficient/standard output (fhelium/engine/ckks_engine.py:700-738)."""
+        if not isinstance(plaintext, Plaintext):
+            raise TypeError(f"encrypt expects Plaintext, got {type(plaintext).__name__}")
+        pt = self._integer_plaintext(plaintext)
+        self._public_level(pt.level)
+        return self._encrypt_coefficients(pt.data.to(self.device, torch.int64), pt.level, pt.scale, public_key)
+
+    def decrypt(self, ct: Ciphertext, secret_key: SecretKey | None = None) -> Plaintext:
+        """Decryption to float64 coefficients [*batch, N] (approximate
+        coefficients, for decode) (fhelium/engine/ckks_engine.py:740-771)."""
+        if not isinstance(ct, Ciphertext):
+            raise TypeError(f"decrypt expects Ciphertext, got {type(ct).__name__}")
+        coeffs = self.decrypt_coefficients(ct, secret_key)
+        data = torch.tensor(np.asarray(coeffs, dtype=np.float64), dtype=torch.float64, device=self.device)
+        return Plaintext(message=None, data=data, level=ct.level, scale=ct.scale, context_id=self.context_id,
+                         representation="approximate_coefficients", polynomial_domain="coefficient")
+
+    def zero_plaintext_like(self, plaintext: Plaintext) -> Plaintext:
+        """Semantic zero in the same representation and state
+        (fhelium/engine/ckks_engine.py:1431-1489)."""
+        self._check_context(plaintext)
+        if plaintext.is_approximate_coefficients:
+            out = plaintext.clone()
+            out.data.zero_()
+            return out
+        zero = torch.zeros((*plaintext.batch_shape, self.num_slots), dtype=torch.complex128, device=self.device)
+        if plaintext.is_slots:
+            return Plaintext(message=zero, level=plaintext.level, scale=plaintext.scale)
+        encoded = self.encode(zero, level=plaintext.level, scale=plaintext.scale)
+        if plaintext.is_integer_coefficients:
+            return encoded
+        basis = plaintext.modulus_basis or "Q"
+        if plaintext.residue_representation == "standard":
+            return self.integer_coefficients_to_rns(encoded, modulus_basis=basis)
+        if plaintext.polynomial_domain == "coefficient":
+            return self.prepare_plaintext_for_addition(encoded, modulus_basis=basis)
+        return self.prepare_plaintext_for_multiplication(encoded, modulus_basis=basis)
+
+    def _plaintext_operand(self, pt: Plaintext, ct: Ciphertext, domain: str) -> torch.Tensor:
+        """The plaintext's residues over the ciphertext's Q_level rows in the
+        operation's state (coefficient/Montgomery for addition, NTT/Montgomery
+        for multiplication), preparing slots or integer plaintexts first."""
+        self._check_context(pt)
+        if pt.level != ct.level:
+            raise ValueError(f"plaintext level {pt.level} != ciphertext level {ct.level}")
+        if not pt.is_rns:
+            pt = (self.prepare_plaintext_for_addition(pt) if domain == "coefficient"
+                  else self.prepare_plaintext_for_multiplication(pt))
+        if pt.polynomial_domain != domain or pt.residue_representation != "montgomery":
+            raise ValueError(f"plaintext must be {domain}-domain Montgomery residues, got "
+                             f"{pt.polynomial_domain}/{pt.residue_representation}")
+        data = pt.data[..., : ct.limb_count, :]     # a Q_level P plaintext contributes its Q rows
+        if data.dim() > 2 and tuple(data.shape[:-2]) != ct.batch_shape:
+            raise ValueError("a batched plaintext must match the ciphertext's batch shape")
+        return data
+
+    @property
+    def _param_rows(self) -> torch.Tensor:
+        """The reference's [8, QP] parameter rows (csrc/ops/common/rns_parameters.h:6-16)."""
+        if getattr(self, "_param_rows_cache", None) is None:
+            bits = self.config.buffer_bit_length
+            half, R = bits // 2, 1 << bits
+            cols = []
+            for q in self.moduli:
+                ninv = (-pow(q, -1, R)) % R
+                r2 = (R * R) % q
+                cols.append([2 * q, q & ((1 << half) - 1), q >> half, ninv & ((1 << half) - 1), ninv >> half, r2,
+                             (r2 << self.config.scale_bits) % q, (pow(self.n, -1, q) * R) % q])
+            self._param_rows_cache = torch.tensor(cols, dtype=torch.int64).T.contiguous().to(self.device, self.dtype)
+        return self._param_rows_cache
+
+    def add_plaintext(self, ct: Ciphertext, plaintext: Plaintext, *, inplace: bool = False) -> Ciphertext:
+        """c0 + p at exactly the ciphertext's scale, coefficient/standard
+        (fhelium/engine/ckks_engine.py:1964-2066): one fhb_op_add_plaintext launch."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        if plaintext.scale != ct.scale:
+            raise ValueError(f"add_plaintext: ciphertext scale {ct.scale} != plaintext scale {plaintext.scale}")
+        pt = self._plaintext_operand(plaintext, ct, "coefficient").contiguous()
+        rows, b = ct.limb_count, ct.batch_size
+        out = ct.data if inplace else ct.data.clone()
+        params = self._param_rows[:, ct.level: ct.level + rows]
+        bits = 64 if self.dtype == torch.int64 else 32
+        nat.check(self.ctx.lib.fhb_op_add_plaintext(bits, 0, nat.ptr(ct.data[0]), rows * self.n, nat.ptr(pt),
+                                                    rows * self.n if pt.dim() > 2 else 0, self.n, None, 0,
+                                                    nat.ptr(out[0]), rows * self.n, b, rows, self.n,
+                                                    nat.ptr(params), params.stride(0), self._stream()),
+                  "fhb_op_add_plaintext")
+        return ct if inplace else Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
+
+    def add_plaintext_(self, ct: Ciphertext, plaintext: Plaintext) -> Ciphertext:
+        return self.add_plaintext(ct, plaintext, inplace=True)
+
+    def multiply_plaintext_(self, ct: Ciphertext, plaintext: Plaintext) -> Ciphertext:
+        return self.multiply_plaintext(ct, plaintext, inplace=True)
+
+    # ------------------------------------------------------------------
+    # the rest of fh.CkksEngine's public API
+    # (fhelium/engine/ckks_engine.py:246-262, 455-460, 1208-1345, 1491-1530,
+    #  1677-1960, 2298-2346, 2560-2620)
+    # ------------------------------------------------------------------
+    @property
+    def final_public_level(self) -> int:
+        return self.public_level_count - 1
+
+    @property
+    def rng(self) -> torch.Generator:
+        """The engine's seeded device generator (keys, encryption noise)."""
+        return self._gen
+
+    def set_public_key(self, key: PublicKey) -> None:
+        self.validate_public_key(key)
+        self._public_key = key
+
+    @staticmethod
+    def _replace(target: Ciphertext, result: Ciphertext) -> Ciphertext:
+        """Give `target` the result's tensor and state (the reference's replace_)."""
+        if target.data.shape == result.data.shape and target.data.dtype == result.data.dtype:
+            target.data.copy_(result.data)
+        else:
+            target.data = result.data
+        target.level, target.scale = result.level, result.scale
+        target.polynomial_domain, target.residue_representation = result.polynomial_domain, result.residue_representation
+        return target
+
+    def add_(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+        return self.add(lhs, rhs, inplace=True)
+
+    def subtract_(self, lhs: Ciphertext, rhs: Ciphertext) -> Ciphertext:
+        return self.subtract(lhs, rhs, inplace=True)
+
+    def negate(self, ct: Ciphertext, *, inplace: bool = False) -> Ciphertext:
+        """-ct, canonical residues (fhelium/engine/ckks_engine.py:1919-1957)."""
+        self._check_ct(ct)
+        out = ct.data if inplace else torch.empty_like(ct.data)
+        rows = ct.limb_count
+        self.ctx.call("fhb_rns_binary", nat.OP_NEGATE, nat.ptr(ct.data), None, nat.ptr(out),
+                      ct.component_count * ct.batch_size, rows, ct.level, 0, self._stream())
+        if inplace:
+            return ct
+        return Ciphertext(out, ct.level, ct.scale, ct.polynomial_domain, ct.residue_representation)
+
+    def negate_(self, ct: Ciphertext) -> Ciphertext:
+        return self.negate(ct, inplace=True)
+
+    def sum_ciphertexts(self, ciphertexts: Sequence[Ciphertext]) -> Ciphertext:
+        if not ciphertexts:
+            raise ValueError("sum_ciphertexts requires at least one value")
+        result = ciphertexts[0].clone()
+        for ct in ciphertexts[1:]:
+            if ct.scale != result.scale:
+                raise ValueError("sum_ciphertexts needs equal scales")
+            self.add_(result, ct)
+        return result
+
+    def sum_ciphertext_batch(self, batch: Ciphertext, *, dim: int = 0) -> Ciphertext:
+        """Sum over one batch axis by pairwise halving (fhelium/engine/ckks_engine.py:1808-1850)."""
+        shape = batch.batch_shape
+        if not shape:
+            raise ValueError("sum_ciphertext_batch requires a batched value")
+        d = dim if dim >= 0 else dim + len(shape)
+        if not 0 <= d < len(shape):
+            raise IndexError(f"Batch dimension {dim} is outside shape {shape}")
+        cur = batch.data
+        tails = []
+        while cur.size(d + 1) > 1:
+            count = cur.size(d + 1)
+            pairs = count // 2
+            if count % 2:
+                tails.append(cur.narrow(d + 1, count - 1, 1))
+            lhs = Ciphertext(cur.narrow(d + 1, 0, pairs).contiguous(), batch.level, batch.scale,
+                             batch.polynomial_domain, batch.residue_representation)
+            rhs = Ciphertext(cur.narrow(d + 1, pairs, pairs).contiguous(), batch.level, batch.scale,
+                             batch.polynomial_domain, batch.residue_representation)
+            cur = self.add(lhs, rhs).data
+        for tail in reversed(tails):
+            cur = self.add(Ciphertext(cur.contiguous(), batch.level, batch.scale, batch.polynomial_domain,
+                                      batch.residue_representation),
+                           Ciphertext(tail.contiguous(), batch.level, batch.scale, batch.polynomial_domain,
+                                      batch.residue_representation)).data
+        return Ciphertext(cur.select(d + 1, 0).contiguous(), batch.level, batch.scale, batch.polynomial_domain,
+                          batch.residue_representation)
+
+    def switch_key(self, ct: Ciphertext, key: KeySwitchKey) -> Ciphertext:
+        """(c0, c1) under s_src -> (c0 + KS(c1)) under s_dst for a key made by
+        create_key_switch_key(s_src, s_dst) (fhelium/engine/ckks_engine.py:1677-1706):
+        the rotation path with the identity automorphism (g = 1)."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        self.validate_key_switch_key(key)
+        out = torch.empty_like(ct.data)
+        scratch, nbytes = self._scratch_for(ct.batch_size, ct.level)
+        self.ctx.call("fhb_ckks_rotate", nat.ptr(ct.data), nat.ptr(key.data), nat.ptr(out), nat.ptr(scratch), nbytes,
+                      ct.batch_size, ct.level, 1, self._stream())
+        return Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
+
+    def mod_switch_to_next_level(self, ct: Ciphertext) -> Ciphertext:
+        if ct.level >= self.final_public_level:
+            raise ValueError(f"level {ct.level} is already the final public level")
+        return self.mod_switch_to_level(ct, ct.level + 1)
+
+    def mod_switch_to_next_level_(self, ct: Ciphertext) -> Ciphertext:
+        return self._replace(ct, self.mod_switch_to_next_level(ct))
+
+    def mod_switch_to_level_(self, ct: Ciphertext, target_level: int) -> Ciphertext:
+        return self._replace(ct, self.mod_switch_to_level(ct, target_level))
+
+    def rescale_to_next_level_(self, ct: Ciphertext, *, rounding: str = "nearest") -> Ciphertext:
+        return self._replace(ct, self.rescale_to_next_level(ct, rounding=rounding))
+
+    def reinterpret_at_scale_(self, ct: Ciphertext, target_scale: float, *,
+                              max_relative_change: float | None = None) -> Ciphertext:
+        if max_relative_change is not None and abs(target_scale / ct.scale - 1.0) > max_relative_change:
+            raise ValueError("target scale changes the value by more than max_relative_change")
+        ct.scale = float(target_scale)
+        return ct
+
+    def encrypt_zero_like(self, ct: Ciphertext, public_key: PublicKey | None = None) -> Ciphertext:
+        """A fresh encryption of zero in ct's level, scale, batch and domain."""
+        self._check_ct(ct)
+        zero = torch.zeros((*ct.batch_shape, self.num_slots), dtype=torch.complex128, device=self.device)
+        result = self.encrypt_message(zero, public_key, level=ct.level, scale=ct.scale)
+        return self.coefficient_domain_to_ntt_domain_(result) if ct.polynomial_domain == "ntt" else result
+
+    def rotate_by_step_(self, ct: Ciphertext, rotation_step: int) -> Ciphertext:
+        return self._replace(ct, self.rotate_by_step(ct, rotation_step))
+
+    def rotate_many_with_keys(self, ct: Ciphertext, rotation_keys: Sequence[RotationKey], *,
+                              use_hoisting: bool = True) -> list[Ciphertext]:
+        """One rotation per caller-owned key, sharing one ModUp when hoisting."""
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        self._check_ct(ct)
+        for key in rotation_keys:
+            self.validate_key_switch_key(key)
+        if not use_hoisting or len(rotation_keys) < 2:
+            return [self.rotate_with_key(ct, k) for k in rotation_keys]
+        prepared = self.prepare_rotation_digits(ct)
+        return [self.apply_prepared_rotation(ct, prepared, k) for k in rotation_keys]
+
+    def validate_ciphertext(self, ciphertext: Ciphertext) -> None:
+        if not isinstance(ciphertext, Ciphertext):
+            raise TypeError(f"Expected Ciphertext, got {type(ciphertext).__name__}")
+        self._check_ct(ciphertext)
+
+    def validate_public_key(self, key: PublicKey) -> None:
+        if type(key) is not PublicKey:
+            raise TypeError(f"Expected PublicKey, got {type(key).__name__}")
+        d = key.data
+        if d.device != self.device or d.dtype != self.dtype or tuple(d.shape) != (2, self.num_q, self.n):
+            raise ValueError(f"public key must be [2, {self.num_q}, {self.n}] {self.dtype} on {self.device}")
+
+    def validate_key_switch_key(self, key: KeySwitchKey) -> None:
+        if not isinstance(key, KeySwitchKey):
+            raise TypeError(f"Expected KeySwitchKey, got {type(key).__name__}")
+        d = key.data
+        want = (self.key_digit_count, 2, self.qp_rows, self.n)
+        if d.device != self.device or d.dtype != self.dtype or tuple(d.shape) != want or not d.is_contiguous():
+            raise ValueError(f"key-switch key must be a contiguous {list(want)} {self.dtype} tensor on {self.device}")
+        if isinstance(key, RotationKey):
+            if type(key.rotation_step) is not int:
+                raise TypeError("RotationKey rotation_step must be an integer")
 
     def __repr__(self) -> str:
         return f"CkksEngine({self.config}, device={self.device})"

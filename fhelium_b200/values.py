@@ -78,6 +78,69 @@ class Ciphertext:
             raise ValueError(f"expected {components} components, got {self.component_count}")
 
 
+@dataclass(eq=False)
+class Plaintext:
+    """One CKKS plaintext (or dense batch) in one exact state, with the
+    reference's fields (fhelium/core/plaintext.py:19-200):
+
+      representation "slots"                    message [*batch, slot] (not encoded; data None)
+                     "integer_coefficients"     data int64 [*batch, N], coefficient domain
+                     "approximate_coefficients" data float64 [*batch, N] (decryption output; decode only)
+                     "rns"                      data [*batch, limb, N] over prime_ids, with
+                                                polynomial_domain, modulus_basis, residue_representation
+    """
+
+    message: torch.Tensor | None
+    level: int
+    scale: float
+    data: torch.Tensor | None = None
+    context_id: str | None = None
+    representation: str = "slots"
+    polynomial_domain: str | None = None
+    modulus_basis: str | None = None
+    residue_representation: str | None = None
+    prime_ids: tuple = ()
+
+    def __post_init__(self):
+        if (self.message is None) == (self.data is None):
+            raise ValueError("Plaintext must own exactly one representation: slots message or encoded data")
+        if self.representation not in ("slots", "integer_coefficients", "approximate_coefficients", "rns"):
+            raise ValueError(f"Unsupported Plaintext representation: {self.representation!r}")
+        if (self.data is None) != (self.representation == "slots"):
+            raise ValueError("a slots Plaintext holds a message; every other representation holds data")
+        if not (self.scale > 0 and self.scale < float("inf")):
+            raise ValueError("Plaintext scale must be positive and finite")
+        if self.level < 0:
+            raise ValueError("Plaintext level must be non-negative")
+        self.prime_ids = tuple(int(i) for i in self.prime_ids)
+
+    @property
+    def is_slots(self) -> bool:
+        return self.representation == "slots"
+
+    @property
+    def is_integer_coefficients(self) -> bool:
+        return self.representation == "integer_coefficients"
+
+    @property
+    def is_approximate_coefficients(self) -> bool:
+        return self.representation == "approximate_coefficients"
+
+    @property
+    def is_rns(self) -> bool:
+        return self.representation == "rns"
+
+    @property
+    def batch_shape(self) -> tuple[int, ...]:
+        if self.data is None:
+            return tuple(self.message.shape[:-1]) if self.message.ndim > 0 else ()
+        return tuple(self.data.shape[:-2] if self.is_rns else self.data.shape[:-1])
+
+    def clone(self) -> "Plaintext":
+        return replace(self, message=None if self.message is None else self.message.clone(),
+                       data=None if self.data is None else self.data.clone())
+
+
 @dataclass
 class SecretKey:
     data: torch.Tensor  # [QP, N] NTT/Montgomery

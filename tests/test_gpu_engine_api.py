@@ -1,0 +1,189 @@
+"""The rest of fh.CkksEngine's public API on the GPU: Plaintext values
+(plaintext / encode / integer_coefficients_to_rns / prepare_* / decode),
+encrypt / decrypt, plaintext addition and multiplication, negate, sums,
+switch_key, in-place variants, level switches and validation.
+
+Decrypted results are checked against an FP64 model with the reference's
+bounds (tests/test_ckks_operation_correctness.py:48-51: 2e-5 for additions
+and key switching, 3e-5 for products) on slots8192_scale40_levels7_int64;
+operations that must not change residues are checked bit for bit.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+from fhelium_b200.config import Preset
+from fhelium_b200.engine import CkksEngine
+from fhelium_b200.values import Ciphertext, Plaintext, PublicKey
+
+pytestmark = pytest.mark.gpu
+
+ATOL_ADD = 2e-5
+ATOL_MUL = 3e-5
+
+
+@pytest.fixture(scope="module")
+def engine():
+    return CkksEngine(Preset.slots8192_scale40_levels7_int64, rng_seed=3)
+
+
+def _msg(engine, batch, seed):
+    g = torch.Generator().manual_seed(seed)
+    return torch.rand((batch, engine.num_slots), dtype=torch.float64, generator=g) * 0.1 - 0.05
+
+
+def _dec(engine, ct, sk=None):
+    return engine.decode(engine.decrypt(ct, sk), is_real=True).numpy()
+
+
+def test_plaintext_states_and_round_trip(engine):
+    x = _msg(engine, 2, 0)
+    slots = engine.plaintext(x, level=1)
+    assert slots.is_slots and slots.level == 1 and slots.scale == engine.config.default_scale
+    ints = engine.encode(x, level=1)
+    assert ints.is_integer_coefficients and ints.data.shape == (2, engine.n)
+    np.testing.assert_allclose(engine.decode(ints, is_real=True).numpy(), x.numpy(), atol=1e-9)
+    rns = engine.integer_coefficients_to_rns(ints)
+    assert rns.is_rns and rns.data.shape == (2, engine.num_q - 1, engine.n)
+    assert rns.prime_ids == tuple(range(1, engine.num_q))
+    qp = engine.integer_coefficients_to_rns(ints, modulus_basis="QP")
+    assert qp.data.shape[-2] == engine.qp_rows - 1
+    mont = engine.standard_residues_to_montgomery_residues(rns)
+    assert mont.residue_representation == "montgomery" and rns.residue_representation == "standard"
+    back = engine.montgomery_residues_to_standard_residues(mont)
+    assert torch.equal(back.data, rns.data)
+    ntt = engine.coefficient_domain_to_ntt_domain(rns)
+    assert ntt.polynomial_domain == "ntt" and ntt.residue_representation == "montgomery"
+    assert torch.equal(engine.ntt_domain_to_coefficient_domain(ntt).data, rns.data)
+    mult = engine.prepare_plaintext_for_multiplication(ints)
+    assert mult.polynomial_domain == "ntt"
+    q = torch.tensor(engine.moduli[1: engine.num_q], dtype=torch.int64, device=engine.device)[:, None]
+    assert torch.equal(mult.data.to(torch.int64) % q, ntt.data.to(torch.int64) % q)
+    with pytest.raises(ValueError, match="RNS reconstruction is not implicit"):
+        engine.decode(rns)
+
+
+def test_encrypt_decrypt(engine):
+    x = _msg(engine, 3, 1)
+    ct = engine.encrypt(engine.encode(x))
+    assert ct.polynomial_domain == "coefficient" and ct.data.shape == (2, 3, engine.num_q, engine.n)
+    np.testing.assert_allclose(_dec(engine, ct), x.numpy(), atol=ATOL_ADD)
+    ct1 = engine.encrypt(engine.plaintext(x, level=2, scale=2.0 ** 35))   # slots are encoded first
+    assert ct1.level == 2 and ct1.scale == 2.0 ** 35
+    np.testing.assert_allclose(_dec(engine, ct1), x.numpy(), atol=ATOL_ADD * 32)
+    pt = engine.decrypt(ct)
+    assert pt.is_approximate_coefficients and pt.data.dtype == torch.float64
+    with pytest.raises(TypeError):
+        engine.encrypt(x)
+
+
+def test_plaintext_addition_and_product(engine):
+    x, y = _msg(engine, 2, 2), _msg(engine, 2, 3)
+    ct = engine.encrypt(engine.encode(x))
+    for pt in (engine.prepare_plaintext_for_addition(engine.encode(y)), engine.encode(y), engine.plaintext(y)):
+        s = engine.add_plaintext(ct, pt)
+        np.testing.assert_allclose(_dec(engine, s), (x + y).numpy(), atol=ATOL_ADD)
+    shared = engine.encode(y[0])                                    # one plaintext for the whole batch
+    np.testing.assert_allclose(_dec(engine, engine.add_plaintext(ct, shared)), (x + y[0]).numpy(), atol=ATOL_ADD)
+    c2 = ct.clone()
+    assert engine.add_plaintext_(c2, engine.encode(y)) is c2
+    np.testing.assert_allclose(_dec(engine, c2), (x + y).numpy(), atol=ATOL_ADD)
+    with pytest.raises(ValueError, match="scale"):
+        engine.add_plaintext(ct, engine.encode(y, scale=2.0 ** 30))
+    cn = engine.coefficient_domain_to_ntt_domain(ct)
+    pm = engine.prepare_plaintext_for_multiplication(engine.encode(y, scale=2.0 ** 30))
+    prod = engine.multiply_plaintext(cn, pm)
+    assert prod.scale == ct.scale * 2.0 ** 30
+    np.testing.assert_allclose(_dec(engine, prod), (x * y).numpy(), atol=ATOL_MUL)
+    prod_shared = engine.multiply_plaintext(cn, engine.encode(y[1], scale=2.0 ** 30))
+    np.testing.assert_allclose(_dec(engine, prod_shared), (x * y[1]).numpy(), atol=ATOL_MUL)
+    c3 = cn.clone()
+    engine.multiply_plaintext_(c3, pm)
+    assert torch.equal(c3.data, prod.data) and c3.scale == prod.scale
+
+
+def test_negate_sums_and_in_place_arithmetic(engine):
+    xs = [_msg(engine, 1, 10 + i) for i in range(5)]
+    cts = [engine.encrypt(engine.encode(x)) for x in xs]
+    np.testing.assert_allclose(_dec(engine, engine.negate(cts[0])), -xs[0].numpy(), atol=ATOL_ADD)
+    c = cts[1].clone()
+    engine.negate_(c)
+    assert torch.equal(c.data, engine.negate(cts[1]).data)
+    total = engine.sum_ciphertexts(cts)
+    np.testing.assert_allclose(_dec(engine, total), sum(xs).numpy(), atol=ATOL_ADD)
+    batch = Ciphertext(torch.cat([ct.data for ct in cts], dim=1), 0, cts[0].scale)
+    summed = engine.sum_ciphertext_batch(batch)                      # 5 items: an odd tail
+    assert summed.data.shape == (2, engine.num_q, engine.n)
+    np.testing.assert_allclose(_dec(engine, summed), sum(xs)[0].numpy(), atol=ATOL_ADD)
+    a = cts[2].clone()
+    engine.add_(a, cts[3])
+    assert torch.equal(a.data, engine.add(cts[2], cts[3]).data)
+    engine.subtract_(a, cts[3])
+    np.testing.assert_allclose(_dec(engine, a), xs[2].numpy(), atol=ATOL_ADD)
+
+
+def test_switch_key(engine):
+    x = _msg(engine, 2, 20)
+    ct = engine.encrypt(engine.encode(x))
+    dst = engine.create_secret_key()
+    ksk = engine.create_key_switch_key(engine.secret_key, dst)
+    switched = engine.switch_key(ct, ksk)
+    np.testing.assert_allclose(_dec(engine, switched, dst), x.numpy(), atol=ATOL_ADD)
+    assert np.abs(_dec(engine, switched) - x.numpy()).max() > 1.0      # no longer under the old key
+
+
+def test_level_switches_rotations_and_zero_values(engine):
+    x = _msg(engine, 2, 30)
+    ct = engine.encrypt(engine.encode(x))
+    down = engine.mod_switch_to_next_level(ct)
+    assert down.level == 1
+    np.testing.assert_allclose(_dec(engine, down), x.numpy(), atol=ATOL_ADD)
+    c = ct.clone()
+    engine.mod_switch_to_level_(c, 3)
+    assert c.level == 3 and c.limb_count == engine.num_q - 3
+    r = ct.clone()
+    engine.rotate_by_step_(r, 1)
+    assert torch.equal(r.data, engine.rotate_by_step(ct, 1).data)
+    keys = [engine.rotation_key(s) for s in (1, 2, 5)]
+    hoisted = engine.rotate_many_with_keys(ct, keys)
+    direct = engine.rotate_many_with_keys(ct, keys, use_hoisting=False)
+    # hoisting extends c1 before the automorphism, so it equals the hoisted
+    # step path bit for bit and the direct path after decryption
+    by_steps = engine.rotate_many_by_steps(ct, [1, 2, 5])
+    for h, d, k, s, step in zip(hoisted, direct, keys, by_steps, (1, 2, 5)):
+        assert torch.equal(h.data, s.data)
+        assert torch.equal(d.data, engine.rotate_with_key(ct, k).data)
+        np.testing.assert_allclose(_dec(engine, h), np.roll(x.numpy(), step, axis=-1), atol=ATOL_ADD)
+    z = engine.encrypt_zero_like(ct)
+    np.testing.assert_allclose(_dec(engine, engine.add(ct, z)), x.numpy(), atol=ATOL_ADD)
+    zn = engine.encrypt_zero_like(engine.coefficient_domain_to_ntt_domain(ct))
+    assert zn.polynomial_domain == "ntt"
+    ints = engine.encode(x)
+    for pt in (engine.plaintext(x), ints, engine.integer_coefficients_to_rns(ints),
+               engine.prepare_plaintext_for_addition(ints), engine.prepare_plaintext_for_multiplication(ints)):
+        zero = engine.zero_plaintext_like(pt)
+        assert zero.representation == pt.representation
+        assert zero.polynomial_domain == pt.polynomial_domain and zero.residue_representation == pt.residue_representation
+    s = ct.clone()
+    engine.reinterpret_at_scale_(s, ct.scale * 2)
+    assert s.scale == ct.scale * 2 and torch.equal(s.data, ct.data)
+
+
+def test_validation(engine):
+    x = _msg(engine, 1, 40)
+    ct = engine.encrypt(engine.encode(x))
+    engine.validate_ciphertext(ct)
+    engine.validate_public_key(engine.public_key)
+    engine.validate_key_switch_key(engine.relinearization_key)
+    with pytest.raises(ValueError):
+        engine.validate_public_key(PublicKey(engine.public_key.data[:, 1:]))
+    with pytest.raises(TypeError):
+        engine.validate_key_switch_key(engine.public_key)
+    pk = engine.create_public_key()
+    engine.set_public_key(pk)
+    assert engine.public_key is pk
+    assert engine.final_public_level == engine.public_level_count - 1
+    assert isinstance(engine.rng, torch.Generator)
+    with pytest.raises(ValueError, match="exactly one"):
+        Plaintext(message=None, level=0, scale=1.0)
