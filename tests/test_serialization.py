@@ -99,3 +99,13 @@ def test_engine_context_id_matches_the_files():
     eng.config = CkksConfig.parse("slots8192_scale40_levels7_int64")
     eng.galois_generator = 3
     assert eng.context_id == CID
+
+
+def test_top_level_names_match_the_reference_namespace():
+    """fh.<name> for the evaluation path (fhelium/__init__.py __all__)."""
+    import fhelium_b200 as fh
+    for name in ("CkksConfig", "Preset", "Ciphertext", "Plaintext", "SecretKey", "PublicKey", "KeySwitchKey",
+                 "RelinearizationKey", "RotationKey", "ConjugationKey", "RotationKeySet", "ModulusBasis",
+                 "PolynomialDomain", "ResidueRepresentation", "PlaintextRepresentation", "save_value", "load_value",
+                 "inspect_value"):
+        assert getattr(fh, name) is not None, name
