@@ -7,19 +7,21 @@ state literals and the value-file functions."""
 from typing import Literal
 
 from .config import CkksConfig, Preset
-from .values import (Ciphertext, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey, RotationKey,
-                     RotationKeySet, SecretKey)
+from .values import (COMPRESSED_PLAINTEXT_FORMAT_VERSION, Ciphertext, CompressedPlaintext, KeySwitchKey, Plaintext,
+                     PublicKey, RelinearizationKey, RotationKey, RotationKeySet, SecretKey)
 
 # state literals (fhelium/core/state.py:10-21)
 PlaintextRepresentation = Literal["slots", "integer_coefficients", "approximate_coefficients", "rns"]
 PolynomialDomain = Literal["coefficient", "ntt"]
 ModulusBasis = Literal["Q", "QP"]
 ResidueRepresentation = Literal["standard", "montgomery"]
+CompressedPlaintextLayout = Literal["cyclic", "contiguous", "strided_sparse"]
 
 # A conjugation key is the Galois key of g = 2N - 1 (CkksEngine.create_conjugation_key).
 ConjugationKey = RotationKey
 
-__all__ = ["CkksConfig", "Preset", "CkksEngine", "Ciphertext", "Plaintext", "SecretKey", "PublicKey",
+__all__ = ["CkksConfig", "Preset", "CkksEngine", "Ciphertext", "Plaintext", "CompressedPlaintext",
+           "CompressedPlaintextLayout", "COMPRESSED_PLAINTEXT_FORMAT_VERSION", "SecretKey", "PublicKey",
            "KeySwitchKey", "RelinearizationKey", "RotationKey", "ConjugationKey", "RotationKeySet",
            "PlaintextRepresentation", "PolynomialDomain", "ModulusBasis", "ResidueRepresentation",
            "save_value", "load_value", "inspect_value"]

@@ -26,8 +26,8 @@ import torch
 from . import _native as nat
 from .config import CkksConfig, Preset
 from .encoding import decode_coefficients, encode_real_coefficients
-from .values import (Ciphertext, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey, RotationKey,
-                     RotationKeySet, SecretKey)
+from .values import (Ciphertext, CompressedPlaintext, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey,
+                     RotationKey, RotationKeySet, SecretKey)
 
 
 def galois_element(n: int, step: int, generator: int = 3) -> int:
@@ -290,6 +290,11 @@ class CkksEngine:
         NTT/Montgomery tensor [Q_level, N] with its scale."""
         ct.assert_state(polynomial_domain="ntt", residue_representation="montgomery")
         self._check_ct(ct)
+        if isinstance(plaintext, CompressedPlaintext) and plaintext.compression_layout != "strided_sparse":
+            result = self._multiply_compressed(ct, plaintext)
+            return self._replace(ct, result) if inplace else result
+        if isinstance(plaintext, CompressedPlaintext):
+            plaintext = plaintext.to_plaintext()
         if isinstance(plaintext, Plaintext):
             pt = self._plaintext_operand(plaintext, ct, "ntt")
             scale = ct.scale * plaintext.scale
@@ -954,22 +959,62 @@ class CkksEngine:
             self._param_rows_cache = torch.tensor(cols, dtype=torch.int64).T.contiguous().to(self.device, self.dtype)
         return self._param_rows_cache
 
-    def add_plaintext(self, ct: Ciphertext, plaintext: Plaintext, *, inplace: bool = False) -> Ciphertext:
+    def _compressed_operand(self, pt: CompressedPlaintext, ct: Ciphertext, domain: str):
+        self._check_context(pt)
+        if pt.level != ct.level or pt.ring_dimension != self.n:
+            raise ValueError("compressed plaintext level / ring dimension does not match the ciphertext")
+        if pt.polynomial_domain != domain:
+            raise ValueError(f"compressed plaintext must be {domain}-domain Montgomery residues")
+        data = pt.data[..., : ct.limb_count, :].contiguous()
+        if data.dim() > 2 and tuple(data.shape[:-2]) != ct.batch_shape:
+            raise ValueError("a batched plaintext must match the ciphertext's batch shape")
+        implicit = None
+        if pt.implicit_data is not None:
+            implicit = pt.implicit_data[..., : ct.limb_count].contiguous()
+        return data, implicit
+
+    def _multiply_compressed(self, ct: Ciphertext, pt: CompressedPlaintext) -> Ciphertext:
+        """c_i * p with a repeated operand: one fhb_op_mul_compressed launch per component."""
+        data, _ = self._compressed_operand(pt, ct, "ntt")
+        rows, b = ct.limb_count, ct.batch_size
+        params = self._param_rows[:, ct.level: ct.level + rows]
+        layout = 1 if pt.compression_layout == "cyclic" else 2
+        bits = 64 if self.dtype == torch.int64 else 32
+        out = torch.empty_like(ct.data)
+        for c in range(ct.component_count):
+            nat.check(self.ctx.lib.fhb_op_mul_compressed(
+                bits, layout, nat.ptr(ct.data[c]), rows * self.n, nat.ptr(data),
+                rows * pt.unique_count if data.dim() > 2 else 0, pt.unique_count, nat.ptr(out[c]), rows * self.n, b,
+                rows, self.n, nat.ptr(params), params.stride(0), self._stream()), "fhb_op_mul_compressed")
+        return Ciphertext(out, ct.level, ct.scale * pt.scale, "ntt", "montgomery")
+
+    def add_plaintext(self, ct: Ciphertext, plaintext: "Plaintext | CompressedPlaintext", *,
+                      inplace: bool = False) -> Ciphertext:
         """c0 + p at exactly the ciphertext's scale, coefficient/standard
-        (fhelium/engine/ckks_engine.py:1964-2066): one fhb_op_add_plaintext launch."""
+        (fhelium/engine/ckks_engine.py:1964-2066): one fhb_op_add_plaintext
+        launch (dense, or a compressed plaintext expanded on the fly)."""
         ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
         self._check_ct(ct)
         if plaintext.scale != ct.scale:
             raise ValueError(f"add_plaintext: ciphertext scale {ct.scale} != plaintext scale {plaintext.scale}")
-        pt = self._plaintext_operand(plaintext, ct, "coefficient").contiguous()
+        implicit, istride = None, 0
+        if isinstance(plaintext, CompressedPlaintext):
+            pt, implicit = self._compressed_operand(plaintext, ct, "coefficient")
+            layout = {"cyclic": 1, "contiguous": 2, "strided_sparse": 3}[plaintext.compression_layout]
+            if implicit is not None and implicit.dim() > 1:
+                istride = ct.limb_count
+        else:
+            pt = self._plaintext_operand(plaintext, ct, "coefficient").contiguous()
+            layout = 0
+        extent = pt.size(-1)
         rows, b = ct.limb_count, ct.batch_size
         out = ct.data if inplace else ct.data.clone()
         params = self._param_rows[:, ct.level: ct.level + rows]
         bits = 64 if self.dtype == torch.int64 else 32
-        nat.check(self.ctx.lib.fhb_op_add_plaintext(bits, 0, nat.ptr(ct.data[0]), rows * self.n, nat.ptr(pt),
-                                                    rows * self.n if pt.dim() > 2 else 0, self.n, None, 0,
-                                                    nat.ptr(out[0]), rows * self.n, b, rows, self.n,
-                                                    nat.ptr(params), params.stride(0), self._stream()),
+        nat.check(self.ctx.lib.fhb_op_add_plaintext(bits, layout, nat.ptr(ct.data[0]), rows * self.n, nat.ptr(pt),
+                                                    rows * extent if pt.dim() > 2 else 0, extent,
+                                                    nat.ptr(implicit), istride, nat.ptr(out[0]), rows * self.n, b,
+                                                    rows, self.n, nat.ptr(params), params.stride(0), self._stream()),
                   "fhb_op_add_plaintext")
         return ct if inplace else Ciphertext(out, ct.level, ct.scale, "coefficient", "standard")
 

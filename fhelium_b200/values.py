@@ -141,6 +141,120 @@ class Plaintext:
                        data=None if self.data is None else self.data.clone())
 
 
+COMPRESSED_PLAINTEXT_FORMAT_VERSION = 1
+_COMPRESSION_LAYOUTS = ("cyclic", "contiguous", "strided_sparse")
+
+
+@dataclass(eq=False)
+class CompressedPlaintext:
+    """An operation-ready (Montgomery) RNS plaintext stored compactly as
+    [*batch, limb, unique] (fhelium/core/compressed_plaintext.py:27-560).  The
+    expansion of a compact row to the ring dimension N:
+      "cyclic"          [a, b] -> [a, b, a, b, ...]
+      "contiguous"      [a, b] -> [a, ..., a, b, ..., b]
+      "strided_sparse"  the compact values at positions k (N / unique) apart,
+                        every other position implicit_data[*batch, limb].
+    """
+
+    data: torch.Tensor
+    ring_dimension: int
+    compression_layout: str
+    level: int
+    scale: float
+    context_id: str
+    polynomial_domain: str
+    modulus_basis: str
+    residue_representation: str
+    prime_ids: tuple
+    implicit_data: torch.Tensor | None = None
+    compression_format_version: int = COMPRESSED_PLAINTEXT_FORMAT_VERSION
+
+    def __post_init__(self):
+        if self.compression_layout not in _COMPRESSION_LAYOUTS:
+            raise ValueError(f"Unsupported CompressedPlaintext compression_layout: {self.compression_layout!r}")
+        if self.compression_format_version != COMPRESSED_PLAINTEXT_FORMAT_VERSION:
+            raise ValueError(f"Unsupported CompressedPlaintext compression format version: "
+                             f"{self.compression_format_version}")
+        if self.residue_representation != "montgomery":
+            raise ValueError("Operation-ready CompressedPlaintext data must use Montgomery form")
+        if self.polynomial_domain not in ("coefficient", "ntt") or self.modulus_basis not in ("Q", "QP"):
+            raise ValueError("CompressedPlaintext has an unsupported domain or basis")
+        u, n = self.data.size(-1), int(self.ring_dimension)
+        if not (0 < u < n and u & (u - 1) == 0 and n % u == 0):
+            raise ValueError(f"unique count {u} must be a power of two below the ring dimension {n}")
+        if (self.implicit_data is None) != (self.compression_layout != "strided_sparse"):
+            raise ValueError("implicit_data is required for, and only for, strided_sparse")
+        self.prime_ids = tuple(int(i) for i in self.prime_ids)
+
+    @property
+    def unique_count(self) -> int:
+        return self.data.size(-1)
+
+    @property
+    def repeat_count(self) -> int:
+        return self.ring_dimension // self.unique_count
+
+    @property
+    def batch_shape(self) -> tuple[int, ...]:
+        return tuple(self.data.shape[:-2])
+
+    @classmethod
+    def from_plaintext(cls, plaintext: Plaintext, *, unique_count: int,
+                       compression_layout: str) -> "CompressedPlaintext":
+        """Compress an RNS plaintext whose last axis is exactly representable
+        in the layout (checked bit for bit); raises ValueError otherwise."""
+        if not plaintext.is_rns:
+            raise ValueError("CompressedPlaintext.from_plaintext requires a representation='rns' Plaintext")
+        if compression_layout not in _COMPRESSION_LAYOUTS:
+            raise ValueError(f"Unsupported compression_layout: {compression_layout!r}")
+        data = plaintext.data
+        n = data.size(-1)
+        if not (0 < unique_count < n and unique_count & (unique_count - 1) == 0):
+            raise ValueError(f"unique_count must be a power of two below {n}: {unique_count}")
+        rep = n // unique_count
+        implicit = None
+        if compression_layout == "cyclic":
+            groups = data.reshape(*data.shape[:-1], rep, unique_count)
+            compact = groups[..., 0, :]
+            ok = torch.equal(groups, compact.unsqueeze(-2).expand_as(groups))
+        else:
+            groups = data.reshape(*data.shape[:-1], unique_count, rep)
+            compact = groups[..., :, 0]
+            if compression_layout == "contiguous":
+                ok = torch.equal(groups, compact.unsqueeze(-1).expand_as(groups))
+            else:
+                implicit = groups[..., 0, 1].clone()
+                ok = torch.equal(groups[..., :, 1:], implicit[..., None, None].expand_as(groups[..., :, 1:]))
+        if not ok:
+            raise ValueError(f"Plaintext encoded data is not exactly representable by the requested "
+                             f"{compression_layout!r} compression layout with unique_count={unique_count}")
+        return cls(data=compact.contiguous().clone(), ring_dimension=n, compression_layout=compression_layout,
+                   level=plaintext.level, scale=plaintext.scale, context_id=plaintext.context_id,
+                   polynomial_domain=plaintext.polynomial_domain, modulus_basis=plaintext.modulus_basis,
+                   residue_representation=plaintext.residue_representation, prime_ids=plaintext.prime_ids,
+                   implicit_data=implicit)
+
+    def decompress_data(self) -> torch.Tensor:
+        u, rep = self.unique_count, self.repeat_count
+        if self.compression_layout == "cyclic":
+            return self.data.repeat(*([1] * (self.data.dim() - 1)), rep)
+        if self.compression_layout == "contiguous":
+            return self.data.repeat_interleave(rep, dim=-1)
+        dense = self.implicit_data[..., None].expand(*self.data.shape[:-1], self.ring_dimension).clone()
+        dense[..., ::rep] = self.data
+        return dense
+
+    def to_plaintext(self) -> Plaintext:
+        return Plaintext(message=None, data=self.decompress_data(), level=self.level, scale=self.scale,
+                         context_id=self.context_id, representation="rns", polynomial_domain=self.polynomial_domain,
+                         modulus_basis=self.modulus_basis, residue_representation=self.residue_representation,
+                         prime_ids=self.prime_ids)
+
+    def clone(self) -> "CompressedPlaintext":
+        return replace(self, data=self.data.clone(),
+                       implicit_data=None if self.implicit_data is None else self.implicit_data.clone())
+
+
 @dataclass
 class SecretKey:
     data: torch.Tensor  # [QP, N] NTT/Montgomery

@@ -187,3 +187,37 @@ def test_validation(engine):
     assert isinstance(engine.rng, torch.Generator)
     with pytest.raises(ValueError, match="exactly one"):
         Plaintext(message=None, level=0, scale=1.0)
+
+
+@pytest.mark.parametrize("layout", ["cyclic", "contiguous", "strided_sparse"])
+def test_compressed_plaintexts(engine, layout):
+    """A compressed plaintext gives the same result as its dense expansion:
+    bit for bit for additions, mod q for products."""
+    from fhelium_b200.values import CompressedPlaintext
+    x = _msg(engine, 2, 50)
+    ct = engine.encrypt(engine.encode(x, level=1))
+    rows = engine.num_q - 1
+    g = torch.Generator(device=engine.device).manual_seed(7)
+    q = torch.tensor(engine.moduli[1: engine.num_q], dtype=torch.int64, device=engine.device)
+    u = 64
+    compact = (torch.randint(0, 1 << 62, (rows, u), generator=g, device=engine.device) % q[:, None])
+    implicit = torch.randint(0, 1 << 62, (rows,), generator=g, device=engine.device) % q
+    for domain in ("coefficient", "ntt"):
+        cp = CompressedPlaintext(data=compact.to(engine.dtype), ring_dimension=engine.n, compression_layout=layout,
+                                 level=1, scale=ct.scale if domain == "coefficient" else 2.0 ** 20,
+                                 context_id=engine.context_id, polynomial_domain=domain, modulus_basis="Q",
+                                 residue_representation="montgomery", prime_ids=tuple(range(1, engine.num_q)),
+                                 implicit_data=implicit.to(engine.dtype) if layout == "strided_sparse" else None)
+        dense = cp.to_plaintext()
+        again = CompressedPlaintext.from_plaintext(dense, unique_count=u, compression_layout=layout)
+        assert torch.equal(again.data, cp.data)
+        if domain == "coefficient":
+            got = engine.add_plaintext(ct, cp)
+            assert torch.equal(got.data, engine.add_plaintext(ct, dense).data)
+        else:
+            cn = engine.coefficient_domain_to_ntt_domain(ct)
+            got = engine.multiply_plaintext(cn, cp)
+            want = engine.multiply_plaintext(cn, dense)
+            assert got.scale == want.scale == cn.scale * 2.0 ** 20
+            qq = q[:, None]
+            assert torch.equal(got.data.to(torch.int64) % qq, want.data.to(torch.int64) % qq)

@@ -109,3 +109,26 @@ def test_top_level_names_match_the_reference_namespace():
                  "PolynomialDomain", "ResidueRepresentation", "PlaintextRepresentation", "save_value", "load_value",
                  "inspect_value"):
         assert getattr(fh, name) is not None, name
+
+
+@pytest.mark.parametrize("layout", ["cyclic", "contiguous", "strided_sparse"])
+def test_compressed_plaintext_round_trip(layout):
+    """CompressedPlaintext.from_plaintext / decompress_data are exact inverses
+    on representable data and reject the rest (fhelium/core/compressed_plaintext.py:244-366)."""
+    from fhelium_b200.values import CompressedPlaintext, Plaintext
+    g = torch.Generator().manual_seed(1)
+    compact = torch.randint(0, 1000, (2, 3, 8), generator=g)
+    implicit = torch.randint(0, 1000, (2, 3), generator=g) if layout == "strided_sparse" else None
+    cp = CompressedPlaintext(data=compact, ring_dimension=64, compression_layout=layout, level=0, scale=2.0,
+                             context_id="c", polynomial_domain="ntt", modulus_basis="Q",
+                             residue_representation="montgomery", prime_ids=(0, 1, 2), implicit_data=implicit)
+    dense = cp.to_plaintext()
+    assert dense.data.shape == (2, 3, 64)
+    back = CompressedPlaintext.from_plaintext(dense, unique_count=8, compression_layout=layout)
+    assert torch.equal(back.data, compact)
+    if implicit is not None:
+        assert torch.equal(back.implicit_data, implicit)
+    broken = dense.clone()
+    broken.data[0, 0, 5] += 1
+    with pytest.raises(ValueError, match="not exactly representable"):
+        CompressedPlaintext.from_plaintext(broken, unique_count=8, compression_layout=layout)
