@@ -541,7 +541,7 @@ def main() -> int:
 
     e2e_steps = max(1, min(args.steps, 3))
     trial = {}
-    for chunks in (1, 4, 8):  # pick the chunk count on an untimed pass
+    for chunks in sorted({min(c, host_a.size(1)) for c in (1, 4, 8, 16, 32)}):  # picked on an untimed pass
         e2e_chunks["chunks"] = chunks
         e2e_step()
         torch.cuda.synchronize(dev)
