@@ -349,6 +349,61 @@ def ops_leg(dev, stream, batch=2, steps=3):
     return {"batch": batch, **out}
 
 
+def schema_ops_leg(eng, x, y, kd, stream, steps=5):
+    """The operator-level kernels behind the reference's custom-op schemas
+    (fhb_op_*, served to torch.ops.fhelium_* by fhelium_b200.torch_ops), timed
+    through the C ABI at the headline shape: 32 ciphertexts at L = 35, N = 2^16,
+    int64, P = 4.  x, y: [B, L, N] residues; kd: one key digit [2, QP, N].
+    Algorithmic bytes = every operand read once and every output written once;
+    reported against the measured HBM copy bandwidth."""
+    from fhelium_b200 import _native as nat
+    lib, s = eng.ctx.lib, stream.cuda_stream
+    n, L, P = eng.n, eng.num_q, eng.num_p
+    QP = L + P
+    B = x.size(0)
+    word = 8 if eng.dtype == torch.int64 else 4
+    prm = eng._param_rows
+    try:
+        hbm = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        hbm = 6650.0
+    g = torch.Generator(device=x.device).manual_seed(5)
+    rnd = lambda *shape: torch.randint(0, 1 << 40, shape, generator=g, device=x.device, dtype=eng.dtype)
+    out = torch.empty_like(x)
+    acc0, acc1, digit = torch.zeros(B, QP, n, dtype=eng.dtype, device=x.device), \
+        torch.zeros(B, QP, n, dtype=eng.dtype, device=x.device), rnd(B, QP, n)
+    inv_md, inv_rs = rnd(P, QP), rnd(L - 1)
+    md_out = torch.empty(B, L, n, dtype=eng.dtype, device=x.device)
+    rs_out = torch.empty(B, L - 1, n, dtype=eng.dtype, device=x.device)
+    bits = 64 if eng.dtype == torch.int64 else 32
+    P_ = nat.ptr
+    cases = {
+        "montgomery_mul": (lambda: lib.fhb_op_rns_binary(bits, 0, P_(x), L * n, P_(y), L * n, P_(out), L * n, B, L, n,
+                                                           P_(prm), prm.stride(0), s),
+                           3 * B * L * n * word),
+        "keyswitch_accumulate_digit_products_": (
+            lambda: lib.fhb_op_keyswitch_accumulate(bits, P_(acc0), QP * n, P_(acc1), QP * n, P_(digit), QP * n,
+                                                    P_(kd), QP * n, 0, B, QP, n, P_(prm), prm.stride(0), s),
+            (5 * B * QP + 2 * QP) * n * word),
+        "keyswitch_moddown_qp_to_q": (
+            lambda: lib.fhb_op_moddown(bits, P_(digit), QP * n, P_(digit[:, L:]), QP * n, P_(md_out), L * n, B, L, P,
+                                       n, P_(inv_md), QP, P_(prm), prm.stride(0), s),
+            (B * QP + B * L) * n * word),
+        "rescale_drop_leading_prime_nearest": (
+            lambda: lib.fhb_op_rescale(bits, P_(x[:, 1:]), L * n, P_(x[:, 0]), L * n, P_(rs_out), (L - 1) * n, B,
+                                       L - 1, n, P_(inv_rs), P_(prm[:, 1:]), prm.stride(0), eng.moduli[0] // 2, 1, s),
+            (B * L + B * (L - 1)) * n * word),
+    }
+    res = {"shape": f"batch {B}, L = {L}, P = {P}, N = {n}, {bits}-bit words", "hbm_peak_gbs": hbm}
+    for name, (fn, nbytes) in cases.items():
+        nat.check(fn(), name)
+        torch.cuda.synchronize(x.device)
+        ms = _time_events(lambda: nat.check(fn(), name), steps, stream)
+        res[name] = {"ms": ms, "gbs": nbytes / ms / 1e6, "hbm_frac": nbytes / ms / 1e6 / hbm,
+                     "algorithmic_bytes": nbytes}
+    return res
+
+
 def mixed_batch_leg(dev, stream, count=512, steps=3):
     """Mixed-level batch at slots32768_scale40_levels34_int64: `count`
     ciphertexts with limb counts uniform in 3..35 (uniform [-0.05, 0.05]
@@ -467,7 +522,7 @@ def main() -> int:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-extras", action="store_true", help="skip rotation/parity/CPU legs")
     ap.add_argument("--mixed-count", type=int, default=512, help="ciphertexts of the mixed-level leg (0: skip)")
-    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed", "ops"], default=None,
+    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed", "ops", "schema"], default=None,
                     help="run only this side leg on one GPU and print its result (profiling aid)")
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -483,6 +538,16 @@ def main() -> int:
             res = bootstrap_leg(dev, stream, steps=max(1, args.steps))
         elif args.leg == "ops":
             res = ops_leg(dev, stream, batch=args.batch, steps=args.steps)
+        elif args.leg == "schema":
+            from fhelium_b200.config import Preset
+            from fhelium_b200.engine import CkksEngine
+            eng = CkksEngine(Preset.slots32768_scale40_levels34_int64, device=dev)
+            q = torch.tensor(eng.moduli, dtype=torch.int64, device=dev)[:, None]
+            g = torch.Generator(device=dev).manual_seed(9)
+            rows = lambda b, r: (torch.randint(0, 1 << 62, (b, r, eng.n), generator=g, device=dev) % q[:r])
+            x, y = rows(args.batch, eng.num_q), rows(args.batch, eng.num_q)
+            kd = rows(2, eng.num_q + eng.num_p)
+            res = schema_ops_leg(eng, x, y, kd, stream, steps=max(1, args.steps))
         else:
             res = mixed_batch_leg(dev, stream, args.mixed_count, args.steps)
         print(json.dumps({"leg": args.leg, **res}), flush=True)
@@ -631,6 +696,7 @@ def main() -> int:
         eng.generate_rotation_keys(steps16)
         h_ms = _time_events(lambda: eng.rotate_many_by_steps(rot_in, steps16), 2, stream)
         extras["hoisted_rotations_16_ops_per_s"] = 16 * B / (h_ms / 1000.0)
+        extras["reference_schema_kernels"] = schema_ops_leg(eng, ca.data[0], ca.data[1], rlk.data[0], stream)
         extras["ntt_int32_logN16_36limbs_batch64"] = ntt_leg(dev, stream, args.steps)
         extras["bootstrap_logN16_batch8"] = bootstrap_leg(dev, stream)
         if args.mixed_count > 0:

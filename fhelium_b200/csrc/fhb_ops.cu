@@ -21,6 +21,7 @@
 // words apart and coefficients contiguous; its batch stride (in words) is
 // passed separately, so limb slices of a larger tensor need no copy.
 #include <cstdint>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -88,41 +89,101 @@ using S = typename std::conditional<sizeof(T) == 8, int64_t, int32_t>::type;
   const int row = blockIdx.y;                                             \
   if (k >= n) return;
 
-template <typename T>
-__global__ void k_op_binary(int op, const T* __restrict__ a, int64_t as, const T* __restrict__ b, int64_t bs,
-                            T* __restrict__ out, int64_t os, int64_t batch, int64_t n, const T* __restrict__ params,
-                            int64_t ps) {
-  FHB_OP_INDEX
-  const ColumnPrime<T> p = column_prime(params, ps, row);
-  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
-    const T x = a[bi * as + row * n + k];
-    const T y = b[bi * bs + row * n + k];
-    T r;
-    switch (op) {
-      case 0: r = mont_canonical(x, y, p.q, p.neg_inv); break;
-      case 1: r = add_lazy2(x, y, p.twice_q); break;
-      case 2: r = sub_lazy2(x, y, p.twice_q); break;
-      case 3: r = csub(add_lazy2(x, y, p.twice_q), p.q); break;
-      default: r = csub(sub_lazy2(x, y, p.twice_q), p.q); break;
-    }
-    out[bi * os + row * n + k] = r;
+// Vectorised element-wise kernels: each thread owns V consecutive
+// coefficients of one row (16-byte loads and stores when V > 1) and walks the
+// batch items of its z-slice, so the row's constants and the index arithmetic
+// are paid once per thread rather than once per element.
+#define FHB_OP_VINDEX                                                         \
+  const int64_t k = (int64_t(blockIdx.x) * kOpThreads + threadIdx.x) * V;   \
+  const int row = blockIdx.y;                                                 \
+  if (k >= n) return;
+
+template <typename T, int V>
+struct alignas(V * sizeof(T) >= 16 ? 16 : sizeof(T)) Vec {
+  T v[V];
+};
+
+template <typename T, int V>
+__device__ __forceinline__ Vec<T, V> ldv(const T* p) {
+  Vec<T, V> r;
+  if constexpr (V * sizeof(T) == 16) {
+    *reinterpret_cast<uint4*>(r.v) = *reinterpret_cast<const uint4*>(p);
+  } else {
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = p[i];
+  }
+  return r;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void stv(T* p, const Vec<T, V>& r) {
+  if constexpr (V * sizeof(T) == 16) {
+    *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(r.v);
+  } else {
+#pragma unroll
+    for (int i = 0; i < V; ++i) p[i] = r.v[i];
   }
 }
 
+// Representative in [0, q) of a signed value; one or two corrections for the
+// values that occur (|v| < 2q), the general remainder otherwise.
 template <typename T>
-__global__ void k_op_unary(int op, T* __restrict__ x, int64_t xs, int64_t batch, int64_t n,
-                           const T* __restrict__ params, int64_t ps) {
-  FHB_OP_INDEX
+__device__ __forceinline__ T canon_near(int64_t v, T q) {
+  const int64_t qq = static_cast<int64_t>(q);
+  if (v >= -2 * qq && v < 2 * qq) {
+    if (v < 0) v += 2 * qq;
+    if (v >= qq) v -= qq;
+    return static_cast<T>(v);
+  }
+  return canon_signed<T>(v, q);
+}
+
+template <typename T, int OP>
+__device__ __forceinline__ T binary_op(T x, T y, const ColumnPrime<T>& p) {
+  if constexpr (OP == 0) return mont_canonical(x, y, p.q, p.neg_inv);
+  if constexpr (OP == 1) return add_lazy2(x, y, p.twice_q);
+  if constexpr (OP == 2) return sub_lazy2(x, y, p.twice_q);
+  if constexpr (OP == 3) return csub(add_lazy2(x, y, p.twice_q), p.q);
+  return csub(sub_lazy2(x, y, p.twice_q), p.q);
+}
+
+template <typename T, int OP, int V>
+__global__ void k_op_binary(const T* __restrict__ a, int64_t as, const T* __restrict__ b, int64_t bs,
+                            T* __restrict__ out, int64_t os, int64_t batch, int64_t n, const T* __restrict__ params,
+                            int64_t ps) {
+  FHB_OP_VINDEX
   const ColumnPrime<T> p = column_prime(params, ps, row);
+  const int64_t off = row * n + k;
   for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
-    T& v = x[bi * xs + row * n + k];
-    switch (op) {
-      case 0: v = mont_canonical(v, p.r2, p.q, p.neg_inv); break;
-      case 1: v = mont_canonical(v, T(1), p.q, p.neg_inv); break;
-      case 2: v = v < p.q ? v : v - p.q; break;
-      case 3: v = static_cast<S<T>>(v) <= static_cast<S<T>>(p.q >> 1) ? v : T(v - p.q); break;
-      default: v = v + p.q; break;
-    }
+    const Vec<T, V> x = ldv<T, V>(a + bi * as + off);
+    const Vec<T, V> y = ldv<T, V>(b + bi * bs + off);
+    Vec<T, V> r;
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = binary_op<T, OP>(x.v[i], y.v[i], p);
+    stv<T, V>(out + bi * os + off, r);
+  }
+}
+
+template <typename T, int OP>
+__device__ __forceinline__ T unary_op(T v, const ColumnPrime<T>& p) {
+  if constexpr (OP == 0) return mont_canonical(v, p.r2, p.q, p.neg_inv);
+  if constexpr (OP == 1) return mont_canonical(v, T(1), p.q, p.neg_inv);
+  if constexpr (OP == 2) return v < p.q ? v : v - p.q;
+  if constexpr (OP == 3) return static_cast<S<T>>(v) <= static_cast<S<T>>(p.q >> 1) ? v : T(v - p.q);
+  return v + p.q;
+}
+
+template <typename T, int OP, int V>
+__global__ void k_op_unary(T* __restrict__ x, int64_t xs, int64_t batch, int64_t n, const T* __restrict__ params,
+                           int64_t ps) {
+  FHB_OP_VINDEX
+  const ColumnPrime<T> p = column_prime(params, ps, row);
+  const int64_t off = row * n + k;
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
+    Vec<T, V> r = ldv<T, V>(x + bi * xs + off);
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = unary_op<T, OP>(r.v[i], p);
+    stv<T, V>(x + bi * xs + off, r);
   }
 }
 
@@ -138,7 +199,8 @@ __global__ void k_op_lift_centered(const T* __restrict__ coeffs, int64_t cs, T* 
 // (csrc/ops/rns/cpu/rns_arithmetic_cpu.cpp:482-615): digit 0 is the first
 // residue, each next digit (x_r - partial_r) * normaliser_r, and each new
 // digit is propagated into the partial sums of the rows after it.  Digits are
-// canonical; partial sums are carried in 64 bits.
+// canonical; partial sums are kept reduced modulo their row's prime (the
+// digit depends only on x_r - partial_r mod q_r).
 template <typename T>
 __global__ void k_op_mixed_radix_decompose(const T* __restrict__ src, int64_t ss, T* __restrict__ out, int64_t os,
                                            int64_t batch, int rows, int64_t n, const T* __restrict__ normalizers,
@@ -158,15 +220,18 @@ __global__ void k_op_mixed_radix_decompose(const T* __restrict__ src, int64_t ss
     int64_t digit[kMaxDecomposeRows];
     T first = s[0];
     if (first >= q[0]) first -= q[0];
-    for (int r = 0; r < rows; ++r) digit[r] = static_cast<int64_t>(first);
+    for (int r = 0; r < rows; ++r) digit[r] = static_cast<int64_t>(r == 0 ? first : canon_near<T>(first, q[r]));
     for (int step = 0; step + 1 < rows; ++step) {
       const int r = step + 1;
       const int64_t x = static_cast<int64_t>(static_cast<S<T>>(s[r * n]));
-      const T d = mont_canonical(canon_signed<T>(x - digit[r], q[r]),
-                                 canon_signed<T>(static_cast<S<T>>(normalizers[step]), q[r]), q[r], ni[r]);
+      const T d = mont_canonical(canon_near<T>(x - digit[r], q[r]),
+                                 canon_near<T>(static_cast<S<T>>(normalizers[step]), q[r]), q[r], ni[r]);
       digit[r] = static_cast<int64_t>(d);
+      // partial sums kept in [0, q_t): only their residue mod q_t is used
       for (int t = r + 1; t < rows; ++t)
-        digit[t] += static_cast<int64_t>(mont_canonical(d, propagation[step * prop_stride + t], q[t], ni[t]));
+        digit[t] = static_cast<int64_t>(csub(static_cast<T>(digit[t]) +
+                                                 mont_canonical(d, propagation[step * prop_stride + t], q[t], ni[t]),
+                                             q[t]));
     }
     T* o = out + bi * os + k;
     for (int r = 0; r < rows; ++r) o[r * n] = static_cast<T>(digit[r]);
@@ -193,21 +258,27 @@ __global__ void k_op_basis_extend(const T* __restrict__ digits, int64_t ds, int 
 
 // acc_c += digit * key[c][key_row_start + row], c = 0, 1
 // (csrc/ops/ckks/cpu/ckks_cpu.cpp:605-700).
-template <typename T>
+template <typename T, int V>
 __global__ void k_op_keyswitch_accumulate(T* __restrict__ acc0, int64_t a0s, T* __restrict__ acc1, int64_t a1s,
                                           const T* __restrict__ digit, int64_t ds, const T* __restrict__ key,
                                           int64_t key_component_stride, int64_t key_row_start, int64_t batch,
                                           int64_t n, const T* __restrict__ params, int64_t ps) {
-  FHB_OP_INDEX
+  FHB_OP_VINDEX
   const ColumnPrime<T> p = column_prime(params, ps, row);
-  const T k0 = key[(key_row_start + row) * n + k];
-  const T k1 = key[key_component_stride + (key_row_start + row) * n + k];
+  const Vec<T, V> k0 = ldv<T, V>(key + (key_row_start + row) * n + k);
+  const Vec<T, V> k1 = ldv<T, V>(key + key_component_stride + (key_row_start + row) * n + k);
+  const int64_t off = row * n + k;
   for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
-    const T v = digit[bi * ds + row * n + k];
-    T& x0 = acc0[bi * a0s + row * n + k];
-    T& x1 = acc1[bi * a1s + row * n + k];
-    x0 = add_lazy2(x0, mont_canonical(v, k0, p.q, p.neg_inv), p.twice_q);
-    x1 = add_lazy2(x1, mont_canonical(v, k1, p.q, p.neg_inv), p.twice_q);
+    const Vec<T, V> v = ldv<T, V>(digit + bi * ds + off);
+    Vec<T, V> x0 = ldv<T, V>(acc0 + bi * a0s + off);
+    Vec<T, V> x1 = ldv<T, V>(acc1 + bi * a1s + off);
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      x0.v[i] = add_lazy2(x0.v[i], mont_canonical(v.v[i], k0.v[i], p.q, p.neg_inv), p.twice_q);
+      x1.v[i] = add_lazy2(x1.v[i], mont_canonical(v.v[i], k1.v[i], p.q, p.neg_inv), p.twice_q);
+    }
+    stv<T, V>(acc0 + bi * a0s + off, x0);
+    stv<T, V>(acc1 + bi * a1s + off, x1);
   }
 }
 
@@ -230,9 +301,9 @@ __global__ void k_op_moddown(const T* __restrict__ qr, int64_t qs, const T* __re
       const ColumnPrime<T> p = column_prime(params, ps, qn + r);
       T v = chain[r];
       for (int lower = pn - 1; lower > r; --lower) {
-        const T diff = sub_lazy2(v, chain[lower], p.twice_q);
-        const T inv = canon_signed<T>(static_cast<S<T>>(inverse[(pn - lower - 1) * inv_stride + r + qn]), p.q);
-        v = mont_canonical(canon_signed<T>(static_cast<int64_t>(diff), p.q), inv, p.q, p.neg_inv);
+        const T diff = sub_lazy2(v, chain[lower], p.twice_q);   // [0, 2q)
+        const T inv = canon_near<T>(static_cast<S<T>>(inverse[(pn - lower - 1) * inv_stride + r + qn]), p.q);
+        v = mont_canonical(csub(diff, p.q), inv, p.q, p.neg_inv);
       }
       chain[r] = v;
     }
@@ -241,9 +312,9 @@ __global__ void k_op_moddown(const T* __restrict__ qr, int64_t qs, const T* __re
       T v = mont_canonical(qr[bi * qs + i * n + k], p.r2, p.q, p.neg_inv);
       for (int r = pn - 1; r >= 0; --r) {
         const T pm = mont_canonical(chain[r], p.r2, p.q, p.neg_inv);
-        v = sub_lazy2(v, pm, p.twice_q);
-        const T inv = canon_signed<T>(static_cast<S<T>>(inverse[(pn - r - 1) * inv_stride + i]), p.q);
-        v = mont_canonical(canon_signed<T>(static_cast<int64_t>(v), p.q), inv, p.q, p.neg_inv);
+        v = sub_lazy2(v, pm, p.twice_q);                            // [0, 2q)
+        const T inv = canon_near<T>(static_cast<S<T>>(inverse[(pn - r - 1) * inv_stride + i]), p.q);
+        v = mont_canonical(csub(v, p.q), inv, p.q, p.neg_inv);
       }
       v = mont_canonical(v, T(1), p.q, p.neg_inv);
       out[bi * os + i * n + k] = v < p.q ? v : v - p.q;
@@ -254,20 +325,28 @@ __global__ void k_op_moddown(const T* __restrict__ qr, int64_t qs, const T* __re
 // Rescale by the dropped leading prime: (x_j - x_drop) * q_drop^-1, plus one
 // when rounding to nearest and x_drop > floor(q_drop / 2)
 // (csrc/ops/ckks/cpu/ckks_cpu.cpp:203-262).  Canonical output.
-template <typename T>
+template <typename T, int V>
 __global__ void k_op_rescale(const T* __restrict__ rem, int64_t rs, const T* __restrict__ dropped, int64_t ds,
                              T* __restrict__ out, int64_t os, int64_t batch, int64_t n,
                              const T* __restrict__ inverse_mont, const T* __restrict__ params, int64_t ps,
                              int64_t half_drop, int nearest) {
-  FHB_OP_INDEX
+  FHB_OP_VINDEX
   const ColumnPrime<T> p = column_prime(params, ps, row);
-  const T inv = canon_signed<T>(static_cast<S<T>>(inverse_mont[row]), p.q);
+  const T inv = canon_near<T>(static_cast<S<T>>(inverse_mont[row]), p.q);
+  const int64_t off = row * n + k;
   for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
-    const int64_t dv = static_cast<S<T>>(dropped[bi * ds + k]);
-    const int64_t x = static_cast<S<T>>(rem[bi * rs + row * n + k]);
-    T quo = mont_canonical(canon_signed<T>(x - dv, p.q), inv, p.q, p.neg_inv);
-    if (nearest && dv > half_drop) quo += 1;
-    out[bi * os + row * n + k] = quo < p.q ? quo : quo - p.q;
+    const Vec<T, V> d = ldv<T, V>(dropped + bi * ds + k);
+    const Vec<T, V> x = ldv<T, V>(rem + bi * rs + off);
+    Vec<T, V> r;
+#pragma unroll
+    for (int i = 0; i < V; ++i) {
+      const int64_t dv = static_cast<S<T>>(d.v[i]);
+      T quo = mont_canonical(canon_near<T>(static_cast<int64_t>(static_cast<S<T>>(x.v[i])) - dv, p.q), inv, p.q,
+                             p.neg_inv);
+      if (nearest && dv > half_drop) quo += 1;
+      r.v[i] = quo < p.q ? quo : quo - p.q;
+    }
+    stv<T, V>(out + bi * os + off, r);
   }
 }
 
@@ -365,6 +444,30 @@ int log2_exact(int64_t v) {
   return (int64_t{1} << s) == v ? s : -1;
 }
 
+// Vector kernels: V coefficients per thread; z-slices of the batch only as
+// many as needed for about 16 blocks per SM.
+dim3 op_grid_v(int64_t n, int v, int64_t rows, int64_t batch) {
+  const int64_t xb = (n / v + kOpThreads - 1) / kOpThreads;
+  int64_t z = (148 * 16 + xb * rows - 1) / (xb * rows);
+  if (z > batch) z = batch;
+  if (z > 65535) z = 65535;
+  if (z < 1) z = 1;
+  return dim3(static_cast<unsigned>(xb), static_cast<unsigned>(rows), static_cast<unsigned>(z));
+}
+
+// 16-byte vectors are used when every operand start and batch stride, and n,
+// are whole vectors.
+template <typename T>
+bool vec_ok(int64_t n, std::initializer_list<const void*> ptrs, std::initializer_list<int64_t> strides) {
+  constexpr int64_t V = 16 / sizeof(T);
+  if (n % V) return false;
+  for (const void* p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) % 16) return false;
+  for (int64_t st : strides)
+    if (st % V) return false;
+  return true;
+}
+
 dim3 op_grid(int64_t n, int64_t rows, int64_t batch) {
   const int64_t z = batch < 65535 ? batch : 65535;
   return dim3(static_cast<unsigned>((n + kOpThreads - 1) / kOpThreads), static_cast<unsigned>(rows),
@@ -404,6 +507,30 @@ bool empty(int64_t batch, int64_t rows, int64_t n) { return batch == 0 || rows =
 
 using fhb::fail;
 
+// Launch of one compile-time op at vector width VW or 1 (names of the calling entry point).
+#define FHB_BIN(OPN)                                                                                            \
+  case OPN:                                                                                                    \
+    if (vec)                                                                                                   \
+      fhb::k_op_binary<T, OPN, VW><<<g, fhb::kOpThreads, 0, st>>>((const T*)lhs, lhs_batch_stride, (const T*)rhs, \
+                                                                  rhs_batch_stride, (T*)out, out_batch_stride,  \
+                                                                  batch, n, (const T*)params, param_row_stride); \
+    else                                                                                                       \
+      fhb::k_op_binary<T, OPN, 1><<<g, fhb::kOpThreads, 0, st>>>((const T*)lhs, lhs_batch_stride, (const T*)rhs,  \
+                                                                 rhs_batch_stride, (T*)out, out_batch_stride,   \
+                                                                 batch, n, (const T*)params, param_row_stride); \
+    break;
+
+#define FHB_UN(OPN)                                                                                             \
+  case OPN:                                                                                                    \
+    if (vec)                                                                                                   \
+      fhb::k_op_unary<T, OPN, VW><<<g, fhb::kOpThreads, 0, st>>>((T*)residues, batch_stride, batch, n,           \
+                                                                 (const T*)params, param_row_stride);           \
+    else                                                                                                       \
+      fhb::k_op_unary<T, OPN, 1><<<g, fhb::kOpThreads, 0, st>>>((T*)residues, batch_stride, batch, n,            \
+                                                                (const T*)params, param_row_stride);            \
+    break;
+
+
 extern "C" {
 
 int fhb_op_rns_binary(int residue_bits, int op, const void* lhs, int64_t lhs_batch_stride, const void* rhs,
@@ -413,10 +540,13 @@ int fhb_op_rns_binary(int residue_bits, int op, const void* lhs, int64_t lhs_bat
   if (op < 0 || op > 4) return fail(-2, "unknown binary op");
   if (fhb::empty(batch, rows, n)) return 0;
   FHB_NONNULL(lhs) FHB_NONNULL(rhs) FHB_NONNULL(out) FHB_NONNULL(params)
-  FHB_DISPATCH(residue_bits,
-               fhb::k_op_binary<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
-                   op, (const T*)lhs, lhs_batch_stride, (const T*)rhs, rhs_batch_stride, (T*)out,
-                   out_batch_stride, batch, n, (const T*)params, param_row_stride))
+  FHB_DISPATCH(residue_bits, {
+    const bool vec = fhb::vec_ok<T>(n, {lhs, rhs, out}, {lhs_batch_stride, rhs_batch_stride, out_batch_stride});
+    constexpr int VW = 16 / sizeof(T);
+    const dim3 g = fhb::op_grid_v(n, vec ? VW : 1, rows, batch);
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (op) { FHB_BIN(0) FHB_BIN(1) FHB_BIN(2) FHB_BIN(3) FHB_BIN(4) }
+  })
   return fhb::launch_status();
 }
 
@@ -426,9 +556,13 @@ int fhb_op_rns_unary(int residue_bits, int op, void* residues, int64_t batch_str
   if (op < 0 || op > 4) return fail(-2, "unknown unary op");
   if (fhb::empty(batch, rows, n)) return 0;
   FHB_NONNULL(residues) FHB_NONNULL(params)
-  FHB_DISPATCH(residue_bits,
-               fhb::k_op_unary<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
-                   op, (T*)residues, batch_stride, batch, n, (const T*)params, param_row_stride))
+  FHB_DISPATCH(residue_bits, {
+    const bool vec = fhb::vec_ok<T>(n, {residues}, {batch_stride});
+    constexpr int VW = 16 / sizeof(T);
+    const dim3 g = fhb::op_grid_v(n, vec ? VW : 1, rows, batch);
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (op) { FHB_UN(0) FHB_UN(1) FHB_UN(2) FHB_UN(3) FHB_UN(4) }
+  })
   return fhb::launch_status();
 }
 
@@ -492,12 +626,20 @@ int fhb_op_keyswitch_accumulate(int residue_bits, void* acc0, int64_t acc0_batch
   if (key_row_start < 0) return fail(-4, "negative key row start");
   if (fhb::empty(batch, rows, n)) return 0;
   FHB_NONNULL(acc0) FHB_NONNULL(acc1) FHB_NONNULL(digit) FHB_NONNULL(key_digit) FHB_NONNULL(params)
-  FHB_DISPATCH(residue_bits,
-               fhb::k_op_keyswitch_accumulate<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0,
-                                                   (cudaStream_t)stream>>>(
-                   (T*)acc0, acc0_batch_stride, (T*)acc1, acc1_batch_stride, (const T*)digit, digit_batch_stride,
-                   (const T*)key_digit, key_component_stride, key_row_start, batch, n, (const T*)params,
-                   param_row_stride))
+  FHB_DISPATCH(residue_bits, {
+    const bool vec = fhb::vec_ok<T>(n, {acc0, acc1, digit, key_digit},
+                                    {acc0_batch_stride, acc1_batch_stride, digit_batch_stride, key_component_stride});
+    constexpr int VW = 16 / sizeof(T);
+    const dim3 g = fhb::op_grid_v(n, vec ? VW : 1, rows, batch);
+    if (vec)
+      fhb::k_op_keyswitch_accumulate<T, VW><<<g, fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
+          (T*)acc0, acc0_batch_stride, (T*)acc1, acc1_batch_stride, (const T*)digit, digit_batch_stride,
+          (const T*)key_digit, key_component_stride, key_row_start, batch, n, (const T*)params, param_row_stride);
+    else
+      fhb::k_op_keyswitch_accumulate<T, 1><<<g, fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
+          (T*)acc0, acc0_batch_stride, (T*)acc1, acc1_batch_stride, (const T*)digit, digit_batch_stride,
+          (const T*)key_digit, key_component_stride, key_row_start, batch, n, (const T*)params, param_row_stride);
+  })
   return fhb::launch_status();
 }
 
@@ -524,11 +666,22 @@ int fhb_op_rescale(int residue_bits, const void* remaining, int64_t remaining_ba
   if (int rc = fhb::check_shape(residue_bits, batch, rows, n)) return rc;
   if (fhb::empty(batch, rows, n)) return 0;
   FHB_NONNULL(remaining) FHB_NONNULL(dropped) FHB_NONNULL(out) FHB_NONNULL(inverse_montgomery) FHB_NONNULL(params)
-  FHB_DISPATCH(residue_bits,
-               fhb::k_op_rescale<T><<<fhb::op_grid(n, rows, batch), fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
-                   (const T*)remaining, remaining_batch_stride, (const T*)dropped, dropped_batch_stride, (T*)out,
-                   out_batch_stride, batch, n, (const T*)inverse_montgomery, (const T*)params, param_row_stride,
-                   half_drop_prime, nearest))
+  FHB_DISPATCH(residue_bits, {
+    const bool vec = fhb::vec_ok<T>(n, {remaining, dropped, out},
+                                    {remaining_batch_stride, dropped_batch_stride, out_batch_stride});
+    constexpr int VW = 16 / sizeof(T);
+    const dim3 g = fhb::op_grid_v(n, vec ? VW : 1, rows, batch);
+    if (vec)
+      fhb::k_op_rescale<T, VW><<<g, fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
+          (const T*)remaining, remaining_batch_stride, (const T*)dropped, dropped_batch_stride, (T*)out,
+          out_batch_stride, batch, n, (const T*)inverse_montgomery, (const T*)params, param_row_stride,
+          half_drop_prime, nearest);
+    else
+      fhb::k_op_rescale<T, 1><<<g, fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
+          (const T*)remaining, remaining_batch_stride, (const T*)dropped, dropped_batch_stride, (T*)out,
+          out_batch_stride, batch, n, (const T*)inverse_montgomery, (const T*)params, param_row_stride,
+          half_drop_prime, nearest);
+  })
   return fhb::launch_status();
 }
 
