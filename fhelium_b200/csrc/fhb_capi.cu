@@ -61,6 +61,19 @@ int check_galois(const Context& c, uint32_t g) {
   return 0;
 }
 
+// Grid of the element-wise row kernels: V coefficients per thread, rows on y,
+// z-slices of the batch for about 16 blocks per SM.
+dim3 row_grid(int64_t n, int v, int64_t rows, int64_t batch) {
+  const int64_t xb = (n / v + kEwThreads - 1) / kEwThreads;
+  int64_t z = (148 * 16 + xb * rows - 1) / (xb * rows);
+  if (z > batch) z = batch;
+  if (z > 65535) z = 65535;
+  if (z < 1) z = 1;
+  return dim3(unsigned(xb), unsigned(rows), unsigned(z));
+}
+
+bool aligned16(const void* p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; }
+
 int elementwise_grid(int64_t total) {
   int64_t blocks = (total + 255) / 256;
   const int64_t cap = 148 * 32;
@@ -164,16 +177,26 @@ template <typename T>
 int mul_ntt(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
             cudaStream_t st) {
   const int limbs = c.num_q - level;
-  k_mul_ntt<T><<<elementwise_grid(batch * limbs << c.log_n), 256, 0, st>>>(
-      (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c));
+  constexpr int V = 16 / sizeof(T);
+  if (aligned16(a) && aligned16(b) && aligned16(out))
+    k_mul_ntt<T, V><<<row_grid(c.n(), V, limbs, batch), kEwThreads, 0, st>>>(
+        (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c));
+  else
+    k_mul_ntt<T, 1><<<row_grid(c.n(), 1, limbs, batch), kEwThreads, 0, st>>>(
+        (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c));
   return cuda_status(cudaGetLastError(), "k_mul_ntt");
 }
 
 template <typename T>
 int rns_binary(const Context& c, const void* a, const void* b, void* out, int64_t batch, int rows, int row_start,
                int op, int b_mode, cudaStream_t st) {
-  k_rns_binary<T><<<elementwise_grid(batch * rows << c.log_n), 256, 0, st>>>(
-      (const T*)a, (const T*)b, (T*)out, batch, rows, row_start, c.log_n, op, b_mode, tables<T>(c));
+  constexpr int V = 16 / sizeof(T);
+  if (aligned16(a) && (b == nullptr || b_mode == 2 || aligned16(b)) && aligned16(out))
+    k_rns_binary<T, V><<<row_grid(c.n(), V, rows, batch), kEwThreads, 0, st>>>(
+        (const T*)a, (const T*)b, (T*)out, batch, rows, row_start, c.log_n, op, b_mode, tables<T>(c));
+  else
+    k_rns_binary<T, 1><<<row_grid(c.n(), 1, rows, batch), kEwThreads, 0, st>>>(
+        (const T*)a, (const T*)b, (T*)out, batch, rows, row_start, c.log_n, op, b_mode, tables<T>(c));
   return cuda_status(cudaGetLastError(), "k_rns_binary");
 }
 

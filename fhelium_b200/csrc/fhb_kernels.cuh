@@ -176,18 +176,64 @@ k_mul_to_coefficient(const T* __restrict__ a, const T* __restrict__ b, T* __rest
                                                 epi);
 }
 
+// Element-wise kernels over [batch, rows, N]: each thread owns V consecutive
+// coefficients of one row (16-byte loads and stores when V > 1) and walks the
+// batch items of its z-slice, so the row's constants and the index arithmetic
+// are paid once per thread.  Grid: (N / (256 V), rows, z-slices).
+constexpr int kEwThreads = 256;
+
+template <typename T, int V>
+struct alignas(V * sizeof(T) >= 16 ? 16 : sizeof(T)) EwVec {
+  T v[V];
+};
+
+template <typename T, int V>
+__device__ __forceinline__ EwVec<T, V> ew_load(const T* p) {
+  EwVec<T, V> r;
+  if constexpr (V * sizeof(T) == 16) {
+    *reinterpret_cast<uint4*>(r.v) = *reinterpret_cast<const uint4*>(p);
+  } else {
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = p[i];
+  }
+  return r;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void ew_store(T* p, const EwVec<T, V>& r) {
+  if constexpr (V * sizeof(T) == 16) {
+    *reinterpret_cast<uint4*>(p) = *reinterpret_cast<const uint4*>(r.v);
+  } else {
+#pragma unroll
+    for (int i = 0; i < V; ++i) p[i] = r.v[i];
+  }
+}
+
 // NTT-domain tensor product only (reference multiply): out [3, B, L, N] lazy.
-template <typename T>
+template <typename T, int V>
 __global__ void k_mul_ntt(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
                           int64_t batch, int limbs, int log_n, int level, ChainTables<T> tabs) {
   const int64_t n = int64_t(1) << log_n;
+  const int64_t k = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
+  if (k >= n) return;
+  const int row = blockIdx.y;
+  const PrimeInfo<T>& pp = tabs.prime[level + row];
+  const T q = pp.q, ni = pp.neg_inv, tq = pp.twice_q;
   const int64_t total = batch * limbs * n;
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-    const PrimeInfo<T> p = tabs.prime[level + int((i >> log_n) % limbs)];
-    const T x0 = a[i], x1 = a[total + i], y0 = b[i], y1 = b[total + i];
-    out[i] = Word<T>::mont(x0, y0, p.q, p.neg_inv);
-    out[total + i] = csub(Word<T>::mont(x0, y1, p.q, p.neg_inv) + Word<T>::mont(x1, y0, p.q, p.neg_inv), p.twice_q);
-    out[2 * total + i] = Word<T>::mont(x1, y1, p.q, p.neg_inv);
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
+    const int64_t i = (bi * limbs + row) * n + k;
+    const EwVec<T, V> x0 = ew_load<T, V>(a + i), x1 = ew_load<T, V>(a + total + i);
+    const EwVec<T, V> y0 = ew_load<T, V>(b + i), y1 = ew_load<T, V>(b + total + i);
+    EwVec<T, V> d0, d1, d2;
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      d0.v[e] = Word<T>::mont(x0.v[e], y0.v[e], q, ni);
+      d1.v[e] = csub(Word<T>::mont(x0.v[e], y1.v[e], q, ni) + Word<T>::mont(x1.v[e], y0.v[e], q, ni), tq);
+      d2.v[e] = Word<T>::mont(x1.v[e], y1.v[e], q, ni);
+    }
+    ew_store<T, V>(out + i, d0);
+    ew_store<T, V>(out + total + i, d1);
+    ew_store<T, V>(out + 2 * total + i, d2);
   }
 }
 
@@ -802,28 +848,43 @@ __global__ void k_automorphism(const T* __restrict__ in, T* __restrict__ out, in
 enum RnsOp : int { kOpMontMul = 0, kOpAddLazy = 1, kOpSubLazy = 2, kOpAddCanon = 3, kOpSubCanon = 4,
                    kOpNegCanon = 5 };
 
-template <typename T>
+template <typename T, int V>
 __global__ void k_rns_binary(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out, int64_t batch,
                              int rows, int row_start, int log_n, int op, int b_mode, ChainTables<T> tabs) {
   const int64_t n = int64_t(1) << log_n;
-  const int64_t per = int64_t(rows) * n;
-  const int64_t total = batch * per;
-  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int row = int((idx >> log_n) % rows);
-    const PrimeInfo<T> p = tabs.prime[row_start + row];
-    const T x = a[idx];
-    const T y = op == kOpNegCanon ? T(0) : (b_mode == 0 ? b[idx] : (b_mode == 1 ? b[idx % per] : b[row]));
-    T r;
-    switch (op) {
-      case kOpMontMul: r = Word<T>::mont(x, y, p.q, p.neg_inv); break;
-      case kOpAddLazy: r = csub(x + y, p.twice_q); break;
-      case kOpSubLazy: r = csub(x + p.twice_q - y, p.twice_q); break;
-      case kOpAddCanon: r = csub(reduce_any(x, p) + reduce_any(y, p), p.q); break;
-      case kOpSubCanon: r = csub(reduce_any(x, p) + p.q - reduce_any(y, p), p.q); break;
-      default: { const T c = reduce_any(x, p); r = c ? p.q - c : T(0); }
+  const int64_t k = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
+  if (k >= n) return;
+  const int row = blockIdx.y;
+  const PrimeInfo<T> p = tabs.prime[row_start + row];
+  const int64_t per = int64_t(rows) * n, off = int64_t(row) * n + k;
+  EwVec<T, V> y;
+  if (op == kOpNegCanon) {
+#pragma unroll
+    for (int e = 0; e < V; ++e) y.v[e] = T(0);
+  } else if (b_mode == 1) {
+    y = ew_load<T, V>(b + off);
+  } else if (b_mode == 2) {
+#pragma unroll
+    for (int e = 0; e < V; ++e) y.v[e] = b[row];
+  }
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
+    const int64_t idx = bi * per + off;
+    const EwVec<T, V> x = ew_load<T, V>(a + idx);
+    if (b_mode == 0 && op != kOpNegCanon) y = ew_load<T, V>(b + idx);
+    EwVec<T, V> r;
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const T xv = x.v[e], yv = y.v[e];
+      switch (op) {
+        case kOpMontMul: r.v[e] = Word<T>::mont(xv, yv, p.q, p.neg_inv); break;
+        case kOpAddLazy: r.v[e] = csub(xv + yv, p.twice_q); break;
+        case kOpSubLazy: r.v[e] = csub(xv + p.twice_q - yv, p.twice_q); break;
+        case kOpAddCanon: r.v[e] = csub(reduce_any(xv, p) + reduce_any(yv, p), p.q); break;
+        case kOpSubCanon: r.v[e] = csub(reduce_any(xv, p) + p.q - reduce_any(yv, p), p.q); break;
+        default: { const T c = reduce_any(xv, p); r.v[e] = c ? p.q - c : T(0); }
+      }
     }
-    out[idx] = r;
+    ew_store<T, V>(out + idx, r);
   }
 }
 
