@@ -135,33 +135,6 @@ int modup(const Context& c, const void* comp, void* digits, int64_t batch, int l
   return cuda_status(cudaGetLastError(), "k_modup_digits");
 }
 
-// ModDown of accumulators the library owns (their P rows and, when
-// rescaling, their row 0 are overwritten): the two-phase kernels.
-template <typename T>
-int moddown_owned(const Context& c, void* t0, void* t1, const void* a0, const void* a1, void* out, int64_t batch,
-                  int level, uint32_t add0_galois, int rescale, cudaStream_t st,
-                  const uint32_t* item_galois = nullptr) {
-  const uint32_t ginv = add0_galois == 1 ? 0u : galois_inverse(add0_galois, c.log_n);
-  const int q_limbs = c.num_q - level;
-  const int out_limbs = q_limbs - (rescale ? 1 : 0);
-  if (batch == 0 || out_limbs <= 0) return 0;
-  k_moddown_p<T><<<elementwise_grid(2 * batch << c.log_n), 256, 0, st>>>(
-      (T*)t0, (T*)t1, (const T*)a0, (const T*)a1, batch, c.log_n, level, c.num_q, c.num_p, ginv, item_galois,
-      rescale, tables<T>(c));
-  constexpr int V = 16 / sizeof(T);
-  const bool vec = aligned16(t0) && aligned16(t1) && aligned16(out);
-  const dim3 g = row_grid(c.n(), vec ? V : 1, out_limbs, 2 * batch);
-  if (vec)
-    k_moddown_q<T, V><<<g, kEwThreads, 0, st>>>((const T*)t0, (const T*)t1, (const T*)a0, (const T*)a1, (T*)out,
-                                               batch, c.log_n, level, c.num_q, c.num_p, ginv, item_galois, rescale,
-                                               tables<T>(c), level_tables<T>(c, level));
-  else
-    k_moddown_q<T, 1><<<g, kEwThreads, 0, st>>>((const T*)t0, (const T*)t1, (const T*)a0, (const T*)a1, (T*)out,
-                                               batch, c.log_n, level, c.num_q, c.num_p, ginv, item_galois, rescale,
-                                               tables<T>(c), level_tables<T>(c, level));
-  return cuda_status(cudaGetLastError(), "k_moddown_q");
-}
-
 template <typename T>
 int moddown(const Context& c, const void* t0, const void* t1, const void* a0, const void* a1, void* out,
             int64_t batch, int level, uint32_t add0_galois, int rescale, cudaStream_t st,
@@ -631,7 +604,7 @@ static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* k
                           const void* add1, uint32_t add0_galois, void* out, int64_t batch, int level, int rescale,
                           cudaStream_t st) {
   TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st));
-  return FHB_WORD(fhb::moddown_owned, c, s.t0, s.t1, add0, add1, out, batch, level, add0_galois, rescale, st);
+  return FHB_WORD(fhb::moddown, c, s.t0, s.t1, add0, add1, out, batch, level, add0_galois, rescale, st);
 }
 
 // Relinearisation of an NTT-domain ct3 (coefficient-domain c2 already in
@@ -641,7 +614,7 @@ static int relinearize_tail(const Context& c, const fhb::Scratch& s, const void*
                             int64_t batch, int level, int rescale, cudaStream_t st) {
   TRY(FHB_WORD(fhb::modup, c, s.t0, s.digits, batch, level, 1u, st));
   TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st, nullptr, ct3));
-  return FHB_WORD(fhb::moddown_owned, c, s.t0, s.t1, nullptr, nullptr, out, batch, level, 1u, rescale, st);
+  return FHB_WORD(fhb::moddown, c, s.t0, s.t1, nullptr, nullptr, out, batch, level, 1u, rescale, st);
 }
 
 int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* key, void* out, void* scratch,
@@ -730,7 +703,7 @@ int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
   TRY(FHB_WORD(fhb::modup, c, static_cast<const char*>(ct) + comp, s.digits, batch, level, 1u, st, galois));
   TRY(fhb::ks_core(c, s.digits, nullptr, s.t0, s.t1, batch, level, st, key_ptrs));
-  return FHB_WORD(fhb::moddown_owned, c, s.t0, s.t1, ct, nullptr, out, batch, level, 1u, 0, st, galois);
+  return FHB_WORD(fhb::moddown, c, s.t0, s.t1, ct, nullptr, out, batch, level, 1u, 0, st, galois);
 }
 
 int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,

@@ -792,150 +792,6 @@ __global__ void k_moddown(const T* __restrict__ t0, const T* __restrict__ t1, co
   }
 }
 
-// Two-phase form of k_moddown for accumulators the library owns (the key
-// switches inside relinearisation and rotation), same results bit for bit.
-// Phase 1, one thread per (component, ciphertext, coefficient): the Garner
-// digits of the P part are written back over the accumulator's P rows and,
-// when rescaling, the finished value of the dropped row 0 over its row 0.
-// Phase 2 then computes every output row in parallel (rows on the grid,
-// 16-byte vectors, row constants held in registers) instead of one thread
-// walking all Q rows.
-template <typename T>
-__global__ void k_moddown_p(T* __restrict__ t0, T* __restrict__ t1, const T* __restrict__ add0,
-                            const T* __restrict__ add1, int64_t batch, int log_n, int level, int num_q, int num_p,
-                            uint32_t add0_ginv, const uint32_t* __restrict__ item_galois, int rescale,
-                            ChainTables<T> tabs) {
-  using W = Word<T>;
-  const int64_t n = int64_t(1) << log_n;
-  const int q_limbs = num_q - level;
-  const int qp_limbs = q_limbs + num_p;
-  const int64_t total = 2 * batch * n;
-  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int c = int(idx / (batch * n));
-    const int64_t bi = (idx >> log_n) % batch;
-    const int k = int(idx & (n - 1));
-    T* t = (c == 0 ? t0 : t1) + bi * qp_limbs * n;
-    T e[kMaxDigitWidth];
-    for (int r = 0; r < num_p; ++r) {
-      const PrimeInfo<T>& p = tabs.prime[num_q + r];
-      T x = t[(q_limbs + r) * n + k];
-      T acc = 0;
-      for (int i = 0; i < r; ++i) {
-        const TwPair<T> g = tabs.p_garner[r * kMaxDigitWidth + i];
-        acc = csub(acc + csub(W::shoup(e[i], g.w, g.wp, p.q), p.q), p.q);
-      }
-      if (r > 0) {
-        const TwPair<T> inv = tabs.p_garner[r * kMaxDigitWidth + r];
-        x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
-      }
-      e[r] = x;
-      t[(q_limbs + r) * n + k] = x;
-    }
-    if (rescale) {
-      const int pid = level;
-      const PrimeInfo<T>& p = tabs.prime[pid];
-      T sub = 0;
-      for (int r = 0; r < num_p; ++r) {
-        const TwPair<T> m = tabs.p_mix[r * (num_q + num_p) + pid];
-        sub = csub(sub + csub(W::shoup(e[r], m.w, m.wp, p.q), p.q), p.q);
-      }
-      const TwPair<T> pinv = tabs.p_inv[pid];
-      T v = csub(t[k] + p.q - sub, p.q);
-      v = csub(W::shoup(v, pinv.w, pinv.wp, p.q), p.q);
-      const T* ad = c == 0 ? add0 : add1;
-      if (ad) {
-        bool neg = false;
-        int kk = k;
-        if (c == 0) {
-          const uint32_t gi = item_galois ? (item_galois[bi] == 1 ? 0u : galois_inverse_dev(item_galois[bi], log_n))
-                                          : add0_ginv;
-          if (gi) kk = galois_source(k, log_n, gi, neg);
-        }
-        T x = csub(ad[(bi * q_limbs) * n + kk], p.q);
-        if (neg && x) x = p.q - x;
-        v = csub(v + x, p.q);
-      }
-      t[k] = v;
-    }
-  }
-}
-
-template <typename T, int V>
-__global__ void k_moddown_q(const T* __restrict__ t0, const T* __restrict__ t1, const T* __restrict__ add0,
-                            const T* __restrict__ add1, T* __restrict__ out, int64_t batch, int log_n, int level,
-                            int num_q, int num_p, uint32_t add0_ginv, const uint32_t* __restrict__ item_galois,
-                            int rescale, ChainTables<T> tabs, LevelTables<T> lt) {
-  using W = Word<T>;
-  const int64_t n = int64_t(1) << log_n;
-  const int64_t k = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
-  if (k >= n) return;
-  const int q_limbs = num_q - level;
-  const int qp_limbs = q_limbs + num_p;
-  const int out_limbs = q_limbs - (rescale ? 1 : 0);
-  const int oi = blockIdx.y;
-  const int i = oi + (rescale ? 1 : 0);
-  const int pid = level + i;
-  const PrimeInfo<T>& pp = tabs.prime[pid];
-  const T q = pp.q;
-  TwPair<T> mix[kMaxDigitWidth];
-#pragma unroll
-  for (int r = 0; r < kMaxDigitWidth; ++r)
-    if (r < num_p) mix[r] = tabs.p_mix[r * (num_q + num_p) + pid];
-  const TwPair<T> pinv = tabs.p_inv[pid];
-  TwPair<T> rinv{0, 0};
-  T half0 = 0;
-  if (rescale) {
-    rinv = lt.rescale_inv[pid];
-    half0 = tabs.prime[level].q >> 1;
-  }
-  for (int64_t cb = blockIdx.z; cb < 2 * batch; cb += gridDim.z) {
-    const int c = int(cb / batch);
-    const int64_t bi = cb % batch;
-    const T* t = (c == 0 ? t0 : t1) + bi * qp_limbs * n;
-    const T* ad = c == 0 ? add0 : add1;
-    uint32_t gi = 0;
-    if (c == 0 && ad)
-      gi = item_galois ? (item_galois[bi] == 1 ? 0u : galois_inverse_dev(item_galois[bi], log_n)) : add0_ginv;
-    const EwVec<T, V> ti = ew_load<T, V>(t + i * n + k);
-    EwVec<T, V> sub;
-#pragma unroll
-    for (int e = 0; e < V; ++e) sub.v[e] = 0;
-#pragma unroll
-    for (int r = 0; r < kMaxDigitWidth; ++r) {
-      if (r < num_p) {
-        const EwVec<T, V> er = ew_load<T, V>(t + (q_limbs + r) * n + k);
-#pragma unroll
-        for (int e = 0; e < V; ++e) sub.v[e] = csub(sub.v[e] + csub(W::shoup(er.v[e], mix[r].w, mix[r].wp, q), q), q);
-      }
-    }
-    EwVec<T, V> v0;
-    if (rescale) v0 = ew_load<T, V>(t + k);
-    EwVec<T, V> res;
-#pragma unroll
-    for (int e = 0; e < V; ++e) {
-      T v = csub(ti.v[e] + q - sub.v[e], q);
-      v = csub(W::shoup(v, pinv.w, pinv.wp, q), q);
-      if (ad) {
-        bool neg = false;
-        int kk = int(k) + e;
-        if (gi) kk = galois_source(kk, log_n, gi, neg);
-        T x = csub(ad[(bi * q_limbs + i) * n + kk], q);
-        if (neg && x) x = q - x;
-        v = csub(v + x, q);
-      }
-      if (rescale) {
-        const T x0 = reduce_any(v0.v[e], pp);
-        T r = csub(W::shoup(csub(v + q - x0, q), rinv.w, rinv.wp, q), q);
-        r += (v0.v[e] > half0) ? 1 : 0;
-        v = csub(r, q);
-      }
-      res.v[e] = v;
-    }
-    ew_store<T, V>(out + (int64_t(c) * batch + bi) * out_limbs * n + int64_t(oi) * n + k, res);
-  }
-}
-
 // Standalone rescale of coefficient/standard components: in [K, L, N] ->
 // out [K, L-1, N] (csrc/ops/ckks/cpu/ckks_cpu.cpp:203-262).
 template <typename T>
