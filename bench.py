@@ -634,6 +634,10 @@ def main() -> int:
                                                               nat.ptr(t[1]), B, 0, s),
         "moddown_rescale": lambda: lib.fhb_ckks_moddown(h, nat.ptr(t[0]), nat.ptr(t[1]), nat.ptr(coef[0]),
                                                         nat.ptr(coef[1]), nat.ptr(state["out"].data), B, 0, 1, 1, s),
+        # the two launches the fused step uses before ModUp: NTT-domain tensor
+        # product, then d2 alone to the coefficient domain
+        "tensor_product": lambda: lib.fhb_ckks_multiply(h, nat.ptr(ca.data), nat.ptr(cb.data), nat.ptr(coef), B, 0, s),
+        "inverse_ntt_d2": lambda: lib.fhb_inverse_ntt(h, nat.ptr(coef[2]), nat.ptr(digits), B, L, 0, 2, s),
     }
     per_kernel = {}
     for name, fn in kernels.items():
@@ -670,6 +674,30 @@ def main() -> int:
     modmul_peak = 148 * 8 * 256 * 8 * probe_iters / (probe_ms / 1000.0)
     modmul_achieved = ks_modmul / (per_kernel["keyswitch_core"] / 1000.0)
     step_bytes = B * (4 * L + 2 * (L - 1)) * limb + 10 * 2 * (L + cfg.num_p_primes) * limb
+    # every step kernel against its roofs: algorithmic bytes (each operand row
+    # read once, each output row written once, keys once per launch) over the
+    # measured copy bandwidth, and for the transform / basis-conversion
+    # kernels the modular products per launch over the probe's rate
+    P_ = cfg.num_p_primes
+    rows = lambda r: B * r * limb
+    kroof = {
+        "tensor_product": (rows(7 * L), 0),
+        "inverse_ntt_d2": (rows(2 * L), B * L * (bfly_ + n_)),
+        "mul_to_coefficient": (rows(7 * L), B * L * (4 * n_ + 3 * (bfly_ + n_))),
+        "modup_digits": (rows(2 * L), B * n_ * sum(len(d) * (len(d) + 1) // 2 for _, d in eng.level_digits[0])),
+        "keyswitch_core": (ks_bytes, ks_modmul),
+        "moddown_rescale": (rows(2 * (L + P_) + 2 * L + 2 * (L - 1)),
+                            2 * B * n_ * (P_ * (P_ + 1) // 2 + L * (P_ + 2))),
+    }
+    kernel_roofline = {}
+    for name, (nbytes, nmul) in kroof.items():
+        sec = per_kernel[name] / 1000.0
+        entry = {"ms": per_kernel[name], "algorithmic_bytes": nbytes, "hbm_gbs": nbytes / sec / 1e9,
+                 "hbm_frac": nbytes / sec / 1e9 / peak}
+        if nmul:
+            entry.update({"modmul": nmul, "modmul_per_s": nmul / sec, "modmul_frac": nmul / sec / modmul_peak})
+        entry["bound"] = "hbm" if not nmul or entry["hbm_frac"] > entry["modmul_frac"] else "integer"
+        kernel_roofline[name] = entry
     # DRAM bytes of one k_keyswitch_core launch: 15.7 GB measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on the batch-32 launch of
     # this command, work order 2 (groups of four ciphertexts share the key
@@ -743,6 +771,7 @@ def main() -> int:
                      "algorithmic_bytes_per_launch": ks_bytes, "launch_ms": per_kernel["keyswitch_core"],
                      "note": "int64 Montgomery/Shoup arithmetic on CUDA cores: the kernel is integer-ALU bound"},
         "kernel_ms": per_kernel,
+        "kernel_roofline": kernel_roofline,
         "kernel_ms_note": "each public entry point timed alone on the same inputs; the fused step runs the "
                           "HMult->INTT for d2 only and folds d0, d1 into the key-switch accumulators",
         "step_algorithmic_gbs": step_bytes / (ms / 1000.0) / 1e9,
