@@ -342,6 +342,29 @@ def _check_writable(t: torch.Tensor, name: str) -> None:
               "refers to a single memory location")
 
 
+def _no_overlap(out: torch.Tensor, *others) -> None:
+    """The reference's check_mutable_rns_output (csrc/ops/common/rns_batch.h:87-97,
+    at::assert_no_overlap): a written tensor may not share elements with a
+    read-only operand or table.  Like ATen, the same tensor or two dense tensors
+    with intersecting byte ranges are rejected; other layouts are not examined."""
+    from torch._prims_common import is_non_overlapping_and_dense_or_false as is_non_overlapping_and_dense
+    for other in others:
+        if other is None or other.numel() == 0 or out.numel() == 0:
+            continue
+        if other is out:
+            overlap = True
+        elif out.untyped_storage().data_ptr() != other.untyped_storage().data_ptr():
+            continue
+        elif not (is_non_overlapping_and_dense(out) and is_non_overlapping_and_dense(other)):
+            continue
+        else:
+            a0, b0 = out.data_ptr(), other.data_ptr()
+            overlap = a0 < b0 + other.numel() * other.element_size() and b0 < a0 + out.numel() * out.element_size()
+        if overlap:
+            _fail("unsupported operation: some elements of the input tensor and the written-to tensor refer to "
+                  "a single memory location.")
+
+
 def _cuda(t: torch.Tensor, name: str) -> None:
     if not t.is_cuda:
         _fail(f"{name} must be a CUDA tensor")
@@ -388,6 +411,7 @@ def _binary(op: int, lhs: torch.Tensor, rhs: torch.Tensor, params: torch.Tensor,
 def _unary_(op: int, x: torch.Tensor, params: torch.Tensor) -> None:
     _cuda(x, "residues")
     _check_writable(x, "residues")
+    _no_overlap(x, params)
     bits = _bits(x, "residues")
     rows, n = _rows_n(x, "residues")
     p, ps = _params(params, x, rows)
@@ -415,6 +439,7 @@ def add_canonical(lhs, rhs, rns_params):
 
 def add_canonical_(lhs, rhs, rns_params):
     _check_writable(lhs, "lhs")
+    _no_overlap(lhs, rhs, rns_params)
     _binary(3, lhs, rhs, rns_params, out=lhs)
 
 
@@ -424,6 +449,7 @@ def sub_canonical(lhs, rhs, rns_params):
 
 def sub_canonical_(lhs, rhs, rns_params):
     _check_writable(lhs, "lhs")
+    _no_overlap(lhs, rhs, rns_params)
     _binary(4, lhs, rhs, rns_params, out=lhs)
 
 
@@ -499,6 +525,7 @@ def _row_scalars(x, scalars, params, out=None):
 
 def montgomery_mul_row_scalars_(residues, row_scalars, rns_params):
     _check_writable(residues, "residues")
+    _no_overlap(residues, row_scalars, rns_params)
     _row_scalars(residues, row_scalars, rns_params, out=residues)
 
 
@@ -735,6 +762,7 @@ def _ntt_(x: torch.Tensor, tw: torch.Tensor, params: torch.Tensor, *, inverse: b
     """mode: forward 0 = standard input, 1 = Montgomery input; inverse = fhb_inverse_output."""
     _cuda(x, "residues")
     _check_writable(x, "residues")
+    _no_overlap(x, tw, params, radix_roots, *(schedule or ()))
     ctx, offset, primes, bits, log_n = _transform_context(x, params)
     _same(tw, x, "twiddles")
     if schedule is not None:
@@ -858,6 +886,7 @@ def _plaintext_op(layout: int, inplace: bool):
         def f(ct, strided, implicit, params):
             if inplace:
                 _check_writable(ct, "ciphertext_component")
+                _no_overlap(ct, strided, implicit, params)
                 _add_plaintext(3, ct, strided, params, implicit, out=ct)
                 return None
             return _add_plaintext(3, ct, strided, params, implicit)
@@ -865,6 +894,7 @@ def _plaintext_op(layout: int, inplace: bool):
         def f(ct, pt, params):
             if inplace:
                 _check_writable(ct, "ciphertext_component")
+                _no_overlap(ct, pt, params)
                 _add_plaintext(layout, ct, pt, params, out=ct)
                 return None
             return _add_plaintext(layout, ct, pt, params)
@@ -902,6 +932,7 @@ def rescale_drop_leading_prime_nearest(remaining, inverse_mont, dropped, params,
 
 def rescale_drop_leading_prime_nearest_(remaining, inverse_mont, dropped, params, half_drop_prime):
     _check_writable(remaining, "remaining_residues")
+    _no_overlap(remaining, inverse_mont, dropped, params)
     _rescale(remaining, inverse_mont, dropped, params, half_drop_prime, True, out=remaining)
 
 
@@ -911,6 +942,7 @@ def rescale_drop_leading_prime_truncate(remaining, inverse_mont, dropped, params
 
 def rescale_drop_leading_prime_truncate_(remaining, inverse_mont, dropped, params):
     _check_writable(remaining, "remaining_residues")
+    _no_overlap(remaining, inverse_mont, dropped, params)
     _rescale(remaining, inverse_mont, dropped, params, 0, False, out=remaining)
 
 
@@ -988,6 +1020,8 @@ def keyswitch_accumulate_digit_products_(acc0, acc1, digit, key_digit, params, k
         _fail("accumulators and digit must have the same shape")
     _check_writable(acc0, "accumulator0_qp")
     _check_writable(acc1, "accumulator1_qp")
+    _no_overlap(acc0, acc1, digit, key_digit, params)
+    _no_overlap(acc1, digit, key_digit, params)
     start = int(key_digit_row_start)
     if key_digit.dim() != 3 or key_digit.shape[0] != 2 or key_digit.shape[2] != n:
         _fail(f"key_switch_key_digit must be [2, key_rows, N], got {tuple(key_digit.shape)}")

@@ -290,6 +290,12 @@ def test_keyswitch_ops(ops, family, level):
     got = _n(ops.fhelium_ckks_ops.keyswitch_moddown_qp_to_q(full[:, :-p], full[:, -p:], _c(inv, ctx), _c(prm, ctx)))
     want = orc.keyswitch_moddown(acc[:, :-p], acc[:, -p:], inv, prm, ctx.radix_bits)
     np.testing.assert_array_equal(got, want)
+    # ModDown leaves its P rows (public values) untouched
+    # (reference tests/test_native_operator_invariants.py:201-268)
+    np.testing.assert_array_equal(_n(full), acc)
+    # an in-place op whose read-only operand is the written tensor is rejected
+    with pytest.raises(RuntimeError, match="single memory location"):
+        ops.fhelium_rns_ops.add_canonical_(full, full, _c(prm, ctx))
     _same_on_cpu(ops.fhelium_ckks_ops.keyswitch_moddown_qp_to_q, (acc[:, :-p], acc[:, -p:], inv, prm), ctx, got)
 
 

@@ -96,3 +96,15 @@ def test_checks_are_remembered_per_tensor_not_per_address(torch_ops):
     import gc
     gc.collect()
     assert len(torch_ops._memo) == before - 1                        # forgotten with the tensor
+
+
+def test_written_tensor_may_not_overlap_read_only_operands(torch_ops):
+    """The reference's check_mutable_rns_output (csrc/ops/common/rns_batch.h:87-97)."""
+    x = torch.zeros(2, 5, 8, dtype=torch.int64)
+    with pytest.raises(RuntimeError, match="single memory location"):
+        torch_ops._no_overlap(x, x)                    # lhs_ and rhs are one tensor
+    with pytest.raises(RuntimeError, match="single memory location"):
+        torch_ops._no_overlap(x[0], x[0, 1:3])         # dense views over shared bytes
+    torch_ops._no_overlap(x[0], x[1])                  # disjoint halves
+    torch_ops._no_overlap(x[:, 1:], x[:, 0])           # rows of one tensor (the rescale_ call)
+    torch_ops._no_overlap(x, torch.zeros(3))
