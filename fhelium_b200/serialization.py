@@ -262,7 +262,8 @@ def load_value(path: str | os.PathLike, *, device: torch.device | str = "cpu", e
         if ids != list(range(vm["level"], vm["level"] + len(ids))):
             raise ValueError("Ciphertext prime_ids must run contiguously from its level")
         return Ciphertext(data, vm["level"], float(vm["scale"]), vm["polynomial_domain"],
-                          vm["residue_representation"], vm["modulus_basis"])
+                          vm["residue_representation"], vm["modulus_basis"], context_id=m.get("context_id"),
+                          prime_ids=tuple(ids))
     if ids != list(range(len(ids))):
         raise ValueError(f"{vtype} prime_ids must be the level-zero rows 0..{len(ids) - 1}")
     if vm["polynomial_domain"] != "ntt" or vm["residue_representation"] != "montgomery":

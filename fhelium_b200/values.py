@@ -18,16 +18,95 @@ import torch
 
 @dataclass
 class Ciphertext:
+    """A CKKS ciphertext (or dense batch) in one state (fhelium/core/ciphertext.py:26-384).
+    prime_ids default to the level's contiguous rows (level, level + 1, ...)."""
+
     data: torch.Tensor
     level: int
     scale: float
     polynomial_domain: str = "coefficient"  # "coefficient" | "ntt"
     residue_representation: str = "standard"  # "standard" | "montgomery"
     modulus_basis: str = "Q"
+    context_id: str | None = None
+    prime_ids: tuple = ()
 
     def __post_init__(self):
         if self.data.ndim < 3 or self.data.size(0) not in (2, 3):
             raise ValueError("Ciphertext data must be [component(2|3), *batch, limb, N]")
+        if self.polynomial_domain not in ("coefficient", "ntt"):
+            raise ValueError(f"unsupported polynomial_domain {self.polynomial_domain!r}")
+        if self.residue_representation not in ("standard", "montgomery"):
+            raise ValueError(f"unsupported residue_representation {self.residue_representation!r}")
+        if self.prime_ids:
+            self.prime_ids = tuple(int(i) for i in self.prime_ids)
+            if len(self.prime_ids) != self.data.size(-2):
+                raise ValueError("prime_ids must name every limb row")
+
+    @property
+    def limb_ids(self) -> tuple:
+        return self.prime_ids or tuple(range(self.level, self.level + self.data.size(-2)))
+
+    @property
+    def ring_dimension(self) -> int:
+        return self.data.size(-1)
+
+    @property
+    def is_batched(self) -> bool:
+        return self.data.ndim > 3
+
+    @property
+    def is_ntt_domain(self) -> bool:
+        return self.polynomial_domain == "ntt"
+
+    @property
+    def is_coefficient_domain(self) -> bool:
+        return self.polynomial_domain == "coefficient"
+
+    @property
+    def includes_p(self) -> bool:
+        return self.modulus_basis == "QP"
+
+    def with_data(self, data: torch.Tensor) -> "Ciphertext":
+        """The same state over another tensor of the same layout (no copy)."""
+        if data.ndim != self.data.ndim or data.shape[0] != self.data.shape[0] or data.shape[-2:] != self.data.shape[-2:]:
+            raise ValueError("with_data needs the same component, limb and coefficient extents")
+        return replace(self, data=data)
+
+    def slice_limbs(self, start: int, stop: int) -> "Ciphertext":
+        """A view of limb rows [start, stop) (fhelium/core/ciphertext.py:252-276)."""
+        ids = self.limb_ids[start:stop]
+        return replace(self, data=self.data[..., start:stop, :], level=ids[0] if ids else self.level,
+                       prime_ids=tuple(ids) if self.prime_ids else ())
+
+    def select_batch(self, index: int, *, dim: int = 0) -> "Ciphertext":
+        """A storage-sharing view of one batch item along batch axis `dim`."""
+        if not self.is_batched:
+            raise ValueError("select_batch requires a batched ciphertext")
+        return replace(self, data=self.data.select(dim + 1, index))
+
+    def unbind_batch(self, *, dim: int = 0) -> tuple:
+        return tuple(self.select_batch(i, dim=dim) for i in range(self.data.size(dim + 1)))
+
+    @classmethod
+    def stack_batch(cls, values, *, dim: int = 0) -> "Ciphertext":
+        """Stack ciphertexts of one state into a new batch axis `dim`."""
+        values = list(values)
+        if not values:
+            raise ValueError("stack_batch needs at least one ciphertext")
+        first = values[0]
+        for v in values[1:]:
+            if (v.level, v.scale, v.polynomial_domain, v.residue_representation, v.modulus_basis) != \
+                    (first.level, first.scale, first.polynomial_domain, first.residue_representation,
+                     first.modulus_basis):
+                raise ValueError("stack_batch needs ciphertexts of one level, scale and state")
+        return replace(first, data=torch.stack([v.data for v in values], dim=dim + 1))
+
+    def replace_(self, other: "Ciphertext") -> "Ciphertext":
+        """Take other's tensor and state in place (fhelium/core/ciphertext.py:358-373)."""
+        self.data, self.level, self.scale = other.data, other.level, other.scale
+        self.polynomial_domain, self.residue_representation = other.polynomial_domain, other.residue_representation
+        self.modulus_basis, self.prime_ids = other.modulus_basis, other.prime_ids
+        return self
 
     @property
     def component_count(self) -> int:

@@ -132,3 +132,24 @@ def test_compressed_plaintext_round_trip(layout):
     broken.data[0, 0, 5] += 1
     with pytest.raises(ValueError, match="not exactly representable"):
         CompressedPlaintext.from_plaintext(broken, unique_count=8, compression_layout=layout)
+
+
+def test_ciphertext_batch_and_limb_helpers():
+    """Ciphertext.select_batch / unbind_batch / stack_batch / slice_limbs /
+    with_data / replace_ (fhelium/core/ciphertext.py:221-373)."""
+    data = torch.arange(2 * 3 * 4 * 8, dtype=torch.int64).reshape(2, 3, 4, 8)
+    ct = Ciphertext(data, 2, 4.0, "ntt", "montgomery")
+    assert ct.is_batched and ct.is_ntt_domain and not ct.includes_p and ct.ring_dimension == 8
+    assert ct.limb_ids == (2, 3, 4, 5)
+    items = ct.unbind_batch()
+    assert len(items) == 3 and torch.equal(items[1].data, data[:, 1])
+    again = Ciphertext.stack_batch(items)
+    assert torch.equal(again.data, data) and again.level == 2
+    part = ct.slice_limbs(1, 3)
+    assert part.level == 3 and torch.equal(part.data, data[..., 1:3, :])
+    other = ct.with_data(data + 1)
+    assert torch.equal(other.data, data + 1) and other.scale == 4.0
+    target = Ciphertext(torch.zeros(2, 4, 8, dtype=torch.int64), 0, 1.0)
+    assert target.replace_(items[0]) is target and target.level == 2 and target.is_ntt_domain
+    with pytest.raises(ValueError):
+        Ciphertext(data, 0, 1.0, "frequency")
