@@ -405,7 +405,10 @@ class CkksEngine:
     # rotations (fhelium/engine/ckks_engine.py:2183-2300, 3726-3897)
     # ------------------------------------------------------------------
     def _canonical_step(self, step: int) -> int:
-        return int(step) % self.num_slots
+        """The reference's canonical rotation step: step mod N/2 mapped to
+        [-N/4, N/4) (fhelium/core/keys.py:339-351)."""
+        s = self.num_slots
+        return (int(step) + s // 2) % s - s // 2
 
     def galois_element_for_step(self, step: int) -> int:
         return galois_element(self.n, self._canonical_step(step) % self.n, self.galois_generator)

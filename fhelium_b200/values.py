@@ -373,7 +373,18 @@ class RotationKey(KeySwitchKey):
 
 @dataclass
 class RotationKeySet:
+    """Rotation keys by canonical step (fhelium/core/keys.py:396-460)."""
+
     keys: dict = field(default_factory=dict)
+
+    @staticmethod
+    def canonical(step: int, ring_dimension: int) -> int:
+        s = ring_dimension // 2
+        return (int(step) + s // 2) % s - s // 2
+
+    @property
+    def table(self) -> dict:
+        return self.keys
 
     def __contains__(self, step: int) -> bool:
         return step in self.keys
@@ -382,10 +393,94 @@ class RotationKeySet:
         return self.keys[step]
 
     def __setitem__(self, step: int, key: RotationKey) -> None:
+        if not isinstance(key, RotationKey):
+            raise TypeError(f"RotationKeySet values must be RotationKey objects, got {type(key).__name__}")
         self.keys[step] = key
+
+    def __delitem__(self, step: int) -> None:
+        del self.keys[step]
+
+    def __iter__(self):
+        return iter(self.keys)
 
     def __len__(self) -> int:
         return len(self.keys)
 
+    def values(self):
+        return self.keys.values()
+
+    def items(self):
+        return self.keys.items()
+
+    def add(self, key: RotationKey) -> "RotationKeySet":
+        """Install a key under its own canonical rotation step."""
+        self[self.canonical(key.rotation_step, key.data.size(-1))] = key
+        return self
+
     def steps(self) -> list[int]:
         return sorted(self.keys)
+
+
+@dataclass(frozen=True)
+class EvaluationKeyRequirements:
+    """Key roles and rotations one evaluation needs (fhelium/core/keys.py:462-495)."""
+
+    rotation_steps: frozenset = frozenset()
+    requires_relinearization: bool = False
+    requires_conjugation: bool = False
+
+    def __post_init__(self):
+        steps = frozenset(int(s) for s in self.rotation_steps if int(s) != 0)
+        object.__setattr__(self, "rotation_steps", steps)
+
+
+@dataclass
+class EvaluationKeySet:
+    """The evaluator's keys: rotations, relinearisation, conjugation
+    (fhelium/core/keys.py:497-640); no public or secret key."""
+
+    rotations: RotationKeySet = field(default_factory=RotationKeySet)
+    relinearization: RelinearizationKey | None = None
+    conjugation: RotationKey | None = None
+
+    def __post_init__(self):
+        self.validate()
+
+    def validate(self) -> "EvaluationKeySet":
+        if not isinstance(self.rotations, RotationKeySet):
+            raise TypeError("EvaluationKeySet rotations must be a RotationKeySet")
+        if self.relinearization is not None and not isinstance(self.relinearization, RelinearizationKey):
+            raise TypeError("EvaluationKeySet relinearization must be a RelinearizationKey or None")
+        if self.conjugation is not None and not isinstance(self.conjugation, RotationKey):
+            raise TypeError("EvaluationKeySet conjugation must be a conjugation (Galois 2N - 1) key or None")
+        keys = list(self.rotations.values()) + [k for k in (self.relinearization, self.conjugation) if k is not None]
+        for step, key in self.rotations.items():
+            if RotationKeySet.canonical(key.rotation_step, key.data.size(-1)) != step:
+                raise ValueError(f"EvaluationKeySet rotation mapping does not match its key: "
+                                 f"mapping={step!r}, key={key.rotation_step!r}")
+        if keys:
+            shape = lambda k: (tuple(k.data.shape), k.data.dtype, k.data.device)
+            first = shape(keys[0])
+            if any(shape(k) != first for k in keys[1:]):
+                raise ValueError("EvaluationKeySet members differ in layout, dtype or device")
+        return self
+
+    def require(self, requirements: EvaluationKeyRequirements) -> "EvaluationKeySet":
+        """Raise ValueError naming the first capability that is missing."""
+        if not isinstance(requirements, EvaluationKeyRequirements):
+            raise TypeError("requirements must be an EvaluationKeyRequirements")
+        self.validate()
+        if requirements.rotation_steps:
+            if len(self.rotations):
+                n = next(iter(self.rotations.values())).data.size(-1)
+                need = {RotationKeySet.canonical(s, n) for s in requirements.rotation_steps}
+            else:
+                need = set(requirements.rotation_steps)
+            missing = sorted(need - set(self.rotations))
+            if missing:
+                raise ValueError(f"EvaluationKeySet is missing rotation steps: {missing}")
+        if requirements.requires_relinearization and self.relinearization is None:
+            raise ValueError("EvaluationKeySet is missing a relinearization key")
+        if requirements.requires_conjugation and self.conjugation is None:
+            raise ValueError("EvaluationKeySet is missing a conjugation key")
+        return self

@@ -153,3 +153,26 @@ def test_ciphertext_batch_and_limb_helpers():
     assert target.replace_(items[0]) is target and target.level == 2 and target.is_ntt_domain
     with pytest.raises(ValueError):
         Ciphertext(data, 0, 1.0, "frequency")
+
+
+def test_rotation_steps_and_evaluation_key_sets():
+    """Signed canonical rotation steps and key inventories as the reference
+    defines them (fhelium/core/keys.py:339-351, 396-640)."""
+    from fhelium_b200.values import EvaluationKeyRequirements, EvaluationKeySet, RelinearizationKey, RotationKeySet
+    n = 64                                          # 32 slots: canonical steps in [-16, 16)
+    assert [RotationKeySet.canonical(s, n) for s in (1, -1, 31, 16, -16, 32, 17)] == [1, -1, -1, -16, -16, 0, -15]
+    key = lambda step: RotationKey(torch.zeros(2, 2, 3, n, dtype=torch.int64), rotation_step=step, galois_element=3)
+    rs = RotationKeySet().add(key(1)).add(key(-1))
+    assert sorted(rs) == [-1, 1] and len(rs) == 2
+    with pytest.raises(TypeError):
+        rs[2] = "not a key"
+    ks = EvaluationKeySet(rotations=rs, relinearization=RelinearizationKey(torch.zeros(2, 2, 3, n, dtype=torch.int64)))
+    ks.require(EvaluationKeyRequirements(rotation_steps={1, 31, 0}, requires_relinearization=True))
+    with pytest.raises(ValueError, match="missing rotation steps: \\[2\\]"):
+        ks.require(EvaluationKeyRequirements(rotation_steps={2}))
+    with pytest.raises(ValueError, match="conjugation"):
+        ks.require(EvaluationKeyRequirements(requires_conjugation=True))
+    bad = RotationKeySet()
+    bad.keys[5] = key(1)                            # mapping and key disagree
+    with pytest.raises(ValueError, match="does not match"):
+        EvaluationKeySet(rotations=bad)
