@@ -10,8 +10,8 @@ path: constructing an engine without CUDA or without the library raises.
 Randomness: the reference draws from the external `triton_csprng` package.
 This engine draws from a seeded torch generator on the device instead
 (uniform residues, uniform ternary secrets, rounded Gaussians with
-sigma = config.sigma), and encode rounds to nearest rather than
-stochastically.  Everything after encryption is a deterministic function of
+sigma = config.sigma, and the uniforms of encode's unbiased stochastic
+rounding; encode_rounding="nearest" rounds deterministically instead).  Everything after encryption is a deterministic function of
 the keys and ciphertexts and matches the reference bit for bit.
 """
 
@@ -39,7 +39,8 @@ def galois_element(n: int, step: int, generator: int = 3) -> int:
 class CkksEngine:
     def __init__(self, ckks_config: CkksConfig | Preset | dict | str | None = None, *,
                  device: torch.device | str | None = None, allow_sk_gen: bool = True,
-                 galois_generator: int = 3, rng_seed: int | None = None, ntt_backend: str | None = None):
+                 galois_generator: int = 3, rng_seed: int | None = None, ntt_backend: str | None = None,
+                 encode_rounding: str = "stochastic"):
         if ckks_config is None:
             ckks_config = Preset.slots16384_scale40_levels16_int64
         if isinstance(ckks_config, (Preset, str, dict)):
@@ -56,6 +57,9 @@ class CkksEngine:
             device = torch.device("cuda", torch.cuda.current_device())
         self.device = device
         self.galois_generator = galois_generator
+        if encode_rounding not in ("stochastic", "nearest"):
+            raise ValueError("encode_rounding must be 'stochastic' or 'nearest'")
+        self.encode_rounding = encode_rounding
         self.allow_sk_gen = allow_sk_gen
         self.ntt_backend = ntt_backend or "b200_cluster_radix16"
         cfg = self.config
@@ -674,7 +678,12 @@ class CkksEngine:
         coeffs = encode_real_coefficients(m.to(self.device), self.n, self.galois_generator) * float(scale)
         if coeffs.abs().max().item() >= 2.0 ** 62:
             raise ValueError("encoded coefficients exceed the int64 range; lower the scale")
-        return torch.round(coeffs).to(torch.int64)
+        if self.encode_rounding == "nearest":
+            return torch.round(coeffs).to(torch.int64)
+        # unbiased stochastic rounding, E[SRound(x)] = x (fhelium/engine/slot_embedding.py:100)
+        low = torch.floor(coeffs)
+        u = torch.rand(coeffs.shape, generator=self._gen, device=coeffs.device, dtype=coeffs.dtype)
+        return (low + (u < coeffs - low).to(coeffs.dtype)).to(torch.int64)
 
     def encrypt_message(self, message, public_key: PublicKey | None = None, *, level: int = 0,
                         scale: float | None = None) -> Ciphertext:

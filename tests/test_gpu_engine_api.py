@@ -221,3 +221,22 @@ def test_compressed_plaintexts(engine, layout):
             assert got.scale == want.scale == cn.scale * 2.0 ** 20
             qq = q[:, None]
             assert torch.equal(got.data.to(torch.int64) % qq, want.data.to(torch.int64) % qq)
+
+
+def test_encode_rounding_is_unbiased_and_bounded(engine):
+    """Stochastic rounding (the reference's SRound): every coefficient is the
+    floor or the ceiling of the exact scaled value, and the mean error over
+    many draws is near zero; "nearest" rounds deterministically."""
+    x = _msg(engine, 1, 60)
+    exact = engine.encode(x, scale=2.0 ** 20, level=0)   # one draw
+    from fhelium_b200.encoding import encode_real_coefficients
+    ref = encode_real_coefficients(x.to(engine.device), engine.n, engine.galois_generator) * 2.0 ** 20
+    d = exact.data.to(torch.float64) - ref
+    assert float(d.abs().max()) < 1.0 + 1e-6
+    draws = torch.stack([engine.encode(x, scale=2.0 ** 20).data.to(torch.float64) - ref for _ in range(64)])
+    assert abs(float(draws.mean())) < 0.01                 # unbiased
+    assert float(draws.std()) > 0.2                         # genuinely random, not nearest
+    nearest = CkksEngine(Preset.slots8192_scale40_levels7_int64, rng_seed=3, encode_rounding="nearest")
+    a = nearest.encode(x, scale=2.0 ** 20).data
+    assert torch.equal(a, nearest.encode(x, scale=2.0 ** 20).data)
+    assert float((a.to(torch.float64) - ref).abs().max()) <= 0.5 + 1e-6
