@@ -39,8 +39,8 @@ def galois_element(n: int, step: int, generator: int = 3) -> int:
 class CkksEngine:
     def __init__(self, ckks_config: CkksConfig | Preset | dict | str | None = None, *,
                  device: torch.device | str | None = None, allow_sk_gen: bool = True,
-                 galois_generator: int = 3, rng_seed: int | None = None, ntt_backend: str | None = None,
-                 encode_rounding: str = "stochastic"):
+                 galois_generator: int = 3, ntt_backend: str | None = None, rng_seed: int | None = None,
+                 rng_nonce: int | None = None, encode_rounding: str = "stochastic"):
         if ckks_config is None:
             ckks_config = Preset.slots16384_scale40_levels16_int64
         if isinstance(ckks_config, (Preset, str, dict)):
@@ -72,7 +72,11 @@ class CkksEngine:
         self.ctx = nat.NativeContext(64 if cfg.buffer_bit_length == 62 else 32, cfg.logN, cfg.moduli,
                                      self.num_q, self.num_p, device)
         self._gen = torch.Generator(device=device)
-        self._gen.manual_seed(0 if rng_seed is None else int(rng_seed))
+        # (seed, nonce) -> one 63-bit generator seed; nonce None keeps the seed as given
+        seed = 0 if rng_seed is None else int(rng_seed)
+        if rng_nonce is not None:
+            seed = (seed * 0x9E3779B97F4A7C15 + int(rng_nonce) + 1) % (1 << 63)
+        self._gen.manual_seed(seed)
         self._secret_key: SecretKey | None = None
         self._public_key: PublicKey | None = None
         self._relinearization_key: RelinearizationKey | None = None
