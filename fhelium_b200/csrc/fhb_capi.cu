@@ -129,9 +129,17 @@ int modup(const Context& c, const void* comp, void* digits, int64_t batch, int l
           cudaStream_t st, const uint32_t* item_galois = nullptr) {
   const int limbs = c.num_q - level;
   const uint32_t ginv = galois == 1 ? 0u : galois_inverse(galois, c.log_n);
-  k_modup_digits<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
-      (const T*)comp, (T*)digits, batch, limbs, c.log_n, level, ginv, item_galois, tables<T>(c),
-      level_tables<T>(c, level));
+  const LevelTables<T> lt = level_tables<T>(c, level);
+  if (batch == 0 || lt.num_digits == 0) return 0;
+  constexpr int V = 16 / sizeof(T);
+  const bool vec = aligned16(comp) && aligned16(digits);
+  const dim3 g = row_grid(c.n(), vec ? V : 1, lt.num_digits, batch);
+  if (vec)
+    k_modup_digits<T, V><<<g, kEwThreads, 0, st>>>((const T*)comp, (T*)digits, batch, limbs, c.log_n, level, ginv,
+                                                  item_galois, tables<T>(c), lt);
+  else
+    k_modup_digits<T, 1><<<g, kEwThreads, 0, st>>>((const T*)comp, (T*)digits, batch, limbs, c.log_n, level, ginv,
+                                                  item_galois, tables<T>(c), lt);
   return cuda_status(cudaGetLastError(), "k_modup_digits");
 }
 

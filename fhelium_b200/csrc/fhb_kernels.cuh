@@ -272,44 +272,54 @@ __device__ __forceinline__ int galois_ntt_source(int k, int log_n, uint32_t g) {
 // coefficient/standard (canonical or lazy [0, 2q)); digits: [B, L, N],
 // row r holds the mixed-radix digit of the prime in row r.  When ginv != 0
 // the input is first mapped through sigma_g (rotation).
-template <typename T>
+template <typename T, int V>
 __global__ void k_modup_digits(const T* __restrict__ comp, T* __restrict__ digits, int64_t batch,
                                int limbs, int log_n, int level, uint32_t ginv,
                                const uint32_t* __restrict__ item_galois, ChainTables<T> tabs, LevelTables<T> lt) {
+  // grid: (N / (256 V), digit, z-slices of the batch); V coefficients per thread
   const int64_t n = int64_t(1) << log_n;
-  const int64_t total = batch * n;
+  const int64_t k0 = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
+  if (k0 >= n) return;
   using W = Word<T>;
-  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
-       idx += int64_t(gridDim.x) * blockDim.x) {
-    const int64_t bi = idx >> log_n;
-    const int k = int(idx & (n - 1));
-    bool neg = false;
+  const DigitDesc d = lt.digits[blockIdx.y];
+  const TwPair<T>* g = lt.garner + blockIdx.y * kMaxDigitWidth * kMaxDigitWidth;
+  for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
     // per-item Galois elements (mixed-step rotation batches) override ginv
     const uint32_t gi = item_galois ? (item_galois[bi] == 1 ? 0u : galois_inverse_dev(item_galois[bi], log_n)) : ginv;
-    const int srck = gi ? galois_source(k, log_n, gi, neg) : k;
     const T* src = comp + bi * limbs * n;
     T* dst = digits + bi * limbs * n;
-    for (int a = 0; a < lt.num_digits; ++a) {
-      const DigitDesc d = lt.digits[a];
-      const TwPair<T>* g = lt.garner + a * kMaxDigitWidth * kMaxDigitWidth;
-      T dig[kMaxDigitWidth];
-      for (int r = 0; r < d.alpha; ++r) {
-        const int row = d.prime0 - level + r;
-        const PrimeInfo<T> p = tabs.prime[d.prime0 + r];
-        T x = csub(src[row * n + srck], p.q);
-        if (neg && x) x = p.q - x;
-        T acc = 0;
-        for (int i = 0; i < r; ++i) {
-          const TwPair<T> c = g[r * kMaxDigitWidth + i];
-          acc = csub(acc + csub(W::shoup(dig[i], c.w, c.wp, p.q), p.q), p.q);
+    EwVec<T, V> dig[kMaxDigitWidth];
+    for (int r = 0; r < d.alpha; ++r) {
+      const int row = d.prime0 - level + r;
+      const T q = tabs.prime[d.prime0 + r].q;
+      EwVec<T, V> x;
+      if (gi == 0) {
+        x = ew_load<T, V>(src + row * n + k0);
+#pragma unroll
+        for (int e = 0; e < V; ++e) x.v[e] = csub(x.v[e], q);
+      } else {
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+          bool neg = false;
+          const int srck = galois_source(int(k0) + e, log_n, gi, neg);
+          T y = csub(src[row * n + srck], q);
+          x.v[e] = (neg && y) ? q - y : y;
         }
-        if (r > 0) {
-          const TwPair<T> inv = g[r * kMaxDigitWidth + r];
-          x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
-        }
-        dig[r] = x;
-        dst[row * n + k] = x;
       }
+      if (r > 0) {
+        const TwPair<T> inv = g[r * kMaxDigitWidth + r];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+          T acc = 0;
+          for (int i = 0; i < r; ++i) {
+            const TwPair<T> c = g[r * kMaxDigitWidth + i];
+            acc = csub(acc + csub(W::shoup(dig[i].v[e], c.w, c.wp, q), q), q);
+          }
+          x.v[e] = csub(W::shoup(csub(x.v[e] + q - acc, q), inv.w, inv.wp, q), q);
+        }
+      }
+      dig[r] = x;
+      ew_store<T, V>(dst + row * n + k0, x);
     }
   }
 }
