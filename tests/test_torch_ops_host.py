@@ -108,3 +108,31 @@ def test_written_tensor_may_not_overlap_read_only_operands(torch_ops):
     torch_ops._no_overlap(x[0], x[1])                  # disjoint halves
     torch_ops._no_overlap(x[:, 1:], x[:, 0])           # rows of one tensor (the rescale_ call)
     torch_ops._no_overlap(x, torch.zeros(3))
+
+
+def test_schedule_checks_raise_the_references_messages(torch_ops):
+    """Malformed indexed-NTT schedules fail with the reference's messages
+    (tests/test_ntt_backend.py:258-297 of the reference); a valid schedule that
+    is not the radix-2 plan is refused by name."""
+    log_n = 6
+    fe, fo, _, ie, io, _ = ref_pipeline._schedule(log_n)
+    torch_ops._check_schedule(fe, fo, log_n, False)
+    torch_ops._check_schedule(ie, io, log_n, True)
+    with pytest.raises(RuntimeError, match=r"log2\(N\) stages"):
+        torch_ops._check_schedule(fe[:-1], fo[:-1], log_n, False)
+    bad = fe.clone()
+    bad[0, 0] = 1 << log_n
+    with pytest.raises(RuntimeError, match="out-of-range coefficient index"):
+        torch_ops._check_schedule(bad, fo, log_n, False)
+    dup = fe.clone()
+    dup[0, 1] = dup[0, 0]
+    with pytest.raises(RuntimeError, match="partition every coefficient"):
+        torch_ops._check_schedule(dup, fo, log_n, False)
+    with pytest.raises(RuntimeError, match="radix-2 indexed schedule only"):
+        torch_ops._check_schedule(fo, fe, log_n, False)     # even/odd swapped: a partition, not the plan
+
+
+def test_ops_refuse_host_tensors(torch_ops):
+    x = torch.zeros(1, 2, 16, dtype=torch.int64)
+    with pytest.raises(RuntimeError, match="CUDA tensor"):
+        torch_ops.montgomery_mul(x, x, torch.zeros(8, 2, dtype=torch.int64))
