@@ -374,6 +374,7 @@ def schema_ops_leg(eng, x, y, kd, stream, steps=5):
         torch.zeros(B, QP, n, dtype=eng.dtype, device=x.device), rnd(B, QP, n)
     inv_md, inv_rs = rnd(P, QP), rnd(L - 1)
     md_out = torch.empty(B, L, n, dtype=eng.dtype, device=x.device)
+    ext_out, ext_coef = torch.empty(B, QP, n, dtype=eng.dtype, device=x.device), rnd(3, QP)
     rs_out = torch.empty(B, L - 1, n, dtype=eng.dtype, device=x.device)
     bits = 64 if eng.dtype == torch.int64 else 32
     P_ = nat.ptr
@@ -389,6 +390,10 @@ def schema_ops_leg(eng, x, y, kd, stream, steps=5):
             lambda: lib.fhb_op_moddown(bits, P_(digit), QP * n, P_(digit[:, L:]), QP * n, P_(md_out), L * n, B, L, P,
                                        n, P_(inv_md), QP, P_(prm), prm.stride(0), s),
             (B * QP + B * L) * n * word),
+        "mixed_radix_basis_extend_to_montgomery": (
+            lambda: lib.fhb_op_basis_extend(bits, P_(x), L * n, 4, P_(ext_out), QP * n, B, QP, n, P_(ext_coef), QP,
+                                            P_(prm), prm.stride(0), s),
+            (B * 4 + B * QP) * n * word),
         "rescale_drop_leading_prime_nearest": (
             lambda: lib.fhb_op_rescale(bits, P_(x[:, 1:]), L * n, P_(x[:, 0]), L * n, P_(rs_out), (L - 1) * n, B,
                                        L - 1, n, P_(inv_rs), P_(prm[:, 1:]), prm.stride(0), eng.moduli[0] // 2, 1, s),

@@ -241,18 +241,24 @@ __global__ void k_op_mixed_radix_decompose(const T* __restrict__ src, int64_t ss
 // Exact basis extension sum_r d_r (M_r mod p_j) into Montgomery form, lazy
 // (csrc/ops/rns/cpu/rns_arithmetic_cpu.cpp:616-700): d_0 R^2 reduced, then
 // each further digit's product added with one 2q correction.
-template <typename T>
+template <typename T, int V>
 __global__ void k_op_basis_extend(const T* __restrict__ digits, int64_t ds, int digit_rows, T* __restrict__ out,
                                   int64_t os, int64_t batch, int64_t n, const T* __restrict__ coeffs,
                                   int64_t coeff_stride, const T* __restrict__ params, int64_t ps) {
-  FHB_OP_INDEX
+  FHB_OP_VINDEX
   const ColumnPrime<T> p = column_prime(params, ps, row);
   for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
     const T* d = digits + bi * ds + k;
-    T v = mont_canonical(d[0], p.r2, p.q, p.neg_inv);
-    for (int r = 1; r < digit_rows; ++r)
-      v = add_lazy2(v, mont_canonical(d[r * n], coeffs[(r - 1) * coeff_stride + row], p.q, p.neg_inv), p.twice_q);
-    out[bi * os + row * n + k] = v;
+    Vec<T, V> v = ldv<T, V>(d);
+#pragma unroll
+    for (int i = 0; i < V; ++i) v.v[i] = mont_canonical(v.v[i], p.r2, p.q, p.neg_inv);
+    for (int r = 1; r < digit_rows; ++r) {
+      const T c = coeffs[(r - 1) * coeff_stride + row];
+      const Vec<T, V> x = ldv<T, V>(d + r * n);
+#pragma unroll
+      for (int i = 0; i < V; ++i) v.v[i] = add_lazy2(v.v[i], mont_canonical(x.v[i], c, p.q, p.neg_inv), p.twice_q);
+    }
+    stv<T, V>(out + bi * os + row * n + k, v);
   }
 }
 
@@ -609,11 +615,19 @@ int fhb_op_basis_extend(int residue_bits, const void* digits, int64_t digits_bat
   if (fhb::empty(batch, destination_rows, n)) return 0;
   FHB_NONNULL(digits) FHB_NONNULL(out) FHB_NONNULL(params)
   if (digit_rows > 1 && !coefficients) return fail(-1, "coefficients is NULL");
-  FHB_DISPATCH(residue_bits,
-               fhb::k_op_basis_extend<T><<<fhb::op_grid(n, destination_rows, batch), fhb::kOpThreads, 0,
-                                           (cudaStream_t)stream>>>(
-                   (const T*)digits, digits_batch_stride, digit_rows, (T*)out, out_batch_stride, batch, n,
-                   (const T*)coefficients, coefficient_row_stride, (const T*)params, param_row_stride))
+  FHB_DISPATCH(residue_bits, {
+    const bool vec = fhb::vec_ok<T>(n, {digits, out}, {digits_batch_stride, out_batch_stride});
+    constexpr int VW = 16 / sizeof(T);
+    const dim3 g = fhb::op_grid_v(n, vec ? VW : 1, destination_rows, batch);
+    if (vec)
+      fhb::k_op_basis_extend<T, VW><<<g, fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
+          (const T*)digits, digits_batch_stride, digit_rows, (T*)out, out_batch_stride, batch, n,
+          (const T*)coefficients, coefficient_row_stride, (const T*)params, param_row_stride);
+    else
+      fhb::k_op_basis_extend<T, 1><<<g, fhb::kOpThreads, 0, (cudaStream_t)stream>>>(
+          (const T*)digits, digits_batch_stride, digit_rows, (T*)out, out_batch_stride, batch, n,
+          (const T*)coefficients, coefficient_row_stride, (const T*)params, param_row_stride);
+  })
   return fhb::launch_status();
 }
 
