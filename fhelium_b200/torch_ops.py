@@ -1,7 +1,8 @@
 """CUDA implementations of the reference's custom-op schemas, served by libfhb200.
 
 The reference reaches its kernels through PyTorch custom ops
-(``torch.ops.fhelium_rns_ops``, ``fhelium_ntt_ops``, ``fhelium_ckks_ops``; schemas
+(``torch.ops.fhelium_rns_ops``, ``fhelium_ntt_ops``, ``fhelium_ckks_ops``, and the tuning
+overrides of ``fhelium_ntt_diagnostic_ops``; schemas
 in csrc/ops/rns/rns_arithmetic.cpp:30-72, rns_canonical_arithmetic.cpp:15-23,
 csrc/ops/ntt/forward_ntt.cpp:25-67, inverse_ntt.cpp:23-73, csrc/ops/ckks/ckks.cpp:29-90)
 with one CPU and one CUDA kernel registered per schema
@@ -116,15 +117,6 @@ SCHEMAS: dict[str, dict[str, str]] = {
                                                                 "compact(Tensor standard_residues, Tensor "
                                                                 "outer_twiddles, Tensor radix_root_powers, "
                                                                 "Tensor rns_params) -> Tensor",
-        "forward_ntt_montgomery_compact_grouped_smem_override_": "forward_ntt_montgomery_compact_grouped_smem_"
-                                                                 "override_(Tensor(a!) montgomery_residues, Tensor "
-                                                                 "forward_twiddles, Tensor rns_params, int "
-                                                                 "grouped_stage_count, int shared_memory_log_n) -> ()",
-        "forward_ntt_montgomery_power_of_two_radix_compact_override_": "forward_ntt_montgomery_power_of_two_radix_"
-                                                                       "compact_override_(Tensor(a!) "
-                                                                       "montgomery_residues, Tensor outer_twiddles, "
-                                                                       "Tensor radix_root_powers, Tensor rns_params, "
-                                                                       "int shared_memory_log_n) -> ()",
         "inverse_ntt_montgomery_power_of_two_radix_compact_": "inverse_ntt_montgomery_power_of_two_radix_compact_("
                                                               "Tensor(a!) montgomery_residues, Tensor outer_twiddles, "
                                                               "Tensor radix_root_powers, Tensor rns_params) -> ()",
@@ -140,11 +132,6 @@ SCHEMAS: dict[str, dict[str, str]] = {
                                                                "Tensor(a!) montgomery_residues, Tensor "
                                                                "outer_twiddles, Tensor radix_root_powers, "
                                                                "Tensor rns_params) -> ()",
-        "inverse_ntt_montgomery_power_of_two_radix_compact_override_": "inverse_ntt_montgomery_power_of_two_radix_"
-                                                                       "compact_override_(Tensor(a!) "
-                                                                       "montgomery_residues, Tensor outer_twiddles, "
-                                                                       "Tensor radix_root_powers, Tensor rns_params, "
-                                                                       "int shared_memory_log_n) -> ()",
         "inverse_ntt_montgomery_indexed_": "inverse_ntt_montgomery_indexed_(Tensor(a!) montgomery_residues, "
                                            "Tensor even_indices, Tensor odd_indices, Tensor inverse_twiddles, "
                                            "Tensor rns_params) -> ()",
@@ -170,6 +157,24 @@ SCHEMAS: dict[str, dict[str, str]] = {
         "inverse_ntt_to_centered_compact_grouped_smem_": "inverse_ntt_to_centered_compact_grouped_smem_(Tensor(a!) "
                                                          "montgomery_residues, Tensor inverse_twiddles, "
                                                          "Tensor rns_params, int grouped_stage_count) -> ()",
+    },
+    # tuning-override forms the reference keeps outside its production ABI
+    # (csrc/ops/ntt/forward_ntt.cpp:68-80, inverse_ntt.cpp)
+    "fhelium_ntt_diagnostic_ops": {
+        "forward_ntt_montgomery_compact_grouped_smem_override_": "forward_ntt_montgomery_compact_grouped_smem_"
+                                                                 "override_(Tensor(a!) montgomery_residues, Tensor "
+                                                                 "forward_twiddles, Tensor rns_params, int "
+                                                                 "grouped_stage_count, int shared_memory_log_n) -> ()",
+        "forward_ntt_montgomery_power_of_two_radix_compact_override_": "forward_ntt_montgomery_power_of_two_radix_"
+                                                                       "compact_override_(Tensor(a!) "
+                                                                       "montgomery_residues, Tensor outer_twiddles, "
+                                                                       "Tensor radix_root_powers, Tensor rns_params, "
+                                                                       "int shared_memory_log_n) -> ()",
+        "inverse_ntt_montgomery_power_of_two_radix_compact_override_": "inverse_ntt_montgomery_power_of_two_radix_"
+                                                                       "compact_override_(Tensor(a!) "
+                                                                       "montgomery_residues, Tensor outer_twiddles, "
+                                                                       "Tensor radix_root_powers, Tensor rns_params, "
+                                                                       "int shared_memory_log_n) -> ()",
     },
     "fhelium_ckks_ops": {
         "add_prepared_plaintext_component": "add_prepared_plaintext_component(Tensor ciphertext_component, "
@@ -1066,13 +1071,10 @@ IMPLS = {
         "forward_ntt_montgomery_power_of_two_radix_compact_": _fwd_radix_(1),
         "forward_ntt_to_montgomery_power_of_two_radix_compact_": _fwd_radix_(0),
         "forward_ntt_to_montgomery_power_of_two_radix_compact": forward_ntt_to_montgomery_power_of_two_radix_compact,
-        "forward_ntt_montgomery_compact_grouped_smem_override_": forward_ntt_montgomery_compact_grouped_smem_override_,
-        "forward_ntt_montgomery_power_of_two_radix_compact_override_": _fwd_radix_(1),
         "inverse_ntt_montgomery_power_of_two_radix_compact_": _inv_radix_(_native.INV_MONTGOMERY),
         "inverse_ntt_to_standard_lazy_power_of_two_radix_compact_": _inv_radix_(_native.INV_STANDARD_LAZY),
         "inverse_ntt_to_standard_power_of_two_radix_compact_": _inv_radix_(_native.INV_STANDARD),
         "inverse_ntt_to_centered_power_of_two_radix_compact_": _inv_radix_(_native.INV_CENTERED),
-        "inverse_ntt_montgomery_power_of_two_radix_compact_override_": _inv_radix_(_native.INV_MONTGOMERY),
         "inverse_ntt_montgomery_indexed_": _inv_indexed_(_native.INV_MONTGOMERY),
         "inverse_ntt_to_standard_lazy_indexed_": _inv_indexed_(_native.INV_STANDARD_LAZY),
         "inverse_ntt_to_standard_indexed_": _inv_indexed_(_native.INV_STANDARD),
@@ -1081,6 +1083,11 @@ IMPLS = {
         "inverse_ntt_to_standard_lazy_compact_grouped_smem_": _inv_compact_(_native.INV_STANDARD_LAZY),
         "inverse_ntt_to_standard_compact_grouped_smem_": _inv_compact_(_native.INV_STANDARD),
         "inverse_ntt_to_centered_compact_grouped_smem_": _inv_compact_(_native.INV_CENTERED),
+    },
+    "fhelium_ntt_diagnostic_ops": {
+        "forward_ntt_montgomery_compact_grouped_smem_override_": forward_ntt_montgomery_compact_grouped_smem_override_,
+        "forward_ntt_montgomery_power_of_two_radix_compact_override_": _fwd_radix_(1),
+        "inverse_ntt_montgomery_power_of_two_radix_compact_override_": _inv_radix_(_native.INV_MONTGOMERY),
     },
     "fhelium_ckks_ops": {
         "add_prepared_plaintext_component": _plaintext_op(0, False),

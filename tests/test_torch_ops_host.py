@@ -28,7 +28,7 @@ def torch_ops():
 
 def test_every_served_schema_has_a_cuda_kernel(torch_ops):
     served = torch_ops.served()
-    assert len(served) == 61   # every schema of fhelium_{rns,ntt,ckks}_ops
+    assert len(served) == 61   # 58 of fhelium_{rns,ntt,ckks}_ops + 3 of fhelium_ntt_diagnostic_ops
     for qualname in served:
         assert torch._C._dispatch_has_kernel_for_dispatch_key(qualname, "CUDA"), qualname
     torch_ops.register()   # idempotent
@@ -37,6 +37,15 @@ def test_every_served_schema_has_a_cuda_kernel(torch_ops):
 def test_schemas_are_the_references(torch_ops):
     if not ref_pipeline.available():
         pytest.skip("reference operator library not built")
+    # the served names of each namespace are exactly the reference's: a name
+    # registered under the wrong namespace would appear here as an extra one
+    registered = {}
+    for qualname in torch._C._dispatch_get_all_op_names():
+        ns, _, name = qualname.partition("::")
+        if ns in torch_ops.SCHEMAS:
+            registered.setdefault(ns, set()).add(name)
+    for ns, ops in torch_ops.SCHEMAS.items():
+        assert registered.get(ns) == set(ops), (ns, registered.get(ns, set()) ^ set(ops))
     for ns, ops in torch_ops.SCHEMAS.items():
         for name, schema in ops.items():
             got = str(torch._C._dispatch_find_schema_or_throw(f"{ns}::{name}", "").schema())
