@@ -240,3 +240,28 @@ def test_encode_rounding_is_unbiased_and_bounded(engine):
     a = nearest.encode(x, scale=2.0 ** 20).data
     assert torch.equal(a, nearest.encode(x, scale=2.0 ** 20).data)
     assert float((a.to(torch.float64) - ref).abs().max()) <= 0.5 + 1e-6
+
+
+@pytest.mark.parametrize("level", [0, 2])
+def test_decryption_error_distribution(engine, level):
+    """The reference's statistical noise bound (tests/test_ckks_operation_correctness.py:135-169,
+    349-397): RMS error < 6 N / scale and a 99th-percentile error below
+    factor x N / scale (encrypt 12, rotate 12, rescale 1.25)."""
+    unit = engine.n / engine.config.default_scale
+
+    def check(ct, want, factor):
+        err = (engine.decrypt_message(ct) - want.to(torch.complex128)).abs()
+        assert torch.all(torch.isfinite(err))
+        rms = float(err.square().mean().sqrt())
+        p99 = float(torch.quantile(err.flatten(), 0.99))
+        assert rms < 6.0 * unit, (rms, 6.0 * unit)
+        assert p99 < factor * unit, (p99, factor * unit)
+
+    x, y = _msg(engine, 2, 70 + level), _msg(engine, 2, 80 + level)
+    cx = engine.encrypt_message(x, level=level)
+    check(cx, x, 12.0)
+    check(engine.rotate_by_step(cx, 1), torch.roll(x, 1, dims=-1), 12.0)
+    cy = engine.encrypt_message(y, level=level)
+    prod = engine.multiply_relinearize_rescale(engine.coefficient_domain_to_ntt_domain(cx),
+                                               engine.coefficient_domain_to_ntt_domain(cy))
+    check(prod, x * y, 1.25)
