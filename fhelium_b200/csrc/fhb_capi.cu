@@ -1,4 +1,5 @@
 // extern "C" entry points of libfhb200.so (declared in include/fhb200.h).
+#include <cstdint>
 #include <cstdio>
 #include <string>
 
@@ -605,7 +606,20 @@ int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, 
   const Context& c = *ctx->impl;
   if (level < 0 || level >= c.num_q || batch < 0) return -1;
   const int64_t l = c.num_q - level, lp = l + c.num_p;
-  return (3 * l + l + 2 * lp) * batch * c.n() * fhb::word_bytes(c);
+  const int64_t per_ct = (3 * l + l + 2 * lp) * c.n() * fhb::word_bytes(c);
+  if (batch > INT64_MAX / per_ct) return -1;  // the size does not fit in 64 bits
+  return per_ct * batch;
+}
+
+// Scratch check shared by the entry points that take a caller scratch buffer:
+// a negative batch, an invalid level or a size that overflows is an invalid
+// argument, not a small buffer.
+static int check_scratch(const fhb_context* ctx, int64_t batch, int level, int64_t scratch_bytes) {
+  if (batch < 0) return fail(-2, "batch must be >= 0");
+  const int64_t need = fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level);
+  if (need < 0) return fail(-4, "invalid level, or the scratch size of this batch overflows 64 bits");
+  if (scratch_bytes < need) return fail(-8, "scratch too small");
+  return 0;
 }
 
 static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* key, const void* add0,
@@ -633,7 +647,7 @@ int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* ke
   TRY(fhb::check_ptr(out, "out"));
   TRY(fhb::check_ptr(scratch, "scratch"));
   TRY(fhb::check_level(c, level));
-  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  TRY(check_scratch(ctx, batch, level, scratch_bytes));
   if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
   const int limbs = c.num_q - level;
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
@@ -653,7 +667,7 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   TRY(fhb::check_ptr(out, "out"));
   TRY(fhb::check_ptr(scratch, "scratch"));
   TRY(fhb::check_level(c, level));
-  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  TRY(check_scratch(ctx, batch, level, scratch_bytes));
   if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
   const int limbs = c.num_q - level;
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
@@ -705,7 +719,7 @@ int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t
   TRY(fhb::check_ptr(scratch, "scratch"));
   if (!key_ptrs || !galois) return fail(-2, "key_ptrs and galois must be device arrays of batch entries");
   TRY(fhb::check_level(c, level));
-  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  TRY(check_scratch(ctx, batch, level, scratch_bytes));
   const int limbs = c.num_q - level;
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
@@ -723,7 +737,7 @@ int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, voi
   TRY(fhb::check_ptr(scratch, "scratch"));
   TRY(fhb::check_level(c, level));
   TRY(fhb::check_galois(c, galois));
-  if (scratch_bytes < fhb_ckks_keyswitch_scratch_bytes(ctx, batch, level)) return fail(-8, "scratch too small");
+  TRY(check_scratch(ctx, batch, level, scratch_bytes));
   const int limbs = c.num_q - level;
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);

@@ -793,8 +793,10 @@ class CkksEngine:
         return Plaintext(message=msg, level=level, scale=self._scale_arg(scale))
 
     def encode(self, message, *, level: int = 0, scale=None) -> Plaintext:
-        """Slots -> exact integer coefficients [*batch, N] at `scale`
-        (rounded to nearest; the reference rounds stochastically)."""
+        """Slots -> exact integer coefficients [*batch, N] at `scale`, rounded
+        by the engine's `encode_rounding`: unbiased stochastic rounding by
+        default, as the reference rounds (fhelium/engine/slot_embedding.py:100),
+        or to nearest."""
         if isinstance(message, Plaintext):
             return self._integer_plaintext(message)
         level = self._public_level(level)

@@ -273,10 +273,17 @@ int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* ke
  * that is handed only its input and output buffers, e.g. a plugin inside a
  * host framework whose memory pool owns all device memory, or a serving loop
  * that must not allocate.  Batches needing more than the fixed size
- * (fhb_ckks_keyswitch_scratch_bytes) are rejected with an error.  The first
- * call on a device looks the array's address up (cudaGetSymbolAddress) and
- * should come before any stream capture.  All calls share the array: calls
- * that can overlap on the GPU (other streams, other host threads) race. */
+ * (fhb_ckks_keyswitch_scratch_bytes) are rejected with an error, and so are a
+ * negative batch and an invalid level.  Usable range: the largest batch is
+ * 32 MiB / fhb_ckks_keyswitch_scratch_bytes(ctx, 1, level), e.g. 5 at level 0
+ * of slots8192_scale40_levels7_int64, 1 at level 0 of
+ * slots16384_scale40_levels16_int64, none below level 26 of
+ * slots32768_scale40_levels34_int64 (1 from level 26 on).  The first call on
+ * a device looks the array's address up (cudaGetSymbolAddress) and should
+ * come before any stream capture; the address is kept for the life of the
+ * process, so do not use this entry point across a cudaDeviceReset.  All
+ * calls share the array: calls that can overlap on the GPU (other streams,
+ * other host threads) race. */
 int fhb_ckks_relinearize_noalloc(const fhb_context* ctx, const void* ct3, const void* key, void* out, int64_t batch,
                                  int level, int rescale, fhb_stream stream);
 int64_t fhb_ckks_relinearize_noalloc_max_scratch_bytes(void);

@@ -4,9 +4,10 @@ The CKKS preset moduli must be the very same primes the reference selects, so
 the catalog is data shared with the reference, not something re-derived here.
 This script reads the reference's two safetensors resources
 (``fhelium/config/resources/{scale,message}_primes_v1.safetensors``) and
-writes them as plain JSON keyed ``"<bits>:<ring_dimension>"``.  It is run
-once, in a checkout that has the reference sources; the package only reads
-the JSON.
+writes them as plain JSON keyed ``"<bits>:<ring_dimension>"`` into the
+package's data folder (``fhelium_b200/data/prime_catalog_v1.json``).  It is
+run once, in a checkout that has the reference sources; the package only
+reads the JSON and does not ship this script.
 """
 
 from __future__ import annotations
@@ -19,6 +20,7 @@ from safetensors import safe_open
 
 REFERENCE = os.environ.get("FHELIUM_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
+DATA = os.path.join(os.path.dirname(os.path.dirname(HERE)), "fhelium_b200", "data")
 
 
 def _table(name: str) -> dict:
@@ -39,7 +41,7 @@ def main() -> int:
         "scale": _table("scale_primes_v1.safetensors"),
         "message": _table("message_primes_v1.safetensors"),
     }
-    with open(os.path.join(HERE, "prime_catalog_v1.json"), "w") as fh:
+    with open(os.path.join(DATA, "prime_catalog_v1.json"), "w") as fh:
         json.dump(catalog, fh, separators=(",", ":"))
         fh.write("\n")
     return 0

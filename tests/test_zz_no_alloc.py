@@ -73,3 +73,47 @@ def test_noalloc_rejects_batches_beyond_its_fixed_scratch():
     assert rc != 0
     assert "scratch" in nat.last_error()
     ctx.close()
+
+
+def test_noalloc_rejects_invalid_level_and_negative_batch():
+    cfg = CkksConfig.parse(Preset.slots8192_scale40_levels7_int64)
+    dev = torch.device("cuda", 0)
+    ctx = nat.NativeContext(64, cfg.logN, cfg.moduli, cfg.num_q_primes, cfg.num_p_primes, dev)
+    dummy = torch.zeros(16, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    for batch, level in ((1, cfg.num_q_primes), (1, -1), (-1, 0)):
+        rc = ctx.lib.fhb_ckks_relinearize_noalloc(ctx.handle, dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr(),
+                                                  batch, level, 0, stream)
+        assert rc != 0
+        assert "invalid batch or level" in nat.last_error()
+    ctx.close()
+
+
+@pytest.mark.skipif(torch.cuda.device_count() < 2, reason="needs a second visible GPU")
+def test_noalloc_on_a_device_that_is_not_current():
+    """The context lives on GPU 1 while GPU 0 is current: the scratch address
+    is looked up on GPU 1, the result equals the buffered entry point's, and
+    GPU 0 is current again afterwards."""
+    cfg = CkksConfig.parse(Preset.slots8192_scale40_levels7_int64)
+    dev = torch.device("cuda", 1)
+    ctx = nat.NativeContext(64, cfg.logN, cfg.moduli, cfg.num_q_primes, cfg.num_p_primes, dev)
+    rng = np.random.default_rng(91)
+    key = random_key(rng, cfg, cfg.N)
+    rows = list(range(cfg.num_q_primes))
+    ct3_np = uniform_residues(rng, cfg.moduli, rows, (3, 1), cfg.N, lazy=True)
+    k = torch.from_numpy(key).to(dev)
+    c = torch.from_numpy(ct3_np).to(dev)
+    torch.cuda.set_device(0)
+    with torch.cuda.device(1):
+        want = _relin_with_buffer(ctx, c, k, 1, 0, 0, len(rows), cfg.N, cfg.torch_dtype)
+        torch.cuda.synchronize()
+    out = torch.empty((2, 1, len(rows), cfg.N), dtype=cfg.torch_dtype, device=dev)
+    with torch.cuda.device(1):
+        stream = torch.cuda.current_stream().cuda_stream
+    assert torch.cuda.current_device() == 0
+    nat.check(ctx.lib.fhb_ckks_relinearize_noalloc(ctx.handle, c.data_ptr(), k.data_ptr(), out.data_ptr(), 1, 0, 0,
+                                                   stream), "fhb_ckks_relinearize_noalloc")
+    assert torch.cuda.current_device() == 0
+    torch.cuda.synchronize(1)
+    assert torch.equal(out, want)
+    ctx.close()
