@@ -49,6 +49,7 @@ sys.path.insert(0, ROOT)
 
 PRESET = "slots32768_scale40_levels34_int64"
 KS_TRAFFIC_BYTES_BATCH32 = 12741399552 + 2934590720  # ncu dram read + write, k_keyswitch_core, batch 32 (profiles/)
+KS_EXT_TRAFFIC_BYTES_BATCH32 = None  # same for the key-switch core of the tensor-core form (not yet captured)
 METRIC = "hmult_relin_rescale_ops_per_s_logN16_L35"
 UNIT = "ops/s"
 CONFIG = {
@@ -409,6 +410,40 @@ def schema_ops_leg(eng, x, y, kd, stream, steps=5):
     return res
 
 
+def forms_leg(eng, ca, cb, rlk, stream, steps=5):
+    """The key switch with its basis conversion on the CUDA cores and on the
+    int8 tensor cores, same inputs: HMult+relin+rescale, single rotation and
+    16 hoisted rotations (ops/s), and the bit identity of their outputs."""
+    out, results = {}, {}
+    keep = eng.basis_conversion
+    eng.generate_rotation_keys(list(range(1, 17)))
+    for form in ("cuda_cores", "tensor_cores"):
+        eng.basis_conversion = form
+        res = {}
+        r = eng.multiply_relinearize_rescale(ca, cb, rlk)
+        torch.cuda.synchronize()
+        ms = _time_events(lambda: eng.multiply_relinearize_rescale(ca, cb, rlk), steps, stream)
+        res["hmult_relin_rescale_ops_per_s"] = ca.batch_size / (ms / 1000.0)
+        res["hmult_relin_rescale_ms"] = ms
+        rot = eng.rotate_by_step(r, 1)
+        torch.cuda.synchronize()
+        rms = _time_events(lambda: eng.rotate_by_step(r, 1), steps, stream)
+        res["rotate_ops_per_s"] = r.batch_size / (rms / 1000.0)
+        hoisted = eng.rotate_many_by_steps(r, list(range(1, 17)))
+        torch.cuda.synchronize()
+        hms = _time_events(lambda: eng.rotate_many_by_steps(r, list(range(1, 17))), max(2, steps // 2), stream)
+        res["hoisted_rotations_16_ops_per_s"] = 16 * r.batch_size / (hms / 1000.0)
+        results[form] = (r.data.clone(), rot.data.clone(), torch.stack([h.data for h in hoisted]))
+        out[form] = res
+    a, b = results["cuda_cores"], results["tensor_cores"]
+    out["bit_identical"] = all(bool(torch.equal(x, y)) for x, y in zip(a, b))
+    out["tensor_cores_over_cuda_cores"] = {
+        k: out["tensor_cores"][k] / out["cuda_cores"][k]
+        for k in ("hmult_relin_rescale_ops_per_s", "rotate_ops_per_s", "hoisted_rotations_16_ops_per_s")}
+    eng.basis_conversion = keep
+    return out
+
+
 def mixed_batch_leg(dev, stream, count=512, steps=3):
     """Mixed-level batch at slots32768_scale40_levels34_int64: `count`
     ciphertexts with limb counts uniform in 3..35 (uniform [-0.05, 0.05]
@@ -527,7 +562,9 @@ def main() -> int:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-extras", action="store_true", help="skip rotation/parity/CPU legs")
     ap.add_argument("--mixed-count", type=int, default=512, help="ciphertexts of the mixed-level leg (0: skip)")
-    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed", "ops", "schema"], default=None,
+    ap.add_argument("--basis", choices=["cuda_cores", "tensor_cores"], default="tensor_cores",
+                    help="where the key switch's basis conversion runs in the headline step")
+    ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed", "ops", "schema", "forms"], default=None,
                     help="run only this side leg on one GPU and print its result (profiling aid)")
     args = ap.parse_args()
     ws, rank, local = _dist()
@@ -553,6 +590,12 @@ def main() -> int:
             x, y = rows(args.batch, eng.num_q), rows(args.batch, eng.num_q)
             kd = rows(2, eng.num_q + eng.num_p)
             res = schema_ops_leg(eng, x, y, kd, stream, steps=max(1, args.steps))
+        elif args.leg == "forms":
+            from fhelium_b200.engine import CkksEngine
+            eng = CkksEngine(PRESET, device=dev, rng_seed=7)
+            ca = eng.coefficient_domain_to_ntt_domain(eng.encrypt_message(_messages(args.batch, eng.num_slots, 2)))
+            cb = eng.coefficient_domain_to_ntt_domain(eng.encrypt_message(_messages(args.batch, eng.num_slots, 3)))
+            res = forms_leg(eng, ca, cb, eng.relinearization_key, stream, steps=max(2, args.steps))
         else:
             res = mixed_batch_leg(dev, stream, args.mixed_count, args.steps)
         print(json.dumps({"leg": args.leg, **res}), flush=True)
@@ -565,7 +608,7 @@ def main() -> int:
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     cfg = CkksConfig.parse(PRESET)
-    eng = CkksEngine(cfg, device=dev, rng_seed=1234 + rank)
+    eng = CkksEngine(cfg, device=dev, rng_seed=1234 + rank, basis_conversion=args.basis)
     B = args.batch
     x = _messages(B, eng.num_slots, 2 + 2 * rank)
     y = _messages(B, eng.num_slots, 3 + 2 * rank)
@@ -591,7 +634,8 @@ def main() -> int:
     ms = _max_over_ranks(ms, ws, dev)
     from fhelium_b200 import ranks
     value = ranks.job_rate(B, ws, ms)
-    launches_per_step = 5  # tensor product, INTT of c2, ModUp digits, key-switch core, ModDown+rescale
+    # tensor product, INTT of c2, ModUp digits, (tensor-core basis extension,) key-switch core, ModDown+rescale
+    launches_per_step = 6 if args.basis == "tensor_cores" else 5
 
     # ---- end to end through the public API with host buffers -------------
     host_a = ca.data.cpu().pin_memory()
@@ -644,6 +688,13 @@ def main() -> int:
         "tensor_product": lambda: lib.fhb_ckks_multiply(h, nat.ptr(ca.data), nat.ptr(cb.data), nat.ptr(coef), B, 0, s),
         "inverse_ntt_d2": lambda: lib.fhb_inverse_ntt(h, nat.ptr(coef[2]), nat.ptr(digits), B, L, 0, 2, s),
     }
+    ext = None
+    if args.basis == "tensor_cores":
+        # the tensor-core form's two key-switch kernels
+        ext = torch.empty(int(lib.fhb_tc_basis_extend_words(h, B, 0)), dtype=torch.int64, device=dev)
+        kernels["tc_basis_extend"] = lambda: lib.fhb_tc_basis_extend(h, nat.ptr(digits), nat.ptr(ext), B, 0, s)
+        kernels["keyswitch_core_extended"] = lambda: lib.fhb_ckks_keyswitch_core_extended(
+            h, nat.ptr(ext), nat.ptr(rlk.data), nat.ptr(t[0]), nat.ptr(t[1]), B, 0, s)
     per_kernel = {}
     for name, fn in kernels.items():
         fn()
@@ -694,6 +745,19 @@ def main() -> int:
         "moddown_rescale": (rows(2 * (L + P_) + 2 * L + 2 * (L - 1)),
                             2 * B * n_ * (P_ * (P_ + 1) // 2 + L * (P_ + 2))),
     }
+    int8_ops = {}
+    if ext is not None:
+        nd_ = len(eng.level_digits[0])
+        ext_rows = nd_ * (L + P_)
+        # basis extension: digit rows read once, every extension row written once;
+        # int8 MMA work: per 128 coefficients and 16-row chunk 2 x 128 x N x 32
+        chunk_n = [min(16, L + P_ - 16 * c) * 8 for c in range((L + P_ + 15) // 16)]
+        int8_ops["tc_basis_extend"] = nd_ * B * (n_ // 128) * sum(2 * 128 * ((c + 15) // 16 * 16) * 32
+                                                                  for c in chunk_n)
+        kroof["tc_basis_extend"] = (rows(L) + rows(ext_rows), 0)
+        kroof["keyswitch_core_extended"] = (rows(ext_rows) + rows(2 * (L + P_)) + 2 * dnum_ * (L + P_) * limb,
+                                            ks_modmul - B * qp_ * L * n_)
+    int8_peak, int8_src = _int8_peak_tops()
     kernel_roofline = {}
     for name, (nbytes, nmul) in kroof.items():
         sec = per_kernel[name] / 1000.0
@@ -702,6 +766,9 @@ def main() -> int:
         if nmul:
             entry.update({"modmul": nmul, "modmul_per_s": nmul / sec, "modmul_frac": nmul / sec / modmul_peak})
         entry["bound"] = "hbm" if not nmul or entry["hbm_frac"] > entry["modmul_frac"] else "integer"
+        if name in int8_ops:
+            entry.update({"int8_ops": int8_ops[name], "int8_tops": int8_ops[name] / sec / 1e12,
+                          "int8_frac": int8_ops[name] / sec / 1e12 / int8_peak, "int8_peak_source": int8_src})
         kernel_roofline[name] = entry
     # DRAM bytes of one k_keyswitch_core launch: 15.7 GB measured by ncu
     # (dram__bytes_read.sum + dram__bytes_write.sum) on the batch-32 launch of
@@ -709,6 +776,15 @@ def main() -> int:
     # rows); every destination row re-reads the digit rows of its group, so
     # the traffic grows with the batch and is scaled by the units processed.
     traffic = KS_TRAFFIC_BYTES_BATCH32 * B / 32 if cfg.logN == 16 and L == 35 else None
+    # the dominant kernel of the headline form
+    dom = "keyswitch_core_extended" if ext is not None else "keyswitch_core"
+    dom_kernel = {"keyswitch_core": "k_keyswitch_core", "keyswitch_core_extended": "k_keyswitch_core<PRE>"}[dom]
+    if dom == "keyswitch_core_extended":
+        traffic = (KS_EXT_TRAFFIC_BYTES_BATCH32 * B / 32
+                   if KS_EXT_TRAFFIC_BYTES_BATCH32 and cfg.logN == 16 and L == 35 else None)
+    dom_bytes, dom_modmul = kroof[dom]
+    achieved = dom_bytes / (per_kernel[dom] / 1000.0) / 1e9
+    modmul_achieved = dom_modmul / (per_kernel[dom] / 1000.0)
 
     extras = {}
     if not args.no_extras:
@@ -730,6 +806,7 @@ def main() -> int:
         h_ms = _time_events(lambda: eng.rotate_many_by_steps(rot_in, steps16), 2, stream)
         extras["hoisted_rotations_16_ops_per_s"] = 16 * B / (h_ms / 1000.0)
         extras["reference_schema_kernels"] = schema_ops_leg(eng, ca.data[0], ca.data[1], rlk.data[0], stream)
+        extras["basis_conversion_forms"] = forms_leg(eng, ca, cb, rlk, stream, steps=max(2, min(args.steps, 5)))
         extras["ntt_int32_logN16_36limbs_batch64"] = ntt_leg(dev, stream, args.steps)
         extras["bootstrap_logN16_batch8"] = bootstrap_leg(dev, stream)
         if args.mixed_count > 0:
@@ -761,19 +838,20 @@ def main() -> int:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded uniform messages, engine-generated keys)",
-        "config": dict(CONFIG, batch_per_gpu=B, global_batch=B * ws, parallelism=f"independent ciphertexts x{ws}"),
+        "config": dict(CONFIG, batch_per_gpu=B, global_batch=B * ws, parallelism=f"independent ciphertexts x{ws}",
+                       basis_conversion=args.basis),
         "e2e": {"value": ws * B / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "chunks": e2e_chunks["chunks"],
                 "chunk_trials_ms": trial},
         "gpu_launches": launches_per_step * args.steps,
-        "alu_roofline": {"kernel": "k_keyswitch_core", "unit": "modular products/s",
-                         "modmul_per_launch": ks_modmul, "achieved": modmul_achieved, "peak": modmul_peak,
+        "alu_roofline": {"kernel": dom_kernel, "unit": "modular products/s",
+                         "modmul_per_launch": dom_modmul, "achieved": modmul_achieved, "peak": modmul_peak,
                          "frac": modmul_achieved / modmul_peak,
                          "peak_source": "fhb_modmul_probe: 148x8 CTAs x 256 threads x 8 independent Shoup chains, "
                                         "timed in this run"},
-        "roofline": {"kernel": "k_keyswitch_core", "bound": "hbm", "achieved": achieved, "peak": peak,
+        "roofline": {"kernel": dom_kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                     "algorithmic_bytes_per_launch": ks_bytes, "launch_ms": per_kernel["keyswitch_core"],
+                     "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": per_kernel[dom],
                      "note": "int64 Montgomery/Shoup arithmetic on CUDA cores: the kernel is integer-ALU bound"},
         "kernel_ms": per_kernel,
         "kernel_roofline": kernel_roofline,

@@ -28,6 +28,9 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_tc_forward_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _P]),
     "fhb_tc_inverse_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _P]),
     "fhb_tc_ntt_status": (_I, [_P, ctypes.POINTER(_I)]),
+    "fhb_tc_basis_extend": (_I, [_P, _P, _P, _I64, _I, _P]),
+    "fhb_tc_basis_extend_words": (_I64, [_P, _I64, _I]),
+    "fhb_tc_basis_status": (_I, [_P, ctypes.POINTER(_I)]),
     "fhb_tc_ntt_tables_host": (_I, [ctypes.c_uint64, ctypes.c_uint64, _I, _P, _P]),
     "fhb_last_error": (ctypes.c_char_p, []),
     "fhb_context_create": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, _I, ctypes.POINTER(_P)]),
@@ -41,6 +44,7 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_multiply_to_coefficient": (_I, [_P, _P, _P, _P, _I64, _I, _P]),
     "fhb_ckks_modup_digits": (_I, [_P, _P, _P, _I64, _I, _U32, _P]),
     "fhb_ckks_keyswitch_core": (_I, [_P, _P, _P, _P, _P, _I64, _I, _P]),
+    "fhb_ckks_keyswitch_core_extended": (_I, [_P, _P, _P, _P, _P, _I64, _I, _P]),
     "fhb_ckks_moddown": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I, _U32, _I, _P]),
     "fhb_ckks_prepare_rotation": (_I, [_P, _P, _P, _I64, _I, _P]),
     "fhb_ckks_apply_prepared_rotation": (_I, [_P, _P, _P, _P, _P, _I64, _I, _U32, _P]),
@@ -81,7 +85,9 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_context_create_transform": (_I, [_I, _I, ctypes.POINTER(ctypes.c_uint64), _I, _I, ctypes.POINTER(_P)]),
 }
 
-TUNE_KS_ORDER, TUNE_NTT_FORWARD_EPT, TUNE_NTT_INVERSE_EPT = range(3)
+(TUNE_KS_ORDER, TUNE_NTT_FORWARD_EPT, TUNE_NTT_INVERSE_EPT, TUNE_BASIS_CONVERSION, TUNE_TC_WAIT_US,
+ TUNE_TC_TEST_STALL) = range(6)
+BASIS_CUDA_CORES, BASIS_TENSOR_CORES = 0, 1
 OP_MONTGOMERY_MUL, OP_ADD_LAZY, OP_SUB_LAZY, OP_ADD_CANONICAL, OP_SUB_CANONICAL, OP_NEGATE = range(6)
 INV_MONTGOMERY, INV_STANDARD_LAZY, INV_STANDARD, INV_CENTERED = range(4)
 

@@ -110,8 +110,9 @@ int mul_coef(const Context& c, const void* a, const void* b, void* out, int64_t 
   FHB_DISPATCH(run_mul_coef, c, a, b, out, batch, level, st);
 }
 int ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-            int level, cudaStream_t st, const uint64_t* item_keys = nullptr, const void* ct3 = nullptr) {
-  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys, ct3);
+            int level, cudaStream_t st, const uint64_t* item_keys = nullptr, const void* ct3 = nullptr,
+            bool pre = false) {
+  FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys, ct3, pre);
 }
 int ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
            int64_t batch, int level, cudaStream_t st) {
@@ -271,6 +272,7 @@ struct Scratch {
   char* digits;  // [B, L, N]
   char* t0;      // [B, L+P, N]
   char* t1;      // [B, L+P, N]
+  char* ext;     // tensor-core form only: [D_l, B, L+P, N] digit extensions
 };
 
 Scratch carve(const Context& c, void* base, int64_t batch, int level) {
@@ -281,6 +283,7 @@ Scratch carve(const Context& c, void* base, int64_t batch, int level) {
   s.digits = s.coef + 3 * batch * l * n * w;
   s.t0 = s.digits + batch * l * n * w;
   s.t1 = s.t0 + batch * lp * n * w;
+  s.ext = s.t1 + batch * lp * n * w;
   return s;
 }
 
@@ -365,6 +368,22 @@ int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
       if (value != 0 && value != 8 && value != 16) return fail(-2, "residues per thread must be 0, 8 or 16");
       (param == FHB_TUNE_NTT_FORWARD_EPT ? ctx->impl->ntt_ept_fwd : ctx->impl->ntt_ept_inv) = value;
       return 0;
+    case FHB_TUNE_BASIS_CONVERSION:
+      if (value != 0 && value != 1) return fail(-2, "basis conversion must be 0 (CUDA cores) or 1 (tensor cores)");
+      if (value == 1) {
+        fhb::DeviceGuard guard(ctx->impl->device);
+        TRY(fhb::tc_basis_prepare(*ctx->impl));
+      }
+      ctx->impl->basis_tc = value;
+      return 0;
+    case FHB_TUNE_TC_WAIT_US:
+      if (value < 0) return fail(-2, "wait limit must be >= 0 microseconds");
+      ctx->impl->tc_wait_ns = uint64_t(value) * 1000u;
+      return 0;
+    case FHB_TUNE_TC_TEST_STALL:
+      if (value != 0 && value != 1) return fail(-2, "stall must be 0 or 1");
+      ctx->impl->tc_test_stall = value;
+      return 0;
     default:
       return fail(-2, "unknown tuning parameter");
   }
@@ -376,6 +395,9 @@ int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value) {
     case FHB_TUNE_KS_ORDER: *value = ctx->impl->ks_order; return 0;
     case FHB_TUNE_NTT_FORWARD_EPT: *value = ctx->impl->ntt_ept_fwd; return 0;
     case FHB_TUNE_NTT_INVERSE_EPT: *value = ctx->impl->ntt_ept_inv; return 0;
+    case FHB_TUNE_BASIS_CONVERSION: *value = ctx->impl->basis_tc; return 0;
+    case FHB_TUNE_TC_WAIT_US: *value = int(ctx->impl->tc_wait_ns / 1000u); return 0;
+    case FHB_TUNE_TC_TEST_STALL: *value = ctx->impl->tc_test_stall; return 0;
     default: return fail(-2, "unknown tuning parameter");
   }
 }
@@ -435,6 +457,30 @@ int fhb_tc_ntt_status(const fhb_context* ctx, int* flag) {
   return fhb::tc_ntt_status(*ctx->impl, flag);
 }
 
+int fhb_tc_basis_extend(const fhb_context* ctx, const void* digits, void* ext, int64_t batch, int level,
+                        fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(digits, "digits"));
+  TRY(fhb::check_ptr(ext, "ext"));
+  TRY(fhb::check_level(c, level));
+  if (batch < 0) return fail(-2, "batch must be >= 0");
+  return fhb::tc_extend(*ctx->impl, digits, ext, batch, level, false, st);
+}
+
+int64_t fhb_tc_basis_extend_words(const fhb_context* ctx, int64_t batch, int level) {
+  if (!ctx || !ctx->impl || batch < 0 || level < 0 || level >= ctx->impl->num_q) return -1;
+  return fhb::tc_ext_words(*ctx->impl, batch, level);
+}
+
+int fhb_tc_basis_status(const fhb_context* ctx, int* flag) {
+  fhb_stream stream = nullptr;
+  CTX_OR_FAIL();
+  (void)st;
+  (void)c;
+  if (!flag) return fail(-2, "flag is NULL");
+  return fhb::tc_basis_status(*ctx->impl, flag);
+}
+
 int fhb_tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post) {
   if (!bmat) return fail(-2, "bmat is NULL");
   if (pass < 0 || pass > 5) return fail(-2, "pass must be 0..5");
@@ -486,6 +532,18 @@ int fhb_ckks_keyswitch_core(const fhb_context* ctx, const void* digits, const vo
   return fhb::ks_core(c, digits, key, acc0, acc1, batch, level, st);
 }
 
+int fhb_ckks_keyswitch_core_extended(const fhb_context* ctx, const void* ext, const void* key, void* acc0,
+                                     void* acc1, int64_t batch, int level, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(ext, "ext"));
+  TRY(fhb::check_ptr(key, "key"));
+  TRY(fhb::check_ptr(acc0, "acc0"));
+  TRY(fhb::check_ptr(acc1, "acc1"));
+  TRY(fhb::check_level(c, level));
+  if (batch < 0) return fail(-2, "batch must be >= 0");
+  return fhb::ks_core(c, ext, key, acc0, acc1, batch, level, st, nullptr, nullptr, true);
+}
+
 int fhb_ckks_moddown(const fhb_context* ctx, const void* t0, const void* t1, const void* add0, const void* add1,
                      void* out, int64_t batch, int level, uint32_t add0_galois, int rescale, fhb_stream stream) {
   CTX_OR_FAIL();
@@ -504,6 +562,15 @@ int fhb_ckks_prepare_rotation(const fhb_context* ctx, const void* digits, void* 
   TRY(fhb::check_ptr(digits, "digits"));
   TRY(fhb::check_ptr(prepared, "prepared"));
   TRY(fhb::check_level(c, level));
+  if (batch < 0) return fail(-2, "batch must be >= 0");
+  if (c.basis_tc) {
+    // tensor-core form: extensions straight into the prepared layout
+    // [D_l, B, QP_l, N], then their forward NTT in place (no x R)
+    const int qpl = c.qp() - level;
+    TRY(fhb::tc_extend(*ctx->impl, digits, prepared, batch, level, false, st));
+    const int64_t polys = fhb::tc_ext_words(c, batch, level) / c.n();
+    return fhb::forward(c, prepared, prepared, polys, qpl, level, true, st);
+  }
   return fhb::prepare(c, digits, prepared, batch, level, st);
 }
 
@@ -606,7 +673,8 @@ int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, 
   const Context& c = *ctx->impl;
   if (level < 0 || level >= c.num_q || batch < 0) return -1;
   const int64_t l = c.num_q - level, lp = l + c.num_p;
-  const int64_t per_ct = (3 * l + l + 2 * lp) * c.n() * fhb::word_bytes(c);
+  int64_t per_ct = (3 * l + l + 2 * lp) * c.n() * fhb::word_bytes(c);
+  if (c.basis_tc) per_ct += fhb::tc_ext_words(c, 1, level) * fhb::word_bytes(c);
   if (batch > INT64_MAX / per_ct) return -1;  // the size does not fit in 64 bits
   return per_ct * batch;
 }
@@ -622,10 +690,20 @@ static int check_scratch(const fhb_context* ctx, int64_t batch, int level, int64
   return 0;
 }
 
+// Key-switch core on the ModUp digits in s.digits: with the tensor-core
+// basis conversion the extensions are materialised first (own-digit rows
+// skipped when the core reuses c2 there) and the core only transforms.
+static int ks_core_from_digits(const Context& c, const fhb::Scratch& s, const void* key, int64_t batch, int level,
+                               cudaStream_t st, const uint64_t* item_keys = nullptr, const void* ct3 = nullptr) {
+  if (!c.basis_tc) return fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st, item_keys, ct3);
+  TRY(fhb::tc_extend(const_cast<Context&>(c), s.digits, s.ext, batch, level, ct3 != nullptr, st));
+  return fhb::ks_core(c, s.ext, key, s.t0, s.t1, batch, level, st, item_keys, ct3, true);
+}
+
 static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* key, const void* add0,
                           const void* add1, uint32_t add0_galois, void* out, int64_t batch, int level, int rescale,
                           cudaStream_t st) {
-  TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st));
+  TRY(ks_core_from_digits(c, s, key, batch, level, st));
   return FHB_WORD(fhb::moddown, c, s.t0, s.t1, add0, add1, out, batch, level, add0_galois, rescale, st);
 }
 
@@ -635,7 +713,7 @@ static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* k
 static int relinearize_tail(const Context& c, const fhb::Scratch& s, const void* key, const void* ct3, void* out,
                             int64_t batch, int level, int rescale, cudaStream_t st) {
   TRY(FHB_WORD(fhb::modup, c, s.t0, s.digits, batch, level, 1u, st));
-  TRY(fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st, nullptr, ct3));
+  TRY(ks_core_from_digits(c, s, key, batch, level, st, nullptr, ct3));
   return FHB_WORD(fhb::moddown, c, s.t0, s.t1, nullptr, nullptr, out, batch, level, 1u, rescale, st);
 }
 
@@ -724,7 +802,7 @@ int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
   TRY(FHB_WORD(fhb::modup, c, static_cast<const char*>(ct) + comp, s.digits, batch, level, 1u, st, galois));
-  TRY(fhb::ks_core(c, s.digits, nullptr, s.t0, s.t1, batch, level, st, key_ptrs));
+  TRY(ks_core_from_digits(c, s, nullptr, batch, level, st, key_ptrs));
   return FHB_WORD(fhb::moddown, c, s.t0, s.t1, ct, nullptr, out, batch, level, 1u, 0, st, galois);
 }
 

@@ -176,6 +176,7 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
   }
   level0.push_back({c.num_q - 1});
   levels.assign(c.num_q, LevelTables<T>{});
+  c.level_digits.assign(c.num_q, {});
   for (int level = 0; level < c.num_q; ++level) {
     LevelTables<T>& lt = levels[level];
     std::vector<DigitDesc> dd;
@@ -203,6 +204,7 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
       ext.insert(ext.end(), e.begin(), e.end());
     }
     lt.num_digits = int(dd.size());
+    c.level_digits[level] = dd;
     lt.digits = upload(c, dd);
     lt.garner = upload(c, gar);
     lt.ext = upload(c, ext);
@@ -275,6 +277,7 @@ void destroy_context(Context* c) {
   for (void* p : c->allocations) cudaFree(p);
   cudaSetDevice(prev);
   delete c->tc;
+  delete c->tcb;
   delete c;
 }
 

@@ -57,6 +57,17 @@ struct TcNttTables {
   int* err = nullptr;                 // device flag: a bounded wait gave up
 };
 
+// Tables of the exact int8 tensor-core basis conversion (int64 residues),
+// built on first use.  All device arrays are owned through
+// Context::allocations.
+struct TcBasisTables {
+  std::vector<uint8_t*> bmat;     // per level: [digit][16-row chunk][128 x 32 ks] byte matrices
+  uint64_t* pinfo = nullptr;      // [QP][2]: p, -p^{-1} mod 2^64
+  int ks = 1;                     // K-steps of 32 bytes (digits of up to 4 or 8 primes)
+  int sms = 0;                    // multiprocessors of the context's device (one CTA each)
+  int* err = nullptr;             // device flag: a bounded wait gave up
+};
+
 struct Context {
   int bits = 0;        // 64 or 32
   int log_n = 0;
@@ -75,6 +86,18 @@ struct Context {
   int ntt_ept_inv = 0;  // tuning: same for the inverse NTT and the fused HMult -> inverse NTT
   TcNttTables* tc = nullptr;  // tensor-core NTT tables (null until prepared)
   std::mutex tc_mutex;
+  // tuning: basis conversion of the key switch on the CUDA cores (0) or the
+  // int8 tensor cores (1, int64 contexts)
+  int basis_tc = 0;
+  // limit of the tensor-core kernels' pipeline waits in ns (0 = the default
+  // second); their drain waits always keep the default
+  unsigned long long tc_wait_ns = 0;
+  // test only: tensor-core kernels first wait on a barrier nothing completes
+  // (so their pipeline limit runs out and they report it)
+  int tc_test_stall = 0;
+  TcBasisTables* tcb = nullptr;  // tensor-core basis conversion tables (null until prepared)
+  std::mutex tcb_mutex;
+  std::vector<std::vector<DigitDesc>> level_digits;  // host copy of each level's active digits
   int qp() const { return num_q + num_p; }
   int n() const { return 1 << log_n; }
 };
@@ -102,6 +125,17 @@ int tc_ntt(Context& c, const void* in, void* out, int64_t polys, int rows, int r
 int tc_ntt_status(Context& c, int* flag);
 size_t tc_ntt_table_bytes(int pass);
 void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post);
+
+// Exact int8 tensor-core basis conversion (fhb_tc_basis.cu).  tc_extend
+// writes the extensions of every active digit of `level` to every row of
+// Q_l P: ext [digits][batch][QP_l][N] in [0, 2p) (tc_ext_words words), from
+// the Garner digits [batch][L][N]; skip_own leaves a digit's own rows
+// unwritten.  tc_basis_status reads and clears the device error flag.
+int tc_basis_prepare(Context& c);
+int64_t tc_ext_words(const Context& c, int64_t batch, int level);
+int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st);
+int tc_basis_status(Context& c, int* flag);
+void tc_basis_tables_host(const Context& c, int level, int ks, std::vector<uint8_t>& out);
 
 // Host-side status plumbing shared by the C ABI.
 void set_error(const std::string& msg);

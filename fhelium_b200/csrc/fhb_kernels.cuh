@@ -532,7 +532,11 @@ __device__ __forceinline__ void ks_own_digit_ntt(T (&v)[E], const T* ct3, int64_
 // inverse NTT at the start of ModDown (fhelium/engine/hybrid_keyswitch.py:
 // 321-371, 530-546).  key: [D, 2, QP0, N] NTT/Montgomery level-zero rows.
 // acc0/acc1: [B, QP_l, N]; they double as accumulation scratch.
-template <typename T, int LOGN>
+// PRE (tensor-core form): `digits` holds the extensions already computed by
+// the int8 tensor-core basis conversion, [D_l][B][QP_l][N] in [0, 2p), so
+// the source of each forward NTT is a plain row read instead of the
+// extension sum.
+template <typename T, int LOGN, bool PRE = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
                  T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
@@ -566,6 +570,9 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
     if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
       // uniform over the cluster: skipping the transform skips its barriers everywhere
       ks_own_digit_ntt(v, ct3_own, ct3_stride, p);
+    } else if constexpr (PRE) {
+      RowSource<T, false> src{digits + ((int64_t(a) * batch + bi) * qp_limbs + jrow) * G::kN, 0, 0, p.q};
+      tw.forward_from(src, s, p, v);
     } else {
       ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
                        qp0, d.alpha, LOGN, p.q, p.twice_q};

@@ -78,8 +78,19 @@ int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int6
 
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3) {
+                int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3, bool pre) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
+  if (pre) {
+    // extensions from the tensor-core basis conversion (int64 only)
+    if constexpr (sizeof(T) == 8) {
+      return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN, true>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
+                                     (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level,
+                                     c.qp(), c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys),
+                                     (const T*)ct3, tables<T>(c), level_tables<T>(c, level));
+    } else {
+      return fail(-7, "the tensor-core basis conversion needs an int64 context");
+    }
+  }
   return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
                                  (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(),
                                  c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys), (const T*)ct3,
@@ -120,7 +131,7 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   template int run_inverse<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, int, cudaStream_t);    \
   template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, cudaStream_t); \
   template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
-                                    cudaStream_t, const uint64_t*, const void*);                                \
+                                    cudaStream_t, const uint64_t*, const void*, bool);                          \
   template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
                                    cudaStream_t);                                                               \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \

@@ -1,0 +1,442 @@
+// Exact integer tensor-core basis extension (ModUp stage 2) for int64
+// residues (primes < 2^60) on the 5th-generation tensor cores:
+// tcgen05.mma kind::i8 with int32 accumulators in tensor memory.
+//
+// What it computes (the reference's mixed_radix_basis_extend_to_montgomery,
+// csrc/ops/rns/cuda/mixed_radix_cuda.cu:146-182, restated as a matrix
+// product): for every active hybrid digit a of a level, every ciphertext b,
+// every destination row j of Q_l P (prime p = p_{level + j}) and every
+// coefficient k,
+//   ext[a][b][j][k] = sum_{r < alpha_a} d_r[k] (M_r mod p)   (mod p), in [0, 2p),
+// where d_r are the digit's Garner mixed-radix digits (canonical, < 2^60) and
+// M_r the product of the digit's first r primes.  This is the value the
+// CUDA-core key-switch core computes on the fly as the source of each
+// forward NTT; the tensor-core form materialises it once so the core only
+// transforms.
+//
+// Exact byte form.  Split d_r = sum_u 2^{8u} d_{r,u} (u < 8) and pre-scale the
+// constants per data byte and by 2^64: C'_{r,u} = 2^{8u} 2^64 (M_r mod p) mod p,
+// itself split into bytes C'_{r,u} = sum_e 2^{8e} c_{r,u,e}.  One MMA of
+//   M = 128 coefficients, K = 32 (8 data bytes x 4 digit rows), N = 8 bytes e
+//   x up to 16 destination rows
+// gives acc[k][(j, e)] = sum_{r,u} d_{r,u}[k] c_{r,u,e}(j) < 32 * 255^2 < 2^21
+// (K = 64 and < 2^22 for digits of 5..8 primes), so the sum is exact in int32.
+// The epilogue forms S = sum_e 2^{8e} acc_e < 2^78 = 2^64 (sum_r d_r M_r mod p)
+// (mod p) and one Montgomery reduction by 2^64 returns the extension in
+// [0, 2p) (S < p 2^64 for p > 2^14).  The A operand needs no byte shuffle:
+// in the K-major canonical layout the 8 bytes of a little-endian residue word
+// are 8 consecutive K positions, so the A tile is the digit words themselves,
+// placed two rows to a 16-byte core-matrix row.
+//
+// Kernel: persistent CTAs, one per SM (the 512 TMEM columns are the SM's),
+// each streaming a contiguous range of units (digit, ciphertext, 128
+// coefficients), digit-major, through a warp-specialised pipeline:
+//   loaders (warps 16-17): the digit words of a unit into one of 4 A tiles;
+//       lane 0 of warp 16 also bulk-copies the byte matrix of each new digit
+//       into one of two B buffers;
+//   MMA issuer (warp 18, lane 0): per unit one MMA per 16-row chunk of
+//       destination rows (K-steps of 32) into a ring of 4 TMEM slots of 128
+//       columns;
+//   epilogue (warps 0-15; warp w reads TMEM lane quarter w % 4 and the four
+//       rows 4 (w / 4) .. + 3 of a chunk): recombination, reduction, store.
+// Every mbarrier wait is bounded; a wait that gives up raises a CTA abort
+// flag that releases every other wait and sets the device error flag, and
+// the CTA drains its bulk copies and MMAs (bounded) before it frees TMEM.
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fhb_context.h"
+#include "fhb_tc_common.cuh"
+
+namespace fhb {
+namespace tcb {
+using namespace fhb::tc;
+
+constexpr int kUnit = 128;             // coefficients per unit (MMA M)
+constexpr int kChunkRows = 16;         // destination rows per MMA: N = 8 x 16 = 128 at most
+constexpr int kAccCols = 128;          // TMEM columns per accumulator slot
+constexpr int kAccSlots = 4;
+constexpr int kASlots = 4;
+constexpr int kTmemCols = kAccSlots * kAccCols;  // 512: the whole SM
+constexpr int kEpilogueWarps = 16;
+constexpr int kLoaderWarp0 = 16;
+constexpr int kLoaderWarps = 2;
+constexpr int kMmaWarp = 18;
+constexpr int kThreads = 32 * 19;
+constexpr int kNumBarriers = 2 + 2 + 2 * kASlots + 2 * kAccSlots + 2;  // ... drain, never
+constexpr int kBarrierBytes = 256;
+// Requested even when the tables are smaller, so that no second CTA (which
+// would wait for TMEM) is ever resident beside the first.
+constexpr int kMinSmem = 120 * 1024;
+static_assert(8 * kNumBarriers + 8 <= kBarrierBytes, "barrier area");
+
+struct ExtendArgs {
+  const uint64_t* digits;    // [batch][q_limbs][N]: Garner digits, canonical; row r = prime level + r
+  uint64_t* ext;             // [nd][batch][qp_limbs][N]: extensions, [0, 2p)
+  const uint8_t* bmat;       // [nd][nchunks][128 * K]: byte matrices of this level's digits
+  const uint64_t* pinfo;     // [QP0][2]: p, -p^{-1} mod 2^64
+  const DigitDesc* digit;    // [nd] active digits of this level
+  int64_t batch;
+  int level, q_limbs, qp_limbs, nd, nchunks, log_n;
+  int skip_own;              // 1: leave a digit's own rows unwritten (relinearisation reuses c2 there)
+  int* err;
+  unsigned long long wait_ns;  // limit of the pipeline waits (drain waits keep kWaitNs)
+  int stall;                   // test only: the epilogue first waits on a barrier nothing completes
+};
+
+// Extension value from the eight byte accumulators of one output:
+// S = sum_e 2^{8e} acc_e (< 2^78) and its Montgomery reduction by 2^64.
+__device__ __forceinline__ uint64_t recombine_redc(const uint32_t* acc, uint64_t p, uint64_t pneg) {
+  const uint64_t lo4 = uint64_t(acc[0]) + (uint64_t(acc[1]) << 8) + (uint64_t(acc[2]) << 16) +
+                       (uint64_t(acc[3]) << 24);  // < 2^47
+  const uint64_t hi4 = uint64_t(acc[4]) + (uint64_t(acc[5]) << 8) + (uint64_t(acc[6]) << 16) +
+                       (uint64_t(acc[7]) << 24);
+  const uint64_t slo = lo4 + (hi4 << 32);
+  const uint64_t shi = (hi4 >> 32) + (slo < lo4 ? 1u : 0u);
+  const uint64_t m = slo * pneg;  // S + m p = 0 mod 2^64
+  return shi + __umul64hi(m, p) + (slo != 0 ? 1u : 0u);
+}
+
+template <int KS>
+__global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
+  constexpr int K = 32 * KS;           // bytes of one A / B row
+  constexpr int kSbo = K / 16 * 128;   // byte distance between 8-row groups
+  constexpr int kATile = kUnit * K;
+  constexpr int kBTile = 128 * K;      // byte matrix of one 16-row chunk (128 MMA N rows)
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw0 = smem_addr(smem_raw);
+  const uint32_t base = (raw0 + 1023u) & ~1023u;
+  uint8_t* const gbase = smem_raw + (base - raw0);
+  const int bbytes = args.nchunks * kBTile;
+  const uint32_t b_addr0 = base;  // B buffers [2][bbytes], then A tiles [kASlots][kATile], then barriers
+  const uint32_t a_addr0 = base + 2u * uint32_t(bbytes);
+  uint8_t* const a_tile0 = gbase + 2 * bbytes;
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + 2 * bbytes + kASlots * kATile);
+  const uint32_t bar0 = smem_addr(bars);
+  auto bfull = [&](int x) { return bar0 + 8u * x; };
+  auto bempty = [&](int x) { return bar0 + 8u * (2 + x); };
+  auto afull = [&](int s) { return bar0 + 8u * (4 + s); };
+  auto aempty = [&](int s) { return bar0 + 8u * (4 + kASlots + s); };
+  auto accfull = [&](int s) { return bar0 + 8u * (4 + 2 * kASlots + s); };
+  auto accempty = [&](int s) { return bar0 + 8u * (4 + 2 * kASlots + kAccSlots + s); };
+  const uint32_t drain_bar = bar0 + 8u * (kNumBarriers - 1);
+  const uint32_t never_bar = bar0 + 8u * (kNumBarriers - 2);  // nothing arrives on it
+  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + kNumBarriers);
+  volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t n = int64_t(1) << args.log_n;
+  const int64_t nblk = n / kUnit;
+  const int64_t per_digit = args.batch * nblk;
+  const int64_t units = int64_t(args.nd) * per_digit;
+  const int64_t u_begin = units * blockIdx.x / gridDim.x, u_end = units * (blockIdx.x + 1) / gridDim.x;
+  const int nu = int(u_end - u_begin);
+  const unsigned long long lim = args.wait_ns;
+  // unit i of this CTA -> (digit, ciphertext, coefficient block)
+  auto unit_of = [&](int i, int& a, int64_t& b, int64_t& blk) {
+    const int64_t u = u_begin + i;
+    a = int(u / per_digit);
+    const int64_t r = u % per_digit;
+    b = r / nblk;
+    blk = r % nblk;
+  };
+
+  if (tid == 0) {
+    for (int x = 0; x < 2; ++x) {
+      mbar_init(bfull(x), 1);
+      mbar_init(bempty(x), 1);
+    }
+    for (int s = 0; s < kASlots; ++s) {
+      mbar_init(afull(s), kLoaderWarps);
+      mbar_init(aempty(s), 1);
+    }
+    for (int s = 0; s < kAccSlots; ++s) {
+      mbar_init(accfull(s), 1);
+      mbar_init(accempty(s), kEpilogueWarps);
+    }
+    mbar_init(drain_bar, 1);
+    mbar_init(never_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == kMmaWarp) tmem_alloc(smem_addr(tmem_slot), kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp >= kLoaderWarp0 && warp < kLoaderWarp0 + kLoaderWarps) {
+    // A tiles: word (coefficient m, digit row r) at byte (m / 8) sbo + (r / 2) 128 + (m % 8) 16 + (r % 2) 8,
+    // i.e. its 8 bytes are K positions 8 r .. 8 r + 7; rows r >= alpha are zero.
+    const int lt = tid - kLoaderWarp0 * 32;
+    const bool bthread = lt == 0;  // also streams the byte matrices
+    int cur = -1, dseq = -1;
+    int issued[2] = {0, 0};
+    for (int i = 0; i < nu; ++i) {
+      int a;
+      int64_t b, blk;
+      unit_of(i, a, b, blk);
+      if (a != cur) {
+        cur = a;
+        ++dseq;
+        if (bthread) {
+          const int x = dseq & 1;
+          if (dseq < 2 || mbar_wait(bempty(x), ((dseq >> 1) - 1) & 1, abort, args.err, lim)) {
+            mbar_expect_tx(bfull(x), uint32_t(bbytes));
+            const uint8_t* src = args.bmat + size_t(a) * size_t(bbytes);
+            for (int o = 0; o < bbytes; o += 16384)
+              bulk_load(b_addr0 + uint32_t(x * bbytes + o), src + o, uint32_t(min(16384, bbytes - o)), bfull(x));
+            ++issued[x];
+          }
+        }
+      }
+      if (__shfl_sync(0xffffffffu, (warp == kLoaderWarp0 && lane == 0) ? int(*abort) : 0, 0)) break;
+      const int s = i % kASlots;
+      if (i >= kASlots && !warp_wait(aempty(s), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, lim)) break;
+      const DigitDesc d = args.digit[a];
+      const uint64_t* src = args.digits + (b * args.q_limbs + (d.prime0 - args.level)) * n + blk * kUnit;
+      uint8_t* at = a_tile0 + s * kATile;
+      constexpr int kPerThread = kUnit * KS * 2 / (32 * kLoaderWarps);
+      uint64_t w0[kPerThread], w1[kPerThread];
+#pragma unroll
+      for (int it = 0; it < kPerThread; ++it) {
+        const int idx = lt + it * 32 * kLoaderWarps;
+        const int m = idx & (kUnit - 1), r0 = 2 * (idx >> 7);
+        w0[it] = r0 < d.alpha ? __ldg(src + int64_t(r0) * n + m) : 0;
+        w1[it] = r0 + 1 < d.alpha ? __ldg(src + int64_t(r0 + 1) * n + m) : 0;
+      }
+#pragma unroll
+      for (int it = 0; it < kPerThread; ++it) {
+        const int idx = lt + it * 32 * kLoaderWarps;
+        const int m = idx & (kUnit - 1), r2 = idx >> 7;
+        *reinterpret_cast<ulonglong2*>(at + (m >> 3) * kSbo + r2 * 128 + (m & 7) * 16) =
+            make_ulonglong2(w0[it], w1[it]);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(afull(s));
+    }
+    // after an abort, wait (bounded, default limit) for byte-matrix copies still in flight
+    if (bthread && *abort)
+      for (int x = 0; x < 2; ++x)
+        if (issued[x] > 0) mbar_wait(bfull(x), (issued[x] - 1) & 1, nullptr, args.err, kWaitNs);
+  } else if (warp == kMmaWarp && lane == 0) {
+    int cur = -1, dseq = -1, t = 0;
+    bool ok = true;
+    for (int i = 0; i < nu && ok; ++i) {
+      int a;
+      int64_t b, blk;
+      unit_of(i, a, b, blk);
+      if (a != cur) {
+        if (dseq >= 0) mma_commit(bempty(dseq & 1));  // the previous digit's byte matrix may be overwritten
+        cur = a;
+        ++dseq;
+        if (!mbar_wait(bfull(dseq & 1), (dseq >> 1) & 1, abort, args.err, lim)) break;
+      }
+      const int s = i % kASlots;
+      if (!mbar_wait(afull(s), (i / kASlots) & 1, abort, args.err, lim)) break;
+      tc_fence_after();
+      const uint32_t a_base = a_addr0 + uint32_t(s * kATile);
+      const uint32_t b_base = b_addr0 + uint32_t((dseq & 1) * bbytes);
+      for (int c = 0; c < args.nchunks; ++c, ++t) {
+        const int slot = t % kAccSlots;
+        if (t >= kAccSlots && !mbar_wait(accempty(slot), ((t / kAccSlots) & 1) ^ 1, abort, args.err, lim)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int rows = min(kChunkRows, args.qp_limbs - c * kChunkRows);
+        const uint32_t idesc = instr_desc_u8(uint32_t((rows * 8 + 15) & ~15));
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks)
+          mma_i8(tmem + uint32_t(slot * kAccCols), smem_desc(a_base + ks * 256, 128, kSbo),
+                 smem_desc(b_base + uint32_t(c * kBTile + ks * 256), 128, kSbo), idesc, ks > 0 ? 1u : 0u);
+        mma_commit(accfull(slot));
+      }
+      if (ok) mma_commit(aempty(s));
+    }
+  } else if (warp < kEpilogueWarps) {
+    const int quarter = warp & 3, grp = warp >> 2;
+    const int m = quarter * 32 + lane;
+    const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
+    int t = 0;
+    // test only: a wait that must run out (its limit is the pipeline's)
+    bool ok = !args.stall || warp_wait(never_bar, 0, abort, args.err, lane, lim);
+    for (int i = 0; i < nu && ok; ++i) {
+      int a;
+      int64_t b, blk;
+      unit_of(i, a, b, blk);
+      const DigitDesc d = args.digit[a];
+      const int own0 = args.skip_own ? d.prime0 - args.level : 0, own1 = args.skip_own ? own0 + d.alpha : 0;
+      uint64_t* dst = args.ext + (int64_t(a) * args.batch + b) * args.qp_limbs * n + blk * kUnit + m;
+      for (int c = 0; c < args.nchunks; ++c, ++t) {
+        const int slot = t % kAccSlots;
+        if (!warp_wait(accfull(slot), (t / kAccSlots) & 1, abort, args.err, lane, lim)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        uint32_t acc[32];
+        tmem_ld32(tmem + lane_addr + uint32_t(slot * kAccCols + grp * 32), acc);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(accempty(slot));
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int j = c * kChunkRows + grp * 4 + jj;
+          if (j >= args.qp_limbs || (j >= own0 && j < own1)) continue;
+          const ulonglong2 pi = __ldg(reinterpret_cast<const ulonglong2*>(args.pinfo) + args.level + j);
+          dst[int64_t(j) * n] = recombine_redc(acc + 8 * jj, pi.x, pi.y);
+        }
+      }
+    }
+  }
+
+  __syncthreads();
+  // Drain the MMAs (and the arrivals they signal) before TMEM is freed; the
+  // drain keeps the default limit whatever the pipeline's.
+  if (warp == kMmaWarp && lane == 0) {
+    mma_commit(drain_bar);
+    mbar_wait(drain_bar, 0, nullptr, args.err, kWaitNs);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+}  // namespace tcb
+
+// ------------------------------------------------------------------ host ---
+namespace {
+using u128 = unsigned __int128;
+
+// K-steps of 32 bytes for digits of up to `alpha` primes.
+int ksteps_for(int alpha) { return alpha <= 4 ? 1 : 2; }
+
+int chunks_for(int qp_limbs) { return (qp_limbs + tcb::kChunkRows - 1) / tcb::kChunkRows; }
+
+int smem_for(int nchunks, int ks) {
+  const int k = 32 * ks;
+  const int need = 1024 + 2 * nchunks * 128 * k + tcb::kASlots * tcb::kUnit * k + tcb::kBarrierBytes;
+  return need > tcb::kMinSmem ? need : tcb::kMinSmem;
+}
+}  // namespace
+
+// Byte matrices of one level (host): for each active digit, chunk c and
+// destination row j = 16 c + jl, MMA row n = 8 jl + e, K position
+// kap = 8 r + u holds byte e of 2^{8u} 2^64 (M_r mod p_{level+j}) mod p.
+// Layout per chunk: K-major canonical tile of 128 rows x K bytes.
+void tc_basis_tables_host(const Context& c, int level, int ks, std::vector<uint8_t>& out) {
+  const int k = 32 * ks, sbo = k / 16 * 128, tile = 128 * k;
+  const int qpl = c.qp() - level, nch = chunks_for(qpl);
+  const std::vector<DigitDesc>& dd = c.level_digits[level];
+  out.assign(dd.size() * size_t(nch) * tile, 0);
+  for (size_t a = 0; a < dd.size(); ++a) {
+    for (int j = 0; j < qpl; ++j) {
+      const uint64_t p = c.moduli[level + j];
+      uint8_t* t = out.data() + (a * nch + j / tcb::kChunkRows) * size_t(tile);
+      const int jl = j % tcb::kChunkRows;
+      uint64_t mr = 1 % p;  // M_r mod p, r = 0, 1, ...
+      for (int r = 0; r < dd[a].alpha; ++r) {
+        if (r > 0) mr = uint64_t((u128)mr * (c.moduli[dd[a].prime0 + r - 1] % p) % p);
+        for (int u = 0; u < 8; ++u) {
+          const uint64_t scaled = uint64_t((u128(uint64_t((u128(mr) << (8 * u)) % p)) << 64) % p);
+          const int kap = 8 * r + u;
+          for (int e = 0; e < 8; ++e) t[jl * sbo + (kap >> 4) * 128 + e * 16 + (kap & 15)] = uint8_t(scaled >> (8 * e));
+        }
+      }
+    }
+  }
+}
+
+int tc_basis_prepare(Context& c) {
+  std::lock_guard<std::mutex> lock(c.tcb_mutex);
+  if (c.tcb) return 0;
+  if (c.bits != 64) return fail(-7, "the tensor-core basis conversion needs an int64 context");
+  if (c.log_n < 7) return fail(-7, "ring too small for the tensor-core basis conversion");
+  const int ks = ksteps_for(c.num_p);
+  if (smem_for(chunks_for(c.qp()), ks) > 227 * 1024)
+    return fail(-7, "the chain is too long for the tensor-core basis conversion's shared-memory tables");
+  auto* t = new TcBasisTables();
+  t->ks = ks;
+  std::vector<void*> mine;
+  auto dev_alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    mine.push_back(p);
+    return p;
+  };
+  auto give_up = [&](const char* where) {
+    cudaError_t e = cudaGetLastError();
+    for (void* p : mine) cudaFree(p);
+    delete t;
+    return e != cudaSuccess ? cuda_status(e, where) : fail(-6, std::string("out of memory: ") + where);
+  };
+  std::vector<uint8_t> host;
+  t->bmat.assign(c.num_q, nullptr);
+  for (int level = 0; level < c.num_q; ++level) {
+    tc_basis_tables_host(c, level, ks, host);
+    t->bmat[level] = static_cast<uint8_t*>(dev_alloc(host.size()));
+    if (!t->bmat[level] || cudaMemcpy(t->bmat[level], host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return give_up("tensor-core basis conversion byte matrices");
+  }
+  std::vector<uint64_t> pinfo(2 * size_t(c.qp()));
+  for (int j = 0; j < c.qp(); ++j) {
+    const uint64_t p = c.moduli[j];
+    uint64_t x = 1;  // p^{-1} mod 2^64 by Newton iteration
+    for (int i = 0; i < 6; ++i) x *= 2 - p * x;
+    pinfo[2 * j] = p;
+    pinfo[2 * j + 1] = 0 - x;
+  }
+  t->pinfo = static_cast<uint64_t*>(dev_alloc(pinfo.size() * 8));
+  t->err = static_cast<int*>(dev_alloc(sizeof(int)));
+  if (!t->pinfo || !t->err ||
+      cudaMemcpy(t->pinfo, pinfo.data(), pinfo.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(t->err, 0, sizeof(int)) != cudaSuccess)
+    return give_up("tensor-core basis conversion constants");
+  if (cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess || t->sms < 1)
+    return give_up("multiprocessor count");
+  for (void* p : mine) c.allocations.push_back(p);
+  c.tcb = t;
+  return 0;
+}
+
+int64_t tc_ext_words(const Context& c, int64_t batch, int level) {
+  return int64_t(c.level_digits[level].size()) * batch * (c.qp() - level) * c.n();
+}
+
+int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st) {
+  if (int rc = tc_basis_prepare(c)) return rc;
+  const TcBasisTables& t = *c.tcb;
+  const int nd = int(c.level_digits[level].size());
+  if (batch == 0 || nd == 0) return 0;
+  const int qpl = c.qp() - level, nch = chunks_for(qpl);
+  const int smem = smem_for(nch, t.ks);
+  auto kern = t.ks == 1 ? tcb::k_tc_extend<1> : tcb::k_tc_extend<2>;
+  if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return rc;
+  const int64_t units = int64_t(nd) * batch * (c.n() / tcb::kUnit);
+  const int grid = int(units < t.sms ? units : t.sms);
+  tcb::ExtendArgs a{static_cast<const uint64_t*>(digits), static_cast<uint64_t*>(ext), t.bmat[level], t.pinfo,
+                    c.lv64[level].digits, batch, level, c.num_q - level, qpl, nd, nch, c.log_n,
+                    skip_own ? 1 : 0, t.err, c.tc_wait_ns ? c.tc_wait_ns : tc::kWaitNs, c.tc_test_stall};
+  kern<<<grid, tcb::kThreads, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "k_tc_extend");
+}
+
+int tc_basis_status(Context& c, int* flag) {
+  std::lock_guard<std::mutex> lock(c.tcb_mutex);
+  *flag = 0;
+  if (!c.tcb) return 0;
+  if (cudaError_t e = cudaMemcpy(flag, c.tcb->err, sizeof(int), cudaMemcpyDeviceToHost)) return cuda_status(e, "flag");
+  return cuda_status(cudaMemset(c.tcb->err, 0, sizeof(int)), "flag reset");
+}
+
+}  // namespace fhb

@@ -56,9 +56,11 @@
 #include <vector>
 
 #include "fhb_context.h"
+#include "fhb_tc_common.cuh"
 
 namespace fhb {
 namespace tcntt {
+using namespace fhb::tc;
 
 constexpr int kLogN = 16;
 constexpr int kPolyWords = 1 << kLogN;
@@ -69,7 +71,6 @@ constexpr int kTransposeWarp0 = 8;        // warps 8..11
 constexpr int kTransposeWarps = 4;
 constexpr int kProducerWarp = 12;
 constexpr int kMmaWarp = 13;
-constexpr unsigned long long kWaitNs = 1000000000ull;
 
 // Pass geometry: NK = outputs (and inputs) per instance.
 template <int NK>
@@ -101,131 +102,15 @@ constexpr int smem_bytes() {
 }
 template <int NK>
 constexpr int num_barriers() {
-  return 2 + 2 * (Geom<NK>::kRawSlots + Geom<NK>::kASlots + Geom<NK>::kAccSlots);
+  return 3 + 2 * (Geom<NK>::kRawSlots + Geom<NK>::kASlots + Geom<NK>::kAccSlots);
 }
 static_assert(8 * num_barriers<16>() + 8 <= kBarrierBytes && 8 * num_barriers<64>() + 8 <= kBarrierBytes,
               "barrier area");
 static_assert(smem_bytes<64>() <= 232448, "shared memory per CTA");
 
-// tcgen05 instruction descriptor: D int32 (c_format 2 at bit 4), A and B
-// unsigned 8-bit (formats 0), both K-major, N (N >> 3 at bit 17), M = 128
-// (M >> 4 at bit 24).
-constexpr uint32_t instr_desc(uint32_t n) { return (2u << 4) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
+constexpr uint32_t instr_desc(uint32_t n) { return tc::instr_desc_u8(n); }
 
 // ---------------------------------------------------------------- device ---
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait for the phase of `parity` to complete.  Returns false when
-// the CTA aborted (abort != nullptr) or about one second passed; the latter
-// raises the abort flag and the device error flag.  The global timer is read
-// only every 1024 polls: the common case is a barrier that completes within
-// a few polls.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort, int* err) {
-  if (mbar_test(bar, parity)) return true;
-  unsigned long long t0 = 0;
-  for (uint32_t it = 1;; ++it) {
-    if (mbar_test(bar, parity)) return true;
-    if (abort && *abort) return false;
-    if ((it & 1023) == 0) {
-      const unsigned long long t = global_ns();
-      if (t0 == 0) {
-        t0 = t;
-      } else if (t - t0 > kWaitNs) {
-        if (abort) *abort = 1;
-        atomicExch(err, 1);
-        return false;
-      }
-    }
-  }
-}
-
-// A warp-uniform bounded wait: lane 0 polls and broadcasts the verdict, so
-// warp-collective instructions after it run with all 32 lanes or none.
-__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, volatile int* abort, int* err, int lane) {
-  return __shfl_sync(0xffffffffu, lane == 0 ? mbar_wait(bar, parity, abort, err) : false, 0);
-}
-
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-
-// Shared-memory matrix descriptor, no swizzle, K-major canonical layout:
-// core matrices of 8 rows x 16 bytes (128 contiguous bytes); `lbo` = byte
-// distance between the two K-adjacent core matrices of an MMA, `sbo` = byte
-// distance between 8-row groups.  Version 1 (bit 46) for sm_100.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
-         (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                       uint32_t accumulate) {
-  const uint32_t mask = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
-      ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(mask));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[16]) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-               : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
 // Byte transpose of four words: out[d] = byte d of v0 | byte d of v1 << 8 |
 // byte d of v2 << 16 | byte d of v3 << 24.
 __device__ __forceinline__ void byte_transpose(uint32_t v0, uint32_t v1, uint32_t v2, uint32_t v3,
@@ -273,6 +158,8 @@ struct PassArgs {
   int row_start;
   int ctas_per_row;
   int* err;
+  unsigned long long wait_ns;         // limit of the pipeline waits (drain waits keep kWaitNs)
+  int stall;                          // test only: the epilogue first waits on a barrier nothing completes
 };
 
 // in == out is allowed: a unit's outputs occupy exactly the words its raw
@@ -303,6 +190,7 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
   auto accf_bar = [&](int b) { return bar0 + 8u * (1 + 2 * kRawSlots + 2 * kASlots + b); };
   auto acce_bar = [&](int b) { return bar0 + 8u * (1 + 2 * kRawSlots + 2 * kASlots + kAccSlots + b); };
   const uint32_t drain_bar = bar0 + 8u * (num_barriers<NK>() - 1);
+  const uint32_t never_bar = bar0 + 8u * (num_barriers<NK>() - 2);  // nothing arrives on it
   uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + num_barriers<NK>());
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -333,6 +221,7 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
       mbar_init(acce_bar(b), kEpilogueWarps);
     }
     mbar_init(drain_bar, 1);
+    mbar_init(never_bar, 1);
     *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -356,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     int i = 0;
     for (; i < nu; ++i) {
       const int r = i % kRawSlots, use = i / kRawSlots;
-      if (i >= kRawSlots && !mbar_wait(rawe_bar(r), (use & 1) ^ 1, abort, args.err)) break;
+      if (i >= kRawSlots && !mbar_wait(rawe_bar(r), (use & 1) ^ 1, abort, args.err, args.wait_ns)) break;
       const uint32_t* src = args.in + unit_poly(i) * int64_t(kPolyWords) + inst_offset<KIND>(unit_m0(i));
       const uint32_t dst = rawbuf_addr + r * G::kRawBytes;
       mbar_expect_tx(rawf_bar(r), G::kRawBytes);
@@ -370,9 +259,9 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     }
     // after an abort, wait (bounded) for the copies still in flight
     if (*abort) {
-      mbar_wait(bfull_bar, 0, nullptr, args.err);
+      mbar_wait(bfull_bar, 0, nullptr, args.err, kWaitNs);
       for (int t = i - kRawSlots < 0 ? 0 : i - kRawSlots; t < i; ++t)
-        mbar_wait(rawf_bar(t % kRawSlots), (t / kRawSlots) & 1, nullptr, args.err);
+        mbar_wait(rawf_bar(t % kRawSlots), (t / kRawSlots) & 1, nullptr, args.err, kWaitNs);
     }
   } else if (warp >= kTransposeWarp0 && warp < kTransposeWarp0 + kTransposeWarps) {
     // raw words -> byte planes.  A thread unit = (instance, 4 consecutive k);
@@ -382,8 +271,9 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);  // (8-instance group, 16-k group)
     for (int i = 0; i < nu; ++i) {
       const int b = i % kASlots, r = i % kRawSlots;
-      if (!warp_wait(rawf_bar(r), (i / kRawSlots) & 1, abort, args.err, lane)) break;
-      if (i >= kASlots && !warp_wait(ae_bar(b), ((i / kASlots) & 1) ^ 1, abort, args.err, lane)) break;
+      if (!warp_wait(rawf_bar(r), (i / kRawSlots) & 1, abort, args.err, lane, args.wait_ns)) break;
+      if (i >= kASlots && !warp_wait(ae_bar(b), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, args.wait_ns))
+        break;
       const uint32_t* raw = rawbuf + r * (G::kRawBytes / 4);
       uint8_t* at = a_tile + b * G::kABytes;
       for (int wu = tw; wu < kWarpUnits; wu += kTransposeWarps) {
@@ -421,11 +311,12 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     }
   } else if (warp == kMmaWarp && lane == 0) {
     constexpr uint32_t kIdesc = instr_desc(G::kNmma);
-    bool ok = mbar_wait(bfull_bar, 0, abort, args.err);
+    bool ok = mbar_wait(bfull_bar, 0, abort, args.err, args.wait_ns);
     for (int i = 0; i < nu && ok; ++i) {
       const int b = i % kASlots, c = i % kAccSlots;
-      if (!mbar_wait(af_bar(b), (i / kASlots) & 1, abort, args.err) ||
-          (i >= kAccSlots && !mbar_wait(acce_bar(c), ((i / kAccSlots) & 1) ^ 1, abort, args.err))) {
+      if (!mbar_wait(af_bar(b), (i / kASlots) & 1, abort, args.err, args.wait_ns) ||
+          (i >= kAccSlots &&
+           !mbar_wait(acce_bar(c), ((i / kAccSlots) & 1) ^ 1, abort, args.err, args.wait_ns))) {
         ok = false;
         break;
       }
@@ -468,7 +359,9 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     constexpr bool kAhead = kHalf <= 8;
     uint32_t tws_next[kHalf];
     if (POST && kAhead && nu > 0) load_tw(post + inst_offset<KIND>(unit_m0(0) + ml), tws_next);
-    for (int i = 0; i < nu; ++i) {
+    // test only: a wait that must run out (its limit is the pipeline's)
+    const bool stalled = args.stall && !warp_wait(never_bar, 0, abort, args.err, lane, args.wait_ns);
+    for (int i = 0; i < nu && !stalled; ++i) {
       const int b = i % kAccSlots;
       const int off = inst_offset<KIND>(unit_m0(i) + ml);
       uint32_t* dst = args.out + unit_poly(i) * int64_t(kPolyWords) + off;
@@ -482,7 +375,7 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
           load_tw(post + off, tws);
         }
       }
-      if (!warp_wait(accf_bar(b), (i / kAccSlots) & 1, abort, args.err, lane)) break;
+      if (!warp_wait(accf_bar(b), (i / kAccSlots) & 1, abort, args.err, lane, args.wait_ns)) break;
       tc_fence_after();
 #pragma unroll
       for (int cc = 0; cc < kHalf / kChunk; ++cc) {
@@ -530,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
   // Drain the MMAs (and the arrivals they signal) before TMEM is freed.
   if (warp == kMmaWarp && lane == 0) {
     mma_commit(drain_bar);
-    mbar_wait(drain_bar, 0, nullptr, args.err);
+    mbar_wait(drain_bar, 0, nullptr, args.err, kWaitNs);
   }
   tc_fence_before();
   __syncthreads();
@@ -717,7 +610,7 @@ int launch_pass(const Context& c, const uint32_t* in, uint32_t* out, int pass, i
   if (per_row > units) per_row = units;
   if (per_row < 1) per_row = 1;
   PassArgs a{in, out, c.tc->bmat[pass], POST ? c.tc->post[pass] : nullptr, c.tc->qinfo, batch, rows,
-             row_start, int(per_row), c.tc->err};
+             row_start, int(per_row), c.tc->err, c.tc_wait_ns ? c.tc_wait_ns : kWaitNs, c.tc_test_stall};
   kern<<<dim3(unsigned(rows * per_row)), kThreads, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "k_tc_ntt_pass");
 }

@@ -40,7 +40,8 @@ class CkksEngine:
     def __init__(self, ckks_config: CkksConfig | Preset | dict | str | None = None, *,
                  device: torch.device | str | None = None, allow_sk_gen: bool = True,
                  galois_generator: int = 3, ntt_backend: str | None = None, rng_seed: int | None = None,
-                 rng_nonce: int | None = None, encode_rounding: str = "stochastic"):
+                 rng_nonce: int | None = None, encode_rounding: str = "stochastic",
+                 basis_conversion: str = "cuda_cores"):
         if ckks_config is None:
             ckks_config = Preset.slots16384_scale40_levels16_int64
         if isinstance(ckks_config, (Preset, str, dict)):
@@ -83,6 +84,26 @@ class CkksEngine:
         self._rotation_keys = RotationKeySet()
         self._scratch: torch.Tensor | None = None
         self.level_digits = self._digit_layout()
+        self.basis_conversion = basis_conversion
+
+    # ------------------------------------------------------------------
+    # arithmetic form of the key switch's basis conversion
+    # ------------------------------------------------------------------
+    _BASIS_FORMS = {"cuda_cores": nat.BASIS_CUDA_CORES, "tensor_cores": nat.BASIS_TENSOR_CORES}
+
+    @property
+    def basis_conversion(self) -> str:
+        """Where the key switch's exact basis extension runs: ``"cuda_cores"``
+        (fused into the key-switch core) or ``"tensor_cores"`` (int8 tcgen05
+        MMAs, int64 chains).  Results are bit-identical; no counterpart in
+        the reference, whose basis conversion is CUDA-core only."""
+        return "tensor_cores" if self.ctx.get_tuning(nat.TUNE_BASIS_CONVERSION) else "cuda_cores"
+
+    @basis_conversion.setter
+    def basis_conversion(self, form: str) -> None:
+        if form not in self._BASIS_FORMS:
+            raise ValueError("basis_conversion must be 'cuda_cores' or 'tensor_cores'")
+        self.ctx.set_tuning(nat.TUNE_BASIS_CONVERSION, self._BASIS_FORMS[form])
 
     # ------------------------------------------------------------------
     # layout

@@ -73,9 +73,31 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * FHB_TUNE_NTT_FORWARD_EPT / FHB_TUNE_NTT_INVERSE_EPT: residues per thread of
  * the standalone forward / inverse NTT (and of the fused HMult -> inverse
  * NTT): 8 = radix-8 register passes, 16 = radix-16 passes over half the
- * threads, 0 = the ring's default.  Results do not depend on any of these.
- * No counterpart in the reference (its launch shapes are fixed). */
-enum fhb_tuning_param { FHB_TUNE_KS_ORDER = 0, FHB_TUNE_NTT_FORWARD_EPT = 1, FHB_TUNE_NTT_INVERSE_EPT = 2 };
+ * threads, 0 = the ring's default.
+ * FHB_TUNE_BASIS_CONVERSION: 0 = the key switch's exact basis extension on
+ * the CUDA cores, fused into the key-switch core (default); 1 = on the int8
+ * tensor cores (int64 contexts; fhb_tc_basis_extend), the core then reads the
+ * materialised extensions (key-switch scratch grows by
+ * fhb_tc_basis_extend_words x 8 bytes).  Setting 1 builds its tables
+ * (blocking).
+ * FHB_TUNE_TC_WAIT_US: limit of the tensor-core kernels' pipeline waits in
+ * microseconds (0 = the default second); a wait that runs out makes the
+ * kernel return early and raise its status flag (fhb_tc_basis_status,
+ * fhb_tc_ntt_status).  Their drain waits keep the default.  For tests.
+ * FHB_TUNE_TC_TEST_STALL: 1 = every tensor-core launch first waits on a
+ * barrier that nothing completes, so its pipeline limit runs out and the
+ * abort path (drain, TMEM release, status flag) runs; outputs are then
+ * invalid.  For tests of that path only.
+ * Results do not depend on any of these (stall aside).  No counterpart in the reference
+ * (its launch shapes and arithmetic units are fixed). */
+enum fhb_tuning_param {
+  FHB_TUNE_KS_ORDER = 0,
+  FHB_TUNE_NTT_FORWARD_EPT = 1,
+  FHB_TUNE_NTT_INVERSE_EPT = 2,
+  FHB_TUNE_BASIS_CONVERSION = 3,
+  FHB_TUNE_TC_WAIT_US = 4,
+  FHB_TUNE_TC_TEST_STALL = 5
+};
 int fhb_context_set_tuning(fhb_context* ctx, int param, int value);
 int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);
 
@@ -118,6 +140,20 @@ int fhb_tc_forward_ntt(const fhb_context* ctx, const void* in, void* out, int64_
 int fhb_tc_inverse_ntt(const fhb_context* ctx, const void* in, void* out, int64_t batch, int rows,
                        int row_start, fhb_stream stream);
 int fhb_tc_ntt_status(const fhb_context* ctx, int* flag);
+
+/* Exact int8 tensor-core basis extension (int64 contexts): from the Garner
+ * digits [batch, L, N] of fhb_ckks_modup_digits, ext [D_l, batch, L+P, N]
+ * receives, for every active hybrid digit, its exact extension
+ * sum_r d_r (M_r mod p) to every row of Q_l P, in [0, 2p)
+ * (fhb_tc_basis_extend_words words).  Equals, modulo p, the reference's
+ * mixed_radix_basis_extend_to_montgomery without the Montgomery factor
+ * (csrc/ops/rns/cuda/mixed_radix_cuda.cu:146-182).  fhb_tc_basis_status
+ * synchronises, returns in *flag whether a bounded wait of the kernel gave
+ * up since the last call (outputs then invalid), and clears the flag. */
+int fhb_tc_basis_extend(const fhb_context* ctx, const void* digits, void* ext, int64_t batch, int level,
+                        fhb_stream stream);
+int64_t fhb_tc_basis_extend_words(const fhb_context* ctx, int64_t batch, int level);
+int fhb_tc_basis_status(const fhb_context* ctx, int* flag);
 int fhb_tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint32_t* post);
 
 /* Inverse NTT from NTT/Montgomery lazy input, output per fhb_inverse_output.
@@ -161,6 +197,13 @@ int fhb_ckks_modup_digits(const fhb_context* ctx, const void* comp, void* digits
  * 530-546; csrc/ops/ckks/cuda/keyswitch_cuda.cu:198-292). */
 int fhb_ckks_keyswitch_core(const fhb_context* ctx, const void* digits, const void* key, void* acc0,
                             void* acc1, int64_t batch, int level, fhb_stream stream);
+
+/* The key-switch core of the tensor-core form: as fhb_ckks_keyswitch_core,
+ * but from the digit extensions of fhb_tc_basis_extend ([D_l, batch, L+P, N],
+ * int64 contexts) instead of the Garner digits, so the core only transforms,
+ * multiplies by the key and accumulates.  Same result. */
+int fhb_ckks_keyswitch_core_extended(const fhb_context* ctx, const void* ext, const void* key, void* acc0,
+                                     void* acc1, int64_t batch, int level, fhb_stream stream);
 
 /* ModDown by P, fused with the final addition and optionally the rescale.
  * t0, t1 [batch, L + P, N] canonical; add0, add1 [batch, L, N] canonical or

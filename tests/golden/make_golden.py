@@ -3,7 +3,7 @@
 Run in a checkout where the reference sources exist (FHELIUM_REFERENCE,
 default /root/reference) after `bash oracle/build_ref.sh`:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [names of the fixtures to regenerate]
 
 It copies the reference's Python package to a scratch directory, installs the
 reference's CPU operators compiled from its own sources (oracle/_ref) as the
@@ -62,10 +62,12 @@ class ChaCha20Rng:
 '''
 
 CASES = [
-    # (name, preset, overrides, generator)
-    ("logn14_int64", "slots8192_scale40_levels7_int64", {}, 3),
-    ("logn14_int32", "slots8192_scale25_levels14_int32", {}, 3),
-    ("logn14_int64_gen5", "slots8192_scale40_levels7_int64", {}, 5),
+    # (name, preset, overrides, generator, levels)
+    ("logn14_int64", "slots8192_scale40_levels7_int64", {}, 3, (0, 3)),
+    ("logn14_int32", "slots8192_scale25_levels14_int32", {}, 3, (0, 3)),
+    ("logn14_int64_gen5", "slots8192_scale40_levels7_int64", {}, 5, (0, 3)),
+    # the benchmarked preset: N = 2^16, L = 35 at level 0, 10 hybrid digits
+    ("logn16_int64", "slots32768_scale40_levels34_int64", {}, 3, (0, 30)),
 ]
 
 
@@ -103,7 +105,7 @@ def _record(out, moduli, prime_ids):
     return {"digest": digest(c), "shape": list(c.shape), "head": c.reshape(-1, c.shape[-1])[:4, :2].tolist()}
 
 
-def generate_case(fh, name, preset, overrides, generator):
+def generate_case(fh, name, preset, overrides, generator, levels):
     from fhelium.config import CkksConfig, Preset
     from fhelium.core import Ciphertext, RelinearizationKey, RotationKey
 
@@ -130,7 +132,7 @@ def generate_case(fh, name, preset, overrides, generator):
     rot_steps = [1, -1, 8, 2, 5]
     for i, s in enumerate(rot_steps):
         eng.set_rotation_key(key(910 + i, RotationKey, rotation_step=s))
-    for level in (0, 3):
+    for level in levels:
         ids = list(range(level, nq))
         # forward NTT of a coefficient ciphertext
         seed = 100 + level
@@ -185,8 +187,14 @@ def main() -> int:
         import fhelium as fh
         torch.set_num_threads(os.cpu_count() or 1)
         fixtures = {}
-        for name, preset, overrides, gen in CASES:
-            fixtures[name] = generate_case(fh, name, preset, overrides, gen)
+        only = set(sys.argv[1:])
+        path = os.path.join(HERE, "engine_golden.json")
+        if only and os.path.exists(path):  # regenerate the named fixtures, keep the others
+            fixtures.update(json.load(open(path))["fixtures"])
+        for name, preset, overrides, gen, levels in CASES:
+            if only and name not in only:
+                continue
+            fixtures[name] = generate_case(fh, name, preset, overrides, gen, levels)
             print(name, len(fixtures[name]["cases"]), "cases")
         meta = {"generator": "tests/golden/make_golden.py", "reference": "visualDust/fhelium 0.10.0",
                 "key_seeds": {"relinearization": 900, "rotation": {"1": 910, "-1": 911, "8": 912, "2": 913, "5": 914}}}

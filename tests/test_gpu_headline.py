@@ -6,6 +6,8 @@ Keys are the engine's own (GPU key generation), ciphertexts are the engine's
 own encryptions of uniform [-0.05, 0.05] messages, and the default key-switch
 work order (one destination row across groups of four ciphertexts) is used
 with a batch of 5, so both its full-group and its partial-group branches run.
+Every case runs with the basis conversion on the CUDA cores and on the int8
+tensor cores.
 
 Checks, as the reference checks CPU against CUDA residues
 (tests/test_ckks_operation_correctness.py:256-401 of the reference):
@@ -31,6 +33,7 @@ pytestmark = pytest.mark.gpu
 
 BATCH = 5
 HOISTED_STEPS = list(range(1, 17))
+FORMS = ["cuda_cores", "tensor_cores"]
 
 
 @pytest.fixture(scope="module")
@@ -62,9 +65,11 @@ def hmult_oracle(headline):
     return a, b, key, np.stack(want, axis=1)
 
 
-def test_headline_hmult_relin_rescale_bit_exact(headline, hmult_oracle):
+@pytest.mark.parametrize("form", FORMS)
+def test_headline_hmult_relin_rescale_bit_exact(headline, hmult_oracle, form):
     h = headline
     eng = h["eng"]
+    eng.basis_conversion = form
     a, b, key, want = hmult_oracle
     na, nb = eng.coefficient_domain_to_ntt_domain(h["ca"]), eng.coefficient_domain_to_ntt_domain(h["cb"])
     got = eng.multiply_relinearize_rescale(na, nb, h["rlk"])
@@ -89,10 +94,12 @@ def test_headline_hmult_matches_reference_operators(headline, hmult_oracle):
     np.testing.assert_array_equal(ref, want[:, 0])
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("step", [1, -1])
-def test_headline_rotation_bit_exact(headline, step):
+def test_headline_rotation_bit_exact(headline, step, form):
     h = headline
     eng, orc = h["eng"], h["orc"]
+    eng.basis_conversion = form
     ct = h["ca"]
     got = eng.rotate_by_step(ct, step)
     key = to_np(eng.rotation_key(step).data)
@@ -101,14 +108,22 @@ def test_headline_rotation_bit_exact(headline, step):
     np.testing.assert_array_equal(to_np(got.data)[:, :2], want)
 
 
-def test_headline_hoisted_rotations_bit_exact(headline):
-    """Steps 1..16 sharing one ModUp, against the oracle's hoisted rotation
-    (the reference's hoisting, fhelium/engine/hybrid_keyswitch.py:373-469)."""
+@pytest.fixture(scope="module")
+def hoisted_oracle(headline):
     h = headline
     eng, orc = h["eng"], h["orc"]
     ct = Ciphertext(h["ca"].data[:, :1].contiguous(), 0, h["ca"].scale)
-    got = eng.rotate_many_by_steps(ct, HOISTED_STEPS)
     keys = {s: to_np(eng.rotation_key(s).data) for s in HOISTED_STEPS}
-    want = orc.rotate_hoisted(to_np(ct.data)[:, 0], HOISTED_STEPS, keys, 0)
+    return ct, orc.rotate_hoisted(to_np(ct.data)[:, 0], HOISTED_STEPS, keys, 0)
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_headline_hoisted_rotations_bit_exact(headline, hoisted_oracle, form):
+    """Steps 1..16 sharing one ModUp, against the oracle's hoisted rotation
+    (the reference's hoisting, fhelium/engine/hybrid_keyswitch.py:373-469)."""
+    eng = headline["eng"]
+    eng.basis_conversion = form
+    ct, want = hoisted_oracle
+    got = eng.rotate_many_by_steps(ct, HOISTED_STEPS)
     for s, g, w in zip(HOISTED_STEPS, got, want):
         np.testing.assert_array_equal(to_np(g.data)[:, 0], w, err_msg=f"step {s}")
