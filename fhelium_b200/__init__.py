@@ -7,8 +7,8 @@ state literals and the value-file functions."""
 from typing import Literal
 
 from .config import CkksConfig, Preset
-from .values import (COMPRESSED_PLAINTEXT_FORMAT_VERSION, Ciphertext, CompressedPlaintext, EvaluationKeyRequirements,
-                     EvaluationKeySet, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey, RotationKey,
+from .values import (COMPRESSED_PLAINTEXT_FORMAT_VERSION, Ciphertext, CompressedPlaintext, EncryptionDraws,
+                     EvaluationKeyRequirements, EvaluationKeySet, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey, RotationKey,
                      RotationKeySet, SecretKey)
 
 # state literals (fhelium/core/state.py:10-21)
@@ -24,7 +24,7 @@ ConjugationKey = RotationKey
 __all__ = ["CkksConfig", "Preset", "CkksEngine", "Ciphertext", "Plaintext", "CompressedPlaintext",
            "CompressedPlaintextLayout", "COMPRESSED_PLAINTEXT_FORMAT_VERSION", "SecretKey", "PublicKey",
            "KeySwitchKey", "RelinearizationKey", "RotationKey", "ConjugationKey", "RotationKeySet",
-           "EvaluationKeySet", "EvaluationKeyRequirements",
+           "EvaluationKeySet", "EvaluationKeyRequirements", "EncryptionDraws",
            "PlaintextRepresentation", "PolynomialDomain", "ModulusBasis", "ResidueRepresentation",
            "save_value", "load_value", "inspect_value"]
 

@@ -59,6 +59,8 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_rotate": (_I, [_P, _P, _P, _P, _P, _I64, _I64, _I, _U32, _P]),
     "fhb_ckks_rotate_multi": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _P]),
     "fhb_ckks_keyswitch_sum": (_I, [_P, _P, _P, _P, _P, _I, _I64, _I, _P]),
+    "fhb_ckks_keyswitch_sum_extended": (_I, [_P, _P, _P, _P, _P, _I, _I64, _I, _P]),
+    "fhb_ckks_decrypt_tail": (_I, [_P, _P, _P, _I64, _I, _P]),
     "fhb_ckks_bsgs_inner_product": (_I, [_P, _P, _I64, _P, _I64, _I, _P, _I, _I, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_monomial": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_modraise": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),

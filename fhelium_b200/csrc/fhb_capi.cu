@@ -115,8 +115,8 @@ int ks_core(const Context& c, const void* digits, const void* key, void* acc0, v
   FHB_DISPATCH(run_ks_core, c, digits, key, acc0, acc1, batch, level, st, item_keys, ct3, pre);
 }
 int ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
-           int64_t batch, int level, cudaStream_t st) {
-  FHB_DISPATCH(run_ks_sum, c, digits, key_ptrs, acc0, acc1, giants, batch, level, st);
+           int64_t batch, int level, cudaStream_t st, bool pre = false) {
+  FHB_DISPATCH(run_ks_sum, c, digits, key_ptrs, acc0, acc1, giants, batch, level, st, pre);
 }
 int prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st) {
   FHB_DISPATCH(run_prepare, c, digits, prepared, batch, level, st);
@@ -767,6 +767,53 @@ int fhb_ckks_keyswitch_sum(const fhb_context* ctx, const void* digits, const uin
   if (giants < 1 || batch < 0) return fail(-2, "need giants >= 1 and batch >= 0");
   TRY(fhb::check_level(c, level));
   return fhb::ks_sum(c, digits, key_ptrs, acc0, acc1, giants, batch, level, st);
+}
+
+int fhb_ckks_decrypt_tail(const fhb_context* ctx, const void* phase, double* out, int64_t batch, int level,
+                          fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(phase, "phase"));
+  if (!out) return fail(-2, "out is NULL");
+  TRY(fhb::check_level(c, level));
+  if (batch < 0) return fail(-2, "batch must be >= 0");
+  if (batch == 0) return 0;
+  using u128 = unsigned __int128;
+  const int limbs = c.num_q - level;
+  fhb::DecryptTail t{};
+  t.two = limbs >= 2;
+  t.qb = c.moduli[c.num_q - 1];
+  t.qb_one_s = uint64_t((u128(1) << 64) / t.qb);
+  if (t.two) {
+    t.qa = c.moduli[c.num_q - 2];
+    uint64_t inv = 1, base = t.qa % t.qb, e = t.qb - 2;  // q_a^{-1} mod q_b (q_b prime)
+    for (; e; e >>= 1, base = uint64_t(u128(base) * base % t.qb))
+      if (e & 1) inv = uint64_t(u128(inv) * base % t.qb);
+    t.inv = inv;
+    t.inv_s = uint64_t((u128(inv) << 64) / t.qb);
+    const u128 half = u128(t.qa) * t.qb / 2;
+    t.h0 = uint64_t(half % t.qa);
+    t.h1 = uint64_t(half / t.qa);
+  }
+  const int grid = fhb::elementwise_grid(batch << c.log_n);
+  if (c.bits == 64)
+    fhb::k_decrypt_tail<uint64_t><<<grid, 256, 0, st>>>(static_cast<const uint64_t*>(phase), out, batch, limbs,
+                                                         c.log_n, t);
+  else
+    fhb::k_decrypt_tail<uint32_t><<<grid, 256, 0, st>>>(static_cast<const uint32_t*>(phase), out, batch, limbs,
+                                                         c.log_n, t);
+  return fhb::cuda_status(cudaGetLastError(), "k_decrypt_tail");
+}
+
+int fhb_ckks_keyswitch_sum_extended(const fhb_context* ctx, const void* ext, const uint64_t* key_ptrs, void* acc0,
+                                    void* acc1, int giants, int64_t batch, int level, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(ext, "ext"));
+  TRY(fhb::check_ptr(acc0, "acc0"));
+  TRY(fhb::check_ptr(acc1, "acc1"));
+  if (!key_ptrs) return fail(-2, "key_ptrs is NULL");
+  if (giants < 1 || batch < 0) return fail(-2, "need giants >= 1 and batch >= 0");
+  TRY(fhb::check_level(c, level));
+  return fhb::ks_sum(c, ext, key_ptrs, acc0, acc1, giants, batch, level, st, true);
 }
 
 int fhb_ckks_bsgs_inner_product(const fhb_context* ctx, const void* rot, int64_t rot_stride, const void* pts,

@@ -602,8 +602,10 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
 // ModUp digits (sigma_g applied); key_ptrs: device array of G key addresses;
 // acc0/acc1: [B][QP_l][N].  Used for the giant steps of bootstrapping's
 // linear transforms (the reference rotates and adds each giant step,
-// fhelium/experimental/bootstrap/_linear.py:235-393).
-template <typename T, int LOGN>
+// fhelium/experimental/bootstrap/_linear.py:235-393).  PRE (tensor-core
+// form): `digits` holds the extensions of the giants' digits,
+// [D_l][giants x B][QP_l][N] (giant-major within a digit).
+template <typename T, int LOGN, bool PRE = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_sum(const T* __restrict__ digits, const unsigned long long* __restrict__ key_ptrs, T* __restrict__ acc0,
                 T* __restrict__ acc1, int giants, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
@@ -626,10 +628,16 @@ k_keyswitch_sum(const T* __restrict__ digits, const unsigned long long* __restri
     const T* key = reinterpret_cast<const T*>(key_ptrs[gi]);
     for (int a = 0; a < lt.num_digits; ++a) {
       const DigitDesc d = lt.digits[a];
-      ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
-                       qp0, d.alpha, LOGN, p.q, p.twice_q};
       T v[G::kE];
-      tw.forward_from(src, s, p, v);
+      if constexpr (PRE) {
+        RowSource<T, false> src{
+            digits + ((int64_t(a) * giants * batch + int64_t(gi) * batch + bi) * qp_limbs + jrow) * G::kN, 0, 0, p.q};
+        tw.forward_from(src, s, p, v);
+      } else {
+        ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN),
+                         lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid, qp0, d.alpha, LOGN, p.q, p.twice_q};
+        tw.forward_from(src, s, p, v);
+      }
       key_mac(acc, v, key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own,
               key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own, p);
     }
@@ -1130,6 +1138,63 @@ __global__ void k_add_canonical(const T* __restrict__ a, const T* __restrict__ b
     } else {
       out[idx] = csub(csub(a[idx], p.q) + csub(b[idx], p.q), p.q);
     }
+  }
+}
+
+// Bounded decryption of the reference's decryptor
+// (fhelium/engine/ckks_decryptor.py:180-272): the centred class of the phase
+// modulo the product D of the trailing one or two active Q primes, converted
+// to float64 with the reference's float64 operations in its order, so the
+// result is the same double.  Two primes q_a (row limbs - 2), q_b (row
+// limbs - 1): mixed-radix digits d0 = x_a, d1 = (x_b - d0) q_a^{-1} mod q_b;
+// if (d1, d0) is above floor(D / 2) (compared digit-wise, high digit first)
+// the negated residues are decomposed instead and the value negated; the
+// value is dbl(d1) * dbl(q_a) + dbl(d0), each operation rounded to nearest
+// (no fused multiply-add).  One prime: x > q/2 ? x - q : x.
+struct DecryptTail {
+  uint64_t qa, qb;
+  uint64_t inv, inv_s;   // q_a^{-1} mod q_b and its Shoup companion
+  uint64_t qb_one_s;     // Shoup companion of 1 mod q_b (reduction of x_a)
+  uint64_t h0, h1;       // mixed-radix digits of floor(q_a q_b / 2)
+  int two;               // 1: two trailing primes, 0: one
+};
+
+__device__ __forceinline__ void tail_digits(uint64_t xa, uint64_t xb, const DecryptTail& t, uint64_t& d0,
+                                            uint64_t& d1) {
+  using W = Word<uint64_t>;
+  const uint64_t a_b = csub(W::shoup(xa, 1, t.qb_one_s, t.qb), t.qb);
+  d0 = xa;
+  d1 = csub(W::shoup(csub(xb + t.qb - a_b, t.qb), t.inv, t.inv_s, t.qb), t.qb);
+}
+
+template <typename T>
+__global__ void k_decrypt_tail(const T* __restrict__ phase, double* __restrict__ out, int64_t batch, int limbs,
+                               int log_n, DecryptTail t) {
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t total = batch * n;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total;
+       idx += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t b = idx >> log_n;
+    const int64_t k = idx & (n - 1);
+    const T* row_b = phase + (b * limbs + limbs - 1) * n;
+    uint64_t xb = csub(uint64_t(row_b[k]), t.qb);
+    if (!t.two) {
+      const int64_t c = xb > (t.qb >> 1) ? int64_t(xb) - int64_t(t.qb) : int64_t(xb);
+      out[idx] = __ll2double_rn(c);
+      continue;
+    }
+    uint64_t xa = csub(uint64_t(row_b[k - n]), t.qa);
+    uint64_t d0, d1;
+    tail_digits(xa, xb, t, d0, d1);
+    const bool above = d1 > t.h1 || (d1 == t.h1 && d0 > t.h0);
+    if (above) {
+      xa = xa ? t.qa - xa : 0;
+      xb = xb ? t.qb - xb : 0;
+      tail_digits(xa, xb, t, d0, d1);
+    }
+    const double v = __dadd_rn(__dmul_rn(__ll2double_rn(int64_t(d1)), __ull2double_rn(t.qa)),
+                               __ll2double_rn(int64_t(d0)));
+    out[idx] = above ? -v : v;
   }
 }
 

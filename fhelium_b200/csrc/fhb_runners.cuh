@@ -99,8 +99,18 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
 
 template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
-               int64_t batch, int level, cudaStream_t st) {
+               int64_t batch, int level, cudaStream_t st, bool pre) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
+  if (pre) {
+    if constexpr (sizeof(T) == 8) {
+      return launch_cluster<T, LOGN>(k_keyswitch_sum<T, LOGN, true>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
+                                     (const T*)digits, reinterpret_cast<const unsigned long long*>(key_ptrs),
+                                     (T*)acc0, (T*)acc1, giants, batch, ql, qpl, level, c.qp(), c.ks_order,
+                                     tables<T>(c), level_tables<T>(c, level));
+    } else {
+      return fail(-7, "the tensor-core basis conversion needs an int64 context");
+    }
+  }
   return launch_cluster<T, LOGN>(k_keyswitch_sum<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
                                  (const T*)digits, reinterpret_cast<const unsigned long long*>(key_ptrs), (T*)acc0,
                                  (T*)acc1, giants, batch, ql, qpl, level, c.qp(), c.ks_order, tables<T>(c),
@@ -133,7 +143,7 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
                                     cudaStream_t, const uint64_t*, const void*, bool);                          \
   template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
-                                   cudaStream_t);                                                               \
+                                   cudaStream_t, bool);                                                         \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);

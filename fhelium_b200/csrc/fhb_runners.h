@@ -20,7 +20,7 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
                 int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3, bool pre);
 template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
-               int64_t batch, int level, cudaStream_t st);
+               int64_t batch, int level, cudaStream_t st, bool pre);
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
 template <typename T, int LOGN>

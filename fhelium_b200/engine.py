@@ -26,8 +26,8 @@ import torch
 from . import _native as nat
 from .config import CkksConfig, Preset
 from .encoding import decode_coefficients, encode_real_coefficients
-from .values import (Ciphertext, CompressedPlaintext, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey,
-                     RotationKey, RotationKeySet, SecretKey)
+from .values import (Ciphertext, CompressedPlaintext, EncryptionDraws, KeySwitchKey, Plaintext, PublicKey,
+                     RelinearizationKey, RotationKey, RotationKeySet, SecretKey)
 
 
 def galois_element(n: int, step: int, generator: int = 3) -> int:
@@ -532,8 +532,16 @@ class CkksEngine:
             self.ctx.call("fhb_ckks_modup_digits", nat.ptr(ct.c1), nat.ptr(digits[i]), b, level, key.galois_element, st)
         key_ptrs = torch.tensor([k.data.data_ptr() for k in keys], dtype=torch.int64, device=self.device)
         t = self._empty(2, b, limbs + self.num_p, self.n)
-        self.ctx.call("fhb_ckks_keyswitch_sum", nat.ptr(digits), nat.ptr(key_ptrs), nat.ptr(t[0]), nat.ptr(t[1]),
-                      len(cts), b, level, st)
+        if self.basis_conversion == "tensor_cores":
+            # the giants' digits as one batch of len(cts) x b ciphertexts
+            words = int(self.ctx.lib.fhb_tc_basis_extend_words(self.ctx.handle, len(cts) * b, level))
+            ext = torch.empty(words, dtype=self.dtype, device=self.device)
+            self.ctx.call("fhb_tc_basis_extend", nat.ptr(digits), nat.ptr(ext), len(cts) * b, level, st)
+            self.ctx.call("fhb_ckks_keyswitch_sum_extended", nat.ptr(ext), nat.ptr(key_ptrs), nat.ptr(t[0]),
+                          nat.ptr(t[1]), len(cts), b, level, st)
+        else:
+            self.ctx.call("fhb_ckks_keyswitch_sum", nat.ptr(digits), nat.ptr(key_ptrs), nat.ptr(t[0]),
+                          nat.ptr(t[1]), len(cts), b, level, st)
         add0 = None
         for ct, key in zip(cts, keys):
             rot = self._empty(*ct.c0.shape)
@@ -694,7 +702,7 @@ class CkksEngine:
     # ------------------------------------------------------------------
     # encode / encrypt / decrypt (fhelium/engine/ckks_engine.py:508-866)
     # ------------------------------------------------------------------
-    def encode_coefficients(self, message, scale: float) -> torch.Tensor:
+    def encode_coefficients(self, message, scale: float, rounding: torch.Tensor | None = None) -> torch.Tensor:
         m = torch.as_tensor(message, device=self.device)
         if m.ndim == 0:
             m = m.expand(self.num_slots)
@@ -707,28 +715,42 @@ class CkksEngine:
             return torch.round(coeffs).to(torch.int64)
         # unbiased stochastic rounding, E[SRound(x)] = x (fhelium/engine/slot_embedding.py:100)
         low = torch.floor(coeffs)
-        u = torch.rand(coeffs.shape, generator=self._gen, device=coeffs.device, dtype=coeffs.dtype)
+        if rounding is not None:
+            if tuple(rounding.shape) != tuple(coeffs.shape):
+                raise ValueError("rounding uniforms must have the coefficients' shape [*batch, N]")
+            u = rounding.to(coeffs.device, coeffs.dtype)
+        else:
+            u = torch.rand(coeffs.shape, generator=self._gen, device=coeffs.device, dtype=coeffs.dtype)
         return (low + (u < coeffs - low).to(coeffs.dtype)).to(torch.int64)
 
     def encrypt_message(self, message, public_key: PublicKey | None = None, *, level: int = 0,
-                        scale: float | None = None) -> Ciphertext:
-        """Encode + public-key encryption, coefficient/standard output."""
+                        scale: float | None = None, draws: EncryptionDraws | None = None) -> Ciphertext:
+        """Encode + public-key encryption, coefficient/standard output.
+        `draws` supplies the encryption's random values (see EncryptionDraws)."""
         if not 0 <= level < self.public_level_count:
             raise ValueError("level out of range")
         scale = float(self.config.default_scale if scale is None else scale)
-        return self._encrypt_coefficients(self.encode_coefficients(message, scale), level, scale, public_key)
+        coeffs = self.encode_coefficients(message, scale, None if draws is None else draws.rounding)
+        return self._encrypt_coefficients(coeffs, level, scale, public_key, draws)
 
     def _encrypt_coefficients(self, coeffs: torch.Tensor, level: int, scale: float,
-                              public_key: PublicKey | None) -> Ciphertext:
+                              public_key: PublicKey | None, draws: EncryptionDraws | None = None) -> Ciphertext:
         """(v pk0 + e0 + m, v pk1 + e1) of exact integer coefficients [*batch, N]
         (fhelium/engine/ckks_encryptor.py:181-233)."""
         pk = (public_key or self.public_key).data[:, level:].contiguous()
         batch_shape = tuple(coeffs.shape[:-1])
         L = self.num_q - level
         m = self.forward_ntt(self._lift(coeffs, level, L), level)
-        v = self.forward_ntt(self._lift(self._ternary(*batch_shape, self.n), level, L), level)
-        e0 = self.forward_ntt(self._lift(self._gaussian(*batch_shape, self.n), level, L), level)
-        e1 = self.forward_ntt(self._lift(self._gaussian(*batch_shape, self.n), level, L), level)
+        shape = (*batch_shape, self.n)
+        if draws is None:
+            v_c, e0_c, e1_c = self._ternary(*shape), self._gaussian(*shape), self._gaussian(*shape)
+        else:
+            v_c, e0_c, e1_c = (torch.as_tensor(d).to(self.device, torch.int64) for d in (draws.v, draws.e0, draws.e1))
+            if any(tuple(d.shape) != shape for d in (v_c, e0_c, e1_c)):
+                raise ValueError(f"encryption draws must have shape {shape}")
+        v = self.forward_ntt(self._lift(v_c, level, L), level)
+        e0 = self.forward_ntt(self._lift(e0_c, level, L), level)
+        e1 = self.forward_ntt(self._lift(e1_c, level, L), level)
         c0 = self._binary(nat.OP_MONTGOMERY_MUL, v, pk[0].contiguous(), level, b_mode=1)
         c0 = self._binary(nat.OP_ADD_LAZY, c0, e0, level)
         c0 = self._binary(nat.OP_ADD_LAZY, c0, m, level)
@@ -750,36 +772,24 @@ class CkksEngine:
                 s_pow = self._binary(nat.OP_MONTGOMERY_MUL, s_pow, s, ct.level)
         return self.inverse_ntt(acc, ct.level)
 
-    def decrypt_coefficients(self, ct: Ciphertext, secret_key: SecretKey | None = None) -> np.ndarray:
-        """Centred integer coefficients of the phase (exact CRT over enough
-        trailing primes to cover the value's magnitude)."""
+    def decrypt_coefficients(self, ct: Ciphertext, secret_key: SecretKey | None = None) -> torch.Tensor:
+        """Bounded decryption on the device: float64 [*batch, N], the centred
+        class of the phase modulo the product of the trailing one or two
+        active Q primes, the same doubles as the reference's decryptor
+        (fhelium/engine/ckks_decryptor.py:180-272; fhb_ckks_decrypt_tail)."""
         self._check_ct(ct)
-        phase = self._phase(ct, secret_key).cpu().numpy().astype(object)
-        need_bits = max(62, int(math.log2(max(ct.scale, 2.0))) + 30)
-        ids, bits = [], 0
-        for pid in reversed(range(ct.level, self.num_q)):
-            ids.append(pid)
-            bits += self.moduli[pid].bit_length() - 1
-            if bits >= need_bits:
-                break
-        rows = [pid - ct.level for pid in ids]
-        x = phase[..., rows[0], :]
-        mod = self.moduli[ids[0]]
-        for r, pid in zip(rows[1:], ids[1:]):
-            q = self.moduli[pid]
-            inv = pow(mod, -1, q)
-            t = ((phase[..., r, :] - x) % q) * inv % q
-            x = x + t * mod
-            mod *= q
-        x = np.where(x > mod // 2, x - mod, x)
-        return x
+        phase = self._phase(ct, secret_key).contiguous()
+        out = torch.empty((*ct.data.shape[1:-2], self.n), dtype=torch.float64, device=self.device)
+        self.ctx.call("fhb_ckks_decrypt_tail", nat.ptr(phase), nat.ptr(out), ct.batch_size, ct.level, self._stream())
+        return out
 
     def decrypt_message(self, ct: Ciphertext, secret_key: SecretKey | None = None, *,
                         is_real: bool = False) -> torch.Tensor:
+        """Decrypt and decode at the ciphertext's scale; CPU [*batch, N/2]
+        slots, complex unless is_real (fhelium/engine/ckks_decryptor.py:357)."""
         coeffs = self.decrypt_coefficients(ct, secret_key)
-        vals = torch.tensor(np.asarray(coeffs, dtype=np.float64), dtype=torch.float64)
-        slots = decode_coefficients(vals, self.n, self.galois_generator) / ct.scale
-        return slots.real if is_real else slots
+        slots = decode_coefficients(coeffs, self.n, self.galois_generator) / ct.scale
+        return (slots.real if is_real else slots).cpu()
 
     # ------------------------------------------------------------------
     # Plaintext values (fhelium/engine/ckks_engine.py:508-760,
@@ -925,22 +935,24 @@ class CkksEngine:
         slots = decode_coefficients(vals, self.n, self.galois_generator) / plaintext.scale
         return slots.real if is_real else slots
 
-    def encrypt(self, plaintext: Plaintext, public_key: PublicKey | None = None) -> Ciphertext:
+    def encrypt(self, plaintext: Plaintext, public_key: PublicKey | None = None, *,
+                draws: EncryptionDraws | None = None) -> Ciphertext:
         """Public-key encryption of slots or exact integer coefficients;
-        coefficient/standard output (fhelium/engine/ckks_engine.py:700-738)."""
+        coefficient/standard output (fhelium/engine/ckks_engine.py:700-738).
+        `draws` supplies the encryption's random values (see EncryptionDraws)."""
         if not isinstance(plaintext, Plaintext):
             raise TypeError(f"encrypt expects Plaintext, got {type(plaintext).__name__}")
         pt = self._integer_plaintext(plaintext)
         self._public_level(pt.level)
-        return self._encrypt_coefficients(pt.data.to(self.device, torch.int64), pt.level, pt.scale, public_key)
+        return self._encrypt_coefficients(pt.data.to(self.device, torch.int64), pt.level, pt.scale, public_key,
+                                          draws)
 
     def decrypt(self, ct: Ciphertext, secret_key: SecretKey | None = None) -> Plaintext:
         """Decryption to float64 coefficients [*batch, N] (approximate
         coefficients, for decode) (fhelium/engine/ckks_engine.py:740-771)."""
         if not isinstance(ct, Ciphertext):
             raise TypeError(f"decrypt expects Ciphertext, got {type(ct).__name__}")
-        coeffs = self.decrypt_coefficients(ct, secret_key)
-        data = torch.tensor(np.asarray(coeffs, dtype=np.float64), dtype=torch.float64, device=self.device)
+        data = self.decrypt_coefficients(ct, secret_key)
         return Plaintext(message=None, data=data, level=ct.level, scale=ct.scale, context_id=self.context_id,
                          representation="approximate_coefficients", polynomial_domain="coefficient")
 

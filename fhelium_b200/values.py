@@ -353,6 +353,23 @@ class PublicKey:
 
 
 @dataclass
+class EncryptionDraws:
+    """The random draws of one public-key encryption, supplied by the caller
+    instead of the engine's generator: v (ternary), e0, e1 (the error draws)
+    as signed int64 [*batch, N], and, for encrypt_message, the uniforms in
+    [0, 1) of encode's stochastic rounding as float64 [*batch, N] (None: the
+    engine draws them).  The result is then a deterministic function of the
+    message, the key and these draws, c0 = v pk0 + e0 + m, c1 = v pk1 + e1
+    (fhelium/engine/ckks_encryptor.py:181-233), which is how encryption is
+    compared with the reference's encryptor fed the same values.  No
+    counterpart in the reference, whose draws come from its own CSPRNG."""
+    v: torch.Tensor
+    e0: torch.Tensor
+    e1: torch.Tensor
+    rounding: torch.Tensor | None = None
+
+
+@dataclass
 class KeySwitchKey:
     data: torch.Tensor  # [D, 2, QP, N] NTT/Montgomery
 

@@ -354,6 +354,23 @@ int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, voi
 int fhb_ckks_keyswitch_sum(const fhb_context* ctx, const void* digits, const uint64_t* key_ptrs, void* acc0,
                            void* acc1, int giants, int64_t batch, int level, fhb_stream stream);
 
+/* fhb_ckks_keyswitch_sum of the tensor-core form (int64 contexts): from the
+ * extensions of the giants' digits, i.e. fhb_tc_basis_extend of the digits
+ * [giants, batch, L, N] taken as one batch of giants x batch ciphertexts
+ * (ext [D_l, giants x batch, L+P, N]).  Same result. */
+int fhb_ckks_keyswitch_sum_extended(const fhb_context* ctx, const void* ext, const uint64_t* key_ptrs, void* acc0,
+                                    void* acc1, int giants, int64_t batch, int level, fhb_stream stream);
+
+/* Bounded decryption to float64 coefficients: phase [batch, L, N]
+ * coefficient/standard canonical (c0 + c1 s) -> out [batch, N] float64 (a
+ * DEVICE pointer), the centred representative modulo the product of the
+ * trailing one or two active Q primes, computed with the reference's float64
+ * operations in its order so the doubles are equal.  Replaces
+ * CkksDecryptor._reconstruct_tail_q_coefficients_float64
+ * (fhelium/engine/ckks_decryptor.py:180-272). */
+int fhb_ckks_decrypt_tail(const fhb_context* ctx, const void* phase, double* out, int64_t batch, int level,
+                          fhb_stream stream);
+
 /* Baby-step/giant-step inner products of a diagonal linear transform
  * (bootstrapping's CoeffsToSlots / SlotsToCoeffs):
  *   out[k] = sum_b rot[b] (.) pts[table[k * babies + b]]

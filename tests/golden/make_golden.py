@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from inputs import canonical, digest, key_material, residues  # noqa: E402
+from inputs import canonical, client_inputs, digest, float_digest, key_material, residues  # noqa: E402
 
 REFERENCE = os.environ.get("FHELIUM_REFERENCE", "/root/reference")
 REF_OPS = os.path.join(ROOT, "oracle", "_ref", "libfhelium_ref_cpu_ops.so")
@@ -174,6 +174,44 @@ def generate_case(fh, name, preset, overrides, generator, levels):
             out["cases"].append({"op": "rotate_many_by_steps", "level": level, "seed": seed, "step": s,
                                  "steps": steps, "key_seed": 910 + rot_steps.index(s),
                                  **_record(r.data.numpy(), mod, ids)})
+    out["client"] = client_cases(fh, eng, cfg, levels)
+    return out
+
+
+def client_cases(fh, eng, cfg, levels):
+    """Encryption with injected draws and public key, and decryption with an
+    injected secret key, through the reference's CkksEngine.encrypt /
+    decrypt: the reference's random source is replaced by functions that
+    return the recorded draws (e0 and e1 as its discrete_gaussian rows, v as
+    its randint), so the ciphertext is a deterministic function of inputs."""
+    from fhelium.core import Ciphertext, Plaintext, PublicKey, SecretKey
+
+    dt = cfg.torch_dtype
+    mod, nq, npr, n = cfg.moduli, cfg.num_q_primes, cfg.num_p_primes, cfg.N
+    ctx_id = eng.context.context_id
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dt)
+    out = []
+    batch = 2
+    for level in levels:
+        seed = 1000 + level
+        x = client_inputs(seed, mod, nq, npr, level, n, batch, dt == torch.int32)
+        draws = {"gauss": torch.from_numpy(x["e"].reshape(2 * batch, n)).to(dt),
+                 "v": torch.from_numpy(x["v"]).to(dt)}
+        eng._rng.discrete_gaussian = lambda non_repeats=0, repeats=1: [draws["gauss"]]
+        eng._rng.randint = lambda amax, shift=0, repeats=0: [draws["v"]]
+        pk = PublicKey(t(x["pk"]), ctx_id, tuple(range(nq)))
+        pt = Plaintext(message=None, level=level, scale=2.0 ** 40, data=t(x["m"]), context_id=ctx_id,
+                       representation="integer_coefficients", polynomial_domain="coefficient")
+        r = eng.encrypt(pt, pk)
+        ids = list(range(level, nq))
+        out.append({"op": "encrypt", "level": level, "seed": seed, "batch": batch,
+                    **_record(r.data.numpy(), mod, ids)})
+        sk = SecretKey(t(x["sk"]), ctx_id, tuple(range(nq + npr)))
+        c = Ciphertext(data=t(x["ct"]), level=level, scale=2.0 ** 40, context_id=ctx_id, prime_ids=tuple(ids),
+                       polynomial_domain="coefficient", residue_representation="standard", modulus_basis="Q")
+        d = eng.decrypt(c, sk).data.numpy().astype(np.float64)
+        out.append({"op": "decrypt", "level": level, "seed": seed, "batch": batch, "digest": float_digest(d),
+                    "shape": list(d.shape), "head": d.reshape(-1, d.shape[-1])[:2, :2].tolist()})
     return out
 
 

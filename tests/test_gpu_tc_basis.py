@@ -144,3 +144,21 @@ def test_tc_form_rejected_on_int32_chains():
     with pytest.raises(nat.NativeCallError, match="int64"):
         eng.basis_conversion = "tensor_cores"
     assert eng.basis_conversion == "cuda_cores"
+
+
+@pytest.mark.parametrize("family,log_n,level", [("int64_logn14", 14, 1), ("int64_logn16", 13, 20)])
+def test_tc_form_rotate_and_sum_matches_cuda_core_form(family, log_n, level):
+    """The giant-step sum of bootstrapping (one ModDown for a sum of key
+    switches, fhb_ckks_keyswitch_sum[_extended]) is integer-equal in both forms."""
+    cfg, eng, orc, rng = _setup(family, log_n, 23)
+    rows = orc.q_rows(level)
+    steps = [1, 5, -7, 64]
+    cts = [Ciphertext(to_dev(uniform_residues(rng, cfg.moduli, rows, (2, 2), cfg.N), cfg), level, 1.0)
+           for _ in steps]
+    keys = [RotationKey(to_dev(random_key(rng, cfg, cfg.N), cfg), rotation_step=s % eng.num_slots,
+                        galois_element=eng.galois_element_for_step(s)) for s in steps]
+    outs = {}
+    for form in ("cuda_cores", "tensor_cores"):
+        eng.basis_conversion = form
+        outs[form] = to_np(eng.rotate_and_sum(cts, keys).data)
+    np.testing.assert_array_equal(outs["tensor_cores"], outs["cuda_cores"])
