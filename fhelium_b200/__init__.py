@@ -8,7 +8,7 @@ from typing import Literal
 
 from .config import CkksConfig, Preset
 from .values import (COMPRESSED_PLAINTEXT_FORMAT_VERSION, Ciphertext, CompressedPlaintext, EncryptionDraws,
-                     EvaluationKeyRequirements, EvaluationKeySet, KeySwitchKey, Plaintext, PublicKey, RelinearizationKey, RotationKey,
+                     EvaluationKeyRequirements, EvaluationKeySet, KeySwitchKey, KeySwitchKeyDraws, Plaintext, PublicKey, RelinearizationKey, RotationKey,
                      RotationKeySet, SecretKey)
 
 # state literals (fhelium/core/state.py:10-21)
@@ -25,6 +25,7 @@ __all__ = ["CkksConfig", "Preset", "CkksEngine", "Ciphertext", "Plaintext", "Com
            "CompressedPlaintextLayout", "COMPRESSED_PLAINTEXT_FORMAT_VERSION", "SecretKey", "PublicKey",
            "KeySwitchKey", "RelinearizationKey", "RotationKey", "ConjugationKey", "RotationKeySet",
            "EvaluationKeySet", "EvaluationKeyRequirements", "EncryptionDraws",
+           "KeySwitchKeyDraws",
            "PlaintextRepresentation", "PolynomialDomain", "ModulusBasis", "ResidueRepresentation",
            "save_value", "load_value", "inspect_value"]
 

@@ -26,8 +26,8 @@ import torch
 from . import _native as nat
 from .config import CkksConfig, Preset
 from .encoding import decode_coefficients, encode_real_coefficients
-from .values import (Ciphertext, CompressedPlaintext, EncryptionDraws, KeySwitchKey, Plaintext, PublicKey,
-                     RelinearizationKey, RotationKey, RotationKeySet, SecretKey)
+from .values import (Ciphertext, CompressedPlaintext, EncryptionDraws, KeySwitchKey, KeySwitchKeyDraws, Plaintext,
+                     PublicKey, RelinearizationKey, RotationKey, RotationKeySet, SecretKey)
 
 
 def galois_element(n: int, step: int, generator: int = 3) -> int:
@@ -408,7 +408,8 @@ class CkksEngine:
                       target_level, self._stream())
         return Ciphertext(out, target_level, ct.scale, "coefficient", "standard")
 
-    def create_galois_key(self, galois: int, secret_key: SecretKey | None = None, *, rotation_step: int = 0) -> RotationKey:
+    def create_galois_key(self, galois: int, secret_key: SecretKey | None = None, *, rotation_step: int = 0,
+                          draws: KeySwitchKeyDraws | None = None) -> RotationKey:
         """Key switching sigma_g(s) -> s for any odd g (rotations, conjugation)."""
         s = secret_key or self.secret_key
         coef = self.inverse_ntt(s.data, 0, output=nat.INV_MONTGOMERY)
@@ -416,7 +417,7 @@ class CkksEngine:
         self.ctx.call("fhb_ckks_automorphism", nat.ptr(coef), nat.ptr(rot), 1, self.qp_rows, 0, galois,
                       self._stream())
         rs = self.forward_ntt(rot, 0, montgomery_input=True)
-        ksk = self.create_key_switch_key(SecretKey(rs), s)
+        ksk = self.create_key_switch_key(SecretKey(rs), s, draws=draws)
         return RotationKey(ksk.data, rotation_step=rotation_step, galois_element=galois)
 
     def create_conjugation_key(self, secret_key: SecretKey | None = None) -> RotationKey:
@@ -634,10 +635,12 @@ class CkksEngine:
     def set_secret_key(self, key: SecretKey) -> None:
         self._secret_key = key
 
-    def _encrypt_zero_qp(self, s: torch.Tensor, rows: int, uniform: torch.Tensor | None = None):
+    def _encrypt_zero_qp(self, s: torch.Tensor, rows: int, uniform: torch.Tensor | None = None,
+                         error: torch.Tensor | None = None):
         """(e - a s, a) over the first `rows` level-zero rows, NTT/Montgomery."""
         a = self._uniform_rows(rows=range(rows)) if uniform is None else uniform
-        e = self.forward_ntt(self._lift(self._gaussian(self.n), 0, rows), 0)
+        err = self._gaussian(self.n) if error is None else error.to(self.device, torch.int64).contiguous()
+        e = self.forward_ntt(self._lift(err, 0, rows), 0)
         a_s = self._binary(nat.OP_MONTGOMERY_MUL, a, s[:rows].contiguous(), 0)
         return self._binary(nat.OP_SUB_LAZY, e, a_s, 0), a
 
@@ -652,9 +655,11 @@ class CkksEngine:
             self._public_key = self.create_public_key()
         return self._public_key
 
-    def create_key_switch_key(self, source: SecretKey, destination: SecretKey) -> KeySwitchKey:
+    def create_key_switch_key(self, source: SecretKey, destination: SecretKey, *,
+                              draws: KeySwitchKeyDraws | None = None) -> KeySwitchKey:
         """Digit d: (-a s_dst + e + P s_src on the digit's rows, a)
-        (fhelium/engine/key_generator.py:197-262)."""
+        (fhelium/engine/key_generator.py:197-262); `draws` supplies a and e
+        (see KeySwitchKeyDraws)."""
         P = math.prod(self.moduli[self.num_q:])
         R = 1 << (62 if self.dtype == torch.int64 else 30)
         p_mont = torch.tensor([(P * R) % q for q in self.moduli[: self.num_q]], dtype=self.dtype,
@@ -662,17 +667,26 @@ class CkksEngine:
         src_q = source.data[: self.num_q].contiguous()
         p_src = self._binary(nat.OP_MONTGOMERY_MUL, src_q, p_mont, 0, b_mode=2)
         digits = []
+        if draws is not None:
+            nd, shape = len(self.level_digits[0]), (self.qp_rows, self.n)
+            if tuple(draws.uniform.shape) != (nd, *shape) or tuple(draws.error.shape) != (nd, self.n):
+                raise ValueError(f"key draws must be uniform [{nd}, {shape[0]}, {shape[1]}] and error [{nd}, {self.n}]")
         for kd, ids in self.level_digits[0]:
-            k0, k1 = self._encrypt_zero_qp(destination.data, self.qp_rows)
+            if draws is None:
+                k0, k1 = self._encrypt_zero_qp(destination.data, self.qp_rows)
+            else:
+                a = draws.uniform[kd].to(self.device, self.dtype).contiguous()
+                k0, k1 = self._encrypt_zero_qp(destination.data, self.qp_rows, a, draws.error[kd])
             lo, hi = ids[0], ids[-1] + 1
             k0[lo:hi] = self._binary(nat.OP_ADD_LAZY, k0[lo:hi].contiguous(), p_src[lo:hi].contiguous(), lo)
             digits.append(torch.stack([k0, k1]))
         return KeySwitchKey(torch.stack(digits))
 
-    def create_relinearization_key(self, secret_key: SecretKey | None = None) -> RelinearizationKey:
+    def create_relinearization_key(self, secret_key: SecretKey | None = None, *,
+                                   draws: KeySwitchKeyDraws | None = None) -> RelinearizationKey:
         s = secret_key or self.secret_key
         s2 = self._binary(nat.OP_MONTGOMERY_MUL, s.data, s.data, 0)
-        return RelinearizationKey(self.create_key_switch_key(SecretKey(s2), s).data)
+        return RelinearizationKey(self.create_key_switch_key(SecretKey(s2), s, draws=draws).data)
 
     @property
     def relinearization_key(self) -> RelinearizationKey:
@@ -683,10 +697,12 @@ class CkksEngine:
     def set_relinearization_key(self, key: RelinearizationKey) -> None:
         self._relinearization_key = key
 
-    def create_rotation_key(self, rotation_step: int, secret_key: SecretKey | None = None) -> RotationKey:
+    def create_rotation_key(self, rotation_step: int, secret_key: SecretKey | None = None, *,
+                            draws: KeySwitchKeyDraws | None = None) -> RotationKey:
         """Key from sigma_g(s) back to s (fhelium/engine/key_generator.py:364-412)."""
         step = self._canonical_step(rotation_step)
-        return self.create_galois_key(self.galois_element_for_step(step), secret_key, rotation_step=step)
+        return self.create_galois_key(self.galois_element_for_step(step), secret_key, rotation_step=step,
+                                      draws=draws)
 
     def generate_rotation_keys(self, steps: Iterable[int]) -> None:
         for st in steps:

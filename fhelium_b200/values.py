@@ -370,6 +370,20 @@ class EncryptionDraws:
 
 
 @dataclass
+class KeySwitchKeyDraws:
+    """The random draws of one key-switch key (relinearisation, rotation,
+    conjugation), supplied by the caller: per level-zero key digit, the
+    uniform component a [D, QP, N] (residues taken as NTT/Montgomery values,
+    as the reference's uniform_component_by_key_digit) and the error e
+    [D, N] (signed int64).  Digit d is then (e_d - a_d s_dst + P s_src on
+    the digit's rows, a_d) (fhelium/engine/key_generator.py:197-330), which is
+    how key generation is compared with the reference's key generator fed the
+    same values."""
+    uniform: torch.Tensor
+    error: torch.Tensor
+
+
+@dataclass
 class KeySwitchKey:
     data: torch.Tensor  # [D, 2, QP, N] NTT/Montgomery
 

@@ -59,3 +59,10 @@ def client_inputs(seed: int, moduli, num_q: int, num_p: int, level: int, n: int,
         "e": small_ints(seed + 4, (2, batch, n), 20),
         "ct": residues(seed + 5, moduli, list(range(level, num_q)), (2, batch), n),
     }
+
+
+def key_draws(seed: int, moduli, num_q: int, num_p: int, n: int):
+    """Key-switch key draws: uniform component [D, QP, N] and error [D, N]."""
+    digits = len(range(0, num_q - 1, num_p)) + 1
+    return (residues(seed, moduli, list(range(num_q + num_p)), (digits,), n),
+            small_ints(seed + 1, (digits, n), 20))

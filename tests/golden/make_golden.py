@@ -33,7 +33,8 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, HERE)
 
-from inputs import canonical, client_inputs, digest, float_digest, key_material, residues  # noqa: E402
+from inputs import (canonical, client_inputs, digest, float_digest, key_draws, key_material,  # noqa: E402
+                    residues)
 
 REFERENCE = os.environ.get("FHELIUM_REFERENCE", "/root/reference")
 REF_OPS = os.path.join(ROOT, "oracle", "_ref", "libfhelium_ref_cpu_ops.so")
@@ -212,6 +213,26 @@ def client_cases(fh, eng, cfg, levels):
         d = eng.decrypt(c, sk).data.numpy().astype(np.float64)
         out.append({"op": "decrypt", "level": level, "seed": seed, "batch": batch, "digest": float_digest(d),
                     "shape": list(d.shape), "head": d.reshape(-1, d.shape[-1])[:2, :2].tolist()})
+    # key generation: relinearisation key and one rotation key from an
+    # injected secret key, with the per-digit uniform components and errors
+    # returned in digit order by the replaced random source
+    qp_ids = list(range(nq + npr))
+    for op, seed in (("relinearization_key", 1200), ("rotation_key", 1300)):
+        x = client_inputs(seed, mod, nq, npr, 0, n, 1, dt == torch.int32)
+        uni, err = key_draws(seed + 10, mod, nq, npr, n)
+        queue = {"u": [t(u) for u in uni], "e": [torch.from_numpy(e).to(dt) for e in err]}
+        eng._rng.discrete_gaussian = lambda non_repeats=0, repeats=1: [queue["e"].pop(0).view(1, n)]
+        eng._rng.randint = lambda amax, shift=0, repeats=0: [queue["u"].pop(0)]
+        sk = SecretKey(t(x["sk"]), ctx_id, tuple(qp_ids))
+        kg = eng._key_generator
+        if op == "relinearization_key":
+            k = kg.create_relinearization_key(sk)
+            extra = {}
+        else:
+            k = kg.create_rotation_key(3, secret_key=sk)
+            extra = {"step": 3}
+        assert not queue["u"] and not queue["e"], "every draw consumed once"
+        out.append({"op": op, "level": 0, "seed": seed, **extra, **_record(k.data.numpy(), mod, qp_ids)})
     return out
 
 

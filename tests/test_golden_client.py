@@ -6,9 +6,12 @@ integer-coefficient plaintext under an injected public key, with its random
 source replaced by the recorded draws (v, e0, e1), and CkksEngine.decrypt of
 a ciphertext under an injected secret key (the reference's bounded float64
 reconstruction from the trailing Q primes, fhelium/engine/ckks_decryptor.py:
-180-272).  Encryption outputs are compared as canonical residues (integer
-equal, by digest); decryption outputs as the exact float64 values (by digest
-of their bytes).
+180-272), and the reference key generator's relinearisation and rotation
+keys from an injected secret key with recorded per-digit draws
+(fhelium/engine/key_generator.py:197-412).  Encryption outputs are compared
+as canonical residues (integer equal, by digest); key material modulo q (its
+state is lazy); decryption outputs as the exact float64 values (by digest of
+their bytes).
 
 The CPU test checks the oracle's restatement of both; the GPU test checks
 the engine (encryption with EncryptionDraws, decryption by the
@@ -23,7 +26,7 @@ import pytest
 
 from fhelium_b200.config import CkksConfig
 from oracle import oracle as orc
-from tests.golden.inputs import canonical, client_inputs, digest, float_digest
+from tests.golden.inputs import canonical, client_inputs, digest, float_digest, key_draws
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = json.load(open(os.path.join(HERE, "golden", "engine_golden.json")))
@@ -40,12 +43,12 @@ def _setup(name, index):
     cfg = CkksConfig.parse(fx["preset"], **fx["overrides"])
     case = fx["client"][index]
     x = client_inputs(case["seed"], cfg.moduli, cfg.num_q_primes, cfg.num_p_primes, case["level"], cfg.N,
-                      case["batch"], cfg.buffer_bit_length == 30)
+                      case.get("batch", 1), cfg.buffer_bit_length == 30)
     return cfg, case, x
 
 
-def _check_encrypt(case, out, cfg):
-    ids = list(range(case["level"], cfg.num_q_primes))
+def _check_encrypt(case, out, cfg, ids=None):
+    ids = list(range(case["level"], cfg.num_q_primes)) if ids is None else ids
     c = canonical(out, cfg.moduli, ids)
     assert list(c.shape) == case["shape"]
     assert c.reshape(-1, c.shape[-1])[:4, :2].tolist() == case["head"]
@@ -85,12 +88,44 @@ def _tail_float64(phase: np.ndarray, moduli, level: int, num_q: int) -> np.ndarr
     return np.where(above, -v, v)
 
 
+def _oracle_key(case, cfg, oc, x, generator):
+    """Key-switch key of fhelium/engine/key_generator.py:197-330, restated:
+    digit d = (NTT(e_d) R - a_d s + [P s_src on the digit's rows], a_d)."""
+    nq, npr = cfg.num_q_primes, cfg.num_p_primes
+    qp = list(range(nq + npr))
+    prm = oc.sub_params(qp)
+    rb = oc.radix_bits
+    s = x["sk"]
+    if case["op"] == "relinearization_key":
+        src = orc.montgomery_mul(s, s, prm, rb)
+    else:
+        std = oc.inverse_to_standard(s, qp)
+        src = oc.forward_to_montgomery(oc.automorphism(std, case["step"], qp, generator), qp)
+    p_mont = np.array([(int(np.prod([int(v) for v in cfg.moduli[nq:]], dtype=object)) << rb) % cfg.moduli[i]
+                       for i in qp], dtype=np.int64)
+    psrc = orc.montgomery_mul(src, np.broadcast_to(p_mont[:, None], src.shape), prm, rb)
+    uni, err = key_draws(case["seed"] + 10, cfg.moduli, nq, npr, cfg.N)
+    q = np.array(cfg.moduli, dtype=np.int64)[:, None]
+    digits = []
+    for kd, ids in enumerate(oc.level_zero_digits):
+        e = oc.forward_to_montgomery(np.mod(err[kd][None, :], q), qp)
+        k0 = np.mod(e - orc.montgomery_mul(uni[kd], s, prm, rb), q)
+        lo, hi = ids[0], ids[-1] + 1
+        k0[lo:hi] = np.mod(k0[lo:hi] + psrc[lo:hi], q[lo:hi])
+        digits.append(np.stack([k0, uni[kd]]))
+    return np.stack(digits)
+
+
 @pytest.mark.parametrize("name,index", list(_cases()))
 def test_oracle_reproduces_reference_client(name, index):
     cfg, case, x = _setup(name, index)
     oc = orc.OracleContext(cfg.moduli, cfg.logN, cfg.num_q_primes, cfg.num_p_primes, cfg.buffer_bit_length,
                            cfg.scale_bits)
     level = case["level"]
+    if case["op"].endswith("_key"):
+        _check_encrypt(case, _oracle_key(case, cfg, oc, x, GOLDEN["fixtures"][name]["generator"]), cfg,
+                       list(range(cfg.num_q_primes + cfg.num_p_primes)))
+        return
     rows = oc.q_rows(level)
     q = np.array([cfg.moduli[i] for i in rows], dtype=np.int64)[:, None]
     lift = lambda c: np.mod(c[..., None, :], q)  # signed [*, N] -> canonical [*, L, N]
@@ -118,14 +153,24 @@ def test_gpu_engine_reproduces_reference_client(name, index):
     import torch
 
     from fhelium_b200.engine import CkksEngine
-    from fhelium_b200.values import Ciphertext, EncryptionDraws, Plaintext, PublicKey, SecretKey
+    from fhelium_b200.values import Ciphertext, EncryptionDraws, KeySwitchKeyDraws, Plaintext, PublicKey, SecretKey
 
     cfg, case, x = _setup(name, index)
     fx = GOLDEN["fixtures"][name]
     eng = CkksEngine(cfg, galois_generator=fx["generator"], allow_sk_gen=False)
     dev = lambda a, dt=cfg.torch_dtype: torch.from_numpy(np.ascontiguousarray(a)).to(dt).cuda()
     level = case["level"]
-    if case["op"] == "encrypt":
+    if case["op"].endswith("_key"):
+        uni, err = key_draws(case["seed"] + 10, cfg.moduli, cfg.num_q_primes, cfg.num_p_primes, cfg.N)
+        draws = KeySwitchKeyDraws(uniform=dev(uni), error=dev(err, torch.int64))
+        sk = SecretKey(dev(x["sk"]))
+        if case["op"] == "relinearization_key":
+            k = eng.create_relinearization_key(sk, draws=draws)
+        else:
+            k = eng.create_rotation_key(case["step"], sk, draws=draws)
+        _check_encrypt(case, k.data.cpu().to(torch.int64).numpy(), cfg,
+                       list(range(cfg.num_q_primes + cfg.num_p_primes)))
+    elif case["op"] == "encrypt":
         pt = Plaintext(message=None, data=dev(x["m"], torch.int64), level=level, scale=2.0 ** 40,
                        context_id=eng.context_id, representation="integer_coefficients",
                        polynomial_domain="coefficient")
