@@ -289,15 +289,23 @@ def bootstrap_leg(dev, stream, batch=8, steps=2):
     def step():
         state["out"] = bs(ct)
 
-    step()
-    torch.cuda.synchronize(dev)
-    ms = _time_events(step, steps, stream)
-    err = (eng.decrypt_message(state["out"]) - m).abs()
-    out = {"batch": batch, "ms_per_call": ms, "ms_per_bootstrap": ms / batch,
-           "bootstraps_per_s": batch / (ms / 1e3), "output_level": state["out"].level,
-           "max_abs_err": float(err.max()), "mean_abs_err": float(err.mean()),
-           "precision_bits": -math.log2(float(err.max())), "setup_s": setup_s,
-           "rotation_keys": len(bs.rotation_steps())}
+    out = {"batch": batch, "setup_s": setup_s, "rotation_keys": len(bs.rotation_steps())}
+    # the key switches' basis conversion on the CUDA cores, then on the int8
+    # tensor cores (the default reported above the per-form figures)
+    results = {}
+    for form in ("cuda_cores", "tensor_cores"):
+        eng.basis_conversion = form
+        step()
+        torch.cuda.synchronize(dev)
+        ms = _time_events(step, steps, stream)
+        err = (eng.decrypt_message(state["out"]) - m).abs()
+        results[form] = state["out"].data.clone()
+        out[form] = {"ms_per_call": ms, "ms_per_bootstrap": ms / batch, "bootstraps_per_s": batch / (ms / 1e3),
+                     "output_level": state["out"].level, "max_abs_err": float(err.max()),
+                     "mean_abs_err": float(err.mean()), "precision_bits": -math.log2(float(err.max()))}
+    out.update(out["tensor_cores"])
+    out["forms_bit_identical"] = bool(torch.equal(results["cuda_cores"], results["tensor_cores"]))
+    out["tensor_cores_over_cuda_cores_latency"] = out["cuda_cores"]["ms_per_call"] / out["tensor_cores"]["ms_per_call"]
     del bs, eng, ct, state
     torch.cuda.empty_cache()
     return out

@@ -150,6 +150,10 @@ int moddown(const Context& c, const void* t0, const void* t1, const void* a0, co
             int64_t batch, int level, uint32_t add0_galois, int rescale, cudaStream_t st,
             const uint32_t* item_galois = nullptr) {
   const uint32_t ginv = add0_galois == 1 ? 0u : galois_inverse(add0_galois, c.log_n);
+  if constexpr (sizeof(T) == 8) {
+    if (c.basis_tc)  // P -> Q conversion on the int8 tensor cores
+      return tc_moddown(const_cast<Context&>(c), t0, t1, a0, a1, out, batch, level, ginv, item_galois, rescale, st);
+  }
   k_moddown<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
       (const T*)t0, (const T*)t1, (const T*)a0, (const T*)a1, (T*)out, batch, c.log_n, level, c.num_q, c.num_p,
       ginv, item_galois, rescale, tables<T>(c), level_tables<T>(c, level));

@@ -62,6 +62,7 @@ struct TcNttTables {
 // Context::allocations.
 struct TcBasisTables {
   std::vector<uint8_t*> bmat;     // per level: [digit][16-row chunk][128 x 32 ks] byte matrices
+  std::vector<uint8_t*> md_bmat;  // per level: [16-row chunk of Q_l][128 x 32 ks] ModDown byte matrices
   uint64_t* pinfo = nullptr;      // [QP][2]: p, -p^{-1} mod 2^64
   int ks = 1;                     // K-steps of 32 bytes (digits of up to 4 or 8 primes)
   int sms = 0;                    // multiprocessors of the context's device (one CTA each)
@@ -135,6 +136,11 @@ int tc_basis_prepare(Context& c);
 int64_t tc_ext_words(const Context& c, int64_t batch, int level);
 int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st);
 int tc_basis_status(Context& c, int* flag);
+// ModDown by P (+ addends, + rescale) with the P -> Q conversion on the
+// tensor cores; same arguments and result as the CUDA-core ModDown.
+int tc_moddown(Context& c, const void* t0, const void* t1, const void* add0, const void* add1, void* out,
+               int64_t batch, int level, uint32_t add0_ginv, const uint32_t* item_galois, int rescale,
+               cudaStream_t st);
 void tc_basis_tables_host(const Context& c, int level, int ks, std::vector<uint8_t>& out);
 
 // Host-side status plumbing shared by the C ABI.

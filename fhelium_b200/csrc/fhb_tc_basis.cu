@@ -48,6 +48,7 @@
 #include <vector>
 
 #include "fhb_context.h"
+#include "fhb_kernels.cuh"
 #include "fhb_tc_common.cuh"
 
 namespace fhb {
@@ -312,6 +313,313 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// ModDown by P on the tensor cores (int64): for every Q row i of the level
+// and coefficient k of the key-switch accumulators t (canonical coefficient
+// rows [B][Q_l + P][N], component c = 0, 1),
+//   v_i = (t_i - [t]_P mod q_i) P^{-1} + add_i          (mod q_i)
+// where [t]_P = sum_r e_r (M_r mod q_i) is the exact extension of the P part
+// from its Garner digits e_r, M_r the product of the first r special primes
+// (csrc/ops/ckks/cpu/ckks_cpu.cpp:474-601 computes the same (t - [t]_P) / P
+// by sequential division).  The extension is one int8 MMA per 16-row chunk of
+// Q rows (A = the digits' bytes, B = the bytes of 2^{8u} 2^64 (M_r mod q_i)
+// mod q_i, exactly as in k_tc_extend); the epilogue reduces it by 2^64 and
+// finishes v_i, optionally rescaling by the leading prime in place
+// (csrc/ops/ckks/cpu/ckks_cpu.cpp:203-262): out_{i-1} = (v_i - v_0) q_0^{-1} +
+// [v_0 > q_0 / 2].  The loaders compute the Garner digits and v_0 of each
+// coefficient on the CUDA cores (v_0 is needed by every row's rescale).
+// Same result as k_moddown, word for word.
+constexpr int kMdEpilogueWarps = 16;
+constexpr int kMdLoaderWarp0 = 16;
+constexpr int kMdLoaderWarps = 4;   // one coefficient per loader thread
+constexpr int kMdMmaWarp = 20;
+constexpr int kMdThreads = 32 * 21;
+constexpr int kMdV0Slots = 8;
+constexpr int kMdNumBarriers = 1 + 2 * kASlots + 2 * kAccSlots + 2 * kMdV0Slots + 2;  // ... drain, never
+constexpr int kMdBarrierBytes = 384;
+static_assert(8 * kMdNumBarriers + 8 <= kMdBarrierBytes, "barrier area");
+static_assert(32 * kMdLoaderWarps == kUnit, "one loader thread per coefficient of a unit");
+
+struct ModDownArgs {
+  const uint64_t* t0;          // [B][qp_limbs][N] canonical
+  const uint64_t* t1;
+  const uint64_t* add0;        // nullable [B][q_limbs][N] canonical (read through sigma_g for a rotation)
+  const uint64_t* add1;        // nullable
+  uint64_t* out;               // [2][B][out_limbs][N]
+  const uint8_t* bmat;         // [nchunks][128 K]: P part -> Q_l rows of this level
+  const uint64_t* pinfo;       // [QP0][2]: p, -p^{-1} mod 2^64
+  ChainTables<uint64_t> tabs;  // primes, P Garner / mix / inverse constants
+  const TwPair<uint64_t>* rescale_inv;  // [QP0] of this level
+  const uint32_t* item_galois;          // nullable: per-item Galois element of add0
+  uint32_t add0_ginv;                   // else one inverse Galois element (0: none)
+  int64_t batch;
+  int level, num_q, num_p, q_limbs, out_limbs, nchunks, log_n, rescale;
+  int* err;
+  unsigned long long wait_ns;
+  int stall;
+};
+
+template <int KS>
+__global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) {
+  using W = Word<uint64_t>;
+  constexpr int K = 32 * KS;
+  constexpr int kSbo = K / 16 * 128;
+  constexpr int kATile = kUnit * K;
+  constexpr int kBTile = 128 * K;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw0 = smem_addr(smem_raw);
+  const uint32_t base = (raw0 + 1023u) & ~1023u;
+  uint8_t* const gbase = smem_raw + (base - raw0);
+  const int bbytes = args.nchunks * kBTile;
+  // [B tiles | A tiles | v0 slots | barriers]
+  const uint32_t b_addr = base;
+  const uint32_t a_addr0 = base + uint32_t(bbytes);
+  uint8_t* const a_tile0 = gbase + bbytes;
+  uint64_t* const v0s = reinterpret_cast<uint64_t*>(gbase + bbytes + kASlots * kATile);
+  uint64_t* const bars = v0s + kMdV0Slots * kUnit;
+  const uint32_t bar0 = smem_addr(bars);
+  const uint32_t bfull = bar0;
+  auto afull = [&](int s) { return bar0 + 8u * (1 + s); };
+  auto aempty = [&](int s) { return bar0 + 8u * (1 + kASlots + s); };
+  auto accfull = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + s); };
+  auto accempty = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + kAccSlots + s); };
+  auto v0full = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + 2 * kAccSlots + s); };
+  auto v0empty = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + 2 * kAccSlots + kMdV0Slots + s); };
+  const uint32_t drain_bar = bar0 + 8u * (kMdNumBarriers - 2);
+  const uint32_t never_bar = bar0 + 8u * (kMdNumBarriers - 1);  // nothing arrives on it
+  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + kMdNumBarriers);
+  volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t n = int64_t(1) << args.log_n;
+  const int64_t nblk = n / kUnit;
+  const int64_t per_comp = args.batch * nblk;
+  const int64_t units = 2 * per_comp;
+  const int64_t u_begin = units * blockIdx.x / gridDim.x, u_end = units * (blockIdx.x + 1) / gridDim.x;
+  const int nu = int(u_end - u_begin);
+  const unsigned long long lim = args.wait_ns;
+  const int qp_limbs = args.q_limbs + args.num_p;
+  // unit i of this CTA -> (component, ciphertext, coefficient block)
+  auto unit_of = [&](int i, int& c, int64_t& b, int64_t& blk) {
+    const int64_t u = u_begin + i;
+    c = int(u / per_comp);
+    const int64_t r = u % per_comp;
+    b = r / nblk;
+    blk = r % nblk;
+  };
+  // add_i of component c at coefficient k (sigma_g applied to add0 for rotations)
+  auto addend = [&](int c, int64_t b, int i, int k, uint64_t q) -> uint64_t {
+    const uint64_t* ad = c == 0 ? args.add0 : args.add1;
+    if (!ad) return 0;
+    int kk = k;
+    bool neg = false;
+    if (c == 0) {
+      const uint32_t gi = args.item_galois
+                              ? (args.item_galois[b] == 1 ? 0u : galois_inverse_dev(args.item_galois[b], args.log_n))
+                              : args.add0_ginv;
+      if (gi) kk = galois_source(k, args.log_n, gi, neg);
+    }
+    uint64_t x = csub(ad[(b * args.q_limbs + i) * n + kk], q);
+    return (neg && x) ? q - x : x;
+  };
+
+  if (tid == 0) {
+    mbar_init(bfull, 1);
+    for (int s = 0; s < kASlots; ++s) {
+      mbar_init(afull(s), kMdLoaderWarps);
+      mbar_init(aempty(s), 1);
+    }
+    for (int s = 0; s < kAccSlots; ++s) {
+      mbar_init(accfull(s), 1);
+      mbar_init(accempty(s), kMdEpilogueWarps);
+    }
+    for (int s = 0; s < kMdV0Slots; ++s) {
+      mbar_init(v0full(s), kMdLoaderWarps);
+      mbar_init(v0empty(s), kMdEpilogueWarps);
+    }
+    mbar_init(drain_bar, 1);
+    mbar_init(never_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == kMdMmaWarp) tmem_alloc(smem_addr(tmem_slot), kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp >= kMdLoaderWarp0 && warp < kMdLoaderWarp0 + kMdLoaderWarps) {
+    // Garner digits e_r of the P part of one coefficient -> the A tile (word
+    // (m, r) at (m / 8) sbo + (r / 2) 128 + (m % 8) 16 + (r % 2) 8; rows r >= P
+    // zero); with rescale also v_0 of the coefficient -> its v0 slot
+    const int m = tid - kMdLoaderWarp0 * 32;
+    const bool bthread = m == 0;
+    if (bthread) {  // the level's byte matrices, once
+      mbar_expect_tx(bfull, uint32_t(bbytes));
+      for (int o = 0; o < bbytes; o += 16384)
+        bulk_load(b_addr + uint32_t(o), args.bmat + o, uint32_t(min(16384, bbytes - o)), bfull);
+    }
+    const PrimeInfo<uint64_t> p0 = args.tabs.prime[args.level];
+    for (int i = 0; i < nu; ++i) {
+      int c;
+      int64_t b, blk;
+      unit_of(i, c, b, blk);
+      const int s = i % kASlots, vs = i % kMdV0Slots;
+      if (i >= kASlots && !warp_wait(aempty(s), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, lim)) break;
+      if (args.rescale && i >= kMdV0Slots &&
+          !warp_wait(v0empty(vs), ((i / kMdV0Slots) & 1) ^ 1, abort, args.err, lane, lim))
+        break;
+      const int k = int(blk * kUnit) + m;
+      const uint64_t* t = (c == 0 ? args.t0 : args.t1) + b * qp_limbs * n;
+      uint64_t e[kMaxDigitWidth];
+#pragma unroll
+      for (int r = 0; r < kMaxDigitWidth; ++r)
+        e[r] = r < args.num_p ? t[(args.q_limbs + r) * n + k] : 0;
+      for (int r = 0; r < args.num_p; ++r) {
+        const PrimeInfo<uint64_t> p = args.tabs.prime[args.num_q + r];
+        uint64_t x = csub(e[r], p.q);
+        if (r > 0) {
+          uint64_t acc = 0;
+          for (int j = 0; j < r; ++j) {
+            const TwPair<uint64_t> g = args.tabs.p_garner[r * kMaxDigitWidth + j];
+            acc = csub(acc + csub(W::shoup(e[j], g.w, g.wp, p.q), p.q), p.q);
+          }
+          const TwPair<uint64_t> inv = args.tabs.p_garner[r * kMaxDigitWidth + r];
+          x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
+        }
+        e[r] = x;
+      }
+      uint8_t* at = a_tile0 + s * kATile + (m >> 3) * kSbo + (m & 7) * 16;
+#pragma unroll
+      for (int r2 = 0; r2 < 2 * KS; ++r2)
+        *reinterpret_cast<ulonglong2*>(at + r2 * 128) =
+            make_ulonglong2(2 * r2 < kMaxDigitWidth ? e[2 * r2] : 0, 2 * r2 + 1 < kMaxDigitWidth ? e[2 * r2 + 1] : 0);
+      if (args.rescale) {
+        uint64_t sub = 0;
+        for (int r = 0; r < args.num_p; ++r) {
+          const TwPair<uint64_t> mx = args.tabs.p_mix[int64_t(r) * (args.num_q + args.num_p) + args.level];
+          sub = csub(sub + csub(W::shoup(e[r], mx.w, mx.wp, p0.q), p0.q), p0.q);
+        }
+        const TwPair<uint64_t> pinv = args.tabs.p_inv[args.level];
+        uint64_t v = csub(csub(t[k], p0.q) + p0.q - sub, p0.q);
+        v = csub(W::shoup(v, pinv.w, pinv.wp, p0.q), p0.q);
+        v0s[vs * kUnit + m] = csub(v + addend(c, b, 0, k, p0.q), p0.q);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(afull(s));
+        if (args.rescale) mbar_arrive(v0full(vs));
+      }
+    }
+    // after an abort, wait (bounded, default limit) for the byte-matrix copy
+    if (bthread && *abort) mbar_wait(bfull, 0, nullptr, args.err, kWaitNs);
+  } else if (warp == kMdMmaWarp && lane == 0) {
+    bool ok = mbar_wait(bfull, 0, abort, args.err, lim);
+    int t = 0;
+    for (int i = 0; i < nu && ok; ++i) {
+      const int s = i % kASlots;
+      if (!mbar_wait(afull(s), (i / kASlots) & 1, abort, args.err, lim)) break;
+      tc_fence_after();
+      const uint32_t a_base = a_addr0 + uint32_t(s * kATile);
+      for (int ch = 0; ch < args.nchunks; ++ch, ++t) {
+        const int slot = t % kAccSlots;
+        if (t >= kAccSlots && !mbar_wait(accempty(slot), ((t / kAccSlots) & 1) ^ 1, abort, args.err, lim)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int rows = min(kChunkRows, args.q_limbs - ch * kChunkRows);
+        const uint32_t idesc = instr_desc_u8(uint32_t((rows * 8 + 15) & ~15));
+#pragma unroll
+        for (int ks = 0; ks < KS; ++ks)
+          mma_i8(tmem + uint32_t(slot * kAccCols), smem_desc(a_base + ks * 256, 128, kSbo),
+                 smem_desc(b_addr + uint32_t(ch * kBTile + ks * 256), 128, kSbo), idesc, ks > 0 ? 1u : 0u);
+        mma_commit(accfull(slot));
+      }
+      if (ok) mma_commit(aempty(s));
+    }
+  } else if (warp < kMdEpilogueWarps) {
+    const int quarter = warp & 3, grp = warp >> 2;
+    const int m = quarter * 32 + lane;
+    const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
+    const uint64_t half0 = args.tabs.prime[args.level].q >> 1;
+    int t = 0;
+    // test only: a wait that must run out (its limit is the pipeline's)
+    bool ok = !args.stall || warp_wait(never_bar, 0, abort, args.err, lane, lim);
+    for (int i = 0; i < nu && ok; ++i) {
+      int c;
+      int64_t b, blk;
+      unit_of(i, c, b, blk);
+      const int k = int(blk * kUnit) + m;
+      const uint64_t* tt = (c == 0 ? args.t0 : args.t1) + b * qp_limbs * n + k;
+      uint64_t* o = args.out + (int64_t(c) * args.batch + b) * args.out_limbs * n + k;
+      const int vs = i % kMdV0Slots;
+      uint64_t v0 = 0;
+      if (args.rescale) {
+        if (!warp_wait(v0full(vs), (i / kMdV0Slots) & 1, abort, args.err, lane, lim)) break;
+        v0 = v0s[vs * kUnit + m];
+      }
+      for (int ch = 0; ch < args.nchunks; ++ch, ++t) {
+        const int slot = t % kAccSlots;
+        if (!warp_wait(accfull(slot), (t / kAccSlots) & 1, abort, args.err, lane, lim)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        uint32_t acc[32];
+        tmem_ld32(tmem + lane_addr + uint32_t(slot * kAccCols + grp * 32), acc);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(accempty(slot));
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int row = ch * kChunkRows + grp * 4 + jj;
+          if (row >= args.q_limbs || (args.rescale && row == 0)) continue;
+          const int pid = args.level + row;
+          const ulonglong2 pi = __ldg(reinterpret_cast<const ulonglong2*>(args.pinfo) + pid);
+          const uint64_t q = pi.x;
+          const uint64_t sub = csub(recombine_redc(acc + 8 * jj, q, pi.y), q);
+          const TwPair<uint64_t> pinv = args.tabs.p_inv[pid];
+          uint64_t v = csub(csub(tt[int64_t(row) * n], q) + q - sub, q);
+          v = csub(W::shoup(v, pinv.w, pinv.wp, q), q);
+          v = csub(v + addend(c, b, row, k, q), q);
+          if (!args.rescale) {
+            o[int64_t(row) * n] = v;
+          } else {
+            const PrimeInfo<uint64_t> p = args.tabs.prime[pid];
+            const uint64_t x0 = reduce_any(v0, p);
+            const TwPair<uint64_t> inv = args.rescale_inv[pid];
+            uint64_t r = csub(W::shoup(csub(v + q - x0, q), inv.w, inv.wp, q), q);
+            r += v0 > half0 ? 1u : 0u;
+            o[int64_t(row - 1) * n] = csub(r, q);
+          }
+        }
+      }
+      if (args.rescale && ok) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(v0empty(vs));
+      }
+    }
+  }
+
+  __syncthreads();
+  if (warp == kMdMmaWarp && lane == 0) {
+    mma_commit(drain_bar);
+    mbar_wait(drain_bar, 0, nullptr, args.err, kWaitNs);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMdMmaWarp) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
 }  // namespace tcb
 
 // ------------------------------------------------------------------ host ---
@@ -357,13 +665,39 @@ void tc_basis_tables_host(const Context& c, int level, int ks, std::vector<uint8
   }
 }
 
+// ModDown byte matrices of one level (host): chunk c, Q row i = 16 c + il,
+// MMA row n = 8 il + e, K position kap = 8 r + u holds byte e of
+// 2^{8u} 2^64 (M_r mod q_{level+i}) mod q, M_r the product of the first r
+// special primes.
+void tc_moddown_tables_host(const Context& c, int level, int ks, std::vector<uint8_t>& out) {
+  const int k = 32 * ks, sbo = k / 16 * 128, tile = 128 * k;
+  const int ql = c.num_q - level;
+  out.assign(size_t(chunks_for(ql)) * tile, 0);
+  for (int i = 0; i < ql; ++i) {
+    const uint64_t q = c.moduli[level + i];
+    uint8_t* t = out.data() + size_t(i / tcb::kChunkRows) * tile;
+    const int il = i % tcb::kChunkRows;
+    uint64_t mr = 1 % q;
+    for (int r = 0; r < c.num_p; ++r) {
+      if (r > 0) mr = uint64_t((u128)mr * (c.moduli[c.num_q + r - 1] % q) % q);
+      for (int u = 0; u < 8; ++u) {
+        const uint64_t scaled = uint64_t((u128(uint64_t((u128(mr) << (8 * u)) % q)) << 64) % q);
+        const int kap = 8 * r + u;
+        for (int e = 0; e < 8; ++e) t[il * sbo + (kap >> 4) * 128 + e * 16 + (kap & 15)] = uint8_t(scaled >> (8 * e));
+      }
+    }
+  }
+}
+
 int tc_basis_prepare(Context& c) {
   std::lock_guard<std::mutex> lock(c.tcb_mutex);
   if (c.tcb) return 0;
   if (c.bits != 64) return fail(-7, "the tensor-core basis conversion needs an int64 context");
   if (c.log_n < 7) return fail(-7, "ring too small for the tensor-core basis conversion");
   const int ks = ksteps_for(c.num_p);
-  if (smem_for(chunks_for(c.qp()), ks) > 227 * 1024)
+  if (smem_for(chunks_for(c.qp()), ks) > 227 * 1024 ||
+      1024 + chunks_for(c.num_q) * 128 * 32 * ks + (tcb::kASlots * tcb::kUnit * 32 * ks) +
+              tcb::kMdV0Slots * tcb::kUnit * 8 + tcb::kMdBarrierBytes > 227 * 1024)
     return fail(-7, "the chain is too long for the tensor-core basis conversion's shared-memory tables");
   auto* t = new TcBasisTables();
   t->ks = ks;
@@ -382,11 +716,17 @@ int tc_basis_prepare(Context& c) {
   };
   std::vector<uint8_t> host;
   t->bmat.assign(c.num_q, nullptr);
+  t->md_bmat.assign(c.num_q, nullptr);
   for (int level = 0; level < c.num_q; ++level) {
     tc_basis_tables_host(c, level, ks, host);
     t->bmat[level] = static_cast<uint8_t*>(dev_alloc(host.size()));
     if (!t->bmat[level] || cudaMemcpy(t->bmat[level], host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
       return give_up("tensor-core basis conversion byte matrices");
+    tc_moddown_tables_host(c, level, ks, host);
+    t->md_bmat[level] = static_cast<uint8_t*>(dev_alloc(host.size()));
+    if (!t->md_bmat[level] ||
+        cudaMemcpy(t->md_bmat[level], host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return give_up("tensor-core ModDown byte matrices");
   }
   std::vector<uint64_t> pinfo(2 * size_t(c.qp()));
   for (int j = 0; j < c.qp(); ++j) {
@@ -429,6 +769,30 @@ int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int leve
                     skip_own ? 1 : 0, t.err, c.tc_wait_ns ? c.tc_wait_ns : tc::kWaitNs, c.tc_test_stall};
   kern<<<grid, tcb::kThreads, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "k_tc_extend");
+}
+
+int tc_moddown(Context& c, const void* t0, const void* t1, const void* add0, const void* add1, void* out,
+               int64_t batch, int level, uint32_t add0_ginv, const uint32_t* item_galois, int rescale,
+               cudaStream_t st) {
+  if (int rc = tc_basis_prepare(c)) return rc;
+  const TcBasisTables& t = *c.tcb;
+  if (batch == 0) return 0;
+  const int ql = c.num_q - level, nch = chunks_for(ql);
+  const int k = 32 * t.ks;
+  int smem = 1024 + nch * 128 * k + tcb::kASlots * tcb::kUnit * k + tcb::kMdV0Slots * tcb::kUnit * 8 +
+             tcb::kMdBarrierBytes;
+  if (smem < tcb::kMinSmem) smem = tcb::kMinSmem;
+  auto kern = t.ks == 1 ? tcb::k_tc_moddown<1> : tcb::k_tc_moddown<2>;
+  if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return rc;
+  const int64_t units = 2 * batch * (c.n() / tcb::kUnit);
+  const int grid = int(units < t.sms ? units : t.sms);
+  tcb::ModDownArgs a{static_cast<const uint64_t*>(t0), static_cast<const uint64_t*>(t1),
+                     static_cast<const uint64_t*>(add0), static_cast<const uint64_t*>(add1),
+                     static_cast<uint64_t*>(out), t.md_bmat[level], t.pinfo, c.t64, c.lv64[level].rescale_inv,
+                     item_galois, add0_ginv, batch, level, c.num_q, c.num_p, ql, ql - (rescale ? 1 : 0), nch,
+                     c.log_n, rescale, t.err, c.tc_wait_ns ? c.tc_wait_ns : tc::kWaitNs, c.tc_test_stall};
+  kern<<<grid, tcb::kMdThreads, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "k_tc_moddown");
 }
 
 int tc_basis_status(Context& c, int* flag) {
