@@ -61,13 +61,21 @@ constexpr int kAccCols = 128;          // TMEM columns per accumulator slot
 constexpr int kAccSlots = 4;
 constexpr int kASlots = 4;
 constexpr int kTmemCols = kAccSlots * kAccCols;  // 512: the whole SM
-constexpr int kEpilogueWarps = 16;
-constexpr int kLoaderWarp0 = 16;
-constexpr int kLoaderWarps = 2;
-constexpr int kMmaWarp = 18;
-constexpr int kThreads = 32 * 19;
-constexpr int kNumBarriers = 2 + 2 + 2 * kASlots + 2 * kAccSlots + 2;  // ... drain, never
-constexpr int kBarrierBytes = 256;
+constexpr int kEpilogueWarps = 16;     // warps 0..15
+constexpr int kPermuteWarp0 = 16;      // warps 16, 17
+constexpr int kPermuteWarps = 2;
+constexpr int kProducerWarp = 18;
+constexpr int kMmaWarp = 19;
+constexpr int kThreads = 32 * 20;
+constexpr int kRowBytes = kUnit * 8;   // one digit row of a unit, 1 KiB
+// raw staging slots (one unit's digit rows each): deep enough that the
+// bulk copies of several units are in flight behind the one being permuted
+template <int KS>
+constexpr int raw_slots() { return KS == 1 ? 8 : 6; }
+constexpr int kMaxRawSlots = 8;
+constexpr int kPinfoBytes = 2048;      // the level's (p, -p^{-1} mod 2^64) pairs, up to 128 rows
+constexpr int kNumBarriers = 2 + 2 + 2 * kMaxRawSlots + 2 * kASlots + 2 * kAccSlots + 2;  // ... drain, never
+constexpr int kBarrierBytes = 384;
 // Requested even when the tables are smaller, so that no second CTA (which
 // would wait for TMEM) is ever resident beside the first.
 constexpr int kMinSmem = 120 * 1024;
@@ -87,15 +95,44 @@ struct ExtendArgs {
   int stall;                   // test only: the epilogue first waits on a barrier nothing completes
 };
 
+// Position of a CTA's current unit in its contiguous range of the unit list
+// (outer, ciphertext, coefficient block), advanced by counting instead of
+// dividing: a 64-bit division per unit and thread costs as much as the
+// epilogue's arithmetic.
+struct UnitIter {
+  int outer;      // digit (basis extension) or component (ModDown)
+  int64_t b;      // ciphertext
+  int64_t blk;    // block of kUnit coefficients
+  int64_t batch, nblk;
+  __device__ __forceinline__ UnitIter(int64_t u, int64_t batch_, int64_t nblk_) : batch(batch_), nblk(nblk_) {
+    const int64_t per_outer = batch_ * nblk_;
+    outer = int(u / per_outer);
+    const int64_t r = u - int64_t(outer) * per_outer;
+    b = r / nblk_;
+    blk = r - b * nblk_;
+  }
+  __device__ __forceinline__ void next() {
+    if (++blk == nblk) {
+      blk = 0;
+      if (++b == batch) {
+        b = 0;
+        ++outer;
+      }
+    }
+  }
+};
+
 // Extension value from the eight byte accumulators of one output:
 // S = sum_e 2^{8e} acc_e (< 2^78) and its Montgomery reduction by 2^64.
+// Accumulators are < 2^22, so byte-adjacent pairs combine in 32 bits
+// (acc_e + 2^8 acc_{e+1} < 2^31) and the pairs in two 48-bit halves.
 __device__ __forceinline__ uint64_t recombine_redc(const uint32_t* acc, uint64_t p, uint64_t pneg) {
-  const uint64_t lo4 = uint64_t(acc[0]) + (uint64_t(acc[1]) << 8) + (uint64_t(acc[2]) << 16) +
-                       (uint64_t(acc[3]) << 24);  // < 2^47
-  const uint64_t hi4 = uint64_t(acc[4]) + (uint64_t(acc[5]) << 8) + (uint64_t(acc[6]) << 16) +
-                       (uint64_t(acc[7]) << 24);
-  const uint64_t slo = lo4 + (hi4 << 32);
-  const uint64_t shi = (hi4 >> 32) + (slo < lo4 ? 1u : 0u);
+  const uint32_t p01 = acc[0] + (acc[1] << 8), p23 = acc[2] + (acc[3] << 8);
+  const uint32_t p45 = acc[4] + (acc[5] << 8), p67 = acc[6] + (acc[7] << 8);
+  const uint64_t lo = uint64_t(p01) + (uint64_t(p23) << 16);  // S mod 2^32 part, < 2^48
+  const uint64_t hi = uint64_t(p45) + (uint64_t(p67) << 16);  // coefficient of 2^32, < 2^48
+  const uint64_t slo = lo + (hi << 32);
+  const uint64_t shi = (hi >> 32) + (slo < lo ? 1u : 0u);
   const uint64_t m = slo * pneg;  // S + m p = 0 mod 2^64
   return shi + __umul64hi(m, p) + (slo != 0 ? 1u : 0u);
 }
@@ -106,24 +143,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
   constexpr int kSbo = K / 16 * 128;   // byte distance between 8-row groups
   constexpr int kATile = kUnit * K;
   constexpr int kBTile = 128 * K;      // byte matrix of one 16-row chunk (128 MMA N rows)
+  constexpr int kRawSlots = raw_slots<KS>();
+  constexpr int kRawSlotBytes = 4 * KS * kRowBytes;  // up to 4 KS digit rows
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw0 = smem_addr(smem_raw);
   const uint32_t base = (raw0 + 1023u) & ~1023u;
   uint8_t* const gbase = smem_raw + (base - raw0);
   const int bbytes = args.nchunks * kBTile;
-  const uint32_t b_addr0 = base;  // B buffers [2][bbytes], then A tiles [kASlots][kATile], then barriers
-  const uint32_t a_addr0 = base + 2u * uint32_t(bbytes);
-  uint8_t* const a_tile0 = gbase + 2 * bbytes;
-  uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + 2 * bbytes + kASlots * kATile);
+  // [B buffers 2 x bbytes | raw slots | A tiles | pinfo | barriers]
+  const uint32_t b_addr0 = base;
+  const uint32_t rawbuf_addr = base + 2u * uint32_t(bbytes);
+  const uint64_t* const rawbuf = reinterpret_cast<const uint64_t*>(gbase + 2 * bbytes);
+  const uint32_t a_addr0 = rawbuf_addr + uint32_t(kRawSlots * kRawSlotBytes);
+  uint8_t* const a_tile0 = gbase + 2 * bbytes + kRawSlots * kRawSlotBytes;
+  ulonglong2* const spinfo = reinterpret_cast<ulonglong2*>(a_tile0 + kASlots * kATile);
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(a_tile0 + kASlots * kATile + kPinfoBytes);
   const uint32_t bar0 = smem_addr(bars);
   auto bfull = [&](int x) { return bar0 + 8u * x; };
   auto bempty = [&](int x) { return bar0 + 8u * (2 + x); };
-  auto afull = [&](int s) { return bar0 + 8u * (4 + s); };
-  auto aempty = [&](int s) { return bar0 + 8u * (4 + kASlots + s); };
-  auto accfull = [&](int s) { return bar0 + 8u * (4 + 2 * kASlots + s); };
-  auto accempty = [&](int s) { return bar0 + 8u * (4 + 2 * kASlots + kAccSlots + s); };
-  const uint32_t drain_bar = bar0 + 8u * (kNumBarriers - 1);
-  const uint32_t never_bar = bar0 + 8u * (kNumBarriers - 2);  // nothing arrives on it
+  auto rawfull = [&](int r) { return bar0 + 8u * (4 + r); };
+  auto rawempty = [&](int r) { return bar0 + 8u * (4 + kMaxRawSlots + r); };
+  auto afull = [&](int s) { return bar0 + 8u * (4 + 2 * kMaxRawSlots + s); };
+  auto aempty = [&](int s) { return bar0 + 8u * (4 + 2 * kMaxRawSlots + kASlots + s); };
+  auto accfull = [&](int s) { return bar0 + 8u * (4 + 2 * kMaxRawSlots + 2 * kASlots + s); };
+  auto accempty = [&](int s) { return bar0 + 8u * (4 + 2 * kMaxRawSlots + 2 * kASlots + kAccSlots + s); };
+  const uint32_t drain_bar = bar0 + 8u * (kNumBarriers - 2);
+  const uint32_t never_bar = bar0 + 8u * (kNumBarriers - 1);  // nothing arrives on it
   uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + kNumBarriers);
   volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -135,22 +180,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
   const int64_t u_begin = units * blockIdx.x / gridDim.x, u_end = units * (blockIdx.x + 1) / gridDim.x;
   const int nu = int(u_end - u_begin);
   const unsigned long long lim = args.wait_ns;
-  // unit i of this CTA -> (digit, ciphertext, coefficient block)
-  auto unit_of = [&](int i, int& a, int64_t& b, int64_t& blk) {
-    const int64_t u = u_begin + i;
-    a = int(u / per_digit);
-    const int64_t r = u % per_digit;
-    b = r / nblk;
-    blk = r % nblk;
-  };
 
+  for (int j = tid; j < args.qp_limbs; j += kThreads)
+    spinfo[j] = reinterpret_cast<const ulonglong2*>(args.pinfo)[args.level + j];
   if (tid == 0) {
     for (int x = 0; x < 2; ++x) {
       mbar_init(bfull(x), 1);
       mbar_init(bempty(x), 1);
     }
+    for (int r = 0; r < kRawSlots; ++r) {
+      mbar_init(rawfull(r), 1);
+      mbar_init(rawempty(r), kPermuteWarps);
+    }
     for (int s = 0; s < kASlots; ++s) {
-      mbar_init(afull(s), kLoaderWarps);
+      mbar_init(afull(s), kPermuteWarps);
       mbar_init(aempty(s), 1);
     }
     for (int s = 0; s < kAccSlots; ++s) {
@@ -169,68 +212,77 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp >= kLoaderWarp0 && warp < kLoaderWarp0 + kLoaderWarps) {
-    // A tiles: word (coefficient m, digit row r) at byte (m / 8) sbo + (r / 2) 128 + (m % 8) 16 + (r % 2) 8,
-    // i.e. its 8 bytes are K positions 8 r .. 8 r + 7; rows r >= alpha are zero.
-    const int lt = tid - kLoaderWarp0 * 32;
-    const bool bthread = lt == 0;  // also streams the byte matrices
-    int cur = -1, dseq = -1;
+  if (warp == kProducerWarp && lane == 0) {
+    // the byte matrices of each new digit into one of two B buffers, and the
+    // digit rows of each unit (alpha contiguous 1 KiB rows) into a raw slot
+    int cur = -1, dseq = -1, i = 0;
     int issued[2] = {0, 0};
-    for (int i = 0; i < nu; ++i) {
-      int a;
-      int64_t b, blk;
-      unit_of(i, a, b, blk);
+    UnitIter it(u_begin, args.batch, nblk);
+    for (; i < nu; ++i, it.next()) {
+      const int a = it.outer;
+      const int64_t b = it.b, blk = it.blk;
       if (a != cur) {
         cur = a;
         ++dseq;
-        if (bthread) {
-          const int x = dseq & 1;
-          if (dseq < 2 || mbar_wait(bempty(x), ((dseq >> 1) - 1) & 1, abort, args.err, lim)) {
-            mbar_expect_tx(bfull(x), uint32_t(bbytes));
-            const uint8_t* src = args.bmat + size_t(a) * size_t(bbytes);
-            for (int o = 0; o < bbytes; o += 16384)
-              bulk_load(b_addr0 + uint32_t(x * bbytes + o), src + o, uint32_t(min(16384, bbytes - o)), bfull(x));
-            ++issued[x];
-          }
-        }
+        const int x = dseq & 1;
+        if (dseq >= 2 && !mbar_wait(bempty(x), ((dseq >> 1) - 1) & 1, abort, args.err, lim)) break;
+        mbar_expect_tx(bfull(x), uint32_t(bbytes));
+        const uint8_t* src = args.bmat + size_t(a) * size_t(bbytes);
+        for (int o = 0; o < bbytes; o += 16384)
+          bulk_load(b_addr0 + uint32_t(x * bbytes + o), src + o, uint32_t(min(16384, bbytes - o)), bfull(x));
+        ++issued[x];
       }
-      if (__shfl_sync(0xffffffffu, (warp == kLoaderWarp0 && lane == 0) ? int(*abort) : 0, 0)) break;
-      const int s = i % kASlots;
-      if (i >= kASlots && !warp_wait(aempty(s), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, lim)) break;
+      const int r = i % kRawSlots;
+      if (i >= kRawSlots && !mbar_wait(rawempty(r), ((i / kRawSlots) & 1) ^ 1, abort, args.err, lim)) break;
       const DigitDesc d = args.digit[a];
       const uint64_t* src = args.digits + (b * args.q_limbs + (d.prime0 - args.level)) * n + blk * kUnit;
+      mbar_expect_tx(rawfull(r), uint32_t(d.alpha * kRowBytes));
+      for (int rr = 0; rr < d.alpha; ++rr)
+        bulk_load(rawbuf_addr + uint32_t(r * kRawSlotBytes + rr * kRowBytes), src + int64_t(rr) * n, kRowBytes,
+                  rawfull(r));
+    }
+    // after an abort, wait (bounded, default limit) for the copies still in flight
+    if (*abort) {
+      for (int x = 0; x < 2; ++x)
+        if (issued[x] > 0) mbar_wait(bfull(x), (issued[x] - 1) & 1, nullptr, args.err, kWaitNs);
+      for (int t = i - kRawSlots < 0 ? 0 : i - kRawSlots; t < i; ++t)
+        mbar_wait(rawfull(t % kRawSlots), (t / kRawSlots) & 1, nullptr, args.err, kWaitNs);
+    }
+  } else if (warp >= kPermuteWarp0 && warp < kPermuteWarp0 + kPermuteWarps) {
+    // raw rows -> A tile: word (coefficient m, digit row r) at byte
+    // (m / 8) sbo + (r / 2) 128 + (m % 8) 16 + (r % 2) 8, i.e. its 8 bytes are
+    // K positions 8 r .. 8 r + 7; rows r >= alpha are zero.
+    const int lt = tid - kPermuteWarp0 * 32;
+    UnitIter it(u_begin, args.batch, nblk);
+    for (int i = 0; i < nu; ++i, it.next()) {
+      const int a = it.outer;
+      const int r = i % kRawSlots, s = i % kASlots;
+      if (!warp_wait(rawfull(r), (i / kRawSlots) & 1, abort, args.err, lane, lim)) break;
+      if (i >= kASlots && !warp_wait(aempty(s), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, lim)) break;
+      const int alpha = args.digit[a].alpha;
+      const uint64_t* raw = rawbuf + r * (kRawSlotBytes / 8);
       uint8_t* at = a_tile0 + s * kATile;
-      constexpr int kPerThread = kUnit * KS * 2 / (32 * kLoaderWarps);
-      uint64_t w0[kPerThread], w1[kPerThread];
 #pragma unroll
-      for (int it = 0; it < kPerThread; ++it) {
-        const int idx = lt + it * 32 * kLoaderWarps;
-        const int m = idx & (kUnit - 1), r0 = 2 * (idx >> 7);
-        w0[it] = r0 < d.alpha ? __ldg(src + int64_t(r0) * n + m) : 0;
-        w1[it] = r0 + 1 < d.alpha ? __ldg(src + int64_t(r0 + 1) * n + m) : 0;
-      }
-#pragma unroll
-      for (int it = 0; it < kPerThread; ++it) {
-        const int idx = lt + it * 32 * kLoaderWarps;
+      for (int it = 0; it < kUnit * 2 * KS / (32 * kPermuteWarps); ++it) {
+        const int idx = lt + it * 32 * kPermuteWarps;
         const int m = idx & (kUnit - 1), r2 = idx >> 7;
-        *reinterpret_cast<ulonglong2*>(at + (m >> 3) * kSbo + r2 * 128 + (m & 7) * 16) =
-            make_ulonglong2(w0[it], w1[it]);
+        const uint64_t w0 = 2 * r2 < alpha ? raw[(2 * r2) * kUnit + m] : 0;
+        const uint64_t w1 = 2 * r2 + 1 < alpha ? raw[(2 * r2 + 1) * kUnit + m] : 0;
+        *reinterpret_cast<ulonglong2*>(at + (m >> 3) * kSbo + r2 * 128 + (m & 7) * 16) = make_ulonglong2(w0, w1);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(afull(s));
+      if (lane == 0) {
+        mbar_arrive(rawempty(r));
+        mbar_arrive(afull(s));
+      }
     }
-    // after an abort, wait (bounded, default limit) for byte-matrix copies still in flight
-    if (bthread && *abort)
-      for (int x = 0; x < 2; ++x)
-        if (issued[x] > 0) mbar_wait(bfull(x), (issued[x] - 1) & 1, nullptr, args.err, kWaitNs);
   } else if (warp == kMmaWarp && lane == 0) {
     int cur = -1, dseq = -1, t = 0;
     bool ok = true;
-    for (int i = 0; i < nu && ok; ++i) {
-      int a;
-      int64_t b, blk;
-      unit_of(i, a, b, blk);
+    UnitIter it(u_begin, args.batch, nblk);
+    for (int i = 0; i < nu && ok; ++i, it.next()) {
+      const int a = it.outer;
       if (a != cur) {
         if (dseq >= 0) mma_commit(bempty(dseq & 1));  // the previous digit's byte matrix may be overwritten
         cur = a;
@@ -266,10 +318,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
     int t = 0;
     // test only: a wait that must run out (its limit is the pipeline's)
     bool ok = !args.stall || warp_wait(never_bar, 0, abort, args.err, lane, lim);
-    for (int i = 0; i < nu && ok; ++i) {
-      int a;
-      int64_t b, blk;
-      unit_of(i, a, b, blk);
+    UnitIter it(u_begin, args.batch, nblk);
+    for (int i = 0; i < nu && ok; ++i, it.next()) {
+      const int a = it.outer;
+      const int64_t b = it.b, blk = it.blk;
       const DigitDesc d = args.digit[a];
       const int own0 = args.skip_own ? d.prime0 - args.level : 0, own1 = args.skip_own ? own0 + d.alpha : 0;
       uint64_t* dst = args.ext + (int64_t(a) * args.batch + b) * args.qp_limbs * n + blk * kUnit + m;
@@ -286,12 +338,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(accempty(slot));
+        const int j0 = c * kChunkRows + grp * 4;
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-          const int j = c * kChunkRows + grp * 4 + jj;
-          if (j >= args.qp_limbs || (j >= own0 && j < own1)) continue;
-          const ulonglong2 pi = __ldg(reinterpret_cast<const ulonglong2*>(args.pinfo) + args.level + j);
-          dst[int64_t(j) * n] = recombine_redc(acc + 8 * jj, pi.x, pi.y);
+          const int j = j0 + jj;
+          if (j < args.qp_limbs && (j < own0 || j >= own1)) {
+            const ulonglong2 pi = spinfo[j];
+            dst[int64_t(j) * n] = recombine_redc(acc + 8 * jj, pi.x, pi.y);
+          }
         }
       }
     }
@@ -313,7 +367,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
   }
 }
 
-
 // ---------------------------------------------------------------------------
 // ModDown by P on the tensor cores (int64): for every Q row i of the level
 // and coefficient k of the key-switch accumulators t (canonical coefficient
@@ -334,9 +387,12 @@ constexpr int kMdEpilogueWarps = 16;
 constexpr int kMdLoaderWarp0 = 16;
 constexpr int kMdLoaderWarps = 4;   // one coefficient per loader thread
 constexpr int kMdMmaWarp = 20;
-constexpr int kMdThreads = 32 * 21;
+constexpr int kMdProducerWarp = 21;
+constexpr int kMdThreads = 32 * 22;
 constexpr int kMdV0Slots = 8;
-constexpr int kMdNumBarriers = 1 + 2 * kASlots + 2 * kAccSlots + 2 * kMdV0Slots + 2;  // ... drain, never
+constexpr int kMdRawSlots = 6;      // one unit's P rows and row 0 each (bulk copies in flight)
+constexpr int kMdRawSlotBytes = (kMaxDigitWidth + 1) * kRowBytes;
+constexpr int kMdNumBarriers = 1 + 2 * kMdRawSlots + 2 * kASlots + 2 * kAccSlots + 2 * kMdV0Slots + 2;
 constexpr int kMdBarrierBytes = 384;
 static_assert(8 * kMdNumBarriers + 8 <= kMdBarrierBytes, "barrier area");
 static_assert(32 * kMdLoaderWarps == kUnit, "one loader thread per coefficient of a unit");
@@ -372,20 +428,25 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
   const uint32_t base = (raw0 + 1023u) & ~1023u;
   uint8_t* const gbase = smem_raw + (base - raw0);
   const int bbytes = args.nchunks * kBTile;
-  // [B tiles | A tiles | v0 slots | barriers]
+  // [B tiles | raw slots | A tiles | v0 slots | barriers]
   const uint32_t b_addr = base;
-  const uint32_t a_addr0 = base + uint32_t(bbytes);
-  uint8_t* const a_tile0 = gbase + bbytes;
-  uint64_t* const v0s = reinterpret_cast<uint64_t*>(gbase + bbytes + kASlots * kATile);
+  const uint32_t rawbuf_addr = base + uint32_t(bbytes);
+  const uint64_t* const rawbuf = reinterpret_cast<const uint64_t*>(gbase + bbytes);
+  const uint32_t a_addr0 = rawbuf_addr + uint32_t(kMdRawSlots * kMdRawSlotBytes);
+  uint8_t* const a_tile0 = gbase + bbytes + kMdRawSlots * kMdRawSlotBytes;
+  uint64_t* const v0s = reinterpret_cast<uint64_t*>(a_tile0 + kASlots * kATile);
   uint64_t* const bars = v0s + kMdV0Slots * kUnit;
   const uint32_t bar0 = smem_addr(bars);
   const uint32_t bfull = bar0;
-  auto afull = [&](int s) { return bar0 + 8u * (1 + s); };
-  auto aempty = [&](int s) { return bar0 + 8u * (1 + kASlots + s); };
-  auto accfull = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + s); };
-  auto accempty = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + kAccSlots + s); };
-  auto v0full = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + 2 * kAccSlots + s); };
-  auto v0empty = [&](int s) { return bar0 + 8u * (1 + 2 * kASlots + 2 * kAccSlots + kMdV0Slots + s); };
+  auto rawfull = [&](int r) { return bar0 + 8u * (1 + r); };
+  auto rawempty = [&](int r) { return bar0 + 8u * (1 + kMdRawSlots + r); };
+  constexpr int kA0 = 1 + 2 * kMdRawSlots;
+  auto afull = [&](int s) { return bar0 + 8u * (kA0 + s); };
+  auto aempty = [&](int s) { return bar0 + 8u * (kA0 + kASlots + s); };
+  auto accfull = [&](int s) { return bar0 + 8u * (kA0 + 2 * kASlots + s); };
+  auto accempty = [&](int s) { return bar0 + 8u * (kA0 + 2 * kASlots + kAccSlots + s); };
+  auto v0full = [&](int s) { return bar0 + 8u * (kA0 + 2 * kASlots + 2 * kAccSlots + s); };
+  auto v0empty = [&](int s) { return bar0 + 8u * (kA0 + 2 * kASlots + 2 * kAccSlots + kMdV0Slots + s); };
   const uint32_t drain_bar = bar0 + 8u * (kMdNumBarriers - 2);
   const uint32_t never_bar = bar0 + 8u * (kMdNumBarriers - 1);  // nothing arrives on it
   uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + kMdNumBarriers);
@@ -400,32 +461,31 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
   const int nu = int(u_end - u_begin);
   const unsigned long long lim = args.wait_ns;
   const int qp_limbs = args.q_limbs + args.num_p;
-  // unit i of this CTA -> (component, ciphertext, coefficient block)
-  auto unit_of = [&](int i, int& c, int64_t& b, int64_t& blk) {
-    const int64_t u = u_begin + i;
-    c = int(u / per_comp);
-    const int64_t r = u % per_comp;
-    b = r / nblk;
-    blk = r % nblk;
-  };
-  // add_i of component c at coefficient k (sigma_g applied to add0 for rotations)
-  auto addend = [&](int c, int64_t b, int i, int k, uint64_t q) -> uint64_t {
-    const uint64_t* ad = c == 0 ? args.add0 : args.add1;
-    if (!ad) return 0;
-    int kk = k;
-    bool neg = false;
+  // where the addend of component c, ciphertext b, coefficient k is read:
+  // add0 through sigma_g for a rotation (source index and sign), add1 as is
+  auto addend_source = [&](int c, int64_t b, int k, int& kk, bool& neg) {
+    kk = k;
+    neg = false;
     if (c == 0) {
       const uint32_t gi = args.item_galois
                               ? (args.item_galois[b] == 1 ? 0u : galois_inverse_dev(args.item_galois[b], args.log_n))
                               : args.add0_ginv;
       if (gi) kk = galois_source(k, args.log_n, gi, neg);
     }
+  };
+  auto addend = [&](int c, int64_t b, int i, int kk, bool neg, uint64_t q) -> uint64_t {
+    const uint64_t* ad = c == 0 ? args.add0 : args.add1;
+    if (!ad) return 0;
     uint64_t x = csub(ad[(b * args.q_limbs + i) * n + kk], q);
     return (neg && x) ? q - x : x;
   };
 
   if (tid == 0) {
     mbar_init(bfull, 1);
+    for (int r = 0; r < kMdRawSlots; ++r) {
+      mbar_init(rawfull(r), 1);
+      mbar_init(rawempty(r), kMdLoaderWarps);
+    }
     for (int s = 0; s < kASlots; ++s) {
       mbar_init(afull(s), kMdLoaderWarps);
       mbar_init(aempty(s), 1);
@@ -450,46 +510,71 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp >= kMdLoaderWarp0 && warp < kMdLoaderWarp0 + kMdLoaderWarps) {
+  if (warp == kMdProducerWarp && lane == 0) {
+    // the level's byte matrices once, then per unit the P rows (and row 0,
+    // for the rescale) of its 128 coefficients into a raw slot
+    mbar_expect_tx(bfull, uint32_t(bbytes));
+    for (int o = 0; o < bbytes; o += 16384)
+      bulk_load(b_addr + uint32_t(o), args.bmat + o, uint32_t(min(16384, bbytes - o)), bfull);
+    const int rows = args.num_p + (args.rescale ? 1 : 0);
+    int i = 0;
+    UnitIter it(u_begin, args.batch, nblk);
+    for (; i < nu; ++i, it.next()) {
+      const int c = it.outer;
+      const int64_t b = it.b, blk = it.blk;
+      const int r = i % kMdRawSlots;
+      if (i >= kMdRawSlots && !mbar_wait(rawempty(r), ((i / kMdRawSlots) & 1) ^ 1, abort, args.err, lim)) break;
+      const uint64_t* t = (c == 0 ? args.t0 : args.t1) + b * qp_limbs * n + blk * kUnit;
+      mbar_expect_tx(rawfull(r), uint32_t(rows * kRowBytes));
+      for (int rr = 0; rr < args.num_p; ++rr)
+        bulk_load(rawbuf_addr + uint32_t(r * kMdRawSlotBytes + rr * kRowBytes), t + int64_t(args.q_limbs + rr) * n,
+                  kRowBytes, rawfull(r));
+      if (args.rescale)
+        bulk_load(rawbuf_addr + uint32_t(r * kMdRawSlotBytes + args.num_p * kRowBytes), t, kRowBytes, rawfull(r));
+    }
+    // after an abort, wait (bounded, default limit) for the copies still in flight
+    if (*abort) {
+      mbar_wait(bfull, 0, nullptr, args.err, kWaitNs);
+      for (int u = i - kMdRawSlots < 0 ? 0 : i - kMdRawSlots; u < i; ++u)
+        mbar_wait(rawfull(u % kMdRawSlots), (u / kMdRawSlots) & 1, nullptr, args.err, kWaitNs);
+    }
+  } else if (warp >= kMdLoaderWarp0 && warp < kMdLoaderWarp0 + kMdLoaderWarps) {
     // Garner digits e_r of the P part of one coefficient -> the A tile (word
     // (m, r) at (m / 8) sbo + (r / 2) 128 + (m % 8) 16 + (r % 2) 8; rows r >= P
     // zero); with rescale also v_0 of the coefficient -> its v0 slot
     const int m = tid - kMdLoaderWarp0 * 32;
-    const bool bthread = m == 0;
-    if (bthread) {  // the level's byte matrices, once
-      mbar_expect_tx(bfull, uint32_t(bbytes));
-      for (int o = 0; o < bbytes; o += 16384)
-        bulk_load(b_addr + uint32_t(o), args.bmat + o, uint32_t(min(16384, bbytes - o)), bfull);
-    }
     const PrimeInfo<uint64_t> p0 = args.tabs.prime[args.level];
-    for (int i = 0; i < nu; ++i) {
-      int c;
-      int64_t b, blk;
-      unit_of(i, c, b, blk);
-      const int s = i % kASlots, vs = i % kMdV0Slots;
+    UnitIter it(u_begin, args.batch, nblk);
+    for (int i = 0; i < nu; ++i, it.next()) {
+      const int c = it.outer;
+      const int64_t b = it.b, blk = it.blk;
+      const int r = i % kMdRawSlots, s = i % kASlots, vs = i % kMdV0Slots;
+      if (!warp_wait(rawfull(r), (i / kMdRawSlots) & 1, abort, args.err, lane, lim)) break;
       if (i >= kASlots && !warp_wait(aempty(s), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, lim)) break;
       if (args.rescale && i >= kMdV0Slots &&
           !warp_wait(v0empty(vs), ((i / kMdV0Slots) & 1) ^ 1, abort, args.err, lane, lim))
         break;
       const int k = int(blk * kUnit) + m;
-      const uint64_t* t = (c == 0 ? args.t0 : args.t1) + b * qp_limbs * n;
+      const uint64_t* raw = rawbuf + r * (kMdRawSlotBytes / 8);
       uint64_t e[kMaxDigitWidth];
 #pragma unroll
-      for (int r = 0; r < kMaxDigitWidth; ++r)
-        e[r] = r < args.num_p ? t[(args.q_limbs + r) * n + k] : 0;
-      for (int r = 0; r < args.num_p; ++r) {
-        const PrimeInfo<uint64_t> p = args.tabs.prime[args.num_q + r];
-        uint64_t x = csub(e[r], p.q);
-        if (r > 0) {
+      for (int rr = 0; rr < kMaxDigitWidth; ++rr) e[rr] = rr < args.num_p ? raw[rr * kUnit + m] : 0;
+      const uint64_t t0v = args.rescale ? raw[args.num_p * kUnit + m] : 0;
+      __syncwarp();
+      if (lane == 0) mbar_arrive(rawempty(r));
+      for (int rr = 0; rr < args.num_p; ++rr) {
+        const PrimeInfo<uint64_t> p = args.tabs.prime[args.num_q + rr];
+        uint64_t x = csub(e[rr], p.q);
+        if (rr > 0) {
           uint64_t acc = 0;
-          for (int j = 0; j < r; ++j) {
-            const TwPair<uint64_t> g = args.tabs.p_garner[r * kMaxDigitWidth + j];
+          for (int j = 0; j < rr; ++j) {
+            const TwPair<uint64_t> g = args.tabs.p_garner[rr * kMaxDigitWidth + j];
             acc = csub(acc + csub(W::shoup(e[j], g.w, g.wp, p.q), p.q), p.q);
           }
-          const TwPair<uint64_t> inv = args.tabs.p_garner[r * kMaxDigitWidth + r];
+          const TwPair<uint64_t> inv = args.tabs.p_garner[rr * kMaxDigitWidth + rr];
           x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
         }
-        e[r] = x;
+        e[rr] = x;
       }
       uint8_t* at = a_tile0 + s * kATile + (m >> 3) * kSbo + (m & 7) * 16;
 #pragma unroll
@@ -498,14 +583,17 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
             make_ulonglong2(2 * r2 < kMaxDigitWidth ? e[2 * r2] : 0, 2 * r2 + 1 < kMaxDigitWidth ? e[2 * r2 + 1] : 0);
       if (args.rescale) {
         uint64_t sub = 0;
-        for (int r = 0; r < args.num_p; ++r) {
-          const TwPair<uint64_t> mx = args.tabs.p_mix[int64_t(r) * (args.num_q + args.num_p) + args.level];
-          sub = csub(sub + csub(W::shoup(e[r], mx.w, mx.wp, p0.q), p0.q), p0.q);
+        for (int rr = 0; rr < args.num_p; ++rr) {
+          const TwPair<uint64_t> mx = args.tabs.p_mix[int64_t(rr) * (args.num_q + args.num_p) + args.level];
+          sub = csub(sub + csub(W::shoup(e[rr], mx.w, mx.wp, p0.q), p0.q), p0.q);
         }
         const TwPair<uint64_t> pinv = args.tabs.p_inv[args.level];
-        uint64_t v = csub(csub(t[k], p0.q) + p0.q - sub, p0.q);
+        uint64_t v = csub(csub(t0v, p0.q) + p0.q - sub, p0.q);
         v = csub(W::shoup(v, pinv.w, pinv.wp, p0.q), p0.q);
-        v0s[vs * kUnit + m] = csub(v + addend(c, b, 0, k, p0.q), p0.q);
+        int kk;
+        bool neg;
+        addend_source(c, b, k, kk, neg);
+        v0s[vs * kUnit + m] = csub(v + addend(c, b, 0, kk, neg, p0.q), p0.q);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -514,8 +602,6 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
         if (args.rescale) mbar_arrive(v0full(vs));
       }
     }
-    // after an abort, wait (bounded, default limit) for the byte-matrix copy
-    if (bthread && *abort) mbar_wait(bfull, 0, nullptr, args.err, kWaitNs);
   } else if (warp == kMdMmaWarp && lane == 0) {
     bool ok = mbar_wait(bfull, 0, abort, args.err, lim);
     int t = 0;
@@ -549,11 +635,14 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
     int t = 0;
     // test only: a wait that must run out (its limit is the pipeline's)
     bool ok = !args.stall || warp_wait(never_bar, 0, abort, args.err, lane, lim);
-    for (int i = 0; i < nu && ok; ++i) {
-      int c;
-      int64_t b, blk;
-      unit_of(i, c, b, blk);
+    UnitIter it(u_begin, args.batch, nblk);
+    for (int i = 0; i < nu && ok; ++i, it.next()) {
+      const int c = it.outer;
+      const int64_t b = it.b, blk = it.blk;
       const int k = int(blk * kUnit) + m;
+      int kk;
+      bool neg;
+      addend_source(c, b, k, kk, neg);
       const uint64_t* tt = (c == 0 ? args.t0 : args.t1) + b * qp_limbs * n + k;
       uint64_t* o = args.out + (int64_t(c) * args.batch + b) * args.out_limbs * n + k;
       const int vs = i % kMdV0Slots;
@@ -564,6 +653,17 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
       }
       for (int ch = 0; ch < args.nchunks; ++ch, ++t) {
         const int slot = t % kAccSlots;
+        // this item's accumulator rows and addends are requested before the
+        // wait, so their latency overlaps it
+        uint64_t tv[4], av[4];
+        bool valid[4];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const int row = ch * kChunkRows + grp * 4 + jj;
+          valid[jj] = row < args.q_limbs && !(args.rescale && row == 0);
+          tv[jj] = valid[jj] ? tt[int64_t(row) * n] : 0;
+          av[jj] = valid[jj] ? addend(c, b, row, kk, neg, args.tabs.prime[args.level + row].q) : 0;
+        }
         if (!warp_wait(accfull(slot), (t / kAccSlots) & 1, abort, args.err, lane, lim)) {
           ok = false;
           break;
@@ -578,15 +678,15 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
           const int row = ch * kChunkRows + grp * 4 + jj;
-          if (row >= args.q_limbs || (args.rescale && row == 0)) continue;
+          if (!valid[jj]) continue;
           const int pid = args.level + row;
           const ulonglong2 pi = __ldg(reinterpret_cast<const ulonglong2*>(args.pinfo) + pid);
           const uint64_t q = pi.x;
           const uint64_t sub = csub(recombine_redc(acc + 8 * jj, q, pi.y), q);
           const TwPair<uint64_t> pinv = args.tabs.p_inv[pid];
-          uint64_t v = csub(csub(tt[int64_t(row) * n], q) + q - sub, q);
+          uint64_t v = csub(csub(tv[jj], q) + q - sub, q);
           v = csub(W::shoup(v, pinv.w, pinv.wp, q), q);
-          v = csub(v + addend(c, b, row, k, q), q);
+          v = csub(v + av[jj], q);
           if (!args.rescale) {
             o[int64_t(row) * n] = v;
           } else {
@@ -633,7 +733,9 @@ int chunks_for(int qp_limbs) { return (qp_limbs + tcb::kChunkRows - 1) / tcb::kC
 
 int smem_for(int nchunks, int ks) {
   const int k = 32 * ks;
-  const int need = 1024 + 2 * nchunks * 128 * k + tcb::kASlots * tcb::kUnit * k + tcb::kBarrierBytes;
+  const int raw = (ks == 1 ? tcb::raw_slots<1>() : tcb::raw_slots<2>()) * 4 * ks * tcb::kRowBytes;
+  const int need = 1024 + 2 * nchunks * 128 * k + raw + tcb::kASlots * tcb::kUnit * k + tcb::kPinfoBytes +
+                   tcb::kBarrierBytes;
   return need > tcb::kMinSmem ? need : tcb::kMinSmem;
 }
 }  // namespace
@@ -695,9 +797,11 @@ int tc_basis_prepare(Context& c) {
   if (c.bits != 64) return fail(-7, "the tensor-core basis conversion needs an int64 context");
   if (c.log_n < 7) return fail(-7, "ring too small for the tensor-core basis conversion");
   const int ks = ksteps_for(c.num_p);
+  if (c.qp() > tcb::kPinfoBytes / 16) return fail(-7, "the chain is too long for the tensor-core basis conversion");
   if (smem_for(chunks_for(c.qp()), ks) > 227 * 1024 ||
-      1024 + chunks_for(c.num_q) * 128 * 32 * ks + (tcb::kASlots * tcb::kUnit * 32 * ks) +
-              tcb::kMdV0Slots * tcb::kUnit * 8 + tcb::kMdBarrierBytes > 227 * 1024)
+      1024 + chunks_for(c.num_q) * 128 * 32 * ks + tcb::kMdRawSlots * tcb::kMdRawSlotBytes +
+              tcb::kASlots * tcb::kUnit * 32 * ks + tcb::kMdV0Slots * tcb::kUnit * 8 + tcb::kMdBarrierBytes >
+          227 * 1024)
     return fail(-7, "the chain is too long for the tensor-core basis conversion's shared-memory tables");
   auto* t = new TcBasisTables();
   t->ks = ks;
@@ -779,7 +883,8 @@ int tc_moddown(Context& c, const void* t0, const void* t1, const void* add0, con
   if (batch == 0) return 0;
   const int ql = c.num_q - level, nch = chunks_for(ql);
   const int k = 32 * t.ks;
-  int smem = 1024 + nch * 128 * k + tcb::kASlots * tcb::kUnit * k + tcb::kMdV0Slots * tcb::kUnit * 8 +
+  int smem = 1024 + nch * 128 * k + tcb::kMdRawSlots * tcb::kMdRawSlotBytes + tcb::kASlots * tcb::kUnit * k +
+             tcb::kMdV0Slots * tcb::kUnit * 8 +
              tcb::kMdBarrierBytes;
   if (smem < tcb::kMinSmem) smem = tcb::kMinSmem;
   auto kern = t.ks == 1 ? tcb::k_tc_moddown<1> : tcb::k_tc_moddown<2>;
