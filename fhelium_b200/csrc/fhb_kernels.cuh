@@ -540,7 +540,7 @@ template <typename T, int LOGN, bool PRE = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
                  T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
-                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ ct3,
+                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ ct3, int64_t ct3_stride,
                  ChainTables<T> tabs, LevelTables<T> lt) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
@@ -561,7 +561,6 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   tw.stage(false);
   const bool add = ct3 != nullptr && jrow < q_limbs;
   const T* ct3_own = add ? ct3 + (bi * q_limbs + jrow) * int64_t(G::kN) + own : nullptr;
-  const int64_t ct3_stride = batch * q_limbs * int64_t(G::kN);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;

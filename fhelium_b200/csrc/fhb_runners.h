@@ -17,7 +17,10 @@ int run_mul_coef(const Context& c, const void* a, const void* b, void* out, int6
                  cudaStream_t st);
 template <typename T, int LOGN>
 int run_ks_core(const Context& c, const void* digits, const void* key, void* acc0, void* acc1, int64_t batch,
-                int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3, bool pre);
+                int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3, bool pre,
+                int64_t ct3_pitch = 0);
+template <typename T, int LOGN>
+int run_ks_idle_sms(const Context& c, int sms);
 template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
                int64_t batch, int level, cudaStream_t st, bool pre);

@@ -338,14 +338,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(accempty(slot));
+        // four independent outputs computed unconditionally (the rows past
+        // the level read a valid pinfo row and are not stored), so their
+        // multiply chains interleave
         const int j0 = c * kChunkRows + grp * 4;
+        uint64_t res[4];
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+          const ulonglong2 pi = spinfo[min(j0 + jj, args.qp_limbs - 1)];
+          res[jj] = recombine_redc(acc + 8 * jj, pi.x, pi.y);
+        }
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
           const int j = j0 + jj;
-          if (j < args.qp_limbs && (j < own0 || j >= own1)) {
-            const ulonglong2 pi = spinfo[j];
-            dst[int64_t(j) * n] = recombine_redc(acc + 8 * jj, pi.x, pi.y);
-          }
+          if (j < args.qp_limbs && (j < own0 || j >= own1)) dst[int64_t(j) * n] = res[jj];
         }
       }
     }
@@ -385,17 +391,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_tc_extend(ExtendArgs args) {
 // Same result as k_moddown, word for word.
 constexpr int kMdEpilogueWarps = 16;
 constexpr int kMdLoaderWarp0 = 16;
-constexpr int kMdLoaderWarps = 4;   // one coefficient per loader thread
-constexpr int kMdMmaWarp = 20;
-constexpr int kMdProducerWarp = 21;
-constexpr int kMdThreads = 32 * 22;
+constexpr int kMdLoaderWarps = 2;   // two coefficients per loader thread
+constexpr int kMdMmaWarp = 18;
+constexpr int kMdProducerWarp = 19;
+constexpr int kMdThreads = 32 * 20;
 constexpr int kMdV0Slots = 8;
 constexpr int kMdRawSlots = 6;      // one unit's P rows and row 0 each (bulk copies in flight)
 constexpr int kMdRawSlotBytes = (kMaxDigitWidth + 1) * kRowBytes;
 constexpr int kMdNumBarriers = 1 + 2 * kMdRawSlots + 2 * kASlots + 2 * kAccSlots + 2 * kMdV0Slots + 2;
 constexpr int kMdBarrierBytes = 384;
 static_assert(8 * kMdNumBarriers + 8 <= kMdBarrierBytes, "barrier area");
-static_assert(32 * kMdLoaderWarps == kUnit, "one loader thread per coefficient of a unit");
+static_assert(64 * kMdLoaderWarps == kUnit, "two coefficients of a unit per loader thread");
 
 struct ModDownArgs {
   const uint64_t* t0;          // [B][qp_limbs][N] canonical
@@ -542,7 +548,7 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
     // Garner digits e_r of the P part of one coefficient -> the A tile (word
     // (m, r) at (m / 8) sbo + (r / 2) 128 + (m % 8) 16 + (r % 2) 8; rows r >= P
     // zero); with rescale also v_0 of the coefficient -> its v0 slot
-    const int m = tid - kMdLoaderWarp0 * 32;
+    const int lt = tid - kMdLoaderWarp0 * 32;
     const PrimeInfo<uint64_t> p0 = args.tabs.prime[args.level];
     UnitIter it(u_begin, args.batch, nblk);
     for (int i = 0; i < nu; ++i, it.next()) {
@@ -554,46 +560,55 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
       if (args.rescale && i >= kMdV0Slots &&
           !warp_wait(v0empty(vs), ((i / kMdV0Slots) & 1) ^ 1, abort, args.err, lane, lim))
         break;
-      const int k = int(blk * kUnit) + m;
       const uint64_t* raw = rawbuf + r * (kMdRawSlotBytes / 8);
-      uint64_t e[kMaxDigitWidth];
+      uint64_t e2[2][kMaxDigitWidth], t0v[2];
 #pragma unroll
-      for (int rr = 0; rr < kMaxDigitWidth; ++rr) e[rr] = rr < args.num_p ? raw[rr * kUnit + m] : 0;
-      const uint64_t t0v = args.rescale ? raw[args.num_p * kUnit + m] : 0;
+      for (int h = 0; h < 2; ++h) {
+        const int m = lt + 64 * h;
+#pragma unroll
+        for (int rr = 0; rr < kMaxDigitWidth; ++rr) e2[h][rr] = rr < args.num_p ? raw[rr * kUnit + m] : 0;
+        t0v[h] = args.rescale ? raw[args.num_p * kUnit + m] : 0;
+      }
       __syncwarp();
       if (lane == 0) mbar_arrive(rawempty(r));
-      for (int rr = 0; rr < args.num_p; ++rr) {
-        const PrimeInfo<uint64_t> p = args.tabs.prime[args.num_q + rr];
-        uint64_t x = csub(e[rr], p.q);
-        if (rr > 0) {
-          uint64_t acc = 0;
-          for (int j = 0; j < rr; ++j) {
-            const TwPair<uint64_t> g = args.tabs.p_garner[rr * kMaxDigitWidth + j];
-            acc = csub(acc + csub(W::shoup(e[j], g.w, g.wp, p.q), p.q), p.q);
-          }
-          const TwPair<uint64_t> inv = args.tabs.p_garner[rr * kMaxDigitWidth + rr];
-          x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
-        }
-        e[rr] = x;
-      }
-      uint8_t* at = a_tile0 + s * kATile + (m >> 3) * kSbo + (m & 7) * 16;
 #pragma unroll
-      for (int r2 = 0; r2 < 2 * KS; ++r2)
-        *reinterpret_cast<ulonglong2*>(at + r2 * 128) =
-            make_ulonglong2(2 * r2 < kMaxDigitWidth ? e[2 * r2] : 0, 2 * r2 + 1 < kMaxDigitWidth ? e[2 * r2 + 1] : 0);
-      if (args.rescale) {
-        uint64_t sub = 0;
+      for (int h = 0; h < 2; ++h) {
+        const int m = lt + 64 * h;
+        const int k = int(blk * kUnit) + m;
+        uint64_t* e = e2[h];
         for (int rr = 0; rr < args.num_p; ++rr) {
-          const TwPair<uint64_t> mx = args.tabs.p_mix[int64_t(rr) * (args.num_q + args.num_p) + args.level];
-          sub = csub(sub + csub(W::shoup(e[rr], mx.w, mx.wp, p0.q), p0.q), p0.q);
+          const PrimeInfo<uint64_t> p = args.tabs.prime[args.num_q + rr];
+          uint64_t x = csub(e[rr], p.q);
+          if (rr > 0) {
+            uint64_t acc = 0;
+            for (int j = 0; j < rr; ++j) {
+              const TwPair<uint64_t> g = args.tabs.p_garner[rr * kMaxDigitWidth + j];
+              acc = csub(acc + csub(W::shoup(e[j], g.w, g.wp, p.q), p.q), p.q);
+            }
+            const TwPair<uint64_t> inv = args.tabs.p_garner[rr * kMaxDigitWidth + rr];
+            x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
+          }
+          e[rr] = x;
         }
-        const TwPair<uint64_t> pinv = args.tabs.p_inv[args.level];
-        uint64_t v = csub(csub(t0v, p0.q) + p0.q - sub, p0.q);
-        v = csub(W::shoup(v, pinv.w, pinv.wp, p0.q), p0.q);
-        int kk;
-        bool neg;
-        addend_source(c, b, k, kk, neg);
-        v0s[vs * kUnit + m] = csub(v + addend(c, b, 0, kk, neg, p0.q), p0.q);
+        uint8_t* at = a_tile0 + s * kATile + (m >> 3) * kSbo + (m & 7) * 16;
+#pragma unroll
+        for (int r2 = 0; r2 < 2 * KS; ++r2)
+          *reinterpret_cast<ulonglong2*>(at + r2 * 128) = make_ulonglong2(
+              2 * r2 < kMaxDigitWidth ? e[2 * r2] : 0, 2 * r2 + 1 < kMaxDigitWidth ? e[2 * r2 + 1] : 0);
+        if (args.rescale) {
+          uint64_t sub = 0;
+          for (int rr = 0; rr < args.num_p; ++rr) {
+            const TwPair<uint64_t> mx = args.tabs.p_mix[int64_t(rr) * (args.num_q + args.num_p) + args.level];
+            sub = csub(sub + csub(W::shoup(e[rr], mx.w, mx.wp, p0.q), p0.q), p0.q);
+          }
+          const TwPair<uint64_t> pinv = args.tabs.p_inv[args.level];
+          uint64_t v = csub(csub(t0v[h], p0.q) + p0.q - sub, p0.q);
+          v = csub(W::shoup(v, pinv.w, pinv.wp, p0.q), p0.q);
+          int kk;
+          bool neg;
+          addend_source(c, b, k, kk, neg);
+          v0s[vs * kUnit + m] = csub(v + addend(c, b, 0, kk, neg, p0.q), p0.q);
+        }
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
@@ -677,8 +692,9 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
         if (lane == 0) mbar_arrive(accempty(slot));
 #pragma unroll
         for (int jj = 0; jj < 4; ++jj) {
-          const int row = ch * kChunkRows + grp * 4 + jj;
-          if (!valid[jj]) continue;
+          // computed for every row (past the level on the last prime's
+          // constants) and stored only where valid, so the four chains interleave
+          const int row = min(ch * kChunkRows + grp * 4 + jj, args.q_limbs - 1);
           const int pid = args.level + row;
           const ulonglong2 pi = __ldg(reinterpret_cast<const ulonglong2*>(args.pinfo) + pid);
           const uint64_t q = pi.x;
@@ -688,14 +704,14 @@ __global__ void __launch_bounds__(kMdThreads, 1) k_tc_moddown(ModDownArgs args) 
           v = csub(W::shoup(v, pinv.w, pinv.wp, q), q);
           v = csub(v + av[jj], q);
           if (!args.rescale) {
-            o[int64_t(row) * n] = v;
+            if (valid[jj]) o[int64_t(row) * n] = v;
           } else {
             const PrimeInfo<uint64_t> p = args.tabs.prime[pid];
             const uint64_t x0 = reduce_any(v0, p);
             const TwPair<uint64_t> inv = args.rescale_inv[pid];
             uint64_t r = csub(W::shoup(csub(v + q - x0, q), inv.w, inv.wp, q), q);
             r += v0 > half0 ? 1u : 0u;
-            o[int64_t(row - 1) * n] = csub(r, q);
+            if (valid[jj]) o[int64_t(row - 1) * n] = csub(r, q);
           }
         }
       }
@@ -848,6 +864,17 @@ int tc_basis_prepare(Context& c) {
     return give_up("tensor-core basis conversion constants");
   if (cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess || t->sms < 1)
     return give_up("multiprocessor count");
+  bool ok = cudaStreamCreateWithFlags(&t->aux, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&t->ev_start, cudaEventDisableTiming) == cudaSuccess;
+  for (int x = 0; x < 2 && ok; ++x)
+    ok = cudaEventCreateWithFlags(&t->ev_ext[x], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&t->ev_core[x], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    for (cudaEvent_t e : {t->ev_start, t->ev_ext[0], t->ev_ext[1], t->ev_core[0], t->ev_core[1]})
+      if (e) cudaEventDestroy(e);
+    if (t->aux) cudaStreamDestroy(t->aux);
+    return give_up("auxiliary stream and events");
+  }
   for (void* p : mine) c.allocations.push_back(p);
   c.tcb = t;
   return 0;
@@ -857,7 +884,8 @@ int64_t tc_ext_words(const Context& c, int64_t batch, int level) {
   return int64_t(c.level_digits[level].size()) * batch * (c.qp() - level) * c.n();
 }
 
-int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st) {
+int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st,
+              int grid_cap) {
   if (int rc = tc_basis_prepare(c)) return rc;
   const TcBasisTables& t = *c.tcb;
   const int nd = int(c.level_digits[level].size());
@@ -867,7 +895,8 @@ int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int leve
   auto kern = t.ks == 1 ? tcb::k_tc_extend<1> : tcb::k_tc_extend<2>;
   if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return rc;
   const int64_t units = int64_t(nd) * batch * (c.n() / tcb::kUnit);
-  const int grid = int(units < t.sms ? units : t.sms);
+  const int cap = grid_cap > 0 && grid_cap < t.sms ? grid_cap : t.sms;
+  const int grid = int(units < cap ? units : cap);
   tcb::ExtendArgs a{static_cast<const uint64_t*>(digits), static_cast<uint64_t*>(ext), t.bmat[level], t.pinfo,
                     c.lv64[level].digits, batch, level, c.num_q - level, qpl, nd, nch, c.log_n,
                     skip_own ? 1 : 0, t.err, c.tc_wait_ns ? c.tc_wait_ns : tc::kWaitNs, c.tc_test_stall};
