@@ -445,6 +445,21 @@ def forms_leg(eng, ca, cb, rlk, stream, steps=5):
         out[form] = res
     a, b = results["cuda_cores"], results["tensor_cores"]
     out["bit_identical"] = all(bool(torch.equal(x, y)) for x, y in zip(a, b))
+    # variant of the tensor-core form, HMult+relin+rescale only: ModDown on
+    # the tensor cores too
+    import fhelium_b200._native as nat
+    eng.basis_conversion = "tensor_cores"
+    variants = {}
+    for name, param, value in (("tc_moddown", nat.TUNE_TC_MODDOWN, 1),):
+        keep_v = eng.ctx.get_tuning(param)
+        eng.ctx.set_tuning(param, value)
+        r = eng.multiply_relinearize_rescale(ca, cb, rlk)
+        torch.cuda.synchronize()
+        ms = _time_events(lambda: eng.multiply_relinearize_rescale(ca, cb, rlk), steps, stream)
+        variants[name] = {"hmult_relin_rescale_ops_per_s": ca.batch_size / (ms / 1000.0),
+                          "bit_identical": bool(torch.equal(r.data, a[0]))}
+        eng.ctx.set_tuning(param, keep_v)
+    out["tensor_cores_variants"] = variants
     out["tensor_cores_over_cuda_cores"] = {
         k: out["tensor_cores"][k] / out["cuda_cores"][k]
         for k in ("hmult_relin_rescale_ops_per_s", "rotate_ops_per_s", "hoisted_rotations_16_ops_per_s")}

@@ -1,8 +1,6 @@
 // extern "C" entry points of libfhb200.so (declared in include/fhb200.h).
-#include <algorithm>
 #include <cstdint>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "../../include/fhb200.h"
@@ -120,22 +118,6 @@ int ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void*
            int64_t batch, int level, cudaStream_t st, bool pre = false) {
   FHB_DISPATCH(run_ks_sum, c, digits, key_ptrs, acc0, acc1, giants, batch, level, st, pre);
 }
-}  // namespace
-int ks_idle_sms(const Context& c) {
-  int sms = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess) return 0;
-  if (c.bits != 64) return 0;
-  switch (c.log_n) {
-    case 12: return run_ks_idle_sms<uint64_t, 12>(c, sms);
-    case 13: return run_ks_idle_sms<uint64_t, 13>(c, sms);
-    case 14: return run_ks_idle_sms<uint64_t, 14>(c, sms);
-    case 15: return run_ks_idle_sms<uint64_t, 15>(c, sms);
-    case 16: return run_ks_idle_sms<uint64_t, 16>(c, sms);
-    case 17: return run_ks_idle_sms<uint64_t, 17>(c, sms);
-    default: return 0;
-  }
-}
-namespace {
 int prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st) {
   FHB_DISPATCH(run_prepare, c, digits, prepared, batch, level, st);
 }
@@ -169,7 +151,7 @@ int moddown(const Context& c, const void* t0, const void* t1, const void* a0, co
             const uint32_t* item_galois = nullptr) {
   const uint32_t ginv = add0_galois == 1 ? 0u : galois_inverse(add0_galois, c.log_n);
   if constexpr (sizeof(T) == 8) {
-    if (c.basis_tc)  // P -> Q conversion on the int8 tensor cores
+    if (c.basis_tc && c.tc_moddown)  // P -> Q conversion on the int8 tensor cores
       return tc_moddown(const_cast<Context&>(c), t0, t1, a0, a1, out, batch, level, ginv, item_galois, rescale, st);
   }
   k_moddown<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
@@ -406,6 +388,10 @@ int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
       if (value != 0 && value != 1) return fail(-2, "stall must be 0 or 1");
       ctx->impl->tc_test_stall = value;
       return 0;
+    case FHB_TUNE_TC_MODDOWN:
+      if (value != 0 && value != 1) return fail(-2, "value must be 0 or 1");
+      ctx->impl->tc_moddown = value;
+      return 0;
     default:
       return fail(-2, "unknown tuning parameter");
   }
@@ -420,6 +406,7 @@ int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value) {
     case FHB_TUNE_BASIS_CONVERSION: *value = ctx->impl->basis_tc; return 0;
     case FHB_TUNE_TC_WAIT_US: *value = int(ctx->impl->tc_wait_ns / 1000u); return 0;
     case FHB_TUNE_TC_TEST_STALL: *value = ctx->impl->tc_test_stall; return 0;
+    case FHB_TUNE_TC_MODDOWN: *value = ctx->impl->tc_moddown; return 0;
     default: return fail(-2, "unknown tuning parameter");
   }
 }
@@ -696,11 +683,8 @@ int64_t fhb_ckks_keyswitch_scratch_bytes(const fhb_context* ctx, int64_t batch, 
   if (level < 0 || level >= c.num_q || batch < 0) return -1;
   const int64_t l = c.num_q - level, lp = l + c.num_p;
   int64_t per_ct = (3 * l + l + 2 * lp) * c.n() * fhb::word_bytes(c);
-  // tensor-core form: the extensions of batch + 1 ciphertexts (two group
-  // buffers of ceil(batch / groups) fit in it for every grouping used)
+  // tensor-core form: the extensions of every digit to every row
   if (c.basis_tc) per_ct += fhb::tc_ext_words(c, 1, level) * fhb::word_bytes(c);
-  if (c.basis_tc && batch > INT64_MAX / per_ct - 1) return -1;
-  if (c.basis_tc) return per_ct * batch + fhb::tc_ext_words(c, 1, level) * fhb::word_bytes(c);
   if (batch > INT64_MAX / per_ct) return -1;  // the size does not fit in 64 bits
   return per_ct * batch;
 }
@@ -719,45 +703,11 @@ static int check_scratch(const fhb_context* ctx, int64_t batch, int level, int64
 // Key-switch core on the ModUp digits in s.digits: with the tensor-core
 // basis conversion the extensions are materialised first (own-digit rows
 // skipped when the core reuses c2 there) and the core only transforms.
-// From 8 ciphertexts on the batch runs in 2 or 4 groups: while the core
-// works on group g (caller's stream), the extensions of group g + 1 are
-// computed on the context's auxiliary stream on the SMs the core's clusters
-// leave idle; two extension buffers alternate and events order everything,
-// so a stream capture sees the auxiliary stream fork and join.
-static int ks_core_from_digits(const Context& cc, const fhb::Scratch& s, const void* key, int64_t batch, int level,
+static int ks_core_from_digits(const Context& c, const fhb::Scratch& s, const void* key, int64_t batch, int level,
                                cudaStream_t st, const uint64_t* item_keys = nullptr, const void* ct3 = nullptr) {
-  if (!cc.basis_tc) return fhb::ks_core(cc, s.digits, key, s.t0, s.t1, batch, level, st, item_keys, ct3);
-  Context& c = const_cast<Context&>(cc);
-  TRY(fhb::tc_basis_prepare(c));
-  fhb::TcBasisTables& t = *c.tcb;
-  std::lock_guard<std::mutex> lock(c.overlap_mutex);
-  if (t.idle_sms < 0) t.idle_sms = fhb::ks_idle_sms(c);
-  const bool skip = ct3 != nullptr;
-  const int groups = t.idle_sms >= 8 ? (batch >= 16 ? 4 : (batch >= 8 ? 2 : 1)) : 1;
-  if (groups == 1) {
-    TRY(fhb::tc_extend(c, s.digits, s.ext, batch, level, skip, st));
-    return fhb::ks_core(c, s.ext, key, s.t0, s.t1, batch, level, st, item_keys, ct3, true);
-  }
-  const int64_t w = fhb::word_bytes(c), n = c.n(), l = c.num_q - level, lp = l + c.num_p;
-  const int64_t per_group = (batch + groups - 1) / groups;
-  char* buf[2] = {s.ext, s.ext + fhb::tc_ext_words(c, per_group, level) * w};
-  const int64_t pitch = batch * l * n;  // component pitch of ct3 [3, batch, L, N]
-  TRY(fhb::cuda_status(cudaEventRecord(t.ev_start, st), "cudaEventRecord"));
-  TRY(fhb::cuda_status(cudaStreamWaitEvent(t.aux, t.ev_start, 0), "cudaStreamWaitEvent"));
-  for (int g = 0; g < groups; ++g) {
-    const int64_t b0 = g * per_group, bg = std::min(per_group, batch - b0);
-    if (bg <= 0) break;
-    const int x = g & 1;
-    if (g >= 2) TRY(fhb::cuda_status(cudaStreamWaitEvent(t.aux, t.ev_core[x], 0), "cudaStreamWaitEvent"));
-    TRY(fhb::tc_extend(c, s.digits + b0 * l * n * w, buf[x], bg, level, skip, t.aux, g == 0 ? 0 : t.idle_sms));
-    TRY(fhb::cuda_status(cudaEventRecord(t.ev_ext[x], t.aux), "cudaEventRecord"));
-    TRY(fhb::cuda_status(cudaStreamWaitEvent(st, t.ev_ext[x], 0), "cudaStreamWaitEvent"));
-    TRY(fhb::ks_core(c, buf[x], key, s.t0 + b0 * lp * n * w, s.t1 + b0 * lp * n * w, bg, level, st,
-                     item_keys ? item_keys + b0 : nullptr,
-                     ct3 ? static_cast<const char*>(ct3) + b0 * l * n * w : nullptr, true, pitch));
-    TRY(fhb::cuda_status(cudaEventRecord(t.ev_core[x], st), "cudaEventRecord"));
-  }
-  return 0;
+  if (!c.basis_tc) return fhb::ks_core(c, s.digits, key, s.t0, s.t1, batch, level, st, item_keys, ct3);
+  TRY(fhb::tc_extend(const_cast<Context&>(c), s.digits, s.ext, batch, level, ct3 != nullptr, st));
+  return fhb::ks_core(c, s.ext, key, s.t0, s.t1, batch, level, st, item_keys, ct3, true);
 }
 
 static int keyswitch_tail(const Context& c, const fhb::Scratch& s, const void* key, const void* add0,

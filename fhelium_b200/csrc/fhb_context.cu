@@ -277,12 +277,6 @@ void destroy_context(Context* c) {
   for (void* p : c->allocations) cudaFree(p);
   cudaSetDevice(prev);
   delete c->tc;
-  if (c->tcb) {
-    for (cudaEvent_t e : {c->tcb->ev_start, c->tcb->ev_ext[0], c->tcb->ev_ext[1], c->tcb->ev_core[0],
-                          c->tcb->ev_core[1]})
-      if (e) cudaEventDestroy(e);
-    if (c->tcb->aux) cudaStreamDestroy(c->tcb->aux);
-  }
   delete c->tcb;
   delete c;
 }

@@ -67,13 +67,6 @@ struct TcBasisTables {
   int ks = 1;                     // K-steps of 32 bytes (digits of up to 4 or 8 primes)
   int sms = 0;                    // multiprocessors of the context's device (one CTA each)
   int* err = nullptr;             // device flag: a bounded wait gave up
-  // overlap of the extensions with the key-switch core: an auxiliary stream
-  // and its events (created with the tables, outside any stream capture)
-  cudaStream_t aux = nullptr;
-  cudaEvent_t ev_start = nullptr;
-  cudaEvent_t ev_ext[2] = {nullptr, nullptr};
-  cudaEvent_t ev_core[2] = {nullptr, nullptr};
-  int idle_sms = -1;              // SMs the core's clusters leave idle (-1: not yet measured)
 };
 
 struct Context {
@@ -97,6 +90,9 @@ struct Context {
   // tuning: basis conversion of the key switch on the CUDA cores (0) or the
   // int8 tensor cores (1, int64 contexts)
   int basis_tc = 0;
+  // tuning, with basis_tc: ModDown's P -> Q conversion on the tensor cores
+  // (1) or on the CUDA cores (0, default: faster on B200)
+  int tc_moddown = 0;
   // limit of the tensor-core kernels' pipeline waits in ns (0 = the default
   // second); their drain waits always keep the default
   unsigned long long tc_wait_ns = 0;
@@ -105,7 +101,6 @@ struct Context {
   int tc_test_stall = 0;
   TcBasisTables* tcb = nullptr;  // tensor-core basis conversion tables (null until prepared)
   std::mutex tcb_mutex;
-  std::mutex overlap_mutex;      // issue order of the overlapped key-switch groups (shared events)
   std::vector<std::vector<DigitDesc>> level_digits;  // host copy of each level's active digits
   int qp() const { return num_q + num_p; }
   int n() const { return 1 << log_n; }
@@ -142,11 +137,8 @@ void tc_ntt_tables_host(uint64_t q, uint64_t psi, int pass, uint8_t* bmat, uint3
 // unwritten.  tc_basis_status reads and clears the device error flag.
 int tc_basis_prepare(Context& c);
 int64_t tc_ext_words(const Context& c, int64_t batch, int level);
-int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st,
-              int grid_cap = 0);
+int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st);
 int tc_basis_status(Context& c, int* flag);
-// SMs the key-switch core's clusters leave idle (fhb_runners.cuh).
-int ks_idle_sms(const Context& c);
 // ModDown by P (+ addends, + rescale) with the P -> Q conversion on the
 // tensor cores; same arguments and result as the CUDA-core ModDown.
 int tc_moddown(Context& c, const void* t0, const void* t1, const void* add0, const void* add1, void* out,

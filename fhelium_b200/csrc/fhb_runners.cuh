@@ -99,39 +99,6 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
                                  ct3_pitch, tables<T>(c), level_tables<T>(c, level));
 }
 
-// SMs that the key-switch core's clusters leave without a cluster (cluster
-// placement stays inside a GPC, so e.g. 15 clusters of 8 fill 120 of 148
-// SMs): the tensor-core form runs its basis extensions there, overlapped.
-template <typename T, int LOGN>
-int run_ks_idle_sms(const Context& c, int sms) {
-  using G = NttGeom<T, LOGN>;
-  if constexpr (sizeof(T) != 8) {
-    return 0;
-  } else {
-    auto kern = k_keyswitch_core<T, LOGN, true>;
-    const size_t smem = KsAcc<T, LOGN>::smem_bytes();
-    if (ensure_dynamic_smem(reinterpret_cast<const void*>(kern), int(smem)) != 0) return 0;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(unsigned(G::kC * 64));
-    cfg.blockDim = dim3(G::kThreads);
-    cfg.dynamicSmemBytes = smem;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = G::kC;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = G::kC > 1 ? 1 : 0;
-    int clusters = 0;
-    if (G::kC <= 1 || cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess) {
-      cudaGetLastError();
-      return 0;
-    }
-    const int idle = sms - clusters * G::kC;
-    return idle > 0 ? idle : 0;
-  }
-}
-
 template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
                int64_t batch, int level, cudaStream_t st, bool pre) {
@@ -177,7 +144,6 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   template int run_mul_coef<T, LOGN>(const Context&, const void*, const void*, void*, int64_t, int, cudaStream_t); \
   template int run_ks_core<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int,        \
                                     cudaStream_t, const uint64_t*, const void*, bool, int64_t);                 \
-  template int run_ks_idle_sms<T, LOGN>(const Context&, int);                                                     \
   template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
                                    cudaStream_t, bool);                                                         \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \

@@ -20,8 +20,6 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
                 int level, cudaStream_t st, const uint64_t* item_keys, const void* ct3, bool pre,
                 int64_t ct3_pitch = 0);
 template <typename T, int LOGN>
-int run_ks_idle_sms(const Context& c, int sms);
-template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
                int64_t batch, int level, cudaStream_t st, bool pre);
 template <typename T, int LOGN>

@@ -864,17 +864,6 @@ int tc_basis_prepare(Context& c) {
     return give_up("tensor-core basis conversion constants");
   if (cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess || t->sms < 1)
     return give_up("multiprocessor count");
-  bool ok = cudaStreamCreateWithFlags(&t->aux, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreateWithFlags(&t->ev_start, cudaEventDisableTiming) == cudaSuccess;
-  for (int x = 0; x < 2 && ok; ++x)
-    ok = cudaEventCreateWithFlags(&t->ev_ext[x], cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&t->ev_core[x], cudaEventDisableTiming) == cudaSuccess;
-  if (!ok) {
-    for (cudaEvent_t e : {t->ev_start, t->ev_ext[0], t->ev_ext[1], t->ev_core[0], t->ev_core[1]})
-      if (e) cudaEventDestroy(e);
-    if (t->aux) cudaStreamDestroy(t->aux);
-    return give_up("auxiliary stream and events");
-  }
   for (void* p : mine) c.allocations.push_back(p);
   c.tcb = t;
   return 0;
@@ -884,8 +873,7 @@ int64_t tc_ext_words(const Context& c, int64_t batch, int level) {
   return int64_t(c.level_digits[level].size()) * batch * (c.qp() - level) * c.n();
 }
 
-int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st,
-              int grid_cap) {
+int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int level, bool skip_own, cudaStream_t st) {
   if (int rc = tc_basis_prepare(c)) return rc;
   const TcBasisTables& t = *c.tcb;
   const int nd = int(c.level_digits[level].size());
@@ -895,8 +883,7 @@ int tc_extend(Context& c, const void* digits, void* ext, int64_t batch, int leve
   auto kern = t.ks == 1 ? tcb::k_tc_extend<1> : tcb::k_tc_extend<2>;
   if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return rc;
   const int64_t units = int64_t(nd) * batch * (c.n() / tcb::kUnit);
-  const int cap = grid_cap > 0 && grid_cap < t.sms ? grid_cap : t.sms;
-  const int grid = int(units < cap ? units : cap);
+  const int grid = int(units < t.sms ? units : t.sms);
   tcb::ExtendArgs a{static_cast<const uint64_t*>(digits), static_cast<uint64_t*>(ext), t.bmat[level], t.pinfo,
                     c.lv64[level].digits, batch, level, c.num_q - level, qpl, nd, nch, c.log_n,
                     skip_own ? 1 : 0, t.err, c.tc_wait_ns ? c.tc_wait_ns : tc::kWaitNs, c.tc_test_stall};

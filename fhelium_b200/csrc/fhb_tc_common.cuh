@@ -40,19 +40,14 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Longest time one try_wait may park the thread before it re-checks (ns):
-// the hardware resumes it as soon as the phase completes, so waiting threads
-// do not spin through the issue slots of the warps that do the work.
-constexpr uint32_t kSuspendNs = 20000;
-
 __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(bar), "r"(parity), "r"(kSuspendNs)
+      : "r"(bar), "r"(parity)
       : "memory");
   return ok != 0;
 }
@@ -60,8 +55,8 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
 // Bounded wait for the phase of `parity` to complete.  Returns false when
 // the CTA aborted (abort != nullptr) or `limit_ns` of the global timer
 // passed; the latter raises the abort flag and the device error flag.  The
-// timer is read every 64 polls (each poll may park the thread up to
-// kSuspendNs): the common case is a barrier that completes within a poll.
+// timer is read only every 1024 polls: the common case is a barrier that
+// completes within a few polls.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort, int* err,
                                           unsigned long long limit_ns = kWaitNs) {
   if (mbar_test(bar, parity)) return true;
@@ -69,7 +64,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
   for (uint32_t it = 1;; ++it) {
     if (mbar_test(bar, parity)) return true;
     if (abort && *abort) return false;
-    if ((it & 63) == 0) {
+    if ((it & 1023) == 0) {
       const unsigned long long t = global_ns();
       if (t0 == 0) {
         t0 = t;

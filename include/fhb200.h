@@ -88,6 +88,9 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * barrier that nothing completes, so its pipeline limit runs out and the
  * abort path (drain, TMEM release, status flag) runs; outputs are then
  * invalid.  For tests of that path only.
+ * FHB_TUNE_TC_MODDOWN (with the tensor-core form): 1 = ModDown's P -> Q
+ * conversion on the tensor cores too, 0 = on the CUDA cores (default: faster
+ * on B200).
  * Results do not depend on any of these (stall aside).  No counterpart in the reference
  * (its launch shapes and arithmetic units are fixed). */
 enum fhb_tuning_param {
@@ -96,7 +99,8 @@ enum fhb_tuning_param {
   FHB_TUNE_NTT_INVERSE_EPT = 2,
   FHB_TUNE_BASIS_CONVERSION = 3,
   FHB_TUNE_TC_WAIT_US = 4,
-  FHB_TUNE_TC_TEST_STALL = 5
+  FHB_TUNE_TC_TEST_STALL = 5,
+  FHB_TUNE_TC_MODDOWN = 6
 };
 int fhb_context_set_tuning(fhb_context* ctx, int param, int value);
 int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);

@@ -162,3 +162,41 @@ def test_tc_form_rotate_and_sum_matches_cuda_core_form(family, log_n, level):
         eng.basis_conversion = form
         outs[form] = to_np(eng.rotate_and_sum(cts, keys).data)
     np.testing.assert_array_equal(outs["tensor_cores"], outs["cuda_cores"])
+
+
+@pytest.mark.parametrize("tc_moddown", [0, 1])
+@pytest.mark.parametrize("batch", [9, 16])
+def test_tc_form_full_ring_batches_and_moddown_variants(batch, tc_moddown):
+    """The tensor-core form on the full N = 2^16 ring with batches of 9 and 16
+    (both work-order-2 group branches), with ModDown on the CUDA cores or the
+    tensor cores: every output equals the CUDA-core form's, and one item
+    equals the oracle."""
+    cfg, eng, orc, rng = _setup("int64_logn16", 16, 24)
+    level = 30
+    rows = orc.q_rows(level)
+    ct3 = uniform_residues(rng, cfg.moduli, rows, (3, batch), cfg.N, lazy=True)
+    a = uniform_residues(rng, cfg.moduli, rows, (2, batch), cfg.N, lazy=True)
+    b = uniform_residues(rng, cfg.moduli, rows, (2, batch), cfg.N, lazy=True)
+    ct = uniform_residues(rng, cfg.moduli, rows, (2, batch), cfg.N)
+    key = random_key(rng, cfg, cfg.N)
+    rlk = RelinearizationKey(to_dev(key, cfg))
+    steps = [1 + (i % 5) for i in range(batch)]
+    rkeys = {s: RotationKey(to_dev(random_key(rng, cfg, cfg.N), cfg), rotation_step=s,
+                            galois_element=eng.galois_element_for_step(s)) for s in sorted(set(steps))}
+    x3 = Ciphertext(to_dev(ct3, cfg), level, 1.0, "ntt", "montgomery")
+    ca = Ciphertext(to_dev(a, cfg), level, 2.0 ** 30, "ntt", "montgomery")
+    cb = Ciphertext(to_dev(b, cfg), level, 2.0 ** 30, "ntt", "montgomery")
+    c = Ciphertext(to_dev(ct, cfg), level, 1.0)
+
+    def run():
+        return (to_np(eng.relinearize(x3, rlk).data), to_np(eng.multiply_relinearize_rescale(ca, cb, rlk).data),
+                to_np(eng.rotate_with_key(c, rkeys[1]).data),
+                to_np(eng.rotate_items_with_keys(c, [rkeys[s] for s in steps]).data))
+
+    plain = run()
+    eng.basis_conversion = "tensor_cores"
+    eng.ctx.set_tuning(nat.TUNE_TC_MODDOWN, tc_moddown)
+    tc = run()
+    for x, y in zip(tc, plain):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(tc[0][:, batch - 1], orc.relinearize(ct3[:, batch - 1], key, level))
