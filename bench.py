@@ -471,11 +471,15 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
     """Mixed-level batch at slots32768_scale40_levels34_int64: `count`
     ciphertexts with limb counts uniform in 3..35 (uniform [-0.05, 0.05]
     messages), each with a seeded op (HMult+relin+rescale with a same-level
-    partner, or a rotation by a step uniform in +-[1, 2^14]).  The batched
-    form (one CUDA graph, knobs from the autotuner) against one engine call
-    sequence per ciphertext; every result compared bit for bit."""
+    partner, or a rotation by a step uniform in +-[1, 2^14]).  Three forms,
+    every result compared bit for bit with one engine call sequence per
+    ciphertext: the descriptor-driven items path (six launches per chunk of
+    items, whatever their levels), the per-(kind, level) group graph (knobs
+    from the autotuner), and the per-ciphertext loop itself.  The rotation
+    keys (one per distinct step, about 0.4 GB each) dominate the memory."""
     from fhelium_b200 import autotune
-    from fhelium_b200.batch import HMULT, MixedBatchExecutor, run_per_ciphertext, sample_mixed_workload
+    from fhelium_b200.batch import (HMULT, MixedBatchExecutor, MixedItemsExecutor, run_per_ciphertext,
+                                    sample_mixed_workload)
     from fhelium_b200.engine import CkksEngine
     eng = CkksEngine(PRESET, device=dev, rng_seed=9)
     levels, ops = sample_mixed_workload(eng.num_q, count, seed=0)
@@ -487,11 +491,34 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
             eng.rotation_key(op.step)
     torch.cuda.synchronize(dev)
     keygen_s = time.perf_counter() - t0
+    def mismatches(ex):
+        bad = 0
+        for i, op in enumerate(ops):
+            want = run_per_ciphertext(eng, cts, [op])[0].data.view(2, -1, eng.n)
+            bad += int(not torch.equal(ex.result_view(i), want))
+        return bad
+
+    # one executor alive at a time: the keys leave little room for two
+    items = MixedItemsExecutor(eng, cts, ops)
+    items.run()
+    torch.cuda.synchronize(dev)
+    items_ms = _time_events(items.run, max(3, steps), stream)
+    bad = {"items": mismatches(items)}
+    item_chunks, item_launches = len(items.chunks), items.launches_per_run
+    peak_gb = {"items": torch.cuda.max_memory_allocated(dev) / 1e9}
+    del items
+    torch.cuda.empty_cache()
     ex = MixedBatchExecutor(eng, cts, ops)
     tune = autotune.tune_mixed_batch(eng, ex, ks_orders=(0, 1), streams=(1, 2, 4), repeats=2)
+    torch.cuda.empty_cache()
     ex.run()
     torch.cuda.synchronize(dev)
     batched_ms = _time_events(ex.run, max(3, steps), stream)
+    bad["groups"] = mismatches(ex)
+    groups, group_launches = len(ex.groups), ex.launches_per_run
+    peak_gb["groups"] = torch.cuda.max_memory_allocated(dev) / 1e9
+    del ex
+    torch.cuda.empty_cache()
 
     def per_ct():
         run_per_ciphertext(eng, cts, ops)
@@ -499,22 +526,22 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
     per_ct()
     torch.cuda.synchronize(dev)
     loop_ms = _time_events(per_ct, 2, stream)
-    mismatches = 0
-    for i, op in enumerate(ops):
-        want = run_per_ciphertext(eng, cts, [op])[0]
-        if not torch.equal(ex.result_view(i), want.data.view(2, -1, eng.n)):
-            mismatches += 1
     n_rot = sum(1 for op in ops if op.kind != HMULT)
+    best = min(items_ms, batched_ms)
     out = {"ciphertexts": count, "hmult_ops": count - n_rot, "rotate_ops": n_rot,
            "distinct_rotation_keys": len({eng._canonical_step(op.step) for op in ops if op.kind != HMULT}),
-           "groups": len(ex.groups), "library_launches_per_pass": ex.launches_per_run,
+           "basis_conversion": eng.basis_conversion,
+           "items_ms": items_ms, "items_ops_per_s": count / (items_ms / 1e3), "items_chunks": item_chunks,
+           "items_library_launches_per_pass": item_launches,
+           "groups": groups, "library_launches_per_pass": group_launches,
            "batched_graph_ms": batched_ms, "batched_ops_per_s": count / (batched_ms / 1e3),
            "per_ciphertext_ms": loop_ms, "per_ciphertext_ops_per_s": count / (loop_ms / 1e3),
-           "speedup": loop_ms / batched_ms, "bit_exact_mismatches": mismatches,
+           "speedup": loop_ms / best, "items_over_groups": batched_ms / items_ms,
+           "bit_exact_mismatches": bad, "peak_allocated_gb": peak_gb,
            "autotune": {"ks_order": tune["ks_order"], "streams": tune["streams"], "cached": tune["cached"],
                         "candidates": tune.get("candidates")},
            "keygen_s": keygen_s}
-    del ex, cts, eng
+    del cts, eng
     torch.cuda.empty_cache()
     return out
 
@@ -828,12 +855,23 @@ def main() -> int:
         eng.generate_rotation_keys(steps16)
         h_ms = _time_events(lambda: eng.rotate_many_by_steps(rot_in, steps16), 2, stream)
         extras["hoisted_rotations_16_ops_per_s"] = 16 * B / (h_ms / 1000.0)
-        extras["reference_schema_kernels"] = schema_ops_leg(eng, ca.data[0], ca.data[1], rlk.data[0], stream)
-        extras["basis_conversion_forms"] = forms_leg(eng, ca, cb, rlk, stream, steps=max(2, min(args.steps, 5)))
-        extras["ntt_int32_logN16_36limbs_batch64"] = ntt_leg(dev, stream, args.steps)
-        extras["bootstrap_logN16_batch8"] = bootstrap_leg(dev, stream)
+
+        def leg(name, fn):
+            # a secondary leg that fails (e.g. out of memory) is reported, and
+            # the headline line is still printed
+            try:
+                extras[name] = fn()
+            except Exception as exc:  # report, never hide
+                extras[name] = f"error: {type(exc).__name__}: {str(exc)[:300]}"
+            eng._scratch = None  # the headline engine's key-switch scratch is re-made on demand
+            torch.cuda.empty_cache()
+
+        leg("reference_schema_kernels", lambda: schema_ops_leg(eng, ca.data[0], ca.data[1], rlk.data[0], stream))
+        leg("basis_conversion_forms", lambda: forms_leg(eng, ca, cb, rlk, stream, steps=max(2, min(args.steps, 5))))
+        leg("ntt_int32_logN16_36limbs_batch64", lambda: ntt_leg(dev, stream, args.steps))
+        leg("bootstrap_logN16_batch8", lambda: bootstrap_leg(dev, stream))
         if args.mixed_count > 0:
-            extras["mixed_level_batch"] = mixed_batch_leg(dev, stream, args.mixed_count, args.steps)
+            leg("mixed_level_batch", lambda: mixed_batch_leg(dev, stream, args.mixed_count, args.steps))
         # decrypted error of the product (first ciphertext)
         dec = eng.decrypt_message(Ciphertext(state["out"].data[:, :1].contiguous(), 1, state["out"].scale),
                                   is_real=True)

@@ -21,6 +21,23 @@ _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I64 = ctypes.c_int64
 _U32 = ctypes.c_uint32
+class KsItem(ctypes.Structure):
+    """fhb_ks_item: one ciphertext's operation in a mixed-level batch."""
+    _fields_ = [("kind", ctypes.c_int32), ("level", ctypes.c_int32), ("galois", ctypes.c_uint32),
+                ("reserved", ctypes.c_int32), ("a", ctypes.c_void_p), ("b", ctypes.c_void_p),
+                ("key", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
+class ItemsPlanInfo(ctypes.Structure):
+    """fhb_items_plan_info: sizes and counts of a mixed-level batch plan."""
+    _fields_ = [("plan_bytes", ctypes.c_int64), ("scratch_bytes", ctypes.c_int64), ("items", ctypes.c_int32),
+                ("hmult_items", ctypes.c_int32), ("forward_units", ctypes.c_int32),
+                ("inverse_units", ctypes.c_int32), ("core_units", ctypes.c_int32), ("max_limbs", ctypes.c_int32),
+                ("max_digits", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+ITEM_HMULT_RELIN_RESCALE, ITEM_ROTATE = 0, 1
+
 SIGNATURES: dict[str, tuple] = {
     "fhb_version": (_I, []),
     "fhb_modmul_probe": (_I, [_P, _P, _I, _I, _P]),
@@ -61,6 +78,9 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_keyswitch_sum": (_I, [_P, _P, _P, _P, _P, _I, _I64, _I, _P]),
     "fhb_ckks_keyswitch_sum_extended": (_I, [_P, _P, _P, _P, _P, _I, _I64, _I, _P]),
     "fhb_ckks_decrypt_tail": (_I, [_P, _P, _P, _I64, _I, _P]),
+    "fhb_ckks_items_plan_info": (_I, [_P, ctypes.POINTER(KsItem), _I, ctypes.POINTER(ItemsPlanInfo)]),
+    "fhb_ckks_items_plan": (_I, [_P, ctypes.POINTER(KsItem), _I, _P, _P, ctypes.POINTER(ItemsPlanInfo)]),
+    "fhb_ckks_items_run": (_I, [_P, _P, ctypes.POINTER(ItemsPlanInfo), _P]),
     "fhb_ckks_bsgs_inner_product": (_I, [_P, _P, _I64, _P, _I64, _I, _P, _I, _I, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_monomial": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_modraise": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),

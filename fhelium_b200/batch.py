@@ -26,6 +26,7 @@ same residues bit for bit.
 
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass, field
 from typing import Sequence
 
@@ -132,25 +133,7 @@ class MixedBatchExecutor:
 
     # ---------------------------------------------------------------- plan
     def _validate(self) -> None:
-        eng = self.engine
-        for ct in self.cts:
-            ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
-            eng._check_ct(ct)
-            if ct.batch_size != 1:
-                raise ValueError("mixed batches take ciphertexts of batch size 1")
-        for op in self.ops:
-            if not 0 <= op.index < len(self.cts):
-                raise ValueError(f"op {op} refers to a missing ciphertext")
-            if op.kind == HMULT:
-                if not 0 <= op.partner < len(self.cts):
-                    raise ValueError(f"op {op} has no partner")
-                a, b = self.cts[op.index], self.cts[op.partner]
-                if a.level != b.level:
-                    raise ValueError(f"op {op}: partner is at another level")
-                if a.limb_count < 2:
-                    raise ValueError(f"op {op}: no level left to rescale into")
-            elif op.kind != ROTATE:
-                raise ValueError(f"unknown op kind {op.kind!r}")
+        _validate(self.engine, self.cts, self.ops)
 
     def _plan(self) -> list[_Group]:
         eng = self.engine
@@ -279,19 +262,175 @@ class MixedBatchExecutor:
         return g.out[:, j]
 
     def result(self, op_index: int) -> Ciphertext:
-        eng = self.engine
-        op = self.ops[op_index]
-        ct = self.cts[op.index]
-        data = self.result_view(op_index).contiguous().view(2, *ct.batch_shape, -1, eng.n)
-        if op_index in self._copies:
-            return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
-        if op.kind == HMULT:
-            scale = eng.rescale_to_next_output_scale(ct.scale * self.cts[op.partner].scale, level=ct.level)
-            return Ciphertext(data, ct.level + 1, scale, "coefficient", "standard")
-        return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
+        return _result(self, op_index)
 
     def results(self) -> list[Ciphertext]:
         return [self.result(i) for i in range(len(self.ops))]
+
+
+class MixedItemsExecutor:
+    """A fixed mixed batch as six library launches, whatever its levels.
+
+    Every ciphertext's operation becomes one item descriptor (level, Galois
+    element, operand, key and output addresses) in a device plan, and each
+    stage of the key switch (forward NTT of the HMult operands, tensor
+    product, inverse NTT of d2, ModUp digits, key-switch core, ModDown) is
+    ONE launch over all items, with work lists that map clusters to
+    (item, row) units.  The operands are read in place (no gathers), so
+    updating the ciphertexts' tensors between runs is seen.  Every item in
+    flight holds its own scratch (ModUp digits, two Q_l P accumulators, and
+    for HMult the operands' NTTs and ct3), so a batch whose scratch would
+    pass ``max_scratch_bytes`` runs as several such six-launch chunks in
+    stream order over one shared scratch.  Results are integer-equal to
+    :class:`MixedBatchExecutor` and to :func:`run_per_ciphertext`.
+    """
+
+    def __init__(self, engine, ciphertexts: Sequence[Ciphertext], ops: Sequence[MixedOp], *,
+                 use_graph: bool = True, max_scratch_bytes: int = 8 << 30):
+        self.engine = engine
+        self.cts = list(ciphertexts)
+        self.ops = list(ops)
+        self.use_graph = use_graph
+        _validate(engine, self.cts, self.ops)
+        eng = engine
+        self._copies: set[int] = set()
+        self._outs: dict[int, torch.Tensor] = {}
+        self._keys = []
+        items = []
+        relin = None
+        for i, op in enumerate(self.ops):
+            ct = self.cts[op.index]
+            if not ct.data.is_contiguous():
+                raise ValueError(f"op {op}: ciphertext storage must be contiguous")
+            if op.kind == ROTATE and eng._canonical_step(op.step) == 0:
+                self._copies.add(i)
+                continue
+            if op.kind == HMULT:
+                relin = relin if relin is not None else eng.relinearization_key
+                out = eng._empty(2, ct.limb_count - 1, eng.n)
+                b = self.cts[op.partner].data
+                if not b.is_contiguous():
+                    raise ValueError(f"op {op}: partner storage must be contiguous")
+                items.append(nat.KsItem(nat.ITEM_HMULT_RELIN_RESCALE, ct.level, 1, 0, nat.ptr(ct.data),
+                                        nat.ptr(b), nat.ptr(relin.data), nat.ptr(out)))
+            else:
+                key = eng.rotation_key(op.step)
+                self._keys.append(key)
+                out = eng._empty(2, ct.limb_count, eng.n)
+                items.append(nat.KsItem(nat.ITEM_ROTATE, ct.level, int(key.galois_element), 0, nat.ptr(ct.data),
+                                        None, nat.ptr(key.data), nat.ptr(out)))
+            self._outs[i] = out
+        self._relin = relin
+        self._graph: torch.cuda.CUDAGraph | None = None
+        self.count = len(items)
+        self.chunks: list[tuple[nat.ItemsPlanInfo, torch.Tensor]] = []
+        if self.count == 0:
+            return
+        ctx = eng.ctx
+
+        def plan_info(batch):
+            info = nat.ItemsPlanInfo()
+            ctx.call("fhb_ckks_items_plan_info", (nat.KsItem * len(batch))(*batch), len(batch), ctypes.byref(info))
+            return info
+
+        # Items of one level (and key) side by side; chunks cut where the
+        # scratch of the items in flight would pass max_scratch_bytes.
+        order = sorted(range(self.count), key=lambda j: (items[j].level, items[j].kind, items[j].key or 0))
+        sizes = {j: int(plan_info([items[j]]).scratch_bytes) for j in order}
+        parts, cur, used = [], [], 0
+        for j in order:
+            if cur and used + sizes[j] > max_scratch_bytes:
+                parts.append(cur)
+                cur, used = [], 0
+            cur.append(items[j])
+            used += sizes[j]
+        parts.append(cur)
+        infos = [plan_info(part) for part in parts]
+        self.scratch = torch.empty(max(max(int(i.scratch_bytes) for i in infos), 16), dtype=torch.uint8,
+                                   device=eng.device)
+        for part, info in zip(parts, infos):
+            plan = torch.empty(max(int(info.plan_bytes), 16), dtype=torch.uint8, device=eng.device)
+            ctx.call("fhb_ckks_items_plan", (nat.KsItem * len(part))(*part), len(part), nat.ptr(plan),
+                     nat.ptr(self.scratch), ctypes.byref(info))
+            self.chunks.append((info, plan))
+
+    def _issue(self) -> None:
+        eng = self.engine
+        st = torch.cuda.current_stream(eng.device).cuda_stream
+        for info, plan in self.chunks:  # in stream order: the chunks share one scratch
+            eng.ctx.call("fhb_ckks_items_run", nat.ptr(plan), ctypes.byref(info), st)
+
+    def capture(self) -> None:
+        eng = self.engine
+        self._issue()  # first run eagerly: sets kernel attributes outside the capture
+        torch.cuda.synchronize(eng.device)
+        graph = torch.cuda.CUDAGraph()
+        cap = torch.cuda.Stream(eng.device)
+        cap.wait_stream(torch.cuda.current_stream(eng.device))
+        with torch.cuda.graph(graph, stream=cap):
+            self._issue()
+        torch.cuda.current_stream(eng.device).wait_stream(cap)
+        self._graph = graph
+
+    def run(self) -> None:
+        """One pass over the whole batch on the current stream."""
+        if not self.use_graph:
+            self._issue()
+            return
+        if self._graph is None:
+            self.capture()
+        self._graph.replay()
+
+    @property
+    def launches_per_run(self) -> int:
+        """Library kernels one run launches."""
+        return sum(6 if info.hmult_items else 3 for info, _ in self.chunks)
+
+    def result_view(self, op_index: int) -> torch.Tensor:
+        """[2, limbs, N] view of op `op_index`'s result."""
+        if op_index in self._copies:
+            return self.cts[self.ops[op_index].index].data.view(2, -1, self.engine.n)
+        return self._outs[op_index]
+
+    def result(self, op_index: int) -> Ciphertext:
+        return _result(self, op_index)
+
+    def results(self) -> list[Ciphertext]:
+        return [self.result(i) for i in range(len(self.ops))]
+
+
+def _validate(eng, cts: Sequence[Ciphertext], ops: Sequence[MixedOp]) -> None:
+    for ct in cts:
+        ct.assert_state(polynomial_domain="coefficient", residue_representation="standard", components=2)
+        eng._check_ct(ct)
+        if ct.batch_size != 1:
+            raise ValueError("mixed batches take ciphertexts of batch size 1")
+    for op in ops:
+        if not 0 <= op.index < len(cts):
+            raise ValueError(f"op {op} refers to a missing ciphertext")
+        if op.kind == HMULT:
+            if not 0 <= op.partner < len(cts):
+                raise ValueError(f"op {op} has no partner")
+            a, b = cts[op.index], cts[op.partner]
+            if a.level != b.level:
+                raise ValueError(f"op {op}: partner is at another level")
+            if a.limb_count < 2:
+                raise ValueError(f"op {op}: no level left to rescale into")
+        elif op.kind != ROTATE:
+            raise ValueError(f"unknown op kind {op.kind!r}")
+
+
+def _result(ex, op_index: int) -> Ciphertext:
+    eng = ex.engine
+    op = ex.ops[op_index]
+    ct = ex.cts[op.index]
+    data = ex.result_view(op_index).contiguous().view(2, *ct.batch_shape, -1, eng.n)
+    if op_index in ex._copies:
+        return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
+    if op.kind == HMULT:
+        scale = eng.rescale_to_next_output_scale(ct.scale * ex.cts[op.partner].scale, level=ct.level)
+        return Ciphertext(data, ct.level + 1, scale, "coefficient", "standard")
+    return Ciphertext(data, ct.level, ct.scale, "coefficient", "standard")
 
 
 def run_per_ciphertext(engine, ciphertexts: Sequence[Ciphertext], ops: Sequence[MixedOp]) -> list[Ciphertext]:

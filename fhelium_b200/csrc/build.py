@@ -23,7 +23,8 @@ LIB = os.path.join(LIB_DIR, "libfhb200.so")
 # (source, object name, extra defines): the cluster kernels are instantiated
 # once per ring degree so that nvcc can compile them in parallel.
 SOURCES = [("fhb_context.cu", "fhb_context.o", []), ("fhb_capi.cu", "fhb_capi.o", []), ("fhb_ops.cu", "fhb_ops.o", []),
-           ("fhb_noalloc.cu", "fhb_noalloc.o", []), ("fhb_tc_ntt.cu", "fhb_tc_ntt.o", []), ("fhb_tc_basis.cu", "fhb_tc_basis.o", [])] + [
+           ("fhb_noalloc.cu", "fhb_noalloc.o", []), ("fhb_tc_ntt.cu", "fhb_tc_ntt.o", []), ("fhb_tc_basis.cu", "fhb_tc_basis.o", []),
+           ("fhb_items.cu", "fhb_items.o", [])] + [
     ("fhb_inst_logn.cu", f"fhb_inst_logn{k}.o", [f"-DFHB_LOGN={k}"]) for k in range(12, 18)]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

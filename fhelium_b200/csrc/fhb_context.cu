@@ -93,7 +93,7 @@ uint64_t prefix_product_mod(const std::vector<uint64_t>& mods, int k, uint64_t m
 }
 
 template <typename T>
-bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& levels) {
+bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& levels, LevelTables<T>*& levels_dev) {
   const int qp = c.qp();
   const uint64_t n = c.n();
   const int radix_bits = sizeof(T) == 8 ? 62 : 30;
@@ -215,6 +215,8 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
     lt.rescale_inv = upload(c, rs);
     if (!lt.digits || !lt.garner || !lt.ext || !lt.rescale_inv) return false;
   }
+  levels_dev = upload(c, levels);
+  if (!levels_dev) return false;
   return t.prime && t.tw_fwd && t.tw_inv && t.p_garner && t.p_mix && t.p_inv && t.p_rinv;
 }
 
@@ -257,7 +259,8 @@ Context* build_context(int bits, int log_n, const uint64_t* moduli, int num_q, i
   c->num_p = num_p;
   c->device = device;
   c->moduli.assign(moduli, moduli + num_q + num_p);
-  bool ok = bits == 64 ? build_tables<uint64_t>(*c, c->t64, c->lv64) : build_tables<uint32_t>(*c, c->t32, c->lv32);
+  bool ok = bits == 64 ? build_tables<uint64_t>(*c, c->t64, c->lv64, c->lv64_dev)
+                       : build_tables<uint32_t>(*c, c->t32, c->lv32, c->lv32_dev);
   if (!ok) {
     cudaError_t e = cudaGetLastError();
     *status = e != cudaSuccess ? cuda_status(e, "context tables") : fail(-3, "no primitive 2N-th root for a modulus");

@@ -81,6 +81,10 @@ struct Context {
   ChainTables<uint32_t> t32;
   std::vector<LevelTables<uint64_t>> lv64;
   std::vector<LevelTables<uint32_t>> lv32;
+  // the same per-level tables as a device array [num_q] (kernels over
+  // ciphertexts of several levels index it by each item's level)
+  LevelTables<uint64_t>* lv64_dev = nullptr;
+  LevelTables<uint32_t>* lv32_dev = nullptr;
   std::vector<void*> allocations;
   int ks_order = 2;  // tuning: work order of the key-switch clusters (see ks_work)
   int ntt_ept_fwd = 0;  // tuning: residues per thread of the standalone forward NTT (0 = default)
@@ -118,6 +122,12 @@ template <>
 inline const LevelTables<uint64_t>& level_tables<uint64_t>(const Context& c, int level) { return c.lv64[level]; }
 template <>
 inline const LevelTables<uint32_t>& level_tables<uint32_t>(const Context& c, int level) { return c.lv32[level]; }
+template <typename T>
+inline const LevelTables<T>* level_tables_dev(const Context& c);
+template <>
+inline const LevelTables<uint64_t>* level_tables_dev<uint64_t>(const Context& c) { return c.lv64_dev; }
+template <>
+inline const LevelTables<uint32_t>* level_tables_dev<uint32_t>(const Context& c) { return c.lv32_dev; }
 
 // Exact int8 tensor-core NTT (fhb_tc_ntt.cu).  tc_ntt_prepare builds the
 // tables once (blocking); tc_ntt runs both passes of one direction;

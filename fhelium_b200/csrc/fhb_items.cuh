@@ -1,0 +1,302 @@
+// Key switches of ciphertexts at mixed levels, driven by a device table of
+// item descriptors: every stage is one launch over all items, whatever their
+// levels, instead of one launch sequence per level.
+//
+// An item is one ciphertext (batch 1) with its own operation:
+//   kind 0  HMult + relinearise + rescale of a (lhs) and b (rhs), both
+//           [2, L, N] coefficient/standard, with the relinearisation key;
+//   kind 1  rotation of a [2, L, N] coefficient/standard by its own Galois
+//           element with its own rotation key.
+// The stages mirror the fused batch path (forward NTT of the operands, the
+// tensor product, the inverse NTT of d2, ModUp digits, the key-switch core
+// with c0, c1 folded in for relinearisation, ModDown with the rescale or
+// with sigma_g(c0)), and use the same building blocks, so every result is
+// integer-equal to the per-level batch calls.  Work lists of (item, row)
+// units map the cluster kernels' clusters to items; the element-wise kernels
+// take the item from the grid's z dimension.
+#pragma once
+#include "fhb_kernels.cuh"
+
+namespace fhb {
+
+struct KsItem {
+  int32_t kind;         // 0: HMult + relinearise + rescale, 1: rotation
+  int32_t level;
+  uint32_t galois;      // rotation: Galois element of the step; 1 for HMult
+  int32_t reserved;
+  const void* a;        // [2, L, N] coefficient/standard (lhs, or the rotated ciphertext)
+  const void* b;        // HMult rhs [2, L, N] coefficient/standard; null for a rotation
+  const void* key;      // [D, 2, QP0, N] NTT/Montgomery key
+  void* out;            // HMult [2, L - 1, N]; rotation [2, L, N]; coefficient/standard
+  void* ab;             // scratch: HMult [2 operands][2][L][N] NTT/Montgomery
+  void* coef;           // scratch: HMult ct3 [3, L, N] NTT/Montgomery
+  void* digits;         // scratch: [L, N] ModUp digits
+  void* t0;             // scratch: [L + P, N] (d2 in the coefficient domain, then accumulator 0)
+  void* t1;             // scratch: [L + P, N] accumulator 1
+};
+
+struct ItemUnit {
+  int32_t item;
+  int32_t row;          // forward NTT: operand * 2 L + component * L + row
+};
+
+// Tensor product of the HMult items (k_mul_ntt per item): grid (N / (256 V),
+// rows, HMult items), rows past an item's level return.
+template <typename T, int V>
+__global__ void k_items_mul(const KsItem* __restrict__ items, const int32_t* __restrict__ hmult, int num_q,
+                            int log_n, ChainTables<T> tabs) {
+  const KsItem it = items[hmult[blockIdx.z]];
+  const int limbs = num_q - it.level;
+  const int row = blockIdx.y;
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t k = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
+  if (row >= limbs || k >= n) return;
+  const PrimeInfo<T>& pp = tabs.prime[it.level + row];
+  const T q = pp.q, ni = pp.neg_inv, tq = pp.twice_q;
+  const T* ab = static_cast<const T*>(it.ab);
+  const int64_t comp = int64_t(limbs) * n, i = int64_t(row) * n + k;
+  const EwVec<T, V> x0 = ew_load<T, V>(ab + i), x1 = ew_load<T, V>(ab + comp + i);
+  const EwVec<T, V> y0 = ew_load<T, V>(ab + 2 * comp + i), y1 = ew_load<T, V>(ab + 3 * comp + i);
+  EwVec<T, V> d0, d1, d2;
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    d0.v[e] = Word<T>::mont(x0.v[e], y0.v[e], q, ni);
+    d1.v[e] = csub(Word<T>::mont(x0.v[e], y1.v[e], q, ni) + Word<T>::mont(x1.v[e], y0.v[e], q, ni), tq);
+    d2.v[e] = Word<T>::mont(x1.v[e], y1.v[e], q, ni);
+  }
+  T* out = static_cast<T*>(it.coef);
+  ew_store<T, V>(out + i, d0);
+  ew_store<T, V>(out + comp + i, d1);
+  ew_store<T, V>(out + 2 * comp + i, d2);
+}
+
+// ModUp digits of every item (k_modup_digits per item): the source is d2 in
+// the coefficient domain (t0) for HMult, c1 through sigma_g for a rotation.
+// Grid (N / (256 V), digits, items), digits past an item's level return.
+template <typename T, int V>
+__global__ void k_items_modup(const KsItem* __restrict__ items, const LevelTables<T>* __restrict__ levels,
+                              int num_q, int log_n, ChainTables<T> tabs) {
+  const KsItem it = items[blockIdx.z];
+  const LevelTables<T> lt = levels[it.level];
+  if (int(blockIdx.y) >= lt.num_digits) return;
+  const int64_t n = int64_t(1) << log_n;
+  const int64_t k0 = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
+  if (k0 >= n) return;
+  using W = Word<T>;
+  const int limbs = num_q - it.level;
+  const DigitDesc d = lt.digits[blockIdx.y];
+  const TwPair<T>* g = lt.garner + blockIdx.y * kMaxDigitWidth * kMaxDigitWidth;
+  const uint32_t gi = (it.kind == 0 || it.galois == 1) ? 0u : galois_inverse_dev(it.galois, log_n);
+  const T* src = it.kind == 0 ? static_cast<const T*>(it.t0) : static_cast<const T*>(it.a) + int64_t(limbs) * n;
+  T* dst = static_cast<T*>(it.digits);
+  EwVec<T, V> dig[kMaxDigitWidth];
+  for (int r = 0; r < d.alpha; ++r) {
+    const int row = d.prime0 - it.level + r;
+    const T q = tabs.prime[d.prime0 + r].q;
+    EwVec<T, V> x;
+    if (gi == 0) {
+      x = ew_load<T, V>(src + row * n + k0);
+#pragma unroll
+      for (int e = 0; e < V; ++e) x.v[e] = csub(x.v[e], q);
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        bool neg = false;
+        const int srck = galois_source(int(k0) + e, log_n, gi, neg);
+        T y = csub(src[row * n + srck], q);
+        x.v[e] = (neg && y) ? q - y : y;
+      }
+    }
+    if (r > 0) {
+      const TwPair<T> inv = g[r * kMaxDigitWidth + r];
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        T acc = 0;
+        for (int i = 0; i < r; ++i) {
+          const TwPair<T> c = g[r * kMaxDigitWidth + i];
+          acc = csub(acc + csub(W::shoup(dig[i].v[e], c.w, c.wp, q), q), q);
+        }
+        x.v[e] = csub(W::shoup(csub(x.v[e] + q - acc, q), inv.w, inv.wp, q), q);
+      }
+    }
+    dig[r] = x;
+    ew_store<T, V>(dst + row * n + k0, x);
+  }
+}
+
+// ModDown of every item (k_moddown per item): HMult items rescale by the
+// leading prime (c0, c1 are already in the accumulators); rotations add
+// sigma_g(c0).  Grid (N / 256, items), one coefficient per thread.
+template <typename T>
+__global__ void k_items_moddown(const KsItem* __restrict__ items, const LevelTables<T>* __restrict__ levels,
+                                int num_q, int num_p, int log_n, ChainTables<T> tabs) {
+  using W = Word<T>;
+  const KsItem it = items[blockIdx.y];
+  const int64_t n = int64_t(1) << log_n;
+  const int k = int(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int level = it.level;
+  const int q_limbs = num_q - level, qp0 = num_q + num_p;
+  const int rescale = it.kind == 0 ? 1 : 0;
+  const int out_limbs = q_limbs - rescale;
+  const uint32_t gi = (it.kind == 0 || it.galois == 1) ? 0u : galois_inverse_dev(it.galois, log_n);
+  bool neg = false;
+  const int ak = gi ? galois_source(k, log_n, gi, neg) : k;
+  const LevelTables<T> lt = levels[level];
+  for (int c = 0; c < 2; ++c) {
+    const T* t = static_cast<const T*>(c == 0 ? it.t0 : it.t1);
+    const T* ad = (it.kind == 1 && c == 0) ? static_cast<const T*>(it.a) : nullptr;
+    T e[kMaxDigitWidth];
+    for (int r = 0; r < num_p; ++r) {
+      const PrimeInfo<T> p = tabs.prime[num_q + r];
+      T x = t[(q_limbs + r) * n + k];
+      T acc = 0;
+      for (int i = 0; i < r; ++i) {
+        const TwPair<T> g = tabs.p_garner[r * kMaxDigitWidth + i];
+        acc = csub(acc + csub(W::shoup(e[i], g.w, g.wp, p.q), p.q), p.q);
+      }
+      if (r > 0) {
+        const TwPair<T> inv = tabs.p_garner[r * kMaxDigitWidth + r];
+        x = csub(W::shoup(csub(x + p.q - acc, p.q), inv.w, inv.wp, p.q), p.q);
+      }
+      e[r] = x;
+    }
+    T* o = static_cast<T*>(it.out) + int64_t(c) * out_limbs * n;
+    T v0 = 0;
+    for (int i = 0; i < q_limbs; ++i) {
+      const int pid = level + i;
+      const PrimeInfo<T> p = tabs.prime[pid];
+      T sub = 0;
+      for (int r = 0; r < num_p; ++r) {
+        const TwPair<T> m = tabs.p_mix[r * qp0 + pid];
+        sub = csub(sub + csub(W::shoup(e[r], m.w, m.wp, p.q), p.q), p.q);
+      }
+      const TwPair<T> pinv = tabs.p_inv[pid];
+      T v = csub(t[i * n + k] + p.q - sub, p.q);
+      v = csub(W::shoup(v, pinv.w, pinv.wp, p.q), p.q);
+      if (ad) {
+        T x = csub(ad[i * n + ak], p.q);
+        if (neg && x) x = p.q - x;
+        v = csub(v + x, p.q);
+      }
+      if (!rescale) {
+        o[i * n + k] = v;
+      } else if (i == 0) {
+        v0 = v;
+      } else {
+        const T x0 = reduce_any(v0, p);
+        const TwPair<T> inv = lt.rescale_inv[pid];
+        T r = csub(W::shoup(csub(v + p.q - x0, p.q), inv.w, inv.wp, p.q), p.q);
+        r += (v0 > (tabs.prime[level].q >> 1)) ? 1 : 0;
+        o[(i - 1) * n + k] = csub(r, p.q);
+      }
+    }
+  }
+}
+
+// Forward NTT of the HMult operands (k_ntt_forward per row): one cluster per
+// unit (item, operand 2 L + component L + row), coefficient/standard ->
+// NTT/Montgomery (x R), lazy [0, 2q), into the item's `ab`.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_items_ntt_forward(const KsItem* __restrict__ items, const ItemUnit* __restrict__ units, int num_q,
+                    ChainTables<T> tabs) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const ItemUnit u = units[blockIdx.x / G::kC];
+  const KsItem it = items[u.item];
+  const int limbs = num_q - it.level;
+  const int op = u.row / (2 * limbs), rem = u.row - op * 2 * limbs;  // rem = component L + row
+  const int pid = it.level + rem % limbs;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  RowSource<T, true> src{static_cast<const T*>(op == 0 ? it.a : it.b) + int64_t(rem) * G::kN, p.rmod, p.rmod_s,
+                         p.q};
+  T v[G::kE];
+  Ntt<T, LOGN>::forward_from(src, s, TwGlobal<T, LOGN>(tabs.tw_fwd + int64_t(pid) * G::kN), p.q, p.twice_q, rank,
+                             v);
+#pragma unroll
+  for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+  store16(static_cast<T*>(it.ab) + int64_t(u.row) * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
+}
+
+// Inverse NTT of d2 of the HMult items (k_ntt_inverse per row): one cluster
+// per unit (item, row), NTT/Montgomery -> coefficient/standard canonical,
+// into the item's t0.
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_items_ntt_inverse(const KsItem* __restrict__ items, const ItemUnit* __restrict__ units, int num_q,
+                    ChainTables<T> tabs) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const ItemUnit u = units[blockIdx.x / G::kC];
+  const KsItem it = items[u.item];
+  const int limbs = num_q - it.level;
+  const int pid = it.level + u.row;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  T v[G::kE];
+  load16(static_cast<const T*>(it.coef) + int64_t(2 * limbs + u.row) * G::kN + int64_t(rank) * G::kM +
+             threadIdx.x * G::kE,
+         v);
+  InvEpilogue<T> epi = make_inv_epilogue<T>(static_cast<T*>(it.t0) + int64_t(u.row) * G::kN, p, kInvStandard, true);
+  Ntt<T, LOGN>::inverse(s, TwGlobal<T, LOGN>(tabs.tw_inv + int64_t(pid) * G::kN), p.q, p.twice_q, rank, v, epi);
+}
+
+// Key-switch core of every item (k_keyswitch_core per (ciphertext, row)):
+// one cluster per unit (item, destination row of Q_l P).  For HMult items
+// the NTT-domain ct3 is folded in (c0, c1 as P c_k, own-digit rows from c2).
+template <typename T, int LOGN>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_items_core(const KsItem* __restrict__ items, const ItemUnit* __restrict__ units,
+             const LevelTables<T>* __restrict__ levels, int num_q, int num_p, ChainTables<T> tabs) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const int rank = cluster_rank<T, LOGN>();
+  const ItemUnit u = units[blockIdx.x / G::kC];
+  const KsItem it = items[u.item];
+  const int level = it.level, jrow = u.row, q_limbs = num_q - level, qp0 = num_q + num_p;
+  const int pid = level + jrow;
+  const PrimeInfo<T> p = tabs.prime[pid];
+  const LevelTables<T> lt = levels[level];
+  const T* dig = static_cast<const T*>(it.digits);
+  const T* key = static_cast<const T*>(it.key);
+  T* acc0 = static_cast<T*>(it.t0) + int64_t(jrow) * G::kN;
+  T* acc1 = static_cast<T*>(it.t1) + int64_t(jrow) * G::kN;
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  KsAcc<T, LOGN> acc(s, acc0 + own, acc1 + own);
+  KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(false);
+  const bool add = it.kind == 0 && jrow < q_limbs;
+  const T* ct3_own = add ? static_cast<const T*>(it.coef) + int64_t(jrow) * G::kN + own : nullptr;
+  const int64_t ct3_stride = int64_t(q_limbs) * G::kN;
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
+    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
+    T v[G::kE];
+    if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
+      ks_own_digit_ntt(v, ct3_own, ct3_stride, p);
+    } else {
+      ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
+                       qp0, d.alpha, LOGN, p.q, p.twice_q};
+      tw.forward_from(src, s, p, v);
+    }
+    key_mac(acc, v, key0, key1, p);
+  }
+  tw.stage(true);
+  T v[G::kE];
+  acc.get(0, v);
+  if (add) ks_add_p_scaled(v, 0, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
+  InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0, p, kInvStandard, false);
+  tw.inverse(s, p, v, e0);
+  acc.get(1, v);
+  if (add) ks_add_p_scaled(v, 1, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
+  InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1, p, kInvStandard, false);
+  tw.inverse(s, p, v, e1);
+}
+
+}  // namespace fhb

@@ -2,6 +2,7 @@
 // instantiated per LOGN in its own translation unit (fhb_inst_logn.cu), so
 // the kernel templates compile in parallel.
 #pragma once
+#include "fhb_items.cuh"
 #include "fhb_kernels.cuh"
 
 namespace fhb {
@@ -137,6 +138,21 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
                                  galois == 1 ? 0u : galois, c.ks_order, tables<T>(c), level_tables<T>(c, level));
 }
 
+// ---- mixed-level item stages (fhb_items.cuh): one cluster per unit ----------
+template <typename T, int LOGN>
+int run_items(const Context& c, int stage, const void* items, const void* units, int64_t count, cudaStream_t st) {
+  const auto* it = static_cast<const KsItem*>(items);
+  const auto* un = static_cast<const ItemUnit*>(units);
+  if (stage == 0)
+    return launch_cluster<T, LOGN>(k_items_ntt_forward<T, LOGN>, count, ntt_smem<T, LOGN>(), st, it, un, c.num_q,
+                                   tables<T>(c));
+  if (stage == 1)
+    return launch_cluster<T, LOGN>(k_items_ntt_inverse<T, LOGN>, count, ntt_smem<T, LOGN>(), st, it, un, c.num_q,
+                                   tables<T>(c));
+  return launch_cluster<T, LOGN>(k_items_core<T, LOGN>, count, KsAcc<T, LOGN>::smem_bytes(), st, it, un,
+                                 level_tables_dev<T>(c), c.num_q, c.num_p, tables<T>(c));
+}
+
 // Explicit instantiation of every runner for one (T, LOGN).
 #define FHB_INSTANTIATE_RUNNERS(T, LOGN)                                                                       \
   template int run_forward<T, LOGN>(const Context&, const void*, void*, int64_t, int, int, bool, cudaStream_t);   \
@@ -147,6 +163,7 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
   template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
                                    cudaStream_t, bool);                                                         \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
+  template int run_items<T, LOGN>(const Context&, int, const void*, const void*, int64_t, cudaStream_t);         \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);
 

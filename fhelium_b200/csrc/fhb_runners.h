@@ -22,6 +22,10 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
 template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
                int64_t batch, int level, cudaStream_t st, bool pre);
+// Mixed-level item stages: 0 = forward NTT of the HMult operands, 1 =
+// inverse NTT of d2, 2 = key-switch core; `count` units of `units`.
+template <typename T, int LOGN>
+int run_items(const Context& c, int stage, const void* items, const void* units, int64_t count, cudaStream_t st);
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
 template <typename T, int LOGN>

@@ -365,6 +365,44 @@ int fhb_ckks_keyswitch_sum(const fhb_context* ctx, const void* digits, const uin
 int fhb_ckks_keyswitch_sum_extended(const fhb_context* ctx, const void* ext, const uint64_t* key_ptrs, void* acc0,
                                     void* acc1, int giants, int64_t batch, int level, fhb_stream stream);
 
+/* ---- mixed-level batches: one launch per stage over every item ----------
+ * One item is one ciphertext (batch 1) with its own operation and level:
+ * HMult + relinearise + rescale of a and b (kind 0), or a rotation of a by
+ * its own Galois element with its own key (kind 1).  fhb_ckks_items_plan_info
+ * (host only) validates the items and returns the plan and scratch sizes;
+ * fhb_ckks_items_plan writes the device plan (item descriptors with their
+ * scratch regions resolved, and the work lists of the cluster stages) into
+ * `plan` with a blocking copy, binding it to `scratch`; fhb_ckks_items_run
+ * then issues six launches over all items - forward NTT of the HMult
+ * operands, tensor product, inverse NTT of d2, ModUp digits, key-switch
+ * core, ModDown with the rescale or with sigma_g(c0) - with no host call, so
+ * it can be captured in a CUDA graph and replayed (the plan, scratch, inputs
+ * and outputs must stay allocated).  Results are integer-equal to the
+ * per-level calls (fhb_ckks_multiply_relinearize with rescale after a
+ * forward NTT of the operands, fhb_ckks_rotate).  Replaces the reference's
+ * one engine call sequence per ciphertext (fhelium/engine/ckks_engine.py:
+ * 1530-1675, 2183-2300), which has no batched counterpart. */
+enum fhb_item_kind { FHB_ITEM_HMULT_RELIN_RESCALE = 0, FHB_ITEM_ROTATE = 1 };
+typedef struct fhb_ks_item {
+  int32_t kind;       /* fhb_item_kind */
+  int32_t level;
+  uint32_t galois;    /* rotation: Galois element of the step (odd, < 2N); ignored for HMult */
+  int32_t reserved;   /* 0 */
+  const void* a;      /* [2, L, N] coefficient/standard: HMult lhs, or the ciphertext to rotate */
+  const void* b;      /* HMult rhs [2, L, N] coefficient/standard; NULL for a rotation */
+  const void* key;    /* relinearisation or rotation key [D, 2, QP0, N] NTT/Montgomery */
+  void* out;          /* HMult [2, L - 1, N], rotation [2, L, N]: coefficient/standard canonical */
+} fhb_ks_item;
+typedef struct fhb_items_plan_info {
+  int64_t plan_bytes;     /* device bytes of the plan */
+  int64_t scratch_bytes;  /* device scratch bytes of the items */
+  int32_t items, hmult_items, forward_units, inverse_units, core_units, max_limbs, max_digits, reserved;
+} fhb_items_plan_info;
+int fhb_ckks_items_plan_info(const fhb_context* ctx, const fhb_ks_item* items, int count, fhb_items_plan_info* info);
+int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int count, void* plan, void* scratch,
+                        const fhb_items_plan_info* info);
+int fhb_ckks_items_run(const fhb_context* ctx, const void* plan, const fhb_items_plan_info* info, fhb_stream stream);
+
 /* Bounded decryption to float64 coefficients: phase [batch, L, N]
  * coefficient/standard canonical (c0 + c1 s) -> out [batch, N] float64 (a
  * DEVICE pointer), the centred representative modulo the product of the

@@ -1,6 +1,7 @@
 """Mixed-level batches: one CUDA graph over every (kind, level) group against
 one engine call sequence per ciphertext, bit for bit, and the autotuner."""
 
+import ctypes
 import json
 
 import numpy as np
@@ -8,7 +9,8 @@ import pytest
 import torch
 
 from fhelium_b200 import autotune
-from fhelium_b200.batch import HMULT, ROTATE, MixedBatchExecutor, MixedOp, run_per_ciphertext, sample_mixed_workload
+from fhelium_b200.batch import (HMULT, ROTATE, MixedBatchExecutor, MixedItemsExecutor, MixedOp, run_per_ciphertext,
+                                sample_mixed_workload)
 from fhelium_b200.config import Preset
 from fhelium_b200.engine import CkksEngine
 
@@ -43,6 +45,101 @@ def test_mixed_batch_bit_exact(small, streams, use_graph):
         got = ex.result(i)
         assert (got.level, got.scale) == (w.level, w.scale)
         assert torch.equal(got.data, w.data), f"op {i} ({ops[i]}) differs"
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_items_bit_exact(small, use_graph):
+    """Six launches over every level: the same residues as the per-ciphertext loop."""
+    eng, cts, ops, want = small
+    ex = MixedItemsExecutor(eng, cts, ops, use_graph=use_graph)
+    assert ex.launches_per_run == 6 and len(ex.chunks) == 1
+    assert ex.chunks[0][0].max_limbs == max(c.limb_count for c in cts)
+    for _ in range(2):
+        ex.run()
+    torch.cuda.synchronize()
+    for i, w in enumerate(want):
+        got = ex.result(i)
+        assert (got.level, got.scale) == (w.level, w.scale)
+        assert torch.equal(got.data, w.data), f"op {i} ({ops[i]}) differs"
+
+
+def test_items_chunked(small):
+    """A scratch limit below the batch's need splits it into chunks that
+    share one scratch, in stream order; the residues do not change."""
+    eng, cts, ops, want = small
+    one = MixedItemsExecutor(eng, cts, ops, use_graph=False)
+    total = int(one.chunks[0][0].scratch_bytes)
+    del one
+    ex = MixedItemsExecutor(eng, cts, ops, max_scratch_bytes=total // 3)
+    assert len(ex.chunks) >= 3 and ex.scratch.numel() <= total // 3 + (64 << 20)
+    assert sum(info.items for info, _ in ex.chunks) == ex.count
+    ex.run()
+    torch.cuda.synchronize()
+    for i, w in enumerate(want):
+        assert torch.equal(ex.result(i).data, w.data), f"op {i} ({ops[i]}) differs"
+
+
+def test_items_inputs_updated_between_replays(small):
+    eng, cts, ops, _ = small
+    mine = [c.clone() for c in cts]
+    ex = MixedItemsExecutor(eng, mine, ops)
+    ex.run()
+    first = ex.result(0).data.clone()
+    i0 = ops[0].index
+    other = next(j for j, c in enumerate(cts) if j != i0 and c.level == cts[i0].level)
+    mine[i0].data.copy_(cts[other].data)
+    ex.run()
+    assert not torch.equal(ex.result(0).data, first)
+    mine[i0].data.copy_(cts[i0].data)
+    ex.run()
+    assert torch.equal(ex.result(0).data, first)
+
+
+def test_items_rotations_only_and_zero_step(small):
+    eng, cts, _, _ = small
+    ops = [MixedOp(ROTATE, 0, step=0), MixedOp(ROTATE, 1, step=3), MixedOp(ROTATE, 2, step=-5),
+           MixedOp(ROTATE, 3, step=eng.num_slots)]
+    ex = MixedItemsExecutor(eng, cts, ops)
+    assert ex.launches_per_run == 3 and ex.count == 2
+    ex.run()
+    want = run_per_ciphertext(eng, cts, ops)
+    assert torch.equal(ex.result(0).data, cts[0].data)
+    assert torch.equal(ex.result(3).data, cts[3].data)
+    for i in (1, 2):
+        assert torch.equal(ex.result(i).data, want[i].data)
+
+
+@pytest.mark.parametrize("preset", [Preset.slots32768_scale40_levels34_int64, Preset.slots16384_scale25_levels29_int32])
+def test_items_large_ring_and_int32(preset):
+    """logN 16 with 64-bit words, and a 32-bit-word chain (logN 15)."""
+    eng = CkksEngine(preset, rng_seed=5)
+    count = 10
+    cts, ops = _workload(eng, count, seed=21, max_step=1 << 10)
+    want = run_per_ciphertext(eng, cts, ops)
+    ex = MixedItemsExecutor(eng, cts, ops)
+    ex.run()
+    torch.cuda.synchronize()
+    for i, w in enumerate(want):
+        assert torch.equal(ex.result(i).data, w.data), f"op {i} ({ops[i]}) differs"
+
+
+def test_items_rejects_unaligned_and_bad_level(small):
+    from fhelium_b200 import _native as nat
+    eng, cts, _, _ = small
+    ct = cts[0]
+    out = eng._empty(2, ct.limb_count, eng.n)
+    key = eng.rotation_key(1)
+    good = nat.KsItem(nat.ITEM_ROTATE, ct.level, int(key.galois_element), 0, nat.ptr(ct.data), None,
+                      nat.ptr(key.data), nat.ptr(out))
+    info = nat.ItemsPlanInfo()
+    arr = (nat.KsItem * 1)(good)
+    eng.ctx.call("fhb_ckks_items_plan_info", arr, 1, ctypes.byref(info))
+    assert info.items == 1 and info.hmult_items == 0 and info.core_units == ct.limb_count + eng.num_p
+    for field, value in (("a", nat.ptr(ct.data) + 8), ("level", eng.num_q), ("galois", 2), ("kind", 7)):
+        bad = nat.KsItem.from_buffer_copy(good)
+        setattr(bad, field, value)
+        with pytest.raises(nat.NativeCallError):
+            eng.ctx.call("fhb_ckks_items_plan_info", (nat.KsItem * 1)(bad), 1, ctypes.byref(info))
 
 
 def test_mixed_batch_decrypts(small):
