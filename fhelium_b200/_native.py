@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "fhb_ckks_items_plan_info": (_I, [_P, ctypes.POINTER(KsItem), _I, ctypes.POINTER(ItemsPlanInfo)]),
     "fhb_ckks_items_plan": (_I, [_P, ctypes.POINTER(KsItem), _I, _P, _P, ctypes.POINTER(ItemsPlanInfo)]),
     "fhb_ckks_items_run": (_I, [_P, _P, ctypes.POINTER(ItemsPlanInfo), _P]),
+    "fhb_ckks_items_status": (_I, [_P, _P, ctypes.POINTER(ItemsPlanInfo), ctypes.POINTER(ctypes.c_int)]),
     "fhb_ckks_bsgs_inner_product": (_I, [_P, _P, _I64, _P, _I64, _I, _P, _I, _I, _P, _I64, _I64, _I, _I, _P]),
     "fhb_ckks_monomial": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
     "fhb_ckks_modraise": (_I, [_P, _P, _P, _I64, _I, _I, _I, _P]),
@@ -108,7 +109,7 @@ SIGNATURES: dict[str, tuple] = {
 }
 
 (TUNE_KS_ORDER, TUNE_NTT_FORWARD_EPT, TUNE_NTT_INVERSE_EPT, TUNE_BASIS_CONVERSION, TUNE_TC_WAIT_US,
- TUNE_TC_TEST_STALL, TUNE_TC_MODDOWN) = range(7)
+ TUNE_TC_TEST_STALL, TUNE_TC_MODDOWN, TUNE_TC_NTT_FUSED) = range(8)
 BASIS_CUDA_CORES, BASIS_TENSOR_CORES = 0, 1
 OP_MONTGOMERY_MUL, OP_ADD_LAZY, OP_SUB_LAZY, OP_ADD_CANONICAL, OP_SUB_CANONICAL, OP_NEGATE = range(6)
 INV_MONTGOMERY, INV_STANDARD_LAZY, INV_STANDARD, INV_CENTERED = range(4)

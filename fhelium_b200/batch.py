@@ -296,7 +296,7 @@ class MixedItemsExecutor:
         self._copies: set[int] = set()
         self._outs: dict[int, torch.Tensor] = {}
         self._keys = []
-        items = []
+        items, item_ops = [], []
         relin = None
         for i, op in enumerate(self.ops):
             ct = self.cts[op.index]
@@ -313,17 +313,20 @@ class MixedItemsExecutor:
                     raise ValueError(f"op {op}: partner storage must be contiguous")
                 items.append(nat.KsItem(nat.ITEM_HMULT_RELIN_RESCALE, ct.level, 1, 0, nat.ptr(ct.data),
                                         nat.ptr(b), nat.ptr(relin.data), nat.ptr(out)))
+                item_ops.append(i)
             else:
                 key = eng.rotation_key(op.step)
                 self._keys.append(key)
                 out = eng._empty(2, ct.limb_count, eng.n)
                 items.append(nat.KsItem(nat.ITEM_ROTATE, ct.level, int(key.galois_element), 0, nat.ptr(ct.data),
                                         None, nat.ptr(key.data), nat.ptr(out)))
+                item_ops.append(i)
             self._outs[i] = out
         self._relin = relin
         self._graph: torch.cuda.CUDAGraph | None = None
         self.count = len(items)
         self.chunks: list[tuple[nat.ItemsPlanInfo, torch.Tensor]] = []
+        self.chunk_ops: list[list[int]] = []  # op index of every item of each chunk, in plan order
         if self.count == 0:
             return
         ctx = eng.ctx
@@ -342,9 +345,11 @@ class MixedItemsExecutor:
             if cur and used + sizes[j] > max_scratch_bytes:
                 parts.append(cur)
                 cur, used = [], 0
-            cur.append(items[j])
+            cur.append(j)
             used += sizes[j]
         parts.append(cur)
+        self.chunk_ops = [[item_ops[j] for j in part] for part in parts]
+        parts = [[items[j] for j in part] for part in parts]
         infos = [plan_info(part) for part in parts]
         self.scratch = torch.empty(max(max(int(i.scratch_bytes) for i in infos), 16), dtype=torch.uint8,
                                    device=eng.device)
@@ -385,6 +390,17 @@ class MixedItemsExecutor:
     def launches_per_run(self) -> int:
         """Library kernels one run launches."""
         return sum(6 if info.hmult_items else 3 for info, _ in self.chunks)
+
+    def status(self) -> int:
+        """First error the kernels raised since the last call (0: none), after
+        waiting for the device; see fhb_ckks_items_status for the codes."""
+        torch.cuda.synchronize(self.engine.device)
+        worst = 0
+        for info, plan in self.chunks:
+            word = ctypes.c_int(0)
+            self.engine.ctx.call("fhb_ckks_items_status", nat.ptr(plan), ctypes.byref(info), ctypes.byref(word))
+            worst = worst or int(word.value)
+        return worst
 
     def result_view(self, op_index: int) -> torch.Tensor:
         """[2, limbs, N] view of op `op_index`'s result."""

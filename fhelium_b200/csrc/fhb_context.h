@@ -97,6 +97,9 @@ struct Context {
   // tuning, with basis_tc: ModDown's P -> Q conversion on the tensor cores
   // (1) or on the CUDA cores (0, default: faster on B200)
   int tc_moddown = 0;
+  // tuning: the tensor-core NTT's 16-point pass fused with the adjacent
+  // 64-point pass (1) or three separate passes (0, default: faster on B200)
+  int tc_ntt_fused = 0;
   // limit of the tensor-core kernels' pipeline waits in ns (0 = the default
   // second); their drain waits always keep the default
   unsigned long long tc_wait_ns = 0;

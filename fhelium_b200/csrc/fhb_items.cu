@@ -10,6 +10,7 @@
 // and replayed.  The reference runs such a batch as one engine call sequence
 // per ciphertext (fhelium/engine/ckks_engine.py:1530-1675, 2183-2300).
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -26,11 +27,13 @@ namespace fhb {
 namespace {
 
 constexpr int64_t kRegionAlign = 256;
+// the device descriptors open the plan; tests address a descriptor's level by this layout
+static_assert(sizeof(KsItem) == 88 && offsetof(KsItem, level) == 4, "device descriptor layout");
 
 int64_t align_up(int64_t x) { return (x + kRegionAlign - 1) / kRegionAlign * kRegionAlign; }
 
 struct PlanLayout {
-  int64_t items_off, hmult_off, fwd_off, inv_off, core_off, plan_bytes;
+  int64_t items_off, hmult_off, fwd_off, inv_off, core_off, status_off, plan_bytes;
 };
 
 PlanLayout layout_of(const fhb_items_plan_info& info) {
@@ -40,7 +43,8 @@ PlanLayout layout_of(const fhb_items_plan_info& info) {
   l.fwd_off = l.hmult_off + align_up(int64_t(info.hmult_items) * 4);
   l.inv_off = l.fwd_off + align_up(int64_t(info.forward_units) * int64_t(sizeof(ItemUnit)));
   l.core_off = l.inv_off + align_up(int64_t(info.inverse_units) * int64_t(sizeof(ItemUnit)));
-  l.plan_bytes = l.core_off + align_up(int64_t(info.core_units) * int64_t(sizeof(ItemUnit)));
+  l.status_off = l.core_off + align_up(int64_t(info.core_units) * int64_t(sizeof(ItemUnit)));
+  l.plan_bytes = l.status_off + kRegionAlign;
   return l;
 }
 
@@ -85,12 +89,12 @@ int check_item(const Context& c, const fhb_ks_item& it, int i) {
   return 0;
 }
 
-int run_stage(const Context& c, int stage, const void* items, const void* units, int64_t count, cudaStream_t st) {
+int run_stage(const Context& c, int stage, const ItemsView& iv, const void* units, int64_t count, cudaStream_t st) {
   if (count == 0) return 0;
-#define FHB_ITEMS_CASE(L)                                                                   \
-  case L:                                                                                   \
-    return c.bits == 64 ? run_items<uint64_t, L>(c, stage, items, units, count, st)         \
-                        : run_items<uint32_t, L>(c, stage, items, units, count, st);
+#define FHB_ITEMS_CASE(L)                                                                                  \
+  case L:                                                                                                  \
+    return c.bits == 64 ? run_items<uint64_t, L>(c, stage, iv.items, iv.count, iv.status, units, count, st) \
+                        : run_items<uint32_t, L>(c, stage, iv.items, iv.count, iv.status, units, count, st);
   switch (c.log_n) {
     FHB_ITEMS_CASE(12)
     FHB_ITEMS_CASE(13)
@@ -108,24 +112,25 @@ template <typename T>
 int run_elementwise(const Context& c, const char* plan, const PlanLayout& l, const fhb_items_plan_info& info,
                     cudaStream_t st) {
   constexpr int V = 16 / sizeof(T);
-  const auto* items = reinterpret_cast<const KsItem*>(plan + l.items_off);
+  const ItemsView iv{reinterpret_cast<const KsItem*>(plan + l.items_off), info.items,
+                     reinterpret_cast<int*>(const_cast<char*>(plan) + l.status_off)};
   const int64_t n = c.n();
   const unsigned xb = unsigned((n / V + kEwThreads - 1) / kEwThreads);
   if (info.hmult_items > 0) {
-    int rc = run_stage(c, 0, items, plan + l.fwd_off, info.forward_units, st);
+    int rc = run_stage(c, 0, iv, plan + l.fwd_off, info.forward_units, st);
     if (rc) return rc;
     k_items_mul<T, V><<<dim3(xb, unsigned(info.max_limbs), unsigned(info.hmult_items)), kEwThreads, 0, st>>>(
-        items, reinterpret_cast<const int32_t*>(plan + l.hmult_off), c.num_q, c.log_n, tables<T>(c));
+        iv, reinterpret_cast<const int32_t*>(plan + l.hmult_off), c.num_q, c.log_n, tables<T>(c));
     if (int e = cuda_status(cudaGetLastError(), "k_items_mul")) return e;
-    rc = run_stage(c, 1, items, plan + l.inv_off, info.inverse_units, st);
+    rc = run_stage(c, 1, iv, plan + l.inv_off, info.inverse_units, st);
     if (rc) return rc;
   }
   k_items_modup<T, V><<<dim3(xb, unsigned(info.max_digits), unsigned(info.items)), kEwThreads, 0, st>>>(
-      items, level_tables_dev<T>(c), c.num_q, c.log_n, tables<T>(c));
+      iv, level_tables_dev<T>(c), c.num_q, c.log_n, tables<T>(c));
   if (int e = cuda_status(cudaGetLastError(), "k_items_modup")) return e;
-  if (int rc = run_stage(c, 2, items, plan + l.core_off, info.core_units, st)) return rc;
+  if (int rc = run_stage(c, 2, iv, plan + l.core_off, info.core_units, st)) return rc;
   k_items_moddown<T><<<dim3(unsigned((n + 255) / 256), unsigned(info.items)), 256, 0, st>>>(
-      items, level_tables_dev<T>(c), c.num_q, c.num_p, c.log_n, tables<T>(c));
+      iv, level_tables_dev<T>(c), c.num_q, c.num_p, c.log_n, tables<T>(c));
   return cuda_status(cudaGetLastError(), "k_items_moddown");
 }
 
@@ -204,6 +209,7 @@ int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int co
       for (int r = 0; r < 4 * ll; ++r) fwd[nf++] = fhb::ItemUnit{i, r};
       for (int r = 0; r < ll; ++r) inv[ni++] = fhb::ItemUnit{i, r};
     }
+    d.check = fhb::item_check(d);
     dev_items[i] = d;
   }
   // Core work list: items of one (level, key) back to back, and within such
@@ -228,6 +234,21 @@ int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int co
   }
   fhb::ItemsDeviceGuard guard(c.device);
   return fhb::cuda_status(cudaMemcpy(plan, host.data(), host.size(), cudaMemcpyHostToDevice), "plan upload");
+}
+
+int fhb_ckks_items_status(const fhb_context* ctx, void* plan, const fhb_items_plan_info* info, int* status) {
+  if (!ctx || !ctx->impl) return fail(-1, "context is NULL");
+  if (!plan || !info || !status || info->items < 1) return fail(-2, "NULL plan, plan info or status");
+  const fhb::Context& c = *ctx->impl;
+  fhb::ItemsDeviceGuard guard(c.device);
+  int* word = reinterpret_cast<int*>(static_cast<char*>(plan) + fhb::layout_of(*info).status_off);
+  int value = 0;
+  if (int e = fhb::cuda_status(cudaMemcpy(&value, word, sizeof(int), cudaMemcpyDeviceToHost), "status read"))
+    return e;
+  *status = value;
+  if (value != 0)
+    return fhb::cuda_status(cudaMemset(word, 0, sizeof(int)), "status reset");
+  return 0;
 }
 
 int fhb_ckks_items_run(const fhb_context* ctx, const void* plan, const fhb_items_plan_info* info,

@@ -23,7 +23,7 @@ struct KsItem {
   int32_t kind;         // 0: HMult + relinearise + rescale, 1: rotation
   int32_t level;
   uint32_t galois;      // rotation: Galois element of the step; 1 for HMult
-  int32_t reserved;
+  uint32_t check;       // item_check() of the other fields, written by the planner
   const void* a;        // [2, L, N] coefficient/standard (lhs, or the rotated ciphertext)
   const void* b;        // HMult rhs [2, L, N] coefficient/standard; null for a rotation
   const void* key;      // [D, 2, QP0, N] NTT/Montgomery key
@@ -40,12 +40,71 @@ struct ItemUnit {
   int32_t row;          // forward NTT: operand * 2 L + component * L + row
 };
 
+// Check word of a descriptor: FNV-1a over every field but the check itself.
+// The planner validates the fields on the host and stores the word; every
+// kernel recomputes it before it uses the item, so a descriptor changed in
+// device memory after planning is skipped (and reported) instead of being
+// trusted for addressing.
+__host__ __device__ __forceinline__ uint32_t fnv_mix(uint32_t h, uint64_t w) {
+  h = (h ^ uint32_t(w)) * 16777619u;
+  return (h ^ uint32_t(w >> 32)) * 16777619u;
+}
+
+__host__ __device__ __forceinline__ uint32_t item_check(const KsItem& it) {
+  uint32_t h = 2166136261u;
+  h = fnv_mix(h, (uint64_t(uint32_t(it.kind)) << 32) | uint32_t(it.level));
+  h = fnv_mix(h, it.galois);
+  const void* const ptrs[9] = {it.a, it.b, it.key, it.out, it.ab, it.coef, it.digits, it.t0, it.t1};
+#pragma unroll
+  for (int i = 0; i < 9; ++i) h = fnv_mix(h, uint64_t(reinterpret_cast<uintptr_t>(ptrs[i])));
+  return h;
+}
+
+// Status codes of a run (the first one raised is kept).
+enum ItemsStatus : int {
+  kItemsOk = 0,
+  kItemsBadIndex = 1,    // a work list names an item outside the plan
+  kItemsBadCheck = 2,    // a descriptor no longer matches its check word
+  kItemsBadRow = 3,      // a work-list row outside the item's rows
+  kItemsBadKind = 4,     // the HMult list names a rotation
+};
+
+struct ItemsView {
+  const KsItem* items;
+  int32_t count;
+  int* status;
+};
+
+__device__ __forceinline__ void items_raise(int* status, int code) {
+  if (*reinterpret_cast<volatile int*>(status) == 0) atomicCAS(status, 0, code);
+}
+
+// Fetches item `idx` into `it`; false (status raised) when the index or the
+// descriptor is not the planned one.
+__device__ __forceinline__ bool items_fetch(const ItemsView& v, int idx, KsItem& it) {
+  if (idx < 0 || idx >= v.count) {
+    items_raise(v.status, kItemsBadIndex);
+    return false;
+  }
+  it = v.items[idx];
+  if (it.check != item_check(it)) {
+    items_raise(v.status, kItemsBadCheck);
+    return false;
+  }
+  return true;
+}
+
 // Tensor product of the HMult items (k_mul_ntt per item): grid (N / (256 V),
 // rows, HMult items), rows past an item's level return.
 template <typename T, int V>
-__global__ void k_items_mul(const KsItem* __restrict__ items, const int32_t* __restrict__ hmult, int num_q,
-                            int log_n, ChainTables<T> tabs) {
-  const KsItem it = items[hmult[blockIdx.z]];
+__global__ void k_items_mul(ItemsView iv, const int32_t* __restrict__ hmult, int num_q, int log_n,
+                            ChainTables<T> tabs) {
+  KsItem it;
+  if (!items_fetch(iv, hmult[blockIdx.z], it)) return;
+  if (it.kind != 0) {
+    items_raise(iv.status, kItemsBadKind);
+    return;
+  }
   const int limbs = num_q - it.level;
   const int row = blockIdx.y;
   const int64_t n = int64_t(1) << log_n;
@@ -74,9 +133,10 @@ __global__ void k_items_mul(const KsItem* __restrict__ items, const int32_t* __r
 // the coefficient domain (t0) for HMult, c1 through sigma_g for a rotation.
 // Grid (N / (256 V), digits, items), digits past an item's level return.
 template <typename T, int V>
-__global__ void k_items_modup(const KsItem* __restrict__ items, const LevelTables<T>* __restrict__ levels,
-                              int num_q, int log_n, ChainTables<T> tabs) {
-  const KsItem it = items[blockIdx.z];
+__global__ void k_items_modup(ItemsView iv, const LevelTables<T>* __restrict__ levels, int num_q, int log_n,
+                              ChainTables<T> tabs) {
+  KsItem it;
+  if (!items_fetch(iv, int(blockIdx.z), it)) return;
   const LevelTables<T> lt = levels[it.level];
   if (int(blockIdx.y) >= lt.num_digits) return;
   const int64_t n = int64_t(1) << log_n;
@@ -128,10 +188,11 @@ __global__ void k_items_modup(const KsItem* __restrict__ items, const LevelTable
 // leading prime (c0, c1 are already in the accumulators); rotations add
 // sigma_g(c0).  Grid (N / 256, items), one coefficient per thread.
 template <typename T>
-__global__ void k_items_moddown(const KsItem* __restrict__ items, const LevelTables<T>* __restrict__ levels,
-                                int num_q, int num_p, int log_n, ChainTables<T> tabs) {
+__global__ void k_items_moddown(ItemsView iv, const LevelTables<T>* __restrict__ levels, int num_q, int num_p,
+                                int log_n, ChainTables<T> tabs) {
   using W = Word<T>;
-  const KsItem it = items[blockIdx.y];
+  KsItem it;
+  if (!items_fetch(iv, int(blockIdx.y), it)) return;
   const int64_t n = int64_t(1) << log_n;
   const int k = int(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -199,15 +260,24 @@ __global__ void k_items_moddown(const KsItem* __restrict__ items, const LevelTab
 // NTT/Montgomery (x R), lazy [0, 2q), into the item's `ab`.
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_items_ntt_forward(const KsItem* __restrict__ items, const ItemUnit* __restrict__ units, int num_q,
-                    ChainTables<T> tabs) {
+k_items_ntt_forward(ItemsView iv, const ItemUnit* __restrict__ units, int num_q, ChainTables<T> tabs) {
   using G = NttGeom<T, LOGN>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
+  // every CTA of the cluster reads the same unit, so an early return is cluster-uniform
   const ItemUnit u = units[blockIdx.x / G::kC];
-  const KsItem it = items[u.item];
+  KsItem it;
+  if (!items_fetch(iv, u.item, it)) return;
   const int limbs = num_q - it.level;
+  if (it.kind != 0) {
+    items_raise(iv.status, kItemsBadKind);
+    return;
+  }
+  if (u.row < 0 || u.row >= 4 * limbs) {
+    items_raise(iv.status, kItemsBadRow);
+    return;
+  }
   const int op = u.row / (2 * limbs), rem = u.row - op * 2 * limbs;  // rem = component L + row
   const int pid = it.level + rem % limbs;
   const PrimeInfo<T> p = tabs.prime[pid];
@@ -226,15 +296,23 @@ k_items_ntt_forward(const KsItem* __restrict__ items, const ItemUnit* __restrict
 // into the item's t0.
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_items_ntt_inverse(const KsItem* __restrict__ items, const ItemUnit* __restrict__ units, int num_q,
-                    ChainTables<T> tabs) {
+k_items_ntt_inverse(ItemsView iv, const ItemUnit* __restrict__ units, int num_q, ChainTables<T> tabs) {
   using G = NttGeom<T, LOGN>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
   const ItemUnit u = units[blockIdx.x / G::kC];
-  const KsItem it = items[u.item];
+  KsItem it;
+  if (!items_fetch(iv, u.item, it)) return;
   const int limbs = num_q - it.level;
+  if (it.kind != 0) {
+    items_raise(iv.status, kItemsBadKind);
+    return;
+  }
+  if (u.row < 0 || u.row >= limbs) {
+    items_raise(iv.status, kItemsBadRow);
+    return;
+  }
   const int pid = it.level + u.row;
   const PrimeInfo<T> p = tabs.prime[pid];
   T v[G::kE];
@@ -250,15 +328,20 @@ k_items_ntt_inverse(const KsItem* __restrict__ items, const ItemUnit* __restrict
 // the NTT-domain ct3 is folded in (c0, c1 as P c_k, own-digit rows from c2).
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_items_core(const KsItem* __restrict__ items, const ItemUnit* __restrict__ units,
-             const LevelTables<T>* __restrict__ levels, int num_q, int num_p, ChainTables<T> tabs) {
+k_items_core(ItemsView iv, const ItemUnit* __restrict__ units, const LevelTables<T>* __restrict__ levels, int num_q,
+             int num_p, ChainTables<T> tabs) {
   using G = NttGeom<T, LOGN>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
   const ItemUnit u = units[blockIdx.x / G::kC];
-  const KsItem it = items[u.item];
+  KsItem it;
+  if (!items_fetch(iv, u.item, it)) return;
   const int level = it.level, jrow = u.row, q_limbs = num_q - level, qp0 = num_q + num_p;
+  if (jrow < 0 || jrow >= q_limbs + num_p) {
+    items_raise(iv.status, kItemsBadRow);
+    return;
+  }
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const LevelTables<T> lt = levels[level];

@@ -140,16 +140,17 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
 
 // ---- mixed-level item stages (fhb_items.cuh): one cluster per unit ----------
 template <typename T, int LOGN>
-int run_items(const Context& c, int stage, const void* items, const void* units, int64_t count, cudaStream_t st) {
-  const auto* it = static_cast<const KsItem*>(items);
+int run_items(const Context& c, int stage, const void* items, int item_count, int* status, const void* units,
+              int64_t count, cudaStream_t st) {
+  const ItemsView iv{static_cast<const KsItem*>(items), item_count, status};
   const auto* un = static_cast<const ItemUnit*>(units);
   if (stage == 0)
-    return launch_cluster<T, LOGN>(k_items_ntt_forward<T, LOGN>, count, ntt_smem<T, LOGN>(), st, it, un, c.num_q,
+    return launch_cluster<T, LOGN>(k_items_ntt_forward<T, LOGN>, count, ntt_smem<T, LOGN>(), st, iv, un, c.num_q,
                                    tables<T>(c));
   if (stage == 1)
-    return launch_cluster<T, LOGN>(k_items_ntt_inverse<T, LOGN>, count, ntt_smem<T, LOGN>(), st, it, un, c.num_q,
+    return launch_cluster<T, LOGN>(k_items_ntt_inverse<T, LOGN>, count, ntt_smem<T, LOGN>(), st, iv, un, c.num_q,
                                    tables<T>(c));
-  return launch_cluster<T, LOGN>(k_items_core<T, LOGN>, count, KsAcc<T, LOGN>::smem_bytes(), st, it, un,
+  return launch_cluster<T, LOGN>(k_items_core<T, LOGN>, count, KsAcc<T, LOGN>::smem_bytes(), st, iv, un,
                                  level_tables_dev<T>(c), c.num_q, c.num_p, tables<T>(c));
 }
 
@@ -163,7 +164,7 @@ int run_items(const Context& c, int stage, const void* items, const void* units,
   template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
                                    cudaStream_t, bool);                                                         \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
-  template int run_items<T, LOGN>(const Context&, int, const void*, const void*, int64_t, cudaStream_t);         \
+  template int run_items<T, LOGN>(const Context&, int, const void*, int, int*, const void*, int64_t, cudaStream_t); \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);
 

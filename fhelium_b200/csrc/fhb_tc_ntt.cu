@@ -147,6 +147,76 @@ __device__ __forceinline__ int raw_index(int ml, int k) {
   return ml * NK + k;
 }
 
+// Byte planes of one 128-instance tile: instance ml's input k is raw word
+// raw_index<KIND, NK>(ml, k); byte d of it goes to K position d NK + k of row
+// ml of the K-major canonical A tile.  Transposer warp tw of kTransposeWarps
+// takes every kTransposeWarps-th (8-instance group, 16-k group); a thread
+// handles (instance, 4 consecutive k), so a warp's 32 four-byte stores fall
+// in 32 distinct banks.
+template <int KIND, int NK>
+__device__ __forceinline__ void transpose_tile(const uint32_t* raw, uint8_t* at, int tw, int lane) {
+  using G = Geom<NK>;
+  const int r8 = lane >> 2, q4 = lane & 3;
+  constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);
+  for (int wu = tw; wu < kWarpUnits; wu += kTransposeWarps) {
+    const int ml = (wu % (kUnit / 8)) * 8 + r8;
+    const int k = (wu / (kUnit / 8)) * 16 + q4 * 4;
+    uint32_t v0, v1, v2, v3;
+    if (KIND == 3) {
+      const uint4 v = *reinterpret_cast<const uint4*>(raw + raw_index<KIND, NK>(ml, k));
+      v0 = v.x;
+      v1 = v.y;
+      v2 = v.z;
+      v3 = v.w;
+    } else {
+      v0 = raw[raw_index<KIND, NK>(ml, k)];
+      v1 = raw[raw_index<KIND, NK>(ml, k + 1)];
+      v2 = raw[raw_index<KIND, NK>(ml, k + 2)];
+      v3 = raw[raw_index<KIND, NK>(ml, k + 3)];
+    }
+    uint32_t w[4];
+    byte_transpose(v0, v1, v2, v3, w[0], w[1], w[2], w[3]);
+    const uint32_t rowoff = uint32_t((ml & 7) * 16 + (ml >> 3) * G::kSbo);
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+      const int kap = d * NK + k;
+      *reinterpret_cast<uint32_t*>(at + rowoff + (kap >> 4) * 128 + (kap & 15)) = w[d];
+    }
+  }
+}
+
+// kChunk outputs [c0, c0 + kChunk) of this lane's instance from the four
+// byte accumulators at TMEM address taddr + e NK (taddr = lane quarter +
+// accumulator set + c0): S = sum_e 2^{8e} acc_e < 2^49, one Montgomery
+// reduction by 2^32 (A W mod q in [0, 2q)), the twiddle tws[j] = t 2^32 mod q
+// by a second one when POST, then the canonical residue.
+template <int NK, int kChunk, bool POST>
+__device__ __forceinline__ void reduce_chunk(uint32_t taddr, const uint32_t* tws, uint32_t q, uint32_t qneg,
+                                             uint32_t (&res)[16]) {
+  uint32_t acc[4][16];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    if (kChunk == 16)
+      tmem_ld16(taddr + uint32_t(e * NK), acc[e]);
+    else
+      tmem_ld8(taddr + uint32_t(e * NK), acc[e]);
+  }
+  tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < kChunk; ++j) {
+    const uint64_t sum = uint64_t(acc[0][j]) + (uint64_t(acc[1][j]) << 8) + (uint64_t(acc[2][j]) << 16) +
+                         (uint64_t(acc[3][j]) << 24);
+    const uint32_t mm = uint32_t(sum) * qneg;
+    uint32_t r = uint32_t((sum + uint64_t(mm) * q) >> 32);  // S 2^-32 mod q, in [0, 2q)
+    if (POST) {
+      const uint64_t pr = uint64_t(r) * tws[j];  // < 2 q^2 < q 2^32
+      const uint32_t m2 = uint32_t(pr) * qneg;
+      r = uint32_t((pr + uint64_t(m2) * q) >> 32);  // r t mod q, in [0, 2q)
+    }
+    res[j] = r >= q ? r - q : r;
+  }
+}
+
 struct PassArgs {
   const uint32_t* in;
   uint32_t* out;
@@ -264,44 +334,14 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
         mbar_wait(rawf_bar(t % kRawSlots), (t / kRawSlots) & 1, nullptr, args.err, kWaitNs);
     }
   } else if (warp >= kTransposeWarp0 && warp < kTransposeWarp0 + kTransposeWarps) {
-    // raw words -> byte planes.  A thread unit = (instance, 4 consecutive k);
-    // a warp covers 8 instances x 4 k-quads (one 16-k group), so its 32
-    // four-byte stores fall in 32 distinct banks.
-    const int tw = warp - kTransposeWarp0, r8 = lane >> 2, q4 = lane & 3;
-    constexpr int kWarpUnits = (kUnit / 8) * (NK / 16);  // (8-instance group, 16-k group)
+    // raw words -> byte planes
+    const int tw = warp - kTransposeWarp0;
     for (int i = 0; i < nu; ++i) {
       const int b = i % kASlots, r = i % kRawSlots;
       if (!warp_wait(rawf_bar(r), (i / kRawSlots) & 1, abort, args.err, lane, args.wait_ns)) break;
       if (i >= kASlots && !warp_wait(ae_bar(b), ((i / kASlots) & 1) ^ 1, abort, args.err, lane, args.wait_ns))
         break;
-      const uint32_t* raw = rawbuf + r * (G::kRawBytes / 4);
-      uint8_t* at = a_tile + b * G::kABytes;
-      for (int wu = tw; wu < kWarpUnits; wu += kTransposeWarps) {
-        const int ml = (wu % (kUnit / 8)) * 8 + r8;
-        const int k = (wu / (kUnit / 8)) * 16 + q4 * 4;
-        uint32_t v0, v1, v2, v3;
-        if (KIND == 3) {
-          const uint4 v = *reinterpret_cast<const uint4*>(raw + raw_index<KIND, NK>(ml, k));
-          v0 = v.x;
-          v1 = v.y;
-          v2 = v.z;
-          v3 = v.w;
-        } else {
-          v0 = raw[raw_index<KIND, NK>(ml, k)];
-          v1 = raw[raw_index<KIND, NK>(ml, k + 1)];
-          v2 = raw[raw_index<KIND, NK>(ml, k + 2)];
-          v3 = raw[raw_index<KIND, NK>(ml, k + 3)];
-        }
-        uint32_t w[4];
-        byte_transpose(v0, v1, v2, v3, w[0], w[1], w[2], w[3]);
-        // byte (ml, kappa) of the K-major tile, kappa = d NK + k
-        const uint32_t rowoff = uint32_t((ml & 7) * 16 + (ml >> 3) * G::kSbo);
-#pragma unroll
-        for (int d = 0; d < 4; ++d) {
-          const int kap = d * NK + k;
-          *reinterpret_cast<uint32_t*>(at + rowoff + (kap >> 4) * 128 + (kap & 15)) = w[d];
-        }
-      }
+      transpose_tile<KIND, NK>(rawbuf + r * (G::kRawBytes / 4), a_tile + b * G::kABytes, tw, lane);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) {
@@ -380,29 +420,9 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
 #pragma unroll
       for (int cc = 0; cc < kHalf / kChunk; ++cc) {
         const int c0 = half * kHalf + cc * kChunk;
-        uint32_t acc[4][16];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          if (kChunk == 16)
-            tmem_ld16(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
-          else
-            tmem_ld8(tmem + lane_addr + uint32_t(b * G::kNmma + e * NK + c0), acc[e]);
-        }
-        tmem_wait_ld();
         uint32_t res[16];
-#pragma unroll
-        for (int j = 0; j < kChunk; ++j) {
-          const uint64_t sum = uint64_t(acc[0][j]) + (uint64_t(acc[1][j]) << 8) + (uint64_t(acc[2][j]) << 16) +
-                               (uint64_t(acc[3][j]) << 24);
-          const uint32_t mm = uint32_t(sum) * qneg;
-          uint32_t r = uint32_t((sum + uint64_t(mm) * q) >> 32);  // S 2^-32 mod q, in [0, 2q)
-          if (POST) {
-            const uint64_t pr = uint64_t(r) * tws[cc * kChunk + j];  // < 2 q^2 < q 2^32
-            const uint32_t m2 = uint32_t(pr) * qneg;
-            r = uint32_t((pr + uint64_t(m2) * q) >> 32);  // r t mod q, in [0, 2q)
-          }
-          res[j] = r >= q ? r - q : r;
-        }
+        reduce_chunk<NK, kChunk, POST>(tmem + lane_addr + uint32_t(b * G::kNmma + c0), tws + cc * kChunk, q, qneg,
+                                       res);
         if (S == 1) {
           uint4* o = reinterpret_cast<uint4*>(dst + c0);
 #pragma unroll
@@ -431,6 +451,366 @@ __global__ void __launch_bounds__(kThreads, Geom<NK>::kCtasPerSm) k_tc_ntt_pass(
     __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(G::kTmemCols));
+  }
+}
+
+// ------------------------------------------------ fused passes 2 and 3 ---
+// The 64-point pass over i2 (kind 2) and the 16-point pass over i3 (kind 3)
+// of the 8 consecutive 1024-word blocks 1024 P1 .. 1024 (P1 + 8) - 1 of a
+// polynomial read and write exactly those 8192 words: the kind-2 instances
+// 128 u .. 128 u + 127 and the kind-3 instances 512 u .. 512 u + 511 of unit
+// u.  So one CTA runs both passes on a unit with one HBM read and one write:
+// forward = pass 2 (kind 2, twiddled) then pass 3 (kind 3), inverse = inverse
+// pass 1 (kind 3, twiddled) then inverse pass 2 (kind 2, twiddled).  The
+// first stage's canonical outputs are written back over the unit's raw words
+// in shared memory (each output sits where its input was), and the second
+// stage transposes them from there like a raw copy.
+//
+// Roles as in k_tc_ntt_pass; per unit i (r = i % 2 raw slot):
+//   producer     copy(i) into raw slot r                    [rawf(r)]
+//   transposers  A tile of stage 1 from raw r               [af1]  (needs ae1)
+//                A tiles of stage 2 from raw r (stage-1 out) [af2, rawe(r)] (needs stg(r), ae2)
+//   MMA          stage 1 -> TMEM columns [0, 256)            [ae1, accf1] (needs af1, acce1)
+//                stage 2 -> TMEM columns [256, 512)          [ae2, accf2] (needs af2, acce2)
+//   epilogue     stage 1: reduce, twiddle -> raw r           [acce1, stg(r)] (needs accf1)
+//                stage 2: reduce (, twiddle) -> global        [acce2] (needs accf2)
+// Each role runs unit i + 1's first stage before unit i's second one, so
+// the copy of unit i + 1 and both stages overlap; single A tiles and TMEM
+// regions per stage (the two stages take all 512 columns), two raw slots.
+// Measured on B200 (64 x 36 limbs): exact, but the serial two-stage chain per
+// unit with one CTA per SM makes it slower than the two passes it replaces
+// (0.76 against 0.60 ms), so it is selected by FHB_TUNE_TC_NTT_FUSED only.
+constexpr int kFWords = 8 * 1024;                  // words of a unit
+constexpr int kFRawBytes = kFWords * 4;            // 32 KiB
+constexpr int kFUnitsPerPoly = kPolyWords / kFWords;
+constexpr int kFTiles16 = kFWords / 16 / kUnit;    // 128-instance tiles of the 16-point stage
+constexpr int kFCols = 256;                        // TMEM columns of one stage
+static_assert(Geom<64>::kABytes == kFTiles16 * Geom<16>::kABytes && Geom<64>::kNmma == kFCols &&
+                  kFTiles16 * Geom<16>::kNmma == kFCols,
+              "both stages fill one 32 KiB A area and 256 TMEM columns");
+constexpr int kFNumBarriers = 19;
+// smem: [B64 | B16 | raw 0 | raw 1 | A64 | A16 x 4 | barriers]
+constexpr int kFSmem = 1024 + Geom<64>::kBBytes + Geom<16>::kBBytes + 2 * kFRawBytes + 2 * Geom<64>::kABytes +
+                       kBarrierBytes;
+static_assert(kFSmem <= 232448 && 8 * kFNumBarriers + 8 <= kBarrierBytes, "fused pass shared memory");
+
+struct FusedArgs {
+  const uint32_t* in;
+  uint32_t* out;
+  const uint8_t* bmat64;    // [QP][64-point byte matrix] of the kind-2 stage
+  const uint8_t* bmat16;    // [QP][16-point byte matrix] of the kind-3 stage
+  const uint32_t* post1;    // [QP][N] twiddles of stage 1
+  const uint32_t* post2;    // [QP][N] twiddles of stage 2, or null
+  const uint32_t* qinfo;
+  int64_t batch;
+  int rows;
+  int row_start;
+  int ctas_per_row;
+  int* err;
+  unsigned long long wait_ns;
+  int stall;
+};
+
+// Span offset of output / input n of local instance ml of a kind-2 tile, or
+// of tile t of the kind-3 stage.
+__device__ __forceinline__ int span2(int ml, int n) { return (ml >> 4) * 1024 + n * 16 + (ml & 15); }
+__device__ __forceinline__ int span3(int t, int ml, int n) { return (t * kUnit + ml) * 16 + n; }
+
+template <bool INV>
+__global__ void __launch_bounds__(kThreads, 1) k_tc_ntt_fused(FusedArgs args) {
+  // stage 1 / stage 2 shapes: forward (kind 2, 64) then (kind 3, 16); inverse the reverse
+  constexpr int NK1 = INV ? 16 : 64, NK2 = INV ? 64 : 16;
+  constexpr bool POST2 = INV;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw0 = smem_addr(smem_raw);
+  const uint32_t base = (raw0 + 1023u) & ~1023u;
+  uint8_t* const gbase = smem_raw + (base - raw0);
+  const uint32_t b64_addr = base, b16_addr = base + Geom<64>::kBBytes;
+  const uint32_t rawbuf_addr = b16_addr + Geom<16>::kBBytes;
+  uint32_t* const rawbuf = reinterpret_cast<uint32_t*>(gbase + (rawbuf_addr - base));
+  const uint32_t a64_addr = rawbuf_addr + 2 * kFRawBytes, a16_addr = a64_addr + Geom<64>::kABytes;
+  uint8_t* const a64 = gbase + (a64_addr - base);
+  uint8_t* const a16 = gbase + (a16_addr - base);
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(gbase + (a16_addr - base) + Geom<64>::kABytes);
+  const uint32_t bar0 = smem_addr(bars);
+  // barriers: b_full, rawf[2], rawe[2], stg[2], af1, ae1, af2, ae2, accf1, acce1, accf2, acce2, never, drain
+  const uint32_t bfull_bar = bar0;
+  auto rawf_bar = [&](int r) { return bar0 + 8u * (1 + r); };
+  auto rawe_bar = [&](int r) { return bar0 + 8u * (3 + r); };
+  auto stg_bar = [&](int r) { return bar0 + 8u * (5 + r); };
+  const uint32_t af1 = bar0 + 8u * 7, ae1 = bar0 + 8u * 8, af2 = bar0 + 8u * 9, ae2 = bar0 + 8u * 10;
+  const uint32_t accf1 = bar0 + 8u * 11, acce1 = bar0 + 8u * 12, accf2 = bar0 + 8u * 13, acce2 = bar0 + 8u * 14;
+  const uint32_t never_bar = bar0 + 8u * 15, drain_bar = bar0 + 8u * 16;
+  uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + kFNumBarriers);
+  volatile int* const abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int row = blockIdx.x / args.ctas_per_row, part = blockIdx.x % args.ctas_per_row;
+  const int64_t units = args.batch * kFUnitsPerPoly;
+  const int64_t u_begin = units * part / args.ctas_per_row, u_end = units * (part + 1) / args.ctas_per_row;
+  const int nu = int(u_end - u_begin);
+  const int prime = args.row_start + row;
+  // unit i: words [unit_word(i), unit_word(i) + 8192) of the buffer
+  auto unit_word = [&](int i) {
+    const int64_t u = u_begin + i;
+    return ((u / kFUnitsPerPoly) * args.rows + row) * int64_t(kPolyWords) + (u % kFUnitsPerPoly) * kFWords;
+  };
+  auto unit_span = [&](int i) { return int((u_begin + i) % kFUnitsPerPoly) * kFWords; };  // within the polynomial
+
+  if (tid == 0) {
+    mbar_init(bfull_bar, 1);
+    for (int r = 0; r < 2; ++r) {
+      mbar_init(rawf_bar(r), 1);
+      mbar_init(rawe_bar(r), kTransposeWarps);
+      mbar_init(stg_bar(r), kEpilogueWarps);
+    }
+    mbar_init(af1, kTransposeWarps);
+    mbar_init(ae1, 1);
+    mbar_init(af2, kTransposeWarps);
+    mbar_init(ae2, 1);
+    mbar_init(accf1, 1);
+    mbar_init(acce1, kEpilogueWarps);
+    mbar_init(accf2, 1);
+    mbar_init(acce2, kEpilogueWarps);
+    mbar_init(never_bar, 1);
+    mbar_init(drain_bar, 1);
+    *abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == kMmaWarp) tmem_alloc(smem_addr(tmem_slot), 2 * kFCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kProducerWarp && lane == 0) {
+    mbar_expect_tx(bfull_bar, Geom<64>::kBBytes + Geom<16>::kBBytes);
+    const uint8_t* b64src = args.bmat64 + size_t(prime) * Geom<64>::kBBytes;
+    for (int o = 0; o < Geom<64>::kBBytes; o += 16384) bulk_load(b64_addr + o, b64src + o, 16384, bfull_bar);
+    bulk_load(b16_addr, args.bmat16 + size_t(prime) * Geom<16>::kBBytes, Geom<16>::kBBytes, bfull_bar);
+    int i = 0;
+    for (; i < nu; ++i) {
+      const int r = i & 1;
+      if (i >= 2 && !mbar_wait(rawe_bar(r), ((i >> 1) & 1) ^ 1, abort, args.err, args.wait_ns)) break;
+      const uint8_t* src = reinterpret_cast<const uint8_t*>(args.in + unit_word(i));
+      const uint32_t dst = rawbuf_addr + r * kFRawBytes;
+      mbar_expect_tx(rawf_bar(r), kFRawBytes);
+      for (int o = 0; o < kFRawBytes; o += 8192) bulk_load(dst + o, src + o, 8192, rawf_bar(r));
+    }
+    if (*abort) {
+      mbar_wait(bfull_bar, 0, nullptr, args.err, kWaitNs);
+      for (int t = i - 2 < 0 ? 0 : i - 2; t < i; ++t)
+        mbar_wait(rawf_bar(t & 1), (t >> 1) & 1, nullptr, args.err, kWaitNs);
+    }
+  } else if (warp >= kTransposeWarp0 && warp < kTransposeWarp0 + kTransposeWarps) {
+    const int tw = warp - kTransposeWarp0;
+    // stage 1 of unit i from its raw copy
+    auto stage1 = [&](int i) {
+      const int r = i & 1;
+      if (!warp_wait(rawf_bar(r), (i >> 1) & 1, abort, args.err, lane, args.wait_ns)) return false;
+      if (i >= 1 && !warp_wait(ae1, (i & 1) ^ 1, abort, args.err, lane, args.wait_ns)) return false;
+      const uint32_t* raw = rawbuf + r * kFWords;
+      if (INV) {
+#pragma unroll 1
+        for (int t = 0; t < kFTiles16; ++t)
+          transpose_tile<3, 16>(raw + t * kUnit * 16, a16 + t * Geom<16>::kABytes, tw, lane);
+      } else {
+        transpose_tile<2, 64>(raw, a64, tw, lane);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(af1);
+      return true;
+    };
+    // stage 2 of unit i from stage 1's outputs, then the raw slot is free
+    auto stage2 = [&](int i) {
+      const int r = i & 1;
+      if (!warp_wait(stg_bar(r), (i >> 1) & 1, abort, args.err, lane, args.wait_ns)) return false;
+      if (i >= 1 && !warp_wait(ae2, (i & 1) ^ 1, abort, args.err, lane, args.wait_ns)) return false;
+      const uint32_t* raw = rawbuf + r * kFWords;
+      if (INV) {
+        transpose_tile<2, 64>(raw, a64, tw, lane);
+      } else {
+#pragma unroll 1
+        for (int t = 0; t < kFTiles16; ++t)
+          transpose_tile<3, 16>(raw + t * kUnit * 16, a16 + t * Geom<16>::kABytes, tw, lane);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(af2);
+        mbar_arrive(rawe_bar(r));
+      }
+      return true;
+    };
+    bool ok = nu == 0 || stage1(0);
+    for (int i = 0; i < nu && ok; ++i) {
+      if (i + 1 < nu && !stage1(i + 1)) break;
+      ok = stage2(i);
+    }
+  } else if (warp == kMmaWarp && lane == 0) {
+    // one 64-point tile: 8 MMAs of N = 256; four 16-point tiles: 2 MMAs of N = 64 each
+    auto issue64 = [&](uint32_t d_tmem) {
+#pragma unroll
+      for (int st = 0; st < Geom<64>::kSteps; ++st)
+        mma_i8(d_tmem, smem_desc(a64_addr + st * 256, 128, Geom<64>::kSbo),
+               smem_desc(b64_addr + st * 256, 128, Geom<64>::kSbo), instr_desc(Geom<64>::kNmma), st > 0 ? 1u : 0u);
+    };
+    auto issue16 = [&](uint32_t d_tmem) {
+#pragma unroll
+      for (int t = 0; t < kFTiles16; ++t)
+#pragma unroll
+        for (int st = 0; st < Geom<16>::kSteps; ++st)
+          mma_i8(d_tmem + uint32_t(t * Geom<16>::kNmma),
+                 smem_desc(a16_addr + t * Geom<16>::kABytes + st * 256, 128, Geom<16>::kSbo),
+                 smem_desc(b16_addr + st * 256, 128, Geom<16>::kSbo), instr_desc(Geom<16>::kNmma),
+                 st > 0 ? 1u : 0u);
+    };
+    auto mma1 = [&](int i) {
+      if (!mbar_wait(af1, i & 1, abort, args.err, args.wait_ns) ||
+          (i >= 1 && !mbar_wait(acce1, (i & 1) ^ 1, abort, args.err, args.wait_ns)))
+        return false;
+      tc_fence_after();
+      if (INV)
+        issue16(tmem);
+      else
+        issue64(tmem);
+      mma_commit(ae1);
+      mma_commit(accf1);
+      return true;
+    };
+    auto mma2 = [&](int i) {
+      if (!mbar_wait(af2, i & 1, abort, args.err, args.wait_ns) ||
+          (i >= 1 && !mbar_wait(acce2, (i & 1) ^ 1, abort, args.err, args.wait_ns)))
+        return false;
+      tc_fence_after();
+      if (INV)
+        issue64(tmem + kFCols);
+      else
+        issue16(tmem + kFCols);
+      mma_commit(ae2);
+      mma_commit(accf2);
+      return true;
+    };
+    bool ok = mbar_wait(bfull_bar, 0, abort, args.err, args.wait_ns) && (nu == 0 || mma1(0));
+    for (int i = 0; i < nu && ok; ++i) {
+      if (i + 1 < nu && !mma1(i + 1)) break;
+      ok = mma2(i);
+    }
+  } else if (warp < kEpilogueWarps) {
+    const uint32_t q = args.qinfo[2 * prime], qneg = args.qinfo[2 * prime + 1];
+    const uint32_t* post1 = args.post1 + (size_t(prime) << kLogN);
+    const uint32_t* post2 = POST2 ? args.post2 + (size_t(prime) << kLogN) : nullptr;
+    const int quarter = warp & 3, half = warp >> 2;
+    const int ml = quarter * 32 + lane;
+    const uint32_t lane_addr = uint32_t(quarter * 32) << 16;
+    // this thread's 32 outputs of a stage: kind 2 -> outputs [32 half, 32 half + 32)
+    // of instance ml; kind 3 -> outputs [8 half, 8 half + 8) of instance ml of each tile
+    auto load_tw2 = [&](const uint32_t* t, int span, uint32_t (&v)[32]) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = t[span + span2(ml, half * 32 + j)];
+    };
+    auto load_tw3 = [&](const uint32_t* t, int span, uint32_t (&v)[32]) {
+#pragma unroll
+      for (int tt = 0; tt < kFTiles16; ++tt) {
+        const uint4* p = reinterpret_cast<const uint4*>(t + span + span3(tt, ml, half * 8));
+        const uint4 x = p[0], y = p[1];
+        v[8 * tt] = x.x, v[8 * tt + 1] = x.y, v[8 * tt + 2] = x.z, v[8 * tt + 3] = x.w;
+        v[8 * tt + 4] = y.x, v[8 * tt + 5] = y.y, v[8 * tt + 6] = y.z, v[8 * tt + 7] = y.w;
+      }
+    };
+    auto epi1 = [&](int i) {
+      const int r = i & 1;
+      uint32_t tws[32];
+      if (INV)
+        load_tw3(post1, unit_span(i), tws);
+      else
+        load_tw2(post1, unit_span(i), tws);
+      if (!warp_wait(accf1, i & 1, abort, args.err, lane, args.wait_ns)) return false;
+      tc_fence_after();
+      uint32_t* stage = rawbuf + r * kFWords;  // outputs over the unit's raw words
+      if (INV) {
+#pragma unroll
+        for (int tt = 0; tt < kFTiles16; ++tt) {
+          uint32_t res[16];
+          reduce_chunk<16, 8, true>(tmem + lane_addr + uint32_t(tt * Geom<16>::kNmma + half * 8), tws + 8 * tt, q,
+                                    qneg, res);
+          uint4* o = reinterpret_cast<uint4*>(stage + span3(tt, ml, half * 8));
+          o[0] = make_uint4(res[0], res[1], res[2], res[3]);
+          o[1] = make_uint4(res[4], res[5], res[6], res[7]);
+        }
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int c0 = half * 32 + cc * 16;
+          uint32_t res[16];
+          reduce_chunk<64, 16, true>(tmem + lane_addr + uint32_t(c0), tws + 16 * cc, q, qneg, res);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) stage[span2(ml, c0 + j)] = res[j];
+        }
+      }
+      // the slot is overwritten by a bulk copy (async proxy) once stage 2 has read it
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(acce1);
+        mbar_arrive(stg_bar(r));
+      }
+      return true;
+    };
+    auto epi2 = [&](int i) {
+      uint32_t tws[32];
+      if (POST2) load_tw2(post2, unit_span(i), tws);
+      if (!warp_wait(accf2, i & 1, abort, args.err, lane, args.wait_ns)) return false;
+      tc_fence_after();
+      uint32_t* dst = args.out + unit_word(i);
+      if (INV) {
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          const int c0 = half * 32 + cc * 16;
+          uint32_t res[16];
+          reduce_chunk<64, 16, POST2>(tmem + kFCols + lane_addr + uint32_t(c0), tws + 16 * cc, q, qneg, res);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) dst[span2(ml, c0 + j)] = res[j];
+        }
+      } else {
+#pragma unroll
+        for (int tt = 0; tt < kFTiles16; ++tt) {
+          uint32_t res[16];
+          reduce_chunk<16, 8, false>(tmem + kFCols + lane_addr + uint32_t(tt * Geom<16>::kNmma + half * 8), tws, q,
+                                     qneg, res);
+          uint4* o = reinterpret_cast<uint4*>(dst + span3(tt, ml, half * 8));
+          o[0] = make_uint4(res[0], res[1], res[2], res[3]);
+          o[1] = make_uint4(res[4], res[5], res[6], res[7]);
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce2);
+      return true;
+    };
+    // test only: a wait that must run out (its limit is the pipeline's)
+    const bool stalled = args.stall && !warp_wait(never_bar, 0, abort, args.err, lane, args.wait_ns);
+    bool ok = !stalled && (nu == 0 || epi1(0));
+    for (int i = 0; i < nu && ok; ++i) {
+      if (i + 1 < nu && !epi1(i + 1)) break;
+      ok = epi2(i);
+    }
+  }
+
+  __syncthreads();
+  if (warp == kMmaWarp && lane == 0) {
+    mma_commit(drain_bar);
+    mbar_wait(drain_bar, 0, nullptr, args.err, kWaitNs);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == kMmaWarp) {
+    __syncwarp();
+    tc_fence_after();
+    tmem_dealloc(tmem, 2 * kFCols);
   }
 }
 
@@ -614,17 +994,46 @@ int launch_pass(const Context& c, const uint32_t* in, uint32_t* out, int pass, i
   kern<<<dim3(unsigned(rows * per_row)), kThreads, smem, st>>>(a);
   return cuda_status(cudaGetLastError(), "k_tc_ntt_pass");
 }
+
+template <bool INV>
+int launch_fused(const Context& c, const uint32_t* in, uint32_t* out, int64_t polys, int rows, int row_start,
+                 cudaStream_t st) {
+  using namespace tcntt;
+  auto kern = k_tc_ntt_fused<INV>;
+  if (int rc = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), kFSmem)) return rc;
+  // persistent CTAs, one per SM (all of its TMEM), each streaming units of one prime
+  const int64_t batch = polys / rows;
+  const int64_t units = batch * kFUnitsPerPoly;
+  int64_t per_row = 148 / rows;
+  if (per_row > units) per_row = units;
+  if (per_row < 1) per_row = 1;
+  // forward: pass 2 (table 1, twiddled) + pass 3 (table 2); inverse: table 3 (twiddled) + table 4 (twiddled)
+  const int p64 = INV ? 4 : 1, p16 = INV ? 3 : 2;
+  FusedArgs a{in, out, c.tc->bmat[p64], c.tc->bmat[p16], c.tc->post[INV ? 3 : 1], INV ? c.tc->post[4] : nullptr,
+              c.tc->qinfo, batch, rows, row_start, int(per_row), c.tc->err, c.tc_wait_ns ? c.tc_wait_ns : kWaitNs,
+              c.tc_test_stall};
+  kern<<<dim3(unsigned(rows * per_row)), kThreads, kFSmem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "k_tc_ntt_fused");
+}
 }  // namespace
 
-// The three passes of a direction; passes after the first run in place on
-// `out` (every unit writes exactly the words its raw copy read, after the
-// copy landed), so in == out is allowed and no scratch is needed.
+// The passes of a direction; passes after the first run in place on `out`
+// (every unit writes exactly the words its raw copy read, after the copy
+// landed), so in == out is allowed and no scratch is needed.
 int tc_ntt(Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool inverse,
            cudaStream_t st) {
   if (int rc = tc_ntt_prepare(c)) return rc;
   if (polys == 0) return 0;
   const auto* x = static_cast<const uint32_t*>(in);
   auto* y = static_cast<uint32_t*>(out);
+  if (c.tc_ntt_fused) {
+    if (!inverse) {
+      if (int rc = launch_pass<1, 64, true>(c, x, y, 0, polys, rows, row_start, st)) return rc;
+      return launch_fused<false>(c, y, y, polys, rows, row_start, st);
+    }
+    if (int rc = launch_fused<true>(c, x, y, polys, rows, row_start, st)) return rc;
+    return launch_pass<1, 64, false>(c, y, y, 5, polys, rows, row_start, st);
+  }
   if (!inverse) {
     if (int rc = launch_pass<1, 64, true>(c, x, y, 0, polys, rows, row_start, st)) return rc;
     if (int rc = launch_pass<2, 64, true>(c, y, y, 1, polys, rows, row_start, st)) return rc;

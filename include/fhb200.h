@@ -91,6 +91,9 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * FHB_TUNE_TC_MODDOWN (with the tensor-core form): 1 = ModDown's P -> Q
  * conversion on the tensor cores too, 0 = on the CUDA cores (default: faster
  * on B200).
+ * FHB_TUNE_TC_NTT_FUSED: fhb_tc_forward_ntt / fhb_tc_inverse_ntt in two
+ * launches, the 16-point pass fused with the adjacent 64-point pass over each
+ * 8192-word span (1), or in three (0, default: faster on B200).
  * Results do not depend on any of these (stall aside).  No counterpart in the reference
  * (its launch shapes and arithmetic units are fixed). */
 enum fhb_tuning_param {
@@ -100,7 +103,8 @@ enum fhb_tuning_param {
   FHB_TUNE_BASIS_CONVERSION = 3,
   FHB_TUNE_TC_WAIT_US = 4,
   FHB_TUNE_TC_TEST_STALL = 5,
-  FHB_TUNE_TC_MODDOWN = 6
+  FHB_TUNE_TC_MODDOWN = 6,
+  FHB_TUNE_TC_NTT_FUSED = 7
 };
 int fhb_context_set_tuning(fhb_context* ctx, int param, int value);
 int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);
@@ -402,6 +406,15 @@ int fhb_ckks_items_plan_info(const fhb_context* ctx, const fhb_ks_item* items, i
 int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int count, void* plan, void* scratch,
                         const fhb_items_plan_info* info);
 int fhb_ckks_items_run(const fhb_context* ctx, const void* plan, const fhb_items_plan_info* info, fhb_stream stream);
+/* Status word of the runs of a plan since the last read: 0, or the first
+ * error a kernel raised (1: a work list names an item outside the plan; 2: a
+ * device descriptor no longer matches the check word the planner stored
+ * with it; 3: a work-list row outside its item's rows; 4: the HMult list
+ * names a rotation).  Every kernel verifies the item it is about to use, so
+ * a plan changed in device memory after planning makes the affected items
+ * skip their work instead of addressing memory through it.  Reads with a
+ * blocking copy (call after the runs have completed) and resets the word. */
+int fhb_ckks_items_status(const fhb_context* ctx, void* plan, const fhb_items_plan_info* info, int* status);
 
 /* Bounded decryption to float64 coefficients: phase [batch, L, N]
  * coefficient/standard canonical (c0 + c1 s) -> out [batch, N] float64 (a

@@ -79,6 +79,34 @@ def test_items_chunked(small):
         assert torch.equal(ex.result(i).data, w.data), f"op {i} ({ops[i]}) differs"
 
 
+def test_items_detect_a_changed_descriptor(small):
+    """A descriptor changed in device memory after planning no longer
+    matches its check word: every kernel skips that item and the run reports
+    status 2; the other items are exact, and restoring the descriptor
+    restores the item."""
+    eng, cts, ops, want = small
+    ex = MixedItemsExecutor(eng, cts, ops, use_graph=False)
+    ex.run()
+    assert ex.status() == 0
+    _, plan = ex.chunks[0]
+    victim = ex.chunk_ops[0][0]
+    # the device descriptors open the plan, 88 bytes each; bytes 4..7 of the first hold its level
+    level = plan[4:8].clone()
+    plan[4:8] = (level.view(torch.int32) + 1).view(torch.uint8)
+    ex._outs[victim].zero_()
+    ex.run()
+    assert ex.status() == 2
+    assert ex.status() == 0  # reading resets the word
+    assert not ex._outs[victim].any()  # the changed item did no work
+    for i, w in enumerate(want):
+        if i != victim:
+            assert torch.equal(ex.result(i).data, w.data), f"op {i} ({ops[i]}) differs"
+    plan[4:8] = level
+    ex.run()
+    assert ex.status() == 0
+    assert torch.equal(ex.result(victim).data, want[victim].data)
+
+
 def test_items_inputs_updated_between_replays(small):
     eng, cts, ops, _ = small
     mine = [c.clone() for c in cts]

@@ -28,6 +28,16 @@ def ctx():
     c.close()
 
 
+@pytest.fixture(params=[1, 0], ids=["fused", "three_pass"])
+def form(request, ctx):
+    """Both launch forms: the 16-point pass fused with the adjacent 64-point
+    pass (two launches per direction), and three separate passes."""
+    c, _ = ctx
+    c.set_tuning(nat.TUNE_TC_NTT_FUSED, request.param)
+    yield request.param
+    c.set_tuning(nat.TUNE_TC_NTT_FUSED, 0)
+
+
 def _inputs(primes, batch, rows, row_start, seed):
     g = torch.Generator(device="cuda:0")
     g.manual_seed(seed)
@@ -57,7 +67,7 @@ def _plain(c, x, batch, rows, row_start):
 
 
 @pytest.mark.parametrize("batch,rows,row_start", [(2, 36, 0), (3, 5, 3), (1, 1, 35)])
-def test_tensor_core_ntt_matches_cuda_core(ctx, batch, rows, row_start):
+def test_tensor_core_ntt_matches_cuda_core(ctx, form, batch, rows, row_start):
     c, primes = ctx
     x, q = _inputs(primes, batch, rows, row_start, seed=1 + row_start)
     y_plain, z_plain = _plain(c, x, batch, rows, row_start)
@@ -76,7 +86,7 @@ def test_tensor_core_ntt_matches_cuda_core(ctx, batch, rows, row_start):
     assert _status(c) == 0
 
 
-def test_tensor_core_ntt_in_place_and_empty(ctx):
+def test_tensor_core_ntt_in_place_and_empty(ctx, form):
     c, primes = ctx
     x, _ = _inputs(primes, 2, 36, 0, seed=5)
     y = torch.empty_like(x)
@@ -90,7 +100,7 @@ def test_tensor_core_ntt_in_place_and_empty(ctx):
     assert _status(c) == 0
 
 
-def test_tensor_core_ntt_full_workload_round_trip(ctx):
+def test_tensor_core_ntt_full_workload_round_trip(ctx, form):
     """Batch 64 x 36 limbs: round trip exact and forward equal mod q to the
     CUDA-core form over the whole tensor."""
     c, primes = ctx

@@ -52,10 +52,14 @@ def test_tc_ntt_wait_runs_out_then_next_call_is_exact():
     y = torch.empty_like(x)
     assert _status(ctx, "fhb_tc_ntt_status") == 0
     _stalled(ctx, True)
-    nat.check(ctx.lib.fhb_tc_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), 1, 1, 0, s), "stalled forward")
-    torch.cuda.synchronize()  # no CUDA error: the kernel returned
-    assert _status(ctx, "fhb_tc_ntt_status") == 1
-    assert _status(ctx, "fhb_tc_ntt_status") == 0  # read clears it
+    for fused in (1, 0):  # the fused-pass kernel and the separate passes
+        ctx.set_tuning(nat.TUNE_TC_NTT_FUSED, fused)
+        for fn in ("fhb_tc_forward_ntt", "fhb_tc_inverse_ntt"):
+            nat.check(getattr(ctx.lib, fn)(ctx.handle, x.data_ptr(), y.data_ptr(), 1, 1, 0, s), "stalled " + fn)
+            torch.cuda.synchronize()  # no CUDA error: the kernels returned
+            assert _status(ctx, "fhb_tc_ntt_status") == 1
+            assert _status(ctx, "fhb_tc_ntt_status") == 0  # read clears it
+    ctx.set_tuning(nat.TUNE_TC_NTT_FUSED, 0)
     _stalled(ctx, False)
     nat.check(ctx.lib.fhb_tc_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), 1, 1, 0, s), "forward")
     plain = torch.empty_like(x)
