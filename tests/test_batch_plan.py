@@ -50,7 +50,15 @@ def test_cache_round_trip(tmp_path):
 
 
 def test_streaming_chunks_cover_the_batch():
-    from fhelium_b200.streaming import _chunks
+    from fhelium_b200.streaming import _chunks, tapered
     assert _chunks(7, 3) == [(0, 3), (3, 5), (5, 7)]
     assert _chunks(2, 5) == [(0, 1), (1, 2)]
     assert _chunks(32, 4) == [(0, 8), (8, 16), (16, 24), (24, 32)]
+    assert _chunks(5, [2, 2, 1]) == [(0, 2), (2, 4), (4, 5)]
+    for bad in ([2, 2], [3, 0, 2], []):
+        with pytest.raises(ValueError):
+            _chunks(5, bad)
+    assert tapered(32, 2, 4) == [2] * 14 + [1] * 4
+    assert tapered(7, 4, 2) == [4, 1, 1, 1]
+    assert tapered(3, 2, 5) == [1, 1, 1]
+    assert sum(tapered(33, 4, 3)) == 33
