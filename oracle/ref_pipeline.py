@@ -29,10 +29,24 @@ from .oracle import OracleContext
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libfhelium_ref_cpu_ops.so")
+# the same schemas with the reference's CUDA kernels too (build_ref_cuda.sh)
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libfhelium_ref_ops_cuda.so")
+_loaded: list[str] = []
 
 
-def available() -> bool:
-    return os.path.exists(REF_LIB)
+def available(library: str = "cpu") -> bool:
+    return os.path.exists(REF_CUDA_LIB if library == "cuda" else REF_LIB)
+
+
+def _load(library: str) -> None:
+    """Loads one of the two reference libraries once per process; they define
+    the same schemas, so a process holds only one."""
+    path = REF_CUDA_LIB if library == "cuda" else REF_LIB
+    if _loaded and _loaded[0] != path:
+        raise RuntimeError(f"{os.path.basename(_loaded[0])} is already loaded in this process")
+    if not _loaded:
+        torch.ops.load_library(path)
+        _loaded.append(path)
 
 
 def _schedule(log_n: int):
@@ -60,15 +74,25 @@ class ReferenceCpuPipeline:
     """The reference engine's operator sequence.  On "cpu" it runs the
     reference's own CPU operators (oracle/_ref, required).  With a CUDA
     `device` the same calls dispatch to whatever CUDA kernels are registered
-    for the reference's schemas (the reference's library is loaded first when
-    present, so that its schema definitions are the ones in use)."""
+    for the reference's schemas: with library="cpu" the reference's CPU
+    library is loaded first when present (its schema definitions are the ones
+    in use, another library registers the CUDA kernels), with
+    library="cuda" the reference's own CUDA kernels (build_ref_cuda.sh).
+    ntt="compact" uses the reference's default CUDA transform policy
+    (radix2_compact_group8_smem8: grouped radix-2 stages, three per launch,
+    fhelium/config/ntt.py:87-126) instead of the indexed radix-2 form its
+    CPU backend implements."""
 
-    def __init__(self, ctx: OracleContext, threads: int | None = None, device: str | torch.device = "cpu"):
+    def __init__(self, ctx: OracleContext, threads: int | None = None, device: str | torch.device = "cpu",
+                 library: str = "cpu", ntt: str = "indexed"):
         device = torch.device(device)
-        if device.type == "cpu" and not available():
-            raise FileNotFoundError(REF_LIB)
-        if available():
-            torch.ops.load_library(REF_LIB)
+        if (device.type == "cpu" or library == "cuda") and not available(library):
+            raise FileNotFoundError(REF_CUDA_LIB if library == "cuda" else REF_LIB)
+        if available(library):
+            _load(library)
+        if ntt not in ("indexed", "compact"):
+            raise ValueError("ntt must be 'indexed' or 'compact'")
+        self.compact = ntt == "compact"
         if threads:
             torch.set_num_threads(threads)
         self.ctx = ctx
@@ -81,6 +105,7 @@ class ReferenceCpuPipeline:
         self.fe, self.fo, self.ie, self.io = (x.to(device) for x in (fe, fo, ie, io))
         self.fwd_stage = t(np.stack([fwd[j][ft] for j in range(len(ctx.moduli))]))
         self.inv_stage = t(np.stack([inv[j][it] for j in range(len(ctx.moduli))]))
+        self.fwd_compact, self.inv_compact = t(fwd), t(inv)
         self._t = t
         self.rns = torch.ops.fhelium_rns_ops
         self.ntt = torch.ops.fhelium_ntt_ops
@@ -91,10 +116,20 @@ class ReferenceCpuPipeline:
         return self.params[:, start:stop]
 
     def _inverse_to_standard_(self, x, start, stop):
-        self.ntt.inverse_ntt_to_standard_indexed_(x, self.ie, self.io, self.inv_stage[start:stop], self._p(start, stop))
+        if self.compact:
+            self.ntt.inverse_ntt_to_standard_compact_grouped_smem_(x, self.inv_compact[start:stop],
+                                                                   self._p(start, stop), 3)
+        else:
+            self.ntt.inverse_ntt_to_standard_indexed_(x, self.ie, self.io, self.inv_stage[start:stop],
+                                                      self._p(start, stop))
 
     def _forward_montgomery_(self, x, start, stop):
-        self.ntt.forward_ntt_montgomery_indexed_(x, self.fe, self.fo, self.fwd_stage[start:stop], self._p(start, stop))
+        if self.compact:
+            self.ntt.forward_ntt_montgomery_compact_grouped_smem_(x, self.fwd_compact[start:stop],
+                                                                  self._p(start, stop), 3)
+        else:
+            self.ntt.forward_ntt_montgomery_indexed_(x, self.fe, self.fo, self.fwd_stage[start:stop],
+                                                     self._p(start, stop))
 
     def _digit_args(self, level, ids):
         key = (level, ids)
