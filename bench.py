@@ -19,6 +19,9 @@ relinearisation key and rescaled - the whole batch per step.
   cpu_baseline  the reference's own CPU operators (compiled from its sources
               into oracle/_ref) driven in the reference engine's order, on a
               bounded sample (a few ciphertexts) with all host threads.
+  gpu_baseline  the reference's own CUDA kernels (compiled from its sources
+              for sm_100a into oracle/_ref) driven in the same order on this
+              GPU, on the whole batch, in a child process.
 
 Multi-GPU (torchrun): every rank runs the same per-GPU batch on its own
 ciphertexts (independent objects, no collective on the data path);
@@ -498,8 +501,7 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
     from the autotuner), and the per-ciphertext loop itself.  The rotation
     keys (one per distinct step, about 0.4 GB each) dominate the memory."""
     from fhelium_b200 import autotune
-    from fhelium_b200.batch import (HMULT, MixedBatchExecutor, MixedItemsExecutor, run_per_ciphertext,
-                                    sample_mixed_workload)
+    from fhelium_b200.batch import HMULT, MixedBatchExecutor, run_per_ciphertext, sample_mixed_workload
     from fhelium_b200.engine import CkksEngine
     eng = CkksEngine(PRESET, device=dev, rng_seed=9)
     levels, ops = sample_mixed_workload(eng.num_q, count, seed=0)
@@ -519,7 +521,7 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
         return bad
 
     # one executor alive at a time: the keys leave little room for two
-    items = MixedItemsExecutor(eng, cts, ops)
+    items, items_tune = autotune.tune_items(eng, cts, ops, limits=(4 << 30, 8 << 30))
     items.run()
     torch.cuda.synchronize(dev)
     items_ms = _time_events(items.run, max(3, steps), stream)
@@ -553,6 +555,8 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
            "basis_conversion": eng.basis_conversion,
            "items_ms": items_ms, "items_ops_per_s": count / (items_ms / 1e3), "items_chunks": item_chunks,
            "items_library_launches_per_pass": item_launches,
+           "items_autotune": {"ks_order": items_tune["ks_order"], "max_scratch_bytes": items_tune["max_scratch_bytes"],
+                              "cached": items_tune["cached"], "candidates": items_tune.get("candidates")},
            "groups": groups, "library_launches_per_pass": group_launches,
            "batched_graph_ms": batched_ms, "batched_ops_per_s": count / (batched_ms / 1e3),
            "per_ciphertext_ms": loop_ms, "per_ciphertext_ops_per_s": count / (loop_ms / 1e3),
@@ -564,6 +568,29 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
     del cts, eng
     torch.cuda.empty_cache()
     return out
+
+
+def gpu_reference_sample(batch: int, steps: int = 5):
+    """The reference's own CUDA kernels (oracle/_ref, built from its sources
+    for sm_100a) running its engine's HMult -> relinearize -> rescale
+    operator sequence on the same GPU, batch `batch` at level 0 of the
+    headline preset, timed with CUDA events.  A child process: that library
+    defines the reference's operator schemas itself."""
+    import subprocess
+    from oracle.ref_pipeline import available
+    if not available("cuda"):
+        return None
+    cmd = [sys.executable, "-m", "oracle.ref_cuda", "--batch", str(batch), "--steps", str(steps), "--arbiter", "0"]
+    res = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=900)
+    if res.returncode != 0:
+        return {"error": res.stderr.strip().splitlines()[-1][:300] if res.stderr.strip() else "failed"}
+    line = json.loads(res.stdout.strip().splitlines()[-1])
+    return {"value": line["reference_cuda_ops_per_s"], "unit": UNIT, "kind": "reference",
+            "ms_per_step": line["reference_cuda_ms"],
+            "sample": f"its engine's operator sequence through its CUDA kernels ({line['reference_ntt_policy']} NTT), "
+                      f"batch {batch}, level 0, same GPU; this library in the same process: "
+                      f"{line['ours_tensor_cores_ops_per_s']:.1f} ops/s",
+            "ciphertexts_equal": batch - len(line["mismatching_ciphertexts"]), "batch": batch}
 
 
 def cpu_reference_sample(n_ops: int, threads: int, level: int = 0):
@@ -903,6 +930,11 @@ def main() -> int:
         leg("ntt_int32_logN16_36limbs_batch64", lambda: ntt_leg(dev, stream, args.steps))
         leg("bootstrap_logN16_batch8", lambda: bootstrap_leg(dev, stream))
         if args.mixed_count > 0:
+            # the mixed leg holds ~95 GB of rotation keys of its own: the
+            # headline engine's rotation keys (earlier legs only) go first
+            for step in list(eng.rotation_keys):
+                del eng.rotation_keys[step]
+            torch.cuda.empty_cache()
             leg("mixed_level_batch", lambda: mixed_batch_leg(dev, stream, args.mixed_count, args.steps))
         # decrypted error of the product (first ciphertext)
         dec = eng.decrypt_message(Ciphertext(state["out"].data[:, :1].contiguous(), 1, state["out"].scale),
@@ -920,11 +952,17 @@ def main() -> int:
         except Exception as exc:  # report, never hide
             extras["bit_exact_vs_reference_cpu"] = f"error: {exc}"
 
-    cpu = None
+    cpu = gpu_base = None
     if rank == 0 and ws == 1 and not args.no_extras:
         threads = os.cpu_count() or 1
         v, kind, cores, sample = cpu_reference_sample(2, threads)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        eng._scratch = None
+        torch.cuda.empty_cache()
+        try:
+            gpu_base = gpu_reference_sample(B)
+        except Exception as exc:  # report, never hide
+            gpu_base = {"error": f"{type(exc).__name__}: {str(exc)[:300]}"}
 
     csum = clocks.summary()
     line = {
@@ -954,6 +992,7 @@ def main() -> int:
         "step_algorithmic_gbs": step_bytes / (ms / 1000.0) / 1e9,
         "clocks": csum,
         "cpu_baseline": cpu,
+        "gpu_baseline": gpu_base,
         "extras": extras,
     }
     if rank == 0:

@@ -11,6 +11,11 @@ The knobs a run can change without recompiling:
   and the group's digits stay in L2);
 * ``streams``: how many graph branches the mixed-batch executor spreads its
   (kind, level) groups over, i.e. how many groups run side by side;
+* for the descriptor-driven mixed batch (``MixedItemsExecutor``): the
+  key-switch work order inside each (level, key) group of items (0 = the
+  rows of one item back to back, 2 = one row across the group) and the
+  scratch limit of a chunk of items (fewer, larger chunks launch fewer
+  times but hold more scratch);
 * ``ntt_forward_ept`` / ``ntt_inverse_ept`` (FHB_TUNE_NTT_{FORWARD,INVERSE}_EPT):
   residues per thread of the standalone transforms, i.e. the NTT's register
   radix and tile: 8 residues (radix-8 passes, 1024 threads per CTA at
@@ -156,3 +161,45 @@ def tune_mixed_batch(engine, executor, *, ks_orders: Iterable[int] = (0, 1, 2), 
     entry = dict(best, candidates=results)
     _store(cache_path, key, entry)
     return dict(entry, cached=False)
+
+
+def items_workload_key(engine, ciphertexts, ops) -> str:
+    """Device + ring + chain + the multiset of (kind, level) items."""
+    shape = sorted((op.kind, ciphertexts[op.index].level) for op in ops)
+    digest = hashlib.sha256(json.dumps(shape).encode()).hexdigest()[:16]
+    chain = hashlib.sha256(json.dumps([int(m) for m in engine.moduli]).encode()).hexdigest()[:12]
+    dev = torch.cuda.get_device_name(engine.device)
+    return f"{dev}|logN={engine.log_n}|q={engine.num_q}|p={engine.num_p}|chain={chain}|items={digest}"
+
+
+def tune_items(engine, ciphertexts, ops, *, ks_orders: Iterable[int] = (0, 2),
+               limits: Iterable[int] = (4 << 30, 8 << 30, 16 << 30), repeats: int = 3,
+               cache_path: str | None = None, use_cache: bool = True):
+    """Pick (ks_order, max_scratch_bytes) of a MixedItemsExecutor for this
+    batch by timing graph replays of each candidate (built one at a time).
+    Returns ``(executor, entry)``: the executor built with the winner and
+    ``{"ks_order", "max_scratch_bytes", "ms", "candidates", "cached"}``."""
+    from .batch import MixedItemsExecutor
+    cache_path = cache_path or default_cache_path()
+    key = items_workload_key(engine, ciphertexts, ops)
+    if use_cache:
+        hit = _load(cache_path).get(key)
+        if hit and {"ks_order", "max_scratch_bytes"} <= set(hit):
+            ex = MixedItemsExecutor(engine, ciphertexts, ops, ks_order=int(hit["ks_order"]),
+                                    max_scratch_bytes=int(hit["max_scratch_bytes"]))
+            return ex, dict(hit, cached=True)
+    results = []
+    for order in ks_orders:
+        for limit in limits:
+            ex = MixedItemsExecutor(engine, ciphertexts, ops, ks_order=int(order), max_scratch_bytes=int(limit))
+            ms = time_replays(ex.run, engine.device, repeats=repeats)
+            results.append({"ks_order": int(order), "max_scratch_bytes": int(limit), "chunks": len(ex.chunks),
+                            "ms": ms})
+            del ex
+            torch.cuda.empty_cache()
+    best = min(results, key=lambda r: r["ms"])
+    entry = dict(best, candidates=results)
+    _store(cache_path, key, entry)
+    ex = MixedItemsExecutor(engine, ciphertexts, ops, ks_order=best["ks_order"],
+                            max_scratch_bytes=best["max_scratch_bytes"])
+    return ex, dict(entry, cached=False)

@@ -286,11 +286,13 @@ class MixedItemsExecutor:
     """
 
     def __init__(self, engine, ciphertexts: Sequence[Ciphertext], ops: Sequence[MixedOp], *,
-                 use_graph: bool = True, max_scratch_bytes: int = 8 << 30):
+                 use_graph: bool = True, max_scratch_bytes: int = 8 << 30, ks_order: int | None = None):
         self.engine = engine
         self.cts = list(ciphertexts)
         self.ops = list(ops)
         self.use_graph = use_graph
+        self.max_scratch_bytes = int(max_scratch_bytes)
+        self.ks_order = ks_order
         _validate(engine, self.cts, self.ops)
         eng = engine
         self._copies: set[int] = set()
@@ -353,11 +355,18 @@ class MixedItemsExecutor:
         infos = [plan_info(part) for part in parts]
         self.scratch = torch.empty(max(max(int(i.scratch_bytes) for i in infos), 16), dtype=torch.uint8,
                                    device=eng.device)
-        for part, info in zip(parts, infos):
-            plan = torch.empty(max(int(info.plan_bytes), 16), dtype=torch.uint8, device=eng.device)
-            ctx.call("fhb_ckks_items_plan", (nat.KsItem * len(part))(*part), len(part), nat.ptr(plan),
-                     nat.ptr(self.scratch), ctypes.byref(info))
-            self.chunks.append((info, plan))
+        # the plans' key-switch work lists follow the context's work order
+        keep = ctx.get_tuning(nat.TUNE_KS_ORDER)
+        if ks_order is not None:
+            ctx.set_tuning(nat.TUNE_KS_ORDER, int(ks_order))
+        try:
+            for part, info in zip(parts, infos):
+                plan = torch.empty(max(int(info.plan_bytes), 16), dtype=torch.uint8, device=eng.device)
+                ctx.call("fhb_ckks_items_plan", (nat.KsItem * len(part))(*part), len(part), nat.ptr(plan),
+                         nat.ptr(self.scratch), ctypes.byref(info))
+                self.chunks.append((info, plan))
+        finally:
+            ctx.set_tuning(nat.TUNE_KS_ORDER, keep)
 
     def _issue(self) -> None:
         eng = self.engine

@@ -212,9 +212,11 @@ int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int co
     d.check = fhb::item_check(d);
     dev_items[i] = d;
   }
-  // Core work list: items of one (level, key) back to back, and within such
-  // a group one destination row across the group's items, so concurrently
-  // resident clusters share key rows in L2.
+  // Core work list: items of one (level, key) back to back; within such a
+  // group, the context's key-switch work order picks one destination row
+  // across the group's items (orders 1 and 2: concurrently resident
+  // clusters share key rows in L2) or the rows of one item back to back
+  // (order 0: an item's digit rows stay in L2).
   std::vector<int> order(count);
   for (int i = 0; i < count; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
@@ -228,8 +230,13 @@ int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int co
            items[order[g1]].key == items[order[g0]].key)
       ++g1;
     const int lp = c.num_q - items[order[g0]].level + c.num_p;
-    for (int r = 0; r < lp; ++r)
-      for (size_t k = g0; k < g1; ++k) core[nc++] = fhb::ItemUnit{order[k], r};
+    if (c.ks_order == 0) {
+      for (size_t k = g0; k < g1; ++k)
+        for (int r = 0; r < lp; ++r) core[nc++] = fhb::ItemUnit{order[k], r};
+    } else {
+      for (int r = 0; r < lp; ++r)
+        for (size_t k = g0; k < g1; ++k) core[nc++] = fhb::ItemUnit{order[k], r};
+    }
     g0 = g1;
   }
   fhb::ItemsDeviceGuard guard(c.device);

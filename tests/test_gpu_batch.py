@@ -63,6 +63,28 @@ def test_items_bit_exact(small, use_graph):
         assert torch.equal(got.data, w.data), f"op {i} ({ops[i]}) differs"
 
 
+def test_items_work_orders_and_autotune(small, tmp_path):
+    """Both key-switch work orders of the items plan give the same residues;
+    the autotuner picks among (order, scratch limit) and caches the winner."""
+    eng, cts, ops, want = small
+    for order in (0, 2):
+        ex = MixedItemsExecutor(eng, cts, ops, ks_order=order)
+        ex.run()
+        torch.cuda.synchronize()
+        for i, w in enumerate(want):
+            assert torch.equal(ex.result(i).data, w.data), (order, i)
+    path = str(tmp_path / "tune.json")
+    ex, first = autotune.tune_items(eng, cts, ops, limits=(1 << 28, 1 << 34), repeats=1, cache_path=path)
+    assert not first["cached"] and len(first["candidates"]) == 4
+    assert (ex.ks_order, ex.max_scratch_bytes) == (first["ks_order"], first["max_scratch_bytes"])
+    _, second = autotune.tune_items(eng, cts, ops, cache_path=path)
+    assert second["cached"] and second["ks_order"] == first["ks_order"]
+    ex.run()
+    torch.cuda.synchronize()
+    for i, w in enumerate(want):
+        assert torch.equal(ex.result(i).data, w.data)
+
+
 def test_items_chunked(small):
     """A scratch limit below the batch's need splits it into chunks that
     share one scratch, in stream order; the residues do not change."""
