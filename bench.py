@@ -55,6 +55,8 @@ KS_TRAFFIC_BYTES_BATCH32 = 12741399552 + 2934590720  # ncu dram read + write, k_
 # same for the key-switch core of the tensor-core form: captured at batch 8 (3094038784 + 705889536 bytes,
 # 2.01x the batch-4 capture) and scaled by the ciphertexts processed
 KS_EXT_TRAFFIC_BYTES_BATCH32 = 4 * (3094038784 + 705889536)
+# same for the FP64 form of that core (Q rows) with its P-row launch (not yet captured)
+KS_F64_TRAFFIC_BYTES_BATCH32 = None
 METRIC = "hmult_relin_rescale_ops_per_s_logN16_L35"
 UNIT = "ops/s"
 CONFIG = {
@@ -473,7 +475,8 @@ def forms_leg(eng, ca, cb, rlk, stream, steps=5):
     import fhelium_b200._native as nat
     eng.basis_conversion = "tensor_cores"
     variants = {}
-    for name, param, value in (("tc_moddown", nat.TUNE_TC_MODDOWN, 1),):
+    # and the key-switch core's Q rows on the integer pipe instead of FP64
+    for name, param, value in (("tc_moddown", nat.TUNE_TC_MODDOWN, 1), ("integer_core", nat.TUNE_F64_CORE, 0)):
         keep_v = eng.ctx.get_tuning(param)
         eng.ctx.set_tuning(param, value)
         r = eng.multiply_relinearize_rescale(ca, cb, rlk)
@@ -732,7 +735,10 @@ def main() -> int:
     from fhelium_b200 import ranks
     value = ranks.job_rate(B, ws, ms)
     # tensor product, INTT of c2, ModUp digits, (tensor-core basis extension,) key-switch core, ModDown+rescale
-    launches_per_step = 6 if args.basis == "tensor_cores" else 5
+    # (the tensor-core form's core is two launches when its Q rows run in FP64:
+    # the P rows stay on the integer kernel)
+    f64_core = args.basis == "tensor_cores" and bool(eng.ctx.get_tuning(nat.TUNE_F64_CORE))
+    launches_per_step = (7 if f64_core else 6) if args.basis == "tensor_cores" else 5
 
     # ---- end to end through the public API with host buffers -------------
     host_a = ca.data.cpu().pin_memory()
@@ -887,10 +893,12 @@ def main() -> int:
     traffic = KS_TRAFFIC_BYTES_BATCH32 * B / 32 if cfg.logN == 16 and L == 35 else None
     # the dominant kernel of the headline form
     dom = "keyswitch_core_extended" if ext is not None else "keyswitch_core"
-    dom_kernel = {"keyswitch_core": "k_keyswitch_core", "keyswitch_core_extended": "k_keyswitch_core<PRE>"}[dom]
+    dom_kernel = {"keyswitch_core": "k_keyswitch_core",
+                  "keyswitch_core_extended": ("k_keyswitch_core_f64 (Q rows) + k_keyswitch_core<PRE> (P rows)"
+                                              if f64_core else "k_keyswitch_core<PRE>")}[dom]
     if dom == "keyswitch_core_extended":
-        traffic = (KS_EXT_TRAFFIC_BYTES_BATCH32 * B / 32
-                   if KS_EXT_TRAFFIC_BYTES_BATCH32 and cfg.logN == 16 and L == 35 else None)
+        ext_traffic = KS_F64_TRAFFIC_BYTES_BATCH32 if f64_core else KS_EXT_TRAFFIC_BYTES_BATCH32
+        traffic = ext_traffic * B / 32 if ext_traffic and cfg.logN == 16 and L == 35 else None
     dom_bytes, dom_modmul = kroof[dom]
     achieved = dom_bytes / (per_kernel[dom] / 1000.0) / 1e9
     modmul_achieved = dom_modmul / (per_kernel[dom] / 1000.0)
@@ -983,8 +991,10 @@ def main() -> int:
         "roofline": {"kernel": dom_kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": per_kernel[dom],
-                     "note": "int64 Montgomery/Shoup arithmetic (NTT butterflies, key products) on CUDA cores: "
-                             "the kernel is integer-ALU bound"},
+                     "note": ("Q rows: exact FP64 arithmetic on the FP64 pipe, P rows: int64 Shoup/Montgomery; "
+                              "bound by arithmetic issue, not HBM") if f64_core else
+                             ("int64 Montgomery/Shoup arithmetic (NTT butterflies, key products) on CUDA cores: "
+                              "the kernel is integer-ALU bound")},
         "kernel_ms": per_kernel,
         "kernel_roofline": kernel_roofline,
         "kernel_ms_note": "each public entry point timed alone on the same inputs; the fused step runs the "

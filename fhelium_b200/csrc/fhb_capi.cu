@@ -396,6 +396,10 @@ int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
       if (value != 0 && value != 1) return fail(-2, "value must be 0 or 1");
       ctx->impl->tc_ntt_fused = value;
       return 0;
+    case FHB_TUNE_F64_CORE:
+      if (value != 0 && value != 1) return fail(-2, "value must be 0 or 1");
+      ctx->impl->f64_core = value;
+      return 0;
     default:
       return fail(-2, "unknown tuning parameter");
   }
@@ -412,6 +416,7 @@ int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value) {
     case FHB_TUNE_TC_TEST_STALL: *value = ctx->impl->tc_test_stall; return 0;
     case FHB_TUNE_TC_MODDOWN: *value = ctx->impl->tc_moddown; return 0;
     case FHB_TUNE_TC_NTT_FUSED: *value = ctx->impl->tc_ntt_fused; return 0;
+    case FHB_TUNE_F64_CORE: *value = ctx->impl->f64_core && ctx->impl->f64_tables_ok; return 0;
     default: return fail(-2, "unknown tuning parameter");
   }
 }

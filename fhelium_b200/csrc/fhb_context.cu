@@ -143,6 +143,39 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
   t.prime = upload(c, info);
   t.tw_fwd = upload(c, fwd);
   t.tw_inv = upload(c, inv);
+  // FP64 tables of the tensor-core form's key-switch core: the same constants
+  // and twiddles as (c, c / q) double pairs, for int64 chains whose leading Q
+  // primes are below 2^42 (the rows of wider primes keep the integer tables)
+  bool f64 = false;
+  if constexpr (sizeof(T) == 8) {
+    c.f64_prime_end = 0;
+    while (c.f64_prime_end < c.num_q && c.moduli[c.f64_prime_end] < (uint64_t{1} << 42)) ++c.f64_prime_end;
+    f64 = c.f64_prime_end > 0;
+    if (f64) {
+      auto dpair = [](uint64_t w, uint64_t q) { return TwPair<double>{double(w), double(w) / double(q)}; };
+      std::vector<PrimeInfo<double>> dinfo(qp);
+      std::vector<TwPair<double>> dfwd(fwd.size()), dinv(inv.size());
+      for (int j = 0; j < qp; ++j) {
+        const uint64_t q = c.moduli[j];
+        const PrimeInfo<T>& p = info[j];
+        PrimeInfo<double>& d = dinfo[j];
+        d.q = double(q);
+        d.twice_q = 2.0 * double(q);
+        d.one_s = 1.0 / double(q);
+        const TwPair<double> rm = dpair(uint64_t(p.rmod), q), ni = dpair(uint64_t(p.ninv), q),
+                             nr = dpair(uint64_t(p.ninv_rinv), q), ri = dpair(uint64_t(p.rinv), q);
+        d.rmod = rm.w, d.rmod_s = rm.wp, d.ninv = ni.w, d.ninv_s = ni.wp;
+        d.ninv_rinv = nr.w, d.ninv_rinv_s = nr.wp, d.rinv = ri.w, d.rinv_s = ri.wp;
+        for (uint64_t k = 0; k < n; ++k) {
+          dfwd[size_t(j) * n + k] = dpair(uint64_t(fwd[size_t(j) * n + k].w), q);
+          dinv[size_t(j) * n + k] = dpair(uint64_t(inv[size_t(j) * n + k].w), q);
+        }
+      }
+      c.t64f.prime = upload(c, dinfo);
+      c.t64f.tw_fwd = upload(c, dfwd);
+      c.t64f.tw_inv = upload(c, dinv);
+    }
+  }
 
   // ---- ModDown by P -------------------------------------------------------
   std::vector<uint64_t> pm(c.moduli.begin() + c.num_q, c.moduli.end());
@@ -166,6 +199,16 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
   t.p_mix = upload(c, pmix);
   t.p_inv = upload(c, pinv);
   t.p_rinv = upload(c, prinv);
+  if (f64) {
+    // the FP64 core's relinearisation addend P c R: P mod q (not P R^{-1})
+    std::vector<TwPair<double>> dp(qp, TwPair<double>{0.0, 0.0});
+    for (int pid = 0; pid < c.f64_prime_end; ++pid) {
+      const uint64_t m = c.moduli[pid], p_mod = prefix_product_mod(pm, c.num_p, m);
+      dp[pid] = TwPair<double>{double(p_mod), double(p_mod) / double(m)};
+    }
+    c.t64f.p_rinv = upload(c, dp);
+    c.f64_tables_ok = c.t64f.prime && c.t64f.tw_fwd && c.t64f.tw_inv && c.t64f.p_rinv;
+  }
 
   // ---- per level: hybrid digits, Garner and extension constants, rescale --
   std::vector<std::vector<int>> level0;

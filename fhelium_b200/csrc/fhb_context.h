@@ -97,6 +97,15 @@ struct Context {
   // tuning, with basis_tc: ModDown's P -> Q conversion on the tensor cores
   // (1) or on the CUDA cores (0, default: faster on B200)
   int tc_moddown = 0;
+  // FP64 tables for the tensor-core form's key-switch core (int64 chains whose
+  // Q primes are below 2^42): per-prime constants and twiddles as (c, c / q)
+  // double pairs; p_rinv holds P mod q (the FP64 core's accumulators carry R)
+  ChainTables<double> t64f;
+  bool f64_tables_ok = false;
+  int f64_prime_end = 0;  // Q primes [0, f64_prime_end) are below 2^42 (FP64 rows)
+  // tuning: the tensor-core form's key-switch core runs its Q rows in FP64
+  // arithmetic (1, default when the tables exist) or on the integer pipe (0)
+  int f64_core = 1;
   // tuning: the tensor-core NTT's 16-point pass fused with the adjacent
   // 64-point pass (1) or three separate passes (0, default: faster on B200)
   int tc_ntt_fused = 0;

@@ -406,6 +406,11 @@ struct KsAcc {
     c0[e * stride] = csub(c0[e * stride] + Word<T>::mont(x, k0, p.q, p.neg_inv), p.twice_q);
     c1[e * stride] = csub(c1[e * stride] + Word<T>::mont(x, k1, p.q, p.neg_inv), p.twice_q);
   }
+  // FP64 form (T = double): residues times key words (both < 2q), quotient from 1/q
+  __device__ __forceinline__ void mac_f64(int e, T x, T k0, T k1, T q, T twoq, T qinv) {
+    c0[e * stride] = csub(c0[e * stride] + Word<T>::mul_qinv(x, k0, q, qinv), twoq);
+    c1[e * stride] = csub(c1[e * stride] + Word<T>::mul_qinv(x, k1, q, qinv), twoq);
+  }
   __device__ __forceinline__ void get(int which, T (&v)[G::kE]) const {
     const T* c = which ? c1 : c0;
 #pragma unroll
@@ -541,15 +546,18 @@ __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
                  T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
                  const unsigned long long* __restrict__ item_keys, const T* __restrict__ ct3, int64_t ct3_stride,
-                 ChainTables<T> tabs, LevelTables<T> lt) {
+                 ChainTables<T> tabs, LevelTables<T> lt, int row0, int nrows) {
   using G = NttGeom<T, LOGN>;
   using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  int64_t poly, bi;  // poly over [B, QP_l]
+  // units over [B, rows row0 .. row0 + nrows) of QP_l; poly over [B, QP_l]
+  int64_t poly, bi;
   int jrow;
-  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  ks_work(blockIdx.x / G::kC, nrows, batch, order, poly, bi, jrow);
+  jrow += row0;
+  poly = bi * qp_limbs + jrow;
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
@@ -589,6 +597,107 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   if (add) ks_add_p_scaled(v, 1, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
   InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e1);
+}
+
+// ---------------------------------------------------------------------------
+// The key-switch core of the tensor-core form for the Q rows, in FP64
+// arithmetic (int64 chains whose Q primes are below 2^42, rings up to
+// N = 2^16 so the accumulators live in shared memory).  Residues are held as
+// exact integers in doubles and every product is Word<double>'s exact
+// product, so the butterflies run on the FP64 pipe instead of the integer
+// multiply-add pipe; inputs and outputs stay 64-bit words in global memory,
+// converted on load and store.  The key words are used as stored (k R, the
+// Montgomery form), so the accumulators carry a factor R, removed with
+// N^{-1} R^{-1} in the inverse transform's epilogue; for relinearisation
+// the addends enter as P c R (ct3 holds c R, tabs.p_rinv holds P mod q here)
+// and an own-digit row as c2 = (c2 R) R^{-1}.  The outputs are the integer
+// kernel's word for word.  ext: the extensions [D_l][B][QP_l][N] of the
+// tensor-core basis conversion; units over [B, nrows], the leading Q rows
+// whose primes are below 2^42.
+struct U64RowSource {
+  const uint64_t* in;
+  template <int C>
+  __device__ __forceinline__ void column(int m, int stride, double (&x)[C]) const {
+#pragma unroll
+    for (int k = 0; k < C; ++k) x[k] = __ull2double_rn(in[k * stride + m]);
+  }
+};
+
+struct F64InvEpilogue {
+  uint64_t* dst;
+  double q, c, cs;
+  __device__ __forceinline__ void operator()(int pos, double v) const {
+    v = csub(Word<double>::shoup(v, c, cs, q), q);
+    dst[pos] = __double2ull_rz(v);
+  }
+};
+
+template <class Acc, int E>
+__device__ __forceinline__ void key_mac_f64(Acc& acc, const double (&v)[E], const uint64_t* key0,
+                                            const uint64_t* key1, double q, double twoq, double qinv) {
+#pragma unroll
+  for (int i = 0; i < E / 2; ++i) {
+    const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(key0) + i);
+    const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(key1) + i);
+    acc.mac_f64(2 * i, csub(v[2 * i], twoq), __ull2double_rn(a.x), __ull2double_rn(b.x), q, twoq, qinv);
+    acc.mac_f64(2 * i + 1, csub(v[2 * i + 1], twoq), __ull2double_rn(a.y), __ull2double_rn(b.y), q, twoq, qinv);
+  }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(NttGeom<double, LOGN>::kThreads)
+k_keyswitch_core_f64(const uint64_t* __restrict__ ext, const uint64_t* __restrict__ key, uint64_t* __restrict__ acc0,
+                     uint64_t* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
+                     int order, const unsigned long long* __restrict__ item_keys, const uint64_t* __restrict__ ct3,
+                     int64_t ct3_stride, ChainTables<double> tabs, LevelTables<uint64_t> lt, int nrows) {
+  using G = NttGeom<double, LOGN>;
+  using W = Word<double>;
+  static_assert(KsAcc<double, LOGN>::kSmem, "the FP64 core keeps its accumulators in shared memory");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s = reinterpret_cast<double*>(smem_raw);
+  const int rank = cluster_rank<double, LOGN>();
+  int64_t poly, bi;
+  int jrow;
+  ks_work(blockIdx.x / G::kC, nrows, batch, order, poly, bi, jrow);  // rows [0, nrows) of Q_l
+  poly = bi * qp_limbs + jrow;
+  const int pid = level + jrow;
+  const PrimeInfo<double> p = tabs.prime[pid];
+  const double q = p.q, twoq = p.twice_q, qinv = p.one_s;
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  if (item_keys) key = reinterpret_cast<const uint64_t*>(item_keys[bi]);  // mixed-key batch
+  KsAcc<double, LOGN> acc(s, nullptr, nullptr);
+  KsTw<double, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(false);
+  const bool add = ct3 != nullptr;
+  const uint64_t* ct3_own = add ? ct3 + (bi * q_limbs + jrow) * int64_t(G::kN) + own : nullptr;
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    const uint64_t* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
+    const uint64_t* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
+    double v[G::kE];
+    if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
+      // uniform over the cluster: the own digit's NTT residue is c2 itself
+#pragma unroll
+      for (int e = 0; e < G::kE; ++e) v[e] = W::shoup(__ull2double_rn(ct3_own[2 * ct3_stride + e]), p.rinv, p.rinv_s, q);
+    } else {
+      U64RowSource src{ext + ((int64_t(a) * batch + bi) * qp_limbs + jrow) * G::kN};
+      tw.forward_from(src, s, p, v);
+    }
+    key_mac_f64(acc, v, key0, key1, q, twoq, qinv);
+  }
+  tw.stage(true);
+  const TwPair<double> pc = tabs.p_rinv[pid];  // P mod q and its companion (FP64 tables)
+  for (int c = 0; c < 2; ++c) {
+    double v[G::kE];
+    acc.get(c, v);
+    if (add) {
+#pragma unroll
+      for (int e = 0; e < G::kE; ++e)
+        v[e] = csub(v[e] + W::shoup(__ull2double_rn(ct3_own[c * ct3_stride + e]), pc.w, pc.wp, q), twoq);
+    }
+    F64InvEpilogue epi{(c ? acc1 : acc0) + poly * G::kN, q, p.ninv_rinv, p.ninv_rinv_s};
+    tw.inverse(s, p, v, epi);
+  }
 }
 
 // Sum of key switches of several ciphertexts with their own keys, reduced

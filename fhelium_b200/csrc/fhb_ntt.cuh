@@ -30,6 +30,8 @@
 #pragma once
 #include <cooperative_groups.h>
 
+#include <type_traits>
+
 #include "fhb_arith.cuh"
 
 namespace fhb {
@@ -77,7 +79,10 @@ struct NttGeom {
 
 template <typename T>
 __device__ __forceinline__ TwPair<T> ldtw(const TwPair<T>* tw, int i) {
-  if constexpr (sizeof(T) == 8) {
+  if constexpr (std::is_same<T, double>::value) {
+    const double2 v = __ldg(reinterpret_cast<const double2*>(tw + i));
+    return TwPair<T>{v.x, v.y};
+  } else if constexpr (sizeof(T) == 8) {
     const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(tw + i));
     return TwPair<T>{v.x, v.y};
   } else {

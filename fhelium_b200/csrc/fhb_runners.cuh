@@ -2,6 +2,7 @@
 // instantiated per LOGN in its own translation unit (fhb_inst_logn.cu), so
 // the kernel templates compile in parallel.
 #pragma once
+#include <algorithm>
 #include "fhb_items.cuh"
 #include "fhb_kernels.cuh"
 
@@ -83,21 +84,35 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
                 int64_t ct3_pitch) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
   if (ct3_pitch <= 0) ct3_pitch = batch * ql * int64_t(c.n());  // component pitch of ct3 [3, batch, L, N]
+  const auto* ik = reinterpret_cast<const unsigned long long*>(item_keys);
+  // the integer core over rows [row0, row0 + nrows) of Q_l P
+  auto launch_int = [&](auto kern, int row0, int nrows) {
+    return launch_cluster<T, LOGN>(kern, batch * nrows, KsAcc<T, LOGN>::smem_bytes(), st, (const T*)digits,
+                                   (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(), c.ks_order, ik,
+                                   (const T*)ct3, ct3_pitch, tables<T>(c), level_tables<T>(c, level), row0, nrows);
+  };
   if (pre) {
     // extensions from the tensor-core basis conversion (int64 only)
     if constexpr (sizeof(T) == 8) {
-      return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN, true>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
-                                     (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level,
-                                     c.qp(), c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys),
-                                     (const T*)ct3, ct3_pitch, tables<T>(c), level_tables<T>(c, level));
+      if constexpr (KsAcc<double, LOGN>::kSmem) {
+        // the leading Q rows whose primes are below 2^42 in FP64 arithmetic,
+        // the rest (wider Q primes, the P rows) on the integer core
+        const int f64_rows = c.f64_core && c.f64_tables_ok ? std::max(0, std::min(ql, c.f64_prime_end - level)) : 0;
+        if (f64_rows > 0) {
+          if (int rc = launch_int(k_keyswitch_core<T, LOGN, true>, f64_rows, qpl - f64_rows)) return rc;
+          return launch_cluster<double, LOGN>(k_keyswitch_core_f64<LOGN>, batch * f64_rows,
+                                              KsAcc<double, LOGN>::smem_bytes(), st, (const uint64_t*)digits,
+                                              (const uint64_t*)key, (uint64_t*)acc0, (uint64_t*)acc1, batch, ql,
+                                              qpl, level, c.qp(), c.ks_order, ik, (const uint64_t*)ct3, ct3_pitch,
+                                              c.t64f, level_tables<uint64_t>(c, level), f64_rows);
+        }
+      }
+      return launch_int(k_keyswitch_core<T, LOGN, true>, 0, qpl);
     } else {
       return fail(-7, "the tensor-core basis conversion needs an int64 context");
     }
   }
-  return launch_cluster<T, LOGN>(k_keyswitch_core<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
-                                 (const T*)digits, (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(),
-                                 c.ks_order, reinterpret_cast<const unsigned long long*>(item_keys), (const T*)ct3,
-                                 ct3_pitch, tables<T>(c), level_tables<T>(c, level));
+  return launch_int(k_keyswitch_core<T, LOGN>, 0, qpl);
 }
 
 template <typename T, int LOGN>

@@ -200,3 +200,59 @@ def test_tc_form_full_ring_batches_and_moddown_variants(batch, tc_moddown):
     for x, y in zip(tc, plain):
         np.testing.assert_array_equal(x, y)
     np.testing.assert_array_equal(tc[0][:, batch - 1], orc.relinearize(ct3[:, batch - 1], key, level))
+
+
+@pytest.mark.parametrize("family,log_n,level,batch", [("int64_logn14", 14, 0, 3), ("int64_logn16", 16, 0, 5),
+                                                      ("int64_logn16", 16, 30, 2), ("int64_logn16", 13, 12, 6)])
+def test_f64_core_matches_integer_core(family, log_n, level, batch):
+    """The tensor-core form's key-switch core with its Q rows in exact FP64
+    arithmetic (the default where every Q prime is below 2^42) against the
+    same core on the integer pipe: relinearisation, fused HMult, rotation and
+    mixed-step rotation (per-item keys) integer-equal, and against the oracle."""
+    cfg, eng, orc, rng = _setup(family, log_n, 31)
+    eng.basis_conversion = "tensor_cores"
+    assert eng.ctx.get_tuning(nat.TUNE_F64_CORE) == 1
+    rows = orc.q_rows(level)
+    key = random_key(rng, cfg, cfg.N)
+    rlk = RelinearizationKey(to_dev(key, cfg))
+    ct3 = uniform_residues(rng, cfg.moduli, rows, (3, batch), cfg.N, lazy=True)
+    x = Ciphertext(to_dev(ct3, cfg), level, 1.0, "ntt", "montgomery")
+    ct = uniform_residues(rng, cfg.moduli, rows, (2, batch), cfg.N)
+    c = Ciphertext(to_dev(ct, cfg), level, 1.0)
+    keys = [RotationKey(to_dev(random_key(rng, cfg, cfg.N), cfg), rotation_step=s,
+                        galois_element=eng.galois_element_for_step(s)) for s in range(1, batch + 1)]
+    outs = {}
+    for f64 in (1, 0):
+        eng.ctx.set_tuning(nat.TUNE_F64_CORE, f64)
+        res = [to_np(eng.relinearize(x, rlk).data), to_np(eng.rotate_with_key(c, keys[0]).data),
+               to_np(eng.rotate_items_with_keys(c, keys).data)]
+        outs[f64] = res
+    eng.ctx.set_tuning(nat.TUNE_F64_CORE, 1)
+    for got, want in zip(outs[1], outs[0]):
+        np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(outs[1][0][:, batch - 1], orc.relinearize(ct3[:, batch - 1], key, level))
+    if level + 1 < cfg.num_q_primes:
+        a = uniform_residues(rng, cfg.moduli, rows, (2, batch), cfg.N, lazy=True)
+        b = uniform_residues(rng, cfg.moduli, rows, (2, batch), cfg.N, lazy=True)
+        ca = Ciphertext(to_dev(a, cfg), level, 2.0 ** 30, "ntt", "montgomery")
+        cb = Ciphertext(to_dev(b, cfg), level, 2.0 ** 30, "ntt", "montgomery")
+        got = to_np(eng.multiply_relinearize_rescale(ca, cb, rlk).data)
+        eng.ctx.set_tuning(nat.TUNE_F64_CORE, 0)
+        want = to_np(eng.multiply_relinearize_rescale(ca, cb, rlk).data)
+        eng.ctx.set_tuning(nat.TUNE_F64_CORE, 1)
+        np.testing.assert_array_equal(got, want)
+        np.testing.assert_array_equal(got[:, 0], orc.rescale(orc.relinearize(orc.multiply(a[:, 0], b[:, 0], level),
+                                                                             key, level), level))
+
+
+def test_f64_core_unavailable_for_wide_primes():
+    """50-bit Q primes: no FP64 tables, the switch reads back 0, results unchanged."""
+    eng = CkksEngine(Preset.slots8192_scale50_levels5_int64)
+    eng.basis_conversion = "tensor_cores"
+    assert eng.ctx.get_tuning(nat.TUNE_F64_CORE) == 0
+    rng = np.random.default_rng(4)
+    a, b = (eng.coefficient_domain_to_ntt_domain(eng.encrypt_message(rng.uniform(-0.05, 0.05, eng.num_slots)))
+            for _ in range(2))
+    got = eng.multiply_relinearize_rescale(a, b)
+    eng.basis_conversion = "cuda_cores"
+    assert torch.equal(got.data, eng.multiply_relinearize_rescale(a, b).data)
