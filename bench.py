@@ -763,8 +763,8 @@ def main() -> int:
     e2e_steps = max(3, args.steps)
     # chunk schedules x staging slots, picked on untimed passes: equal
     # chunks, or chunks of 2-3 ciphertexts ending in single-ciphertext chunks
-    schedules = {str(c): min(c, B) for c in (1, 16, 32)}
-    for width, tail in ((2, 2), (2, 4), (3, 2)):
+    schedules = {str(c): min(c, B) for c in (1, 4, 8, 16, 32)}
+    for width, tail in ((2, 2), (3, 2), (4, 2), (8, 4)):
         schedules[f"{width}x..+1x{tail}"] = tapered(B, width, tail)
     trial = {}
     for name, chunks in schedules.items():

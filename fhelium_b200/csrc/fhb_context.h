@@ -103,8 +103,9 @@ struct Context {
   ChainTables<double> t64f;
   bool f64_tables_ok = false;
   int f64_prime_end = 0;  // Q primes [0, f64_prime_end) are below 2^42 (FP64 rows)
-  // tuning: the tensor-core form's key-switch core runs its Q rows in FP64
-  // arithmetic (1, default when the tables exist) or on the integer pipe (0)
+  // tuning: the rows of primes below 2^42 run in FP64 arithmetic (1, default
+  // when the tables exist: standalone NTTs and the tensor-core form's
+  // key-switch core) or on the integer pipe (0)
   int f64_core = 1;
   // tuning: the tensor-core NTT's 16-point pass fused with the adjacent
   // 64-point pass (1) or three separate passes (0, default: faster on B200)

@@ -74,12 +74,14 @@ struct RowSource {
 template <typename T, int LOGN, bool TO_MONT, int EPT = 0>
 __global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start,
-              ChainTables<T> tabs) {
+              ChainTables<T> tabs, int sub0, int nsub) {
   using G = NttGeom<T, LOGN, EPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;
+  // units over the rows [sub0, sub0 + nsub) of every polynomial group of `rows`
+  const int64_t unit = blockIdx.x / G::kC;
+  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
   const int pid = row_start + int(poly % rows);
   const PrimeInfo<T> p = tabs.prime[pid];
   RowSource<T, TO_MONT> src{in + poly * G::kN, p.rmod, p.rmod_s, p.q};
@@ -120,12 +122,13 @@ __device__ __forceinline__ InvEpilogue<T> make_inv_epilogue(T* dst, const PrimeI
 template <typename T, int LOGN, int EPT = 0>
 __global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
 k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start, int kind,
-              ChainTables<T> tabs) {
+              ChainTables<T> tabs, int sub0, int nsub) {
   using G = NttGeom<T, LOGN, EPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t poly = blockIdx.x / G::kC;
+  const int64_t unit = blockIdx.x / G::kC;
+  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
   const int pid = row_start + int(poly % rows);
   const PrimeInfo<T> p = tabs.prime[pid];
   T v[G::kE];
@@ -133,6 +136,94 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
   InvEpilogue<T> epi = make_inv_epilogue<T>(out + poly * G::kN, p, kind, true);
   Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v,
                                                 epi);
+}
+
+// FP64 forms of the plain transforms for the rows of primes below 2^42
+// (residues as exact integers in doubles, Word<double> products on the FP64
+// pipe; 64-bit words in memory, converted on load and store), over the rows
+// [sub0, sub0 + nsub) of every group of `rows`.  Same outputs as the integer
+// kernels.
+template <bool TO_MONT>
+struct U64MontSource {
+  const uint64_t* in;
+  double c, cs, q;
+  template <int C>
+  __device__ __forceinline__ void column(int m, int stride, double (&x)[C]) const {
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+      double v = __ull2double_rn(in[k * stride + m]);
+      if constexpr (TO_MONT) v = Word<double>::shoup(v, c, cs, q);
+      x[k] = v;
+    }
+  }
+};
+
+template <int E>
+__device__ __forceinline__ void store_words(uint64_t* p, const double (&v)[E]) {
+  uint64_t w[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) w[e] = __double2ull_rz(v[e]);
+  store16(p, w);
+}
+
+template <int LOGN, bool TO_MONT, int EPT = 0>
+__global__ void __launch_bounds__(NttGeom<double, LOGN, EPT>::kThreads)
+k_ntt_forward_f64(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int rows, int row_start,
+                  ChainTables<double> tabs, int sub0, int nsub) {
+  using G = NttGeom<double, LOGN, EPT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s = reinterpret_cast<double*>(smem_raw);
+  const int rank = cluster_rank<double, LOGN>();
+  const int64_t unit = blockIdx.x / G::kC;
+  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
+  const int pid = row_start + int(poly % rows);
+  const PrimeInfo<double> p = tabs.prime[pid];
+  U64MontSource<TO_MONT> src{in + poly * G::kN, p.rmod, p.rmod_s, p.q};
+  double v[G::kE];
+  Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::forward_from(src, s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q,
+                                                                p.twice_q, rank, v);
+#pragma unroll
+  for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+  store_words(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
+}
+
+struct F64OutEpilogue {
+  uint64_t* dst;
+  double q, c, cs;
+  int kind;
+  __device__ __forceinline__ void operator()(int pos, double v) const {
+    v = Word<double>::shoup(v, c, cs, q);  // [0, 2q)
+    if (kind >= kInvStandard) v = csub(v, q);
+    if (kind == kInvCentered && v > floor(0.5 * q)) {
+      dst[pos] = uint64_t(__double2ll_rz(v - q));
+      return;
+    }
+    dst[pos] = __double2ull_rz(v);
+  }
+};
+
+template <int LOGN, int EPT = 0>
+__global__ void __launch_bounds__(NttGeom<double, LOGN, EPT>::kThreads)
+k_ntt_inverse_f64(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int rows, int row_start, int kind,
+                  ChainTables<double> tabs, int sub0, int nsub) {
+  using G = NttGeom<double, LOGN, EPT>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* s = reinterpret_cast<double*>(smem_raw);
+  const int rank = cluster_rank<double, LOGN>();
+  const int64_t unit = blockIdx.x / G::kC;
+  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
+  const int pid = row_start + int(poly % rows);
+  const PrimeInfo<double> p = tabs.prime[pid];
+  uint64_t w[G::kE];
+  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, w);
+  double v[G::kE];
+#pragma unroll
+  for (int e = 0; e < G::kE; ++e) v[e] = __ull2double_rn(w[e]);
+  const bool std_out = kind != kInvMontgomery;  // Montgomery NTT input: N^-1 R^-1 unless the output stays Montgomery
+  F64OutEpilogue epi{out + poly * G::kN, p.q, std_out ? p.ninv_rinv : p.ninv, std_out ? p.ninv_rinv_s : p.ninv_s,
+                     kind};
+  Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank,
+                                                           v, epi);
 }
 
 // ---------------------------------------------------------------------------

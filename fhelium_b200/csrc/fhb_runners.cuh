@@ -8,6 +8,14 @@
 
 namespace fhb {
 
+// Rows [row_start, row_start + rows) of a transform whose leading k rows
+// have primes below 2^42 and may run in FP64 arithmetic (0 when the
+// context has no FP64 tables or the form is switched off).
+inline int f64_rows(const Context& c, int row_start, int rows) {
+  if (!c.f64_core || !c.f64_tables_ok) return 0;
+  return std::max(0, std::min(rows, c.f64_prime_end - row_start));
+}
+
 template <typename T, int LOGN, int EPT = 0, typename... KArgs, typename... Args>
 int launch_cluster(void (*kernel)(KArgs...), int64_t polys, size_t smem, cudaStream_t stream, Args... args) {
   using G = NttGeom<T, LOGN, EPT>;
@@ -42,11 +50,24 @@ constexpr size_t ntt_smem() {
 template <typename T, int LOGN, int EPT>
 int run_forward_e(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool mont,
                   cudaStream_t st) {
-  if (mont)
-    return launch_cluster<T, LOGN, EPT>(k_ntt_forward<T, LOGN, false, EPT>, polys, ntt_smem<T, LOGN>(), st,
-                                        (const T*)in, (T*)out, rows, row_start, tables<T>(c));
-  return launch_cluster<T, LOGN, EPT>(k_ntt_forward<T, LOGN, true, EPT>, polys, ntt_smem<T, LOGN>(), st,
-                                      (const T*)in, (T*)out, rows, row_start, tables<T>(c));
+  const int64_t groups = polys / rows;
+  // the leading rows of primes below 2^42 in FP64 arithmetic (int64 chains)
+  const int k = sizeof(T) == 8 ? f64_rows(c, row_start, rows) : 0;
+  auto launch_int = [&](auto kern, int sub0, int nsub) {
+    return launch_cluster<T, LOGN, EPT>(kern, groups * nsub, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out, rows,
+                                        row_start, tables<T>(c), sub0, nsub);
+  };
+  auto launch_f64 = [&](auto kern) {
+    return launch_cluster<double, LOGN, EPT>(kern, groups * k, ntt_smem<double, LOGN>(), st, (const uint64_t*)in,
+                                             (uint64_t*)out, rows, row_start, c.t64f, 0, k);
+  };
+  if (k < rows) {
+    const int rc = mont ? launch_int(k_ntt_forward<T, LOGN, false, EPT>, k, rows - k)
+                        : launch_int(k_ntt_forward<T, LOGN, true, EPT>, k, rows - k);
+    if (rc) return rc;
+  }
+  if (k == 0) return 0;
+  return mont ? launch_f64(k_ntt_forward_f64<LOGN, false, EPT>) : launch_f64(k_ntt_forward_f64<LOGN, true, EPT>);
 }
 
 template <typename T, int LOGN>
@@ -56,14 +77,27 @@ int run_forward(const Context& c, const void* in, void* out, int64_t polys, int 
   return run_forward_e<T, LOGN, 0>(c, in, out, polys, rows, row_start, mont, st);
 }
 
+template <typename T, int LOGN, int EPT>
+int run_inverse_e(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
+                  cudaStream_t st) {
+  const int64_t groups = polys / rows;
+  const int k = sizeof(T) == 8 ? f64_rows(c, row_start, rows) : 0;
+  if (k < rows) {
+    const int rc = launch_cluster<T, LOGN, EPT>(k_ntt_inverse<T, LOGN, EPT>, groups * (rows - k), ntt_smem<T, LOGN>(),
+                                                st, (const T*)in, (T*)out, rows, row_start, kind, tables<T>(c), k,
+                                                rows - k);
+    if (rc) return rc;
+  }
+  if (k == 0) return 0;
+  return launch_cluster<double, LOGN, EPT>(k_ntt_inverse_f64<LOGN, EPT>, groups * k, ntt_smem<double, LOGN>(), st,
+                                           (const uint64_t*)in, (uint64_t*)out, rows, row_start, kind, c.t64f, 0, k);
+}
+
 template <typename T, int LOGN>
 int run_inverse(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
                 cudaStream_t st) {
-  if (c.ntt_ept_inv == 16)
-    return launch_cluster<T, LOGN, 16>(k_ntt_inverse<T, LOGN, 16>, polys, ntt_smem<T, LOGN>(), st, (const T*)in,
-                                       (T*)out, rows, row_start, kind, tables<T>(c));
-  return launch_cluster<T, LOGN>(k_ntt_inverse<T, LOGN>, polys, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out,
-                                 rows, row_start, kind, tables<T>(c));
+  if (c.ntt_ept_inv == 16) return run_inverse_e<T, LOGN, 16>(c, in, out, polys, rows, row_start, kind, st);
+  return run_inverse_e<T, LOGN, 0>(c, in, out, polys, rows, row_start, kind, st);
 }
 
 template <typename T, int LOGN>

@@ -94,11 +94,11 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * FHB_TUNE_TC_NTT_FUSED: fhb_tc_forward_ntt / fhb_tc_inverse_ntt in two
  * launches, the 16-point pass fused with the adjacent 64-point pass over each
  * 8192-word span (1), or in three (0, default: faster on B200).
- * FHB_TUNE_F64_CORE (with the tensor-core form, int64 chains whose Q primes
- * are below 2^42, N <= 2^16): 1 = the key-switch core runs its Q rows in
+ * FHB_TUNE_F64_CORE (int64 chains): 1 = the rows of primes below 2^42 run in
  * exact FP64 arithmetic (integers held in doubles, products on the FP64
- * pipe; default), 0 = on the integer pipe.  Reads back 0 where the form is
- * unavailable.
+ * pipe; default) in the standalone forward / inverse NTT and, with the
+ * tensor-core form and N <= 2^16, in the key-switch core; 0 = on the integer
+ * pipe.  Reads back 0 where the chain has no such primes.
  * Results do not depend on any of these (stall aside).  No counterpart in the reference
  * (its launch shapes and arithmetic units are fixed). */
 enum fhb_tuning_param {

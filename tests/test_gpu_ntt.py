@@ -81,3 +81,49 @@ def test_ntt_in_place_and_batch_rows():
     np.testing.assert_array_equal(canon(to_np(t), cfg.moduli, rows), canon(orc.forward_to_montgomery(x, rows), cfg.moduli, rows))
     eng.inverse_ntt(t, 2, out=t)
     np.testing.assert_array_equal(to_np(t), x)
+
+
+@pytest.mark.parametrize("log_n,rows,row_start", [(16, 35, 0), (16, 6, 31), (14, 8, 0), (13, 5, 2)])
+@pytest.mark.parametrize("ept", [0, 16])
+def test_f64_rows_equal_integer_rows(log_n, rows, row_start, ept):
+    """Rows of primes below 2^42 in exact FP64 arithmetic (the default) against
+    the integer path: forward (both input forms) and the lazy inverse kinds
+    equal modulo q and in [0, 2q), the canonical inverse kinds integer-equal,
+    including ranges that straddle the 60-bit rows."""
+    from fhelium_b200 import _native as nat
+    from fhelium_b200.config import CkksConfig, Preset
+    from tests.helpers import reduced_ring
+    cfg = CkksConfig.parse(Preset.slots32768_scale40_levels34_int64)
+    if log_n != cfg.logN:
+        cfg = reduced_ring(cfg, log_n)
+    ctx = nat.NativeContext(64, log_n, cfg.moduli, cfg.num_q_primes, cfg.num_p_primes, torch.device("cuda:0"))
+    assert ctx.get_tuning(nat.TUNE_F64_CORE) == 1
+    ctx.set_tuning(nat.TUNE_NTT_FORWARD_EPT, ept)
+    ctx.set_tuning(nat.TUNE_NTT_INVERSE_EPT, ept)
+    q = torch.tensor(cfg.moduli[row_start:row_start + rows], dtype=torch.int64, device="cuda:0").view(1, rows, 1)
+    g = torch.Generator(device="cuda:0").manual_seed(log_n + rows)
+    x = torch.randint(0, 1 << 62, (3, rows, 1 << log_n), generator=g, device="cuda:0", dtype=torch.int64) % (2 * q)
+    s = torch.cuda.current_stream().cuda_stream
+    outs = {}
+    for f64 in (1, 0):
+        ctx.set_tuning(nat.TUNE_F64_CORE, f64)
+        res = []
+        for mode in (0, 1):
+            y = torch.empty_like(x)
+            nat.check(ctx.lib.fhb_forward_ntt(ctx.handle, x.data_ptr(), y.data_ptr(), 3, rows, row_start, mode, s), "f")
+            res.append(y)
+        for kind in range(4):
+            z = torch.empty_like(x)
+            nat.check(ctx.lib.fhb_inverse_ntt(ctx.handle, res[1].data_ptr(), z.data_ptr(), 3, rows, row_start, kind, s),
+                      "i")
+            res.append(z)
+        outs[f64] = res
+    # forward outputs and the lazy inverse kinds (0, 1) may pick another
+    # representative in [0, 2q): equal modulo q; canonical kinds (2, 3) exactly
+    for i, (a, b) in enumerate(zip(outs[1], outs[0])):
+        if i < 4:
+            assert torch.equal(a % q, b % q), i
+            assert bool((a >= 0).all()) and bool((a < 2 * q).all()), i
+        else:
+            assert torch.equal(a, b), i
+    ctx.close()
