@@ -506,7 +506,9 @@ def mixed_batch_leg(dev, stream, count=512, steps=3):
     from fhelium_b200 import autotune
     from fhelium_b200.batch import HMULT, MixedBatchExecutor, run_per_ciphertext, sample_mixed_workload
     from fhelium_b200.engine import CkksEngine
-    eng = CkksEngine(PRESET, device=dev, rng_seed=9)
+    # the CUDA-core form, as the items path's own key switch: the group
+    # executor's scratch then holds no extensions (the keys leave little room)
+    eng = CkksEngine(PRESET, device=dev, rng_seed=9, basis_conversion="cuda_cores")
     levels, ops = sample_mixed_workload(eng.num_q, count, seed=0)
     msgs = _messages(count, eng.num_slots, 3)
     cts = [eng.encrypt_message(msgs[i], level=lv) for i, lv in enumerate(levels)]

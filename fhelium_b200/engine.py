@@ -41,7 +41,7 @@ class CkksEngine:
                  device: torch.device | str | None = None, allow_sk_gen: bool = True,
                  galois_generator: int = 3, ntt_backend: str | None = None, rng_seed: int | None = None,
                  rng_nonce: int | None = None, encode_rounding: str = "stochastic",
-                 basis_conversion: str = "cuda_cores"):
+                 basis_conversion: str = "auto"):
         if ckks_config is None:
             ckks_config = Preset.slots16384_scale40_levels16_int64
         if isinstance(ckks_config, (Preset, str, dict)):
@@ -101,8 +101,20 @@ class CkksEngine:
 
     @basis_conversion.setter
     def basis_conversion(self, form: str) -> None:
+        """``"auto"`` (the default) picks the tensor-core form where the chain
+        supports it (int64 chains; with the exact FP64 key-switch core it is
+        the faster form) and the CUDA-core form elsewhere."""
+        if form == "auto":
+            if self.dtype == torch.int64:
+                try:
+                    self.ctx.set_tuning(nat.TUNE_BASIS_CONVERSION, nat.BASIS_TENSOR_CORES)
+                    return
+                except nat.NativeCallError:
+                    pass
+            self.ctx.set_tuning(nat.TUNE_BASIS_CONVERSION, nat.BASIS_CUDA_CORES)
+            return
         if form not in self._BASIS_FORMS:
-            raise ValueError("basis_conversion must be 'cuda_cores' or 'tensor_cores'")
+            raise ValueError("basis_conversion must be 'auto', 'cuda_cores' or 'tensor_cores'")
         self.ctx.set_tuning(nat.TUNE_BASIS_CONVERSION, self._BASIS_FORMS[form])
 
     # ------------------------------------------------------------------

@@ -43,7 +43,7 @@ def _setup(family, log_n, seed):
     cfg = CONFIGS[family]()
     if log_n != cfg.logN:
         cfg = reduced_ring(cfg, log_n)
-    eng = CkksEngine(cfg)
+    eng = CkksEngine(cfg, basis_conversion="cuda_cores")  # each test switches forms itself
     return cfg, eng, oracle_for(cfg, log_n), np.random.default_rng(seed)
 
 
