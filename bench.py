@@ -450,6 +450,12 @@ def forms_leg(eng, ca, cb, rlk, stream, steps=5):
     out, results = {}, {}
     keep = eng.basis_conversion
     eng.generate_rotation_keys(list(range(1, 17)))
+    # warm both forms up first (kernel loading, scratch, clocks), then time each
+    for form in ("cuda_cores", "tensor_cores"):
+        eng.basis_conversion = form
+        for _ in range(2):
+            eng.rotate_by_step(eng.multiply_relinearize_rescale(ca, cb, rlk), 1)
+    torch.cuda.synchronize()
     for form in ("cuda_cores", "tensor_cores"):
         eng.basis_conversion = form
         res = {}

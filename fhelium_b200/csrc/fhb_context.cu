@@ -220,6 +220,9 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
   level0.push_back({c.num_q - 1});
   levels.assign(c.num_q, LevelTables<T>{});
   c.level_digits.assign(c.num_q, {});
+  const int d0 = int(level0.size());
+  std::vector<TwPair<double>> ext64f;
+  if (f64) ext64f.assign(size_t(c.num_q) * d0 * kMaxDigitWidth * 2 * qp, TwPair<double>{0.0, 0.0});
   for (int level = 0; level < c.num_q; ++level) {
     LevelTables<T>& lt = levels[level];
     std::vector<DigitDesc> dd;
@@ -245,6 +248,17 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
       for (int r = 0; r < alpha; ++r)
         for (int pid = 0; pid < qp; ++pid) e[size_t(r) * qp + pid] = pair<T>(prefix_product_mod(b, r, c.moduli[pid]), c.moduli[pid]);
       ext.insert(ext.end(), e.begin(), e.end());
+      if (f64) {
+        const int a = int(dd.size()) - 1;
+        for (int r = 0; r < alpha; ++r)
+          for (int pid = 0; pid < c.f64_prime_end; ++pid) {
+            const uint64_t m = c.moduli[pid], cr = prefix_product_mod(b, r, m);
+            const size_t at = ((((size_t(level) * d0 + a) * kMaxDigitWidth + r) * 2) * qp) + pid;
+            const uint64_t hi = mulmod(cr, (uint64_t{1} << 30) % m, m);
+            ext64f[at] = TwPair<double>{double(hi), double(hi) / double(m)};
+            ext64f[at + qp] = TwPair<double>{double(cr), double(cr) / double(m)};
+          }
+      }
     }
     lt.num_digits = int(dd.size());
     c.level_digits[level] = dd;
@@ -260,6 +274,11 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
   }
   levels_dev = upload(c, levels);
   if (!levels_dev) return false;
+  if (f64) {
+    c.ext64f = upload(c, ext64f);
+    c.ext64f_digits = d0;
+    c.f64_tables_ok = c.f64_tables_ok && c.ext64f;
+  }
   return t.prime && t.tw_fwd && t.tw_inv && t.p_garner && t.p_mix && t.p_inv && t.p_rinv;
 }
 

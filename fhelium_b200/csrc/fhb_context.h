@@ -101,6 +101,11 @@ struct Context {
   // Q primes are below 2^42): per-prime constants and twiddles as (c, c / q)
   // double pairs; p_rinv holds P mod q (the FP64 core's accumulators carry R)
   ChainTables<double> t64f;
+  // FP64 extension constants of every level's digits for the FP64 rows:
+  // [level][digit][r][2][QP] pairs, [.][0] = (M_r mod p) 2^30 mod p (for the
+  // 30-bit halves of digits that hold a wider prime), [.][1] = M_r mod p
+  TwPair<double>* ext64f = nullptr;
+  int ext64f_digits = 0;  // digits per level in that layout (those of level 0)
   bool f64_tables_ok = false;
   int f64_prime_end = 0;  // Q primes [0, f64_prime_end) are below 2^42 (FP64 rows)
   // tuning: the rows of primes below 2^42 run in FP64 arithmetic (1, default

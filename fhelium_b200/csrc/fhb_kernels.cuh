@@ -714,6 +714,40 @@ struct U64RowSource {
   }
 };
 
+// Exact extension of one digit to prime p in FP64 (the CUDA-core form's
+// source of the forward transform): sum_r d_r (M_r mod p), lazy [0, 2p).
+// Digit words below 2^42 enter whole; a digit that holds a wider prime has
+// its words split into 30-bit halves against (M_r mod p) 2^30 and M_r mod p.
+struct ExtSourceF64 {
+  const uint64_t* dig;        // the digit's first mixed-radix row of this ciphertext
+  const TwPair<double>* ext;  // [r][2][qp0] of this digit, offset by the destination prime id
+  int qp0, alpha, log_n;
+  bool wide;
+  double q, twice_q;
+  template <int C>
+  __device__ __forceinline__ void column(int m, int stride, double (&x)[C]) const {
+    using W = Word<double>;
+#pragma unroll
+    for (int k = 0; k < C; ++k) x[k] = 0.0;
+    for (int r = 0; r < alpha; ++r) {
+      const TwPair<double> lo = ext[int64_t(r * 2 + 1) * qp0];
+      const uint64_t* row = dig + (int64_t(r) << log_n) + m;
+      if (wide) {
+        const TwPair<double> hi = ext[int64_t(r * 2) * qp0];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+          const uint64_t w = row[k * stride];
+          x[k] = csub(x[k] + W::shoup(__ull2double_rn(w >> 30), hi.w, hi.wp, q), twice_q);
+          x[k] = csub(x[k] + W::shoup(__ull2double_rn(w & ((uint64_t{1} << 30) - 1)), lo.w, lo.wp, q), twice_q);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < C; ++k) x[k] = csub(x[k] + W::shoup(__ull2double_rn(row[k * stride]), lo.w, lo.wp, q), twice_q);
+      }
+    }
+  }
+};
+
 struct F64InvEpilogue {
   uint64_t* dst;
   double q, c, cs;
@@ -735,12 +769,17 @@ __device__ __forceinline__ void key_mac_f64(Acc& acc, const double (&v)[E], cons
   }
 }
 
-template <int LOGN>
+// PRE = false (the CUDA-core form): `ext` holds the ModUp digits [B][L][N]
+// and the extension is computed in the transform's source (ExtSourceF64,
+// constants ext64f [level][digit][r][2][QP] of `ext_digits` digits per level;
+// digits that reach prime id f64_end or beyond hold a wide prime).
+template <int LOGN, bool PRE = true>
 __global__ void __launch_bounds__(NttGeom<double, LOGN>::kThreads)
 k_keyswitch_core_f64(const uint64_t* __restrict__ ext, const uint64_t* __restrict__ key, uint64_t* __restrict__ acc0,
                      uint64_t* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
                      int order, const unsigned long long* __restrict__ item_keys, const uint64_t* __restrict__ ct3,
-                     int64_t ct3_stride, ChainTables<double> tabs, LevelTables<uint64_t> lt, int nrows) {
+                     int64_t ct3_stride, ChainTables<double> tabs, LevelTables<uint64_t> lt, int nrows,
+                     const TwPair<double>* __restrict__ ext64f, int ext_digits, int f64_end) {
   using G = NttGeom<double, LOGN>;
   using W = Word<double>;
   static_assert(KsAcc<double, LOGN>::kSmem, "the FP64 core keeps its accumulators in shared memory");
@@ -770,8 +809,13 @@ k_keyswitch_core_f64(const uint64_t* __restrict__ ext, const uint64_t* __restric
       // uniform over the cluster: the own digit's NTT residue is c2 itself
 #pragma unroll
       for (int e = 0; e < G::kE; ++e) v[e] = W::shoup(__ull2double_rn(ct3_own[2 * ct3_stride + e]), p.rinv, p.rinv_s, q);
-    } else {
+    } else if constexpr (PRE) {
       U64RowSource src{ext + ((int64_t(a) * batch + bi) * qp_limbs + jrow) * G::kN};
+      tw.forward_from(src, s, p, v);
+    } else {
+      ExtSourceF64 src{ext + (bi * q_limbs + (d.prime0 - level)) * int64_t(G::kN),
+                       ext64f + (((int64_t(level) * ext_digits + a) * kMaxDigitWidth) * 2) * qp0 + pid, qp0, d.alpha,
+                       LOGN, d.prime0 + d.alpha > f64_end, q, twoq};
       tw.forward_from(src, s, p, v);
     }
     key_mac_f64(acc, v, key0, key1, q, twoq, qinv);

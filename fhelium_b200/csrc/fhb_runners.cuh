@@ -125,26 +125,31 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
                                    (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(), c.ks_order, ik,
                                    (const T*)ct3, ct3_pitch, tables<T>(c), level_tables<T>(c, level), row0, nrows);
   };
-  if (pre) {
-    // extensions from the tensor-core basis conversion (int64 only)
-    if constexpr (sizeof(T) == 8) {
-      if constexpr (KsAcc<double, LOGN>::kSmem) {
-        // the leading Q rows whose primes are below 2^42 in FP64 arithmetic,
-        // the rest (wider Q primes, the P rows) on the integer core
-        const int f64_rows = c.f64_core && c.f64_tables_ok ? std::max(0, std::min(ql, c.f64_prime_end - level)) : 0;
-        if (f64_rows > 0) {
+  if constexpr (sizeof(T) == 8) {
+    if constexpr (KsAcc<double, LOGN>::kSmem) {
+      // the leading Q rows whose primes are below 2^42 in FP64 arithmetic,
+      // the rest (wider Q primes, the P rows) on the integer core
+      const int f64_rows = c.f64_core && c.f64_tables_ok ? std::max(0, std::min(ql, c.f64_prime_end - level)) : 0;
+      if (f64_rows > 0) {
+        auto launch_f64 = [&](auto kern) {
+          return launch_cluster<double, LOGN>(kern, batch * f64_rows, KsAcc<double, LOGN>::smem_bytes(), st,
+                                              (const uint64_t*)digits, (const uint64_t*)key, (uint64_t*)acc0,
+                                              (uint64_t*)acc1, batch, ql, qpl, level, c.qp(), c.ks_order, ik,
+                                              (const uint64_t*)ct3, ct3_pitch, c.t64f,
+                                              level_tables<uint64_t>(c, level), f64_rows, c.ext64f,
+                                              c.ext64f_digits, c.f64_prime_end);
+        };
+        if (pre) {
           if (int rc = launch_int(k_keyswitch_core<T, LOGN, true>, f64_rows, qpl - f64_rows)) return rc;
-          return launch_cluster<double, LOGN>(k_keyswitch_core_f64<LOGN>, batch * f64_rows,
-                                              KsAcc<double, LOGN>::smem_bytes(), st, (const uint64_t*)digits,
-                                              (const uint64_t*)key, (uint64_t*)acc0, (uint64_t*)acc1, batch, ql,
-                                              qpl, level, c.qp(), c.ks_order, ik, (const uint64_t*)ct3, ct3_pitch,
-                                              c.t64f, level_tables<uint64_t>(c, level), f64_rows);
+          return launch_f64(k_keyswitch_core_f64<LOGN, true>);
         }
+        if (int rc = launch_int(k_keyswitch_core<T, LOGN>, f64_rows, qpl - f64_rows)) return rc;
+        return launch_f64(k_keyswitch_core_f64<LOGN, false>);
       }
-      return launch_int(k_keyswitch_core<T, LOGN, true>, 0, qpl);
-    } else {
-      return fail(-7, "the tensor-core basis conversion needs an int64 context");
     }
+    if (pre) return launch_int(k_keyswitch_core<T, LOGN, true>, 0, qpl);  // extensions of the tensor-core form
+  } else {
+    if (pre) return fail(-7, "the tensor-core basis conversion needs an int64 context");
   }
   return launch_int(k_keyswitch_core<T, LOGN>, 0, qpl);
 }

@@ -202,15 +202,18 @@ def test_tc_form_full_ring_batches_and_moddown_variants(batch, tc_moddown):
     np.testing.assert_array_equal(tc[0][:, batch - 1], orc.relinearize(ct3[:, batch - 1], key, level))
 
 
+@pytest.mark.parametrize("form", ["tensor_cores", "cuda_cores"])
 @pytest.mark.parametrize("family,log_n,level,batch", [("int64_logn14", 14, 0, 3), ("int64_logn16", 16, 0, 5),
                                                       ("int64_logn16", 16, 30, 2), ("int64_logn16", 13, 12, 6)])
-def test_f64_core_matches_integer_core(family, log_n, level, batch):
-    """The tensor-core form's key-switch core with its Q rows in exact FP64
-    arithmetic (the default where every Q prime is below 2^42) against the
-    same core on the integer pipe: relinearisation, fused HMult, rotation and
-    mixed-step rotation (per-item keys) integer-equal, and against the oracle."""
+def test_f64_core_matches_integer_core(family, log_n, level, batch, form):
+    """The key-switch core with the Q rows of primes below 2^42 in exact FP64
+    arithmetic (the default), in both basis-conversion forms (the CUDA-core
+    form computes the extensions in FP64 too, splitting the words of digits
+    that hold the wide base prime), against the same core on the integer
+    pipe: relinearisation, fused HMult, rotation and mixed-step rotation
+    (per-item keys) integer-equal, and against the oracle."""
     cfg, eng, orc, rng = _setup(family, log_n, 31)
-    eng.basis_conversion = "tensor_cores"
+    eng.basis_conversion = form
     assert eng.ctx.get_tuning(nat.TUNE_F64_CORE) == 1
     rows = orc.q_rows(level)
     key = random_key(rng, cfg, cfg.N)
