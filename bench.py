@@ -746,7 +746,9 @@ def main() -> int:
     # (the tensor-core form's core is two launches when its Q rows run in FP64:
     # the P rows stay on the integer kernel)
     f64_core = args.basis == "tensor_cores" and bool(eng.ctx.get_tuning(nat.TUNE_F64_CORE))
-    launches_per_step = (7 if f64_core else 6) if args.basis == "tensor_cores" else 5
+    # tensor product, inverse NTT of d2, ModUp digits, (tensor-core extension,) core, ModDown; the FP64 rows of
+    # the NTT and of the core share their launches with the integer rows
+    launches_per_step = 6 if args.basis == "tensor_cores" else 5
 
     # ---- end to end through the public API with host buffers -------------
     host_a = ca.data.cpu().pin_memory()
@@ -902,7 +904,8 @@ def main() -> int:
     # the dominant kernel of the headline form
     dom = "keyswitch_core_extended" if ext is not None else "keyswitch_core"
     dom_kernel = {"keyswitch_core": "k_keyswitch_core",
-                  "keyswitch_core_extended": ("k_keyswitch_core_f64 (Q rows) + k_keyswitch_core<PRE> (P rows)"
+                  "keyswitch_core_extended": ("k_keyswitch_core_split<PRE> (FP64 rows for the primes below 2^42, "
+                                              "int64 rows for the base prime and P)"
                                               if f64_core else "k_keyswitch_core<PRE>")}[dom]
     if dom == "keyswitch_core_extended":
         ext_traffic = KS_F64_TRAFFIC_BYTES_BATCH32 if f64_core else KS_EXT_TRAFFIC_BYTES_BATCH32

@@ -33,7 +33,7 @@ class ItemsPlanInfo(ctypes.Structure):
     _fields_ = [("plan_bytes", ctypes.c_int64), ("scratch_bytes", ctypes.c_int64), ("items", ctypes.c_int32),
                 ("hmult_items", ctypes.c_int32), ("forward_units", ctypes.c_int32),
                 ("inverse_units", ctypes.c_int32), ("core_units", ctypes.c_int32), ("max_limbs", ctypes.c_int32),
-                ("max_digits", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("max_digits", ctypes.c_int32), ("core_f64_units", ctypes.c_int32)]
 
 
 ITEM_HMULT_RELIN_RESCALE, ITEM_ROTATE = 0, 1

@@ -74,6 +74,14 @@ int64_t item_scratch_bytes(const Context& c, const fhb_ks_item& it) {
   return b;
 }
 
+// Leading rows of an item's Q_l whose primes are below 2^42: the key-switch
+// core runs them in FP64 arithmetic (int64 chains with FP64 tables, unless
+// the FP64 core is switched off).
+int f64_item_rows(const Context& c, int level) {
+  if (c.bits != 64 || !c.f64_tables_ok) return 0;
+  return std::max(0, std::min(c.num_q - level, c.f64_prime_end - level));
+}
+
 int check_item(const Context& c, const fhb_ks_item& it, int i) {
   const std::string at = "item " + std::to_string(i) + ": ";
   if (it.kind != FHB_ITEM_HMULT_RELIN_RESCALE && it.kind != FHB_ITEM_ROTATE) return fail(-2, at + "unknown kind");
@@ -89,12 +97,14 @@ int check_item(const Context& c, const fhb_ks_item& it, int i) {
   return 0;
 }
 
-int run_stage(const Context& c, int stage, const ItemsView& iv, const void* units, int64_t count, cudaStream_t st) {
+int run_stage(const Context& c, int stage, const ItemsView& iv, const void* units, int64_t count, cudaStream_t st,
+              int64_t f64_units = 0) {
   if (count == 0) return 0;
-#define FHB_ITEMS_CASE(L)                                                                                  \
-  case L:                                                                                                  \
-    return c.bits == 64 ? run_items<uint64_t, L>(c, stage, iv.items, iv.count, iv.status, units, count, st) \
-                        : run_items<uint32_t, L>(c, stage, iv.items, iv.count, iv.status, units, count, st);
+#define FHB_ITEMS_CASE(L)                                                                                       \
+  case L:                                                                                                       \
+    return c.bits == 64                                                                                         \
+               ? run_items<uint64_t, L>(c, stage, iv.items, iv.count, iv.status, units, count, st, f64_units) \
+               : run_items<uint32_t, L>(c, stage, iv.items, iv.count, iv.status, units, count, st);
   switch (c.log_n) {
     FHB_ITEMS_CASE(12)
     FHB_ITEMS_CASE(13)
@@ -128,7 +138,7 @@ int run_elementwise(const Context& c, const char* plan, const PlanLayout& l, con
   k_items_modup<T, V><<<dim3(xb, unsigned(info.max_digits), unsigned(info.items)), kEwThreads, 0, st>>>(
       iv, level_tables_dev<T>(c), c.num_q, c.log_n, tables<T>(c));
   if (int e = cuda_status(cudaGetLastError(), "k_items_modup")) return e;
-  if (int rc = run_stage(c, 2, iv, plan + l.core_off, info.core_units, st)) return rc;
+  if (int rc = run_stage(c, 2, iv, plan + l.core_off, info.core_units, st, info.core_f64_units)) return rc;
   k_items_moddown<T><<<dim3(unsigned((n + 255) / 256), unsigned(info.items)), 256, 0, st>>>(
       iv, level_tables_dev<T>(c), c.num_q, c.num_p, c.log_n, tables<T>(c));
   return cuda_status(cudaGetLastError(), "k_items_moddown");
@@ -156,6 +166,7 @@ int fhb_ckks_items_plan_info(const fhb_context* ctx, const fhb_ks_item* items, i
     r.max_limbs = std::max(r.max_limbs, l);
     r.max_digits = std::max(r.max_digits, int(c.level_digits[items[i].level].size()));
     r.core_units += l + c.num_p;
+    r.core_f64_units += fhb::f64_item_rows(c, items[i].level);
     if (items[i].kind == FHB_ITEM_HMULT_RELIN_RESCALE) {
       ++r.hmult_items;
       r.forward_units += 4 * l;

@@ -257,13 +257,20 @@ __global__ void k_items_moddown(ItemsView iv, const LevelTables<T>* __restrict__
 
 // Forward NTT of the HMult operands (k_ntt_forward per row): one cluster per
 // unit (item, operand 2 L + component L + row), coefficient/standard ->
-// NTT/Montgomery (x R), lazy [0, 2q), into the item's `ab`.
-template <typename T, int LOGN>
+// NTT/Montgomery (x R), lazy [0, 2q), into the item's `ab`.  SPLIT (int64
+// chains with FP64 tables): the rows whose primes are below 2^42 (prime id
+// < f64_end) run the transform in FP64 arithmetic (as k_ntt_forward's SPLIT
+// form does); their lazy words may differ from the integer transform's by q,
+// which the later stages (all modular, canonical at the end) do not see.
+template <typename T, int LOGN, bool SPLIT = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_items_ntt_forward(ItemsView iv, const ItemUnit* __restrict__ units, int num_q, ChainTables<T> tabs) {
+k_items_ntt_forward(ItemsView iv, const ItemUnit* __restrict__ units, int num_q, ChainTables<T> tabs,
+                    ChainTables<double> tabs64f, int f64_end) {
   using G = NttGeom<T, LOGN>;
+  static_assert(!SPLIT || (sizeof(T) == 8 && NttGeom<double, LOGN>::kC == G::kC &&
+                           NttGeom<double, LOGN>::kThreads == G::kThreads),
+                "the FP64 rows share the integer transform's geometry");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
   // every CTA of the cluster reads the same unit, so an early return is cluster-uniform
   const ItemUnit u = units[blockIdx.x / G::kC];
@@ -280,26 +287,42 @@ k_items_ntt_forward(ItemsView iv, const ItemUnit* __restrict__ units, int num_q,
   }
   const int op = u.row / (2 * limbs), rem = u.row - op * 2 * limbs;  // rem = component L + row
   const int pid = it.level + rem % limbs;
+  const T* in = static_cast<const T*>(op == 0 ? it.a : it.b) + int64_t(rem) * G::kN;
+  T* out = static_cast<T*>(it.ab) + int64_t(u.row) * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  if constexpr (SPLIT) {
+    if (pid < f64_end) {
+      const PrimeInfo<double> p = tabs64f.prime[pid];
+      U64MontSource<true> src{reinterpret_cast<const uint64_t*>(in), p.rmod, p.rmod_s, p.q};
+      double v[G::kE];
+      Ntt<double, LOGN>::forward_from(src, reinterpret_cast<double*>(smem_raw),
+                                      TwGlobal<double, LOGN>(tabs64f.tw_fwd + int64_t(pid) * G::kN), p.q, p.twice_q,
+                                      rank, v);
+#pragma unroll
+      for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+      store_words(reinterpret_cast<uint64_t*>(out), v);
+      return;
+    }
+  }
   const PrimeInfo<T> p = tabs.prime[pid];
-  RowSource<T, true> src{static_cast<const T*>(op == 0 ? it.a : it.b) + int64_t(rem) * G::kN, p.rmod, p.rmod_s,
-                         p.q};
+  RowSource<T, true> src{in, p.rmod, p.rmod_s, p.q};
   T v[G::kE];
-  Ntt<T, LOGN>::forward_from(src, s, TwGlobal<T, LOGN>(tabs.tw_fwd + int64_t(pid) * G::kN), p.q, p.twice_q, rank,
-                             v);
+  Ntt<T, LOGN>::forward_from(src, reinterpret_cast<T*>(smem_raw), TwGlobal<T, LOGN>(tabs.tw_fwd + int64_t(pid) * G::kN),
+                             p.q, p.twice_q, rank, v);
 #pragma unroll
   for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
-  store16(static_cast<T*>(it.ab) + int64_t(u.row) * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
+  store16(out, v);
 }
 
 // Inverse NTT of d2 of the HMult items (k_ntt_inverse per row): one cluster
 // per unit (item, row), NTT/Montgomery -> coefficient/standard canonical,
-// into the item's t0.
-template <typename T, int LOGN>
+// into the item's t0.  SPLIT: rows of primes below 2^42 in FP64 arithmetic
+// (as k_ntt_inverse's SPLIT form), the same canonical words.
+template <typename T, int LOGN, bool SPLIT = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_items_ntt_inverse(ItemsView iv, const ItemUnit* __restrict__ units, int num_q, ChainTables<T> tabs) {
+k_items_ntt_inverse(ItemsView iv, const ItemUnit* __restrict__ units, int num_q, ChainTables<T> tabs,
+                    ChainTables<double> tabs64f, int f64_end) {
   using G = NttGeom<T, LOGN>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
   const ItemUnit u = units[blockIdx.x / G::kC];
   KsItem it;
@@ -314,72 +337,89 @@ k_items_ntt_inverse(ItemsView iv, const ItemUnit* __restrict__ units, int num_q,
     return;
   }
   const int pid = it.level + u.row;
+  const T* in = static_cast<const T*>(it.coef) + int64_t(2 * limbs + u.row) * G::kN + int64_t(rank) * G::kM +
+                threadIdx.x * G::kE;
+  T* out = static_cast<T*>(it.t0) + int64_t(u.row) * G::kN;
+  T w[G::kE];
+  load16(in, w);
+  if constexpr (SPLIT) {
+    if (pid < f64_end) {
+      const PrimeInfo<double> p = tabs64f.prime[pid];
+      double v[G::kE];
+#pragma unroll
+      for (int e = 0; e < G::kE; ++e) v[e] = __ull2double_rn(w[e]);
+      F64OutEpilogue epi{reinterpret_cast<uint64_t*>(out), p.q, p.ninv_rinv, p.ninv_rinv_s, kInvStandard};
+      Ntt<double, LOGN>::inverse(reinterpret_cast<double*>(smem_raw),
+                                 TwGlobal<double, LOGN>(tabs64f.tw_inv + int64_t(pid) * G::kN), p.q, p.twice_q, rank,
+                                 v, epi);
+      return;
+    }
+  }
   const PrimeInfo<T> p = tabs.prime[pid];
-  T v[G::kE];
-  load16(static_cast<const T*>(it.coef) + int64_t(2 * limbs + u.row) * G::kN + int64_t(rank) * G::kM +
-             threadIdx.x * G::kE,
-         v);
-  InvEpilogue<T> epi = make_inv_epilogue<T>(static_cast<T*>(it.t0) + int64_t(u.row) * G::kN, p, kInvStandard, true);
-  Ntt<T, LOGN>::inverse(s, TwGlobal<T, LOGN>(tabs.tw_inv + int64_t(pid) * G::kN), p.q, p.twice_q, rank, v, epi);
+  InvEpilogue<T> epi = make_inv_epilogue<T>(out, p, kInvStandard, true);
+  Ntt<T, LOGN>::inverse(reinterpret_cast<T*>(smem_raw), TwGlobal<T, LOGN>(tabs.tw_inv + int64_t(pid) * G::kN), p.q,
+                        p.twice_q, rank, w, epi);
 }
 
 // Key-switch core of every item (k_keyswitch_core per (ciphertext, row)):
 // one cluster per unit (item, destination row of Q_l P).  For HMult items
 // the NTT-domain ct3 is folded in (c0, c1 as P c_k, own-digit rows from c2).
+// Returns false (status raised) for a unit outside its item's rows.
+__device__ __forceinline__ bool items_core_unit(const ItemsView& iv, const ItemUnit& u, int num_q, int num_p,
+                                                KsItem& it) {
+  if (!items_fetch(iv, u.item, it)) return false;
+  if (u.row < 0 || u.row >= num_q - it.level + num_p) {
+    items_raise(iv.status, kItemsBadRow);
+    return false;
+  }
+  return true;
+}
+
 template <typename T, int LOGN>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_items_core(ItemsView iv, const ItemUnit* __restrict__ units, const LevelTables<T>* __restrict__ levels, int num_q,
              int num_p, ChainTables<T> tabs) {
   using G = NttGeom<T, LOGN>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s = reinterpret_cast<T*>(smem_raw);
-  const int rank = cluster_rank<T, LOGN>();
+  const ItemUnit u = units[blockIdx.x / G::kC];  // the same unit on every CTA of the cluster
+  KsItem it;
+  if (!items_core_unit(iv, u, num_q, num_p, it)) return;
+  const int q_limbs = num_q - it.level;
+  ks_core_unit<T, LOGN, false>(static_cast<const T*>(it.digits), static_cast<const T*>(it.key),
+                               static_cast<T*>(it.t0), static_cast<T*>(it.t1), 1, q_limbs, q_limbs + num_p, it.level,
+                               num_q + num_p, it.kind == 0 ? static_cast<const T*>(it.coef) : nullptr,
+                               int64_t(q_limbs) * G::kN, tabs, levels[it.level], 0, u.row, smem_raw,
+                               cluster_rank<T, LOGN>());
+}
+
+// The same for an int64 chain with FP64 tables: the units of rows whose
+// primes are below 2^42 run the FP64 body (k_keyswitch_core_split), the
+// others the integer body, in one launch.  ext64f [level][digit][r][2][QP]
+// of ext_digits digits per level.
+template <int LOGN>
+__global__ void __launch_bounds__(NttGeom<double, LOGN>::kThreads)
+k_items_core_split(ItemsView iv, const ItemUnit* __restrict__ units, const LevelTables<uint64_t>* __restrict__ levels,
+                   int num_q, int num_p, ChainTables<uint64_t> tabs, ChainTables<double> tabs64f,
+                   const TwPair<double>* __restrict__ ext64f, int ext_digits, int f64_end) {
+  using G = NttGeom<double, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const ItemUnit u = units[blockIdx.x / G::kC];
   KsItem it;
-  if (!items_fetch(iv, u.item, it)) return;
-  const int level = it.level, jrow = u.row, q_limbs = num_q - level, qp0 = num_q + num_p;
-  if (jrow < 0 || jrow >= q_limbs + num_p) {
-    items_raise(iv.status, kItemsBadRow);
-    return;
-  }
-  const int pid = level + jrow;
-  const PrimeInfo<T> p = tabs.prime[pid];
-  const LevelTables<T> lt = levels[level];
-  const T* dig = static_cast<const T*>(it.digits);
-  const T* key = static_cast<const T*>(it.key);
-  T* acc0 = static_cast<T*>(it.t0) + int64_t(jrow) * G::kN;
-  T* acc1 = static_cast<T*>(it.t1) + int64_t(jrow) * G::kN;
-  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
-  KsAcc<T, LOGN> acc(s, acc0 + own, acc1 + own);
-  KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
-  tw.stage(false);
-  const bool add = it.kind == 0 && jrow < q_limbs;
-  const T* ct3_own = add ? static_cast<const T*>(it.coef) + int64_t(jrow) * G::kN + own : nullptr;
-  const int64_t ct3_stride = int64_t(q_limbs) * G::kN;
-  for (int a = 0; a < lt.num_digits; ++a) {
-    const DigitDesc d = lt.digits[a];
-    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
-    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
-    T v[G::kE];
-    if (add && pid >= d.prime0 && pid < d.prime0 + d.alpha) {
-      ks_own_digit_ntt(v, ct3_own, ct3_stride, p);
-    } else {
-      ExtSource<T> src{dig + (int64_t(d.prime0 - level) << LOGN), lt.ext + int64_t(a) * kMaxDigitWidth * qp0 + pid,
-                       qp0, d.alpha, LOGN, p.q, p.twice_q};
-      tw.forward_from(src, s, p, v);
-    }
-    key_mac(acc, v, key0, key1, p);
-  }
-  tw.stage(true);
-  T v[G::kE];
-  acc.get(0, v);
-  if (add) ks_add_p_scaled(v, 0, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
-  InvEpilogue<T> e0 = make_inv_epilogue<T>(acc0, p, kInvStandard, false);
-  tw.inverse(s, p, v, e0);
-  acc.get(1, v);
-  if (add) ks_add_p_scaled(v, 1, ct3_own, ct3_stride, p, tabs.p_rinv[pid]);
-  InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1, p, kInvStandard, false);
-  tw.inverse(s, p, v, e1);
+  if (!items_core_unit(iv, u, num_q, num_p, it)) return;
+  const int q_limbs = num_q - it.level, qp_limbs = q_limbs + num_p, qp0 = num_q + num_p;
+  const uint64_t* ct3 = it.kind == 0 ? static_cast<const uint64_t*>(it.coef) : nullptr;
+  const int rank = cluster_rank<double, LOGN>();
+  const LevelTables<uint64_t> lt = levels[it.level];
+  if (it.level + u.row < f64_end)
+    ks_core_unit_f64<LOGN, false>(static_cast<const uint64_t*>(it.digits), static_cast<const uint64_t*>(it.key),
+                                  static_cast<uint64_t*>(it.t0), static_cast<uint64_t*>(it.t1), 1, q_limbs, qp_limbs,
+                                  it.level, qp0, ct3, int64_t(q_limbs) * G::kN, tabs64f, lt, ext64f, ext_digits,
+                                  f64_end, 0, u.row, smem_raw, rank);
+  else
+    ks_core_unit<uint64_t, LOGN, false>(static_cast<const uint64_t*>(it.digits),
+                                        static_cast<const uint64_t*>(it.key), static_cast<uint64_t*>(it.t0),
+                                        static_cast<uint64_t*>(it.t1), 1, q_limbs, qp_limbs, it.level, qp0, ct3,
+                                        int64_t(q_limbs) * G::kN, tabs, lt, 0, u.row, smem_raw, rank);
 }
 
 }  // namespace fhb

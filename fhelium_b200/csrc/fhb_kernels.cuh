@@ -71,26 +71,84 @@ struct RowSource {
   }
 };
 
-template <typename T, int LOGN, bool TO_MONT, int EPT = 0>
+// FP64 forms of the transforms for the rows of primes below 2^42: residues
+// as exact integers in doubles, Word<double> products on the FP64 pipe,
+// 64-bit words in memory, converted on load and store.
+template <bool TO_MONT>
+struct U64MontSource {
+  const uint64_t* in;
+  double c, cs, q;
+  template <int C>
+  __device__ __forceinline__ void column(int m, int stride, double (&x)[C]) const {
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+      double v = __ull2double_rn(in[k * stride + m]);
+      if constexpr (TO_MONT) v = Word<double>::shoup(v, c, cs, q);
+      x[k] = v;
+    }
+  }
+};
+
+template <int E>
+__device__ __forceinline__ void store_words(uint64_t* p, const double (&v)[E]) {
+  uint64_t w[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) w[e] = __double2ull_rz(v[e]);
+  store16(p, w);
+}
+
+struct F64OutEpilogue {
+  uint64_t* dst;
+  double q, c, cs;
+  int kind;
+  __device__ __forceinline__ void operator()(int pos, double v) const {
+    v = Word<double>::shoup(v, c, cs, q);  // [0, 2q)
+    if (kind >= kInvStandard) v = csub(v, q);
+    if (kind == kInvCentered && v > floor(0.5 * q)) {
+      dst[pos] = uint64_t(__double2ll_rz(v - q));
+      return;
+    }
+    dst[pos] = __double2ull_rz(v);
+  }
+};
+
+// Plain forward NTT of `rows`-row groups of polynomials, one cluster per
+// polynomial.  SPLIT (int64 chains with FP64 tables): the leading f64_rows
+// rows of every group, whose primes are below 2^42, run the transform in
+// FP64 arithmetic in the same launch (a cluster-uniform branch); their lazy
+// outputs equal the integer transform's modulo q.
+template <typename T, int LOGN, bool TO_MONT, int EPT = 0, bool SPLIT = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
-k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start,
-              ChainTables<T> tabs, int sub0, int nsub) {
+k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start, ChainTables<T> tabs,
+              ChainTables<double> tabs64f, int f64_rows) {
   using G = NttGeom<T, LOGN, EPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  // units over the rows [sub0, sub0 + nsub) of every polynomial group of `rows`
-  const int64_t unit = blockIdx.x / G::kC;
-  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
-  const int pid = row_start + int(poly % rows);
+  const int64_t poly = blockIdx.x / G::kC;
+  const int row = int(poly % rows), pid = row_start + row;
+  T* dst = out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  if constexpr (SPLIT) {
+    static_assert(sizeof(T) == 8, "FP64 rows exist in int64 chains only");
+    if (row < f64_rows) {
+      const PrimeInfo<double> p = tabs64f.prime[pid];
+      U64MontSource<TO_MONT> src{reinterpret_cast<const uint64_t*>(in) + poly * G::kN, p.rmod, p.rmod_s, p.q};
+      double v[G::kE];
+      Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::forward_from(
+          src, reinterpret_cast<double*>(smem_raw), tabs64f.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v);
+#pragma unroll
+      for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+      store_words(reinterpret_cast<uint64_t*>(dst), v);
+      return;
+    }
+  }
   const PrimeInfo<T> p = tabs.prime[pid];
   RowSource<T, TO_MONT> src{in + poly * G::kN, p.rmod, p.rmod_s, p.q};
   T v[G::kE];
-  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::forward_from(src, s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q,
-                                                     rank, v);
+  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::forward_from(src, reinterpret_cast<T*>(smem_raw),
+                                                     tabs.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v);
 #pragma unroll
   for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
-  store16(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
+  store16(dst, v);
 }
 
 template <typename T>
@@ -118,112 +176,39 @@ __device__ __forceinline__ InvEpilogue<T> make_inv_epilogue(T* dst, const PrimeI
   return e;
 }
 
-// Plain inverse NTT from NTT/Montgomery lazy input.
-template <typename T, int LOGN, int EPT = 0>
+// Plain inverse NTT from NTT/Montgomery lazy input.  SPLIT: the leading
+// f64_rows rows of every group in FP64 arithmetic, the same output words.
+template <typename T, int LOGN, int EPT = 0, bool SPLIT = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN, EPT>::kThreads)
-k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start, int kind,
-              ChainTables<T> tabs, int sub0, int nsub) {
+k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_start, int kind, ChainTables<T> tabs,
+              ChainTables<double> tabs64f, int f64_rows) {
   using G = NttGeom<T, LOGN, EPT>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
-  const int64_t unit = blockIdx.x / G::kC;
-  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
-  const int pid = row_start + int(poly % rows);
-  const PrimeInfo<T> p = tabs.prime[pid];
-  T v[G::kE];
-  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
-  InvEpilogue<T> epi = make_inv_epilogue<T>(out + poly * G::kN, p, kind, true);
-  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v,
-                                                epi);
-}
-
-// FP64 forms of the plain transforms for the rows of primes below 2^42
-// (residues as exact integers in doubles, Word<double> products on the FP64
-// pipe; 64-bit words in memory, converted on load and store), over the rows
-// [sub0, sub0 + nsub) of every group of `rows`.  Same outputs as the integer
-// kernels.
-template <bool TO_MONT>
-struct U64MontSource {
-  const uint64_t* in;
-  double c, cs, q;
-  template <int C>
-  __device__ __forceinline__ void column(int m, int stride, double (&x)[C]) const {
+  const int64_t poly = blockIdx.x / G::kC;
+  const int row = int(poly % rows), pid = row_start + row;
+  T w[G::kE];
+  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, w);
+  if constexpr (SPLIT) {
+    static_assert(sizeof(T) == 8, "FP64 rows exist in int64 chains only");
+    if (row < f64_rows) {
+      const PrimeInfo<double> p = tabs64f.prime[pid];
+      double v[G::kE];
 #pragma unroll
-    for (int k = 0; k < C; ++k) {
-      double v = __ull2double_rn(in[k * stride + m]);
-      if constexpr (TO_MONT) v = Word<double>::shoup(v, c, cs, q);
-      x[k] = v;
-    }
-  }
-};
-
-template <int E>
-__device__ __forceinline__ void store_words(uint64_t* p, const double (&v)[E]) {
-  uint64_t w[E];
-#pragma unroll
-  for (int e = 0; e < E; ++e) w[e] = __double2ull_rz(v[e]);
-  store16(p, w);
-}
-
-template <int LOGN, bool TO_MONT, int EPT = 0>
-__global__ void __launch_bounds__(NttGeom<double, LOGN, EPT>::kThreads)
-k_ntt_forward_f64(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int rows, int row_start,
-                  ChainTables<double> tabs, int sub0, int nsub) {
-  using G = NttGeom<double, LOGN, EPT>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* s = reinterpret_cast<double*>(smem_raw);
-  const int rank = cluster_rank<double, LOGN>();
-  const int64_t unit = blockIdx.x / G::kC;
-  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
-  const int pid = row_start + int(poly % rows);
-  const PrimeInfo<double> p = tabs.prime[pid];
-  U64MontSource<TO_MONT> src{in + poly * G::kN, p.rmod, p.rmod_s, p.q};
-  double v[G::kE];
-  Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::forward_from(src, s, tabs.tw_fwd + int64_t(pid) * G::kN, p.q,
-                                                                p.twice_q, rank, v);
-#pragma unroll
-  for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
-  store_words(out + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, v);
-}
-
-struct F64OutEpilogue {
-  uint64_t* dst;
-  double q, c, cs;
-  int kind;
-  __device__ __forceinline__ void operator()(int pos, double v) const {
-    v = Word<double>::shoup(v, c, cs, q);  // [0, 2q)
-    if (kind >= kInvStandard) v = csub(v, q);
-    if (kind == kInvCentered && v > floor(0.5 * q)) {
-      dst[pos] = uint64_t(__double2ll_rz(v - q));
+      for (int e = 0; e < G::kE; ++e) v[e] = __ull2double_rn(w[e]);
+      const bool std_out = kind != kInvMontgomery;  // N^-1 R^-1 unless the output stays Montgomery
+      F64OutEpilogue epi{reinterpret_cast<uint64_t*>(out) + poly * G::kN, p.q, std_out ? p.ninv_rinv : p.ninv,
+                         std_out ? p.ninv_rinv_s : p.ninv_s, kind};
+      Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::inverse(reinterpret_cast<double*>(smem_raw),
+                                                               tabs64f.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q,
+                                                               rank, v, epi);
       return;
     }
-    dst[pos] = __double2ull_rz(v);
   }
-};
-
-template <int LOGN, int EPT = 0>
-__global__ void __launch_bounds__(NttGeom<double, LOGN, EPT>::kThreads)
-k_ntt_inverse_f64(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int rows, int row_start, int kind,
-                  ChainTables<double> tabs, int sub0, int nsub) {
-  using G = NttGeom<double, LOGN, EPT>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* s = reinterpret_cast<double*>(smem_raw);
-  const int rank = cluster_rank<double, LOGN>();
-  const int64_t unit = blockIdx.x / G::kC;
-  const int64_t poly = unit / nsub * rows + sub0 + unit % nsub;
-  const int pid = row_start + int(poly % rows);
-  const PrimeInfo<double> p = tabs.prime[pid];
-  uint64_t w[G::kE];
-  load16(in + poly * G::kN + int64_t(rank) * G::kM + threadIdx.x * G::kE, w);
-  double v[G::kE];
-#pragma unroll
-  for (int e = 0; e < G::kE; ++e) v[e] = __ull2double_rn(w[e]);
-  const bool std_out = kind != kInvMontgomery;  // Montgomery NTT input: N^-1 R^-1 unless the output stays Montgomery
-  F64OutEpilogue epi{out + poly * G::kN, p.q, std_out ? p.ninv_rinv : p.ninv, std_out ? p.ninv_rinv_s : p.ninv_s,
-                     kind};
-  Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::inverse(s, tabs.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q, rank,
-                                                           v, epi);
+  const PrimeInfo<T> p = tabs.prime[pid];
+  InvEpilogue<T> epi = make_inv_epilogue<T>(out + poly * G::kN, p, kind, true);
+  Ntt<T, LOGN, TwGlobal<T, LOGN>, EPT>::inverse(reinterpret_cast<T*>(smem_raw), tabs.tw_inv + int64_t(pid) * G::kN,
+                                                p.q, p.twice_q, rank, w, epi);
 }
 
 // ---------------------------------------------------------------------------
@@ -632,29 +617,21 @@ __device__ __forceinline__ void ks_own_digit_ntt(T (&v)[E], const T* ct3, int64_
 // the int8 tensor-core basis conversion, [D_l][B][QP_l][N] in [0, 2p), so
 // the source of each forward NTT is a plain row read instead of the
 // extension sum.
-template <typename T, int LOGN, bool PRE = false>
-__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
-                 T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
-                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ ct3, int64_t ct3_stride,
-                 ChainTables<T> tabs, LevelTables<T> lt, int row0, int nrows) {
+// One unit (ciphertext bi, row jrow of Q_l P) of the key-switch core.
+template <typename T, int LOGN, bool PRE>
+__device__ __forceinline__ void ks_core_unit(const T* __restrict__ digits, const T* __restrict__ key,
+                                             T* __restrict__ acc0, T* __restrict__ acc1, int64_t batch, int q_limbs,
+                                             int qp_limbs, int level, int qp0, const T* __restrict__ ct3,
+                                             int64_t ct3_stride, const ChainTables<T>& tabs, const LevelTables<T>& lt,
+                                             int64_t bi, int jrow, unsigned char* smem_raw, int rank) {
   using G = NttGeom<T, LOGN>;
-  using W = Word<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
-  const int rank = cluster_rank<T, LOGN>();
-  // units over [B, rows row0 .. row0 + nrows) of QP_l; poly over [B, QP_l]
-  int64_t poly, bi;
-  int jrow;
-  ks_work(blockIdx.x / G::kC, nrows, batch, order, poly, bi, jrow);
-  jrow += row0;
-  poly = bi * qp_limbs + jrow;
+  const int64_t poly = bi * qp_limbs + jrow;
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
   const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
   const T* dig = digits + bi * q_limbs * int64_t(G::kN);
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
-  if (item_keys) key = reinterpret_cast<const T*>(item_keys[bi]);  // mixed-key batch
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
@@ -690,21 +667,34 @@ k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __r
   tw.inverse(s, p, v, e1);
 }
 
+template <typename T, int LOGN, bool PRE = false>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_keyswitch_core(const T* __restrict__ digits, const T* __restrict__ key, T* __restrict__ acc0,
+                 T* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0, int order,
+                 const unsigned long long* __restrict__ item_keys, const T* __restrict__ ct3, int64_t ct3_stride,
+                 ChainTables<T> tabs, LevelTables<T> lt) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int64_t poly, bi;
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  if (item_keys) key = reinterpret_cast<const T*>(item_keys[bi]);  // mixed-key batch
+  ks_core_unit<T, LOGN, PRE>(digits, key, acc0, acc1, batch, q_limbs, qp_limbs, level, qp0, ct3, ct3_stride, tabs,
+                             lt, bi, jrow, smem_raw, cluster_rank<T, LOGN>());
+}
+
 // ---------------------------------------------------------------------------
-// The key-switch core of the tensor-core form for the Q rows, in FP64
-// arithmetic (int64 chains whose Q primes are below 2^42, rings up to
-// N = 2^16 so the accumulators live in shared memory).  Residues are held as
-// exact integers in doubles and every product is Word<double>'s exact
-// product, so the butterflies run on the FP64 pipe instead of the integer
-// multiply-add pipe; inputs and outputs stay 64-bit words in global memory,
-// converted on load and store.  The key words are used as stored (k R, the
-// Montgomery form), so the accumulators carry a factor R, removed with
-// N^{-1} R^{-1} in the inverse transform's epilogue; for relinearisation
-// the addends enter as P c R (ct3 holds c R, tabs.p_rinv holds P mod q here)
-// and an own-digit row as c2 = (c2 R) R^{-1}.  The outputs are the integer
-// kernel's word for word.  ext: the extensions [D_l][B][QP_l][N] of the
-// tensor-core basis conversion; units over [B, nrows], the leading Q rows
-// whose primes are below 2^42.
+// The key-switch core's rows whose primes are below 2^42, in FP64
+// arithmetic (int64 chains, rings up to N = 2^16 so the accumulators live in
+// shared memory).  Residues are held as exact integers in doubles and every
+// product is Word<double>'s exact product, so the butterflies run on the
+// FP64 pipe instead of the integer multiply-add pipe; inputs and outputs
+// stay 64-bit words in global memory, converted on load and store.  The key
+// words are used as stored (k R, the Montgomery form), so the accumulators
+// carry a factor R, removed with N^{-1} R^{-1} in the inverse transform's
+// epilogue; for relinearisation the addends enter as P c R (ct3 holds c R,
+// tabs.p_rinv holds P mod q in the FP64 tables) and an own-digit row as
+// c2 = (c2 R) R^{-1}.  The outputs are the integer core's words.
 struct U64RowSource {
   const uint64_t* in;
   template <int C>
@@ -769,32 +759,31 @@ __device__ __forceinline__ void key_mac_f64(Acc& acc, const double (&v)[E], cons
   }
 }
 
-// PRE = false (the CUDA-core form): `ext` holds the ModUp digits [B][L][N]
-// and the extension is computed in the transform's source (ExtSourceF64,
-// constants ext64f [level][digit][r][2][QP] of `ext_digits` digits per level;
-// digits that reach prime id f64_end or beyond hold a wide prime).
-template <int LOGN, bool PRE = true>
-__global__ void __launch_bounds__(NttGeom<double, LOGN>::kThreads)
-k_keyswitch_core_f64(const uint64_t* __restrict__ ext, const uint64_t* __restrict__ key, uint64_t* __restrict__ acc0,
-                     uint64_t* __restrict__ acc1, int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
-                     int order, const unsigned long long* __restrict__ item_keys, const uint64_t* __restrict__ ct3,
-                     int64_t ct3_stride, ChainTables<double> tabs, LevelTables<uint64_t> lt, int nrows,
-                     const TwPair<double>* __restrict__ ext64f, int ext_digits, int f64_end) {
+// One unit (ciphertext bi, Q row jrow) of the FP64 core.  PRE (tensor-core
+// form): `ext` holds the extensions [D_l][B][QP_l][N] of the tensor-core
+// basis conversion.  PRE = false (CUDA-core form): `ext` holds the ModUp
+// digits [B][L][N] and the extension is computed in the transform's source
+// (ExtSourceF64, constants ext64f [level][digit][r][2][QP] of `ext_digits`
+// digits per level; digits that reach prime id f64_end or beyond hold a wide
+// prime).
+template <int LOGN, bool PRE>
+__device__ __forceinline__ void ks_core_unit_f64(const uint64_t* __restrict__ ext, const uint64_t* __restrict__ key,
+                                                 uint64_t* __restrict__ acc0, uint64_t* __restrict__ acc1,
+                                                 int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
+                                                 const uint64_t* __restrict__ ct3, int64_t ct3_stride,
+                                                 const ChainTables<double>& tabs, const LevelTables<uint64_t>& lt,
+                                                 const TwPair<double>* __restrict__ ext64f, int ext_digits,
+                                                 int f64_end, int64_t bi, int jrow, unsigned char* smem_raw,
+                                                 int rank) {
   using G = NttGeom<double, LOGN>;
   using W = Word<double>;
   static_assert(KsAcc<double, LOGN>::kSmem, "the FP64 core keeps its accumulators in shared memory");
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   double* s = reinterpret_cast<double*>(smem_raw);
-  const int rank = cluster_rank<double, LOGN>();
-  int64_t poly, bi;
-  int jrow;
-  ks_work(blockIdx.x / G::kC, nrows, batch, order, poly, bi, jrow);  // rows [0, nrows) of Q_l
-  poly = bi * qp_limbs + jrow;
+  const int64_t poly = bi * qp_limbs + jrow;
   const int pid = level + jrow;
   const PrimeInfo<double> p = tabs.prime[pid];
   const double q = p.q, twoq = p.twice_q, qinv = p.one_s;
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
-  if (item_keys) key = reinterpret_cast<const uint64_t*>(item_keys[bi]);  // mixed-key batch
   KsAcc<double, LOGN> acc(s, nullptr, nullptr);
   KsTw<double, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
@@ -833,6 +822,36 @@ k_keyswitch_core_f64(const uint64_t* __restrict__ ext, const uint64_t* __restric
     F64InvEpilogue epi{(c ? acc1 : acc0) + poly * G::kN, q, p.ninv_rinv, p.ninv_rinv_s};
     tw.inverse(s, p, v, epi);
   }
+}
+
+// The whole key-switch core of an int64 chain in one launch: the units of
+// the leading f64_rows Q rows (primes below 2^42) run the FP64 body, the
+// others (wider Q primes, the P rows) the integer body.  The branch is
+// uniform over a cluster, and one launch lets the two kinds of units share
+// the GPU instead of running one after the other.
+template <int LOGN, bool PRE>
+__global__ void __launch_bounds__(NttGeom<double, LOGN>::kThreads)
+k_keyswitch_core_split(const uint64_t* __restrict__ digits, const uint64_t* __restrict__ key,
+                       uint64_t* __restrict__ acc0, uint64_t* __restrict__ acc1, int64_t batch, int q_limbs,
+                       int qp_limbs, int level, int qp0, int order, const unsigned long long* __restrict__ item_keys,
+                       const uint64_t* __restrict__ ct3, int64_t ct3_stride, ChainTables<uint64_t> tabs,
+                       LevelTables<uint64_t> lt, ChainTables<double> tabs64f, int f64_rows,
+                       const TwPair<double>* __restrict__ ext64f, int ext_digits, int f64_end) {
+  using G = NttGeom<double, LOGN>;
+  static_assert(NttGeom<uint64_t, LOGN>::kC == G::kC && NttGeom<uint64_t, LOGN>::kThreads == G::kThreads,
+                "one geometry for both bodies");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int64_t poly, bi;
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  if (item_keys) key = reinterpret_cast<const uint64_t*>(item_keys[bi]);  // mixed-key batch
+  const int rank = cluster_rank<double, LOGN>();
+  if (jrow < f64_rows)
+    ks_core_unit_f64<LOGN, PRE>(digits, key, acc0, acc1, batch, q_limbs, qp_limbs, level, qp0, ct3, ct3_stride,
+                                tabs64f, lt, ext64f, ext_digits, f64_end, bi, jrow, smem_raw, rank);
+  else
+    ks_core_unit<uint64_t, LOGN, PRE>(digits, key, acc0, acc1, batch, q_limbs, qp_limbs, level, qp0, ct3,
+                                      ct3_stride, tabs, lt, bi, jrow, smem_raw, rank);
 }
 
 // Sum of key switches of several ciphertexts with their own keys, reduced

@@ -50,24 +50,17 @@ constexpr size_t ntt_smem() {
 template <typename T, int LOGN, int EPT>
 int run_forward_e(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, bool mont,
                   cudaStream_t st) {
-  const int64_t groups = polys / rows;
-  // the leading rows of primes below 2^42 in FP64 arithmetic (int64 chains)
+  // the leading rows of primes below 2^42 in FP64 arithmetic (int64 chains), same launch
   const int k = sizeof(T) == 8 ? f64_rows(c, row_start, rows) : 0;
-  auto launch_int = [&](auto kern, int sub0, int nsub) {
-    return launch_cluster<T, LOGN, EPT>(kern, groups * nsub, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out, rows,
-                                        row_start, tables<T>(c), sub0, nsub);
+  auto launch = [&](auto kern) {
+    return launch_cluster<T, LOGN, EPT>(kern, polys, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out, rows, row_start,
+                                        tables<T>(c), c.t64f, k);
   };
-  auto launch_f64 = [&](auto kern) {
-    return launch_cluster<double, LOGN, EPT>(kern, groups * k, ntt_smem<double, LOGN>(), st, (const uint64_t*)in,
-                                             (uint64_t*)out, rows, row_start, c.t64f, 0, k);
-  };
-  if (k < rows) {
-    const int rc = mont ? launch_int(k_ntt_forward<T, LOGN, false, EPT>, k, rows - k)
-                        : launch_int(k_ntt_forward<T, LOGN, true, EPT>, k, rows - k);
-    if (rc) return rc;
+  if constexpr (sizeof(T) == 8) {
+    if (k > 0)
+      return mont ? launch(k_ntt_forward<T, LOGN, false, EPT, true>) : launch(k_ntt_forward<T, LOGN, true, EPT, true>);
   }
-  if (k == 0) return 0;
-  return mont ? launch_f64(k_ntt_forward_f64<LOGN, false, EPT>) : launch_f64(k_ntt_forward_f64<LOGN, true, EPT>);
+  return mont ? launch(k_ntt_forward<T, LOGN, false, EPT>) : launch(k_ntt_forward<T, LOGN, true, EPT>);
 }
 
 template <typename T, int LOGN>
@@ -80,17 +73,15 @@ int run_forward(const Context& c, const void* in, void* out, int64_t polys, int 
 template <typename T, int LOGN, int EPT>
 int run_inverse_e(const Context& c, const void* in, void* out, int64_t polys, int rows, int row_start, int kind,
                   cudaStream_t st) {
-  const int64_t groups = polys / rows;
   const int k = sizeof(T) == 8 ? f64_rows(c, row_start, rows) : 0;
-  if (k < rows) {
-    const int rc = launch_cluster<T, LOGN, EPT>(k_ntt_inverse<T, LOGN, EPT>, groups * (rows - k), ntt_smem<T, LOGN>(),
-                                                st, (const T*)in, (T*)out, rows, row_start, kind, tables<T>(c), k,
-                                                rows - k);
-    if (rc) return rc;
+  auto launch = [&](auto kern) {
+    return launch_cluster<T, LOGN, EPT>(kern, polys, ntt_smem<T, LOGN>(), st, (const T*)in, (T*)out, rows, row_start,
+                                        kind, tables<T>(c), c.t64f, k);
+  };
+  if constexpr (sizeof(T) == 8) {
+    if (k > 0) return launch(k_ntt_inverse<T, LOGN, EPT, true>);
   }
-  if (k == 0) return 0;
-  return launch_cluster<double, LOGN, EPT>(k_ntt_inverse_f64<LOGN, EPT>, groups * k, ntt_smem<double, LOGN>(), st,
-                                           (const uint64_t*)in, (uint64_t*)out, rows, row_start, kind, c.t64f, 0, k);
+  return launch(k_ntt_inverse<T, LOGN, EPT>);
 }
 
 template <typename T, int LOGN>
@@ -119,39 +110,35 @@ int run_ks_core(const Context& c, const void* digits, const void* key, void* acc
   const int ql = c.num_q - level, qpl = ql + c.num_p;
   if (ct3_pitch <= 0) ct3_pitch = batch * ql * int64_t(c.n());  // component pitch of ct3 [3, batch, L, N]
   const auto* ik = reinterpret_cast<const unsigned long long*>(item_keys);
-  // the integer core over rows [row0, row0 + nrows) of Q_l P
-  auto launch_int = [&](auto kern, int row0, int nrows) {
-    return launch_cluster<T, LOGN>(kern, batch * nrows, KsAcc<T, LOGN>::smem_bytes(), st, (const T*)digits,
+  auto launch_int = [&](auto kern) {
+    return launch_cluster<T, LOGN>(kern, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st, (const T*)digits,
                                    (const T*)key, (T*)acc0, (T*)acc1, batch, ql, qpl, level, c.qp(), c.ks_order, ik,
-                                   (const T*)ct3, ct3_pitch, tables<T>(c), level_tables<T>(c, level), row0, nrows);
+                                   (const T*)ct3, ct3_pitch, tables<T>(c), level_tables<T>(c, level));
   };
   if constexpr (sizeof(T) == 8) {
     if constexpr (KsAcc<double, LOGN>::kSmem) {
+      static_assert(KsAcc<double, LOGN>::smem_bytes() == KsAcc<T, LOGN>::smem_bytes(), "one smem size for both");
       // the leading Q rows whose primes are below 2^42 in FP64 arithmetic,
-      // the rest (wider Q primes, the P rows) on the integer core
+      // the rest (wider Q primes, the P rows) on the integer body, one launch
       const int f64_rows = c.f64_core && c.f64_tables_ok ? std::max(0, std::min(ql, c.f64_prime_end - level)) : 0;
       if (f64_rows > 0) {
-        auto launch_f64 = [&](auto kern) {
-          return launch_cluster<double, LOGN>(kern, batch * f64_rows, KsAcc<double, LOGN>::smem_bytes(), st,
+        auto launch_split = [&](auto kern) {
+          return launch_cluster<double, LOGN>(kern, batch * qpl, KsAcc<double, LOGN>::smem_bytes(), st,
                                               (const uint64_t*)digits, (const uint64_t*)key, (uint64_t*)acc0,
                                               (uint64_t*)acc1, batch, ql, qpl, level, c.qp(), c.ks_order, ik,
-                                              (const uint64_t*)ct3, ct3_pitch, c.t64f,
-                                              level_tables<uint64_t>(c, level), f64_rows, c.ext64f,
+                                              (const uint64_t*)ct3, ct3_pitch, tables<uint64_t>(c),
+                                              level_tables<uint64_t>(c, level), c.t64f, f64_rows, c.ext64f,
                                               c.ext64f_digits, c.f64_prime_end);
         };
-        if (pre) {
-          if (int rc = launch_int(k_keyswitch_core<T, LOGN, true>, f64_rows, qpl - f64_rows)) return rc;
-          return launch_f64(k_keyswitch_core_f64<LOGN, true>);
-        }
-        if (int rc = launch_int(k_keyswitch_core<T, LOGN>, f64_rows, qpl - f64_rows)) return rc;
-        return launch_f64(k_keyswitch_core_f64<LOGN, false>);
+        return pre ? launch_split(k_keyswitch_core_split<LOGN, true>)
+                   : launch_split(k_keyswitch_core_split<LOGN, false>);
       }
     }
-    if (pre) return launch_int(k_keyswitch_core<T, LOGN, true>, 0, qpl);  // extensions of the tensor-core form
+    if (pre) return launch_int(k_keyswitch_core<T, LOGN, true>);  // extensions of the tensor-core form
   } else {
     if (pre) return fail(-7, "the tensor-core basis conversion needs an int64 context");
   }
-  return launch_int(k_keyswitch_core<T, LOGN>, 0, qpl);
+  return launch_int(k_keyswitch_core<T, LOGN>);
 }
 
 template <typename T, int LOGN>
@@ -195,15 +182,34 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
 // ---- mixed-level item stages (fhb_items.cuh): one cluster per unit ----------
 template <typename T, int LOGN>
 int run_items(const Context& c, int stage, const void* items, int item_count, int* status, const void* units,
-              int64_t count, cudaStream_t st) {
+              int64_t count, cudaStream_t st, int64_t f64_units) {
   const ItemsView iv{static_cast<const KsItem*>(items), item_count, status};
   const auto* un = static_cast<const ItemUnit*>(units);
-  if (stage == 0)
-    return launch_cluster<T, LOGN>(k_items_ntt_forward<T, LOGN>, count, ntt_smem<T, LOGN>(), st, iv, un, c.num_q,
-                                   tables<T>(c));
-  if (stage == 1)
-    return launch_cluster<T, LOGN>(k_items_ntt_inverse<T, LOGN>, count, ntt_smem<T, LOGN>(), st, iv, un, c.num_q,
-                                   tables<T>(c));
+  // int64 chains with FP64 tables: the rows of primes below 2^42 in FP64 arithmetic
+  const bool split = sizeof(T) == 8 && c.f64_core && c.f64_tables_ok && c.f64_prime_end > 0;
+  if (stage < 2) {
+    auto launch = [&](auto kern) {
+      return launch_cluster<T, LOGN>(kern, count, ntt_smem<T, LOGN>(), st, iv, un, c.num_q, tables<T>(c), c.t64f,
+                                     c.f64_prime_end);
+    };
+    if constexpr (sizeof(T) == 8) {
+      if (split)
+        return stage == 0 ? launch(k_items_ntt_forward<T, LOGN, true>) : launch(k_items_ntt_inverse<T, LOGN, true>);
+    }
+    return stage == 0 ? launch(k_items_ntt_forward<T, LOGN>) : launch(k_items_ntt_inverse<T, LOGN>);
+  }
+  // stage 2, the key-switch core; on an int64 chain with FP64 tables the
+  // units of rows whose primes are below 2^42 run in FP64 arithmetic
+  if constexpr (sizeof(T) == 8) {
+    if constexpr (KsAcc<double, LOGN>::kSmem) {
+      static_assert(KsAcc<double, LOGN>::smem_bytes() == KsAcc<T, LOGN>::smem_bytes(), "one smem size for both");
+      if (split && f64_units > 0)
+        return launch_cluster<double, LOGN>(k_items_core_split<LOGN>, count, KsAcc<double, LOGN>::smem_bytes(), st,
+                                            iv, un, level_tables_dev<uint64_t>(c), c.num_q, c.num_p,
+                                            tables<uint64_t>(c), c.t64f, c.ext64f, c.ext64f_digits,
+                                            c.f64_prime_end);
+    }
+  }
   return launch_cluster<T, LOGN>(k_items_core<T, LOGN>, count, KsAcc<T, LOGN>::smem_bytes(), st, iv, un,
                                  level_tables_dev<T>(c), c.num_q, c.num_p, tables<T>(c));
 }
@@ -218,7 +224,8 @@ int run_items(const Context& c, int stage, const void* items, int item_count, in
   template int run_ks_sum<T, LOGN>(const Context&, const void*, const uint64_t*, void*, void*, int, int64_t, int, \
                                    cudaStream_t, bool);                                                         \
   template int run_prepare<T, LOGN>(const Context&, const void*, void*, int64_t, int, cudaStream_t);            \
-  template int run_items<T, LOGN>(const Context&, int, const void*, int, int*, const void*, int64_t, cudaStream_t); \
+  template int run_items<T, LOGN>(const Context&, int, const void*, int, int*, const void*, int64_t, cudaStream_t, \
+                                  int64_t);                                                                     \
   template int run_apply_prepared<T, LOGN>(const Context&, const void*, const void*, void*, void*, int64_t, int, \
                                            uint32_t, cudaStream_t);
 

@@ -23,10 +23,11 @@ template <typename T, int LOGN>
 int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, void* acc0, void* acc1, int giants,
                int64_t batch, int level, cudaStream_t st, bool pre);
 // Mixed-level item stages: 0 = forward NTT of the HMult operands, 1 =
-// inverse NTT of d2, 2 = key-switch core; `count` units of `units`.
+// inverse NTT of d2, 2 = key-switch core; `count` units of `units`, of
+// which the leading `f64_units` (stage 2) may run in FP64 arithmetic.
 template <typename T, int LOGN>
 int run_items(const Context& c, int stage, const void* items, int item_count, int* status, const void* units,
-              int64_t count, cudaStream_t st);
+              int64_t count, cudaStream_t st, int64_t f64_units = 0);
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level, cudaStream_t st);
 template <typename T, int LOGN>

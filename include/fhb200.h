@@ -406,7 +406,8 @@ typedef struct fhb_ks_item {
 typedef struct fhb_items_plan_info {
   int64_t plan_bytes;     /* device bytes of the plan */
   int64_t scratch_bytes;  /* device scratch bytes of the items */
-  int32_t items, hmult_items, forward_units, inverse_units, core_units, max_limbs, max_digits, reserved;
+  int32_t items, hmult_items, forward_units, inverse_units, core_units, max_limbs, max_digits;
+  int32_t core_f64_units; /* key-switch units whose rows' primes are below 2^42 (run in FP64 arithmetic) */
 } fhb_items_plan_info;
 int fhb_ckks_items_plan_info(const fhb_context* ctx, const fhb_ks_item* items, int count, fhb_items_plan_info* info);
 int fhb_ckks_items_plan(const fhb_context* ctx, const fhb_ks_item* items, int count, void* plan, void* scratch,

@@ -63,6 +63,29 @@ def test_items_bit_exact(small, use_graph):
         assert torch.equal(got.data, w.data), f"op {i} ({ops[i]}) differs"
 
 
+def test_items_f64_core_matches_integer_core(small):
+    """The items' rows of primes below 2^42 run the FP64 key-switch body, the
+    others the integer body, in one launch.  With the FP64 core switched off
+    every unit runs the integer core: the residues are the same."""
+    from fhelium_b200 import _native as nat
+    eng, cts, ops, want = small
+    ex = MixedItemsExecutor(eng, cts, ops, use_graph=False)
+    info = ex.chunks[0][0]
+    assert 0 < info.core_f64_units < info.core_units
+    try:
+        for flag in (0, 1):
+            eng.ctx.set_tuning(nat.TUNE_F64_CORE, flag)
+            for i in range(len(want)):
+                ex._outs[i].zero_()
+            ex.run()
+            torch.cuda.synchronize()
+            assert ex.status() == 0
+            for i, w in enumerate(want):
+                assert torch.equal(ex.result(i).data, w.data), (flag, i, ops[i])
+    finally:
+        eng.ctx.set_tuning(nat.TUNE_F64_CORE, 1)
+
+
 def test_items_work_orders_and_autotune(small, tmp_path):
     """Both key-switch work orders of the items plan give the same residues;
     the autotuner picks among (order, scratch limit) and caches the winner."""
