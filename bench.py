@@ -55,8 +55,10 @@ KS_TRAFFIC_BYTES_BATCH32 = 12741399552 + 2934590720  # ncu dram read + write, k_
 # same for the key-switch core of the tensor-core form: captured at batch 8 (3094038784 + 705889536 bytes,
 # 2.01x the batch-4 capture) and scaled by the ciphertexts processed
 KS_EXT_TRAFFIC_BYTES_BATCH32 = 4 * (3094038784 + 705889536)
-# same for the FP64 form of that core (Q rows) with its P-row launch (not yet captured)
-KS_F64_TRAFFIC_BYTES_BATCH32 = None
+# same for that core with its FP64 rows (k_keyswitch_core_split): captured at batch 8 (3085136640 + 355092224
+# bytes; the key and digit rows are re-read per group of four ciphertexts, so the traffic grows with the batch)
+# and scaled by the ciphertexts processed
+KS_F64_TRAFFIC_BYTES_BATCH32 = 4 * (3085136640 + 355092224)
 METRIC = "hmult_relin_rescale_ops_per_s_logN16_L35"
 UNIT = "ops/s"
 CONFIG = {
