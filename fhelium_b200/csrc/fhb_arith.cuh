@@ -75,13 +75,39 @@ struct Word<double> {
     const T r = fma(-qt, q, h) + l;
     return r < 0.0 ? r + q : r;
   }
-  // The same with the quotient taken from h and qinv = 1 / q (for products
-  // of two residues, where no per-word companion exists): x, w < 2q.
+  // The same with the quotient taken from h and qinv = 1 / q rounded (for
+  // products of two residues, and for twiddles stored without a companion):
+  // h qinv carries a relative error below 2^-51, so for x w / q < 2^47 the
+  // estimate is again within one of floor(x w / q).
   __device__ __forceinline__ static T mul_qinv(T x, T w, T q, T qinv) {
     const T h = x * w;
     const T l = fma(x, w, -h);
     const T qt = floor(h * qinv);
     const T r = fma(-qt, q, h) + l;
+    return r < 0.0 ? r + q : r;
+  }
+  // Balanced forms for signed residues (the FP64 transforms): the quotient
+  // estimate rounded to nearest.  Its relative error is below 2^-51, so for
+  // |x w / q| < 2^47 it is within 0.05 of x w / q and the result x w - qt q
+  // lies in (-0.55 q, 0.55 q) with no correction, exactly (every
+  // intermediate is an integer below 2^53).
+  __device__ __forceinline__ static T shoup_bal(T x, T w, T wc, T q) {
+    const T h = x * w;
+    const T l = fma(x, w, -h);
+    const T qt = rint(x * wc);
+    return fma(-qt, q, h) + l;
+  }
+  __device__ __forceinline__ static T mul_qinv_bal(T x, T w, T q, T qinv) {
+    const T h = x * w;
+    const T l = fma(x, w, -h);
+    const T qt = rint(h * qinv);
+    return fma(-qt, q, h) + l;
+  }
+  // x - rint(x / q) q for an integer |x| < 2^50: in (-0.51 q, 0.51 q), exact.
+  __device__ __forceinline__ static T reduce_bal(T x, T q, T qinv) { return fma(-rint(x * qinv), q, x); }
+  // A balanced value to the lazy unsigned range [0, 2q) (|x| < 2^50).
+  __device__ __forceinline__ static T to_lazy(T x, T q, T qinv) {
+    const T r = reduce_bal(x, q, qinv);
     return r < 0.0 ? r + q : r;
   }
 };

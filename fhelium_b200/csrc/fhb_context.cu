@@ -143,9 +143,11 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
   t.prime = upload(c, info);
   t.tw_fwd = upload(c, fwd);
   t.tw_inv = upload(c, inv);
-  // FP64 tables of the tensor-core form's key-switch core: the same constants
-  // and twiddles as (c, c / q) double pairs, for int64 chains whose leading Q
-  // primes are below 2^42 (the rows of wider primes keep the integer tables)
+  // FP64 tables of the rows of primes below 2^42 (int64 chains whose leading
+  // Q primes are that narrow; the rows of wider primes keep the integer
+  // tables): the constants and the twiddles as (c, c / q) double pairs, and
+  // the twiddles also as plain values (the standalone transforms' products
+  // take the quotient from 1/q)
   bool f64 = false;
   if constexpr (sizeof(T) == 8) {
     c.f64_prime_end = 0;
@@ -154,7 +156,8 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
     if (f64) {
       auto dpair = [](uint64_t w, uint64_t q) { return TwPair<double>{double(w), double(w) / double(q)}; };
       std::vector<PrimeInfo<double>> dinfo(qp);
-      std::vector<TwPair<double>> dfwd(fwd.size()), dinv(inv.size());
+      std::vector<TwPair<double>> dfwd(fwd.size(), TwPair<double>{0.0, 0.0}), dinv(inv.size(), TwPair<double>{0.0, 0.0});
+      std::vector<double> vfwd(fwd.size(), 0.0), vinv(inv.size(), 0.0);
       for (int j = 0; j < qp; ++j) {
         const uint64_t q = c.moduli[j];
         const PrimeInfo<T>& p = info[j];
@@ -166,14 +169,20 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
                              nr = dpair(uint64_t(p.ninv_rinv), q), ri = dpair(uint64_t(p.rinv), q);
         d.rmod = rm.w, d.rmod_s = rm.wp, d.ninv = ni.w, d.ninv_s = ni.wp;
         d.ninv_rinv = nr.w, d.ninv_rinv_s = nr.wp, d.rinv = ri.w, d.rinv_s = ri.wp;
+        if (j >= c.f64_prime_end) continue;
         for (uint64_t k = 0; k < n; ++k) {
-          dfwd[size_t(j) * n + k] = dpair(uint64_t(fwd[size_t(j) * n + k].w), q);
-          dinv[size_t(j) * n + k] = dpair(uint64_t(inv[size_t(j) * n + k].w), q);
+          const size_t at = size_t(j) * n + k;
+          dfwd[at] = dpair(uint64_t(fwd[at].w), q);
+          dinv[at] = dpair(uint64_t(inv[at].w), q);
+          vfwd[at] = dfwd[at].w;
+          vinv[at] = dinv[at].w;
         }
       }
       c.t64f.prime = upload(c, dinfo);
       c.t64f.tw_fwd = upload(c, dfwd);
       c.t64f.tw_inv = upload(c, dinv);
+      c.t64f.twv_fwd = upload(c, vfwd);
+      c.t64f.twv_inv = upload(c, vinv);
     }
   }
 
@@ -207,7 +216,8 @@ bool build_tables(Context& c, ChainTables<T>& t, std::vector<LevelTables<T>>& le
       dp[pid] = TwPair<double>{double(p_mod), double(p_mod) / double(m)};
     }
     c.t64f.p_rinv = upload(c, dp);
-    c.f64_tables_ok = c.t64f.prime && c.t64f.tw_fwd && c.t64f.tw_inv && c.t64f.p_rinv;
+    c.f64_tables_ok = c.t64f.prime && c.t64f.tw_fwd && c.t64f.tw_inv && c.t64f.twv_fwd && c.t64f.twv_inv &&
+                      c.t64f.p_rinv;
   }
 
   // ---- per level: hybrid digits, Garner and extension constants, rescale --

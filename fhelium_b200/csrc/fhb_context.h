@@ -36,6 +36,11 @@ struct ChainTables {
   // value x = y R gives P y, the form in which an addend d enters the key-
   // switch accumulators before ModDown ((t + P d - [t]_P) / P = (t - [t]_P) / P + d).
   TwPair<T>* p_rinv = nullptr;    // [QP]
+  // FP64 tables only: the twiddle values alone, [QP][N] in the order of
+  // tw_fwd / tw_inv, for the standalone transforms, whose butterflies take
+  // the quotient from the product and 1/q (prime.one_s).
+  T* twv_fwd = nullptr;
+  T* twv_inv = nullptr;
 };
 
 // Per-level key-switch / rescale tables (device).

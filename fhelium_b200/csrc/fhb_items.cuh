@@ -294,11 +294,11 @@ k_items_ntt_forward(ItemsView iv, const ItemUnit* __restrict__ units, int num_q,
       const PrimeInfo<double> p = tabs64f.prime[pid];
       U64MontSource<true> src{reinterpret_cast<const uint64_t*>(in), p.rmod, p.rmod_s, p.q};
       double v[G::kE];
-      Ntt<double, LOGN>::forward_from(src, reinterpret_cast<double*>(smem_raw),
-                                      TwGlobal<double, LOGN>(tabs64f.tw_fwd + int64_t(pid) * G::kN), p.q, p.twice_q,
-                                      rank, v);
+      Ntt<double, LOGN, TwGlobalQ<LOGN>>::forward_from(src, reinterpret_cast<double*>(smem_raw),
+                                                       TwGlobalQ<LOGN>{tabs64f.twv_fwd + int64_t(pid) * G::kN, p.one_s},
+                                                       p.q, p.one_s, rank, v);
 #pragma unroll
-      for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+      for (int e = 0; e < G::kE; ++e) v[e] = Word<double>::to_lazy(v[e], p.q, p.one_s);
       store_words(reinterpret_cast<uint64_t*>(out), v);
       return;
     }
@@ -349,9 +349,9 @@ k_items_ntt_inverse(ItemsView iv, const ItemUnit* __restrict__ units, int num_q,
 #pragma unroll
       for (int e = 0; e < G::kE; ++e) v[e] = __ull2double_rn(w[e]);
       F64OutEpilogue epi{reinterpret_cast<uint64_t*>(out), p.q, p.ninv_rinv, p.ninv_rinv_s, kInvStandard};
-      Ntt<double, LOGN>::inverse(reinterpret_cast<double*>(smem_raw),
-                                 TwGlobal<double, LOGN>(tabs64f.tw_inv + int64_t(pid) * G::kN), p.q, p.twice_q, rank,
-                                 v, epi);
+      Ntt<double, LOGN, TwGlobalQ<LOGN>>::inverse(reinterpret_cast<double*>(smem_raw),
+                                                  TwGlobalQ<LOGN>{tabs64f.twv_inv + int64_t(pid) * G::kN, p.one_s},
+                                                  p.q, p.one_s, rank, v, epi);
       return;
     }
   }

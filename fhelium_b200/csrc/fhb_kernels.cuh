@@ -133,10 +133,11 @@ k_ntt_forward(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
       const PrimeInfo<double> p = tabs64f.prime[pid];
       U64MontSource<TO_MONT> src{reinterpret_cast<const uint64_t*>(in) + poly * G::kN, p.rmod, p.rmod_s, p.q};
       double v[G::kE];
-      Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::forward_from(
-          src, reinterpret_cast<double*>(smem_raw), tabs64f.tw_fwd + int64_t(pid) * G::kN, p.q, p.twice_q, rank, v);
+      Ntt<double, LOGN, TwGlobalQ<LOGN>, EPT>::forward_from(
+          src, reinterpret_cast<double*>(smem_raw), TwGlobalQ<LOGN>{tabs64f.twv_fwd + int64_t(pid) * G::kN, p.one_s},
+          p.q, p.one_s, rank, v);
 #pragma unroll
-      for (int e = 0; e < G::kE; ++e) v[e] = csub(v[e], p.twice_q);
+      for (int e = 0; e < G::kE; ++e) v[e] = Word<double>::to_lazy(v[e], p.q, p.one_s);
       store_words(reinterpret_cast<uint64_t*>(dst), v);
       return;
     }
@@ -199,9 +200,9 @@ k_ntt_inverse(const T* __restrict__ in, T* __restrict__ out, int rows, int row_s
       const bool std_out = kind != kInvMontgomery;  // N^-1 R^-1 unless the output stays Montgomery
       F64OutEpilogue epi{reinterpret_cast<uint64_t*>(out) + poly * G::kN, p.q, std_out ? p.ninv_rinv : p.ninv,
                          std_out ? p.ninv_rinv_s : p.ninv_s, kind};
-      Ntt<double, LOGN, TwGlobal<double, LOGN>, EPT>::inverse(reinterpret_cast<double*>(smem_raw),
-                                                               tabs64f.tw_inv + int64_t(pid) * G::kN, p.q, p.twice_q,
-                                                               rank, v, epi);
+      Ntt<double, LOGN, TwGlobalQ<LOGN>, EPT>::inverse(reinterpret_cast<double*>(smem_raw),
+                                                       TwGlobalQ<LOGN>{tabs64f.twv_inv + int64_t(pid) * G::kN, p.one_s},
+                                                       p.q, p.one_s, rank, v, epi);
       return;
     }
   }
@@ -426,22 +427,30 @@ struct KsTw {
       __syncthreads();
     }
   }
+  // the transforms' second modulus argument: 2q, or 1/q for the balanced FP64 rows
+  __device__ __forceinline__ static T m2(const PrimeInfo<T>& p) {
+    if constexpr (std::is_same<T, double>::value) {
+      return p.one_s;
+    } else {
+      return p.twice_q;
+    }
+  }
   template <class Src>
   __device__ __forceinline__ void forward_from(Src& src, T* data, const PrimeInfo<T>& p, T (&v)[G::kE]) const {
     if constexpr (kShared) {
-      Ntt<T, LOGN, TwShared<T, LOGN>>::forward_from(src, data, TwShared<T, LOGN>{gf, st, rank * G::kM}, p.q,
-                                                    p.twice_q, rank, v);
+      Ntt<T, LOGN, TwShared<T, LOGN>>::forward_from(src, data, TwShared<T, LOGN>{gf, st, rank * G::kM}, p.q, m2(p),
+                                                    rank, v);
     } else {
-      Ntt<T, LOGN>::forward_from(src, data, TwGlobal<T, LOGN>(gf), p.q, p.twice_q, rank, v);
+      Ntt<T, LOGN>::forward_from(src, data, TwGlobal<T, LOGN>(gf), p.q, m2(p), rank, v);
     }
   }
   template <class Epi>
   __device__ __forceinline__ void inverse(T* data, const PrimeInfo<T>& p, const T (&v)[G::kE], Epi& epi) const {
     if constexpr (kShared) {
-      Ntt<T, LOGN, TwShared<T, LOGN>>::inverse(data, TwShared<T, LOGN>{gi, st, rank * G::kM}, p.q, p.twice_q, rank, v,
+      Ntt<T, LOGN, TwShared<T, LOGN>>::inverse(data, TwShared<T, LOGN>{gi, st, rank * G::kM}, p.q, m2(p), rank, v,
                                                epi);
     } else {
-      Ntt<T, LOGN>::inverse(data, TwGlobal<T, LOGN>(gi), p.q, p.twice_q, rank, v, epi);
+      Ntt<T, LOGN>::inverse(data, TwGlobal<T, LOGN>(gi), p.q, m2(p), rank, v, epi);
     }
   }
 };
@@ -482,10 +491,12 @@ struct KsAcc {
     c0[e * stride] = csub(c0[e * stride] + Word<T>::mont(x, k0, p.q, p.neg_inv), p.twice_q);
     c1[e * stride] = csub(c1[e * stride] + Word<T>::mont(x, k1, p.q, p.neg_inv), p.twice_q);
   }
-  // FP64 form (T = double): residues times key words (both < 2q), quotient from 1/q
-  __device__ __forceinline__ void mac_f64(int e, T x, T k0, T k1, T q, T twoq, T qinv) {
-    c0[e * stride] = csub(c0[e * stride] + Word<T>::mul_qinv(x, k0, q, qinv), twoq);
-    c1[e * stride] = csub(c1[e * stride] + Word<T>::mul_qinv(x, k1, q, qinv), twoq);
+  // FP64 form (T = double, balanced): forward outputs |x| < 11 q times key
+  // words below 2q, quotient from 1/q; each term in (-0.55 q, 0.55 q), summed
+  // without reduction (the sum is reduced once before the inverse transform)
+  __device__ __forceinline__ void mac_f64(int e, T x, T k0, T k1, T q, T qinv) {
+    c0[e * stride] += Word<T>::mul_qinv_bal(x, k0, q, qinv);
+    c1[e * stride] += Word<T>::mul_qinv_bal(x, k1, q, qinv);
   }
   __device__ __forceinline__ void get(int which, T (&v)[G::kE]) const {
     const T* c = which ? c1 : c0;
@@ -749,13 +760,13 @@ struct F64InvEpilogue {
 
 template <class Acc, int E>
 __device__ __forceinline__ void key_mac_f64(Acc& acc, const double (&v)[E], const uint64_t* key0,
-                                            const uint64_t* key1, double q, double twoq, double qinv) {
+                                            const uint64_t* key1, double q, double qinv) {
 #pragma unroll
   for (int i = 0; i < E / 2; ++i) {
     const ulonglong2 a = __ldg(reinterpret_cast<const ulonglong2*>(key0) + i);
     const ulonglong2 b = __ldg(reinterpret_cast<const ulonglong2*>(key1) + i);
-    acc.mac_f64(2 * i, csub(v[2 * i], twoq), __ull2double_rn(a.x), __ull2double_rn(b.x), q, twoq, qinv);
-    acc.mac_f64(2 * i + 1, csub(v[2 * i + 1], twoq), __ull2double_rn(a.y), __ull2double_rn(b.y), q, twoq, qinv);
+    acc.mac_f64(2 * i, v[2 * i], __ull2double_rn(a.x), __ull2double_rn(b.x), q, qinv);
+    acc.mac_f64(2 * i + 1, v[2 * i + 1], __ull2double_rn(a.y), __ull2double_rn(b.y), q, qinv);
   }
 }
 
@@ -785,6 +796,8 @@ __device__ __forceinline__ void ks_core_unit_f64(const uint64_t* __restrict__ ex
   const double q = p.q, twoq = p.twice_q, qinv = p.one_s;
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
   KsAcc<double, LOGN> acc(s, nullptr, nullptr);
+  // (w, w / q) twiddle pairs: the quotient estimate does not wait for the
+  // product, which measured faster here than value-only twiddles
   KsTw<double, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
   const bool add = ct3 != nullptr;
@@ -807,17 +820,19 @@ __device__ __forceinline__ void ks_core_unit_f64(const uint64_t* __restrict__ ex
                        LOGN, d.prime0 + d.alpha > f64_end, q, twoq};
       tw.forward_from(src, s, p, v);
     }
-    key_mac_f64(acc, v, key0, key1, q, twoq, qinv);
+    key_mac_f64(acc, v, key0, key1, q, qinv);
   }
   tw.stage(true);
   const TwPair<double> pc = tabs.p_rinv[pid];  // P mod q and its companion (FP64 tables)
   for (int c = 0; c < 2; ++c) {
     double v[G::kE];
     acc.get(c, v);
+#pragma unroll
+    for (int e = 0; e < G::kE; ++e) v[e] = W::reduce_bal(v[e], q, qinv);  // |v| < 0.51 q
     if (add) {
 #pragma unroll
       for (int e = 0; e < G::kE; ++e)
-        v[e] = csub(v[e] + W::shoup(__ull2double_rn(ct3_own[c * ct3_stride + e]), pc.w, pc.wp, q), twoq);
+        v[e] += W::shoup_bal(__ull2double_rn(ct3_own[c * ct3_stride + e]), pc.w, pc.wp, q);
     }
     F64InvEpilogue epi{(c ? acc1 : acc0) + poly * G::kN, q, p.ninv_rinv, p.ninv_rinv_s};
     tw.inverse(s, p, v, epi);

@@ -26,7 +26,16 @@
 // The inverse mirrors this: the first pass starts from E consecutive
 // values per thread (from registers), the cross-CTA stages come last and
 // read the other CTAs' blocks through distributed shared memory.
-// Forward butterflies keep Harvey's lazy range [0, 4q), inverse ones [0, 2q).
+// Integer residues: forward butterflies keep Harvey's lazy range [0, 4q),
+// inverse ones [0, 2q).  FP64 residues (T = double, primes below 2^42,
+// N <= 2^16) run balanced: signed values, every twiddle product reduced
+// with a quotient rounded to nearest to (-0.55 q, 0.55 q) and no conditional
+// subtraction, so a forward value grows by at most 0.55 q per stage
+// (|x| < 2q + 16 * 0.55 q < 11 q) and an inverse sum at most doubles per
+// stage, with every value reduced to (-0.51 q, 0.51 q) when a pass stores it
+// to shared memory (an inverse pass of at most 16 stages' growth from inputs
+// below 2q keeps every product operand below 32 q < 2^47).  For T = double
+// the transforms' `twoq` argument carries 1 / q instead.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -96,6 +105,7 @@ __device__ __forceinline__ TwPair<T> ldtw(const TwPair<T>* tw, int i) {
 // TwGlobal reads the prime's row straight from global memory (L2).
 template <typename T, int LOGN>
 struct TwGlobal {
+  static constexpr bool kQFromProduct = false;  // (w, floor(w 2^W / q)) pairs: Shoup products
   const TwPair<T>* g;
   __device__ __forceinline__ TwGlobal(const TwPair<T>* row) : g(row) {}
   __device__ __forceinline__ TwPair<T> fwd(int st, int ng) const { return ldtw(g, (1 << st) + (ng >> (LOGN - st))); }
@@ -112,6 +122,7 @@ struct TwGlobal {
 // Cross-CTA stages (at most 7 distinct twiddles) still read global memory.
 template <typename T, int LOGN>
 struct TwShared {
+  static constexpr bool kQFromProduct = false;
   using G = NttGeom<T, LOGN>;
   const TwPair<T>* g;
   const TwPair<T>* s;
@@ -143,6 +154,23 @@ struct TwShared {
   }
 };
 
+// FP64 rows: the twiddle values alone from global memory (8 bytes each,
+// half the load traffic of pairs).  The butterflies take the quotient from
+// the product and 1/q (Word<double>::mul_qinv), which the accessor hands out
+// in the pair's second slot.
+template <int LOGN>
+struct TwGlobalQ {
+  static constexpr bool kQFromProduct = true;
+  const double* g;
+  double qinv;
+  __device__ __forceinline__ TwPair<double> fwd(int st, int ng) const {
+    return TwPair<double>{__ldg(g + (1 << st) + (ng >> (LOGN - st))), qinv};
+  }
+  __device__ __forceinline__ TwPair<double> inv(int j, int ng) const {
+    return TwPair<double>{__ldg(g + ((1 << LOGN) >> (j + 1)) + (ng >> (j + 1))), qinv};
+  }
+};
+
 template <typename T, int LOGN, class TW = TwGlobal<T, LOGN>, int EPT = 0>
 struct Ntt {
   using G = NttGeom<T, LOGN, EPT>;
@@ -158,17 +186,48 @@ struct Ntt {
     return t;
   }
 
+  static constexpr bool kBal = std::is_same<T, double>::value;
+
+  // y w mod q: Shoup's product with the twiddle's companion, in [0, 2q); or
+  // (FP64) balanced, with the companion or, for value-only twiddles, the
+  // product's own quotient estimate (the accessor hands 1/q out in .wp)
+  __device__ __forceinline__ static T tw_mul(T y, const TwPair<T>& w, T q) {
+    if constexpr (kBal) {
+      if constexpr (TW::kQFromProduct) {
+        return W::mul_qinv_bal(y, w.w, q, w.wp);
+      } else {
+        return W::shoup_bal(y, w.w, w.wp, q);
+      }
+    } else {
+      return W::shoup(y, w.w, w.wp, q);
+    }
+  }
+
   __device__ __forceinline__ static void fwd_bfly(T& x, T& y, const TwPair<T>& w, T q, T twoq) {
-    const T xx = csub(x, twoq);
-    const T t = W::shoup(y, w.w, w.wp, q);
-    x = xx + t;
-    y = xx - t + twoq;
+    if constexpr (kBal) {
+      const T t = tw_mul(y, w, q);
+      const T xx = x;
+      x = xx + t;
+      y = xx - t;
+    } else {
+      const T xx = csub(x, twoq);
+      const T t = tw_mul(y, w, q);
+      x = xx + t;
+      y = xx - t + twoq;
+    }
   }
   __device__ __forceinline__ static void inv_bfly(T& x, T& y, const TwPair<T>& w, T q, T twoq) {
-    const T s = x + y;
-    const T d = x - y + twoq;
-    x = csub(s, twoq);
-    y = W::shoup(d, w.w, w.wp, q);
+    if constexpr (kBal) {
+      const T s = x + y;
+      const T d = x - y;
+      x = s;
+      y = tw_mul(d, w, q);
+    } else {
+      const T s = x + y;
+      const T d = x - y + twoq;
+      x = csub(s, twoq);
+      y = tw_mul(d, w, q);
+    }
   }
 
   // ---- forward -----------------------------------------------------------
@@ -255,7 +314,8 @@ struct Ntt {
     }
   }
 
-  // Forward transform of one polynomial whose input residues (< 4q) are
+  // Forward transform of one polynomial whose input residues (< 4q; FP64:
+  // < 2q) are
   // produced on demand: src.column(m, stride, x) fills x[c] with the input
   // at position c * stride + m of the polynomial (0 <= position < N).  On return out[e] holds the (lazy, < 4q)
   // output at local position tid() * E + e of CTA `rank`.  Starts with a
@@ -317,7 +377,10 @@ struct Ntt {
         for (int i = 0; i < kGs; ++i) epi(ng0 + i * kHl, v[i]);
       } else {
 #pragma unroll
-        for (int i = 0; i < kGs; ++i) s[G::sidx(n0 + i * kHl)] = v[i];
+        for (int i = 0; i < kGs; ++i) {
+          if constexpr (kBal) v[i] = W::reduce_bal(v[i], q, twoq);  // twoq holds 1/q here
+          s[G::sidx(n0 + i * kHl)] = v[i];
+        }
       }
     }
   }
@@ -372,8 +435,9 @@ struct Ntt {
   }
 
   // Inverse transform of the values `in` (thread-contiguous layout, as left
-  // by `forward_from`, each < 2q).  Every output is handed to
-  // epi(position, v) with v in [0, 2q); s is scratch.  Ends with a cluster
+  // by `forward_from`, each < 2q; FP64: |x| < 2q, balanced).  Every output
+  // is handed to epi(position, v) with v in [0, 2q) (FP64: |v| < 8q,
+  // balanced); s is scratch.  Ends with a cluster
   // barrier so that shared memory may be reused (and so that peers never
   // outlive reads).
   template <class Epi>
