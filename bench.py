@@ -458,24 +458,30 @@ def forms_leg(eng, ca, cb, rlk, stream, steps=5):
         for _ in range(2):
             eng.rotate_by_step(eng.multiply_relinearize_rescale(ca, cb, rlk), 1)
     torch.cuda.synchronize()
-    for form in ("cuda_cores", "tensor_cores"):
-        eng.basis_conversion = form
-        res = {}
-        r = eng.multiply_relinearize_rescale(ca, cb, rlk)
-        torch.cuda.synchronize()
-        ms = _time_events(lambda: eng.multiply_relinearize_rescale(ca, cb, rlk), steps, stream)
-        res["hmult_relin_rescale_ops_per_s"] = ca.batch_size / (ms / 1000.0)
-        res["hmult_relin_rescale_ms"] = ms
-        rot = eng.rotate_by_step(r, 1)
-        torch.cuda.synchronize()
-        rms = _time_events(lambda: eng.rotate_by_step(r, 1), steps, stream)
-        res["rotate_ops_per_s"] = r.batch_size / (rms / 1000.0)
-        hoisted = eng.rotate_many_by_steps(r, list(range(1, 17)))
-        torch.cuda.synchronize()
-        hms = _time_events(lambda: eng.rotate_many_by_steps(r, list(range(1, 17))), max(2, steps // 2), stream)
-        res["hoisted_rotations_16_ops_per_s"] = 16 * r.batch_size / (hms / 1000.0)
-        results[form] = (r.data.clone(), rot.data.clone(), torch.stack([h.data for h in hoisted]))
-        out[form] = res
+    # three interleaved rounds (the forms alternate which goes first), the
+    # best time of each form and operation, so that drift over the leg does
+    # not favour one form
+    best: dict = {}
+    for rnd in range(3):
+        for form in (("cuda_cores", "tensor_cores") if rnd % 2 == 0 else ("tensor_cores", "cuda_cores")):
+            eng.basis_conversion = form
+            r = eng.multiply_relinearize_rescale(ca, cb, rlk)
+            torch.cuda.synchronize()
+            ms = _time_events(lambda: eng.multiply_relinearize_rescale(ca, cb, rlk), steps, stream)
+            rot = eng.rotate_by_step(r, 1)
+            torch.cuda.synchronize()
+            rms = _time_events(lambda: eng.rotate_by_step(r, 1), steps, stream)
+            hoisted = eng.rotate_many_by_steps(r, list(range(1, 17)))
+            torch.cuda.synchronize()
+            hms = _time_events(lambda: eng.rotate_many_by_steps(r, list(range(1, 17))), max(2, steps // 2), stream)
+            if rnd == 0:
+                results[form] = (r.data.clone(), rot.data.clone(), torch.stack([h.data for h in hoisted]))
+            b = best.setdefault(form, [ms, rms, hms])
+            best[form] = [min(x, y) for x, y in zip(b, (ms, rms, hms))]
+    for form, (ms, rms, hms) in best.items():
+        out[form] = {"hmult_relin_rescale_ops_per_s": ca.batch_size / (ms / 1000.0), "hmult_relin_rescale_ms": ms,
+                     "rotate_ops_per_s": ca.batch_size / (rms / 1000.0),
+                     "hoisted_rotations_16_ops_per_s": 16 * ca.batch_size / (hms / 1000.0)}
     a, b = results["cuda_cores"], results["tensor_cores"]
     out["bit_identical"] = all(bool(torch.equal(x, y)) for x, y in zip(a, b))
     # variant of the tensor-core form, HMult+relin+rescale only: ModDown on

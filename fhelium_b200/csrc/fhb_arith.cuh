@@ -88,9 +88,9 @@ struct Word<double> {
   }
   // Balanced forms for signed residues (the FP64 transforms): the quotient
   // estimate rounded to nearest.  Its relative error is below 2^-51, so for
-  // |x w / q| < 2^47 it is within 0.05 of x w / q and the result x w - qt q
-  // lies in (-0.55 q, 0.55 q) with no correction, exactly (every
-  // intermediate is an integer below 2^53).
+  // |x w / q| < 2^48 it is within 0.1 of x w / q and the result x w - qt q
+  // lies in (-0.6 q, 0.6 q) with no correction, exactly (every intermediate
+  // is an integer below 2^53).
   __device__ __forceinline__ static T shoup_bal(T x, T w, T wc, T q) {
     const T h = x * w;
     const T l = fma(x, w, -h);

@@ -491,8 +491,8 @@ struct KsAcc {
     c0[e * stride] = csub(c0[e * stride] + Word<T>::mont(x, k0, p.q, p.neg_inv), p.twice_q);
     c1[e * stride] = csub(c1[e * stride] + Word<T>::mont(x, k1, p.q, p.neg_inv), p.twice_q);
   }
-  // FP64 form (T = double, balanced): forward outputs |x| < 11 q times key
-  // words below 2q, quotient from 1/q; each term in (-0.55 q, 0.55 q), summed
+  // FP64 form (T = double, balanced): forward outputs |x| < 20 q times key
+  // words below 2q, quotient from 1/q; each term in (-0.6 q, 0.6 q), summed
   // without reduction (the sum is reduced once before the inverse transform)
   __device__ __forceinline__ void mac_f64(int e, T x, T k0, T k1, T q, T qinv) {
     c0[e * stride] += Word<T>::mul_qinv_bal(x, k0, q, qinv);
@@ -716,9 +716,11 @@ struct U64RowSource {
 };
 
 // Exact extension of one digit to prime p in FP64 (the CUDA-core form's
-// source of the forward transform): sum_r d_r (M_r mod p), lazy [0, 2p).
-// Digit words below 2^42 enter whole; a digit that holds a wider prime has
-// its words split into 30-bit halves against (M_r mod p) 2^30 and M_r mod p.
+// source of the forward transform): sum_r d_r (M_r mod p), balanced: every
+// term reduced to (-0.6 p, 0.6 p) and summed unreduced (16 terms at most,
+// below 9.6 p).  Digit words below 2^42 enter whole; a digit that holds a
+// wider prime has its words split into 30-bit halves against
+// (M_r mod p) 2^30 and M_r mod p.
 struct ExtSourceF64 {
   const uint64_t* dig;        // the digit's first mixed-radix row of this ciphertext
   const TwPair<double>* ext;  // [r][2][qp0] of this digit, offset by the destination prime id
@@ -738,23 +740,24 @@ struct ExtSourceF64 {
 #pragma unroll
         for (int k = 0; k < C; ++k) {
           const uint64_t w = row[k * stride];
-          x[k] = csub(x[k] + W::shoup(__ull2double_rn(w >> 30), hi.w, hi.wp, q), twice_q);
-          x[k] = csub(x[k] + W::shoup(__ull2double_rn(w & ((uint64_t{1} << 30) - 1)), lo.w, lo.wp, q), twice_q);
+          x[k] += W::shoup_bal(__ull2double_rn(w >> 30), hi.w, hi.wp, q);
+          x[k] += W::shoup_bal(__ull2double_rn(w & ((uint64_t{1} << 30) - 1)), lo.w, lo.wp, q);
         }
       } else {
 #pragma unroll
-        for (int k = 0; k < C; ++k) x[k] = csub(x[k] + W::shoup(__ull2double_rn(row[k * stride]), lo.w, lo.wp, q), twice_q);
+        for (int k = 0; k < C; ++k) x[k] += W::shoup_bal(__ull2double_rn(row[k * stride]), lo.w, lo.wp, q);
       }
     }
   }
 };
 
+// Canonical output of a balanced inverse transform: v c mod q in [0, q).
 struct F64InvEpilogue {
   uint64_t* dst;
   double q, c, cs;
   __device__ __forceinline__ void operator()(int pos, double v) const {
-    v = csub(Word<double>::shoup(v, c, cs, q), q);
-    dst[pos] = __double2ull_rz(v);
+    v = Word<double>::shoup_bal(v, c, cs, q);
+    dst[pos] = __double2ull_rz(v < 0.0 ? v + q : v);
   }
 };
 

@@ -29,13 +29,14 @@
 // Integer residues: forward butterflies keep Harvey's lazy range [0, 4q),
 // inverse ones [0, 2q).  FP64 residues (T = double, primes below 2^42,
 // N <= 2^16) run balanced: signed values, every twiddle product reduced
-// with a quotient rounded to nearest to (-0.55 q, 0.55 q) and no conditional
-// subtraction, so a forward value grows by at most 0.55 q per stage
-// (|x| < 2q + 16 * 0.55 q < 11 q) and an inverse sum at most doubles per
-// stage, with every value reduced to (-0.51 q, 0.51 q) when a pass stores it
-// to shared memory (an inverse pass of at most 16 stages' growth from inputs
-// below 2q keeps every product operand below 32 q < 2^47).  For T = double
-// the transforms' `twoq` argument carries 1 / q instead.
+// with a quotient rounded to nearest to (-0.6 q, 0.6 q) and no conditional
+// subtraction, so a forward value grows by at most 0.6 q per stage (inputs
+// below 10 q leave the 16 stages below 20 q) and an inverse sum at most
+// doubles per stage, with every value reduced to (-0.51 q, 0.51 q) when a
+// pass stores it to shared memory (a pass of at most 4 stages from inputs
+// below 2q keeps every product operand below 32 q).  Every product operand
+// stays below 2^48 q / w.  For T = double the transforms' `twoq` argument
+// carries 1 / q instead.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -315,7 +316,7 @@ struct Ntt {
   }
 
   // Forward transform of one polynomial whose input residues (< 4q; FP64:
-  // < 2q) are
+  // |x| < 10q) are
   // produced on demand: src.column(m, stride, x) fills x[c] with the input
   // at position c * stride + m of the polynomial (0 <= position < N).  On return out[e] holds the (lazy, < 4q)
   // output at local position tid() * E + e of CTA `rank`.  Starts with a
