@@ -55,7 +55,10 @@ KS_TRAFFIC_BYTES_BATCH32 = 12741399552 + 2934590720  # ncu dram read + write, k_
 # same for the key-switch core of the tensor-core form: captured at batch 8 (3094038784 + 705889536 bytes,
 # 2.01x the batch-4 capture) and scaled by the ciphertexts processed
 KS_EXT_TRAFFIC_BYTES_BATCH32 = 4 * (3094038784 + 705889536)
-# same for that core with its FP64 rows (k_keyswitch_core_split): captured at batch 8 (3085136640 + 355092224
+# the CUDA-core form's core with its FP64 rows (k_keyswitch_core_split<false>, the extension computed in FP64 in
+# the core): not yet captured
+KS_SPLIT_TRAFFIC_BYTES_BATCH32 = None
+# the tensor-core form's core with its FP64 rows (k_keyswitch_core_split<PRE>): captured at batch 8 (3085136640 + 355092224
 # bytes; the key and digit rows are re-read per group of four ciphertexts, so the traffic grows with the batch)
 # and scaled by the ciphertexts processed
 KS_F64_TRAFFIC_BYTES_BATCH32 = 4 * (3085136640 + 355092224)
@@ -678,8 +681,9 @@ def main() -> int:
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-extras", action="store_true", help="skip rotation/parity/CPU legs")
     ap.add_argument("--mixed-count", type=int, default=512, help="ciphertexts of the mixed-level leg (0: skip)")
-    ap.add_argument("--basis", choices=["cuda_cores", "tensor_cores"], default="tensor_cores",
-                    help="where the key switch's basis conversion runs in the headline step")
+    ap.add_argument("--basis", choices=["auto", "cuda_cores", "tensor_cores"], default="auto",
+                    help="where the key switch's basis conversion runs in the headline step (auto: the "
+                         "engine's default for the chain)")
     ap.add_argument("--leg", choices=["ntt_int32", "bootstrap", "mixed", "ops", "schema", "forms"], default=None,
                     help="run only this side leg on one GPU and print its result (profiling aid)")
     args = ap.parse_args()
@@ -725,6 +729,7 @@ def main() -> int:
     torch.cuda.set_device(dev)
     cfg = CkksConfig.parse(PRESET)
     eng = CkksEngine(cfg, device=dev, rng_seed=1234 + rank, basis_conversion=args.basis)
+    form = eng.basis_conversion  # the resolved form
     B = args.batch
     x = _messages(B, eng.num_slots, 2 + 2 * rank)
     y = _messages(B, eng.num_slots, 3 + 2 * rank)
@@ -753,10 +758,10 @@ def main() -> int:
     # tensor product, INTT of c2, ModUp digits, (tensor-core basis extension,) key-switch core, ModDown+rescale
     # (the tensor-core form's core is two launches when its Q rows run in FP64:
     # the P rows stay on the integer kernel)
-    f64_core = args.basis == "tensor_cores" and bool(eng.ctx.get_tuning(nat.TUNE_F64_CORE))
+    f64_core = bool(eng.ctx.get_tuning(nat.TUNE_F64_CORE))
     # tensor product, inverse NTT of d2, ModUp digits, (tensor-core extension,) core, ModDown; the FP64 rows of
     # the NTT and of the core share their launches with the integer rows
-    launches_per_step = 6 if args.basis == "tensor_cores" else 5
+    launches_per_step = 6 if form == "tensor_cores" else 5
 
     # ---- end to end through the public API with host buffers -------------
     host_a = ca.data.cpu().pin_memory()
@@ -821,7 +826,7 @@ def main() -> int:
         "inverse_ntt_d2": lambda: lib.fhb_inverse_ntt(h, nat.ptr(coef[2]), nat.ptr(digits), B, L, 0, 2, s),
     }
     ext = None
-    if args.basis == "tensor_cores":
+    if form == "tensor_cores":
         # the tensor-core form's two key-switch kernels
         ext = torch.empty(int(lib.fhb_tc_basis_extend_words(h, B, 0)), dtype=torch.int64, device=dev)
         kernels["tc_basis_extend"] = lambda: lib.fhb_tc_basis_extend(h, nat.ptr(digits), nat.ptr(ext), B, 0, s)
@@ -861,6 +866,30 @@ def main() -> int:
     # a peak: the best of three timings (each of three launches)
     probe_ms = min(_time_events(probe, 3, stream) for _ in range(3))
     modmul_peak = 148 * 8 * 256 * 8 * probe_iters / (probe_ms / 1000.0)
+    # the FP64 rows' balanced product, probed the same way; the key-switch
+    # core's attainable rate is the row-weighted mix of the two
+    f64_rows = 0
+    probe_f64_ms = None
+    if f64_core:
+        probe_f64 = torch.empty(148 * 8 * 256, dtype=torch.float64, device=dev)
+        probe64 = lambda: nat.check(lib.fhb_modmul_probe_f64(h, probe_f64.data_ptr(), 148 * 8, probe_iters, s),
+                                    "probe f64")
+        probe64()
+        torch.cuda.synchronize(dev)
+        probe_f64_ms = min(_time_events(probe64, 3, stream) for _ in range(3))
+        modmul_peak_f64 = 148 * 8 * 256 * 8 * probe_iters / (probe_f64_ms / 1000.0)
+        f64_rows = sum(1 for q in cfg.q_moduli if int(q) < (1 << 42))
+    else:
+        modmul_peak_f64 = None
+
+    def mixed_peak(share):
+        """attainable modular-product rate of a kernel running `share` of its rows in FP64"""
+        return 1.0 / (share / modmul_peak_f64 + (1.0 - share) / modmul_peak) if modmul_peak_f64 else modmul_peak
+
+    ks_peak = mixed_peak(f64_rows / (L + cfg.num_p_primes))
+    # kernels whose rows of primes below 2^42 run in FP64, and their FP64 share
+    f64_share = {"inverse_ntt_d2": f64_rows / L, "keyswitch_core": f64_rows / (L + cfg.num_p_primes),
+                 "keyswitch_core_extended": f64_rows / (L + cfg.num_p_primes)}
     modmul_achieved = ks_modmul / (per_kernel["keyswitch_core"] / 1000.0)
     step_bytes = B * (4 * L + 2 * (L - 1)) * limb + 10 * 2 * (L + cfg.num_p_primes) * limb
     # every step kernel against its roofs: algorithmic bytes (each operand row
@@ -897,7 +926,8 @@ def main() -> int:
         entry = {"ms": per_kernel[name], "algorithmic_bytes": nbytes, "hbm_gbs": nbytes / sec / 1e9,
                  "hbm_frac": nbytes / sec / 1e9 / peak}
         if nmul:
-            entry.update({"modmul": nmul, "modmul_per_s": nmul / sec, "modmul_frac": nmul / sec / modmul_peak})
+            kpeak = mixed_peak(f64_share.get(name, 0.0))
+            entry.update({"modmul": nmul, "modmul_per_s": nmul / sec, "modmul_frac": nmul / sec / kpeak})
         entry["bound"] = "hbm" if not nmul or entry["hbm_frac"] > entry["modmul_frac"] else "integer"
         if name in int8_ops:
             entry.update({"int8_ops": int8_ops[name], "int8_tops": int8_ops[name] / sec / 1e12,
@@ -911,13 +941,18 @@ def main() -> int:
     traffic = KS_TRAFFIC_BYTES_BATCH32 * B / 32 if cfg.logN == 16 and L == 35 else None
     # the dominant kernel of the headline form
     dom = "keyswitch_core_extended" if ext is not None else "keyswitch_core"
-    dom_kernel = {"keyswitch_core": "k_keyswitch_core",
+    dom_kernel = {"keyswitch_core": ("k_keyswitch_core_split<false> (FP64 rows for the primes below 2^42 with the "
+                                     "extension computed in FP64, int64 rows for the base prime and P)"
+                                     if f64_core else "k_keyswitch_core"),
                   "keyswitch_core_extended": ("k_keyswitch_core_split<PRE> (FP64 rows for the primes below 2^42, "
                                               "int64 rows for the base prime and P)"
                                               if f64_core else "k_keyswitch_core<PRE>")}[dom]
     if dom == "keyswitch_core_extended":
         ext_traffic = KS_F64_TRAFFIC_BYTES_BATCH32 if f64_core else KS_EXT_TRAFFIC_BYTES_BATCH32
         traffic = ext_traffic * B / 32 if ext_traffic and cfg.logN == 16 and L == 35 else None
+    elif f64_core:
+        traffic = (KS_SPLIT_TRAFFIC_BYTES_BATCH32 * B / 32
+                   if KS_SPLIT_TRAFFIC_BYTES_BATCH32 and cfg.logN == 16 and L == 35 else None)
     dom_bytes, dom_modmul = kroof[dom]
     achieved = dom_bytes / (per_kernel[dom] / 1000.0) / 1e9
     modmul_achieved = dom_modmul / (per_kernel[dom] / 1000.0)
@@ -997,16 +1032,19 @@ def main() -> int:
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded uniform messages, engine-generated keys)",
         "config": dict(CONFIG, batch_per_gpu=B, global_batch=B * ws, parallelism=f"independent ciphertexts x{ws}",
-                       basis_conversion=args.basis),
+                       basis_conversion=form),
         "e2e": {"value": ws * B / (e2e_ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "chunks": e2e_chunks["chunks"], "staging_buffers": e2e_chunks["buffers"],
                 "chunk_trials_ms": trial},
         "gpu_launches": launches_per_step * args.steps,
         "alu_roofline": {"kernel": dom_kernel, "unit": "modular products/s",
-                         "modmul_per_launch": dom_modmul, "achieved": modmul_achieved, "peak": modmul_peak,
-                         "frac": modmul_achieved / modmul_peak, "probe_ms": probe_ms,
-                         "peak_source": "fhb_modmul_probe: 148x8 CTAs x 256 threads x 8 independent Shoup chains, "
-                                        "timed in this run"},
+                         "modmul_per_launch": dom_modmul, "achieved": modmul_achieved, "peak": ks_peak,
+                         "frac": modmul_achieved / ks_peak, "probe_ms": probe_ms,
+                         "int64_peak": modmul_peak, "f64_peak": modmul_peak_f64, "f64_probe_ms": probe_f64_ms,
+                         "f64_rows": f64_rows,
+                         "peak_source": "fhb_modmul_probe (int64 Shoup) and fhb_modmul_probe_f64 (balanced FP64): "
+                                        "148x8 CTAs x 256 threads x 8 independent chains, timed in this run; the "
+                                        "peak is their mix weighted by the rows each form runs"},
         "roofline": {"kernel": dom_kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": per_kernel[dom],

@@ -41,6 +41,7 @@ ITEM_HMULT_RELIN_RESCALE, ITEM_ROTATE = 0, 1
 SIGNATURES: dict[str, tuple] = {
     "fhb_version": (_I, []),
     "fhb_modmul_probe": (_I, [_P, _P, _I, _I, _P]),
+    "fhb_modmul_probe_f64": (_I, [_P, _P, _I, _I, _P]),
     "fhb_tc_ntt_prepare": (_I, [_P]),
     "fhb_tc_forward_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _P]),
     "fhb_tc_inverse_ntt": (_I, [_P, _P, _P, _I64, _I, _I, _P]),

@@ -324,6 +324,15 @@ int fhb_modmul_probe(const fhb_context* ctx, void* out, int blocks, int iters, f
   return fhb::cuda_status(cudaGetLastError(), "k_modmul_probe");
 }
 
+int fhb_modmul_probe_f64(const fhb_context* ctx, void* out, int blocks, int iters, fhb_stream stream) {
+  CTX_OR_FAIL();
+  TRY(fhb::check_ptr(out, "out"));
+  if (blocks < 1 || iters < 1) return fail(-2, "need blocks >= 1 and iters >= 1");
+  if (!c.f64_tables_ok) return fail(-7, "the chain has no rows of primes below 2^42 (no FP64 tables)");
+  fhb::k_modmul_probe_f64<8><<<blocks, 256, 0, st>>>(static_cast<double*>(out), iters, c.t64f);
+  return fhb::cuda_status(cudaGetLastError(), "k_modmul_probe_f64");
+}
+
 const char* fhb_last_error(void) { return fhb::last_error(); }
 
 int fhb_context_create(int residue_bits, int log_n, const uint64_t* moduli, int num_q, int num_p, int device,

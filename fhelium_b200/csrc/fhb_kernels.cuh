@@ -934,25 +934,24 @@ k_keyswitch_sum(const T* __restrict__ digits, const unsigned long long* __restri
 
 // Hoisting stage 1: materialise NTT-domain extended digits once
 // (fhelium/engine/hybrid_keyswitch.py:373-417).  prepared: [D_l, B, QP_l, N]
-// standard NTT-domain values in [0, 2p).
+// standard NTT-domain values in [0, 2p).  SPLIT (int64 chains with FP64
+// tables): the units of the leading f64_rows rows (primes below 2^42) run
+// the extension and the transform in balanced FP64 arithmetic, the others
+// the integer body, in one launch; both store lazy words in [0, 2p) (equal
+// modulo p, not word for word).
 template <typename T, int LOGN>
-__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64_t batch, int q_limbs,
-                   int qp_limbs, int level, int qp0, int order, ChainTables<T> tabs, LevelTables<T> lt) {
+__device__ __forceinline__ void prepare_unit(const T* __restrict__ digits, T* __restrict__ prepared, int64_t batch,
+                                             int q_limbs, int qp_limbs, int level, int qp0, const ChainTables<T>& tabs,
+                                             const LevelTables<T>& lt, int64_t bi, int jrow, unsigned char* smem_raw,
+                                             int rank) {
   using G = NttGeom<T, LOGN>;
-  using W = Word<T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s = reinterpret_cast<T*>(smem_raw);
-  const int rank = cluster_rank<T, LOGN>();
-  int64_t poly, bi;  // poly over [B, QP_l]
-  int jrow;
-  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  const int64_t poly = bi * qp_limbs + jrow;
   const int pid = level + jrow;
   const PrimeInfo<T> p = tabs.prime[pid];
-  const TwPair<T>* twf = tabs.tw_fwd + int64_t(pid) * G::kN;
   const T* dig = digits + bi * q_limbs * int64_t(G::kN);
   const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
-  KsTw<T, LOGN> tw(smem_raw, twf, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   tw.stage(false);
   for (int a = 0; a < lt.num_digits; ++a) {
     const DigitDesc d = lt.digits[a];
@@ -966,26 +965,145 @@ k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64
   }
 }
 
+template <int LOGN>
+__device__ __forceinline__ void prepare_unit_f64(const uint64_t* __restrict__ digits, uint64_t* __restrict__ prepared,
+                                                 int64_t batch, int q_limbs, int qp_limbs, int level, int qp0,
+                                                 const ChainTables<double>& tabs, const LevelTables<uint64_t>& lt,
+                                                 const TwPair<double>* __restrict__ ext64f, int ext_digits,
+                                                 int f64_end, int64_t bi, int jrow, unsigned char* smem_raw,
+                                                 int rank) {
+  using G = NttGeom<double, LOGN>;
+  double* s = reinterpret_cast<double*>(smem_raw);
+  const int64_t poly = bi * qp_limbs + jrow;
+  const int pid = level + jrow;
+  const PrimeInfo<double> p = tabs.prime[pid];
+  const int64_t own = int64_t(rank) * G::kM + threadIdx.x * G::kE;
+  KsTw<double, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(false);
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    ExtSourceF64 src{digits + (bi * q_limbs + (d.prime0 - level)) * int64_t(G::kN),
+                     ext64f + (((int64_t(level) * ext_digits + a) * kMaxDigitWidth) * 2) * qp0 + pid, qp0, d.alpha,
+                     LOGN, d.prime0 + d.alpha > f64_end, p.q, p.twice_q};
+    double v[G::kE];
+    tw.forward_from(src, s, p, v);
+#pragma unroll
+    for (int e = 0; e < G::kE; ++e) v[e] = Word<double>::to_lazy(v[e], p.q, p.one_s);
+    store_words(prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN + own, v);
+  }
+}
+
+template <typename T, int LOGN, bool SPLIT = false>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_prepare_rotation(const T* __restrict__ digits, T* __restrict__ prepared, int64_t batch, int q_limbs,
+                   int qp_limbs, int level, int qp0, int order, ChainTables<T> tabs, LevelTables<T> lt,
+                   ChainTables<double> tabs64f, int f64_rows, const TwPair<double>* __restrict__ ext64f,
+                   int ext_digits, int f64_end) {
+  using G = NttGeom<T, LOGN>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int rank = cluster_rank<T, LOGN>();
+  int64_t poly, bi;  // poly over [B, QP_l]
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  if constexpr (SPLIT) {
+    static_assert(sizeof(T) == 8, "FP64 rows exist in int64 chains only");
+    if (jrow < f64_rows) {
+      prepare_unit_f64<LOGN>(reinterpret_cast<const uint64_t*>(digits), reinterpret_cast<uint64_t*>(prepared), batch,
+                             q_limbs, qp_limbs, level, qp0, tabs64f, lt, ext64f, ext_digits, f64_end, bi, jrow,
+                             smem_raw, rank);
+      return;
+    }
+  }
+  prepare_unit<T, LOGN>(digits, prepared, batch, q_limbs, qp_limbs, level, qp0, tabs, lt, bi, jrow, smem_raw, rank);
+}
+
+// The NTT-domain automorphism keeps a CTA's block whole: destination k's
+// CTA is given by the low log C bits of br(k), and the low log C bits of the
+// source's natural index depend only on those.  So the M destinations of
+// CTA `rank` read one contiguous block of M source words, which the CTA
+// copies into shared memory with 16-byte loads before gathering from it.
+template <typename T, int LOGN>
+__device__ __forceinline__ int galois_source_block(int rank, uint32_t galois) {
+  using G = NttGeom<T, LOGN>;
+  return galois_ntt_source(rank * G::kM, LOGN, galois) >> G::kLogM;
+}
+
+template <typename T, int LOGN>
+__device__ __forceinline__ void stage_block(T* dst, const T* src) {
+  using G = NttGeom<T, LOGN>;
+  constexpr int kVec = G::kM * int(sizeof(T)) / 16;
+  static_assert(kVec % G::kThreads == 0, "whole 16-byte vectors per thread");
+#pragma unroll
+  for (int i = threadIdx.x; i < kVec; i += G::kThreads)
+    reinterpret_cast<uint4*>(dst)[i] = __ldg(reinterpret_cast<const uint4*>(src) + i);
+}
+
 // Hoisting stage 2: per rotation step, NTT-domain automorphism of the
 // prepared digits + key inner product + inverse NTT of both accumulators
-// (fhelium/engine/hybrid_keyswitch.py:419-469).
-template <typename T, int LOGN>
+// (fhelium/engine/hybrid_keyswitch.py:419-469).  The automorphism gathers
+// from a staged copy of the source block (galois_source_block) in the NTT
+// working area, which is free until the inverse transform.  SPLIT: the units
+// of the leading f64_rows rows in balanced FP64 arithmetic (the key used as
+// stored, k R, and R removed with N^{-1} R^{-1}), the same canonical outputs.
+template <typename T, int LOGN, bool SPLIT = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
 k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ key, T* __restrict__ acc0,
                           T* __restrict__ acc1, int64_t batch, int qp_limbs, int level, int qp0,
-                          uint32_t galois, int order, ChainTables<T> tabs, LevelTables<T> lt) {
+                          uint32_t galois, int order, ChainTables<T> tabs, LevelTables<T> lt,
+                          ChainTables<double> tabs64f, int f64_rows) {
   using G = NttGeom<T, LOGN>;
-  using W = Word<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* s = reinterpret_cast<T*>(smem_raw);
   const int rank = cluster_rank<T, LOGN>();
   int64_t poly, bi;
   int jrow;
   ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
   (void)bi;
   const int pid = level + jrow;
-  const PrimeInfo<T> p = tabs.prime[pid];
   const int own = rank * G::kM + threadIdx.x * G::kE;
+  const int blk = galois ? galois_source_block<T, LOGN>(rank, galois) : rank;
+  T* staged = reinterpret_cast<T*>(smem_raw);  // the NTT working area, M words
+  if constexpr (SPLIT) {
+    static_assert(sizeof(T) == 8, "FP64 rows exist in int64 chains only");
+    if (jrow < f64_rows) {
+      double* s = reinterpret_cast<double*>(smem_raw);
+      const PrimeInfo<double> p = tabs64f.prime[pid];
+      const double q = p.q, qinv = p.one_s;
+      KsAcc<double, LOGN> acc(s, nullptr, nullptr);
+      KsTw<double, LOGN> tw(smem_raw, tabs64f.tw_fwd + int64_t(pid) * G::kN, tabs64f.tw_inv + int64_t(pid) * G::kN,
+                            rank);
+      for (int a = 0; a < lt.num_digits; ++a) {
+        const DigitDesc d = lt.digits[a];
+        const T* pr = prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN;
+        const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
+        const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
+        if (galois) {
+          __syncthreads();  // the previous digit's gathers are done
+          stage_block<T, LOGN>(staged, pr + int64_t(blk) * G::kM);
+          __syncthreads();
+        }
+#pragma unroll 4
+        for (int e = 0; e < G::kE; ++e) {
+          const T x = galois ? staged[galois_ntt_source(own + e, LOGN, galois) - blk * G::kM] : __ldg(pr + own + e);
+          acc.mac_f64(e, __ull2double_rn(x), __ull2double_rn(__ldg(key0 + e)), __ull2double_rn(__ldg(key1 + e)), q,
+                      qinv);
+        }
+      }
+      if (galois) __syncthreads();  // the inverse transform reuses the working area
+      tw.stage(true);
+      for (int c = 0; c < 2; ++c) {
+        double v[G::kE];
+        acc.get(c, v);
+#pragma unroll
+        for (int e = 0; e < G::kE; ++e) v[e] = Word<double>::reduce_bal(v[e], q, qinv);
+        F64InvEpilogue epi{reinterpret_cast<uint64_t*>(c ? acc1 : acc0) + poly * G::kN, q, p.ninv_rinv,
+                           p.ninv_rinv_s};
+        tw.inverse(s, p, v, epi);
+      }
+      return;
+    }
+  }
+  T* s = reinterpret_cast<T*>(smem_raw);
+  const PrimeInfo<T> p = tabs.prime[pid];
   KsAcc<T, LOGN> acc(s, acc0 + poly * G::kN + own, acc1 + poly * G::kN + own);
   KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
   for (int a = 0; a < lt.num_digits; ++a) {
@@ -993,12 +1111,18 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
     const T* pr = prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN;
     const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN + own;
     const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN + own;
+    if (galois) {
+      __syncthreads();
+      stage_block<T, LOGN>(staged, pr + int64_t(blk) * G::kM);
+      __syncthreads();
+    }
 #pragma unroll 4
     for (int e = 0; e < G::kE; ++e) {
-      const int src = galois ? galois_ntt_source(own + e, LOGN, galois) : own + e;
-      acc.mac(e, __ldg(pr + src), __ldg(key0 + e), __ldg(key1 + e), p);
+      const T x = galois ? staged[galois_ntt_source(own + e, LOGN, galois) - blk * G::kM] : __ldg(pr + own + e);
+      acc.mac(e, x, __ldg(key0 + e), __ldg(key1 + e), p);
     }
   }
+  if (galois) __syncthreads();
   tw.stage(true);
   T v[G::kE];
   acc.get(0, v);
@@ -1305,6 +1429,26 @@ __global__ void k_modmul_probe(T* __restrict__ out, int iters, ChainTables<T> ta
   T acc = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i) acc ^= x[i];
+  out[blockIdx.x * int64_t(blockDim.x) + threadIdx.x] = acc;
+}
+
+// The same for the balanced FP64 product of the rows of primes below 2^42
+// (Word<double>::shoup_bal on the FP64 tables' first prime): the
+// attainable rate of the FP64 rows' modular products.
+template <int CHAINS>
+__global__ void k_modmul_probe_f64(double* __restrict__ out, int iters, ChainTables<double> tabs) {
+  const PrimeInfo<double> p = tabs.prime[0];
+  const TwPair<double> w = tabs.tw_fwd[1];
+  double x[CHAINS];
+#pragma unroll
+  for (int i = 0; i < CHAINS; ++i) x[i] = double((threadIdx.x + i * 977 + blockIdx.x) % 65521u);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < CHAINS; ++i) x[i] = Word<double>::shoup_bal(x[i], w.w, w.wp, p.q);
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int i = 0; i < CHAINS; ++i) acc += x[i];
   out[blockIdx.x * int64_t(blockDim.x) + threadIdx.x] = acc;
 }
 

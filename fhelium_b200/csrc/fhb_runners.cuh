@@ -161,22 +161,48 @@ int run_ks_sum(const Context& c, const void* digits, const uint64_t* key_ptrs, v
                                  level_tables<T>(c, level));
 }
 
+// Rows [0, k) of Q_l (primes below 2^42) of a key-switch kernel at `level`
+// that run in FP64 arithmetic (int64 chains with FP64 tables, N <= 2^16).
+template <typename T, int LOGN>
+int ks_f64_rows(const Context& c, int level) {
+  if constexpr (sizeof(T) == 8 && KsAcc<double, LOGN>::kSmem) {
+    static_assert(KsAcc<double, LOGN>::smem_bytes() == KsAcc<T, LOGN>::smem_bytes(), "one smem size for both");
+    return c.f64_core && c.f64_tables_ok ? std::max(0, std::min(c.num_q - level, c.f64_prime_end - level)) : 0;
+  }
+  return 0;
+}
+
 template <typename T, int LOGN>
 int run_prepare(const Context& c, const void* digits, void* prepared, int64_t batch, int level,
                 cudaStream_t st) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
-  return launch_cluster<T, LOGN>(k_prepare_rotation<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
-                                 (const T*)digits, (T*)prepared, batch, ql, qpl, level, c.qp(), c.ks_order,
-                                 tables<T>(c), level_tables<T>(c, level));
+  const int k = ks_f64_rows<T, LOGN>(c, level);
+  auto launch = [&](auto kern) {
+    return launch_cluster<T, LOGN>(kern, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st, (const T*)digits,
+                                   (T*)prepared, batch, ql, qpl, level, c.qp(), c.ks_order, tables<T>(c),
+                                   level_tables<T>(c, level), c.t64f, k, c.ext64f, c.ext64f_digits, c.f64_prime_end);
+  };
+  if constexpr (sizeof(T) == 8) {
+    if (k > 0) return launch(k_prepare_rotation<T, LOGN, true>);
+  }
+  return launch(k_prepare_rotation<T, LOGN>);
 }
 
 template <typename T, int LOGN>
 int run_apply_prepared(const Context& c, const void* prepared, const void* key, void* acc0, void* acc1,
                        int64_t batch, int level, uint32_t galois, cudaStream_t st) {
   const int ql = c.num_q - level, qpl = ql + c.num_p;
-  return launch_cluster<T, LOGN>(k_apply_prepared_rotation<T, LOGN>, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st,
-                                 (const T*)prepared, (const T*)key, (T*)acc0, (T*)acc1, batch, qpl, level, c.qp(),
-                                 galois == 1 ? 0u : galois, c.ks_order, tables<T>(c), level_tables<T>(c, level));
+  const int k = ks_f64_rows<T, LOGN>(c, level);
+  auto launch = [&](auto kern) {
+    return launch_cluster<T, LOGN>(kern, batch * qpl, KsAcc<T, LOGN>::smem_bytes(), st, (const T*)prepared,
+                                   (const T*)key, (T*)acc0, (T*)acc1, batch, qpl, level, c.qp(),
+                                   galois == 1 ? 0u : galois, c.ks_order, tables<T>(c), level_tables<T>(c, level),
+                                   c.t64f, k);
+  };
+  if constexpr (sizeof(T) == 8) {
+    if (k > 0) return launch(k_apply_prepared_rotation<T, LOGN, true>);
+  }
+  return launch(k_apply_prepared_rotation<T, LOGN>);
 }
 
 // ---- mixed-level item stages (fhb_items.cuh): one cluster per unit ----------

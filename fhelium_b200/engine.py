@@ -101,11 +101,13 @@ class CkksEngine:
 
     @basis_conversion.setter
     def basis_conversion(self, form: str) -> None:
-        """``"auto"`` (the default) picks the tensor-core form where the chain
-        supports it (int64 chains; with the exact FP64 key-switch core it is
-        the faster form) and the CUDA-core form elsewhere."""
+        """``"auto"`` (the default) picks, on int64 chains, the CUDA-core form
+        when the chain's leading Q primes are below 2^42 (the key-switch core
+        then computes their extensions in exact FP64 arithmetic itself, which
+        measured faster than materialising them on the tensor cores) and the
+        tensor-core form otherwise; int32 chains take the CUDA-core form."""
         if form == "auto":
-            if self.dtype == torch.int64:
+            if self.dtype == torch.int64 and not self.ctx.get_tuning(nat.TUNE_F64_CORE):
                 try:
                     self.ctx.set_tuning(nat.TUNE_BASIS_CONVERSION, nat.BASIS_TENSOR_CORES)
                     return

@@ -50,6 +50,9 @@ int fhb_version(void);
  * products, the attainable modular-multiplication rate the NTT-based
  * kernels are measured against.  No counterpart in the reference. */
 int fhb_modmul_probe(const fhb_context* ctx, void* out, int blocks, int iters, fhb_stream stream);
+/* Diagnostic: the same for the balanced FP64 product of the rows of primes
+ * below 2^42 (out: blocks * 256 doubles); -7 when the chain has none. */
+int fhb_modmul_probe_f64(const fhb_context* ctx, void* out, int blocks, int iters, fhb_stream stream);
 const char* fhb_last_error(void);
 
 /* Build the device tables (twiddles with Shoup companions, Montgomery

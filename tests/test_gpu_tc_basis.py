@@ -210,8 +210,9 @@ def test_f64_core_matches_integer_core(family, log_n, level, batch, form):
     arithmetic (the default), in both basis-conversion forms (the CUDA-core
     form computes the extensions in FP64 too, splitting the words of digits
     that hold the wide base prime), against the same core on the integer
-    pipe: relinearisation, fused HMult, rotation and mixed-step rotation
-    (per-item keys) integer-equal, and against the oracle."""
+    pipe: relinearisation, fused HMult, rotation, mixed-step rotation
+    (per-item keys) and hoisted rotations integer-equal, and against the
+    oracle."""
     cfg, eng, orc, rng = _setup(family, log_n, 31)
     eng.basis_conversion = form
     assert eng.ctx.get_tuning(nat.TUNE_F64_CORE) == 1
@@ -229,6 +230,8 @@ def test_f64_core_matches_integer_core(family, log_n, level, batch, form):
         eng.ctx.set_tuning(nat.TUNE_F64_CORE, f64)
         res = [to_np(eng.relinearize(x, rlk).data), to_np(eng.rotate_with_key(c, keys[0]).data),
                to_np(eng.rotate_items_with_keys(c, keys).data)]
+        # hoisted: the prepared digits and every per-step key switch
+        res += [to_np(r.data) for r in eng.rotate_many_with_keys(c, keys[:3])]
         outs[f64] = res
     eng.ctx.set_tuning(nat.TUNE_F64_CORE, 1)
     for got, want in zip(outs[1], outs[0]):
