@@ -110,7 +110,7 @@ SIGNATURES: dict[str, tuple] = {
 }
 
 (TUNE_KS_ORDER, TUNE_NTT_FORWARD_EPT, TUNE_NTT_INVERSE_EPT, TUNE_BASIS_CONVERSION, TUNE_TC_WAIT_US,
- TUNE_TC_TEST_STALL, TUNE_TC_MODDOWN, TUNE_TC_NTT_FUSED, TUNE_F64_CORE) = range(9)
+ TUNE_TC_TEST_STALL, TUNE_TC_MODDOWN, TUNE_TC_NTT_FUSED, TUNE_F64_CORE, TUNE_OVERLAP_CHUNKS) = range(10)
 BASIS_CUDA_CORES, BASIS_TENSOR_CORES = 0, 1
 OP_MONTGOMERY_MUL, OP_ADD_LAZY, OP_SUB_LAZY, OP_ADD_CANONICAL, OP_SUB_CANONICAL, OP_NEGATE = range(6)
 INV_MONTGOMERY, INV_STANDARD_LAZY, INV_STANDARD, INV_CENTERED = range(4)

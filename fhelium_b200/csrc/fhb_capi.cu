@@ -1,6 +1,8 @@
 // extern "C" entry points of libfhb200.so (declared in include/fhb200.h).
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 
 #include "../../include/fhb200.h"
@@ -145,18 +147,20 @@ int modup(const Context& c, const void* comp, void* digits, int64_t batch, int l
   return cuda_status(cudaGetLastError(), "k_modup_digits");
 }
 
+// out_pitch: words between the output's components (0: batch * out rows * N).
 template <typename T>
 int moddown(const Context& c, const void* t0, const void* t1, const void* a0, const void* a1, void* out,
             int64_t batch, int level, uint32_t add0_galois, int rescale, cudaStream_t st,
-            const uint32_t* item_galois = nullptr) {
+            const uint32_t* item_galois = nullptr, int64_t out_pitch = 0) {
   const uint32_t ginv = add0_galois == 1 ? 0u : galois_inverse(add0_galois, c.log_n);
   if constexpr (sizeof(T) == 8) {
     if (c.basis_tc && c.tc_moddown)  // P -> Q conversion on the int8 tensor cores
       return tc_moddown(const_cast<Context&>(c), t0, t1, a0, a1, out, batch, level, ginv, item_galois, rescale, st);
   }
+  if (out_pitch <= 0) out_pitch = batch * (c.num_q - level - (rescale ? 1 : 0)) * c.n();
   k_moddown<T><<<elementwise_grid(batch << c.log_n), 256, 0, st>>>(
       (const T*)t0, (const T*)t1, (const T*)a0, (const T*)a1, (T*)out, batch, c.log_n, level, c.num_q, c.num_p,
-      ginv, item_galois, rescale, tables<T>(c), level_tables<T>(c, level));
+      ginv, item_galois, rescale, tables<T>(c), level_tables<T>(c, level), out_pitch);
   return cuda_status(cudaGetLastError(), "k_moddown");
 }
 
@@ -185,17 +189,21 @@ int add(const Context& c, const void* a, const void* b, void* out, int64_t polys
   return cuda_status(cudaGetLastError(), "k_add_canonical");
 }
 
+// in_pitch: words between the input components (0: batch * rows * N); the
+// output [3, batch, rows, N] is contiguous.
 template <typename T>
 int mul_ntt(const Context& c, const void* a, const void* b, void* out, int64_t batch, int level,
-            cudaStream_t st) {
+            cudaStream_t st, int64_t in_pitch = 0) {
   const int limbs = c.num_q - level;
   constexpr int V = 16 / sizeof(T);
-  if (aligned16(a) && aligned16(b) && aligned16(out))
+  const int64_t out_pitch = batch * limbs * c.n();
+  if (in_pitch <= 0) in_pitch = out_pitch;
+  if (aligned16(a) && aligned16(b) && aligned16(out) && in_pitch % V == 0)
     k_mul_ntt<T, V><<<row_grid(c.n(), V, limbs, batch), kEwThreads, 0, st>>>(
-        (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c));
+        (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c), in_pitch, out_pitch);
   else
     k_mul_ntt<T, 1><<<row_grid(c.n(), 1, limbs, batch), kEwThreads, 0, st>>>(
-        (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c));
+        (const T*)a, (const T*)b, (T*)out, batch, limbs, c.log_n, level, tables<T>(c), in_pitch, out_pitch);
   return cuda_status(cudaGetLastError(), "k_mul_ntt");
 }
 
@@ -409,6 +417,10 @@ int fhb_context_set_tuning(fhb_context* ctx, int param, int value) {
       if (value != 0 && value != 1) return fail(-2, "value must be 0 or 1");
       ctx->impl->f64_core = value;
       return 0;
+    case FHB_TUNE_OVERLAP_CHUNKS:
+      if (value < 1 || value > fhb::kMaxOverlapChunks) return fail(-2, "value must be in 1..8");
+      ctx->impl->overlap_chunks = value;
+      return 0;
     default:
       return fail(-2, "unknown tuning parameter");
   }
@@ -426,6 +438,7 @@ int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value) {
     case FHB_TUNE_TC_MODDOWN: *value = ctx->impl->tc_moddown; return 0;
     case FHB_TUNE_TC_NTT_FUSED: *value = ctx->impl->tc_ntt_fused; return 0;
     case FHB_TUNE_F64_CORE: *value = ctx->impl->f64_core && ctx->impl->f64_tables_ok; return 0;
+    case FHB_TUNE_OVERLAP_CHUNKS: *value = ctx->impl->overlap_chunks; return 0;
     default: return fail(-2, "unknown tuning parameter");
   }
 }
@@ -764,6 +777,110 @@ int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* ke
   return relinearize_tail(c, s, key, ct3, out, batch, level, rescale, st);
 }
 
+// Streams (priorities: [0] highest, [1] and [2] lowest) and events of the
+// chunked fused HMult, created once per context.
+static int overlap_resources(Context& c) {
+  if (c.ov_streams[2]) return 0;
+  int least = 0, greatest = 0;
+  TRY(fhb::cuda_status(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities"));
+  c.ov_events.assign(4 * fhb::kMaxOverlapChunks + 4, nullptr);
+  for (cudaEvent_t& ev : c.ov_events)
+    TRY(fhb::cuda_status(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "overlap event"));
+  const int prio[3] = {greatest, least, least};
+  for (int i = 0; i < 3; ++i)
+    TRY(fhb::cuda_status(cudaStreamCreateWithPriority(&c.ov_streams[i], cudaStreamNonBlocking, prio[i]),
+                         "overlap stream"));
+  return 0;
+}
+
+// HMult + relinearise (+ rescale) of a batch cut into k chunks.  The key-
+// switch core runs in 8-CTA clusters, which leave SMs idle (15 clusters
+// resident on 148 SMs at N = 2^16); the element-wise stages of the other
+// chunks fill them.  Streams: [0] (highest priority) the inverse NTTs of d2
+// and the cores, [1] the tensor products and ModUp digits, [2] the ModDowns:
+//   [1]: tp0 tp1 | mu0 tp2 | mu1 tp3 | mu2 ...   ([1] waits for inv_i before mu_i)
+//   [0]: inv0 inv1 | core0 inv2 | core1 inv3 | core2 ...
+//   [2]: md0 | md1 | ...                          (md_i after core_i)
+// so chunk i+1's ModUp and chunk i-1's ModDown run beside chunk i's core.
+// Every wait is enqueued after the record it waits for.  Results are those
+// of the one-pass call; the chunks' scratch regions are disjoint slices.
+static int multiply_relinearize_chunked(const fhb_context* ctx, const char* a, const char* b, const void* key,
+                                        char* out, char* scratch, int64_t batch, int level, int rescale,
+                                        cudaStream_t st, int k) {
+  const Context& c = *ctx->impl;
+  Context& cm = const_cast<Context&>(c);
+  std::lock_guard<std::mutex> lock(cm.ov_mutex);
+  TRY(overlap_resources(cm));
+  const int limbs = c.num_q - level, out_limbs = limbs - (rescale ? 1 : 0);
+  const int64_t wb = fhb::word_bytes(c), n = c.n();
+  const int64_t in_pitch = batch * limbs * n, out_pitch = batch * out_limbs * n;  // words
+  const int64_t per_ct = fhb_ckks_keyswitch_scratch_bytes(ctx, 1, level);
+  int64_t b0[fhb::kMaxOverlapChunks + 1];
+  const int64_t base = std::max<int64_t>(4, batch / k / 4 * 4);  // whole key-switch groups of four
+  for (int i = 0; i < k; ++i) b0[i] = std::min<int64_t>(batch, i * base);
+  b0[k] = batch;
+  cudaStream_t hi = cm.ov_streams[0], pre = cm.ov_streams[1], post = cm.ov_streams[2];
+  const cudaEvent_t* ev = cm.ov_events.data();
+  enum { kTp = 0, kInv = 1, kMu = 2, kCore = 3 };
+  auto E = [&](int kind, int i) { return ev[4 + 4 * i + kind]; };
+  auto rec = [&](cudaEvent_t e, cudaStream_t s) { return fhb::cuda_status(cudaEventRecord(e, s), "overlap record"); };
+  auto wait = [&](cudaStream_t s, cudaEvent_t e) {
+    return fhb::cuda_status(cudaStreamWaitEvent(s, e, 0), "overlap wait");
+  };
+  auto bc = [&](int i) { return b0[i + 1] - b0[i]; };
+  auto scr = [&](int i) { return fhb::carve(c, scratch + per_ct * b0[i], bc(i), level); };
+  auto tp = [&](int i) -> int {
+    const int64_t off = b0[i] * limbs * n * wb;
+    TRY(FHB_WORD(fhb::mul_ntt, c, a + off, b + off, scr(i).coef, bc(i), level, pre, in_pitch));
+    return rec(E(kTp, i), pre);
+  };
+  auto inv = [&](int i) -> int {
+    const fhb::Scratch s = scr(i);
+    TRY(wait(hi, E(kTp, i)));
+    TRY(fhb::inverse(c, s.coef + 2 * bc(i) * limbs * n * wb, s.t0, bc(i) * limbs, limbs, level, fhb::kInvStandard,
+                     hi));
+    return rec(E(kInv, i), hi);
+  };
+  auto mu = [&](int i) -> int {
+    const fhb::Scratch s = scr(i);
+    TRY(wait(pre, E(kInv, i)));
+    TRY(FHB_WORD(fhb::modup, c, s.t0, s.digits, bc(i), level, 1u, pre));
+    return rec(E(kMu, i), pre);
+  };
+  auto core = [&](int i) -> int {
+    const fhb::Scratch s = scr(i);
+    TRY(wait(hi, E(kMu, i)));
+    TRY(ks_core_from_digits(c, s, key, bc(i), level, hi, nullptr, s.coef));
+    return rec(E(kCore, i), hi);
+  };
+  auto md = [&](int i) -> int {
+    const fhb::Scratch s = scr(i);
+    TRY(wait(post, E(kCore, i)));
+    return FHB_WORD(fhb::moddown, c, s.t0, s.t1, nullptr, nullptr, out + b0[i] * out_limbs * n * wb, bc(i), level,
+                    1u, rescale, post, nullptr, out_pitch);
+  };
+  TRY(rec(ev[0], st));
+  for (cudaStream_t s : {hi, pre, post}) TRY(wait(s, ev[0]));
+  TRY(tp(0));
+  if (k > 1) TRY(tp(1));
+  TRY(inv(0));
+  if (k > 1) TRY(inv(1));
+  TRY(mu(0));
+  if (k > 2) TRY(tp(2));
+  for (int i = 0; i < k; ++i) {
+    TRY(core(i));
+    TRY(md(i));
+    if (i + 1 < k) {
+      TRY(mu(i + 1));
+      if (i + 3 < k) TRY(tp(i + 3));
+    }
+    if (i + 2 < k) TRY(inv(i + 2));
+  }
+  for (int j = 0; j < 3; ++j) TRY(rec(ev[1 + j], cm.ov_streams[j]));
+  for (int j = 0; j < 3; ++j) TRY(wait(st, ev[1 + j]));
+  return 0;
+}
+
 int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const void* b, const void* key, void* out,
                                   void* scratch, int64_t scratch_bytes, int64_t batch, int level, int rescale,
                                   fhb_stream stream) {
@@ -777,6 +894,16 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   TRY(check_scratch(ctx, batch, level, scratch_bytes));
   if (rescale && level + 1 >= c.num_q) return fail(-4, "cannot rescale at the last level");
   const int limbs = c.num_q - level;
+  // a batch of at least two chunks of 8: chunks overlapped (not under stream
+  // capture, and not with ModDown on the tensor cores, which writes whole
+  // batches)
+  const int k = int(std::min<int64_t>(c.overlap_chunks, batch / 8));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  TRY(fhb::cuda_status(cudaStreamIsCapturing(st, &cap), "capture status"));
+  if (k > 1 && cap == cudaStreamCaptureStatusNone && !(c.basis_tc && c.tc_moddown))
+    return multiply_relinearize_chunked(ctx, static_cast<const char*>(a), static_cast<const char*>(b), key,
+                                        static_cast<char*>(out), static_cast<char*>(scratch), batch, level, rescale,
+                                        st, k);
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
   // ct3 = a x b into the scratch (elementwise, every SM), then the

@@ -350,6 +350,9 @@ void destroy_context(Context* c) {
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
   for (void* p : c->allocations) cudaFree(p);
+  for (cudaStream_t s : c->ov_streams)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : c->ov_events) cudaEventDestroy(e);
   cudaSetDevice(prev);
   delete c->tc;
   delete c->tcb;

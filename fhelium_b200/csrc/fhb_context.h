@@ -12,6 +12,7 @@
 namespace fhb {
 
 constexpr int kMaxDigitWidth = 8;  // hybrid digit width bound (= P count)
+constexpr int kMaxOverlapChunks = 8;  // chunks of the overlapped fused HMult
 
 // One active hybrid digit at one level.
 struct DigitDesc {
@@ -114,9 +115,18 @@ struct Context {
   bool f64_tables_ok = false;
   int f64_prime_end = 0;  // Q primes [0, f64_prime_end) are below 2^42 (FP64 rows)
   // tuning: the rows of primes below 2^42 run in FP64 arithmetic (1, default
-  // when the tables exist: standalone NTTs and the tensor-core form's
-  // key-switch core) or on the integer pipe (0)
+  // when the tables exist: the NTTs and the key-switch kernels) or on the
+  // integer pipe (0)
   int f64_core = 1;
+  // tuning: chunks of the fused HMult + relinearise (+ rescale) call whose
+  // element-wise stages run beside the other chunks' key-switch cores (1 =
+  // one pass over the batch); streams and events created on first use and
+  // guarded by ov_mutex: [0] the cores and transforms (highest priority),
+  // [1] tensor products and ModUp digits, [2] ModDown (lowest priority)
+  int overlap_chunks = 4;
+  cudaStream_t ov_streams[3] = {};
+  std::vector<cudaEvent_t> ov_events;
+  std::mutex ov_mutex;
   // tuning: the tensor-core NTT's 16-point pass fused with the adjacent
   // 64-point pass (1) or three separate passes (0, default: faster on B200)
   int tc_ntt_fused = 0;

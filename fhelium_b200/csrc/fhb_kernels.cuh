@@ -289,18 +289,18 @@ __device__ __forceinline__ void ew_store(T* p, const EwVec<T, V>& r) {
 // NTT-domain tensor product only (reference multiply): out [3, B, L, N] lazy.
 template <typename T, int V>
 __global__ void k_mul_ntt(const T* __restrict__ a, const T* __restrict__ b, T* __restrict__ out,
-                          int64_t batch, int limbs, int log_n, int level, ChainTables<T> tabs) {
+                          int64_t batch, int limbs, int log_n, int level, ChainTables<T> tabs, int64_t in_pitch,
+                          int64_t out_pitch) {
   const int64_t n = int64_t(1) << log_n;
   const int64_t k = (int64_t(blockIdx.x) * kEwThreads + threadIdx.x) * V;
   if (k >= n) return;
   const int row = blockIdx.y;
   const PrimeInfo<T>& pp = tabs.prime[level + row];
   const T q = pp.q, ni = pp.neg_inv, tq = pp.twice_q;
-  const int64_t total = batch * limbs * n;
   for (int64_t bi = blockIdx.z; bi < batch; bi += gridDim.z) {
     const int64_t i = (bi * limbs + row) * n + k;
-    const EwVec<T, V> x0 = ew_load<T, V>(a + i), x1 = ew_load<T, V>(a + total + i);
-    const EwVec<T, V> y0 = ew_load<T, V>(b + i), y1 = ew_load<T, V>(b + total + i);
+    const EwVec<T, V> x0 = ew_load<T, V>(a + i), x1 = ew_load<T, V>(a + in_pitch + i);
+    const EwVec<T, V> y0 = ew_load<T, V>(b + i), y1 = ew_load<T, V>(b + in_pitch + i);
     EwVec<T, V> d0, d1, d2;
 #pragma unroll
     for (int e = 0; e < V; ++e) {
@@ -309,8 +309,8 @@ __global__ void k_mul_ntt(const T* __restrict__ a, const T* __restrict__ b, T* _
       d2.v[e] = Word<T>::mont(x1.v[e], y1.v[e], q, ni);
     }
     ew_store<T, V>(out + i, d0);
-    ew_store<T, V>(out + total + i, d1);
-    ew_store<T, V>(out + 2 * total + i, d2);
+    ew_store<T, V>(out + out_pitch + i, d1);
+    ew_store<T, V>(out + 2 * out_pitch + i, d2);
   }
 }
 
@@ -1144,13 +1144,14 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
 // the integers), then (when rescale) the nearest-rounded division by the
 // leading prime of csrc/ops/ckks/cpu/ckks_cpu.cpp:203-262:
 //   out_i = (v_i - v_0) q_0^{-1} + [v_0 > q_0/2]  (mod q_i), i >= 1.
-// out: [2, B, Q_l (- 1 if rescale), N] canonical.
+// out: [2, B, Q_l (- 1 if rescale), N] canonical, components out_pitch
+// words apart (a slice of a larger batch when the pitch exceeds the slice).
 template <typename T>
 __global__ void k_moddown(const T* __restrict__ t0, const T* __restrict__ t1, const T* __restrict__ add0,
                           const T* __restrict__ add1, T* __restrict__ out, int64_t batch, int log_n,
                           int level, int num_q, int num_p, uint32_t add0_ginv,
                           const uint32_t* __restrict__ item_galois, int rescale, ChainTables<T> tabs,
-                          LevelTables<T> lt) {
+                          LevelTables<T> lt, int64_t out_pitch) {
   using W = Word<T>;
   const int64_t n = int64_t(1) << log_n;
   const int q_limbs = num_q - level;
@@ -1187,7 +1188,7 @@ __global__ void k_moddown(const T* __restrict__ t0, const T* __restrict__ t1, co
         }
         e[r] = x;
       }
-      T* o = out + (int64_t(c) * batch + bi) * out_limbs * n;
+      T* o = out + int64_t(c) * out_pitch + bi * out_limbs * n;
       T v0 = 0;
       for (int i = 0; i < q_limbs; ++i) {
         const int pid = level + i;

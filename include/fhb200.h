@@ -102,6 +102,11 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * pipe; default) in the standalone forward / inverse NTT and, with the
  * tensor-core form and N <= 2^16, in the key-switch core; 0 = on the integer
  * pipe.  Reads back 0 where the chain has no such primes.
+ * FHB_TUNE_OVERLAP_CHUNKS (1..8, default 4): fhb_ckks_multiply_relinearize
+ * cuts a batch of at least 16 ciphertexts into at most this many chunks and
+ * runs one chunk's tensor product, ModUp digits and ModDown on low-priority
+ * streams beside another chunk's key-switch core, whose 8-CTA clusters
+ * leave SMs idle; 1 = one pass over the batch.
  * Results do not depend on any of these (stall aside).  No counterpart in the reference
  * (its launch shapes and arithmetic units are fixed). */
 enum fhb_tuning_param {
@@ -113,7 +118,8 @@ enum fhb_tuning_param {
   FHB_TUNE_TC_TEST_STALL = 5,
   FHB_TUNE_TC_MODDOWN = 6,
   FHB_TUNE_TC_NTT_FUSED = 7,
-  FHB_TUNE_F64_CORE = 8
+  FHB_TUNE_F64_CORE = 8,
+  FHB_TUNE_OVERLAP_CHUNKS = 9
 };
 int fhb_context_set_tuning(fhb_context* ctx, int param, int value);
 int fhb_context_get_tuning(const fhb_context* ctx, int param, int* value);

@@ -9,8 +9,10 @@ equal modulo q.
 
 import numpy as np
 import pytest
+import torch
 
 from fhelium_b200 import _native as nat
+from fhelium_b200.config import Preset
 from fhelium_b200.engine import CkksEngine
 from fhelium_b200.values import Ciphertext, RelinearizationKey, RotationKey
 from oracle import oracle as orc_mod
@@ -183,3 +185,28 @@ def test_automorphism_and_add_match_oracle():
     eng.ctx.call("fhb_ckks_automorphism", s.data.data_ptr(), out.data_ptr(), 2, len(rows), 0, g, eng._stream())
     want = orc.automorphism(to_np(s.data).reshape(2, len(rows), cfg.N), 3, rows)
     np.testing.assert_array_equal(to_np(out).reshape(2, len(rows), cfg.N), want)
+
+
+@pytest.mark.parametrize("preset,batch,level", [(Preset.slots8192_scale40_levels7_int64, 26, 1),
+                                                (Preset.slots32768_scale40_levels34_int64, 16, 20)])
+@pytest.mark.parametrize("form", ["cuda_cores", "tensor_cores"])
+def test_fused_hmult_overlapped_chunks_bit_identical(preset, batch, level, form):
+    """fhb_ckks_multiply_relinearize cuts a batch of >= 16 into chunks whose
+    element-wise stages run beside the other chunks' key-switch cores on
+    their own streams: every chunk count gives the one-pass residues (uneven
+    last chunk included)."""
+    eng = CkksEngine(preset, rng_seed=5, basis_conversion=form)
+    rng = np.random.default_rng(batch)
+    msgs = [rng.uniform(-0.05, 0.05, (batch, eng.num_slots)) for _ in range(2)]
+    ca, cb = (eng.coefficient_domain_to_ntt_domain(eng.encrypt_message(m, level=level)) for m in msgs)
+    got = {}
+    try:
+        for chunks in (1, 2, 3, 4):
+            eng.ctx.set_tuning(nat.TUNE_OVERLAP_CHUNKS, chunks)
+            got[chunks] = eng.multiply_relinearize_rescale(ca, cb).data.clone()
+    finally:
+        eng.ctx.set_tuning(nat.TUNE_OVERLAP_CHUNKS, 4)
+    for chunks in (2, 3, 4):
+        assert torch.equal(got[chunks], got[1]), chunks
+    got = np.asarray(eng.decrypt_message(eng.multiply_relinearize_rescale(ca, cb)))
+    assert float(np.abs(got - msgs[0] * msgs[1]).max()) < 3e-5
