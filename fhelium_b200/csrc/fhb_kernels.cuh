@@ -1038,7 +1038,8 @@ __device__ __forceinline__ void stage_block(T* dst, const T* src) {
     reinterpret_cast<uint4*>(dst)[i] = __ldg(reinterpret_cast<const uint4*>(src) + i);
 }
 
-// Hoisting stage 2: per rotation step, NTT-domain automorphism of the
+// Hoisting stage 2 for rings whose key-switch accumulators live outside
+// shared memory (N = 2^17): per rotation step, NTT-domain automorphism of the
 // prepared digits + key inner product + inverse NTT of both accumulators
 // (fhelium/engine/hybrid_keyswitch.py:419-469).  The automorphism gathers
 // from a staged copy of the source block (galois_source_block) in the NTT
@@ -1047,7 +1048,7 @@ __device__ __forceinline__ void stage_block(T* dst, const T* src) {
 // stored, k R, and R removed with N^{-1} R^{-1}), the same canonical outputs.
 template <typename T, int LOGN, bool SPLIT = false>
 __global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
-k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ key, T* __restrict__ acc0,
+k_apply_prepared_rotation_staged(const T* __restrict__ prepared, const T* __restrict__ key, T* __restrict__ acc0,
                           T* __restrict__ acc1, int64_t batch, int qp_limbs, int level, int qp0,
                           uint32_t galois, int order, ChainTables<T> tabs, LevelTables<T> lt,
                           ChainTables<double> tabs64f, int f64_rows) {
@@ -1131,6 +1132,136 @@ k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ 
   acc.get(1, v);
   InvEpilogue<T> e1 = make_inv_epilogue<T>(acc1 + poly * G::kN, p, kInvStandard, false);
   tw.inverse(s, p, v, e1);
+}
+
+// Hoisting stage 2 with the accumulators in registers (rings whose key-
+// switch accumulators fit in shared memory, 8 residues per thread): thread
+// t of CTA `rank` accumulates destinations base + j * threads + t, so a
+// warp covers 32 consecutive destinations, whose sources under the
+// NTT-domain automorphism are a permutation of one aligned group of 32
+// (the low five bits of k become the top bits of br(k), and the odd g
+// permutes them): the gathers, like the key loads, are 256-byte coalesced
+// global loads, with no staging and no barrier in the digit loop.  The sums
+// then pass through shared memory once (padded, conflict-free) into the
+// thread-contiguous layout of the inverse transform.
+template <typename T, int LOGN>
+struct ApplyRegs {
+  using G = NttGeom<T, LOGN>;
+  static constexpr bool kOk = KsAcc<T, LOGN>::kSmem && G::kE == 8;
+};
+
+template <typename T, int LOGN>
+__device__ __forceinline__ void apply_transpose(unsigned char* smem_raw, const T (&a0)[NttGeom<T, LOGN>::kE],
+                                                const T (&a1)[NttGeom<T, LOGN>::kE], T* r1) {
+  using G = NttGeom<T, LOGN>;
+  T* w = reinterpret_cast<T*>(smem_raw);
+#pragma unroll
+  for (int j = 0; j < G::kE; ++j) {
+    w[G::sidx(j * G::kThreads + threadIdx.x)] = a0[j];
+    r1[G::sidx(j * G::kThreads + threadIdx.x)] = a1[j];
+  }
+  __syncthreads();
+}
+
+// Hoisting stage 2: per rotation step, NTT-domain automorphism of the
+// prepared digits + key inner product + inverse NTT of both accumulators
+// (fhelium/engine/hybrid_keyswitch.py:419-469).  SPLIT: the units of the
+// leading f64_rows rows in balanced FP64 arithmetic (the key used as stored,
+// k R, and R removed with N^{-1} R^{-1}), the same canonical outputs.
+template <typename T, int LOGN, bool SPLIT = false>
+__global__ void __launch_bounds__(NttGeom<T, LOGN>::kThreads)
+k_apply_prepared_rotation(const T* __restrict__ prepared, const T* __restrict__ key, T* __restrict__ acc0,
+                          T* __restrict__ acc1, int64_t batch, int qp_limbs, int level, int qp0,
+                          uint32_t galois, int order, ChainTables<T> tabs, LevelTables<T> lt,
+                          ChainTables<double> tabs64f, int f64_rows) {
+  using G = NttGeom<T, LOGN>;
+  static_assert(ApplyRegs<T, LOGN>::kOk, "register accumulators need the shared-memory accumulator room");
+  constexpr int E = G::kE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int rank = cluster_rank<T, LOGN>();
+  int64_t poly, bi;
+  int jrow;
+  ks_work(blockIdx.x / G::kC, qp_limbs, batch, order, poly, bi, jrow);
+  (void)bi;
+  const int pid = level + jrow;
+  const int base = rank * G::kM;
+  // the second sum's transpose area: the key-switch accumulator room
+  T* r1 = reinterpret_cast<T*>(smem_raw) + G::kSmemElems;
+  if constexpr (SPLIT) {
+    static_assert(sizeof(T) == 8, "FP64 rows exist in int64 chains only");
+    if (jrow < f64_rows) {
+      const PrimeInfo<double> p = tabs64f.prime[pid];
+      const double q = p.q, qinv = p.one_s;
+      double a0[E], a1[E];
+#pragma unroll
+      for (int j = 0; j < E; ++j) a0[j] = a1[j] = 0.0;
+      for (int a = 0; a < lt.num_digits; ++a) {
+        const DigitDesc d = lt.digits[a];
+        const T* pr = prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN;
+        const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN;
+        const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN;
+#pragma unroll
+        for (int j = 0; j < E; ++j) {
+          const int dst = base + j * G::kThreads + int(threadIdx.x);
+          const int src = galois ? galois_ntt_source(dst, LOGN, galois) : dst;
+          const double x = __ull2double_rn(__ldg(pr + src));
+          a0[j] += Word<double>::mul_qinv_bal(x, __ull2double_rn(__ldg(key0 + dst)), q, qinv);
+          a1[j] += Word<double>::mul_qinv_bal(x, __ull2double_rn(__ldg(key1 + dst)), q, qinv);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < E; ++j) {
+        a0[j] = Word<double>::reduce_bal(a0[j], q, qinv);
+        a1[j] = Word<double>::reduce_bal(a1[j], q, qinv);
+      }
+      double* w = reinterpret_cast<double*>(smem_raw);
+      double* r1d = reinterpret_cast<double*>(r1);
+      apply_transpose<double, LOGN>(smem_raw, a0, a1, r1d);
+      KsTw<double, LOGN> tw(smem_raw, tabs64f.tw_fwd + int64_t(pid) * G::kN, tabs64f.tw_inv + int64_t(pid) * G::kN,
+                            rank);
+      tw.stage(true);
+      for (int c = 0; c < 2; ++c) {
+        double v[E];
+#pragma unroll
+        for (int e = 0; e < E; ++e) v[e] = (c ? r1d : w)[G::sidx(int(threadIdx.x) * E + e)];
+        if (c == 0) __syncthreads();  // every thread has its values before the transform reuses the area
+        F64InvEpilogue epi{reinterpret_cast<uint64_t*>(c ? acc1 : acc0) + poly * G::kN, q, p.ninv_rinv,
+                           p.ninv_rinv_s};
+        tw.inverse(w, p, v, epi);
+      }
+      return;
+    }
+  }
+  const PrimeInfo<T> p = tabs.prime[pid];
+  T a0[E], a1[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) a0[j] = a1[j] = 0;
+  for (int a = 0; a < lt.num_digits; ++a) {
+    const DigitDesc d = lt.digits[a];
+    const T* pr = prepared + (int64_t(a) * batch * qp_limbs + poly) * G::kN;
+    const T* key0 = key + ((int64_t(d.key_digit) * 2 + 0) * qp0 + pid) * G::kN;
+    const T* key1 = key + ((int64_t(d.key_digit) * 2 + 1) * qp0 + pid) * G::kN;
+#pragma unroll
+    for (int j = 0; j < E; ++j) {
+      const int dst = base + j * G::kThreads + int(threadIdx.x);
+      const int src = galois ? galois_ntt_source(dst, LOGN, galois) : dst;
+      const T x = __ldg(pr + src);
+      a0[j] = csub(a0[j] + Word<T>::mont(x, __ldg(key0 + dst), p.q, p.neg_inv), p.twice_q);
+      a1[j] = csub(a1[j] + Word<T>::mont(x, __ldg(key1 + dst), p.q, p.neg_inv), p.twice_q);
+    }
+  }
+  T* w = reinterpret_cast<T*>(smem_raw);
+  apply_transpose<T, LOGN>(smem_raw, a0, a1, r1);
+  KsTw<T, LOGN> tw(smem_raw, tabs.tw_fwd + int64_t(pid) * G::kN, tabs.tw_inv + int64_t(pid) * G::kN, rank);
+  tw.stage(true);
+  for (int c = 0; c < 2; ++c) {
+    T v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = (c ? r1 : w)[G::sidx(int(threadIdx.x) * E + e)];
+    if (c == 0) __syncthreads();
+    InvEpilogue<T> epi = make_inv_epilogue<T>((c ? acc1 : acc0) + poly * G::kN, p, kInvStandard, false);
+    tw.inverse(w, p, v, epi);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -199,10 +199,17 @@ int run_apply_prepared(const Context& c, const void* prepared, const void* key, 
                                    galois == 1 ? 0u : galois, c.ks_order, tables<T>(c), level_tables<T>(c, level),
                                    c.t64f, k);
   };
-  if constexpr (sizeof(T) == 8) {
-    if (k > 0) return launch(k_apply_prepared_rotation<T, LOGN, true>);
+  if constexpr (ApplyRegs<T, LOGN>::kOk) {
+    if constexpr (sizeof(T) == 8) {
+      if (k > 0) return launch(k_apply_prepared_rotation<T, LOGN, true>);
+    }
+    return launch(k_apply_prepared_rotation<T, LOGN>);
+  } else {
+    if constexpr (sizeof(T) == 8) {
+      if (k > 0) return launch(k_apply_prepared_rotation_staged<T, LOGN, true>);
+    }
+    return launch(k_apply_prepared_rotation_staged<T, LOGN>);
   }
-  return launch(k_apply_prepared_rotation<T, LOGN>);
 }
 
 // ---- mixed-level item stages (fhb_items.cuh): one cluster per unit ----------
