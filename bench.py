@@ -56,8 +56,10 @@ KS_TRAFFIC_BYTES_BATCH32 = 12741399552 + 2934590720  # ncu dram read + write, k_
 # 2.01x the batch-4 capture) and scaled by the ciphertexts processed
 KS_EXT_TRAFFIC_BYTES_BATCH32 = 4 * (3094038784 + 705889536)
 # the CUDA-core form's core with its FP64 rows (k_keyswitch_core_split<false>, the extension computed in FP64 in
-# the core): not yet captured
-KS_SPLIT_TRAFFIC_BYTES_BATCH32 = None
+# the core, the default for this chain): captured at batch 8 (3810678272 + 360568320 bytes; every destination row
+# re-reads its group's digit rows and the group's key rows, so the traffic grows with the batch) and scaled by the
+# ciphertexts processed
+KS_SPLIT_TRAFFIC_BYTES_BATCH32 = 4 * (3810678272 + 360568320)
 # the tensor-core form's core with its FP64 rows (k_keyswitch_core_split<PRE>): captured at batch 8 (3085136640 + 355092224
 # bytes; the key and digit rows are re-read per group of four ciphertexts, so the traffic grows with the batch)
 # and scaled by the ciphertexts processed
