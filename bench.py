@@ -763,7 +763,9 @@ def main() -> int:
     f64_core = bool(eng.ctx.get_tuning(nat.TUNE_F64_CORE))
     # tensor product, inverse NTT of d2, ModUp digits, (tensor-core extension,) core, ModDown; the FP64 rows of
     # the NTT and of the core share their launches with the integer rows
-    launches_per_step = 6 if form == "tensor_cores" else 5
+    # per chunk of the overlapped call (batches of 16 or more run in up to FHB_TUNE_OVERLAP_CHUNKS chunks)
+    chunks_per_step = max(1, min(int(eng.ctx.get_tuning(nat.TUNE_OVERLAP_CHUNKS)), B // 8))
+    launches_per_step = (6 if form == "tensor_cores" else 5) * (chunks_per_step if chunks_per_step > 1 else 1)
 
     # ---- end to end through the public API with host buffers -------------
     host_a = ca.data.cpu().pin_memory()
