@@ -777,6 +777,12 @@ int fhb_ckks_relinearize(const fhb_context* ctx, const void* ct3, const void* ke
   return relinearize_tail(c, s, key, ct3, out, batch, level, rescale, st);
 }
 
+// True when the byte ranges [a, a + na) and [b, b + nb) share a byte.
+static bool ranges_overlap(const void* a, int64_t na, const void* b, int64_t nb) {
+  const auto x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+  return x < y + uintptr_t(nb) && y < x + uintptr_t(na);
+}
+
 // Streams (priorities: [0] highest, [1] and [2] lowest) and events of the
 // chunked fused HMult, created once per context.
 static int overlap_resources(Context& c) {
@@ -900,7 +906,11 @@ int fhb_ckks_multiply_relinearize(const fhb_context* ctx, const void* a, const v
   const int k = int(std::min<int64_t>(c.overlap_chunks, batch / 8));
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   TRY(fhb::cuda_status(cudaStreamIsCapturing(st, &cap), "capture status"));
-  if (k > 1 && cap == cudaStreamCaptureStatusNone && !(c.basis_tc && c.tc_moddown))
+  // a chunk's ModDown must not overwrite input a later chunk still reads
+  const int64_t in_bytes = 2 * batch * limbs * c.n() * fhb::word_bytes(c);
+  const int64_t out_bytes = 2 * batch * (limbs - (rescale ? 1 : 0)) * c.n() * fhb::word_bytes(c);
+  const bool alias = ranges_overlap(out, out_bytes, a, in_bytes) || ranges_overlap(out, out_bytes, b, in_bytes);
+  if (k > 1 && cap == cudaStreamCaptureStatusNone && !(c.basis_tc && c.tc_moddown) && !alias)
     return multiply_relinearize_chunked(ctx, static_cast<const char*>(a), static_cast<const char*>(b), key,
                                         static_cast<char*>(out), static_cast<char*>(scratch), batch, level, rescale,
                                         st, k);
@@ -1009,6 +1019,55 @@ int fhb_ckks_rotate_multi(const fhb_context* ctx, const void* ct, const uint64_t
   return FHB_WORD(fhb::moddown, c, s.t0, s.t1, ct, nullptr, out, batch, level, 1u, 0, st, galois);
 }
 
+// Rotation of a batch cut into k chunks, overlapped like the fused HMult:
+// the ModUp digits (through sigma_g) of every chunk on stream [1] up front,
+// the cores on stream [0] (highest priority), the ModDowns (+ sigma_g(c0)) on
+// stream [2], so the element-wise stages run on the SMs the cores' clusters
+// leave idle.  Results are those of the one-pass call.
+static int rotate_chunked(const fhb_context* ctx, const char* ct, const void* key, char* out, char* scratch,
+                          int64_t batch, int level, uint32_t galois, cudaStream_t st, int k) {
+  const Context& c = *ctx->impl;
+  Context& cm = const_cast<Context&>(c);
+  std::lock_guard<std::mutex> lock(cm.ov_mutex);
+  TRY(overlap_resources(cm));
+  const int limbs = c.num_q - level;
+  const int64_t wb = fhb::word_bytes(c), n = c.n();
+  const int64_t pitch = batch * limbs * n;  // words between the components of ct and out
+  const int64_t per_ct = fhb_ckks_keyswitch_scratch_bytes(ctx, 1, level);
+  int64_t b0[fhb::kMaxOverlapChunks + 1];
+  const int64_t base = std::max<int64_t>(4, batch / k / 4 * 4);
+  for (int i = 0; i < k; ++i) b0[i] = std::min<int64_t>(batch, i * base);
+  b0[k] = batch;
+  cudaStream_t hi = cm.ov_streams[0], pre = cm.ov_streams[1], post = cm.ov_streams[2];
+  const cudaEvent_t* ev = cm.ov_events.data();
+  auto E = [&](int kind, int i) { return ev[4 + 4 * i + kind]; };  // 0: ModUp done, 1: core done
+  auto bc = [&](int i) { return b0[i + 1] - b0[i]; };
+  auto scr = [&](int i) { return fhb::carve(c, scratch + per_ct * b0[i], bc(i), level); };
+  auto rec = [&](cudaEvent_t e, cudaStream_t s) { return fhb::cuda_status(cudaEventRecord(e, s), "overlap record"); };
+  auto wait = [&](cudaStream_t s, cudaEvent_t e) {
+    return fhb::cuda_status(cudaStreamWaitEvent(s, e, 0), "overlap wait");
+  };
+  TRY(rec(ev[0], st));
+  for (cudaStream_t s : {hi, pre, post}) TRY(wait(s, ev[0]));
+  for (int i = 0; i < k; ++i) {
+    TRY(FHB_WORD(fhb::modup, c, ct + (pitch + b0[i] * limbs * n) * wb, scr(i).digits, bc(i), level, galois, pre));
+    TRY(rec(E(0, i), pre));
+  }
+  for (int i = 0; i < k; ++i) {
+    const fhb::Scratch s = scr(i);
+    TRY(wait(hi, E(0, i)));
+    TRY(ks_core_from_digits(c, s, key, bc(i), level, hi));
+    TRY(rec(E(1, i), hi));
+    TRY(wait(post, E(1, i)));
+    const int64_t off = b0[i] * limbs * n * wb;
+    TRY(FHB_WORD(fhb::moddown, c, s.t0, s.t1, ct + off, nullptr, out + off, bc(i), level, galois, 0, post, nullptr,
+                 pitch));
+  }
+  for (int j = 0; j < 3; ++j) TRY(rec(ev[1 + j], cm.ov_streams[j]));
+  for (int j = 0; j < 3; ++j) TRY(wait(st, ev[1 + j]));
+  return 0;
+}
+
 int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, void* out, void* scratch,
                     int64_t scratch_bytes, int64_t batch, int level, uint32_t galois, fhb_stream stream) {
   CTX_OR_FAIL();
@@ -1020,6 +1079,17 @@ int fhb_ckks_rotate(const fhb_context* ctx, const void* ct, const void* key, voi
   TRY(fhb::check_galois(c, galois));
   TRY(check_scratch(ctx, batch, level, scratch_bytes));
   const int limbs = c.num_q - level;
+  // chunks overlapped as in fhb_ckks_multiply_relinearize (not when out
+  // overlaps ct: a chunk's ModDown must not overwrite input another chunk
+  // still reads)
+  const int k = int(std::min<int64_t>(c.overlap_chunks, batch / 8));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  TRY(fhb::cuda_status(cudaStreamIsCapturing(st, &cap), "capture status"));
+  const int64_t ct_bytes = 2 * batch * limbs * c.n() * fhb::word_bytes(c);
+  if (k > 1 && cap == cudaStreamCaptureStatusNone && !(c.basis_tc && c.tc_moddown) &&
+      !ranges_overlap(out, ct_bytes, ct, ct_bytes))
+    return rotate_chunked(ctx, static_cast<const char*>(ct), key, static_cast<char*>(out),
+                          static_cast<char*>(scratch), batch, level, galois, st, k);
   const fhb::Scratch s = fhb::carve(c, scratch, batch, level);
   const int64_t comp = batch * limbs * c.n() * fhb::word_bytes(c);
   TRY(FHB_WORD(fhb::modup, c, static_cast<const char*>(ct) + comp, s.digits, batch, level, galois, st));

@@ -210,3 +210,27 @@ def test_fused_hmult_overlapped_chunks_bit_identical(preset, batch, level, form)
         assert torch.equal(got[chunks], got[1]), chunks
     got = np.asarray(eng.decrypt_message(eng.multiply_relinearize_rescale(ca, cb)))
     assert float(np.abs(got - msgs[0] * msgs[1]).max()) < 3e-5
+
+
+@pytest.mark.parametrize("preset,batch,level", [(Preset.slots8192_scale40_levels7_int64, 26, 1),
+                                                (Preset.slots32768_scale40_levels34_int64, 16, 20)])
+@pytest.mark.parametrize("form", ["cuda_cores", "tensor_cores"])
+def test_rotation_overlapped_chunks_bit_identical(preset, batch, level, form):
+    """fhb_ckks_rotate overlaps its chunks like the fused HMult: every chunk
+    count gives the one-pass residues."""
+    eng = CkksEngine(preset, rng_seed=6, basis_conversion=form)
+    rng = np.random.default_rng(batch + 1)
+    msg = rng.uniform(-0.05, 0.05, (batch, eng.num_slots))
+    ct = eng.encrypt_message(msg, level=level)
+    eng.generate_rotation_keys([3])
+    got = {}
+    try:
+        for chunks in (1, 2, 3, 4):
+            eng.ctx.set_tuning(nat.TUNE_OVERLAP_CHUNKS, chunks)
+            got[chunks] = eng.rotate_by_step(ct, 3).data.clone()
+    finally:
+        eng.ctx.set_tuning(nat.TUNE_OVERLAP_CHUNKS, 4)
+    for chunks in (2, 3, 4):
+        assert torch.equal(got[chunks], got[1]), chunks
+    dec = np.asarray(eng.decrypt_message(eng.rotate_by_step(ct, 3)))
+    assert float(np.abs(dec - np.roll(msg, 3, axis=1)).max()) < 2e-5
