@@ -78,7 +78,9 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * NTT): 8 = radix-8 register passes, 16 = radix-16 passes over half the
  * threads, 0 = the ring's default.
  * FHB_TUNE_BASIS_CONVERSION: 0 = the key switch's exact basis extension on
- * the CUDA cores, fused into the key-switch core (default); 1 = on the int8
+ * the CUDA cores, fused into the key-switch core (the context's default; the
+ * Python engine's "auto" keeps it on chains with FP64 rows and sets 1 on
+ * other int64 chains); 1 = on the int8
  * tensor cores (int64 contexts; fhb_tc_basis_extend), the core then reads the
  * materialised extensions (key-switch scratch grows by
  * fhb_tc_basis_extend_words x 8 bytes).  Setting 1 builds its tables
@@ -98,15 +100,19 @@ int fhb_context_root(const fhb_context* ctx, int prime_id, uint64_t* psi);
  * launches, the 16-point pass fused with the adjacent 64-point pass over each
  * 8192-word span (1), or in three (0, default: faster on B200).
  * FHB_TUNE_F64_CORE (int64 chains): 1 = the rows of primes below 2^42 run in
- * exact FP64 arithmetic (integers held in doubles, products on the FP64
- * pipe; default) in the standalone forward / inverse NTT and, with the
- * tensor-core form and N <= 2^16, in the key-switch core; 0 = on the integer
- * pipe.  Reads back 0 where the chain has no such primes.
+ * exact FP64 arithmetic (integers held in doubles, balanced residues,
+ * products on the FP64 pipe; default) in the forward / inverse NTTs and, for
+ * N <= 2^16, in the key-switch core (both basis-conversion forms), the
+ * hoisted-rotation kernels and the mixed-level items stages; 0 = on the
+ * integer pipe.  Reads back 0 where the chain has no such primes.
  * FHB_TUNE_OVERLAP_CHUNKS (1..8, default 4): fhb_ckks_multiply_relinearize
- * cuts a batch of at least 16 ciphertexts into at most this many chunks and
- * runs one chunk's tensor product, ModUp digits and ModDown on low-priority
- * streams beside another chunk's key-switch core, whose 8-CTA clusters
- * leave SMs idle; 1 = one pass over the batch.
+ * and fhb_ckks_rotate cut a batch of at least 16 ciphertexts into at most
+ * this many chunks and run one chunk's element-wise stages (tensor product,
+ * ModUp digits, ModDown) on low-priority streams beside another chunk's
+ * key-switch core, whose 8-CTA clusters leave SMs idle; 1 = one pass over
+ * the batch.  The streams belong to the context and are forked from and
+ * joined back into the caller's stream.  Under stream capture, or when the
+ * output overlaps an input, the call runs in one pass.
  * Results do not depend on any of these (stall aside).  No counterpart in the reference
  * (its launch shapes and arithmetic units are fixed). */
 enum fhb_tuning_param {
